@@ -1,0 +1,131 @@
+"""Seeded synthetic polygon layers for the join-and-clip workloads.
+
+Layers are returned in the reference's join layout (spatialJoin3.cu:205-212,
+SEQ_Overlay.h:352-380): interleaved FP64 coordinates with each polygon's closing
+vertex stored, ``vnum`` = vertex count including the closing vertex, ``vps`` = its
+inclusive prefix sum.  Star polygons (vertices at sorted uniform angles around a
+centre, counter-clockwise) are simple by construction.
+
+Workloads (all FP64):
+  * ``small_join``: two layers of 2,000 stars, seed 0; vertex count U{8..64};
+    centre U[0,1000]^2; base radius log-normal(ln 5, 0.5); radius = base*U(0.6,1.0).
+  * ``large_pair``: one 1,000,000-vertex star (radius U(0.8,1.2), centre 0,0) and one
+    500,000-vertex star (radius U(0.7,1.3), centre (0.05,0.03)), seed 1.
+  * ``batched_join``: two layers of 200,000 stars, seed 2; vertex count
+    floor(Pareto(alpha=1.5, x_m=4)) capped at 100,000; centres from a 64-component
+    Gaussian mixture over [0,1e5]^2 (sigma 2,000, means U[0,1e5]^2); base radius
+    log-normal(ln 50, 0.7); radius = base*U(0.6,1.0).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+class Layer:
+    """One polygon layer in the reference layout (closing vertex stored)."""
+
+    def __init__(self, xy: np.ndarray, vnum: np.ndarray):
+        self.xy = np.ascontiguousarray(xy, dtype=np.float64).reshape(-1)
+        self.vnum = np.ascontiguousarray(vnum, dtype=np.int32)
+        self.vps = np.cumsum(self.vnum, dtype=np.int64)
+
+    @property
+    def n_polys(self) -> int:
+        return int(self.vnum.shape[0])
+
+    @property
+    def n_vertices(self) -> int:
+        return int(self.vps[-1]) if self.vnum.shape[0] else 0
+
+    def ring(self, i: int) -> np.ndarray:
+        """Open ring (n x 2) of polygon i, closing vertex dropped."""
+        end = int(self.vps[i])
+        start = end - int(self.vnum[i])
+        return self.xy[2 * start:2 * (end - 1)].reshape(-1, 2)
+
+    @staticmethod
+    def from_rings(rings) -> "Layer":
+        vnum = np.array([len(r) + 1 for r in rings], dtype=np.int32)
+        parts = []
+        for r in rings:
+            r = np.asarray(r, dtype=np.float64).reshape(-1, 2)
+            parts.append(np.vstack([r, r[:1]]))
+        xy = np.vstack(parts) if parts else np.zeros((0, 2))
+        return Layer(xy, vnum)
+
+
+def star_layer(rng: np.random.Generator, counts: np.ndarray, centres: np.ndarray,
+               base_r: np.ndarray, rmin: float = 0.6, rmax: float = 1.0) -> Layer:
+    """Vectorised star polygons: per polygon, sorted U[0,2pi) angles and radius
+    base*U(rmin,rmax); the closing vertex repeats the first."""
+    counts = np.asarray(counts, dtype=np.int64)
+    n = counts.shape[0]
+    total = int(counts.sum())
+    pid = np.repeat(np.arange(n), counts)
+    ang = rng.uniform(0.0, 2.0 * np.pi, size=total)
+    # sort angles within each polygon: key = polygon id + angle/(2pi)
+    order = np.lexsort((ang, pid))
+    ang = ang[order]
+    rad = np.repeat(base_r, counts) * rng.uniform(rmin, rmax, size=total)
+    x = np.repeat(centres[:, 0], counts) + rad * np.cos(ang)
+    y = np.repeat(centres[:, 1], counts) + rad * np.sin(ang)
+    # insert the closing vertex after each polygon
+    vnum = counts + 1
+    ends = np.cumsum(vnum)
+    starts = ends - vnum
+    out = np.empty((int(ends[-1]) if n else 0, 2), dtype=np.float64)
+    mask = np.ones(out.shape[0], dtype=bool)
+    mask[ends - 1] = False
+    out[mask, 0] = x
+    out[mask, 1] = y
+    out[ends - 1] = out[starts]
+    return Layer(out, vnum.astype(np.int32))
+
+
+def small_join(seed: int = 0, n: int = 2000):
+    rng = np.random.default_rng(seed)
+    layers = []
+    for _ in range(2):
+        counts = rng.integers(8, 65, size=n)
+        centres = rng.uniform(0.0, 1000.0, size=(n, 2))
+        base = rng.lognormal(np.log(5.0), 0.5, size=n)
+        layers.append(star_layer(rng, counts, centres, base))
+    return layers[0], layers[1]
+
+
+def large_pair(seed: int = 1, n_subject: int = 1_000_000, n_clip: int = 500_000):
+    rng = np.random.default_rng(seed)
+    subj = star_layer(rng, np.array([n_subject]), np.array([[0.0, 0.0]]), np.array([1.0]), 0.8, 1.2)
+    clip = star_layer(rng, np.array([n_clip]), np.array([[0.05, 0.03]]), np.array([1.0]), 0.7, 1.3)
+    return subj, clip
+
+
+def batched_join(seed: int = 2, n: int = 200_000, components: int = 64,
+                 extent: float = 1e5, sigma: float = 2000.0, cap: int = 100_000):
+    rng = np.random.default_rng(seed)
+    means = rng.uniform(0.0, extent, size=(components, 2))
+    layers = []
+    for _ in range(2):
+        counts = np.minimum(np.floor(4.0 * (1.0 + rng.pareto(1.5, size=n))), cap).astype(np.int64)
+        comp = rng.integers(0, components, size=n)
+        centres = means[comp] + rng.normal(0.0, sigma, size=(n, 2))
+        base = rng.lognormal(np.log(50.0), 0.7, size=n)
+        layers.append(star_layer(rng, counts, centres, base))
+    return layers[0], layers[1]
+
+
+def random_star_pairs(seed: int, npairs: int, vmin: int = 3, vmax: int = 40,
+                      spread: float = 1.0):
+    """Independent star pairs near the origin, for clip parity tests."""
+    rng = np.random.default_rng(seed)
+    pairs = []
+    for _ in range(npairs):
+        nv = rng.integers(vmin, vmax + 1, size=2)
+        ps = []
+        for k in range(2):
+            ang = np.sort(rng.uniform(0.0, 2 * np.pi, size=nv[k]))
+            r = rng.uniform(0.3, 1.0, size=nv[k])
+            c = rng.uniform(-0.5 * spread, 0.5 * spread, size=2)
+            ps.append(np.stack([c[0] + r * np.cos(ang), c[1] + r * np.sin(ang)], axis=1))
+        pairs.append((ps[0], ps[1]))
+    return pairs

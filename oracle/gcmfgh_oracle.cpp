@@ -1,0 +1,645 @@
+// gcmfgh_oracle.cpp -- CPU ORACLE. TEST INFRASTRUCTURE ONLY.
+//
+// A plain, sequential C++ restatement of the reference's join-and-clip path, used by
+// tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker.
+// It is never linked into, called by, or shipped with the product library.
+//
+// Parity pin: the clip half is checked against the reference's own sequential GH code
+// compiled from its sources (oracle/_ref/ghclip_ref, see oracle/ref/) on the reference's
+// Fig goldens and on seeded random pairs; tests/golden/ holds the fixtures.
+//
+// What it restates (reference paths are relative to the reference repository root):
+//   * MBR per polygon over all stored vertices (SEQ_Overlay.h:316-344; the closing
+//     vertex is stored and therefore included).
+//   * MBR candidate predicate of the sort-based sweep join (GPU_MBR.h:339-415,
+//     420-539 over keys sorted stably by (value, endpoint index)).  Worked out on
+//     values, the sweep accepts a (base b, overlay o) pair iff
+//       x1o <= x2b && x1b <= x2o && !(x1o == x2b)  and  y1o <= y2b && y1b <= y2o,
+//     i.e. closed overlap except where the overlay starts exactly where the base ends.
+//   * Common MBR and containment candidates (GPU_Join.h:461-508).
+//   * Point-in-polygon crossing parity (GPU_Join.h:882-939, SEQ_Overlay.h:52-61).
+//   * Common-MBR edge filter (GPU_Join.h:562-580, 676-699).
+//   * Segment-intersection refine (GPU_Join.h:363-446).
+//   * Greiner-Hormann clip: GPU intersection phase semantics (gppolyclip_mDIV512.cu:
+//     95-169 classification, 345-371 edge-box filter, 382-415 CMBR edge filter,
+//     463-547 counts, 1461 invalid check) followed by the CPU phases of
+//     GH-CUDA/lib/polyclip.h (computeIntersections :188-268 vertex insertion and
+//     linking, step-1 labels :343-397 as computed on the GPU :1171-1223, chains
+//     :405-451, special cases :474-541, entry/exit :549-655, split pairs :661-714,
+//     crossing candidates :723-734, tracing :743-783, clean-up :791-807) and
+//     polygon.h (pointInPoly :427-448, getNonIntersectionPoint/Vertex :480-512).
+//
+// Arithmetic: every geometric expression is written in the reference's operation
+// order; the Makefile builds with -ffp-contract=off so no a*b+c is fused.
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <algorithm>
+#include <numeric>
+
+namespace {
+
+enum Label : int8_t { NONE = 0, CROSSING, BOUNCING, LEFT_ON, RIGHT_ON, ON_ON, ON_LEFT, ON_RIGHT,
+                      DELAYED_CROSSING, DELAYED_BOUNCING };
+enum EnEx : int8_t { EXIT = 0, ENTRY = 1, NEITHER = 2 };
+enum RelPos { LEFT, RIGHT, IS_P_m, IS_P_p };
+
+struct Pt { double x, y; };
+
+inline double A3(double px, double py, double qx, double qy, double rx, double ry) {
+  // twice the signed area of (P,Q,R): point2D.h:78-80, gppolyclip_mDIV512.cu:16-18
+  return (qx - px) * (ry - py) - (qy - py) * (rx - px);
+}
+
+// Intersection type of [P1,P2] x [Q1,Q2] with alpha (on P) and beta (on Q):
+// gppolyclip_mDIV512.cu:95-169 (== polyclip.h:60-179), including the reference's use
+// of |alpha| when classifying beta in the collinear branch (:157, polyclip.h:156).
+int classify(Pt P1, Pt P2, Pt Q1, Pt Q2, double eps, double& alpha, double& beta) {
+  double AP1 = A3(P1.x, P1.y, Q1.x, Q1.y, Q2.x, Q2.y);
+  double AP2 = A3(P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y);
+  if (std::fabs(AP1 - AP2) > eps) {
+    double AQ1 = A3(Q1.x, Q1.y, P1.x, P1.y, P2.x, P2.y);
+    double AQ2 = A3(Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y);
+    alpha = AP1 / (AP1 - AP2);
+    beta = AQ1 / (AQ1 - AQ2);
+    bool a0 = false, a01 = false, b0 = false, b01 = false;
+    if (alpha > eps && alpha < 1.0 - eps) a01 = true;
+    else if (std::fabs(alpha) <= eps) a0 = true;
+    if (beta > eps && beta < 1.0 - eps) b01 = true;
+    else if (std::fabs(beta) <= eps) b0 = true;
+    if (a01 && b01) return 1;
+    if (a0 && b01) return 2;
+    if (b0 && a01) return 3;
+    if (a0 && b0) return 4;
+  } else if (std::fabs(AP1) < eps) {
+    double dPx = P2.x - P1.x, dPy = P2.y - P1.y;
+    double dQx = Q2.x - Q1.x, dQy = Q2.y - Q1.y;
+    double PQx = Q1.x - P1.x, PQy = Q1.y - P1.y;
+    alpha = (PQx * dPx + PQy * dPy) / (dPx * dPx + dPy * dPy);
+    beta = -(PQx * dQx + PQy * dQy) / (dQx * dQx + dQy * dQy);
+    bool a0 = false, a01 = false, an = false, b0 = false, b01 = false, bn = false;
+    if (alpha > eps && alpha < 1.0 - eps) a01 = true;
+    else if (std::fabs(alpha) <= eps) a0 = true;
+    else an = true;
+    if (beta > eps && beta < 1.0 - eps) b01 = true;
+    else if (std::fabs(alpha) <= eps) b0 = true;
+    else bn = true;
+    if (a01 && b01) return 5;
+    if (an && b01) return 6;
+    if (bn && a01) return 7;
+    if (a0 && b0) return 8;
+  }
+  return 0;
+}
+
+// gppolyclip_mDIV512.cu:345-371
+inline bool edgeBoxesTouch(Pt P1, Pt P2, Pt Q1, Pt Q2) {
+  double minPX = std::min(P1.x, P2.x), maxPX = std::max(P1.x, P2.x);
+  double minPY = std::min(P1.y, P2.y), maxPY = std::max(P1.y, P2.y);
+  double minQX = std::min(Q1.x, Q2.x), maxQX = std::max(Q1.x, Q2.x);
+  double minQY = std::min(Q1.y, Q2.y), maxQY = std::max(Q1.y, Q2.y);
+  if (minPX > maxQX || maxPX < minQX) return false;
+  if (minPY > maxQY || maxPY < minQY) return false;
+  return true;
+}
+
+// gppolyclip_mDIV512.cu:406-413 (same closed test as GPU_Join.h:576-577)
+inline bool edgeTouchesBox(Pt P1, Pt P2, const double* c) {
+  double minX = std::min(P1.x, P2.x), minY = std::min(P1.y, P2.y);
+  double maxX = std::max(P1.x, P2.x), maxY = std::max(P1.y, P2.y);
+  if (minX > c[2] || maxX < c[0]) return false;
+  if (minY > c[3] || maxY < c[1]) return false;
+  return true;
+}
+
+struct Rec { int p, q; double a, b; int type; };
+
+// One polygon ring with explicit links (polygon.h:40-113 vertex/insertVertex).
+struct Ring {
+  std::vector<double> x, y;
+  std::vector<int> next, prev, nbr;
+  std::vector<uint8_t> inter, source;
+  std::vector<int8_t> label, enex;
+  int root = 0;
+  int add(double X, double Y, bool src) {
+    x.push_back(X); y.push_back(Y); next.push_back(-1); prev.push_back(-1); nbr.push_back(-1);
+    inter.push_back(0); source.push_back(src ? 1 : 0); label.push_back(NONE); enex.push_back(NEITHER);
+    return (int)x.size() - 1;
+  }
+  void insertAfter(int v, int after) {   // insertVertex(V, curr) with alpha = -1 (polygon.h:106-112)
+    int c = next[after];
+    next[prev[c]] = v; prev[v] = prev[c]; next[v] = c; prev[c] = v;
+  }
+};
+
+struct Clipper {
+  double eps, epsClean;
+  bool uni, filters;
+  Ring R[2];                                   // R[0] = P, R[1] = Q
+  std::vector<std::vector<Pt>> out;            // result components
+  long long count1P = 0, count1Q = 0, typeCount[9] = {0};
+  int status = 0;                              // 0 ok, 1 invalid, 2 disjoint MBRs
+
+  static void link(Ring& a, int i, Ring& b, int j) {   // polygon.h:89-94
+    a.nbr[i] = j; b.nbr[j] = i; a.inter[i] = 1; b.inter[j] = 1;
+  }
+
+  // polygon.h:427-448 over the ring's current vertices (edges(ALL)).
+  static bool pointInPoly(const Ring& Rg, double Rx, double Ry) {
+    int w = 0;
+    int one = Rg.root;
+    do {
+      int two = Rg.next[one];
+      double P0x = Rg.x[one], P0y = Rg.y[one], P1x = Rg.x[two], P1y = Rg.y[two];
+      if ((P0y < Ry) != (P1y < Ry)) {
+        if (P0x >= Rx) {
+          if (P1x > Rx) w = w + 2 * (P1y > P0y) - 1;
+          else if ((A3(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
+        } else if (P1x > Rx) {
+          if ((A3(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
+        }
+      }
+      one = two;
+    } while (one != Rg.root);
+    return (w % 2) != 0;
+  }
+
+  RelPos oracleRel(int qv, const Ring& P, int p1, int p2, int p3) const {  // polyclip.h:297-326
+    const Ring& Q = R[1];
+    if (P.inter[p1] && P.nbr[p1] == qv) return IS_P_m;
+    if (P.inter[p3] && P.nbr[p3] == qv) return IS_P_p;
+    double s1 = A3(Q.x[qv], Q.y[qv], P.x[p1], P.y[p1], P.x[p2], P.y[p2]);
+    double s2 = A3(Q.x[qv], Q.y[qv], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+    double s3 = A3(P.x[p1], P.y[p1], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+    if (s3 > 0) return (s1 > 0 && s2 > 0) ? LEFT : RIGHT;
+    return (s1 < 0 && s2 < 0) ? RIGHT : LEFT;
+  }
+
+  static Label initialLabel(RelPos m, RelPos p) {   // gppolyclip_mDIV512.cu:237-252
+    auto has = [&](RelPos a, RelPos b) { return (m == a && p == b) || (m == b && p == a); };
+    if (has(LEFT, RIGHT)) return CROSSING;
+    if ((m == LEFT && p == LEFT) || (m == RIGHT && p == RIGHT)) return BOUNCING;
+    if (has(IS_P_p, RIGHT)) return LEFT_ON;
+    if (has(IS_P_p, LEFT)) return RIGHT_ON;
+    if (has(IS_P_p, IS_P_m)) return ON_ON;
+    if (has(IS_P_m, RIGHT)) return ON_LEFT;
+    if (has(IS_P_m, LEFT)) return ON_RIGHT;
+    return NONE;
+  }
+
+  // vertices of ring rg with intersection flag set, starting at `start` (inclusive if it
+  // qualifies), in ring order, evaluated lazily like vertexIterator (polygon.h:194-264).
+  template <class F> void forIntersections(Ring& rg, int start, F f) {
+    int V = start;
+    if (!rg.inter[V]) {
+      do { V = rg.next[V]; } while (!rg.inter[V] && V != start);
+      if (V == start) return;
+    }
+    for (;;) {
+      f(V);
+      do { V = rg.next[V]; } while (!rg.inter[V] && V != start);
+      if (V == start) return;
+    }
+  }
+
+  bool noCrossingVertex(const Ring& rg) const {      // polygon.h:465-475
+    int v = rg.root;
+    do {
+      if (rg.inter[v]) {
+        if (rg.label[v] == CROSSING || rg.label[v] == DELAYED_CROSSING) return false;
+        if (uni && (rg.label[v] == BOUNCING || rg.label[v] == DELAYED_BOUNCING)) return false;
+      }
+      v = rg.next[v];
+    } while (v != rg.root);
+    return true;
+  }
+  static bool allOnOn(const Ring& rg) {                // polygon.h:453-458
+    int v = rg.root;
+    do { if (rg.label[v] != ON_ON) return false; v = rg.next[v]; } while (v != rg.root);
+    return true;
+  }
+  // polygon.h:480-491 (first non-intersection vertex, else a safe edge midpoint)
+  static bool nonIntersectionPoint(const Ring& rg, const Ring& other, double& px, double& py) {
+    int v = rg.root;
+    do { if (!rg.inter[v]) { px = rg.x[v]; py = rg.y[v]; return true; } v = rg.next[v]; } while (v != rg.root);
+    v = rg.root;
+    do {
+      int nb = rg.nbr[v], nx = rg.next[v];
+      if (nb >= 0 && rg.nbr[nx] != other.prev[nb] && rg.nbr[nx] != other.next[nb]) {
+        px = 0.5 * (rg.x[v] + rg.x[nx]); py = 0.5 * (rg.y[v] + rg.y[nx]); return true;
+      }
+      v = rg.next[v];
+    } while (v != rg.root);
+    return false;
+  }
+  // polygon.h:496-512 (may insert a temporary midpoint vertex)
+  static int nonIntersectionVertex(Ring& rg, const Ring& other) {
+    int v = rg.root;
+    do { if (!rg.inter[v]) return v; v = rg.next[v]; } while (v != rg.root);
+    v = rg.root;
+    do {
+      int nb = rg.nbr[v], nx = rg.next[v];
+      if (nb >= 0 && rg.nbr[nx] != other.prev[nb] && rg.nbr[nx] != other.next[nb]) {
+        int t = rg.add(0.5 * (rg.x[v] + rg.x[nx]), 0.5 * (rg.y[v] + rg.y[nx]), false);
+        rg.insertAfter(t, v);
+        return t;
+      }
+      v = rg.next[v];
+    } while (v != rg.root);
+    return -1;
+  }
+  std::vector<Pt> ringPoints(const Ring& rg) const {
+    std::vector<Pt> pts;
+    int v = rg.root;
+    do { pts.push_back({rg.x[v], rg.y[v]}); v = rg.next[v]; } while (v != rg.root);
+    return pts;
+  }
+
+  void run(const double* P, int nP, const double* Q, int nQ) {
+    out.clear();
+    // ---- MBRs and CMBR (ghcuda.cpp:94-125, readShapefile.h:304-330)
+    double mb[2][4];
+    const double* src[2] = {P, Q};
+    int n[2] = {nP, nQ};
+    for (int s = 0; s < 2; ++s) {
+      double mnx = src[s][0], mny = src[s][1], mxx = mnx, mxy = mny;
+      for (int i = 0; i < n[s]; ++i) {
+        double X = src[s][2 * i], Y = src[s][2 * i + 1];
+        if (mxx < X) mxx = X;
+        if (mnx > X) mnx = X;
+        if (mxy < Y) mxy = Y;
+        if (mny > Y) mny = Y;
+      }
+      mb[s][0] = mnx; mb[s][1] = mny; mb[s][2] = mxx; mb[s][3] = mxy;
+    }
+    if (filters) {
+      if (mb[0][0] > mb[1][2] || mb[0][2] < mb[1][0] || mb[0][1] > mb[1][3] || mb[0][3] < mb[1][1]) {
+        status = 2;
+        return;
+      }
+    }
+    double cmbr[4] = {std::max(mb[0][0], mb[1][0]), std::max(mb[0][1], mb[1][1]),
+                      std::min(mb[0][2], mb[1][2]), std::min(mb[0][3], mb[1][3])};
+
+    // ---- intersection records (gpuCountIntersections / polyclip.h:202-268)
+    std::vector<Rec> recs;
+    std::vector<uint8_t> cmP(nP, 1), cmQ(nQ, 1);
+    auto ptP = [&](int i) { return Pt{P[2 * i], P[2 * i + 1]}; };
+    auto ptQ = [&](int i) { return Pt{Q[2 * i], Q[2 * i + 1]}; };
+    if (filters) {
+      for (int i = 0; i < nP; ++i) cmP[i] = edgeTouchesBox(ptP(i), ptP((i + 1) % nP), cmbr);
+      for (int j = 0; j < nQ; ++j) cmQ[j] = edgeTouchesBox(ptQ(j), ptQ((j + 1) % nQ), cmbr);
+    }
+    for (int i = 0; i < nP; ++i) {
+      Pt P1 = ptP(i), P2 = ptP((i + 1) % nP);
+      for (int j = 0; j < nQ; ++j) {
+        Pt Q1 = ptQ(j), Q2 = ptQ((j + 1) % nQ);
+        double a = 0, b = 0;
+        if (filters) {
+          if (!edgeBoxesTouch(P1, P2, Q1, Q2)) continue;
+          int tp = (cmP[i] || cmQ[j]) ? classify(P1, P2, Q1, Q2, eps, a, b) : 0;
+          if (cmP[i] && tp) count1P++;
+          if (cmQ[j]) {
+            double a2, b2;
+            if (classify(Q1, Q2, P1, P2, eps, a2, b2)) count1Q++;
+          }
+          if (tp && cmP[i] && cmQ[j]) { recs.push_back({i, j, a, b, tp}); typeCount[tp]++; }
+        } else {
+          int tp = classify(P1, P2, Q1, Q2, eps, a, b);
+          if (tp) { recs.push_back({i, j, a, b, tp}); typeCount[tp]++; count1P++; count1Q++; }
+        }
+      }
+    }
+    if (filters && count1P != count1Q) { status = 1; return; }   // gppolyclip_mDIV512.cu:1461
+
+    // ---- merged rings: source vertex of each edge followed by inserted vertices in
+    // ascending parameter; equal parameters keep the later-inserted vertex first
+    // (insertVertex, polygon.h:101-113, over the loop order of polyclip.h:202-205).
+    Ring& RP = R[0];
+    Ring& RQ = R[1];
+    RP = Ring(); RQ = Ring();
+    std::vector<std::vector<int>> onP(nP), onQ(nQ);
+    for (int r = 0; r < (int)recs.size(); ++r) {
+      int t = recs[r].type;
+      if (t == 1 || t == 3 || t == 5 || t == 7) onP[recs[r].p].push_back(r);
+      if (t == 1 || t == 2 || t == 5 || t == 6) onQ[recs[r].q].push_back(r);
+    }
+    std::vector<int> srcP(nP), srcQ(nQ), insP(recs.size(), -1), insQ(recs.size(), -1);
+    for (int i = 0; i < nP; ++i) {
+      srcP[i] = RP.add(P[2 * i], P[2 * i + 1], true);
+      std::vector<int>& L = onP[i];
+      std::stable_sort(L.begin(), L.end(), [&](int u, int v) {
+        if (recs[u].a != recs[v].a) return recs[u].a < recs[v].a;
+        return recs[u].q > recs[v].q;
+      });
+      for (int r : L) {
+        const Rec& rc = recs[r];
+        double X, Y;
+        if (rc.type == 1) {
+          Pt P1 = ptP(rc.p), P2 = ptP((rc.p + 1) % nP);
+          X = (1.0 - rc.a) * P1.x + rc.a * P2.x;
+          Y = (1.0 - rc.a) * P1.y + rc.a * P2.y;
+        } else {                                   // copy of Q1 (types 3, 5, 7)
+          X = Q[2 * rc.q]; Y = Q[2 * rc.q + 1];
+        }
+        insP[r] = RP.add(X, Y, false);
+      }
+    }
+    for (int j = 0; j < nQ; ++j) {
+      srcQ[j] = RQ.add(Q[2 * j], Q[2 * j + 1], true);
+      std::vector<int>& L = onQ[j];
+      std::stable_sort(L.begin(), L.end(), [&](int u, int v) {
+        if (recs[u].b != recs[v].b) return recs[u].b < recs[v].b;
+        return recs[u].p > recs[v].p;
+      });
+      for (int r : L) {
+        const Rec& rc = recs[r];
+        double X, Y;
+        if (rc.type == 1) { X = RP.x[insP[r]]; Y = RP.y[insP[r]]; }
+        else { X = P[2 * rc.p]; Y = P[2 * rc.p + 1]; }   // copy of P1 (types 2, 5, 6)
+        insQ[r] = RQ.add(X, Y, false);
+      }
+    }
+    for (Ring* rg : {&RP, &RQ}) {
+      int m = (int)rg->x.size();
+      for (int v = 0; v < m; ++v) { rg->next[v] = (v + 1) % m; rg->prev[v] = (v + m - 1) % m; }
+      rg->root = 0;
+    }
+    // links in the reference's loop order (p outer, q inner): polyclip.h:215-267
+    for (int r = 0; r < (int)recs.size(); ++r) {
+      const Rec& rc = recs[r];
+      switch (rc.type) {
+        case 1: link(RP, insP[r], RQ, insQ[r]); break;
+        case 5: link(RP, srcP[rc.p], RQ, insQ[r]); link(RP, insP[r], RQ, srcQ[rc.q]); break;
+        case 2: case 6: link(RP, srcP[rc.p], RQ, insQ[r]); break;
+        case 3: case 7: link(RP, insP[r], RQ, srcQ[rc.q]); break;
+        case 4: case 8: link(RP, srcP[rc.p], RQ, srcQ[rc.q]); break;
+      }
+    }
+
+    // ---- step 1: initial labels on P, copied to the neighbour on Q
+    forIntersections(RP, RP.root, [&](int I) {
+      int nb = RP.nbr[I];
+      RelPos qm = oracleRel(RQ.prev[nb], RP, RP.prev[I], I, RP.next[I]);
+      RelPos qp = oracleRel(RQ.next[nb], RP, RP.prev[I], I, RP.next[I]);
+      Label L = initialLabel(qm, qp);
+      if (L != NONE) { RP.label[I] = L; RQ.label[nb] = L; }
+    });
+
+    // ---- step 2: intersection chains (polyclip.h:405-451)
+    forIntersections(RP, RP.root, [&](int I0) {
+      if (RP.label[I0] == LEFT_ON || RP.label[I0] == RIGHT_ON) {
+        RelPos x = RP.label[I0] == LEFT_ON ? LEFT : RIGHT;
+        int X = I0, I = I0;
+        do {
+          RP.label[I] = NONE;
+          RQ.label[RP.nbr[I]] = NONE;
+          I = RP.next[I];
+        } while (RP.label[I] == ON_ON);
+        RelPos y = RP.label[I] == ON_LEFT ? LEFT : RIGHT;
+        Label ct = (x != y) ? DELAYED_CROSSING : DELAYED_BOUNCING;
+        RP.label[X] = ct; RP.label[I] = ct;
+        RQ.label[RP.nbr[X]] = ct; RQ.label[RP.nbr[I]] = ct;
+      }
+    });
+
+    // ---- step 3.5: components without crossings (polyclip.h:474-541)
+    bool noInter[2] = {false, false}, ident[2] = {false, false};
+    for (int s = 0; s < 2; ++s) {
+      Ring& A = R[s];
+      Ring& B = R[1 - s];
+      if (noCrossingVertex(A)) {
+        noInter[s] = true;
+        if (allOnOn(A)) ident[s] = true;
+        else {
+          double px = 0, py = 0;
+          nonIntersectionPoint(A, B, px, py);
+          bool inside = pointInPoly(B, px, py);
+          if (inside ^ uni) out.push_back(ringPoints(A));
+        }
+      }
+    }
+    if (ident[0] && ident[1]) out.push_back(ringPoints(RP));
+
+    // ---- step 4: entry/exit flags (polyclip.h:549-655)
+    std::vector<int> split[2], cand[2];
+    for (int s = 0; s < 2; ++s) {
+      if (noInter[s]) continue;
+      Ring& A = R[s];
+      Ring& B = R[1 - s];
+      int V = nonIntersectionVertex(A, B);
+      if (V < 0) continue;
+      int st = ENTRY;
+      if (pointInPoly(B, A.x[V], A.y[V])) st = EXIT;
+      bool first = true;
+      auto toggle = [&]() { st = (st == ENTRY) ? EXIT : ENTRY; };
+      forIntersections(A, V, [&](int I) {
+        if (A.label[I] == CROSSING) { A.enex[I] = st; toggle(); }
+        if (A.label[I] == BOUNCING && ((st == EXIT) ^ uni)) split[s].push_back(I);
+        if (A.label[I] == DELAYED_CROSSING) {
+          A.enex[I] = st;
+          if (first) { if ((st == EXIT) ^ uni) A.label[I] = CROSSING; first = false; }
+          else { if ((st == ENTRY) ^ uni) A.label[I] = CROSSING; first = true; toggle(); }
+        }
+        if (A.label[I] == DELAYED_BOUNCING) {
+          A.enex[I] = st;
+          if (first) { if ((st == EXIT) ^ uni) cand[s].push_back(I); first = false; }
+          else { if ((st == ENTRY) ^ uni) cand[s].push_back(I); first = true; }
+          toggle();
+        }
+      });
+    }
+
+    // ---- step 5: split vertex pairs (polyclip.h:661-714), processed in P ring order
+    {
+      std::vector<uint8_t> inSplitQ(RQ.x.size(), 0);
+      for (int v : split[1]) inSplitQ[v] = 1;
+      std::vector<int> order = split[0];
+      for (int IP : order) {
+        int IQ = RP.nbr[IP];
+        if (IQ < 0 || IQ >= (int)inSplitQ.size() || !inSplitQ[IQ]) continue;
+        int VP = RP.add(RP.x[IP], RP.y[IP], false);
+        int VQ = RQ.add(RQ.x[IQ], RQ.y[IQ], false);
+        double sP = A3(RP.x[RP.prev[IP]], RP.y[RP.prev[IP]], RP.x[IP], RP.y[IP], RP.x[RP.next[IP]], RP.y[RP.next[IP]]);
+        double sQ = A3(RQ.x[RQ.prev[IQ]], RQ.y[RQ.prev[IQ]], RQ.x[IQ], RQ.y[IQ], RQ.x[RQ.next[IQ]], RQ.y[RQ.next[IQ]]);
+        if (sP * sQ > 0) { link(RP, IP, RQ, VQ); link(RP, VP, RQ, IQ); }
+        else link(RP, VP, RQ, VQ);
+        RP.insertAfter(VP, IP);
+        RQ.insertAfter(VQ, IQ);
+        int8_t e1 = uni ? ENTRY : EXIT, e2 = uni ? EXIT : ENTRY;
+        RP.enex[IP] = e1; RP.enex[VP] = e2; RQ.enex[IQ] = e1; RQ.enex[VQ] = e2;
+        RP.label[IP] = CROSSING; RP.label[VP] = CROSSING; RQ.label[IQ] = CROSSING; RQ.label[VQ] = CROSSING;
+      }
+    }
+    // ---- step 6: crossing candidates (polyclip.h:723-734)
+    {
+      std::vector<uint8_t> inCandQ(RQ.x.size(), 0);
+      for (int v : cand[1]) inCandQ[v] = 1;
+      for (int IP : cand[0]) {
+        int IQ = RP.nbr[IP];
+        if (IQ >= 0 && inCandQ[IQ]) { RP.label[IP] = CROSSING; RQ.label[IQ] = CROSSING; }
+      }
+    }
+
+    // ---- tracing (polyclip.h:743-783)
+    {
+      int V0 = RP.root;
+      auto isStart = [&](int v) { return RP.inter[v] && RP.label[v] == CROSSING; };
+      int I = V0;
+      bool have = isStart(I);
+      if (!have) {
+        do { I = RP.next[I]; } while (!isStart(I) && I != V0);
+        have = (I != V0);
+      }
+      // The reference walks until it is back at I; a malformed labelling can make that
+      // walk endless, so it is bounded here and reported as status 3.
+      long long budget = 4 * (long long)(RP.x.size() + RQ.x.size()) + 16;
+      while (have) {
+        std::vector<Pt> comp;
+        int side = 0, V = I;
+        RP.inter[V] = 0;
+        do {
+          if (--budget < 0) { status = 3; out.clear(); return; }
+          Ring* cur = &R[side];
+          int st = cur->enex[V];
+          if (st == ENTRY) st = EXIT; else if (st == EXIT) st = ENTRY;
+          do {
+            if (--budget < 0) { status = 3; out.clear(); return; }
+            if ((st == EXIT) ^ uni) V = cur->next[V]; else V = cur->prev[V];
+            cur->inter[V] = 0;
+            comp.push_back({cur->x[V], cur->y[V]});
+          } while (!(cur->enex[V] == st) && !(side == 0 && V == I));
+          if (!(side == 0 && V == I)) {
+            if (cur->nbr[V] < 0) { status = 3; out.clear(); return; }
+            V = cur->nbr[V];
+            side = 1 - side;
+            R[side].inter[V] = 0;
+          }
+        } while (!(side == 0 && V == I));
+        out.push_back(comp);
+        // advance the CROSSING_INTERSECTION iterator from I
+        do { I = RP.next[I]; } while (!isStart(I) && I != V0);
+        have = (I != V0);
+      }
+    }
+
+    // ---- clean-up (polyclip.h:791-807): drop the root while it is collinear, then
+    // one forward pass over the remaining vertices.
+    for (auto& comp : out) {
+      int m = (int)comp.size();
+      if (m == 0) continue;
+      std::vector<int> nx(m), pv(m);
+      for (int i = 0; i < m; ++i) { nx[i] = (i + 1) % m; pv[i] = (i + m - 1) % m; }
+      int root = 0, alive = m;
+      auto area = [&](int v) {
+        return std::fabs(A3(comp[pv[v]].x, comp[pv[v]].y, comp[v].x, comp[v].y, comp[nx[v]].x, comp[nx[v]].y));
+      };
+      auto remove = [&](int v) {
+        if (root == v) { root = nx[v]; if (nx[root] == root) root = -1; }
+        nx[pv[v]] = nx[v]; pv[nx[v]] = pv[v];
+        --alive;
+      };
+      while (root >= 0 && area(root) < epsClean) remove(root);
+      std::vector<Pt> res;
+      if (root >= 0) {
+        int start = root, v = root;
+        do {
+          int nxt = nx[v];
+          if (area(v) < epsClean) remove(v);
+          v = nxt;
+        } while (v != start && root >= 0);
+        if (root >= 0) {
+          v = root;
+          do { res.push_back(comp[v]); v = nx[v]; } while (v != root);
+        }
+      }
+      comp.swap(res);
+    }
+    std::vector<std::vector<Pt>> kept;
+    for (auto& c : out) if (!c.empty()) kept.push_back(std::move(c));
+    out.swap(kept);
+  }
+};
+
+// ------------------------------------------------------------------ result store
+struct Store {
+  std::vector<int32_t> status, ncomp;
+  std::vector<int64_t> count1, nrec;
+  std::vector<int32_t> compSize;
+  std::vector<double> xy;
+  void clear() { status.clear(); ncomp.clear(); count1.clear(); nrec.clear(); compSize.clear(); xy.clear(); }
+} g_store;
+
+void storeResult(const Clipper& c) {
+  g_store.status.push_back(c.status);
+  g_store.ncomp.push_back((int32_t)c.out.size());
+  g_store.count1.push_back(c.count1P);
+  long long nr = 0;
+  for (int t = 1; t < 9; ++t) nr += c.typeCount[t];
+  g_store.nrec.push_back(nr);
+  for (auto& comp : c.out) {
+    g_store.compSize.push_back((int32_t)comp.size());
+    for (auto& p : comp) { g_store.xy.push_back(p.x); g_store.xy.push_back(p.y); }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Clip one pair.  P, Q: open rings (no closing vertex), interleaved x,y.
+// flags bit0: union instead of intersection.  bit1: GPU-path semantics (CMBR and edge-box
+// filters, P/Q count cross-check); without it, the reference's CPU path (every edge pair).
+int orc_clip_pair(const double* P, int nP, const double* Q, int nQ, double eps, double epsClean, int flags) {
+  g_store.clear();
+  Clipper c;
+  c.eps = eps; c.epsClean = epsClean; c.uni = flags & 1; c.filters = (flags >> 1) & 1;
+  c.run(P, nP, Q, nQ);
+  storeResult(c);
+  return c.status;
+}
+
+// Clip a batch of layer pairs with the GCMF-GH swap rule (ghcuda.cpp:64-91): the
+// polygon with more vertices becomes P, ties keep the base polygon as P.
+// Layers use the reference's join layout: interleaved coordinates with the closing
+// vertex stored, vnum counts it, vps is the inclusive prefix sum of vnum.
+int64_t orc_clip_batch(const double* bxy, const int32_t* bvnum, const int64_t* bvps,
+                       const double* oxy, const int32_t* ovnum, const int64_t* ovps,
+                       const int32_t* pid, const int32_t* qid, int64_t npairs,
+                       double eps, double epsClean, int flags) {
+  g_store.clear();
+  for (int64_t k = 0; k < npairs; ++k) {
+    int b = pid[k], o = qid[k];
+    int nb = bvnum[b] - 1, no = ovnum[o] - 1;
+    const double* pb = bxy + 2 * (bvps[b] - bvnum[b]);
+    const double* po = oxy + 2 * (ovps[o] - ovnum[o]);
+    Clipper c;
+    c.eps = eps; c.epsClean = epsClean; c.uni = flags & 1; c.filters = (flags >> 1) & 1;
+    if (nb < no) c.run(po, no, pb, nb);
+    else c.run(pb, nb, po, no);
+    storeResult(c);
+  }
+  return (int64_t)g_store.status.size();
+}
+
+int64_t orc_result_sizes(int64_t* out3) {   // npairs, ncomponents, nvertices
+  out3[0] = (int64_t)g_store.status.size();
+  out3[1] = (int64_t)g_store.compSize.size();
+  out3[2] = (int64_t)g_store.xy.size() / 2;
+  return out3[0];
+}
+
+void orc_result_copy(int32_t* status, int32_t* ncomp, int64_t* count1, int64_t* nrec,
+                     int32_t* compSize, double* xy) {
+  if (status) std::copy(g_store.status.begin(), g_store.status.end(), status);
+  if (ncomp) std::copy(g_store.ncomp.begin(), g_store.ncomp.end(), ncomp);
+  if (count1) std::copy(g_store.count1.begin(), g_store.count1.end(), count1);
+  if (nrec) std::copy(g_store.nrec.begin(), g_store.nrec.end(), nrec);
+  if (compSize) std::copy(g_store.compSize.begin(), g_store.compSize.end(), compSize);
+  if (xy) std::copy(g_store.xy.begin(), g_store.xy.end(), xy);
+}
+
+}  // extern "C"

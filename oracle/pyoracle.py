@@ -1,0 +1,169 @@
+"""ctypes front end of the CPU oracle (oracle/gcmfgh_oracle.cpp) and of the reference's
+own sequential clipper binary (oracle/_ref/ghclip_ref).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg, as the checker.  The product library never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgcmfgh_oracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "ghclip_ref")
+
+FLAG_UNION = 1
+FLAG_GPU_SEMANTICS = 2
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        d, i32, i64 = ctypes.c_double, ctypes.c_int, ctypes.c_int64
+        vp = ctypes.c_void_p
+        L.orc_clip_pair.argtypes = [vp, i32, vp, i32, d, d, i32]
+        L.orc_clip_pair.restype = i32
+        L.orc_clip_batch.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i64, d, d, i32]
+        L.orc_clip_batch.restype = i64
+        L.orc_result_sizes.argtypes = [vp]
+        L.orc_result_sizes.restype = i64
+        L.orc_result_copy.argtypes = [vp] * 6
+        L.orc_result_copy.restype = None
+        for name in ("orc_join",):
+            if hasattr(L, name):
+                pass
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class ClipResult:
+    """Per-pair status, component lists and intersection counts."""
+
+    def __init__(self, status, ncomp, count1, nrec, comp_size, xy):
+        self.status = status
+        self.ncomp = ncomp
+        self.count1 = count1
+        self.nrec = nrec
+        self.comp_size = comp_size
+        self.xy = xy
+        self.comp_off = np.concatenate([[0], np.cumsum(comp_size, dtype=np.int64)])
+        self.pair_comp_off = np.concatenate([[0], np.cumsum(ncomp, dtype=np.int64)])
+
+    def components(self, k):
+        out = []
+        for c in range(self.pair_comp_off[k], self.pair_comp_off[k + 1]):
+            a, b = self.comp_off[c], self.comp_off[c + 1]
+            out.append(self.xy[2 * a:2 * b].reshape(-1, 2))
+        return out
+
+
+def _collect():
+    L = lib()
+    sz = np.zeros(3, dtype=np.int64)
+    L.orc_result_sizes(_p(sz))
+    npairs, ncomp, nv = (int(v) for v in sz)
+    status = np.zeros(npairs, np.int32)
+    ncmp = np.zeros(npairs, np.int32)
+    count1 = np.zeros(npairs, np.int64)
+    nrec = np.zeros(npairs, np.int64)
+    csz = np.zeros(ncomp, np.int32)
+    xy = np.zeros(2 * nv, np.float64)
+    L.orc_result_copy(_p(status), _p(ncmp), _p(count1), _p(nrec), _p(csz), _p(xy))
+    return ClipResult(status, ncmp, count1, nrec, csz, xy)
+
+
+def clip_pair(P, Q, eps=1e-7, eps_clean=None, union=False, gpu_semantics=True):
+    P = np.ascontiguousarray(P, np.float64).reshape(-1)
+    Q = np.ascontiguousarray(Q, np.float64).reshape(-1)
+    flags = (FLAG_UNION if union else 0) | (FLAG_GPU_SEMANTICS if gpu_semantics else 0)
+    lib().orc_clip_pair(_p(P), len(P) // 2, _p(Q), len(Q) // 2, eps,
+                        eps if eps_clean is None else eps_clean, flags)
+    return _collect()
+
+
+def clip_batch(base, overlay, pid, qid, eps=1e-7, eps_clean=None, union=False,
+               gpu_semantics=True):
+    """Clip the listed (base, overlay) pairs with the reference's swap rule."""
+    pid = np.ascontiguousarray(pid, np.int32)
+    qid = np.ascontiguousarray(qid, np.int32)
+    flags = (FLAG_UNION if union else 0) | (FLAG_GPU_SEMANTICS if gpu_semantics else 0)
+    lib().orc_clip_batch(_p(base.xy), _p(base.vnum), _p(base.vps),
+                         _p(overlay.xy), _p(overlay.vnum), _p(overlay.vps),
+                         _p(pid), _p(qid), len(pid), eps,
+                         eps if eps_clean is None else eps_clean, flags)
+    return _collect()
+
+
+# ---------------------------------------------------------------- reference binary
+
+def ref_available() -> bool:
+    return os.path.exists(REF_BIN)
+
+
+def write_pair_batch(path, pairs):
+    with open(path, "wb") as f:
+        f.write(struct.pack("<q", len(pairs)))
+        for P, Q in pairs:
+            P = np.ascontiguousarray(P, np.float64).reshape(-1, 2)
+            Q = np.ascontiguousarray(Q, np.float64).reshape(-1, 2)
+            f.write(struct.pack("<ii", len(P), len(Q)))
+            f.write(P.tobytes())
+            f.write(Q.tobytes())
+
+
+def read_result_batch(path):
+    data = open(path, "rb").read()
+    off = 0
+    (n,) = struct.unpack_from("<q", data, off)
+    off += 8
+    res = []
+    for _ in range(n):
+        (nc,) = struct.unpack_from("<i", data, off)
+        off += 4
+        comps = []
+        for _ in range(nc):
+            (nv,) = struct.unpack_from("<i", data, off)
+            off += 4
+            comps.append(np.frombuffer(data, np.float64, 2 * nv, off).reshape(-1, 2).copy())
+            off += 16 * nv
+        res.append(comps)
+    return res
+
+
+def ref_clip_pairs(pairs, union=False):
+    """Run the reference's own sequential clipper (built from its sources) on pairs."""
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        fout = os.path.join(td, "out.bin")
+        write_pair_batch(fin, pairs)
+        cmd = [REF_BIN, "batch", fin, fout] + (["union"] if union else [])
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+        return read_result_batch(fout)
+
+
+def ref_time_pairs(pairs, reps=1, union=False):
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        write_pair_batch(fin, pairs)
+        cmd = [REF_BIN, "time", fin, str(reps)] + (["union"] if union else [])
+        out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout.split()
+        return float(out[0]), int(out[1])
