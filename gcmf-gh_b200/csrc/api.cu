@@ -1,0 +1,415 @@
+// api.cu -- the C ABI (include/gcmfgh.h): contexts, device arenas, argument checks and
+// result export.  The reference's entry points exit the process on errors
+// (GPU_Manage.h:25-44, ghcuda.cpp:109-116); these return a status instead.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include "common.cuh"
+#include "engine.cuh"
+#include "prims.cuh"
+#include "../../include/gcmfgh.h"
+
+namespace gcmfgh {
+
+void* Arena::take(size_t bytes) {
+  bytes = (bytes + 255) & ~size_t(255);
+  while (cur_ < chunks_.size()) {
+    Chunk& c = chunks_[cur_];
+    if (c.off + bytes <= c.cap) {
+      void* p = c.base + c.off;
+      c.off += bytes;
+      return p;
+    }
+    ++cur_;
+  }
+  size_t last = chunks_.empty() ? 0 : chunks_.back().cap;
+  size_t cap = bytes > 2 * last ? bytes : 2 * last;
+  if (cap < (size_t(64) << 20)) cap = size_t(64) << 20;
+  char* p = nullptr;
+  if (cudaMalloc(&p, cap) != cudaSuccess) {
+    cudaGetLastError();
+    cap = bytes;                                  // retry with the exact size
+    if (cudaMalloc(&p, cap) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  }
+  chunks_.push_back({p, cap, bytes});
+  cur_ = chunks_.size() - 1;
+  return p;
+}
+
+void Arena::release() {
+  for (auto& c : chunks_) cudaFree(c.base);
+  chunks_.clear();
+  cur_ = 0;
+}
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__global__ void clip_stats_kernel(const int32_t* __restrict__ status, int64_t n, unsigned long long* out) {
+  int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  unsigned long long c[3] = {0, 0, 0};
+  if (i < n) {
+    int s = status[i];
+    if (s == 1) c[0] = 1;
+    if (s == 2) c[1] = 1;
+    if (s == 3) c[2] = 1;
+  }
+  for (int j = 0; j < 3; ++j) {
+    unsigned long long v = warp_sum(c[j]);
+    if (lane_id() == 0 && v) atomicAdd(&out[j], v);
+  }
+}
+
+}  // namespace
+}  // namespace gcmfgh
+
+using namespace gcmfgh;
+
+struct gcmfgh_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  Arena join_arena, clip_arena, layer_arena, pair_arena;
+  int* d_err = nullptr;
+  int64_t* h_scratch = nullptr;   // pinned
+  unsigned long long* d_stats = nullptr;
+  JoinDev join;
+  bool have_join = false;
+  ClipDev clip;
+  bool have_clip = false;
+  ClipParams prm;
+  int last_err = 0;
+  const double* join_b = nullptr;
+  const double* join_o = nullptr;
+  int64_t join_nb = 0, join_no = 0;
+};
+
+namespace {
+
+gcmfgh_status to_status(int st) { return static_cast<gcmfgh_status>(st); }
+
+bool layer_ok(const gcmfgh_layer* L) {
+  if (!L || L->n_polys < 0) return false;
+  if (L->n_polys == 0) return true;
+  if (!L->coords || !L->vnum || !L->vps) return false;
+  if (reinterpret_cast<uintptr_t>(L->coords) % 16 != 0) return false;   // 128-bit vertex loads
+  return true;
+}
+
+LayerDev to_dev(const gcmfgh_layer* L) { return LayerDev{L->coords, L->vnum, L->vps, L->n_polys}; }
+
+gcmfgh_status finish(gcmfgh_ctx* c, int st) {
+  if (st != ST_OK) {
+    cudaStreamSynchronize(c->stream);
+    cudaError_t e = cudaGetLastError();
+    (void)e;
+    return to_status(st);
+  }
+  if (cudaMemcpyAsync(c->h_scratch + 60, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+    return GCMFGH_CUDA_ERROR;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  if (cudaGetLastError() != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  int e = *reinterpret_cast<int*>(c->h_scratch + 60);
+  c->last_err = e;
+  if (e == DEV_TIMEOUT) return GCMFGH_DEVICE_ERROR;
+  return GCMFGH_OK;
+}
+
+gcmfgh_status clip_info(gcmfgh_ctx* c, gcmfgh_clip_info* info) {
+  if (!info) return GCMFGH_OK;
+  info->n_pairs = c->clip.n_pairs;
+  info->n_components = c->clip.n_components;
+  info->n_vertices = c->clip.n_vertices;
+  info->n_invalid = info->n_disjoint = info->n_error = 0;
+  if (c->clip.n_pairs > 0) {
+    cudaMemsetAsync(c->d_stats, 0, 3 * sizeof(unsigned long long), c->stream);
+    clip_stats_kernel<<<(unsigned)((c->clip.n_pairs + kThreads - 1) / kThreads), kThreads, 0, c->stream>>>(
+        c->clip.status, c->clip.n_pairs, c->d_stats);
+    cudaMemcpyAsync(c->h_scratch, c->d_stats, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GCMFGH_CUDA_ERROR;
+    info->n_invalid = c->h_scratch[0];
+    info->n_disjoint = c->h_scratch[1];
+    info->n_error = c->h_scratch[2];
+  }
+  return GCMFGH_OK;
+}
+
+gcmfgh_status run_clip_ctx(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o,
+                           const int32_t* pid, const int32_t* qid, int64_t n, gcmfgh_clip_info* info) {
+  c->clip_arena.reset();
+  c->have_clip = false;
+  cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  int st = run_clip(to_dev(b), to_dev(o), pid, qid, n, c->prm, c->clip_arena, c->clip, c->d_err,
+                    c->h_scratch, c->stream);
+  gcmfgh_status r = finish(c, st);
+  if (r != GCMFGH_OK) return r;
+  c->have_clip = true;
+  return clip_info(c, info);
+}
+
+struct FieldRef { const void* p; int64_t count; int esize; };
+
+FieldRef join_field(const gcmfgh_ctx* c, int f) {
+  const JoinDev& J = c->join;
+  int64_t K = J.n_pairs;
+  switch (f) {
+    case GCMF_PAIR_BASE: return {J.b, K, 4};
+    case GCMF_PAIR_OVERLAY: return {J.o, K, 4};
+    case GCMF_CMBR: return {J.cmbr, 4 * K, 8};
+    case GCMF_PIP_TYPE: return {J.pip_type, K, 1};
+    case GCMF_PIP_FLAG: return {J.pip_flag, K, 1};
+    case GCMF_JOIN_FLAG: return {J.join_flag, K, 1};
+    case GCMF_BASE_EDGES: return {J.bE, K, 4};
+    case GCMF_OVERLAY_EDGES: return {J.oE, K, 4};
+    case GCMF_SEG_FLAG: return {J.seg_flag, K, 1};
+    case GCMF_CLIP_FLAG: return {J.clip, K, 1};
+    case GCMF_CLIP_BASE: return {J.clip_b, J.n_clip, 4};
+    case GCMF_CLIP_OVERLAY: return {J.clip_o, J.n_clip, 4};
+    case GCMF_MBR_BASE: return {J.mbr_b, J.mbr_b ? 4 * c->join_nb : 0, 8};
+    case GCMF_MBR_OVERLAY: return {J.mbr_o, J.mbr_o ? 4 * c->join_no : 0, 8};
+    case GCMF_VALID_BASE: return {J.valid_b, J.valid_b ? c->join_nb : 0, 1};
+    case GCMF_VALID_OVERLAY: return {J.valid_o, J.valid_o ? c->join_no : 0, 1};
+  }
+  return {nullptr, -1, 0};
+}
+
+FieldRef clip_field(const gcmfgh_ctx* c, int f) {
+  const ClipDev& C = c->clip;
+  switch (f) {
+    case GH_STATUS: return {C.status, C.n_pairs, 4};
+    case GH_NCOMP: return {C.ncomp, C.n_pairs, 4};
+    case GH_COMP_OFFSET: return {C.comp_off, C.n_pairs, 8};
+    case GH_COUNT1: return {C.count1, C.n_pairs, 8};
+    case GH_COMP_SIZE: return {C.comp_size, C.n_components, 4};
+    case GH_VERT_OFFSET: return {C.vert_off, C.n_pairs, 8};
+    case GH_XY: return {C.xy, 2 * C.n_vertices, 8};
+    case GH_SWAPPED: return {C.swapped, C.n_pairs, 4};
+  }
+  return {nullptr, -1, 0};
+}
+
+gcmfgh_status copy_field(gcmfgh_ctx* c, FieldRef r, void* dst, int64_t cap, int on_dev, int64_t* bytes) {
+  if (r.count < 0) return GCMFGH_INVALID_ARGUMENT;
+  int64_t nb = r.count * r.esize;
+  if (bytes) *bytes = nb;
+  if (!dst) return GCMFGH_OK;
+  if (cap < nb) return GCMFGH_CAPACITY;
+  if (nb == 0) return GCMFGH_OK;
+  if (!r.p) return GCMFGH_NOT_READY;
+  cudaError_t e = cudaMemcpyAsync(dst, r.p, (size_t)nb, on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                  c->stream);
+  if (e != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  return GCMFGH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gcmfgh_status_string(gcmfgh_status s) {
+  switch (s) {
+    case GCMFGH_OK: return "ok";
+    case GCMFGH_INVALID_ARGUMENT: return "invalid argument";
+    case GCMFGH_CUDA_ERROR: return "CUDA error";
+    case GCMFGH_OUT_OF_MEMORY: return "out of device memory";
+    case GCMFGH_DEVICE_ERROR: return "device-side error";
+    case GCMFGH_NOT_READY: return "no result yet";
+    case GCMFGH_CAPACITY: return "destination too small";
+    case GCMFGH_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+gcmfgh_status gcmfgh_create(int device, gcmfgh_ctx** out) {
+  if (!out) return GCMFGH_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return GCMFGH_NO_DEVICE; }
+  if (device < 0 || device >= n) return GCMFGH_INVALID_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  gcmfgh_ctx* c = new (std::nothrow) gcmfgh_ctx();
+  if (!c) return GCMFGH_OUT_OF_MEMORY;
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->d_err, 64) != cudaSuccess ||
+      cudaMalloc(&c->d_stats, 64) != cudaSuccess ||
+      cudaMallocHost(&c->h_scratch, 64 * sizeof(int64_t)) != cudaSuccess) {
+    gcmfgh_destroy(c);
+    return GCMFGH_CUDA_ERROR;
+  }
+  c->stream = c->own;
+  cudaMemset(c->d_err, 0, 64);
+  *out = c;
+  return GCMFGH_OK;
+}
+
+gcmfgh_status gcmfgh_destroy(gcmfgh_ctx* c) {
+  if (!c) return GCMFGH_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->join_arena.release();
+  c->clip_arena.release();
+  c->layer_arena.release();
+  c->pair_arena.release();
+  if (c->d_err) cudaFree(c->d_err);
+  if (c->d_stats) cudaFree(c->d_stats);
+  if (c->h_scratch) cudaFreeHost(c->h_scratch);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return GCMFGH_OK;
+}
+
+gcmfgh_status gcmfgh_set_stream(gcmfgh_ctx* c, void* stream) {
+  if (!c) return GCMFGH_INVALID_ARGUMENT;
+  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own;
+  return GCMFGH_OK;
+}
+
+gcmfgh_status gcmfgh_set_params(gcmfgh_ctx* c, double eps, double eps_clean, int union_mode) {
+  if (!c || !(eps >= 0) || !(eps_clean >= 0)) return GCMFGH_INVALID_ARGUMENT;
+  c->prm.eps = eps;
+  c->prm.eps_clean = eps_clean;
+  c->prm.union_mode = union_mode ? 1 : 0;
+  return GCMFGH_OK;
+}
+
+int gcmfgh_last_device_error(gcmfgh_ctx* c) { return c ? c->last_err : -1; }
+
+gcmfgh_status gcmf_join(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, gcmfgh_join_info* info) {
+  if (!c || !layer_ok(b) || !layer_ok(o)) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->join_arena.reset();
+  c->have_join = false;
+  cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  int st = run_join(to_dev(b), to_dev(o), c->join_arena, c->join, c->d_err, c->h_scratch, c->stream);
+  gcmfgh_status r = finish(c, st);
+  if (r != GCMFGH_OK) return r;
+  c->have_join = true;
+  c->join_b = b->coords;
+  c->join_o = o->coords;
+  c->join_nb = b->n_polys;
+  c->join_no = o->n_polys;
+  if (info) {
+    info->n_pairs = c->join.n_pairs;
+    info->n_pip_candidates = c->join.n_pip_candidates;
+    info->n_within = c->join.n_within;
+    info->n_cmf = c->join.n_cmf;
+    info->n_seg = c->join.n_seg;
+    info->n_clip = c->join.n_clip;
+  }
+  return GCMFGH_OK;
+}
+
+gcmfgh_status gcmf_join_get(gcmfgh_ctx* c, int f, void* dst, int64_t cap, int on_dev, int64_t* bytes) {
+  if (!c) return GCMFGH_INVALID_ARGUMENT;
+  if (!c->have_join) return GCMFGH_NOT_READY;
+  return copy_field(c, join_field(c, f), dst, cap, on_dev, bytes);
+}
+
+gcmfgh_status gcmf_join_ptr(gcmfgh_ctx* c, int f, const void** p, int64_t* count) {
+  if (!c || !p) return GCMFGH_INVALID_ARGUMENT;
+  if (!c->have_join) return GCMFGH_NOT_READY;
+  FieldRef r = join_field(c, f);
+  if (r.count < 0) return GCMFGH_INVALID_ARGUMENT;
+  *p = r.p;
+  if (count) *count = r.count;
+  return GCMFGH_OK;
+}
+
+gcmfgh_status gh_clip_batch(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, const int32_t* pid,
+                            const int32_t* qid, int64_t n, gcmfgh_clip_info* info) {
+  if (!c || !layer_ok(b) || !layer_ok(o) || n < 0 || (n > 0 && (!pid || !qid))) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->prm.no_swap = 0;
+  return run_clip_ctx(c, b, o, pid, qid, n, info);
+}
+
+gcmfgh_status gh_clip_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, gcmfgh_clip_info* info) {
+  if (!c || !layer_ok(b) || !layer_ok(o)) return GCMFGH_INVALID_ARGUMENT;
+  if (!c->have_join) return GCMFGH_NOT_READY;
+  if (b->coords != c->join_b || o->coords != c->join_o) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->prm.no_swap = 0;
+  return run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, c->join.n_clip, info);
+}
+
+gcmfgh_status gh_clip_get(gcmfgh_ctx* c, int f, void* dst, int64_t cap, int on_dev, int64_t* bytes) {
+  if (!c) return GCMFGH_INVALID_ARGUMENT;
+  if (!c->have_clip) return GCMFGH_NOT_READY;
+  return copy_field(c, clip_field(c, f), dst, cap, on_dev, bytes);
+}
+
+gcmfgh_status gh_clip_ptr(gcmfgh_ctx* c, int f, const void** p, int64_t* count) {
+  if (!c || !p) return GCMFGH_INVALID_ARGUMENT;
+  if (!c->have_clip) return GCMFGH_NOT_READY;
+  FieldRef r = clip_field(c, f);
+  if (r.count < 0) return GCMFGH_INVALID_ARGUMENT;
+  *p = r.p;
+  if (count) *count = r.count;
+  return GCMFGH_OK;
+}
+
+gcmfgh_status gh_clip_pair(gcmfgh_ctx* c, const double* P, int32_t nP, const double* Q, int32_t nQ,
+                           gcmfgh_clip_info* info) {
+  if (!c || !P || !Q || nP < 1 || nQ < 1) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->pair_arena.reset();
+  // two one-polygon layers in the reference layout (closing vertex appended)
+  int64_t nv = (int64_t)nP + 1 + nQ + 1;
+  double* xy = c->pair_arena.take_n<double>(2 * nv);
+  int32_t* vn = c->pair_arena.take_n<int32_t>(4);
+  int64_t* vp = c->pair_arena.take_n<int64_t>(4);
+  int32_t* ids = c->pair_arena.take_n<int32_t>(2);
+  if (!xy || !vn || !vp || !ids) return GCMFGH_OUT_OF_MEMORY;
+  double* hxy = static_cast<double*>(malloc(sizeof(double) * 2 * nv));
+  if (!hxy) return GCMFGH_OUT_OF_MEMORY;
+  memcpy(hxy, P, sizeof(double) * 2 * nP);
+  hxy[2 * nP] = P[0]; hxy[2 * nP + 1] = P[1];
+  memcpy(hxy + 2 * (nP + 1), Q, sizeof(double) * 2 * nQ);
+  hxy[2 * (nP + 1 + nQ)] = Q[0]; hxy[2 * (nP + 1 + nQ) + 1] = Q[1];
+  int32_t hvn[2] = {nP + 1, nQ + 1};
+  int64_t hvp[2] = {(int64_t)nP + 1, (int64_t)nQ + 1};
+  int32_t hid[2] = {0, 0};
+  cudaMemcpyAsync(xy, hxy, sizeof(double) * 2 * nv, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(vn, hvn, sizeof(hvn), cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(vp, hvp, sizeof(hvp), cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(ids, hid, sizeof(hid), cudaMemcpyHostToDevice, c->stream);
+  cudaStreamSynchronize(c->stream);
+  free(hxy);
+  gcmfgh_layer lb{xy, vn, vp, 1, (int64_t)nP + 1};
+  gcmfgh_layer lo{xy + 2 * (nP + 1), vn + 1, vp + 1, 1, (int64_t)nQ + 1};
+  c->prm.no_swap = 1;
+  gcmfgh_status r = run_clip_ctx(c, &lb, &lo, ids, ids + 1, 1, info);
+  c->prm.no_swap = 0;
+  return r;
+}
+
+gcmfgh_status gcmfgh_join_clip_host(gcmfgh_ctx* c, const gcmfgh_layer* bh, const gcmfgh_layer* oh,
+                                    gcmfgh_join_info* jinfo, gcmfgh_clip_info* cinfo) {
+  if (!c || !bh || !oh || bh->n_polys < 0 || oh->n_polys < 0) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->layer_arena.reset();
+  gcmfgh_layer dl[2];
+  const gcmfgh_layer* hl[2] = {bh, oh};
+  for (int i = 0; i < 2; ++i) {
+    const gcmfgh_layer* h = hl[i];
+    double* xy = c->layer_arena.take_n<double>(2 * h->n_vertices);
+    int32_t* vn = c->layer_arena.take_n<int32_t>(h->n_polys);
+    int64_t* vp = c->layer_arena.take_n<int64_t>(h->n_polys);
+    if (!xy || !vn || !vp) return GCMFGH_OUT_OF_MEMORY;
+    if (h->n_polys > 0) {
+      if (!h->coords || !h->vnum || !h->vps) return GCMFGH_INVALID_ARGUMENT;
+      cudaMemcpyAsync(xy, h->coords, sizeof(double) * 2 * h->n_vertices, cudaMemcpyHostToDevice, c->stream);
+      cudaMemcpyAsync(vn, h->vnum, sizeof(int32_t) * h->n_polys, cudaMemcpyHostToDevice, c->stream);
+      cudaMemcpyAsync(vp, h->vps, sizeof(int64_t) * h->n_polys, cudaMemcpyHostToDevice, c->stream);
+    }
+    dl[i] = gcmfgh_layer{xy, vn, vp, h->n_polys, h->n_vertices};
+  }
+  gcmfgh_status r = gcmf_join(c, &dl[0], &dl[1], jinfo);
+  if (r != GCMFGH_OK) return r;
+  return gh_clip_joined(c, &dl[0], &dl[1], cinfo);
+}
+
+}  // extern "C"

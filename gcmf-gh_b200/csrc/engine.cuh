@@ -1,0 +1,105 @@
+// engine.cuh -- host-side plumbing shared by the join and clip pipelines: the device
+// workspace arena, layer views and the result records the C ABI hands out.
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <vector>
+#include <cuda_runtime.h>
+
+namespace gcmfgh {
+
+// Status codes of the C ABI (mirrored in include/gcmfgh.h).
+enum Status : int {
+  ST_OK = 0,
+  ST_INVALID_ARGUMENT = 1,
+  ST_CUDA_ERROR = 2,
+  ST_OUT_OF_MEMORY = 3,
+  ST_DEVICE_ERROR = 4,     // a kernel raised its error word (capacity, trace budget, timeout)
+  ST_NOT_READY = 5,
+  ST_CAPACITY = 6,         // caller buffer too small (two-call size query)
+  ST_NO_DEVICE = 7,
+};
+
+// Bump allocator over device chunks.  Chunks are kept across calls and reused after
+// reset(); a request that does not fit opens a new chunk (cudaMalloc), so pointers
+// handed out since the last reset() stay valid.
+class Arena {
+ public:
+  ~Arena() { release(); }
+  void reset() { cur_ = 0; if (!chunks_.empty()) chunks_[0].off = 0; for (auto& c : chunks_) c.off = 0; }
+  void* take(size_t bytes);           // nullptr on allocation failure
+  template <class T> T* take_n(int64_t n) { return static_cast<T*>(take(sizeof(T) * (size_t)(n > 0 ? n : 1))); }
+  void release();
+  size_t reserved() const { size_t s = 0; for (auto& c : chunks_) s += c.cap; return s; }
+ private:
+  struct Chunk { char* base; size_t cap; size_t off; };
+  std::vector<Chunk> chunks_;
+  size_t cur_ = 0;
+};
+
+// A polygon layer in the reference's join layout, device pointers:
+// coords interleaved x,y with each polygon's closing vertex stored (spatialJoin3.cu:211),
+// vnum = vertices per polygon including the closing one, vps = inclusive prefix of vnum.
+struct LayerDev {
+  const double* xy;
+  const int32_t* vnum;
+  const int64_t* vps;
+  int64_t n;
+};
+
+// Join outputs (device, owned by the join arena).  Pairs are sorted by (base, overlay).
+struct JoinDev {
+  int64_t n_pairs = 0, n_pip_candidates = 0, n_within = 0, n_cmf = 0, n_seg = 0, n_clip = 0;
+  int32_t* b = nullptr;          // [n_pairs]
+  int32_t* o = nullptr;
+  double* cmbr = nullptr;        // [4 n_pairs]
+  int8_t* pip_type = nullptr;    // 0 none, 1 overlay may contain base, 2 base may contain overlay
+  int8_t* pip_flag = nullptr;    // containment confirmed
+  int8_t* join_flag = nullptr;   // survived the common-MBR edge filter
+  int32_t* bE = nullptr;         // edges touching the common MBR (0 when filtered out)
+  int32_t* oE = nullptr;
+  int8_t* seg_flag = nullptr;    // some surviving edge pair intersects
+  int8_t* clip = nullptr;        // pip_flag || seg_flag
+  int32_t* clip_b = nullptr;     // [n_clip] the clip set, same order
+  int32_t* clip_o = nullptr;
+  double* mbr_b = nullptr;       // [4 nb] layer MBRs
+  double* mbr_o = nullptr;
+  uint8_t* valid_b = nullptr;
+  uint8_t* valid_o = nullptr;
+};
+
+// Clip parameters (reference defaults: EPSILON 1e-7 in GH-CUDA/lib/constants.h:4).
+struct ClipParams {
+  double eps = 1e-7;          // intersection classification
+  double eps_clean = 1e-7;    // collinear-vertex removal in the clean-up
+  int union_mode = 0;         // polyclip.h:42 UNION
+  int no_swap = 0;            // 1: clip base as P even when it has fewer vertices
+};
+
+// Clip outputs (device, owned by the clip arena).
+struct ClipDev {
+  int64_t n_pairs = 0, n_components = 0, n_vertices = 0;
+  int32_t* status = nullptr;      // per pair: 0 ok, 1 invalid (P/Q counts differ), 2 disjoint MBRs, 3 trace error
+  int32_t* ncomp = nullptr;       // per pair
+  int64_t* comp_off = nullptr;    // per pair, first component index
+  int64_t* count1 = nullptr;      // per pair, edge pairs classified as intersecting (P side)
+  int32_t* comp_size = nullptr;   // per component vertex count
+  int64_t* vert_off = nullptr;    // per pair, first vertex
+  double* xy = nullptr;           // [2 n_vertices]
+  int32_t* swapped = nullptr;     // per pair: 1 when the overlay polygon was P
+};
+
+struct Timing {
+  float ms[16] = {0};
+};
+
+int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s);
+
+int run_join(const LayerDev& base, const LayerDev& ovl, Arena& arena, JoinDev& out,
+             int* d_err, int64_t* h_scratch, cudaStream_t s);
+
+int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, const int32_t* d_qid,
+             int64_t n_pairs, const ClipParams& prm, Arena& arena, ClipDev& out,
+             int* d_err, int64_t* h_scratch, cudaStream_t s);
+
+}  // namespace gcmfgh

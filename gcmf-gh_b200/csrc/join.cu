@@ -1,0 +1,480 @@
+// join.cu -- GCMF spatial join on sm_100a: MBR build, sort-and-sweep MBR filter,
+// common MBR + containment candidates, point-in-polygon, common-MBR edge filter and
+// segment-intersection refine.
+//
+// Reference path (spatialJoin3.cu:254-348): SortBaseMBROverlap (Join.h:5-153), GetCMBR
+// (Join.h:397-432), PointInPolygonTest (Join.h:437-467), CountCMF/ApplyCMF
+// (Join.h:157-287), SegmentIntersectJoin (Join.h:356-393).
+//
+// Layout in HBM: layers stay in the reference's interleaved FP64 layout (16 B per
+// vertex, read as one 128-bit load per vertex).  Per layer the MBRs are kept as
+// [minx, miny, maxx, maxy] FP64 rows plus a sorted structure-of-arrays copy (x1, x2,
+// y1, y2, id) in ascending x1 order, which is what the sweep streams.
+#include <algorithm>
+#include "common.cuh"
+#include "engine.cuh"
+#include "prims.cuh"
+
+namespace gcmfgh {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarpsPerBlock = kThreads / 32;
+
+inline unsigned blocks_for_warps(int64_t warps) {
+  return (unsigned)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
+}
+inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+// ---------------------------------------------------------------- J0: MBRs
+// One warp per polygon, 128-bit vertex loads.  The MBR covers every stored vertex,
+// the closing one included (SEQ_Overlay.h:316-344).  Zero-width or zero-height MBRs are
+// rejected like the reference reader does (SEQ_Overlay.h:336-344): such a polygon never
+// joins.  Valid polygons get the order-preserving key of their x1 for the sweep sort.
+__global__ void __launch_bounds__(kThreads)
+mbr_kernel(LayerDev L, double* __restrict__ mbr, uint8_t* __restrict__ valid,
+           uint64_t* __restrict__ key, uint32_t* __restrict__ id, unsigned long long* n_valid) {
+  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  if (w >= L.n) return;
+  const int nv = L.vnum[w];
+  const int64_t s = L.vps[w] - nv;
+  const double2* v = reinterpret_cast<const double2*>(L.xy) + s;
+  double x1 = INFINITY, y1 = INFINITY, x2 = -INFINITY, y2 = -INFINITY;
+  for (int k = lane_id(); k < nv; k += 32) {
+    double2 p = __ldg(v + k);
+    x1 = fmin(x1, p.x); x2 = fmax(x2, p.x);
+    y1 = fmin(y1, p.y); y2 = fmax(y2, p.y);
+  }
+  x1 = warp_min(x1); y1 = warp_min(y1); x2 = warp_max(x2); y2 = warp_max(y2);
+  if (lane_id() == 0) {
+    bool ok = nv >= 2 && x1 != x2 && y1 != y2;
+    reinterpret_cast<double4*>(mbr)[w] = make_double4(x1, y1, x2, y2);
+    valid[w] = ok ? 1 : 0;
+    key[w] = ok ? ordered_key(x1) : ~0ull;
+    id[w] = (uint32_t)w;
+    if (ok) atomicAdd(n_valid, 1ull);
+  }
+}
+
+struct SortedMbr { double *x1, *x2, *y1, *y2; uint32_t* id; int64_t n; };
+
+__global__ void gather_sorted_kernel(const double* __restrict__ mbr, const uint32_t* __restrict__ ids,
+                                     int64_t n, SortedMbr S) {
+  int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  uint32_t id = ids[i];
+  double4 m = reinterpret_cast<const double4*>(mbr)[id];
+  S.x1[i] = m.x; S.y1[i] = m.y; S.x2[i] = m.z; S.y2[i] = m.w; S.id[i] = id;
+}
+
+// first index with a[i] >= x
+__device__ __forceinline__ int64_t lower_bound_d(const double* a, int64_t n, double x) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) { int64_t m = (lo + hi) >> 1; if (a[m] < x) lo = m + 1; else hi = m; }
+  return lo;
+}
+// first index with a[i] > x
+__device__ __forceinline__ int64_t upper_bound_d(const double* a, int64_t n, double x) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) { int64_t m = (lo + hi) >> 1; if (a[m] <= x) lo = m + 1; else hi = m; }
+  return lo;
+}
+
+// ---------------------------------------------------------------- J2: sweep
+// The reference sorts all x endpoints (stable on endpoint index, base before overlay)
+// and lets each polygon scan the sorted positions strictly between its own endpoints
+// for other-layer starts, then checks y (GPU_MBR.h:339-415, 420-539).  On values this
+// accepts (b, o) iff [x1b <= x1o < x2b] or [x1o < x1b <= x2o], with closed y overlap.
+// Here each base polygon takes the overlays that start in [x1b, x2b) and each overlay
+// takes the bases that start in (x1o, x2o]; both ranges are binary searches in the
+// other layer's x1-sorted array, and only the y test remains inside the range.
+// mode 0: count per element, mode 1: emit keys (b << obits | o) at offs[element].
+template <int kMode>
+__global__ void __launch_bounds__(kThreads)
+sweep_kernel(SortedMbr B, SortedMbr O, int32_t* __restrict__ cnt, const int64_t* __restrict__ offs,
+             uint64_t* __restrict__ keys, int obits) {
+  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  if (w >= B.n + O.n) return;
+  const bool base_side = w < B.n;
+  const SortedMbr& me = base_side ? B : O;
+  const SortedMbr& ot = base_side ? O : B;
+  const int64_t i = base_side ? w : w - B.n;
+  const double mx1 = me.x1[i], mx2 = me.x2[i], my1 = me.y1[i], my2 = me.y2[i];
+  int64_t lo, hi;
+  if (base_side) { lo = lower_bound_d(ot.x1, ot.n, mx1); hi = lower_bound_d(ot.x1, ot.n, mx2); }
+  else { lo = upper_bound_d(ot.x1, ot.n, mx1); hi = upper_bound_d(ot.x1, ot.n, mx2); }
+  int c = 0;
+  int64_t pos = (kMode == 1) ? offs[w] : 0;
+  const uint64_t myid = me.id[i];
+  for (int64_t k0 = lo; k0 < hi; k0 += 32) {
+    int64_t k = k0 + lane_id();
+    bool hit = false;
+    if (k < hi) hit = ot.y1[k] <= my2 && my1 <= ot.y2[k];
+    unsigned m = __ballot_sync(0xffffffffu, hit);
+    if (kMode == 1 && hit) {
+      uint64_t oid = ot.id[k];
+      uint64_t b = base_side ? myid : oid, o = base_side ? oid : myid;
+      keys[pos + __popc(m & lanemask_lt())] = (b << obits) | o;
+    }
+    c += __popc(m);
+    pos += __popc(m);
+  }
+  if (kMode == 0 && lane_id() == 0) cnt[w] = c;
+}
+
+// ---------------------------------------------------------------- J3: common MBR
+// GPU_Join.h:468-506: CMBR = intersection of the FP64 MBRs; pip_type 1 when the base
+// MBR equals the CMBR (the overlay may contain the base), 2 when the overlay MBR does.
+__global__ void cmbr_kernel(const uint64_t* __restrict__ keys, int64_t K, int obits,
+                            const double* __restrict__ mb, const double* __restrict__ mo,
+                            int32_t* __restrict__ ob, int32_t* __restrict__ oo,
+                            double* __restrict__ cmbr, int8_t* __restrict__ pip_type) {
+  int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  if (k >= K) return;
+  uint64_t key = keys[k];
+  int32_t b = (int32_t)(key >> obits);
+  int32_t o = (int32_t)(key & ((1ull << obits) - 1));
+  ob[k] = b; oo[k] = o;
+  double4 B = reinterpret_cast<const double4*>(mb)[b];
+  double4 O = reinterpret_cast<const double4*>(mo)[o];
+  double x1 = B.x, y1 = B.y, x2 = B.z, y2 = B.w;
+  double a1 = O.x, b1 = O.y, a2 = O.z, b2 = O.w;
+  double cx1 = (a1 > x1 ? a1 : x1), cx2 = (a2 < x2 ? a2 : x2);
+  double cy1 = (b1 > y1 ? b1 : y1), cy2 = (b2 < y2 ? b2 : y2);
+  reinterpret_cast<double4*>(cmbr)[k] = make_double4(cx1, cy1, cx2, cy2);
+  int8_t t = 0;
+  if (x1 == cx1 && x2 == cx2 && y1 == cy1 && y2 == cy2) t = 1;
+  else if (a1 == cx1 && a2 == cx2 && b1 == cy1 && b2 == cy2) t = 2;
+  pip_type[k] = t;
+}
+
+// ---------------------------------------------------------------- J4: containment
+// Crossing parity of the contained candidate's first vertex against the other polygon's
+// stored ring, edges (i, i-1) for every stored vertex i (GPU_Join.h:856-939).  A warp per
+// candidate pair; the parity of the per-lane parities equals the reference's XOR scan.
+__global__ void __launch_bounds__(kThreads)
+pip_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32_t* __restrict__ po,
+           const int8_t* __restrict__ pip_type, int64_t K, int8_t* __restrict__ pip_flag,
+           int8_t* __restrict__ join_flag) {
+  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  if (w >= K) return;
+  int t = pip_type[w];
+  if (t == 0) {
+    if (lane_id() == 0) { pip_flag[w] = 0; join_flag[w] = 1; }
+    return;
+  }
+  int b = pb[w], o = po[w];
+  const LayerDev& Lp = (t == 1) ? Lb : Lo;     // layer of the point
+  const LayerDev& Lr = (t == 1) ? Lo : Lb;     // layer of the ring
+  int ip = (t == 1) ? b : o, ir = (t == 1) ? o : b;
+  const double2* pt = reinterpret_cast<const double2*>(Lp.xy) + (Lp.vps[ip] - Lp.vnum[ip]);
+  const double2 P = pt[0];
+  const int nv = Lr.vnum[ir];
+  const double2* v = reinterpret_cast<const double2*>(Lr.xy) + (Lr.vps[ir] - nv);
+  int par = 0;
+  for (int i = lane_id(); i < nv; i += 32) {
+    int j = (i == 0) ? nv - 1 : i - 1;
+    double2 a = __ldg(v + i), c = __ldg(v + j);
+    double Y1 = a.y, Y2 = c.y, X1 = a.x, X2 = c.x;
+    if ((Y1 > P.y) == (Y2 > P.y)) continue;
+    if (P.x < (X2 - X1) * (P.y - Y1) / (Y2 - Y1) + X1) par ^= 1;
+  }
+  int inside = __popc(__ballot_sync(0xffffffffu, par)) & 1;
+  if (lane_id() == 0) { pip_flag[w] = (int8_t)inside; join_flag[w] = inside ? 0 : 1; }
+}
+
+// ---------------------------------------------------------------- J5: common-MBR filter
+// Edges whose box touches the CMBR (GPU_Join.h:562-580); edge k of a stored ring runs
+// from vertex k to k+1 and the last one from the closing vertex back to vertex 0.
+// mode 0 counts (and drops pairs with an empty side, :604-613), mode 1 writes the
+// surviving edge ids in ascending order (Apply_CMF :676-733, 32-bit ids here).
+template <int kMode>
+__global__ void __launch_bounds__(kThreads)
+cmf_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32_t* __restrict__ po,
+           const double* __restrict__ cmbr, int64_t K, int8_t* __restrict__ join_flag,
+           int32_t* __restrict__ bE, int32_t* __restrict__ oE,
+           const int64_t* __restrict__ bOff, const int64_t* __restrict__ oOff,
+           int32_t* __restrict__ bList, int32_t* __restrict__ oList) {
+  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  if (w >= K) return;
+  if (!join_flag[w]) {
+    if (kMode == 0 && lane_id() == 0) { bE[w] = 0; oE[w] = 0; }
+    return;
+  }
+  if (kMode == 1 && bE[w] == 0) return;
+  double4 c = reinterpret_cast<const double4*>(cmbr)[w];
+  int counts[2];
+  for (int side = 0; side < 2; ++side) {
+    const LayerDev& L = side == 0 ? Lb : Lo;
+    int id = side == 0 ? pb[w] : po[w];
+    const int nv = L.vnum[id];
+    const double2* v = reinterpret_cast<const double2*>(L.xy) + (L.vps[id] - nv);
+    int64_t pos = 0;
+    int32_t* list = nullptr;
+    if (kMode == 1) { pos = side == 0 ? bOff[w] : oOff[w]; list = side == 0 ? bList : oList; }
+    int cnt = 0;
+    for (int k0 = 0; k0 < nv; k0 += 32) {
+      int k = k0 + lane_id();
+      bool hit = false;
+      if (k < nv) {
+        double2 a = __ldg(v + k), b = __ldg(v + ((k < nv - 1) ? k + 1 : 0));
+        hit = edge_touches_box(a.x, a.y, b.x, b.y, c.x, c.y, c.z, c.w);
+      }
+      unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (kMode == 1 && hit) list[pos + cnt + __popc(m & lanemask_lt())] = k;
+      cnt += __popc(m);
+    }
+    counts[side] = cnt;
+  }
+  if (kMode == 0 && lane_id() == 0) {
+    if (counts[0] == 0 || counts[1] == 0) { join_flag[w] = 0; bE[w] = 0; oE[w] = 0; }
+    else { bE[w] = counts[0]; oE[w] = counts[1]; }
+  }
+}
+
+// ---------------------------------------------------------------- J6: refine
+// Does any surviving (base edge, overlay edge) pair intersect?  The closed-form test of
+// GPU_Join.h:373-446 in its operation order: zero-length base edges are skipped, box
+// rejects, the collinear branch via slopes and intercepts, then the intersection point
+// against both edges' extents.  A warp per pair over the flattened bE x oE grid, with an
+// early exit as soon as any lane finds an intersection (the reference's shared joinFlag).
+__device__ __forceinline__ bool segment_hit(double bX1, double bY1, double bX2, double bY2,
+                                            double oX1, double oY1, double oX2, double oY2) {
+  if (bX1 == bX2 && bY1 == bY2) return false;
+  if (((bX2 < oX1) && (bX2 < oX2)) && ((bX1 < oX1) && (bX1 < oX2))) return false;
+  if (((bX2 > oX1) && (bX2 > oX2)) && ((bX1 > oX1) && (bX1 > oX2))) return false;
+  if (((bY2 < oY1) && (bY2 < oY2)) && ((bY1 < oY1) && (bY1 < oY2))) return false;
+  if (((bY2 > oY1) && (bY2 > oY2)) && ((bY1 > oY1) && (bY1 > oY2))) return false;
+  double denom = ((bX1 - bX2) * (oY1 - oY2)) - ((bY1 - bY2) * (oX1 - oX2));
+  if (denom == 0) {
+    if ((oX1 == oX2 && oX1 == bX1) || (bX1 == bX2 && bX1 == oX1)) return true;
+    double oM = (oY2 - oY1) / (oX2 - oX1);
+    double bM = (bY2 - bY1) / (bX2 - bX1);
+    double oB = oY1 - oM * oX1;
+    double bB = bY1 - bM * bX1;
+    return oB == bB;
+  }
+  double nomX = (((bX1 * bY2) - (bY1 * bX2)) * (oX1 - oX2)) - ((bX1 - bX2) * ((oX1 * oY2) - (oY1 * oX2)));
+  double nomY = ((((bX1 * bY2) - (bY1 * bX2)) * (oY1 - oY2)) - (((bY1 - bY2) * ((oX1 * oY2) - (oY1 * oX2)))));
+  double x0 = nomX / denom, y0 = nomY / denom;
+  if ((x0 > bX1 && x0 > bX2) || (x0 < bX1 && x0 < bX2)) return false;
+  if ((x0 > oX1 && x0 > oX2) || (x0 < oX1 && x0 < oX2)) return false;
+  if ((y0 > bY1 && y0 > bY2) || (y0 < bY1 && y0 < bY2)) return false;
+  if ((y0 > oY1 && y0 > oY2) || (y0 < oY1 && y0 < oY2)) return false;
+  return true;
+}
+
+__global__ void __launch_bounds__(kThreads)
+refine_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32_t* __restrict__ po,
+              int64_t K, const int8_t* __restrict__ join_flag,
+              const int32_t* __restrict__ bE, const int32_t* __restrict__ oE,
+              const int64_t* __restrict__ bOff, const int64_t* __restrict__ oOff,
+              const int32_t* __restrict__ bList, const int32_t* __restrict__ oList,
+              int8_t* __restrict__ seg_flag) {
+  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  if (w >= K) return;
+  if (!join_flag[w]) { if (lane_id() == 0) seg_flag[w] = 0; return; }
+  const int nb = bE[w], no = oE[w];
+  const int b = pb[w], o = po[w];
+  const int bV = Lb.vnum[b], oV = Lo.vnum[o];
+  const double2* bv = reinterpret_cast<const double2*>(Lb.xy) + (Lb.vps[b] - bV);
+  const double2* ov = reinterpret_cast<const double2*>(Lo.xy) + (Lo.vps[o] - oV);
+  const int32_t* bl = bList + bOff[w];
+  const int32_t* ol = oList + oOff[w];
+  const int64_t total = (int64_t)nb * no;
+  int found = 0;
+  for (int64_t t0 = 0; t0 < total && !found; t0 += 32) {
+    int64_t t = t0 + lane_id();
+    bool hit = false;
+    if (t < total) {
+      int be = bl[t / no], oe = ol[t % no];
+      double2 b1 = __ldg(bv + be), b2 = __ldg(bv + ((be < bV - 1) ? be + 1 : 0));
+      double2 o1 = __ldg(ov + oe), o2 = __ldg(ov + ((oe < oV - 1) ? oe + 1 : 0));
+      hit = segment_hit(b1.x, b1.y, b2.x, b2.y, o1.x, o1.y, o2.x, o2.y);
+    }
+    found = __any_sync(0xffffffffu, hit);
+  }
+  if (lane_id() == 0) seg_flag[w] = (int8_t)found;
+}
+
+// ---------------------------------------------------------------- clip set + stats
+__global__ void clip_flag_kernel(const int8_t* __restrict__ pip_type, const int8_t* __restrict__ pip,
+                                 const int8_t* __restrict__ join, const int8_t* __restrict__ seg,
+                                 int64_t K, int8_t* __restrict__ clip, uint8_t* __restrict__ clip_u8,
+                                 unsigned long long* stats) {
+  int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  unsigned long long s[4] = {0, 0, 0, 0};
+  if (k < K) {
+    int8_t c = (pip[k] || seg[k]) ? 1 : 0;
+    clip[k] = c;
+    clip_u8[k] = (uint8_t)c;
+    s[0] = pip_type[k] != 0; s[1] = pip[k] != 0; s[2] = join[k] != 0; s[3] = seg[k] != 0;
+  }
+  for (int j = 0; j < 4; ++j) {
+    unsigned long long v = warp_sum(s[j]);
+    if (lane_id() == 0 && v) atomicAdd(&stats[j], v);
+  }
+}
+
+__global__ void clip_compact_kernel(const int8_t* __restrict__ clip, const int64_t* __restrict__ off,
+                                    const int32_t* __restrict__ b, const int32_t* __restrict__ o,
+                                    int64_t K, int32_t* __restrict__ cb, int32_t* __restrict__ co) {
+  int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  if (k >= K || !clip[k]) return;
+  cb[off[k]] = b[k];
+  co[off[k]] = o[k];
+}
+
+// MBRs only (the clip pipeline's common MBRs), same definition as mbr_kernel
+__global__ void __launch_bounds__(kThreads)
+mbr_only_kernel(LayerDev L, double* __restrict__ mbr) {
+  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  if (w >= L.n) return;
+  const int nv = L.vnum[w];
+  const double2* v = reinterpret_cast<const double2*>(L.xy) + (L.vps[w] - nv);
+  double x1 = INFINITY, y1 = INFINITY, x2 = -INFINITY, y2 = -INFINITY;
+  for (int k = lane_id(); k < nv; k += 32) {
+    double2 p = __ldg(v + k);
+    x1 = fmin(x1, p.x); x2 = fmax(x2, p.x);
+    y1 = fmin(y1, p.y); y2 = fmax(y2, p.y);
+  }
+  x1 = warp_min(x1); y1 = warp_min(y1); x2 = warp_max(x2); y2 = warp_max(y2);
+  if (lane_id() == 0) reinterpret_cast<double4*>(mbr)[w] = make_double4(x1, y1, x2, y2);
+}
+
+int bits_for(int64_t n) {
+  int b = 1;
+  while ((1ll << b) < n) ++b;
+  return b;
+}
+
+}  // namespace
+
+int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s) {
+  if (L.n > 0) mbr_only_kernel<<<blocks_for_warps(L.n), kThreads, 0, s>>>(L, mbr);
+  return ST_OK;
+}
+
+int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* d_err,
+             int64_t* h_scratch, cudaStream_t s) {
+  J = JoinDev();
+  const int64_t nb = Lb.n, no = Lo.n;
+  if (nb <= 0 || no <= 0) return ST_OK;
+  // ---- J0 MBRs + sort keys
+  J.mbr_b = A.take_n<double>(4 * nb); J.mbr_o = A.take_n<double>(4 * no);
+  J.valid_b = A.take_n<uint8_t>(nb); J.valid_o = A.take_n<uint8_t>(no);
+  const int64_t nmax = std::max(nb, no);
+  uint64_t* keyB = A.take_n<uint64_t>(nb);
+  uint64_t* keyO = A.take_n<uint64_t>(no);
+  uint32_t* idB = A.take_n<uint32_t>(nb);
+  uint32_t* idO = A.take_n<uint32_t>(no);
+  uint64_t* kAlt = A.take_n<uint64_t>(nmax);
+  uint32_t* vAlt = A.take_n<uint32_t>(nmax);
+  unsigned long long* d_cnt = A.take_n<unsigned long long>(8);
+  void* tmp = A.take(std::max(radix_temp_bytes(nmax), scan_temp_bytes(nmax)));
+  if (!J.mbr_b || !J.mbr_o || !J.valid_b || !J.valid_o || !keyB || !keyO || !idB || !idO || !kAlt ||
+      !vAlt || !d_cnt || !tmp)
+    return ST_OUT_OF_MEMORY;
+  cudaMemsetAsync(d_cnt, 0, 8 * sizeof(unsigned long long), s);
+  mbr_kernel<<<blocks_for_warps(nb), kThreads, 0, s>>>(Lb, J.mbr_b, J.valid_b, keyB, idB, d_cnt + 0);
+  mbr_kernel<<<blocks_for_warps(no), kThreads, 0, s>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1);
+  // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
+  radix_sort_pairs(keyB, idB, kAlt, vAlt, nb, 64, tmp, d_err, s);
+  radix_sort_pairs(keyO, idO, kAlt, vAlt, no, 64, tmp, d_err, s);
+  cudaMemcpyAsync(h_scratch, d_cnt, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+  const int64_t nvb = h_scratch[0], nvo = h_scratch[1];
+  SortedMbr SB{A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb),
+               A.take_n<uint32_t>(nvb), nvb};
+  SortedMbr SO{A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo),
+               A.take_n<uint32_t>(nvo), nvo};
+  int32_t* cnt = A.take_n<int32_t>(nvb + nvo);
+  int64_t* offs = A.take_n<int64_t>(nvb + nvo);
+  int64_t* d_total = A.take_n<int64_t>(4);
+  if (!SB.x1 || !SB.x2 || !SB.y1 || !SB.y2 || !SB.id || !SO.x1 || !SO.x2 || !SO.y1 || !SO.y2 ||
+      !SO.id || !cnt || !offs || !d_total)
+    return ST_OUT_OF_MEMORY;
+  if (nvb) gather_sorted_kernel<<<blocks_for(nvb), kThreads, 0, s>>>(J.mbr_b, idB, nvb, SB);
+  if (nvo) gather_sorted_kernel<<<blocks_for(nvo), kThreads, 0, s>>>(J.mbr_o, idO, nvo, SO);
+  // ---- J2 sweep: count, scan, emit, canonical sort
+  const int obits = bits_for(no);
+  const int bbits = bits_for(nb);
+  if (obits + bbits > 64) return ST_INVALID_ARGUMENT;
+  const int64_t ne = nvb + nvo;
+  if (ne > 0) {
+    sweep_kernel<0><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr, nullptr, obits);
+    void* stmp = A.take(scan_temp_bytes(ne));
+    if (!stmp) return ST_OUT_OF_MEMORY;
+    exclusive_scan_i32(cnt, offs, ne, d_total, stmp, d_err, s);
+  } else {
+    cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
+  }
+  cudaMemcpyAsync(h_scratch, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+  const int64_t K = h_scratch[0];
+  J.n_pairs = K;
+  if (K == 0) return ST_OK;
+  uint64_t* pkeys = A.take_n<uint64_t>(K);
+  uint32_t* pvals = A.take_n<uint32_t>(K);
+  uint64_t* pkAlt = A.take_n<uint64_t>(K);
+  uint32_t* pvAlt = A.take_n<uint32_t>(K);
+  void* rtmp = A.take(radix_temp_bytes(K));
+  if (!pkeys || !pvals || !pkAlt || !pvAlt || !rtmp) return ST_OUT_OF_MEMORY;
+  sweep_kernel<1><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs, pkeys, obits);
+  radix_sort_pairs(pkeys, pvals, pkAlt, pvAlt, K, ((obits + bbits + 7) / 8) * 8, rtmp, d_err, s);
+  // ---- J3 CMBR + containment candidates
+  J.b = A.take_n<int32_t>(K); J.o = A.take_n<int32_t>(K);
+  J.cmbr = A.take_n<double>(4 * K);
+  J.pip_type = A.take_n<int8_t>(K); J.pip_flag = A.take_n<int8_t>(K);
+  J.join_flag = A.take_n<int8_t>(K); J.seg_flag = A.take_n<int8_t>(K); J.clip = A.take_n<int8_t>(K);
+  J.bE = A.take_n<int32_t>(K); J.oE = A.take_n<int32_t>(K);
+  int64_t* bOff = A.take_n<int64_t>(K);
+  int64_t* oOff = A.take_n<int64_t>(K);
+  uint8_t* clipU8 = A.take_n<uint8_t>(K);
+  int64_t* clipOff = A.take_n<int64_t>(K);
+  void* stmpK = A.take(scan_temp_bytes(K));
+  if (!J.b || !J.o || !J.cmbr || !J.pip_type || !J.pip_flag || !J.join_flag || !J.seg_flag || !J.clip ||
+      !J.bE || !J.oE || !bOff || !oOff || !clipU8 || !clipOff || !stmpK)
+    return ST_OUT_OF_MEMORY;
+  cmbr_kernel<<<blocks_for(K), kThreads, 0, s>>>(pkeys, K, obits, J.mbr_b, J.mbr_o, J.b, J.o, J.cmbr,
+                                                 J.pip_type);
+  // ---- J4 point in polygon
+  pip_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.pip_type, K, J.pip_flag,
+                                                      J.join_flag);
+  // ---- J5 common-MBR edge filter: count, offsets, lists
+  cmf_kernel<0><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                         J.oE, nullptr, nullptr, nullptr, nullptr);
+  exclusive_scan_i32(J.bE, bOff, K, d_total + 1, stmpK, d_err, s);
+  exclusive_scan_i32(J.oE, oOff, K, d_total + 2, stmpK, d_err, s);
+  cudaMemcpyAsync(h_scratch, d_total + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+  const int64_t nBl = h_scratch[0], nOl = h_scratch[1];
+  int32_t* bList = A.take_n<int32_t>(nBl);
+  int32_t* oList = A.take_n<int32_t>(nOl);
+  if (!bList || !oList) return ST_OUT_OF_MEMORY;
+  cmf_kernel<1><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                         J.oE, bOff, oOff, bList, oList);
+  // ---- J6 refine
+  refine_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, K, J.join_flag, J.bE, J.oE,
+                                                         bOff, oOff, bList, oList, J.seg_flag);
+  // ---- clip set = containment pairs + pairs with intersecting edges
+  clip_flag_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.pip_type, J.pip_flag, J.join_flag, J.seg_flag, K,
+                                                      J.clip, clipU8, d_cnt + 2);
+  exclusive_scan_u8(clipU8, clipOff, K, d_total + 3, stmpK, d_err, s);
+  cudaMemcpyAsync(h_scratch, d_total + 3, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(h_scratch + 1, d_cnt + 2, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+  J.n_clip = h_scratch[0];
+  J.n_pip_candidates = h_scratch[1];
+  J.n_within = h_scratch[2];
+  J.n_cmf = h_scratch[3];
+  J.n_seg = h_scratch[4];
+  J.clip_b = A.take_n<int32_t>(J.n_clip);
+  J.clip_o = A.take_n<int32_t>(J.n_clip);
+  if (!J.clip_b || !J.clip_o) return ST_OUT_OF_MEMORY;
+  clip_compact_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.clip, clipOff, J.b, J.o, K, J.clip_b, J.clip_o);
+  return ST_OK;
+}
+
+}  // namespace gcmfgh

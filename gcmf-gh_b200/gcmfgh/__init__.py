@@ -1,0 +1,232 @@
+"""Python front end of libgcmfgh.so (the C ABI in include/gcmfgh.h).
+
+The engine itself is C++/CUDA; this module only moves arrays across the C ABI with
+ctypes.  Device memory comes from torch tensors on the context's device.  Nothing here
+computes results: if the shared library or the GPU is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import synth  # noqa: F401  (re-exported for harness code)
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libgcmfgh.so")
+
+# gcmf_join_field
+JOIN_FIELDS = {
+    "b": (0, np.int32), "o": (1, np.int32), "cmbr": (2, np.float64), "pip_type": (3, np.int8),
+    "pip_flag": (4, np.int8), "join_flag": (5, np.int8), "bE": (6, np.int32), "oE": (7, np.int32),
+    "seg_flag": (8, np.int8), "clip": (9, np.int8), "clip_b": (10, np.int32), "clip_o": (11, np.int32),
+    "mbr_b": (12, np.float64), "mbr_o": (13, np.float64), "valid_b": (14, np.uint8),
+    "valid_o": (15, np.uint8),
+}
+# gh_clip_field
+CLIP_FIELDS = {
+    "status": (0, np.int32), "ncomp": (1, np.int32), "comp_off": (2, np.int64),
+    "count1": (3, np.int64), "comp_size": (4, np.int32), "vert_off": (5, np.int64),
+    "xy": (6, np.float64), "swapped": (7, np.int32),
+}
+
+
+class GcmfghError(RuntimeError):
+    pass
+
+
+class Layer(ctypes.Structure):
+    _fields_ = [("coords", ctypes.c_void_p), ("vnum", ctypes.c_void_p), ("vps", ctypes.c_void_p),
+                ("n_polys", ctypes.c_int64), ("n_vertices", ctypes.c_int64)]
+
+
+class JoinInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in
+                ("n_pairs", "n_pip_candidates", "n_within", "n_cmf", "n_seg", "n_clip")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+class ClipInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in
+                ("n_pairs", "n_components", "n_vertices", "n_invalid", "n_disjoint", "n_error")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GcmfghError(f"{LIB_PATH} is not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, i64, d = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+        P = ctypes.POINTER
+        L.gcmfgh_create.argtypes = [ctypes.c_int, P(vp)]
+        L.gcmfgh_destroy.argtypes = [vp]
+        L.gcmfgh_set_stream.argtypes = [vp, vp]
+        L.gcmfgh_set_params.argtypes = [vp, d, d, ctypes.c_int]
+        L.gcmfgh_status_string.argtypes = [ctypes.c_int]
+        L.gcmfgh_status_string.restype = ctypes.c_char_p
+        L.gcmfgh_last_device_error.argtypes = [vp]
+        L.gcmf_join.argtypes = [vp, P(Layer), P(Layer), P(JoinInfo)]
+        L.gcmf_join_get.argtypes = [vp, ctypes.c_int, vp, i64, ctypes.c_int, P(i64)]
+        L.gcmf_join_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
+        L.gh_clip_batch.argtypes = [vp, P(Layer), P(Layer), vp, vp, i64, P(ClipInfo)]
+        L.gh_clip_joined.argtypes = [vp, P(Layer), P(Layer), P(ClipInfo)]
+        L.gh_clip_get.argtypes = [vp, ctypes.c_int, vp, i64, ctypes.c_int, P(i64)]
+        L.gh_clip_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
+        L.gh_clip_pair.argtypes = [vp, vp, i32, vp, i32, P(ClipInfo)]
+        L.gcmfgh_join_clip_host.argtypes = [vp, P(Layer), P(Layer), P(JoinInfo), P(ClipInfo)]
+        _lib = L
+    return _lib
+
+
+def _check(st):
+    if st != 0:
+        raise GcmfghError(f"gcmfgh: {lib().gcmfgh_status_string(st).decode()} ({st})")
+
+
+def _np_ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class DeviceLayer:
+    """A layer resident on the GPU (torch tensors) plus its C view."""
+
+    def __init__(self, layer, device="cuda:0"):
+        import torch
+        self.layer = layer
+        self.xy = torch.from_numpy(layer.xy).to(device)
+        self.vnum = torch.from_numpy(layer.vnum).to(device)
+        self.vps = torch.from_numpy(layer.vps).to(device)
+        self.c = Layer(self.xy.data_ptr(), self.vnum.data_ptr(), self.vps.data_ptr(),
+                       layer.n_polys, layer.n_vertices)
+
+
+def host_layer(layer):
+    """C view of a host (numpy) layer for the host-buffer entry point."""
+    return Layer(layer.xy.ctypes.data, layer.vnum.ctypes.data, layer.vps.ctypes.data,
+                 layer.n_polys, layer.n_vertices)
+
+
+class ClipResult:
+    """Per-pair status and result components, host copies (same shape as the oracle's)."""
+
+    def __init__(self, status, ncomp, count1, comp_size, xy, swapped):
+        self.status = status
+        self.ncomp = ncomp
+        self.count1 = count1
+        self.comp_size = comp_size
+        self.xy = xy
+        self.swapped = swapped
+        self.comp_off = np.concatenate([[0], np.cumsum(comp_size, dtype=np.int64)])
+        self.pair_comp_off = np.concatenate([[0], np.cumsum(ncomp, dtype=np.int64)])
+
+    def components(self, k):
+        out = []
+        for c in range(self.pair_comp_off[k], self.pair_comp_off[k + 1]):
+            a, b = self.comp_off[c], self.comp_off[c + 1]
+            out.append(self.xy[2 * a:2 * b].reshape(-1, 2))
+        return out
+
+
+class Engine:
+    """One gcmfgh context on one GPU."""
+
+    def __init__(self, device=0, eps=1e-7, eps_clean=None, union=False):
+        self.device = device
+        h = ctypes.c_void_p()
+        _check(lib().gcmfgh_create(device, ctypes.byref(h)))
+        self.h = h
+        self.set_params(eps, eps if eps_clean is None else eps_clean, union)
+
+    def close(self):
+        if self.h:
+            lib().gcmfgh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, eps=1e-7, eps_clean=1e-7, union=False):
+        _check(lib().gcmfgh_set_params(self.h, eps, eps_clean, 1 if union else 0))
+
+    def set_stream(self, stream_ptr):
+        _check(lib().gcmfgh_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+
+    def last_device_error(self):
+        return lib().gcmfgh_last_device_error(self.h)
+
+    # ---- join
+    def join(self, dbase: DeviceLayer, dovl: DeviceLayer):
+        info = JoinInfo()
+        _check(lib().gcmf_join(self.h, ctypes.byref(dbase.c), ctypes.byref(dovl.c), ctypes.byref(info)))
+        return info.as_dict()
+
+    def _get(self, getter, fields, name):
+        fid, dt = fields[name]
+        nbytes = ctypes.c_int64()
+        _check(getter(self.h, fid, None, 0, 0, ctypes.byref(nbytes)))
+        out = np.empty(nbytes.value // np.dtype(dt).itemsize, dtype=dt)
+        _check(getter(self.h, fid, _np_ptr(out), nbytes.value, 0, ctypes.byref(nbytes)))
+        return out
+
+    def join_field(self, name):
+        return self._get(lib().gcmf_join_get, JOIN_FIELDS, name)
+
+    def clip_field(self, name):
+        return self._get(lib().gh_clip_get, CLIP_FIELDS, name)
+
+    def clip_ptr(self, name):
+        fid, _ = CLIP_FIELDS[name]
+        p = ctypes.c_void_p()
+        n = ctypes.c_int64()
+        _check(lib().gh_clip_ptr(self.h, fid, ctypes.byref(p), ctypes.byref(n)))
+        return p.value, n.value
+
+    # ---- clip
+    def clip_batch(self, dbase: DeviceLayer, dovl: DeviceLayer, pid, qid):
+        import torch
+        dev = dbase.xy.device
+        p = torch.as_tensor(np.ascontiguousarray(pid, np.int32)).to(dev)
+        q = torch.as_tensor(np.ascontiguousarray(qid, np.int32)).to(dev)
+        info = ClipInfo()
+        _check(lib().gh_clip_batch(self.h, ctypes.byref(dbase.c), ctypes.byref(dovl.c),
+                                   ctypes.c_void_p(p.data_ptr()), ctypes.c_void_p(q.data_ptr()),
+                                   len(pid), ctypes.byref(info)))
+        return info.as_dict()
+
+    def clip_joined(self, dbase: DeviceLayer, dovl: DeviceLayer):
+        info = ClipInfo()
+        _check(lib().gh_clip_joined(self.h, ctypes.byref(dbase.c), ctypes.byref(dovl.c), ctypes.byref(info)))
+        return info.as_dict()
+
+    def clip_pair(self, P, Q):
+        P = np.ascontiguousarray(P, np.float64).reshape(-1)
+        Q = np.ascontiguousarray(Q, np.float64).reshape(-1)
+        info = ClipInfo()
+        _check(lib().gh_clip_pair(self.h, _np_ptr(P), len(P) // 2, _np_ptr(Q), len(Q) // 2,
+                                  ctypes.byref(info)))
+        return info.as_dict()
+
+    def clip_result(self):
+        return ClipResult(self.clip_field("status"), self.clip_field("ncomp"), self.clip_field("count1"),
+                          self.clip_field("comp_size"), self.clip_field("xy"), self.clip_field("swapped"))
+
+    # ---- end to end from host buffers
+    def join_clip_host(self, base, ovl):
+        jb, jo = host_layer(base), host_layer(ovl)
+        ji, ci = JoinInfo(), ClipInfo()
+        _check(lib().gcmfgh_join_clip_host(self.h, ctypes.byref(jb), ctypes.byref(jo), ctypes.byref(ji),
+                                           ctypes.byref(ci)))
+        return ji.as_dict(), ci.as_dict()

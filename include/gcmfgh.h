@@ -1,0 +1,155 @@
+/*
+ * gcmfgh.h -- C ABI of the B200 spatial-join-and-clip engine (libgcmfgh.so).
+ *
+ * The engine replaces the hot path of the GCMF-GH reference: the GCMF join driver
+ * behind main.cpp (spatialJoin, main.h:5-7, spatialJoin3.cu:40-412) and the GH-CUDA
+ * clip call (ghcuda, main.h:8-11, GH-CUDA/ghcuda.cpp:385-425, with its inner
+ * calculateIntersections, GH-CUDA/ghcuda.h:6-14).  The reference exports those three
+ * with C++ linkage and no status returns; the C entry points below carry the same data
+ * in plain pointers and sizes, return a status code, and never exit the process.
+ * gcmfgh_shims.h declares C++ functions with the reference's exact signatures.
+ *
+ * Layer layout (the reference's, spatialJoin3.cu:205-212 and SEQ_Overlay.h:352-380):
+ *   coords  interleaved FP64 x,y; each polygon stores its closing vertex (a copy of its
+ *           first vertex) after its last one; 16-byte aligned
+ *   vnum    per polygon, vertex count including the closing vertex (bVNum)
+ *   vps     per polygon, inclusive prefix sum of vnum (bVPSNum)
+ * Polygon i occupies vertices [vps[i]-vnum[i], vps[i]).
+ *
+ * Unless a function says otherwise, layer and pair pointers are device pointers on the
+ * context's device, and every call is ordered on the context's stream and returns when
+ * its results are ready.  Results stay owned by the context and are valid until the
+ * next call of the same kind (join or clip); the *_get functions copy them out.
+ */
+#ifndef GCMFGH_H
+#define GCMFGH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  GCMFGH_OK = 0,
+  GCMFGH_INVALID_ARGUMENT = 1,
+  GCMFGH_CUDA_ERROR = 2,
+  GCMFGH_OUT_OF_MEMORY = 3,
+  GCMFGH_DEVICE_ERROR = 4,   /* a kernel reported a capacity, trace-budget or wait-limit error */
+  GCMFGH_NOT_READY = 5,      /* no result of that kind yet */
+  GCMFGH_CAPACITY = 6,       /* destination smaller than the result (size query first) */
+  GCMFGH_NO_DEVICE = 7
+} gcmfgh_status;
+
+typedef struct gcmfgh_ctx gcmfgh_ctx;
+
+typedef struct {
+  const double* coords;
+  const int32_t* vnum;
+  const int64_t* vps;
+  int64_t n_polys;
+  int64_t n_vertices; /* = vps[n_polys-1]; needed for host-resident layers */
+} gcmfgh_layer;
+
+/* Counts of one join (spatialJoin3.cu:256-363 prints the same stages). */
+typedef struct {
+  int64_t n_pairs;          /* MBR candidates (SortBaseMBROverlap, Join.h:5) */
+  int64_t n_pip_candidates; /* one MBR equals the common MBR (GetCMBR, Join.h:397) */
+  int64_t n_within;         /* containment confirmed (PointInPolygonTest, Join.h:437) */
+  int64_t n_cmf;            /* survived the common-MBR edge filter (CountCMF, Join.h:157) */
+  int64_t n_seg;            /* some edge pair intersects (SegmentIntersectJoin, Join.h:356) */
+  int64_t n_clip;           /* clip set = n_within + n_seg pairs */
+} gcmfgh_join_info;
+
+typedef struct {
+  int64_t n_pairs;
+  int64_t n_components;
+  int64_t n_vertices;
+  int64_t n_invalid;        /* P/Q intersection counts disagree (gppolyclip_mDIV512.cu:1461) */
+  int64_t n_disjoint;       /* MBRs do not overlap (ghcuda.cpp:109-116 exits instead) */
+  int64_t n_error;          /* tracing did not close within its step budget */
+} gcmfgh_clip_info;
+
+/* Join result fields for gcmf_join_get / gcmf_join_ptr. */
+typedef enum {
+  GCMF_PAIR_BASE = 0,    /* int32 [n_pairs], pairs sorted by (base, overlay) */
+  GCMF_PAIR_OVERLAY,     /* int32 [n_pairs] */
+  GCMF_CMBR,             /* f64 [4 n_pairs] minx, miny, maxx, maxy */
+  GCMF_PIP_TYPE,         /* int8 [n_pairs]: 1 overlay may contain base, 2 base may contain overlay */
+  GCMF_PIP_FLAG,         /* int8 [n_pairs] */
+  GCMF_JOIN_FLAG,        /* int8 [n_pairs] */
+  GCMF_BASE_EDGES,       /* int32 [n_pairs] base edges touching the common MBR */
+  GCMF_OVERLAY_EDGES,    /* int32 [n_pairs] */
+  GCMF_SEG_FLAG,         /* int8 [n_pairs] */
+  GCMF_CLIP_FLAG,        /* int8 [n_pairs] */
+  GCMF_CLIP_BASE,        /* int32 [n_clip] */
+  GCMF_CLIP_OVERLAY,     /* int32 [n_clip] */
+  GCMF_MBR_BASE,         /* f64 [4 n_base] */
+  GCMF_MBR_OVERLAY,      /* f64 [4 n_overlay] */
+  GCMF_VALID_BASE,       /* uint8 [n_base] nonzero-area MBR */
+  GCMF_VALID_OVERLAY     /* uint8 [n_overlay] */
+} gcmf_join_field;
+
+/* Clip result fields for gh_clip_get / gh_clip_ptr. */
+typedef enum {
+  GH_STATUS = 0,         /* int32 [n_pairs]: 0 ok, 1 invalid, 2 disjoint, 3 trace error */
+  GH_NCOMP,              /* int32 [n_pairs] result components per pair */
+  GH_COMP_OFFSET,        /* int64 [n_pairs] first component of each pair */
+  GH_COUNT1,             /* int64 [n_pairs] intersecting edge pairs (psP1 total) */
+  GH_COMP_SIZE,          /* int32 [n_components] vertices per component */
+  GH_VERT_OFFSET,        /* int64 [n_pairs] first vertex of each pair */
+  GH_XY,                 /* f64 [2 n_vertices] component vertices, interleaved */
+  GH_SWAPPED             /* int32 [n_pairs] 1 when the overlay polygon was clipped as P */
+} gh_clip_field;
+
+/* ---- context */
+gcmfgh_status gcmfgh_create(int device, gcmfgh_ctx** out);
+gcmfgh_status gcmfgh_destroy(gcmfgh_ctx* ctx);
+/* cudaStream_t as void*; NULL = the context's own stream */
+gcmfgh_status gcmfgh_set_stream(gcmfgh_ctx* ctx, void* stream);
+/* eps: classification tolerance (GH-CUDA/lib/constants.h:4, 1e-7); eps_clean: clean-up
+ * tolerance (polyclip.h:795; 1e-12 where Constants.h:29 overrides it in the merged
+ * build); union_mode: polyclip.h:42 UNION. */
+gcmfgh_status gcmfgh_set_params(gcmfgh_ctx* ctx, double eps, double eps_clean, int union_mode);
+const char* gcmfgh_status_string(gcmfgh_status s);
+/* device error word of the last call (0 none, 1 capacity, 2 trace budget, 4 wait limit) */
+int gcmfgh_last_device_error(gcmfgh_ctx* ctx);
+
+/* ---- join: replaces the stage sequence of spatialJoin (spatialJoin3.cu:197-363) */
+gcmfgh_status gcmf_join(gcmfgh_ctx* ctx, const gcmfgh_layer* base, const gcmfgh_layer* overlay,
+                        gcmfgh_join_info* info);
+/* copy a join field to dst (host if dst_on_device == 0); cap = dst size in bytes;
+ * *bytes receives the field's size (size query: dst NULL) */
+gcmfgh_status gcmf_join_get(gcmfgh_ctx* ctx, int field, void* dst, int64_t cap, int dst_on_device,
+                            int64_t* bytes);
+gcmfgh_status gcmf_join_ptr(gcmfgh_ctx* ctx, int field, const void** dev_ptr, int64_t* count);
+
+/* ---- clip: replaces ghcuda (ghcuda.cpp:385) for a whole batch of pairs.
+ * pid/qid: device int32 [n_pairs] base / overlay polygon ids. */
+gcmfgh_status gh_clip_batch(gcmfgh_ctx* ctx, const gcmfgh_layer* base, const gcmfgh_layer* overlay,
+                            const int32_t* pid, const int32_t* qid, int64_t n_pairs,
+                            gcmfgh_clip_info* info);
+/* clip the clip set of the last gcmf_join on the same layers (no host round trip) */
+gcmfgh_status gh_clip_joined(gcmfgh_ctx* ctx, const gcmfgh_layer* base, const gcmfgh_layer* overlay,
+                             gcmfgh_clip_info* info);
+gcmfgh_status gh_clip_get(gcmfgh_ctx* ctx, int field, void* dst, int64_t cap, int dst_on_device,
+                          int64_t* bytes);
+gcmfgh_status gh_clip_ptr(gcmfgh_ctx* ctx, int field, const void** dev_ptr, int64_t* count);
+
+/* ---- one pair: replaces the per-pair GH_CUDA (ghcuda.cpp:341).  P, Q: host open rings
+ * (no closing vertex) of nP, nQ vertices; P is clipped against Q as given (no swap). */
+gcmfgh_status gh_clip_pair(gcmfgh_ctx* ctx, const double* P, int32_t nP, const double* Q, int32_t nQ,
+                           gcmfgh_clip_info* info);
+
+/* ---- host-resident layers: H2D copies, join, clip of the clip set; results stay on the
+ * device for the *_get calls.  This is the end-to-end path of the reference's main()
+ * (main.cpp:15-29). */
+gcmfgh_status gcmfgh_join_clip_host(gcmfgh_ctx* ctx, const gcmfgh_layer* base_host,
+                                    const gcmfgh_layer* overlay_host, gcmfgh_join_info* jinfo,
+                                    gcmfgh_clip_info* cinfo);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GCMFGH_H */

@@ -643,3 +643,258 @@ void orc_result_copy(int32_t* status, int32_t* ncomp, int64_t* count1, int64_t* 
 }
 
 }  // extern "C"
+
+// ======================================================================= join oracle
+namespace {
+
+struct LayerView {
+  const double* xy; const int32_t* vnum; const int64_t* vps; int64_t n;
+  int64_t start(int64_t i) const { return vps[i] - vnum[i]; }    // first vertex index
+};
+
+// MBR over every stored vertex (SEQ_Overlay.h:316-344); a polygon whose MBR has zero
+// width or height is rejected by the reference reader (":337-344 MBR Error!") and is
+// marked invalid here so it never joins.
+void mbrOf(const LayerView& L, int64_t i, double* m, uint8_t* valid) {
+  int64_t s = L.start(i);
+  int nv = L.vnum[i];
+  double x1 = L.xy[2 * s], y1 = L.xy[2 * s + 1], x2 = x1, y2 = y1;
+  for (int k = 1; k < nv; ++k) {
+    double X = L.xy[2 * (s + k)], Y = L.xy[2 * (s + k) + 1];
+    if (X < x1) x1 = X;
+    if (Y < y1) y1 = Y;
+    if (X > x2) x2 = X;
+    if (Y > y2) y2 = Y;
+  }
+  m[0] = x1; m[1] = y1; m[2] = x2; m[3] = y2;
+  *valid = (nv >= 2 && x1 != x2 && y1 != y2) ? 1 : 0;
+}
+
+inline bool mbrCandidate(const double* b, const double* o) {
+  // sort-based sweep acceptance (GPU_MBR.h:339-415) on exact values, see file header
+  return o[0] <= b[2] && b[0] <= o[2] && !(o[0] == b[2]) && o[1] <= b[3] && b[1] <= o[3];
+}
+
+struct JoinStore {
+  std::vector<int32_t> b, o;
+  std::vector<double> cmbr;
+  std::vector<int8_t> pipType, pipFlag, joinFlag, segFlag, clip;
+  std::vector<int32_t> bE, oE;
+  std::vector<double> mbrB, mbrO;
+  std::vector<uint8_t> validB, validO;
+} g_join;
+
+// point-in-polygon crossing parity of (px,py) against the stored ring of polygon i
+// (GPU_Join.h:882-915 per edge (i, i-1), parity combined by XOR :920-938).
+int pipParity(const LayerView& L, int64_t i, double px, double py) {
+  const double* c = L.xy + 2 * L.start(i);
+  int n = L.vnum[i];
+  int par = 0;
+  for (int a = 0; a < n; ++a) {
+    int j = (a == 0) ? n - 1 : a - 1;
+    double Y1 = c[2 * a + 1], Y2 = c[2 * j + 1], X1 = c[2 * a], X2 = c[2 * j];
+    if ((Y1 > py) == (Y2 > py)) continue;
+    if (px < (X2 - X1) * (py - Y1) / (Y2 - Y1) + X1) par ^= 1;
+  }
+  return par;
+}
+
+// edges of polygon i whose box touches the common MBR (GPU_Join.h:564-580): edge k
+// runs from vertex k to k+1, the last one from the closing vertex back to vertex 0.
+void cmfEdges(const LayerView& L, int64_t i, const double* c, std::vector<int>& out) {
+  const double* v = L.xy + 2 * L.start(i);
+  int n = L.vnum[i];
+  out.clear();
+  for (int k = 0; k < n; ++k) {
+    double x1 = v[2 * k], y1 = v[2 * k + 1];
+    int k2 = (k < n - 1) ? k + 1 : 0;
+    double x2 = v[2 * k2], y2 = v[2 * k2 + 1];
+    if ((c[0] > x1 && c[0] > x2) || (c[2] < x1 && c[2] < x2)) continue;
+    if ((c[1] > y1 && c[1] > y2) || (c[3] < y1 && c[3] < y2)) continue;
+    out.push_back(k);
+  }
+}
+
+// any intersecting pair among the surviving edges (GPU_Join.h:369-446)
+int segmentsIntersect(const LayerView& B, int64_t bi, const std::vector<int>& bl,
+                      const LayerView& O, int64_t oi, const std::vector<int>& ol) {
+  const double* bv = B.xy + 2 * B.start(bi);
+  const double* ov = O.xy + 2 * O.start(oi);
+  int bV = B.vnum[bi], oV = O.vnum[oi];
+  for (int be : bl) {
+    double bX1 = bv[2 * be], bY1 = bv[2 * be + 1];
+    int b2 = (be < bV - 1) ? be + 1 : 0;
+    double bX2 = bv[2 * b2], bY2 = bv[2 * b2 + 1];
+    if (bX1 == bX2 && bY1 == bY2) continue;
+    for (int oe : ol) {
+      double oX1 = ov[2 * oe], oY1 = ov[2 * oe + 1];
+      int o2 = (oe < oV - 1) ? oe + 1 : 0;
+      double oX2 = ov[2 * o2], oY2 = ov[2 * o2 + 1];
+      if (((bX2 < oX1) && (bX2 < oX2)) && ((bX1 < oX1) && (bX1 < oX2))) continue;
+      if (((bX2 > oX1) && (bX2 > oX2)) && ((bX1 > oX1) && (bX1 > oX2))) continue;
+      if (((bY2 < oY1) && (bY2 < oY2)) && ((bY1 < oY1) && (bY1 < oY2))) continue;
+      if (((bY2 > oY1) && (bY2 > oY2)) && ((bY1 > oY1) && (bY1 > oY2))) continue;
+      double denom = ((bX1 - bX2) * (oY1 - oY2)) - ((bY1 - bY2) * (oX1 - oX2));
+      if (denom == 0) {
+        if ((oX1 == oX2 && oX1 == bX1) || (bX1 == bX2 && bX1 == oX1)) return 1;
+        double oM = (oY2 - oY1) / (oX2 - oX1);
+        double bM = (bY2 - bY1) / (bX2 - bX1);
+        double oB = oY1 - oM * oX1;
+        double bB = bY1 - bM * bX1;
+        if (oB == bB) return 1;
+        continue;
+      }
+      double nomX = (((bX1 * bY2) - (bY1 * bX2)) * (oX1 - oX2)) - ((bX1 - bX2) * ((oX1 * oY2) - (oY1 * oX2)));
+      double nomY = ((((bX1 * bY2) - (bY1 * bX2)) * (oY1 - oY2)) - (((bY1 - bY2) * ((oX1 * oY2) - (oY1 * oX2)))));
+      double x0 = nomX / denom, y0 = nomY / denom;
+      if ((x0 > bX1 && x0 > bX2) || (x0 < bX1 && x0 < bX2)) continue;
+      if ((x0 > oX1 && x0 > oX2) || (x0 < oX1 && x0 < oX2)) continue;
+      if ((y0 > bY1 && y0 > bY2) || (y0 < bY1 && y0 < bY2)) continue;
+      if ((y0 > oY1 && y0 > oY2) || (y0 < oY1 && y0 < oY2)) continue;
+      return 1;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_mbr(const double* xy, const int32_t* vnum, const int64_t* vps, int64_t n,
+             double* mbr, uint8_t* valid) {
+  LayerView L{xy, vnum, vps, n};
+  for (int64_t i = 0; i < n; ++i) mbrOf(L, i, mbr + 4 * i, valid + i);
+}
+
+// Candidate pairs by testing every (base, overlay) combination: the pin for the
+// decomposed search in orc_join.  Writes up to cap pairs, returns the count.
+int64_t orc_join_bruteforce(const double* bxy, const int32_t* bvnum, const int64_t* bvps, int64_t nb,
+                            const double* oxy, const int32_t* ovnum, const int64_t* ovps, int64_t no,
+                            int32_t* outB, int32_t* outO, int64_t cap) {
+  LayerView B{bxy, bvnum, bvps, nb}, O{oxy, ovnum, ovps, no};
+  std::vector<double> mb(4 * nb), mo(4 * no);
+  std::vector<uint8_t> vb(nb), vo(no);
+  for (int64_t i = 0; i < nb; ++i) mbrOf(B, i, &mb[4 * i], &vb[i]);
+  for (int64_t i = 0; i < no; ++i) mbrOf(O, i, &mo[4 * i], &vo[i]);
+  int64_t k = 0;
+  for (int64_t i = 0; i < nb; ++i) {
+    if (!vb[i]) continue;
+    for (int64_t j = 0; j < no; ++j) {
+      if (!vo[j] || !mbrCandidate(&mb[4 * i], &mo[4 * j])) continue;
+      if (k < cap) { outB[k] = (int32_t)i; outO[k] = (int32_t)j; }
+      ++k;
+    }
+  }
+  return k;
+}
+
+// The GCMF join: MBR candidates (sorted by base then overlay id), common MBRs,
+// containment candidates and test, common-MBR edge filter, segment refine, and the
+// clip set = contained pairs + pairs with intersecting edges.  Candidates are found by
+// splitting the sweep's two acceptance cases: overlay starts in [x1b, x2b) for each
+// base, base starts in (x1o, x2o] for each overlay; the exact predicate then decides.
+int64_t orc_join(const double* bxy, const int32_t* bvnum, const int64_t* bvps, int64_t nb,
+                 const double* oxy, const int32_t* ovnum, const int64_t* ovps, int64_t no) {
+  LayerView B{bxy, bvnum, bvps, nb}, O{oxy, ovnum, ovps, no};
+  JoinStore& J = g_join;
+  J = JoinStore();
+  J.mbrB.resize(4 * nb); J.mbrO.resize(4 * no); J.validB.resize(nb); J.validO.resize(no);
+  for (int64_t i = 0; i < nb; ++i) mbrOf(B, i, &J.mbrB[4 * i], &J.validB[i]);
+  for (int64_t i = 0; i < no; ++i) mbrOf(O, i, &J.mbrO[4 * i], &J.validO[i]);
+  std::vector<int32_t> sb, so;
+  for (int64_t i = 0; i < nb; ++i) if (J.validB[i]) sb.push_back((int32_t)i);
+  for (int64_t i = 0; i < no; ++i) if (J.validO[i]) so.push_back((int32_t)i);
+  auto byX1 = [](const std::vector<double>& m) {
+    return [&m](int32_t a, int32_t b) { return m[4 * a] < m[4 * b] || (m[4 * a] == m[4 * b] && a < b); };
+  };
+  std::sort(sb.begin(), sb.end(), byX1(J.mbrB));
+  std::sort(so.begin(), so.end(), byX1(J.mbrO));
+  std::vector<double> sbx(sb.size()), sox(so.size());
+  for (size_t i = 0; i < sb.size(); ++i) sbx[i] = J.mbrB[4 * sb[i]];
+  for (size_t i = 0; i < so.size(); ++i) sox[i] = J.mbrO[4 * so[i]];
+  std::vector<std::pair<int32_t, int32_t>> pairs;
+  for (int32_t b : sb) {
+    const double* mb = &J.mbrB[4 * b];
+    size_t lo = std::lower_bound(sox.begin(), sox.end(), mb[0]) - sox.begin();
+    size_t hi = std::lower_bound(sox.begin(), sox.end(), mb[2]) - sox.begin();
+    for (size_t k = lo; k < hi; ++k)
+      if (mbrCandidate(mb, &J.mbrO[4 * so[k]])) pairs.push_back({b, so[k]});
+  }
+  for (int32_t o : so) {
+    const double* mo = &J.mbrO[4 * o];
+    size_t lo = std::upper_bound(sbx.begin(), sbx.end(), mo[0]) - sbx.begin();
+    size_t hi = std::upper_bound(sbx.begin(), sbx.end(), mo[2]) - sbx.begin();
+    for (size_t k = lo; k < hi; ++k)
+      if (mbrCandidate(&J.mbrB[4 * sb[k]], mo)) pairs.push_back({sb[k], o});
+  }
+  std::sort(pairs.begin(), pairs.end());
+  int64_t K = (int64_t)pairs.size();
+  J.b.resize(K); J.o.resize(K); J.cmbr.resize(4 * K); J.pipType.resize(K); J.pipFlag.resize(K);
+  J.joinFlag.resize(K); J.segFlag.resize(K); J.clip.resize(K); J.bE.resize(K); J.oE.resize(K);
+  std::vector<int> bl, ol;
+  for (int64_t k = 0; k < K; ++k) {
+    int32_t b = pairs[k].first, o = pairs[k].second;
+    J.b[k] = b; J.o[k] = o;
+    const double* m1 = &J.mbrB[4 * b];
+    const double* m2 = &J.mbrO[4 * o];
+    double* c = &J.cmbr[4 * k];
+    // GPU_Join.h:475-506
+    double x1 = m1[0], x2 = m1[2], y1 = m1[1], y2 = m1[3];
+    double a1 = m2[0], a2 = m2[2], b1 = m2[1], b2 = m2[3];
+    c[0] = (a1 > x1 ? a1 : x1);
+    c[2] = (a2 < x2 ? a2 : x2);
+    c[1] = (b1 > y1 ? b1 : y1);
+    c[3] = (b2 < y2 ? b2 : y2);
+    int type = 0;
+    if (x1 == c[0] && x2 == c[2] && y1 == c[1] && y2 == c[3]) type = 1;
+    else if (a1 == c[0] && a2 == c[2] && b1 == c[1] && b2 == c[3]) type = 2;
+    J.pipType[k] = (int8_t)type;
+    int join = 1, pip = 0;
+    if (type == 1) {
+      const double* p = B.xy + 2 * B.start(b);
+      pip = pipParity(O, o, p[0], p[1]);
+    } else if (type == 2) {
+      const double* p = O.xy + 2 * O.start(o);
+      pip = pipParity(B, b, p[0], p[1]);
+    }
+    if (pip) join = 0;
+    J.pipFlag[k] = (int8_t)pip;
+    int seg = 0;
+    J.bE[k] = 0; J.oE[k] = 0;
+    if (join) {
+      cmfEdges(B, b, c, bl);
+      cmfEdges(O, o, c, ol);
+      if (bl.empty() || ol.empty()) join = 0;
+      else { J.bE[k] = (int32_t)bl.size(); J.oE[k] = (int32_t)ol.size(); }
+      if (join) seg = segmentsIntersect(B, b, bl, O, o, ol);
+    }
+    J.joinFlag[k] = (int8_t)join;
+    J.segFlag[k] = (int8_t)seg;
+    J.clip[k] = (int8_t)(pip || seg);
+  }
+  return K;
+}
+
+// Copies the last orc_join result; any pointer may be null.
+void orc_join_copy(int32_t* b, int32_t* o, double* cmbr, int8_t* pipType, int8_t* pipFlag,
+                   int8_t* joinFlag, int32_t* bE, int32_t* oE, int8_t* segFlag, int8_t* clip,
+                   double* mbrB, uint8_t* validB, double* mbrO, uint8_t* validO) {
+  JoinStore& J = g_join;
+  if (b) std::copy(J.b.begin(), J.b.end(), b);
+  if (o) std::copy(J.o.begin(), J.o.end(), o);
+  if (cmbr) std::copy(J.cmbr.begin(), J.cmbr.end(), cmbr);
+  if (pipType) std::copy(J.pipType.begin(), J.pipType.end(), pipType);
+  if (pipFlag) std::copy(J.pipFlag.begin(), J.pipFlag.end(), pipFlag);
+  if (joinFlag) std::copy(J.joinFlag.begin(), J.joinFlag.end(), joinFlag);
+  if (bE) std::copy(J.bE.begin(), J.bE.end(), bE);
+  if (oE) std::copy(J.oE.begin(), J.oE.end(), oE);
+  if (segFlag) std::copy(J.segFlag.begin(), J.segFlag.end(), segFlag);
+  if (clip) std::copy(J.clip.begin(), J.clip.end(), clip);
+  if (mbrB) std::copy(J.mbrB.begin(), J.mbrB.end(), mbrB);
+  if (validB) std::copy(J.validB.begin(), J.validB.end(), validB);
+  if (mbrO) std::copy(J.mbrO.begin(), J.mbrO.end(), mbrO);
+  if (validO) std::copy(J.validO.begin(), J.validO.end(), validO);
+}
+
+}  // extern "C"

@@ -167,3 +167,73 @@ def ref_time_pairs(pairs, reps=1, union=False):
         cmd = [REF_BIN, "time", fin, str(reps)] + (["union"] if union else [])
         out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout.split()
         return float(out[0]), int(out[1])
+
+
+# ---------------------------------------------------------------- join
+
+class JoinResult:
+    pass
+
+
+def _join_lib():
+    L = lib()
+    if not getattr(L, "_join_ready", False):
+        vp, i64 = ctypes.c_void_p, ctypes.c_int64
+        L.orc_join.argtypes = [vp, vp, vp, i64, vp, vp, vp, i64]
+        L.orc_join.restype = i64
+        L.orc_join_copy.argtypes = [vp] * 14
+        L.orc_join_copy.restype = None
+        L.orc_join_bruteforce.argtypes = [vp, vp, vp, i64, vp, vp, vp, i64, vp, vp, i64]
+        L.orc_join_bruteforce.restype = i64
+        L.orc_mbr.argtypes = [vp, vp, vp, i64, vp, vp]
+        L.orc_mbr.restype = None
+        L._join_ready = True
+    return L
+
+
+def mbr(layer):
+    L = _join_lib()
+    m = np.zeros(4 * layer.n_polys, np.float64)
+    v = np.zeros(layer.n_polys, np.uint8)
+    L.orc_mbr(_p(layer.xy), _p(layer.vnum), _p(layer.vps), layer.n_polys, _p(m), _p(v))
+    return m.reshape(-1, 4), v
+
+
+def join(base, overlay):
+    L = _join_lib()
+    K = L.orc_join(_p(base.xy), _p(base.vnum), _p(base.vps), base.n_polys,
+                   _p(overlay.xy), _p(overlay.vnum), _p(overlay.vps), overlay.n_polys)
+    r = JoinResult()
+    r.b = np.zeros(K, np.int32)
+    r.o = np.zeros(K, np.int32)
+    r.cmbr = np.zeros(4 * K, np.float64)
+    r.pip_type = np.zeros(K, np.int8)
+    r.pip_flag = np.zeros(K, np.int8)
+    r.join_flag = np.zeros(K, np.int8)
+    r.bE = np.zeros(K, np.int32)
+    r.oE = np.zeros(K, np.int32)
+    r.seg_flag = np.zeros(K, np.int8)
+    r.clip = np.zeros(K, np.int8)
+    r.mbr_b = np.zeros(4 * base.n_polys, np.float64)
+    r.valid_b = np.zeros(base.n_polys, np.uint8)
+    r.mbr_o = np.zeros(4 * overlay.n_polys, np.float64)
+    r.valid_o = np.zeros(overlay.n_polys, np.uint8)
+    L.orc_join_copy(_p(r.b), _p(r.o), _p(r.cmbr), _p(r.pip_type), _p(r.pip_flag),
+                    _p(r.join_flag), _p(r.bE), _p(r.oE), _p(r.seg_flag), _p(r.clip),
+                    _p(r.mbr_b), _p(r.valid_b), _p(r.mbr_o), _p(r.valid_o))
+    r.cmbr = r.cmbr.reshape(-1, 4)
+    return r
+
+
+def join_bruteforce(base, overlay):
+    L = _join_lib()
+    cap = 1 << 22
+    while True:
+        ob = np.zeros(cap, np.int32)
+        oo = np.zeros(cap, np.int32)
+        k = L.orc_join_bruteforce(_p(base.xy), _p(base.vnum), _p(base.vps), base.n_polys,
+                                  _p(overlay.xy), _p(overlay.vnum), _p(overlay.vps),
+                                  overlay.n_polys, _p(ob), _p(oo), cap)
+        if k <= cap:
+            return ob[:k].copy(), oo[:k].copy()
+        cap = int(k)
