@@ -11,6 +11,11 @@
 
 namespace gcmfgh {
 
+unsigned long long& launch_counter() {
+  static unsigned long long n = 0;
+  return n;
+}
+
 void* Arena::take(size_t bytes) {
   bytes = (bytes + 255) & ~size_t(255);
   while (cur_ < chunks_.size()) {
@@ -83,6 +88,7 @@ struct gcmfgh_ctx {
   const double* join_b = nullptr;
   const double* join_o = nullptr;
   int64_t join_nb = 0, join_no = 0;
+  Marks marks[2];                 // stage timing of the last join / clip
 };
 
 namespace {
@@ -121,11 +127,13 @@ gcmfgh_status clip_info(gcmfgh_ctx* c, gcmfgh_clip_info* info) {
   info->n_pairs = c->clip.n_pairs;
   info->n_components = c->clip.n_components;
   info->n_vertices = c->clip.n_vertices;
+  info->n_records = c->clip.n_records;
+  info->n_ring_vertices = c->clip.n_ring_vertices;
   info->n_invalid = info->n_disjoint = info->n_error = 0;
   if (c->clip.n_pairs > 0) {
     cudaMemsetAsync(c->d_stats, 0, 3 * sizeof(unsigned long long), c->stream);
-    clip_stats_kernel<<<(unsigned)((c->clip.n_pairs + kThreads - 1) / kThreads), kThreads, 0, c->stream>>>(
-        c->clip.status, c->clip.n_pairs, c->d_stats);
+    { clip_stats_kernel<<<(unsigned)((c->clip.n_pairs + kThreads - 1) / kThreads), kThreads, 0, c->stream>>>(
+        c->clip.status, c->clip.n_pairs, c->d_stats); note_launch(); }
     cudaMemcpyAsync(c->h_scratch, c->d_stats, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GCMFGH_CUDA_ERROR;
     info->n_invalid = c->h_scratch[0];
@@ -139,9 +147,10 @@ gcmfgh_status run_clip_ctx(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_la
                            const int32_t* pid, const int32_t* qid, int64_t n, gcmfgh_clip_info* info) {
   c->clip_arena.reset();
   c->have_clip = false;
+  c->marks[1].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   int st = run_clip(to_dev(b), to_dev(o), pid, qid, n, c->prm, c->clip_arena, c->clip, c->d_err,
-                    c->h_scratch, c->stream);
+                    c->h_scratch, c->stream, &c->marks[1]);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_clip = true;
@@ -241,8 +250,29 @@ gcmfgh_status gcmfgh_create(int device, gcmfgh_ctx** out) {
   }
   c->stream = c->own;
   cudaMemset(c->d_err, 0, 64);
+  for (auto& m : c->marks)
+    for (int i = 0; i < Marks::kMax; ++i) cudaEventCreate(&m.ev[i]);
   *out = c;
   return GCMFGH_OK;
+}
+
+gcmfgh_status gcmfgh_set_timing(gcmfgh_ctx* c, int on) {
+  if (!c) return GCMFGH_INVALID_ARGUMENT;
+  c->marks[0].on = c->marks[1].on = (on != 0);
+  return GCMFGH_OK;
+}
+
+int gcmfgh_get_timing(gcmfgh_ctx* c, int which, float* ms, const char** names, int cap) {
+  if (!c || which < 0 || which > 1) return -1;
+  Marks& m = c->marks[which];
+  int n = m.n > 1 ? m.n - 1 : 0;
+  for (int i = 0; i < n && i < cap; ++i) {
+    float t = 0;
+    cudaEventElapsedTime(&t, m.ev[i], m.ev[i + 1]);
+    if (ms) ms[i] = t;
+    if (names) names[i] = m.name[i + 1];
+  }
+  return n;
 }
 
 gcmfgh_status gcmfgh_destroy(gcmfgh_ctx* c) {
@@ -257,6 +287,9 @@ gcmfgh_status gcmfgh_destroy(gcmfgh_ctx* c) {
   if (c->d_stats) cudaFree(c->d_stats);
   if (c->h_scratch) cudaFreeHost(c->h_scratch);
   if (c->own) cudaStreamDestroy(c->own);
+  for (auto& m : c->marks)
+    for (int i = 0; i < Marks::kMax; ++i)
+      if (m.ev[i]) cudaEventDestroy(m.ev[i]);
   delete c;
   return GCMFGH_OK;
 }
@@ -277,13 +310,17 @@ gcmfgh_status gcmfgh_set_params(gcmfgh_ctx* c, double eps, double eps_clean, int
 
 int gcmfgh_last_device_error(gcmfgh_ctx* c) { return c ? c->last_err : -1; }
 
+unsigned long long gcmfgh_launch_count(void) { return launch_counter(); }
+
 gcmfgh_status gcmf_join(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, gcmfgh_join_info* info) {
   if (!c || !layer_ok(b) || !layer_ok(o)) return GCMFGH_INVALID_ARGUMENT;
   cudaSetDevice(c->device);
   c->join_arena.reset();
   c->have_join = false;
+  c->marks[0].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
-  int st = run_join(to_dev(b), to_dev(o), c->join_arena, c->join, c->d_err, c->h_scratch, c->stream);
+  int st = run_join(to_dev(b), to_dev(o), c->join_arena, c->join, c->d_err, c->h_scratch, c->stream,
+                    &c->marks[0]);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_join = true;
@@ -384,6 +421,36 @@ gcmfgh_status gh_clip_pair(gcmfgh_ctx* c, const double* P, int32_t nP, const dou
   gcmfgh_status r = run_clip_ctx(c, &lb, &lo, ids, ids + 1, 1, info);
   c->prm.no_swap = 0;
   return r;
+}
+
+gcmfgh_status gcmfgh_exclusive_scan_i32(gcmfgh_ctx* c, const int32_t* d_in, int64_t* d_out, int64_t n,
+                                        int64_t* total) {
+  if (!c || n < 0 || (n > 0 && (!d_in || !d_out))) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->pair_arena.reset();
+  void* tmp = c->pair_arena.take(scan_temp_bytes(n > 0 ? n : 1));
+  int64_t* d_tot = c->pair_arena.take_n<int64_t>(1);
+  if (!tmp || !d_tot) return GCMFGH_OUT_OF_MEMORY;
+  cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  exclusive_scan_i32(d_in, d_out, n, d_tot, tmp, c->d_err, c->stream);
+  cudaMemcpyAsync(c->h_scratch + 32, d_tot, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream);
+  gcmfgh_status r = finish(c, ST_OK);
+  if (r == GCMFGH_OK && total) *total = c->h_scratch[32];
+  return r;
+}
+
+gcmfgh_status gcmfgh_radix_sort_u64(gcmfgh_ctx* c, uint64_t* d_keys, uint32_t* d_vals, int64_t n, int key_bits) {
+  if (!c || n < 0 || (n > 0 && (!d_keys || !d_vals)) || key_bits < 0 || key_bits > 64)
+    return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->pair_arena.reset();
+  uint64_t* ka = c->pair_arena.take_n<uint64_t>(n);
+  uint32_t* va = c->pair_arena.take_n<uint32_t>(n);
+  void* tmp = c->pair_arena.take(radix_temp_bytes(n > 0 ? n : 1));
+  if (!ka || !va || !tmp) return GCMFGH_OUT_OF_MEMORY;
+  cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  radix_sort_pairs(d_keys, d_vals, ka, va, n, ((key_bits + 7) / 8) * 8, tmp, c->d_err, c->stream);
+  return finish(c, ST_OK);
 }
 
 gcmfgh_status gcmfgh_join_clip_host(gcmfgh_ctx* c, const gcmfgh_layer* bh, const gcmfgh_layer* oh,

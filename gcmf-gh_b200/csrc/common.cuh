@@ -26,6 +26,10 @@ GCMFGH_DEV void raise_error(int* err, int code) {
   if (err) atomicCAS(err, 0, code);
 }
 
+// host-side count of kernel launches issued by the library (gcmfgh_launch_count)
+unsigned long long& launch_counter();
+inline void note_launch() { ++launch_counter(); }
+
 // ---- geometry (reference arithmetic, see file header)
 
 // twice the signed area of the triangle (P,Q,R): point2D.h:78-80, gppolyclip_mDIV512.cu:16-18

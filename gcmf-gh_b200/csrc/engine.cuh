@@ -79,6 +79,8 @@ struct ClipParams {
 // Clip outputs (device, owned by the clip arena).
 struct ClipDev {
   int64_t n_pairs = 0, n_components = 0, n_vertices = 0;
+  int64_t n_records = 0;          // intersection records (all pairs)
+  int64_t n_ring_vertices = 0;    // merged-ring vertices, P and Q sides (valid pairs)
   int32_t* status = nullptr;      // per pair: 0 ok, 1 invalid (P/Q counts differ), 2 disjoint MBRs, 3 trace error
   int32_t* ncomp = nullptr;       // per pair
   int64_t* comp_off = nullptr;    // per pair, first component index
@@ -89,17 +91,28 @@ struct ClipDev {
   int32_t* swapped = nullptr;     // per pair: 1 when the overlay polygon was P
 };
 
-struct Timing {
-  float ms[16] = {0};
+// Optional stage timing: an event is recorded on the launching stream at each mark, so
+// the time between consecutive marks is the device time of the stage in between.
+struct Marks {
+  static constexpr int kMax = 24;
+  cudaEvent_t ev[kMax] = {};
+  const char* name[kMax] = {};
+  int n = 0;
+  bool on = false;
+  void mark(const char* label, cudaStream_t s) {
+    if (!on || n >= kMax) return;
+    name[n] = label;
+    cudaEventRecord(ev[n++], s);
+  }
 };
 
 int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s);
 
 int run_join(const LayerDev& base, const LayerDev& ovl, Arena& arena, JoinDev& out,
-             int* d_err, int64_t* h_scratch, cudaStream_t s);
+             int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);
 
 int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, const int32_t* d_qid,
              int64_t n_pairs, const ClipParams& prm, Arena& arena, ClipDev& out,
-             int* d_err, int64_t* h_scratch, cudaStream_t s);
+             int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);
 
 }  // namespace gcmfgh

@@ -802,8 +802,11 @@ out_compact_kernel(int64_t K, const double* __restrict__ xy, const int64_t* __re
 
 int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const int32_t* d_qid,
              int64_t K, const ClipParams& prm, Arena& A, ClipDev& C, int* d_err, int64_t* hs,
-             cudaStream_t s) {
+             cudaStream_t s, Marks* mk) {
+  Marks dummy;
+  if (!mk) mk = &dummy;
   C = ClipDev();
+  mk->mark("clip:start", s);
   C.n_pairs = K;
   if (K <= 0) return ST_OK;
   auto sync = [&]() { return cudaStreamSynchronize(s) == cudaSuccess; };
@@ -834,16 +837,17 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (!D.pS || !D.qS || !D.nP || !D.nQ || !D.pSide || !D.cmbr || !D.status || !C.swapped || !C.count1 ||
       !cP || !cQ || !offP || !offQ || !nchunk || !chunkOff || !eoffP || !eoffQ || !tot || !stK)
     return ST_OUT_OF_MEMORY;
-  setup_kernel<<<blocks_for(K), kThreads, 0, s>>>(Lb, Lo, d_pid, d_qid, K, mb, mo, D, C.swapped, prm.no_swap);
+  { setup_kernel<<<blocks_for(K), kThreads, 0, s>>>(Lb, Lo, d_pid, d_qid, K, mb, mo, D, C.swapped, prm.no_swap); note_launch(); }
   // ---- G1 edge filter
-  edge_filter_kernel<0><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, nullptr, nullptr,
-                                                                 nullptr, nullptr);
+  { edge_filter_kernel<0><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, nullptr, nullptr,
+                                                                 nullptr, nullptr); note_launch(); }
   exclusive_scan_i32(cP, offP, K, tot + 0, stK, d_err, s);
   exclusive_scan_i32(cQ, offQ, K, tot + 1, stK, d_err, s);
   exclusive_scan_i32(D.nP, eoffP, K, tot + 2, stK, d_err, s);
   exclusive_scan_i32(D.nQ, eoffQ, K, tot + 3, stK, d_err, s);
-  chunk_count_kernel<<<blocks_for(K), kThreads, 0, s>>>(cP, cQ, K, nchunk);
+  { chunk_count_kernel<<<blocks_for(K), kThreads, 0, s>>>(cP, cQ, K, nchunk); note_launch(); }
   exclusive_scan_i64(nchunk, chunkOff, K, tot + 4, stK, d_err, s);
+  mk->mark("clip:setup+filter", s);
   cudaMemcpyAsync(hs, tot, 5 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
   const int64_t nLP = hs[0], nLQ = hs[1], nEP = hs[2], nEQ = hs[3], nCh = hs[4];
@@ -855,12 +859,12 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int64_t* qScan = A.take_n<int64_t>(nCh);
   void* stC = A.take(scan_temp_bytes(std::max<int64_t>(nCh, 1)));
   if (!LP || !LQ || !chunkRec || !chunkQ || !recScan || !qScan || !stC) return ST_OUT_OF_MEMORY;
-  edge_filter_kernel<1><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ);
+  { edge_filter_kernel<1><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ); note_launch(); }
   // ---- G2 count
   Records R{};
   if (nCh > 0) {
-    intersect_kernel<0><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, chunkRec, chunkQ, nullptr, R);
+    { intersect_kernel<0><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, chunkRec, chunkQ, nullptr, R); note_launch(); }
     exclusive_scan_i32(chunkRec, recScan, nCh, tot + 5, stC, d_err, s);
     exclusive_scan_i32(chunkQ, qScan, nCh, tot + 6, stC, d_err, s);
   } else {
@@ -869,8 +873,9 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int64_t* recOff = A.take_n<int64_t>(K);
   int32_t* nrec = A.take_n<int32_t>(K);
   if (!recOff || !nrec) return ST_OUT_OF_MEMORY;
-  pair_records_kernel<<<blocks_for(K), kThreads, 0, s>>>(chunkOff, nchunk, recScan, qScan, chunkRec, chunkQ,
-                                                         K, recOff, nrec, C.count1, D);
+  { pair_records_kernel<<<blocks_for(K), kThreads, 0, s>>>(chunkOff, nchunk, recScan, qScan, chunkRec, chunkQ,
+                                                         K, recOff, nrec, C.count1, D); note_launch(); }
+  mk->mark("clip:count", s);
   cudaMemcpyAsync(hs, tot + 5, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
   const int64_t nR = hs[0];
@@ -880,8 +885,9 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   R.t = A.take_n<int8_t>(nR); R.k = A.take_n<int32_t>(nR);
   if (!R.p || !R.q || !R.a || !R.b || !R.t || !R.k) return ST_OUT_OF_MEMORY;
   if (nCh > 0)
-    intersect_kernel<1><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, R);
+    { intersect_kernel<1><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, R); note_launch(); }
+  mk->mark("clip:emit", s);
   // ---- G4 ring layout
   int32_t* insP = A.take_n<int32_t>(nEP);
   int32_t* insQ = A.take_n<int32_t>(nEQ);
@@ -908,10 +914,10 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   cudaMemsetAsync(curP, 0, nEP * sizeof(int32_t), s);
   cudaMemsetAsync(curQ, 0, nEQ * sizeof(int32_t), s);
   if (nR > 0)
-    record_count_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, eoffP, eoffQ, D.status, insP, insQ,
-                                                            srcLinkP, srcLinkQ);
-  edge_slots_kernel<<<blocks_for(nEP), kThreads, 0, s>>>(insP, nEP, szP);
-  edge_slots_kernel<<<blocks_for(nEQ), kThreads, 0, s>>>(insQ, nEQ, szQ);
+    { record_count_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, eoffP, eoffQ, D.status, insP, insQ,
+                                                            srcLinkP, srcLinkQ); note_launch(); }
+  { edge_slots_kernel<<<blocks_for(nEP), kThreads, 0, s>>>(insP, nEP, szP); note_launch(); }
+  { edge_slots_kernel<<<blocks_for(nEQ), kThreads, 0, s>>>(insQ, nEQ, szQ); note_launch(); }
   exclusive_scan_i32(szP, vposP, nEP, tot + 7, stE, d_err, s);
   exclusive_scan_i32(szQ, vposQ, nEQ, tot + 8, stE, d_err, s);
   exclusive_scan_i32(insP, insBaseP, nEP, tot + 9, stE, d_err, s);
@@ -929,17 +935,25 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int64_t* regQ = A.take_n<int64_t>(K);
   if (!insListP || !insListQ || !mP || !mQ || !regSizeP || !regSizeQ || !regP || !regQ) return ST_OUT_OF_MEMORY;
   if (nR > 0)
-    record_scatter_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, eoffP, eoffQ, D.status, insBaseP, curP,
-                                                              insListP, insBaseQ, curQ, insListQ);
-  pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffP, vposP, D.nP, nrec, D.status, K, nEP, vtotP, mP,
-                                                      regSizeP);
-  pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffQ, vposQ, D.nQ, nrec, D.status, K, nEQ, vtotQ, mQ,
-                                                      regSizeQ);
+    { record_scatter_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, eoffP, eoffQ, D.status, insBaseP, curP,
+                                                              insListP, insBaseQ, curQ, insListQ); note_launch(); }
+  { pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffP, vposP, D.nP, nrec, D.status, K, nEP, vtotP, mP,
+                                                      regSizeP); note_launch(); }
+  { pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffQ, vposQ, D.nQ, nrec, D.status, K, nEQ, vtotQ, mQ,
+                                                      regSizeQ); note_launch(); }
   exclusive_scan_i64(regSizeP, regP, K, tot + 11, stK, d_err, s);
   exclusive_scan_i64(regSizeQ, regQ, K, tot + 12, stK, d_err, s);
-  cudaMemcpyAsync(hs, tot + 11, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  {
+    int64_t* junk = A.take_n<int64_t>(K);
+    if (!junk) return ST_OUT_OF_MEMORY;
+    exclusive_scan_i32(mP, junk, K, tot + 13, stK, d_err, s);
+    exclusive_scan_i32(mQ, junk, K, tot + 14, stK, d_err, s);
+  }
+  cudaMemcpyAsync(hs, tot + 11, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
   const int64_t regTotP = hs[0], regTotQ = hs[1];
+  C.n_ring_vertices = hs[2] + hs[3];
+  C.n_records = nR;
   auto take_ring = [&](int64_t n, RingSet& S) {
     S.x = A.take_n<double>(n); S.y = A.take_n<double>(n);
     S.nx = A.take_n<int32_t>(n); S.pv = A.take_n<int32_t>(n); S.nb = A.take_n<int32_t>(n);
@@ -949,17 +963,18 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   };
   RingSet SP, SQ;
   if (!take_ring(regTotP, SP) || !take_ring(regTotQ, SQ)) return ST_OUT_OF_MEMORY;
+  mk->mark("clip:layout", s);
   // ---- G5 ring fill
   if (nEP > 0)
-    ring_fill_kernel<0><<<blocks_for(nEP), kThreads, 0, s>>>(Lb, Lo, D, R, eoffP, nEP, K, vposP, regP, mP, SP,
-                                                             slotP, insBaseP, curP, insListP);
+    { ring_fill_kernel<0><<<blocks_for(nEP), kThreads, 0, s>>>(Lb, Lo, D, R, eoffP, nEP, K, vposP, regP, mP, SP,
+                                                             slotP, insBaseP, curP, insListP); note_launch(); }
   if (nEQ > 0)
-    ring_fill_kernel<1><<<blocks_for(nEQ), kThreads, 0, s>>>(Lb, Lo, D, R, eoffQ, nEQ, K, vposQ, regQ, mQ, SQ,
-                                                             slotQ, insBaseQ, curQ, insListQ);
+    { ring_fill_kernel<1><<<blocks_for(nEQ), kThreads, 0, s>>>(Lb, Lo, D, R, eoffQ, nEQ, K, vposQ, regQ, mQ, SQ,
+                                                             slotQ, insBaseQ, curQ, insListQ); note_launch(); }
   // ---- G6 links
   if (nR > 0)
-    link_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, D.status, eoffP, eoffQ, vposP, vposQ, regP, regQ,
-                                                    slotP, slotQ, srcLinkP, srcLinkQ, SP, SQ);
+    { link_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, D.status, eoffP, eoffQ, vposP, vposQ, regP, regQ,
+                                                    slotP, slotQ, srcLinkP, srcLinkQ, SP, SQ); note_launch(); }
   // ---- G7 label + trace into per-pair output regions
   int64_t* vcap = A.take_n<int64_t>(K);
   int32_t* ccap = A.take_n<int32_t>(K);
@@ -968,7 +983,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int32_t* nc = A.take_n<int32_t>(K);
   int64_t* nv = A.take_n<int64_t>(K);
   if (!vcap || !ccap || !vOff || !cOff || !nc || !nv) return ST_OUT_OF_MEMORY;
-  out_sizes_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, nrec, D.status, K, vcap, ccap);
+  { out_sizes_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, nrec, D.status, K, vcap, ccap); note_launch(); }
   exclusive_scan_i64(vcap, vOff, K, tot + 13, stK, d_err, s);
   exclusive_scan_i32(ccap, cOff, K, tot + 14, stK, d_err, s);
   cudaMemcpyAsync(hs, tot + 13, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
@@ -976,9 +991,11 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   double* oxy = A.take_n<double>(2 * hs[0]);
   int32_t* ocsz = A.take_n<int32_t>(hs[1]);
   if (!oxy || !ocsz) return ST_OUT_OF_MEMORY;
-  label_trace_kernel<<<(unsigned)((K + 127) / 128), 128, 0, s>>>(D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ,
+  mk->mark("clip:fill+link", s);
+  { label_trace_kernel<<<(unsigned)((K + 127) / 128), 128, 0, s>>>(D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ,
                                                                   SP, SQ, oxy, vOff, vcap, ocsz, cOff, ccap, nc,
-                                                                  nv, prm, d_err);
+                                                                  nv, prm, d_err); note_launch(); }
+  mk->mark("clip:label+trace", s);
   // ---- G8 compaction
   C.ncomp = nc;
   C.comp_off = A.take_n<int64_t>(K);
@@ -993,9 +1010,10 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   C.xy = A.take_n<double>(2 * C.n_vertices);
   C.comp_size = A.take_n<int32_t>(C.n_components);
   if (!C.xy || !C.comp_size) return ST_OUT_OF_MEMORY;
-  out_compact_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(K, oxy, vOff, ocsz, cOff, nc, nv, fVOff,
-                                                              C.comp_off, C.xy, C.comp_size);
+  { out_compact_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(K, oxy, vOff, ocsz, cOff, nc, nv, fVOff,
+                                                              C.comp_off, C.xy, C.comp_size); note_launch(); }
   C.vert_off = fVOff;
+  mk->mark("clip:compact", s);
   return ST_OK;
 }
 

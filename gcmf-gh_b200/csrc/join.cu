@@ -352,13 +352,16 @@ int bits_for(int64_t n) {
 }  // namespace
 
 int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s) {
-  if (L.n > 0) mbr_only_kernel<<<blocks_for_warps(L.n), kThreads, 0, s>>>(L, mbr);
+  if (L.n > 0) { mbr_only_kernel<<<blocks_for_warps(L.n), kThreads, 0, s>>>(L, mbr); note_launch(); }
   return ST_OK;
 }
 
 int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* d_err,
-             int64_t* h_scratch, cudaStream_t s) {
+             int64_t* h_scratch, cudaStream_t s, Marks* mk) {
+  Marks dummy;
+  if (!mk) mk = &dummy;
   J = JoinDev();
+  mk->mark("join:start", s);
   const int64_t nb = Lb.n, no = Lo.n;
   if (nb <= 0 || no <= 0) return ST_OK;
   // ---- J0 MBRs + sort keys
@@ -377,11 +380,12 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
       !vAlt || !d_cnt || !tmp)
     return ST_OUT_OF_MEMORY;
   cudaMemsetAsync(d_cnt, 0, 8 * sizeof(unsigned long long), s);
-  mbr_kernel<<<blocks_for_warps(nb), kThreads, 0, s>>>(Lb, J.mbr_b, J.valid_b, keyB, idB, d_cnt + 0);
-  mbr_kernel<<<blocks_for_warps(no), kThreads, 0, s>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1);
+  { mbr_kernel<<<blocks_for_warps(nb), kThreads, 0, s>>>(Lb, J.mbr_b, J.valid_b, keyB, idB, d_cnt + 0); note_launch(); }
+  { mbr_kernel<<<blocks_for_warps(no), kThreads, 0, s>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1); note_launch(); }
   // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
   radix_sort_pairs(keyB, idB, kAlt, vAlt, nb, 64, tmp, d_err, s);
   radix_sort_pairs(keyO, idO, kAlt, vAlt, no, 64, tmp, d_err, s);
+  mk->mark("join:mbr+sort", s);
   cudaMemcpyAsync(h_scratch, d_cnt, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
   const int64_t nvb = h_scratch[0], nvo = h_scratch[1];
@@ -395,21 +399,22 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   if (!SB.x1 || !SB.x2 || !SB.y1 || !SB.y2 || !SB.id || !SO.x1 || !SO.x2 || !SO.y1 || !SO.y2 ||
       !SO.id || !cnt || !offs || !d_total)
     return ST_OUT_OF_MEMORY;
-  if (nvb) gather_sorted_kernel<<<blocks_for(nvb), kThreads, 0, s>>>(J.mbr_b, idB, nvb, SB);
-  if (nvo) gather_sorted_kernel<<<blocks_for(nvo), kThreads, 0, s>>>(J.mbr_o, idO, nvo, SO);
+  if (nvb) { gather_sorted_kernel<<<blocks_for(nvb), kThreads, 0, s>>>(J.mbr_b, idB, nvb, SB); note_launch(); }
+  if (nvo) { gather_sorted_kernel<<<blocks_for(nvo), kThreads, 0, s>>>(J.mbr_o, idO, nvo, SO); note_launch(); }
   // ---- J2 sweep: count, scan, emit, canonical sort
   const int obits = bits_for(no);
   const int bbits = bits_for(nb);
   if (obits + bbits > 64) return ST_INVALID_ARGUMENT;
   const int64_t ne = nvb + nvo;
   if (ne > 0) {
-    sweep_kernel<0><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr, nullptr, obits);
+    { sweep_kernel<0><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr, nullptr, obits); note_launch(); }
     void* stmp = A.take(scan_temp_bytes(ne));
     if (!stmp) return ST_OUT_OF_MEMORY;
     exclusive_scan_i32(cnt, offs, ne, d_total, stmp, d_err, s);
   } else {
     cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
   }
+  mk->mark("join:sweep-count", s);
   cudaMemcpyAsync(h_scratch, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
   const int64_t K = h_scratch[0];
@@ -421,8 +426,9 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   uint32_t* pvAlt = A.take_n<uint32_t>(K);
   void* rtmp = A.take(radix_temp_bytes(K));
   if (!pkeys || !pvals || !pkAlt || !pvAlt || !rtmp) return ST_OUT_OF_MEMORY;
-  sweep_kernel<1><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs, pkeys, obits);
+  { sweep_kernel<1><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs, pkeys, obits); note_launch(); }
   radix_sort_pairs(pkeys, pvals, pkAlt, pvAlt, K, ((obits + bbits + 7) / 8) * 8, rtmp, d_err, s);
+  mk->mark("join:sweep-emit+sort", s);
   // ---- J3 CMBR + containment candidates
   J.b = A.take_n<int32_t>(K); J.o = A.take_n<int32_t>(K);
   J.cmbr = A.take_n<double>(4 * K);
@@ -437,14 +443,15 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   if (!J.b || !J.o || !J.cmbr || !J.pip_type || !J.pip_flag || !J.join_flag || !J.seg_flag || !J.clip ||
       !J.bE || !J.oE || !bOff || !oOff || !clipU8 || !clipOff || !stmpK)
     return ST_OUT_OF_MEMORY;
-  cmbr_kernel<<<blocks_for(K), kThreads, 0, s>>>(pkeys, K, obits, J.mbr_b, J.mbr_o, J.b, J.o, J.cmbr,
-                                                 J.pip_type);
+  { cmbr_kernel<<<blocks_for(K), kThreads, 0, s>>>(pkeys, K, obits, J.mbr_b, J.mbr_o, J.b, J.o, J.cmbr,
+                                                 J.pip_type); note_launch(); }
   // ---- J4 point in polygon
-  pip_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.pip_type, K, J.pip_flag,
-                                                      J.join_flag);
+  { pip_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.pip_type, K, J.pip_flag,
+                                                      J.join_flag); note_launch(); }
+  mk->mark("join:cmbr+pip", s);
   // ---- J5 common-MBR edge filter: count, offsets, lists
-  cmf_kernel<0><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
-                                                         J.oE, nullptr, nullptr, nullptr, nullptr);
+  { cmf_kernel<0><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                         J.oE, nullptr, nullptr, nullptr, nullptr); note_launch(); }
   exclusive_scan_i32(J.bE, bOff, K, d_total + 1, stmpK, d_err, s);
   exclusive_scan_i32(J.oE, oOff, K, d_total + 2, stmpK, d_err, s);
   cudaMemcpyAsync(h_scratch, d_total + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
@@ -453,14 +460,16 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   int32_t* bList = A.take_n<int32_t>(nBl);
   int32_t* oList = A.take_n<int32_t>(nOl);
   if (!bList || !oList) return ST_OUT_OF_MEMORY;
-  cmf_kernel<1><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
-                                                         J.oE, bOff, oOff, bList, oList);
+  { cmf_kernel<1><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                         J.oE, bOff, oOff, bList, oList); note_launch(); }
+  mk->mark("join:cmf", s);
   // ---- J6 refine
-  refine_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, K, J.join_flag, J.bE, J.oE,
-                                                         bOff, oOff, bList, oList, J.seg_flag);
+  { refine_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, K, J.join_flag, J.bE, J.oE,
+                                                         bOff, oOff, bList, oList, J.seg_flag); note_launch(); }
+  mk->mark("join:refine", s);
   // ---- clip set = containment pairs + pairs with intersecting edges
-  clip_flag_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.pip_type, J.pip_flag, J.join_flag, J.seg_flag, K,
-                                                      J.clip, clipU8, d_cnt + 2);
+  { clip_flag_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.pip_type, J.pip_flag, J.join_flag, J.seg_flag, K,
+                                                      J.clip, clipU8, d_cnt + 2); note_launch(); }
   exclusive_scan_u8(clipU8, clipOff, K, d_total + 3, stmpK, d_err, s);
   cudaMemcpyAsync(h_scratch, d_total + 3, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(h_scratch + 1, d_cnt + 2, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
@@ -473,7 +482,8 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   J.clip_b = A.take_n<int32_t>(J.n_clip);
   J.clip_o = A.take_n<int32_t>(J.n_clip);
   if (!J.clip_b || !J.clip_o) return ST_OUT_OF_MEMORY;
-  clip_compact_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.clip, clipOff, J.b, J.o, K, J.clip_b, J.clip_o);
+  { clip_compact_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.clip, clipOff, J.b, J.o, K, J.clip_b, J.clip_o); note_launch(); }
+  mk->mark("join:clipset", s);
   return ST_OK;
 }
 

@@ -108,7 +108,7 @@ void scan_impl(const T* in, int64_t* out, int64_t n, int64_t* total, void* tmp, 
   int64_t tiles = (n + kScanTile - 1) / kScanTile;
   ScanState* st = reinterpret_cast<ScanState*>(tmp);
   cudaMemsetAsync(st, 0, sizeof(ScanState) + tiles * sizeof(unsigned long long), s);
-  scan_kernel<T><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, n, total, st, err);
+  { scan_kernel<T><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, n, total, st, err); note_launch(); }
 }
 
 // ------------------------------------------------------------------ radix sort
@@ -223,9 +223,9 @@ void radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32
   int passes = (key_bits + 7) / 8;
   for (int p = 0; p < passes; ++p) {
     int shift = 8 * p;
-    radix_hist_kernel<<<(unsigned)nb, kRadixThreads, 0, s>>>(ka, n, shift, nb, hist);
+    { radix_hist_kernel<<<(unsigned)nb, kRadixThreads, 0, s>>>(ka, n, shift, nb, hist); note_launch(); }
     exclusive_scan_i64(hist, offs, h, nullptr, stmp, err, s);
-    radix_scatter_kernel<<<(unsigned)nb, kRadixThreads, 0, s>>>(ka, va, kb, vb, n, shift, nb, offs);
+    { radix_scatter_kernel<<<(unsigned)nb, kRadixThreads, 0, s>>>(ka, va, kb, vb, n, shift, nb, offs); note_launch(); }
     uint64_t* tk = ka; ka = kb; kb = tk;
     uint32_t* tv = va; va = vb; vb = tv;
   }

@@ -36,6 +36,11 @@ class GcmfghError(RuntimeError):
     pass
 
 
+def launch_count() -> int:
+    """Kernels launched by libgcmfgh.so in this process so far."""
+    return int(lib().gcmfgh_launch_count())
+
+
 class Layer(ctypes.Structure):
     _fields_ = [("coords", ctypes.c_void_p), ("vnum", ctypes.c_void_p), ("vps", ctypes.c_void_p),
                 ("n_polys", ctypes.c_int64), ("n_vertices", ctypes.c_int64)]
@@ -51,7 +56,8 @@ class JoinInfo(ctypes.Structure):
 
 class ClipInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in
-                ("n_pairs", "n_components", "n_vertices", "n_invalid", "n_disjoint", "n_error")]
+                ("n_pairs", "n_components", "n_vertices", "n_invalid", "n_disjoint", "n_error",
+                 "n_records", "n_ring_vertices")]
 
     def as_dict(self):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
@@ -84,6 +90,14 @@ def lib():
         L.gh_clip_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
         L.gh_clip_pair.argtypes = [vp, vp, i32, vp, i32, P(ClipInfo)]
         L.gcmfgh_join_clip_host.argtypes = [vp, P(Layer), P(Layer), P(JoinInfo), P(ClipInfo)]
+        L.gcmfgh_exclusive_scan_i32.argtypes = [vp, vp, vp, i64, P(i64)]
+        L.gcmfgh_radix_sort_u64.argtypes = [vp, vp, vp, i64, ctypes.c_int]
+        L.gcmfgh_launch_count.argtypes = []
+        L.gcmfgh_launch_count.restype = ctypes.c_ulonglong
+        L.gcmfgh_set_timing.argtypes = [vp, ctypes.c_int]
+        L.gcmfgh_get_timing.argtypes = [vp, ctypes.c_int, P(ctypes.c_float), P(ctypes.c_char_p),
+                                        ctypes.c_int]
+        L.gcmfgh_get_timing.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -167,6 +181,16 @@ class Engine:
     def last_device_error(self):
         return lib().gcmfgh_last_device_error(self.h)
 
+    def set_timing(self, on=True):
+        _check(lib().gcmfgh_set_timing(self.h, 1 if on else 0))
+
+    def timing(self, which):
+        """[(stage, ms)] of the last join (which=0) or clip (which=1)."""
+        ms = (ctypes.c_float * 32)()
+        names = (ctypes.c_char_p * 32)()
+        n = lib().gcmfgh_get_timing(self.h, which, ms, names, 32)
+        return [(names[i].decode(), float(ms[i])) for i in range(max(n, 0))]
+
     # ---- join
     def join(self, dbase: DeviceLayer, dovl: DeviceLayer):
         info = JoinInfo()
@@ -222,6 +246,21 @@ class Engine:
     def clip_result(self):
         return ClipResult(self.clip_field("status"), self.clip_field("ncomp"), self.clip_field("count1"),
                           self.clip_field("comp_size"), self.clip_field("xy"), self.clip_field("swapped"))
+
+    # ---- primitives (device tensors)
+    def exclusive_scan_i32(self, d_in):
+        import torch
+        out = torch.empty(d_in.numel(), dtype=torch.int64, device=d_in.device)
+        tot = ctypes.c_int64()
+        _check(lib().gcmfgh_exclusive_scan_i32(self.h, ctypes.c_void_p(d_in.data_ptr()),
+                                               ctypes.c_void_p(out.data_ptr()), d_in.numel(),
+                                               ctypes.byref(tot)))
+        return out, tot.value
+
+    def radix_sort_u64(self, d_keys, d_vals, key_bits=64):
+        """Sorts int64-typed tensors holding u64 keys in place (unsigned order)."""
+        _check(lib().gcmfgh_radix_sort_u64(self.h, ctypes.c_void_p(d_keys.data_ptr()),
+                                           ctypes.c_void_p(d_vals.data_ptr()), d_keys.numel(), key_bits))
 
     # ---- end to end from host buffers
     def join_clip_host(self, base, ovl):

@@ -68,6 +68,8 @@ typedef struct {
   int64_t n_invalid;        /* P/Q intersection counts disagree (gppolyclip_mDIV512.cu:1461) */
   int64_t n_disjoint;       /* MBRs do not overlap (ghcuda.cpp:109-116 exits instead) */
   int64_t n_error;          /* tracing did not close within its step budget */
+  int64_t n_records;        /* intersecting edge pairs found (all pairs) */
+  int64_t n_ring_vertices;  /* vertices of the merged P and Q rings (valid pairs) */
 } gcmfgh_clip_info;
 
 /* Join result fields for gcmf_join_get / gcmf_join_ptr. */
@@ -114,6 +116,15 @@ gcmfgh_status gcmfgh_set_params(gcmfgh_ctx* ctx, double eps, double eps_clean, i
 const char* gcmfgh_status_string(gcmfgh_status s);
 /* device error word of the last call (0 none, 1 capacity, 2 trace budget, 4 wait limit) */
 int gcmfgh_last_device_error(gcmfgh_ctx* ctx);
+/* Stage timing, replacing the reference's StartTimer/StopTimer pairs around each stage
+ * (GPU_Manage.h:4-19, spatialJoin3.cu:197-375) and its DEBUG_TIMING kernel events
+ * (gppolyclip_mDIV512.cu:1319-1669): when on, CUDA events are recorded on the stream
+ * between stages.  gcmfgh_get_timing(which = 0 join, 1 clip) fills ms[i] / names[i]
+ * (stage ending at mark i+1) for the last call and returns the number of stages. */
+gcmfgh_status gcmfgh_set_timing(gcmfgh_ctx* ctx, int on);
+int gcmfgh_get_timing(gcmfgh_ctx* ctx, int which, float* ms, const char** names, int cap);
+/* number of kernels this library has launched in the process so far */
+unsigned long long gcmfgh_launch_count(void);
 
 /* ---- join: replaces the stage sequence of spatialJoin (spatialJoin3.cu:197-363) */
 gcmfgh_status gcmf_join(gcmfgh_ctx* ctx, const gcmfgh_layer* base, const gcmfgh_layer* overlay,
@@ -140,6 +151,16 @@ gcmfgh_status gh_clip_ptr(gcmfgh_ctx* ctx, int field, const void** dev_ptr, int6
  * (no closing vertex) of nP, nQ vertices; P is clipped against Q as given (no swap). */
 gcmfgh_status gh_clip_pair(gcmfgh_ctx* ctx, const double* P, int32_t nP, const double* Q, int32_t nQ,
                            gcmfgh_clip_info* info);
+
+/* ---- the device primitives the path is built on.  Replace PrefixSum (GPU_Utility.h:128,
+ * a multi-pass inclusive scan, GPU_PrefixSum.h:355) and RadixSort (GPU_Utility.h:242, a
+ * 16-digit decimal LSD sort, GPU_RadixSort.h:27-148).  d_* are device pointers.
+ * exclusive scan: d_out[i] = sum(d_in[0..i-1]); *total (host, may be NULL) = sum(d_in).
+ * radix sort: stable ascending by the low key_bits bits of d_keys, d_vals permuted along. */
+gcmfgh_status gcmfgh_exclusive_scan_i32(gcmfgh_ctx* ctx, const int32_t* d_in, int64_t* d_out, int64_t n,
+                                        int64_t* total);
+gcmfgh_status gcmfgh_radix_sort_u64(gcmfgh_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n,
+                                    int key_bits);
 
 /* ---- host-resident layers: H2D copies, join, clip of the clip set; results stay on the
  * device for the *_get calls.  This is the end-to-end path of the reference's main()

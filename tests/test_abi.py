@@ -1,0 +1,61 @@
+"""CPU checks of the C ABI: the library builds for sm_100a, loads, and exports every
+function include/*.h declares.  No compute call is made (there is no GPU here)."""
+import ctypes
+import glob
+import os
+import re
+import subprocess
+
+from conftest import ROOT, build_library
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{]*\)\s*;", text):
+            name = m.group(1)
+            if name not in {"if", "while", "for", "return", "sizeof"}:
+                names.add(name)
+    return names
+
+
+def test_header_declares_the_entry_points():
+    names = declared_functions()
+    for n in ("gcmf_join", "gh_clip_batch", "gh_clip_pair", "gh_clip_joined", "gcmfgh_create",
+              "gcmfgh_join_clip_host", "gcmfgh_exclusive_scan_i32", "gcmfgh_radix_sort_u64"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = build_library()
+    out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    missing = declared_functions() - exported
+    assert not missing, missing
+
+
+def test_library_loads_and_reports_status_strings():
+    L = ctypes.CDLL(build_library())
+    L.gcmfgh_status_string.restype = ctypes.c_char_p
+    assert L.gcmfgh_status_string(0) == b"ok"
+    assert L.gcmfgh_status_string(6) == b"destination too small"
+
+
+def test_library_built_for_sm100a():
+    lib = build_library()
+    out = subprocess.run(["cuobjdump", "--list-elf", lib], capture_output=True, text=True).stdout
+    assert "sm_100a" in out
+
+
+def test_python_front_end_fails_loudly_without_library(tmp_path, monkeypatch):
+    import gcmfgh
+    monkeypatch.setattr(gcmfgh, "LIB_PATH", str(tmp_path / "missing.so"))
+    monkeypatch.setattr(gcmfgh, "_lib", None)
+    try:
+        gcmfgh.lib()
+    except gcmfgh.GcmfghError:
+        pass
+    else:
+        raise AssertionError("expected GcmfghError")

@@ -1,0 +1,116 @@
+"""GPU parity of the GCMF join (MBR filter, common MBR, containment, common-MBR edge
+filter, segment refine, clip set) and of the end-to-end join+clip against the oracle.
+Candidate sets, flags and counts are integer results and must be identical."""
+import numpy as np
+import pytest
+
+import pyoracle
+from gcmfgh import synth
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["b", "o", "cmbr", "pip_type", "pip_flag", "join_flag", "bE", "oE", "seg_flag", "clip"]
+
+
+def _join_equal(engine, base, ovl):
+    import gcmfgh
+    db, do = gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl)
+    info = engine.join(db, do)
+    o = pyoracle.join(base, ovl)
+    for f in FIELDS:
+        assert np.array_equal(engine.join_field(f).reshape(-1), np.asarray(getattr(o, f)).reshape(-1)), f
+    assert np.array_equal(engine.join_field("valid_b"), o.valid_b)
+    assert np.array_equal(engine.join_field("mbr_b"), o.mbr_b)
+    assert info["n_pairs"] == len(o.b)
+    assert info["n_clip"] == int(o.clip.sum())
+    assert info["n_within"] == int(o.pip_flag.sum()) and info["n_seg"] == int(o.seg_flag.sum())
+    return db, do, info, o
+
+
+def _clip_equal(engine, db, do, base, ovl):
+    info = engine.clip_joined(db, do)
+    r = engine.clip_result()
+    cb, co = engine.join_field("clip_b"), engine.join_field("clip_o")
+    o = pyoracle.clip_batch(base, ovl, cb, co)
+    assert engine.last_device_error() == 0
+    assert np.array_equal(r.status, o.status)
+    assert np.array_equal(r.count1, o.count1)
+    assert np.array_equal(r.ncomp, o.ncomp)
+    assert np.array_equal(r.comp_size, o.comp_size)
+    assert np.array_equal(r.xy, o.xy)
+    return info, r
+
+
+def test_small_join_and_clip(engine):
+    base, ovl = synth.small_join()
+    db, do, info, _ = _join_equal(engine, base, ovl)
+    assert info["n_pairs"] == 1813
+    _clip_equal(engine, db, do, base, ovl)
+
+
+def test_batched_join_and_clip_full_size(engine):
+    """The full 200,000 x 200,000 polygon workload: every candidate, flag and clipped
+    vertex against the oracle."""
+    base, ovl = synth.batched_join()
+    db, do, info, _ = _join_equal(engine, base, ovl)
+    assert info["n_pairs"] > 500000 and info["n_clip"] > 400000
+    cinfo, r = _clip_equal(engine, db, do, base, ovl)
+    assert cinfo["n_error"] == 0
+
+
+def _box(x1, y1, x2, y2):
+    return np.array([[x1, y1], [x2, y1], [x2, y2], [x1, y2]], dtype=np.float64)
+
+
+def test_touching_mbrs_tie_rule(engine):
+    base = synth.Layer.from_rings([_box(0, 0, 1, 1), np.array([[0, 0], [0, 1], [0, 2]], float)])
+    ovl = synth.Layer.from_rings([_box(1, 0, 2, 1), _box(-1, 0, 0, 1), _box(0, 1, 1, 2),
+                                  _box(0.5, 0.5, 3, 3), _box(1, 1, 2, 2), _box(5, 5, 6, 6)])
+    _, _, info, o = _join_equal(engine, base, ovl)
+    assert list(zip(o.b, o.o)) == [(0, 1), (0, 2), (0, 3)]
+
+
+def test_containment_and_duplicates(engine):
+    rings = [_box(0, 0, 10, 10), _box(20, 20, 30, 30), _box(2, 2, 3, 3), _box(2, 2, 3, 3)]
+    base = synth.Layer.from_rings(rings)
+    ovl = synth.Layer.from_rings(rings[::-1] + [_box(25, 15, 35, 25)])
+    db, do, info, o = _join_equal(engine, base, ovl)
+    assert info["n_within"] > 0
+    _clip_equal(engine, db, do, base, ovl)
+
+
+def test_single_and_empty_layers(engine):
+    import gcmfgh
+    one = synth.Layer.from_rings([_box(0, 0, 1, 1)])
+    _join_equal(engine, one, one)
+    empty = synth.Layer(np.zeros((0, 2)), np.zeros(0, np.int32))
+    db, do = gcmfgh.DeviceLayer(one), gcmfgh.DeviceLayer(empty)
+    info = engine.join(db, do)
+    assert info["n_pairs"] == 0 and info["n_clip"] == 0
+
+
+@pytest.mark.parametrize("seed", [11, 12])
+def test_dense_random_layers(engine, seed):
+    """Many overlaps per polygon, varied sizes."""
+    rng = np.random.default_rng(seed)
+    layers = []
+    for _ in range(2):
+        n = 3000
+        counts = rng.integers(3, 200, size=n)
+        centres = rng.uniform(0, 300, size=(n, 2))
+        radius = rng.lognormal(np.log(8.0), 0.6, size=n)
+        layers.append(synth.star_layer(rng, counts, centres, radius))
+    db, do, info, _ = _join_equal(engine, *layers)
+    _clip_equal(engine, db, do, *layers)
+
+
+def test_host_entry_point_equals_device_path(engine):
+    base, ovl = synth.small_join(seed=3, n=1500)
+    import gcmfgh
+    db, do = gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl)
+    ji = engine.join(db, do)
+    ci = engine.clip_joined(db, do)
+    xy = engine.clip_field("xy")
+    ji2, ci2 = engine.join_clip_host(base, ovl)
+    assert ji == ji2 and ci == ci2
+    assert np.array_equal(engine.clip_field("xy"), xy)
