@@ -236,3 +236,80 @@ void radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32
 }
 
 }  // namespace gcmfgh
+
+// ============================================================================
+// Allocation-free scan.  Some callers cannot let a library call cudaMalloc: a host
+// engine that accounts for every byte of device memory through its own pool, or a
+// latency-sensitive loop that must not hit cudaMalloc's implicit device-wide
+// synchronisation.  This variant runs the same look-back scan kernel as
+// exclusive_scan_i32, but its look-back scratch (the tile ticket, one status word per
+// 2,048-element tile and the error word) lives in the file-scope device array below,
+// which every GPU that loads the library holds until the process exits (about 66 KB).
+#include <cstdio>
+#include <mutex>
+#include "../../include/gcmfgh.h"
+
+namespace {
+
+constexpr int64_t kNoAllocMaxTiles = GCMFGH_NOALLOC_SCAN_MAX_ELEMENTS / gcmfgh::kScanTile;
+constexpr int64_t kNoAllocHeaderWords = sizeof(gcmfgh::ScanState) / sizeof(unsigned long long);
+static_assert(GCMFGH_NOALLOC_SCAN_MAX_ELEMENTS % gcmfgh::kScanTile == 0, "whole tiles");
+
+// [header (ticket) | one status word per tile | error word]
+static __device__ __align__(256) unsigned long long
+    g_noalloc_scan_scratch[kNoAllocHeaderWords + kNoAllocMaxTiles + 8];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_ptr[kMaxDevices] = {};
+
+// The device address of the scratch array on the current device.  Host code may not use
+// the array's name as an address (it is a host-side stand-in), so the address is looked
+// up once per device with that device current and cached.
+unsigned long long* noalloc_scratch(int dev) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scan_scratch) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    g_noalloc_ptr[dev] = static_cast<unsigned long long*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" gcmfgh_status gcmfgh_exclusive_scan_i32_noalloc(const int32_t* d_in, int64_t* d_out, int64_t n,
+                                                           int64_t* d_total, void* stream) {
+  if (n < 0 || (n > 0 && (!d_in || !d_out))) return GCMFGH_INVALID_ARGUMENT;
+  if (n > GCMFGH_NOALLOC_SCAN_MAX_ELEMENTS) {
+    fprintf(stderr, "gcmfgh_exclusive_scan_i32_noalloc: n = %lld exceeds the maximum of %lld elements\n",
+            (long long)n, (long long)GCMFGH_NOALLOC_SCAN_MAX_ELEMENTS);
+    return GCMFGH_INVALID_ARGUMENT;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return GCMFGH_CUDA_ERROR;
+  unsigned long long* scratch = noalloc_scratch(dev);
+  if (!scratch) return GCMFGH_CUDA_ERROR;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int* err = reinterpret_cast<int*>(scratch + kNoAllocHeaderWords + kNoAllocMaxTiles);
+  const int64_t tiles = (n + gcmfgh::kScanTile - 1) / gcmfgh::kScanTile;
+  // the array keeps the previous call's contents: zero the ticket, the status words this
+  // call uses and the error word
+  if (cudaMemsetAsync(scratch, 0, (kNoAllocHeaderWords + tiles) * sizeof(unsigned long long), s) != cudaSuccess ||
+      cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess)
+    return GCMFGH_CUDA_ERROR;
+  if (n == 0) {
+    if (d_total && cudaMemsetAsync(d_total, 0, sizeof(int64_t), s) != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  } else {
+    gcmfgh::scan_kernel<int32_t><<<(unsigned)tiles, gcmfgh::kScanThreads, 0, s>>>(
+        d_in, d_out, n, d_total, reinterpret_cast<gcmfgh::ScanState*>(scratch), err);
+    gcmfgh::note_launch();
+  }
+  int h_err = 0;
+  if (cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  return h_err ? GCMFGH_DEVICE_ERROR : GCMFGH_OK;
+}

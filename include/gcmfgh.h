@@ -162,6 +162,23 @@ gcmfgh_status gcmfgh_exclusive_scan_i32(gcmfgh_ctx* ctx, const int32_t* d_in, in
 gcmfgh_status gcmfgh_radix_sort_u64(gcmfgh_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n,
                                     int key_bits);
 
+/* ---- allocation-free exclusive scan.  No counterpart in the reference.
+ * For callers that cannot let a library allocate device memory: engines that account for
+ * every device byte through their own pool, or latency-sensitive loops that must not hit
+ * cudaMalloc's implicit synchronisation.  Same result as gcmfgh_exclusive_scan_i32, but
+ * needs no context and calls no cudaMalloc/cudaFree: its scratch is a fixed device array
+ * inside the library (about 66 KB, held on every GPU that loads the library until the
+ * process exits), so n is limited to GCMFGH_NOALLOC_SCAN_MAX_ELEMENTS; larger n returns
+ * GCMFGH_INVALID_ARGUMENT.  d_in, d_out, d_total (may be NULL) are device pointers on the
+ * current device; stream is a cudaStream_t (NULL = legacy default stream).  The call
+ * returns when the result is ready.  The first call on a device looks the scratch array's
+ * address up (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (other threads, other
+ * streams of the same device) race and must be serialised by the caller. */
+#define GCMFGH_NOALLOC_SCAN_MAX_ELEMENTS (1LL << 24)
+gcmfgh_status gcmfgh_exclusive_scan_i32_noalloc(const int32_t* d_in, int64_t* d_out, int64_t n,
+                                                int64_t* d_total, void* stream);
+
 /* ---- host-resident layers: H2D copies, join, clip of the clip set; results stay on the
  * device for the *_get calls.  This is the end-to-end path of the reference's main()
  * (main.cpp:15-29). */
