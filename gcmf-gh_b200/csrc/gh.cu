@@ -254,7 +254,6 @@ struct RingSet {
   int8_t* lb;       // IntersectionLabel
   int8_t* ee;       // EntryExitLabel
   uint8_t* fl;      // bit0 split candidate, bit1 crossing candidate
-  int64_t* rec;     // record of an inserted vertex (-1 for source / added vertices)
 };
 
 // per pair: ring size, region offset (ring + room for added vertices)
@@ -274,33 +273,89 @@ __global__ void pair_ring_kernel(const int64_t* __restrict__ eoff, const int64_t
 // ---------------------------------------------------------------- G5 ring fill
 // Thread per edge: the edge's source vertex, then its inserted vertices sorted by
 // (parameter ascending, other edge descending).  side 0 fills P rings, side 1 Q rings.
+// An edge of the smaller polygon can cross thousands of edges of a large one; edges with
+// more than kLightEdge insertions are left to heavy_fill_kernel, which sorts them with a
+// block-wide bitonic network.
+constexpr int kLightEdge = 32;
+
+struct EdgeFill {
+  int64_t k, base;
+  int s0, mm, np_;
+  const double2* pvx;
+  const double2* qvx;
+};
+
+template <int kSide>
+__device__ __forceinline__ void write_inserted(const EdgeFill& f, const Records& R, int64_t r, int i,
+                                               RingSet& S, int64_t* slotOfRec) {
+  int t = R.t[r];
+  double X, Y;
+  if (t == 1) {
+    // I = (1-alpha) P1 + alpha P2 (gppolyclip_mDIV512.cu:1029, polyclip.h:220)
+    int pe = R.p[r];
+    double a = R.a[r];
+    double2 P1 = __ldg(f.pvx + pe), P2 = __ldg(f.pvx + (pe + 1 < f.np_ ? pe + 1 : 0));
+    X = (1.0 - a) * P1.x + a * P2.x;
+    Y = (1.0 - a) * P1.y + a * P2.y;
+  } else if (kSide == 0) {          // types 3, 5, 7: a copy of Q1 on P
+    double2 Q1 = __ldg(f.qvx + R.q[r]);
+    X = Q1.x; Y = Q1.y;
+  } else {                          // types 2, 5, 6: a copy of P1 on Q
+    double2 P1 = __ldg(f.pvx + R.p[r]);
+    X = P1.x; Y = P1.y;
+  }
+  int sl = f.s0 + 1 + i;
+  int64_t gs = f.base + sl;
+  S.x[gs] = X; S.y[gs] = Y;
+  S.nx[gs] = (sl + 1) % f.mm; S.pv[gs] = (sl + f.mm - 1) % f.mm; S.nb[gs] = -1;
+  S.it[gs] = 0; S.lb[gs] = L_NONE; S.ee[gs] = E_NEITHER; S.fl[gs] = 0;
+  slotOfRec[r] = sl;
+}
+
+template <int kSide>
+__device__ __forceinline__ bool edge_fill_info(const LayerDev& Lb, const LayerDev& Lo, const PairDev& D,
+                                               const int64_t* eoff, int64_t K, const int64_t* vpos,
+                                               const int64_t* regOff, const int32_t* m, int64_t e, EdgeFill& f) {
+  int64_t k = upper_index(eoff, K, e);
+  if (D.status[k] != 0) return false;
+  const int n = kSide == 0 ? D.nP[k] : D.nQ[k];
+  if ((int)(e - eoff[k]) >= n) return false;
+  const int pside = D.pSide[k];
+  f.k = k;
+  f.mm = m[k];
+  f.base = regOff[k];
+  f.s0 = (int)(vpos[e] - vpos[eoff[k]]);
+  f.pvx = layer_xy(Lb, Lo, pside) + D.pS[k];
+  f.qvx = layer_xy(Lb, Lo, 1 - pside) + D.qS[k];
+  f.np_ = D.nP[k];
+  return true;
+}
+
 template <int kSide>
 __global__ void ring_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R,
                                  const int64_t* __restrict__ eoff, int64_t nE, int64_t K,
                                  const int64_t* __restrict__ vpos, const int64_t* __restrict__ regOff,
                                  const int32_t* __restrict__ m, RingSet S, int64_t* __restrict__ slotOfRec,
                                  const int64_t* __restrict__ insCursorBase, int32_t* __restrict__ insCursor,
-                                 const int64_t* __restrict__ insList) {
+                                 const int64_t* __restrict__ insList, int64_t* __restrict__ heavy,
+                                 unsigned long long* __restrict__ nHeavy) {
   int64_t e = (int64_t)blockIdx.x * kThreads + threadIdx.x;
   if (e >= nE) return;
-  int64_t k = upper_index(eoff, K, e);
-  if (D.status[k] != 0) return;
-  const int n = kSide == 0 ? D.nP[k] : D.nQ[k];
-  const int le = (int)(e - eoff[k]);
-  if (le >= n) return;
-  const int mm = m[k];
-  const int64_t base = regOff[k];
-  const int s0 = (int)(vpos[e] - vpos[eoff[k]]);
-  const int pside = D.pSide[k];
-  const double2* v = layer_xy(Lb, Lo, kSide == 0 ? pside : 1 - pside) + (kSide == 0 ? D.pS[k] : D.qS[k]);
-  double2 A = __ldg(v + le);
-  int64_t g = base + s0;
+  EdgeFill f;
+  if (!edge_fill_info<kSide>(Lb, Lo, D, eoff, K, vpos, regOff, m, e, f)) return;
+  const int le = (int)(e - eoff[f.k]);
+  const double2 A = __ldg((kSide == 0 ? f.pvx : f.qvx) + le);
+  const int64_t g = f.base + f.s0;
   S.x[g] = A.x; S.y[g] = A.y;
-  S.nx[g] = (s0 + 1) % mm; S.pv[g] = (s0 + mm - 1) % mm; S.nb[g] = -1;
-  S.it[g] = 0; S.lb[g] = L_NONE; S.ee[g] = E_NEITHER; S.fl[g] = 0; S.rec[g] = -1;
+  S.nx[g] = (f.s0 + 1) % f.mm; S.pv[g] = (f.s0 + f.mm - 1) % f.mm; S.nb[g] = -1;
+  S.it[g] = 0; S.lb[g] = L_NONE; S.ee[g] = E_NEITHER; S.fl[g] = 0;
   // inserted records of this edge, gathered by record_scatter_kernel into insList
   const int64_t l0 = insCursorBase[e];
   const int cnt = insCursor[e];
+  if (cnt > kLightEdge) {
+    heavy[atomicAdd(nHeavy, 1ull)] = e;
+    return;
+  }
   // insertion sort of the (few) records by (parameter asc, other edge desc)
   int64_t* lst = const_cast<int64_t*>(insList) + l0;
   for (int i = 1; i < cnt; ++i) {
@@ -319,33 +374,77 @@ __global__ void ring_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R,
     }
     lst[j + 1] = r;
   }
-  const double2* pvx = layer_xy(Lb, Lo, pside) + D.pS[k];
-  const double2* qvx = layer_xy(Lb, Lo, 1 - pside) + D.qS[k];
-  const int np_ = D.nP[k];
-  for (int i = 0; i < cnt; ++i) {
-    int64_t r = lst[i];
-    int t = R.t[r];
-    double X, Y;
-    if (t == 1) {
-      // I = (1-alpha) P1 + alpha P2 (gppolyclip_mDIV512.cu:1029, polyclip.h:220)
-      int pe = R.p[r];
-      double a = R.a[r];
-      double2 P1 = __ldg(pvx + pe), P2 = __ldg(pvx + (pe + 1 < np_ ? pe + 1 : 0));
-      X = (1.0 - a) * P1.x + a * P2.x;
-      Y = (1.0 - a) * P1.y + a * P2.y;
-    } else if (kSide == 0) {          // types 3, 5, 7: a copy of Q1 on P
-      double2 Q1 = __ldg(qvx + R.q[r]);
-      X = Q1.x; Y = Q1.y;
-    } else {                          // types 2, 5, 6: a copy of P1 on Q
-      double2 P1 = __ldg(pvx + R.p[r]);
-      X = P1.x; Y = P1.y;
+  for (int i = 0; i < cnt; ++i) write_inserted<kSide>(f, R, lst[i], i, S, slotOfRec);
+}
+
+// Block per heavy edge: bitonic sort of (parameter bits, ~other edge, list position) --
+// ascending parameter, descending other edge -- in shared memory up to kHeavySmem
+// elements, in a global scratch segment beyond; then the vertices are written in order.
+constexpr int kHeavyThreads = 512;
+constexpr int kHeavySmem = 4096;
+
+__device__ void bitonic_sort(uint64_t* key, uint32_t* tie, uint32_t* idx, int npad) {
+  for (int size = 2; size <= npad; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < (npad >> 1); i += blockDim.x) {
+        int lo = 2 * i - (i & (stride - 1));
+        int hi = lo + stride;
+        bool up = (lo & size) == 0;
+        uint64_t ka = key[lo], kb = key[hi];
+        uint32_t ta = tie[lo], tb = tie[hi];
+        bool gt = (ka > kb) || (ka == kb && ta > tb);
+        if (gt == up) {
+          key[lo] = kb; key[hi] = ka;
+          tie[lo] = tb; tie[hi] = ta;
+          uint32_t x = idx[lo]; idx[lo] = idx[hi]; idx[hi] = x;
+        }
+      }
+      __syncthreads();
     }
-    int s = s0 + 1 + i;
-    int64_t gs = base + s;
-    S.x[gs] = X; S.y[gs] = Y;
-    S.nx[gs] = (s + 1) % mm; S.pv[gs] = (s + mm - 1) % mm; S.nb[gs] = -1;
-    S.it[gs] = 0; S.lb[gs] = L_NONE; S.ee[gs] = E_NEITHER; S.fl[gs] = 0; S.rec[gs] = r;
-    slotOfRec[r] = s;
+  }
+}
+
+template <int kSide>
+__global__ void __launch_bounds__(kHeavyThreads)
+heavy_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R, const int64_t* __restrict__ eoff, int64_t K,
+                  const int64_t* __restrict__ vpos, const int64_t* __restrict__ regOff,
+                  const int32_t* __restrict__ m, RingSet S, int64_t* __restrict__ slotOfRec,
+                  const int64_t* __restrict__ insCursorBase, const int32_t* __restrict__ insCursor,
+                  const int64_t* __restrict__ insList, const int64_t* __restrict__ heavy,
+                  const unsigned long long* __restrict__ nHeavy, uint64_t* gkey, uint32_t* gtie, uint32_t* gidx) {
+  extern __shared__ unsigned char smem[];
+  uint64_t* skey = reinterpret_cast<uint64_t*>(smem);
+  uint32_t* stie = reinterpret_cast<uint32_t*>(skey + kHeavySmem);
+  uint32_t* sidx = stie + kHeavySmem;
+  __shared__ EdgeFill f;
+  const unsigned long long nh = *nHeavy;
+  for (unsigned long long h = blockIdx.x; h < nh; h += gridDim.x) {
+    const int64_t e = heavy[h];
+    if (threadIdx.x == 0) edge_fill_info<kSide>(Lb, Lo, D, eoff, K, vpos, regOff, m, e, f);
+    __syncthreads();
+    const int64_t l0 = insCursorBase[e];
+    const int cnt = insCursor[e];
+    int npad = 1;
+    while (npad < cnt) npad <<= 1;
+    uint64_t* key = skey;
+    uint32_t* tie = stie;
+    uint32_t* idx = sidx;
+    if (npad > kHeavySmem) { key = gkey + 2 * l0; tie = gtie + 2 * l0; idx = gidx + 2 * l0; }
+    for (int i = threadIdx.x; i < npad; i += blockDim.x) {
+      if (i < cnt) {
+        int64_t r = insList[l0 + i];
+        key[i] = ordered_key(kSide == 0 ? R.a[r] : R.b[r]);
+        tie[i] = 0xffffffffu - (uint32_t)(kSide == 0 ? R.q[r] : R.p[r]);
+        idx[i] = (uint32_t)i;
+      } else {
+        key[i] = ~0ull; tie[i] = 0xffffffffu; idx[i] = 0xffffffffu;
+      }
+    }
+    __syncthreads();
+    bitonic_sort(key, tie, idx, npad);
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x)
+      write_inserted<kSide>(f, R, insList[l0 + idx[i]], i, S, slotOfRec);
+    __syncthreads();
   }
 }
 
@@ -542,27 +641,36 @@ __device__ void push_ring(OutRegion& O, const Ring& A) {
   O.end();
 }
 
-__global__ void __launch_bounds__(128)
-label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const int32_t* __restrict__ mQ,
-                   const int64_t* __restrict__ regP, const int64_t* __restrict__ regQ,
-                   const int64_t* __restrict__ regSizeP, const int64_t* __restrict__ regSizeQ,
-                   RingSet SP, RingSet SQ, double* __restrict__ outXY, const int64_t* __restrict__ outVOff,
-                   const int64_t* __restrict__ outVCap, int32_t* __restrict__ outCsz,
-                   const int64_t* __restrict__ outCOff, const int32_t* __restrict__ outCCap,
-                   int32_t* __restrict__ outNC, int64_t* __restrict__ outNV, ClipParams prm, int* err) {
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= K) return;
-  outNC[k] = 0; outNV[k] = 0;
-  if (D.status[k] != 0) return;
-  const bool uni = prm.union_mode != 0;
-  Ring R[2] = {ring_of(SP, regP[k], mP[k], (int)regSizeP[k]), ring_of(SQ, regQ[k], mQ[k], (int)regSizeQ[k])};
-  Ring& P = R[0];
-  Ring& Q = R[1];
+// Per-pair state of the labelling and tracing phases.
+struct PairCtx {
+  Ring R[2];
   OutRegion O;
-  O.xy = outXY + 2 * outVOff[k]; O.csz = outCsz + outCOff[k]; O.vcap = outVCap[k]; O.ccap = outCCap[k];
-  O.nv = 0; O.nc = 0; O.overflow = false;
+  bool uni;
+  double eps_clean;
+  int* err;
+  int32_t* status;
+  bool noInter[2];
+  bool ident[2];
+};
 
-  // ---- step 1: initial labels (computed on P, copied to the neighbour on Q)
+__device__ __forceinline__ int8_t toggled(int8_t st) {
+  return (st == E_ENTRY) ? E_EXIT : (st == E_EXIT ? E_ENTRY : st);
+}
+
+__device__ __forceinline__ void fail(PairCtx& c, int code) {
+  raise_error(c.err, code);
+  *c.status = 3;
+}
+
+// ================================================================ sequential phases
+// One thread walks the pair exactly as polyclip.h does.  Used whole when the links are not
+// one-to-one, and for the parts the warp version leaves to one lane (chain anomalies,
+// split vertices, tracing through added vertices).
+
+// step 1: initial labels (computed on P, copied to the neighbour on Q)
+__device__ void seq_step1(PairCtx& c) {
+  Ring& P = c.R[0];
+  Ring& Q = c.R[1];
   for (int s = 0; s < P.m; ++s) {
     if (!P.it[s]) continue;
     int nb = P.nb[s];
@@ -573,7 +681,12 @@ label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const i
     int8_t L = initial_label(a, b);
     if (L != L_NONE) { P.lb[s] = L; Q.lb[nb] = L; }
   }
-  // ---- step 2: intersection chains (polyclip.h:405-451)
+}
+
+// step 2: intersection chains (polyclip.h:405-451)
+__device__ void seq_step2(PairCtx& c) {
+  Ring& P = c.R[0];
+  Ring& Q = c.R[1];
   for (int s = 0; s < P.m; ++s) {
     if (!P.it[s] || (P.lb[s] != L_LEFT_ON && P.lb[s] != L_RIGHT_ON)) continue;
     int x = P.lb[s] == L_LEFT_ON ? R_LEFT : R_RIGHT;
@@ -589,48 +702,52 @@ label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const i
     if (P.nb[X] >= 0) Q.lb[P.nb[X]] = ct;
     if (P.nb[I] >= 0) Q.lb[P.nb[I]] = ct;
   }
-  // ---- step 3.5: components without crossings (polyclip.h:474-541)
-  bool noInter[2], ident[2] = {false, false};
+}
+
+// step 3.5: components without crossings (polyclip.h:474-541)
+__device__ void seq_step35(PairCtx& c) {
   for (int sd = 0; sd < 2; ++sd) {
-    Ring& A = R[sd];
+    Ring& A = c.R[sd];
     bool none = true, allOn = true;
     for (int v = 0; v < A.m; ++v) {
       int8_t l = A.lb[v];
       if (l != L_ON_ON) allOn = false;
       if (A.it[v]) {
         if (l == L_CROSSING || l == L_DELAYED_CROSSING) none = false;
-        if (uni && (l == L_BOUNCING || l == L_DELAYED_BOUNCING)) none = false;
+        if (c.uni && (l == L_BOUNCING || l == L_DELAYED_BOUNCING)) none = false;
       }
     }
-    noInter[sd] = none;
-    if (none) ident[sd] = allOn;
+    c.noInter[sd] = none;
+    c.ident[sd] = none && allOn;
   }
   for (int sd = 0; sd < 2; ++sd) {
-    if (!noInter[sd] || ident[sd]) continue;
-    Ring& A = R[sd];
-    Ring& B = R[1 - sd];
+    if (!c.noInter[sd] || c.ident[sd]) continue;
+    Ring& A = c.R[sd];
+    Ring& B = c.R[1 - sd];
     bool mid;
     int v = first_non_intersection(A, B, mid);
     if (v < 0) continue;
     double px = A.x[v], py = A.y[v];
     if (mid) { int n = A.nx[v]; px = 0.5 * (A.x[v] + A.x[n]); py = 0.5 * (A.y[v] + A.y[n]); }
     bool inside = point_in_ring(B, px, py, -1);
-    if (inside ^ uni) push_ring(O, A);
+    if (inside ^ c.uni) push_ring(c.O, A);
   }
-  if (ident[0] && ident[1]) push_ring(O, P);
+  if (c.ident[0] && c.ident[1]) push_ring(c.O, c.R[0]);
+}
 
-  // ---- step 4: entry/exit flags (polyclip.h:549-655)
+// step 4: entry/exit flags (polyclip.h:549-655)
+__device__ bool seq_step4(PairCtx& c) {
   for (int sd = 0; sd < 2; ++sd) {
-    if (noInter[sd]) continue;
-    Ring& A = R[sd];
-    Ring& B = R[1 - sd];
+    if (c.noInter[sd]) continue;
+    Ring& A = c.R[sd];
+    Ring& B = c.R[1 - sd];
     bool mid;
     int V = first_non_intersection(A, B, mid);
     if (V < 0) continue;
     if (mid) {
       int n = A.nx[V];
       int T = add_vertex(A, 0.5 * (A.x[V] + A.x[n]), 0.5 * (A.y[V] + A.y[n]));
-      if (T < 0) { raise_error(err, DEV_CAPACITY); D.status[k] = 3; return; }
+      if (T < 0) { fail(c, DEV_CAPACITY); return false; }
       insert_after(A, T, V);
       V = T;
     }
@@ -641,28 +758,34 @@ label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const i
     while (I != V && --guard > 0) {
       if (A.it[I]) {
         int8_t l = A.lb[I];
-        if (l == L_CROSSING) { A.ee[I] = st; st = (st == E_ENTRY) ? E_EXIT : (st == E_EXIT ? E_ENTRY : st); }
-        if (A.lb[I] == L_BOUNCING && ((st == E_EXIT) ^ uni)) A.fl[I] |= 1;
+        if (l == L_CROSSING) { A.ee[I] = st; st = toggled(st); }
+        if (A.lb[I] == L_BOUNCING && ((st == E_EXIT) ^ c.uni)) A.fl[I] |= 1;
         if (A.lb[I] == L_DELAYED_CROSSING) {
           A.ee[I] = st;
-          if (first) { if ((st == E_EXIT) ^ uni) A.lb[I] = L_CROSSING; first = false; }
+          if (first) { if ((st == E_EXIT) ^ c.uni) A.lb[I] = L_CROSSING; first = false; }
           else {
-            if ((st == E_ENTRY) ^ uni) A.lb[I] = L_CROSSING;
+            if ((st == E_ENTRY) ^ c.uni) A.lb[I] = L_CROSSING;
             first = true;
-            st = (st == E_ENTRY) ? E_EXIT : (st == E_EXIT ? E_ENTRY : st);
+            st = toggled(st);
           }
         }
         if (A.lb[I] == L_DELAYED_BOUNCING) {
           A.ee[I] = st;
-          if (first) { if ((st == E_EXIT) ^ uni) A.fl[I] |= 2; first = false; }
-          else { if ((st == E_ENTRY) ^ uni) A.fl[I] |= 2; first = true; }
-          st = (st == E_ENTRY) ? E_EXIT : (st == E_EXIT ? E_ENTRY : st);
+          if (first) { if ((st == E_EXIT) ^ c.uni) A.fl[I] |= 2; first = false; }
+          else { if ((st == E_ENTRY) ^ c.uni) A.fl[I] |= 2; first = true; }
+          st = toggled(st);
         }
       }
       I = A.nx[I];
     }
   }
-  // ---- step 5: split vertex pairs (polyclip.h:661-714)
+  return true;
+}
+
+// step 5: split vertex pairs (polyclip.h:661-714)
+__device__ bool seq_step5(PairCtx& c) {
+  Ring& P = c.R[0];
+  Ring& Q = c.R[1];
   const int pm0 = P.used;
   for (int ip = 0; ip < pm0; ++ip) {
     if (!(P.fl[ip] & 1)) continue;
@@ -670,7 +793,7 @@ label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const i
     if (iq < 0 || !(Q.fl[iq] & 1)) continue;
     int vp = add_vertex(P, P.x[ip], P.y[ip]);
     int vq = add_vertex(Q, Q.x[iq], Q.y[iq]);
-    if (vp < 0 || vq < 0) { raise_error(err, DEV_CAPACITY); D.status[k] = 3; return; }
+    if (vp < 0 || vq < 0) { fail(c, DEV_CAPACITY); return false; }
     double sP = area2(P.x[P.pv[ip]], P.y[P.pv[ip]], P.x[ip], P.y[ip], P.x[P.nx[ip]], P.y[P.nx[ip]]);
     double sQ = area2(Q.x[Q.pv[iq]], Q.y[Q.pv[iq]], Q.x[iq], Q.y[iq], Q.x[Q.nx[iq]], Q.y[Q.nx[iq]]);
     if (sP * sQ > 0) {
@@ -681,95 +804,560 @@ label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const i
     }
     insert_after(P, vp, ip);
     insert_after(Q, vq, iq);
-    int8_t e1 = uni ? E_ENTRY : E_EXIT, e2 = uni ? E_EXIT : E_ENTRY;
+    int8_t e1 = c.uni ? E_ENTRY : E_EXIT, e2 = c.uni ? E_EXIT : E_ENTRY;
     P.ee[ip] = e1; P.ee[vp] = e2; Q.ee[iq] = e1; Q.ee[vq] = e2;
     P.lb[ip] = L_CROSSING; P.lb[vp] = L_CROSSING; Q.lb[iq] = L_CROSSING; Q.lb[vq] = L_CROSSING;
   }
-  // ---- step 6: crossing candidates (polyclip.h:723-734)
-  for (int ip = 0; ip < pm0; ++ip) {
+  return true;
+}
+
+// step 6: crossing candidates (polyclip.h:723-734)
+__device__ void seq_step6(PairCtx& c) {
+  Ring& P = c.R[0];
+  Ring& Q = c.R[1];
+  for (int ip = 0; ip < P.m; ++ip) {
     if (!(P.fl[ip] & 2)) continue;
     int iq = P.nb[ip];
     if (iq >= 0 && (Q.fl[iq] & 2)) { P.lb[ip] = L_CROSSING; Q.lb[iq] = L_CROSSING; }
   }
-  // ---- tracing (polyclip.h:743-783): starts at unvisited CROSSING vertices of P in ring
-  // order from slot 0; visited vertices are marked by clearing their intersection flag.
-  {
-    long long budget = 4ll * (P.used + Q.used) + 16;
-    int I = 0;
-    bool have = P.it[I] && P.lb[I] == L_CROSSING;
-    if (!have) {
-      int guard = P.used + 1;
-      do { I = P.nx[I]; } while (!(P.it[I] && P.lb[I] == L_CROSSING) && I != 0 && --guard > 0);
-      have = I != 0 && guard > 0;
-    }
-    while (have) {
-      O.begin();
-      int side = 0, V = I;
-      P.it[V] = 0;
-      do {
-        Ring& C = R[side];
-        int8_t st = C.ee[V];
-        st = (st == E_ENTRY) ? E_EXIT : (st == E_EXIT ? E_ENTRY : st);
-        do {
-          if (--budget < 0) { raise_error(err, DEV_TRACE); D.status[k] = 3; return; }
-          V = ((st == E_EXIT) ^ uni) ? C.nx[V] : C.pv[V];
-          C.it[V] = 0;
-          O.push(C.x[V], C.y[V]);
-        } while (!(C.ee[V] == st) && !(side == 0 && V == I));
-        if (!(side == 0 && V == I)) {
-          int nb = C.nb[V];
-          if (nb < 0) { raise_error(err, DEV_TRACE); D.status[k] = 3; return; }
-          V = nb;
-          side = 1 - side;
-          R[side].it[V] = 0;
-        }
-      } while (!(side == 0 && V == I));
-      O.end();
-      int guard = P.used + 1;
-      do { I = P.nx[I]; } while (!(P.it[I] && P.lb[I] == L_CROSSING) && I != 0 && --guard > 0);
-      have = I != 0 && guard > 0;
-    }
+}
+
+// tracing (polyclip.h:743-783): starts at unvisited CROSSING vertices of P in ring order
+// from slot 0; visited vertices are marked by clearing their intersection flag.
+__device__ bool seq_trace(PairCtx& c) {
+  Ring& P = c.R[0];
+  OutRegion& O = c.O;
+  long long budget = 4ll * (c.R[0].used + c.R[1].used) + 16;
+  int I = 0;
+  bool have = P.it[I] && P.lb[I] == L_CROSSING;
+  if (!have) {
+    int guard = P.used + 1;
+    do { I = P.nx[I]; } while (!(P.it[I] && P.lb[I] == L_CROSSING) && I != 0 && --guard > 0);
+    have = I != 0 && guard > 0;
   }
-  if (O.overflow) { raise_error(err, DEV_CAPACITY); D.status[k] = 3; return; }
-  // ---- clean-up (polyclip.h:791-807): drop the first vertex while it is collinear with
-  // its ring neighbours, then one forward pass that removes every vertex collinear with
-  // the last kept vertex and its original successor; compacted in place.
+  while (have) {
+    O.begin();
+    int side = 0, V = I;
+    P.it[V] = 0;
+    do {
+      Ring& C = c.R[side];
+      int8_t st = toggled(C.ee[V]);
+      do {
+        if (--budget < 0) { fail(c, DEV_TRACE); return false; }
+        V = ((st == E_EXIT) ^ c.uni) ? C.nx[V] : C.pv[V];
+        C.it[V] = 0;
+        O.push(C.x[V], C.y[V]);
+      } while (!(C.ee[V] == st) && !(side == 0 && V == I));
+      if (!(side == 0 && V == I)) {
+        int nb = C.nb[V];
+        if (nb < 0) { fail(c, DEV_TRACE); return false; }
+        V = nb;
+        side = 1 - side;
+        c.R[side].it[V] = 0;
+      }
+    } while (!(side == 0 && V == I));
+    O.end();
+    int guard = P.used + 1;
+    do { I = P.nx[I]; } while (!(P.it[I] && P.lb[I] == L_CROSSING) && I != 0 && --guard > 0);
+    have = I != 0 && guard > 0;
+  }
+  if (O.overflow) { fail(c, DEV_CAPACITY); return false; }
+  return true;
+}
+
+// clean-up of one component (polyclip.h:791-807): drop the first vertex while it is
+// collinear with its ring neighbours, then one forward pass that removes every vertex
+// collinear with the last kept vertex and its original successor.  Reads n vertices at
+// src, writes the kept ones at dst (dst <= src, ascending); returns how many were kept.
+__device__ int seq_cleanup_component(const double* src, double* dst, int n, double eps) {
+  if (n == 0) return 0;
+  const double lx = src[2 * (n - 1)], ly = src[2 * (n - 1) + 1];
+  int r = 0;
+  while (r < n) {
+    int nxt = (r + 1 < n) ? r + 1 : r;    // a lone vertex is its own neighbour
+    double a = area2(lx, ly, src[2 * r], src[2 * r + 1], src[2 * nxt], src[2 * nxt + 1]);
+    if (r == n - 1) a = 0.0;              // ring of the last vertex alone: A(v,v,v)
+    if (fabs(a) < eps) ++r; else break;
+  }
+  if (r >= n) return 0;
+  double kx = src[2 * r], ky = src[2 * r + 1];
+  const double rx = kx, ry = ky;
+  int kept = 1;
+  dst[0] = kx; dst[1] = ky;
+  for (int j = r + 1; j < n; ++j) {
+    double vx = src[2 * j], vy = src[2 * j + 1];
+    double nx = (j + 1 < n) ? src[2 * (j + 1)] : rx, ny = (j + 1 < n) ? src[2 * (j + 1) + 1] : ry;
+    if (fabs(area2(kx, ky, vx, vy, nx, ny)) < eps) continue;
+    dst[2 * kept] = vx; dst[2 * kept + 1] = vy;
+    ++kept;
+    kx = vx; ky = vy;
+  }
+  return kept;
+}
+
+__device__ void seq_cleanup(PairCtx& c, int32_t* outNC, int64_t* outNV) {
+  OutRegion& O = c.O;
   int64_t vin = 0, vout = 0;
   int nc = 0;
-  for (int c = 0; c < O.nc; ++c) {
-    const int n = O.csz[c];
-    double* src = O.xy + 2 * vin;
+  for (int k = 0; k < O.nc; ++k) {
+    const int n = O.csz[k];
+    int kept = seq_cleanup_component(O.xy + 2 * vin, O.xy + 2 * vout, n, c.eps_clean);
     vin += n;
-    if (n == 0) continue;
-    const double lx = src[2 * (n - 1)], ly = src[2 * (n - 1) + 1];
-    int r = 0;
-    while (r < n) {
-      int nxt = (r + 1 < n) ? r + 1 : r;    // a lone vertex is its own neighbour
-      double a = area2(lx, ly, src[2 * r], src[2 * r + 1], src[2 * nxt], src[2 * nxt + 1]);
-      if (r == n - 1) a = 0.0;              // ring of the last vertex alone: A(v,v,v)
-      if (fabs(a) < prm.eps_clean) ++r; else break;
-    }
-    if (r >= n) continue;                  // everything removed
-    // forward pass over v_r .. v_{n-1}; v_r (the root) is kept
-    double* dst = O.xy + 2 * vout;
-    double kx = src[2 * r], ky = src[2 * r + 1];   // last kept
-    const double rx = kx, ry = ky;
-    int kept = 1;
-    double* w = dst;
-    w[0] = kx; w[1] = ky;
-    for (int j = r + 1; j < n; ++j) {
-      double vx = src[2 * j], vy = src[2 * j + 1];
-      double nx = (j + 1 < n) ? src[2 * (j + 1)] : rx, ny = (j + 1 < n) ? src[2 * (j + 1) + 1] : ry;
-      if (fabs(area2(kx, ky, vx, vy, nx, ny)) < prm.eps_clean) continue;
-      w[2 * kept] = vx; w[2 * kept + 1] = vy;
-      ++kept;
-      kx = vx; ky = vy;
-    }
+    if (kept == 0) continue;
     O.csz[nc++] = kept;
     vout += kept;
   }
-  outNC[k] = nc;
-  outNV[k] = vout;
+  *outNC = nc;
+  *outNV = vout;
+}
+
+// the whole pair from `step` on (1: everything, 2: after the initial labels)
+__device__ void seq_pair_from(PairCtx& c, int step, int32_t* outNC, int64_t* outNV) {
+  if (step <= 1) seq_step1(c);
+  seq_step2(c);
+  seq_step35(c);
+  if (!seq_step4(c) || !seq_step5(c)) return;
+  seq_step6(c);
+  if (!seq_trace(c)) return;
+  seq_cleanup(c, outNC, outNV);
+}
+
+// ================================================================ warp phases
+constexpr unsigned kFull = 0xffffffffu;
+
+// winding increment of edge (P0,P1) for point R: polygon.h:433-444
+__device__ __forceinline__ int wind(double P0x, double P0y, double P1x, double P1y, double Rx, double Ry) {
+  if ((P0y < Ry) == (P1y < Ry)) return 0;
+  int d = 2 * (P1y > P0y) - 1;
+  if (P0x >= Rx) {
+    if (P1x > Rx) return d;
+    return ((area2(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) ? d : 0;
+  }
+  if (P1x > Rx) return ((area2(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) ? d : 0;
+  return 0;
+}
+
+// polygon.h:427-448 over ring B in slot order; `after`/`T`: a temporary vertex T inserted
+// after slot `after` (or -1)
+__device__ bool warp_point_in_ring(const Ring& B, double Rx, double Ry, int after, int T) {
+  int w = 0;
+  for (int s = lane_id(); s < B.m; s += 32) {
+    int n = (s + 1 < B.m) ? s + 1 : 0;
+    if (s == after) {
+      w += wind(B.x[s], B.y[s], B.x[T], B.y[T], Rx, Ry);
+      w += wind(B.x[T], B.y[T], B.x[n], B.y[n], Rx, Ry);
+    } else {
+      w += wind(B.x[s], B.y[s], B.x[n], B.y[n], Rx, Ry);
+    }
+  }
+  w = warp_sum(w);
+  return (w % 2) != 0;
+}
+
+// first slot s >= from (slot order, s < n) where pred(s); n if none
+template <class F>
+__device__ int warp_find_first(int from, int n, F pred) {
+  for (int b = from; b < n; b += 32) {
+    int s = b + lane_id();
+    unsigned m = __ballot_sync(kFull, s < n && pred(s));
+    if (m) return b + __ffs(m) - 1;
+  }
+  return n;
+}
+
+__device__ bool warp_links_one_to_one(const Ring& P, const Ring& Q) {
+  bool ok = true;
+  for (int s = lane_id(); s < P.m; s += 32)
+    if (P.it[s]) { int nb = P.nb[s]; if (nb < 0 || nb >= Q.m || Q.nb[nb] != s) ok = false; }
+  for (int s = lane_id(); s < Q.m; s += 32)
+    if (Q.it[s]) { int nb = Q.nb[s]; if (nb < 0 || nb >= P.m || P.nb[nb] != s) ok = false; }
+  return __all_sync(kFull, ok);
+}
+
+__device__ void warp_step1(PairCtx& c) {
+  Ring& P = c.R[0];
+  Ring& Q = c.R[1];
+  for (int s = lane_id(); s < P.m; s += 32) {
+    if (!P.it[s]) continue;
+    int nb = P.nb[s];
+    int pm = (s > 0) ? s - 1 : P.m - 1, pp = (s + 1 < P.m) ? s + 1 : 0;
+    int a = rel_position(P, Q, (nb > 0) ? nb - 1 : Q.m - 1, pm, s, pp);
+    int b = rel_position(P, Q, (nb + 1 < Q.m) ? nb + 1 : 0, pm, s, pp);
+    int8_t L = initial_label(a, b);
+    if (L != L_NONE) { P.lb[s] = L; Q.lb[nb] = L; }
+  }
+  __syncwarp();
+}
+
+// Chains run from a LEFT_ON/RIGHT_ON vertex over ON_ON vertices to an ON_LEFT/ON_RIGHT
+// vertex.  When every chain ends so, chains are disjoint and can be resolved in parallel
+// with the sequential result; otherwise returns false and nothing is changed.
+__device__ bool warp_step2(PairCtx& c) {
+  Ring& P = c.R[0];
+  Ring& Q = c.R[1];
+  const int m = P.m;
+  bool ok = true;
+  for (int s = lane_id(); s < m; s += 32) {
+    if (!P.it[s] || (P.lb[s] != L_LEFT_ON && P.lb[s] != L_RIGHT_ON)) continue;
+    int I = (s + 1 < m) ? s + 1 : 0, guard = m;
+    while (P.lb[I] == L_ON_ON && --guard > 0) I = (I + 1 < m) ? I + 1 : 0;
+    if ((P.lb[I] != L_ON_LEFT && P.lb[I] != L_ON_RIGHT) || !P.it[I]) ok = false;
+  }
+  if (!__all_sync(kFull, ok)) return false;
+  for (int s = lane_id(); s < m; s += 32) {
+    int8_t l0 = P.lb[s];
+    if (!P.it[s] || (l0 != L_LEFT_ON && l0 != L_RIGHT_ON)) continue;
+    int x = l0 == L_LEFT_ON ? R_LEFT : R_RIGHT;
+    int I = (s + 1 < m) ? s + 1 : 0;
+    Q.lb[P.nb[s]] = L_NONE;
+    while (P.lb[I] == L_ON_ON) {
+      P.lb[I] = L_NONE;
+      Q.lb[P.nb[I]] = L_NONE;
+      I = (I + 1 < m) ? I + 1 : 0;
+    }
+    int y = P.lb[I] == L_ON_LEFT ? R_LEFT : R_RIGHT;
+    int8_t ct = (x != y) ? L_DELAYED_CROSSING : L_DELAYED_BOUNCING;
+    P.lb[s] = ct; P.lb[I] = ct;
+    Q.lb[P.nb[s]] = ct; Q.lb[P.nb[I]] = ct;
+  }
+  __syncwarp();
+  return true;
+}
+
+// copies ring A (slot order, no added vertices) as one output component
+__device__ void warp_push_ring(OutRegion& O, const Ring& A) {
+  O.begin();
+  if (O.overflow) return;
+  if (O.nv + A.m > O.vcap) { O.overflow = true; return; }
+  for (int s = lane_id(); s < A.m; s += 32) { O.xy[2 * (O.nv + s)] = A.x[s]; O.xy[2 * (O.nv + s) + 1] = A.y[s]; }
+  if (lane_id() == 0) O.csz[O.nc] = A.m;
+  O.nv += A.m;
+  O.end();
+  __syncwarp();
+}
+
+// first non-intersection slot (slot order = ring order before any insertion), else the
+// first vertex whose edge to the next one is not collinear with the other polygon
+// (polygon.h:480-512); returns -1 if none
+__device__ int warp_first_non_intersection(const Ring& A, const Ring& B, bool& mid) {
+  mid = false;
+  int v = warp_find_first(0, A.m, [&](int s) { return !A.it[s]; });
+  if (v < A.m) return v;
+  // B's own links: B may already hold its temporary vertex when A is Q
+  v = warp_find_first(0, A.m, [&](int s) {
+    int nb = A.nb[s], nx = A.nx[s];
+    return nb >= 0 && A.nb[nx] != B.pv[nb] && A.nb[nx] != B.nx[nb];
+  });
+  if (v < A.m) { mid = true; return v; }
+  return -1;
+}
+
+__device__ void warp_step35(PairCtx& c) {
+  for (int sd = 0; sd < 2; ++sd) {
+    Ring& A = c.R[sd];
+    bool none = true, allOn = true;
+    for (int v = lane_id(); v < A.m; v += 32) {
+      int8_t l = A.lb[v];
+      if (l != L_ON_ON) allOn = false;
+      if (A.it[v]) {
+        if (l == L_CROSSING || l == L_DELAYED_CROSSING) none = false;
+        if (c.uni && (l == L_BOUNCING || l == L_DELAYED_BOUNCING)) none = false;
+      }
+    }
+    none = __all_sync(kFull, none);
+    allOn = __all_sync(kFull, allOn);
+    c.noInter[sd] = none;
+    c.ident[sd] = none && allOn;
+  }
+  for (int sd = 0; sd < 2; ++sd) {
+    if (!c.noInter[sd] || c.ident[sd]) continue;
+    Ring& A = c.R[sd];
+    Ring& B = c.R[1 - sd];
+    bool mid;
+    int v = warp_first_non_intersection(A, B, mid);
+    if (v < 0) continue;
+    double px = A.x[v], py = A.y[v];
+    if (mid) { int n = (v + 1 < A.m) ? v + 1 : 0; px = 0.5 * (A.x[v] + A.x[n]); py = 0.5 * (A.y[v] + A.y[n]); }
+    bool inside = warp_point_in_ring(B, px, py, -1, -1);
+    if (inside ^ c.uni) warp_push_ring(c.O, A);
+  }
+  if (c.ident[0] && c.ident[1]) warp_push_ring(c.O, c.R[0]);
+}
+
+// Entry/exit flags as a warp prefix scan over the ring from the start vertex: the status
+// at a vertex is the start status toggled once per earlier CROSSING, DELAYED_BOUNCING and
+// second-of-a-chain DELAYED_CROSSING; "first chain vertex" alternates over the DELAYED
+// vertices met (polyclip.h:582-653).
+__device__ bool warp_step4(PairCtx& c, int tempAfter[2], int tempSlot[2]) {
+  for (int sd = 0; sd < 2; ++sd) {
+    tempAfter[sd] = -1;
+    tempSlot[sd] = -1;
+  }
+  for (int sd = 0; sd < 2; ++sd) {
+    if (c.noInter[sd]) continue;
+    Ring& A = c.R[sd];
+    Ring& B = c.R[1 - sd];
+    bool mid;
+    int V0 = warp_first_non_intersection(A, B, mid);
+    if (V0 < 0) continue;
+    double qx = A.x[V0], qy = A.y[V0];
+    if (mid) {
+      int T = -1;
+      if (lane_id() == 0) {
+        T = add_vertex(A, 0.5 * (A.x[V0] + A.x[(V0 + 1 < A.m) ? V0 + 1 : 0]),
+                       0.5 * (A.y[V0] + A.y[(V0 + 1 < A.m) ? V0 + 1 : 0]));
+        if (T >= 0) insert_after(A, T, V0);
+      }
+      T = __shfl_sync(kFull, T, 0);
+      A.used = __shfl_sync(kFull, A.used, 0);
+      __syncwarp();
+      if (T < 0) { if (lane_id() == 0) fail(c, DEV_CAPACITY); return false; }
+      tempAfter[sd] = V0;
+      tempSlot[sd] = T;
+      qx = A.x[T];
+      qy = A.y[T];
+    }
+    // the Q pass tests against P's ring including P's temporary vertex
+    int8_t st0 = (sd == 1 ? warp_point_in_ring(B, qx, qy, tempAfter[0], tempSlot[0])
+                          : warp_point_in_ring(B, qx, qy, -1, -1)) ? E_EXIT : E_ENTRY;
+    int carryD = 0, carryT = 0;
+    const int m = A.m;
+    for (int b = 0; b < m; b += 32) {
+      int j = b + lane_id();
+      int s = -1;
+      int8_t L = L_NONE;
+      bool inter = false;
+      if (j < m) {
+        s = V0 + 1 + j;
+        if (s >= m) s -= m;
+        inter = A.it[s];
+        L = inter ? A.lb[s] : L_NONE;
+      }
+      int d = inter && (L == L_DELAYED_CROSSING || L == L_DELAYED_BOUNCING);
+      int dIncl = warp_incl_scan(d);
+      bool first = ((carryD + dIncl - d) & 1) == 0;
+      int t = inter && (L == L_CROSSING || L == L_DELAYED_BOUNCING || (L == L_DELAYED_CROSSING && !first));
+      int tIncl = warp_incl_scan(t);
+      int8_t st = ((carryT + tIncl - t) & 1) ? toggled(st0) : st0;
+      if (inter) {
+        if (L == L_CROSSING) A.ee[s] = st;
+        else if (L == L_BOUNCING) { if ((st == E_EXIT) ^ c.uni) A.fl[s] |= 1; }
+        else if (L == L_DELAYED_CROSSING) {
+          A.ee[s] = st;
+          if (first) { if ((st == E_EXIT) ^ c.uni) A.lb[s] = L_CROSSING; }
+          else if ((st == E_ENTRY) ^ c.uni) A.lb[s] = L_CROSSING;
+        } else if (L == L_DELAYED_BOUNCING) {
+          A.ee[s] = st;
+          if (first) { if ((st == E_EXIT) ^ c.uni) A.fl[s] |= 2; }
+          else if ((st == E_ENTRY) ^ c.uni) A.fl[s] |= 2;
+        }
+      }
+      carryD += __shfl_sync(kFull, dIncl, 31);
+      carryT += __shfl_sync(kFull, tIncl, 31);
+    }
+    __syncwarp();
+  }
+  return true;
+}
+
+__device__ bool warp_any_split(const Ring& P, const Ring& Q) {
+  bool any = false;
+  for (int s = lane_id(); s < P.m; s += 32)
+    if (P.fl[s] & 1) { int nb = P.nb[s]; if (nb >= 0 && (Q.fl[nb] & 1)) any = true; }
+  return __any_sync(kFull, any);
+}
+
+__device__ void warp_step6(PairCtx& c) {
+  Ring& P = c.R[0];
+  Ring& Q = c.R[1];
+  for (int ip = lane_id(); ip < P.m; ip += 32) {
+    if (!(P.fl[ip] & 2)) continue;
+    int iq = P.nb[ip];
+    if (iq >= 0 && (Q.fl[iq] & 2)) { P.lb[ip] = L_CROSSING; Q.lb[iq] = L_CROSSING; }
+  }
+  __syncwarp();
+}
+
+// Tracing when neither ring has added vertices (rings in slot order): each run from V to
+// the next vertex with the target entry/exit flag (or back at the start) is found with a
+// warp ballot and copied with coalesced stores.
+__device__ bool warp_trace(PairCtx& c) {
+  Ring& P = c.R[0];
+  OutRegion& O = c.O;
+  long long budget = 4ll * (c.R[0].used + c.R[1].used) + 16;
+  int from = 0;
+  for (;;) {
+    int I = warp_find_first(from, P.m, [&](int s) { return P.it[s] && P.lb[s] == L_CROSSING; });
+    if (I >= P.m) break;
+    O.begin();
+    if (O.overflow) { if (lane_id() == 0) fail(c, DEV_CAPACITY); return false; }
+    int side = 0, V = I;
+    if (lane_id() == 0) P.it[V] = 0;
+    __syncwarp();
+    do {
+      Ring& C = c.R[side];
+      const int m = C.m;
+      int8_t st = toggled(C.ee[V]);
+      const int dir = ((st == E_EXIT) ^ c.uni) ? 1 : -1;
+      int L = -1;
+      for (int j0 = 1; j0 <= m && L < 0; j0 += 32) {
+        int j = j0 + lane_id();
+        bool hit = false;
+        if (j <= m) {
+          int w = V + dir * (j % m);
+          w = (w % m + m) % m;
+          hit = (C.ee[w] == st) || (side == 0 && w == I);
+        }
+        unsigned msk = __ballot_sync(kFull, hit);
+        if (msk) L = j0 + __ffs(msk) - 1;
+      }
+      if (L < 0) { if (lane_id() == 0) fail(c, DEV_TRACE); return false; }
+      budget -= L;
+      if (budget < 0) { if (lane_id() == 0) fail(c, DEV_TRACE); return false; }
+      if (O.nv + L > O.vcap) { if (lane_id() == 0) fail(c, DEV_CAPACITY); return false; }
+      for (int j0 = 1; j0 <= L; j0 += 32) {
+        int j = j0 + lane_id();
+        if (j <= L) {
+          int w = V + dir * (j % m);
+          w = (w % m + m) % m;
+          C.it[w] = 0;
+          O.xy[2 * (O.nv + j - 1)] = C.x[w];
+          O.xy[2 * (O.nv + j - 1) + 1] = C.y[w];
+        }
+      }
+      O.nv += L;
+      if (lane_id() == 0) O.csz[O.nc] += L;
+      int W = V + dir * (L % m);
+      V = (W % m + m) % m;
+      __syncwarp();
+      if (!(side == 0 && V == I)) {
+        int nb = C.nb[V];
+        if (nb < 0) { if (lane_id() == 0) fail(c, DEV_TRACE); return false; }
+        V = nb;
+        side = 1 - side;
+        if (lane_id() == 0) c.R[side].it[V] = 0;
+        __syncwarp();
+      }
+    } while (!(side == 0 && V == I));
+    O.end();
+    from = I + 1;
+  }
+  return true;
+}
+
+// Clean-up: a component where no vertex is collinear with its two ring neighbours keeps
+// every vertex (the sequential pass would remove nothing), so it is only moved into place;
+// any other component is cleaned by one lane with the sequential pass.
+__device__ void warp_cleanup(PairCtx& c, int32_t* outNC, int64_t* outNV) {
+  OutRegion& O = c.O;
+  int64_t vin = 0, vout = 0;
+  int nc = 0;
+  for (int k = 0; k < O.nc; ++k) {
+    const int n = O.csz[k];
+    const double* src = O.xy + 2 * vin;
+    double* dst = O.xy + 2 * vout;
+    bool flag = false;
+    for (int j = lane_id(); j < n; j += 32) {
+      int p = (j > 0) ? j - 1 : n - 1, q = (j + 1 < n) ? j + 1 : 0;
+      if (fabs(area2(src[2 * p], src[2 * p + 1], src[2 * j], src[2 * j + 1], src[2 * q], src[2 * q + 1])) <
+          c.eps_clean)
+        flag = true;
+    }
+    flag = __any_sync(kFull, flag);
+    int kept;
+    if (!flag) {
+      if (dst != src) {
+        for (int b = 0; b < 2 * n; b += 32) {
+          int i = b + lane_id();
+          double v = (i < 2 * n) ? src[i] : 0.0;
+          __syncwarp();
+          if (i < 2 * n) dst[i] = v;
+        }
+      }
+      kept = n;
+    } else {
+      kept = 0;
+      if (lane_id() == 0) kept = seq_cleanup_component(src, dst, n, c.eps_clean);
+      kept = __shfl_sync(kFull, kept, 0);
+    }
+    __syncwarp();
+    vin += n;
+    if (kept == 0) continue;
+    if (lane_id() == 0) O.csz[nc] = kept;
+    ++nc;
+    vout += kept;
+    __syncwarp();
+  }
+  if (lane_id() == 0) { *outNC = nc; *outNV = vout; }
+}
+
+// One warp per pair.  The warp phases give the sequential result whenever neighbour links
+// are one-to-one (then labels written through a link never collide) and chains are well
+// formed; otherwise lane 0 runs the sequential phases from the first one that could differ.
+__global__ void __launch_bounds__(128)
+label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const int32_t* __restrict__ mQ,
+                   const int64_t* __restrict__ regP, const int64_t* __restrict__ regQ,
+                   const int64_t* __restrict__ regSizeP, const int64_t* __restrict__ regSizeQ,
+                   RingSet SP, RingSet SQ, double* __restrict__ outXY, const int64_t* __restrict__ outVOff,
+                   const int64_t* __restrict__ outVCap, int32_t* __restrict__ outCsz,
+                   const int64_t* __restrict__ outCOff, const int32_t* __restrict__ outCCap,
+                   int32_t* __restrict__ outNC, int64_t* __restrict__ outNV, ClipParams prm, int* err) {
+  int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (k >= K) return;
+  const bool lane0 = lane_id() == 0;
+  if (lane0) { outNC[k] = 0; outNV[k] = 0; }
+  if (D.status[k] != 0) return;
+  PairCtx c;
+  c.R[0] = ring_of(SP, regP[k], mP[k], (int)regSizeP[k]);
+  c.R[1] = ring_of(SQ, regQ[k], mQ[k], (int)regSizeQ[k]);
+  c.O.xy = outXY + 2 * outVOff[k]; c.O.csz = outCsz + outCOff[k]; c.O.vcap = outVCap[k]; c.O.ccap = outCCap[k];
+  c.O.nv = 0; c.O.nc = 0; c.O.overflow = false;
+  c.uni = prm.union_mode != 0;
+  c.eps_clean = prm.eps_clean;
+  c.err = err;
+  c.status = D.status + k;
+  c.noInter[0] = c.noInter[1] = c.ident[0] = c.ident[1] = false;
+
+  if (!warp_links_one_to_one(c.R[0], c.R[1])) {
+    if (lane0) seq_pair_from(c, 1, outNC + k, outNV + k);
+    return;
+  }
+  warp_step1(c);
+  if (!warp_step2(c)) {
+    if (lane0) seq_pair_from(c, 2, outNC + k, outNV + k);
+    return;
+  }
+  warp_step35(c);
+  int tempAfter[2], tempSlot[2];
+  if (!warp_step4(c, tempAfter, tempSlot)) return;
+  if (warp_any_split(c.R[0], c.R[1])) {
+    bool ok = true;
+    if (lane0) ok = seq_step5(c);
+    ok = __shfl_sync(kFull, (int)ok, 0);
+    c.R[0].used = __shfl_sync(kFull, c.R[0].used, 0);
+    c.R[1].used = __shfl_sync(kFull, c.R[1].used, 0);
+    __syncwarp();
+    if (!ok) return;
+  }
+  warp_step6(c);
+  const bool added = c.R[0].used != c.R[0].m || c.R[1].used != c.R[1].m;
+  if (added) {
+    // vertices were added to a ring: trace through the next/prev links on one lane
+    int ok = 1;
+    if (lane0) ok = seq_trace(c) ? 1 : 0;
+    ok = __shfl_sync(kFull, ok, 0);
+    c.O.nv = __shfl_sync(kFull, (long long)c.O.nv, 0);
+    c.O.nc = __shfl_sync(kFull, c.O.nc, 0);
+    __syncwarp();
+    if (!ok) return;
+  } else if (!warp_trace(c)) {
+    return;
+  }
+  if (c.O.overflow) {
+    if (lane0) fail(c, DEV_CAPACITY);
+    return;
+  }
+  warp_cleanup(c, outNC + k, outNV + k);
 }
 
 // ---------------------------------------------------------------- G8 compaction
@@ -958,19 +1546,44 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     S.x = A.take_n<double>(n); S.y = A.take_n<double>(n);
     S.nx = A.take_n<int32_t>(n); S.pv = A.take_n<int32_t>(n); S.nb = A.take_n<int32_t>(n);
     S.it = A.take_n<uint8_t>(n); S.lb = A.take_n<int8_t>(n); S.ee = A.take_n<int8_t>(n);
-    S.fl = A.take_n<uint8_t>(n); S.rec = A.take_n<int64_t>(n);
-    return S.x && S.y && S.nx && S.pv && S.nb && S.it && S.lb && S.ee && S.fl && S.rec;
+    S.fl = A.take_n<uint8_t>(n);
+    return S.x && S.y && S.nx && S.pv && S.nb && S.it && S.lb && S.ee && S.fl;
   };
   RingSet SP, SQ;
   if (!take_ring(regTotP, SP) || !take_ring(regTotQ, SQ)) return ST_OUT_OF_MEMORY;
   mk->mark("clip:layout", s);
-  // ---- G5 ring fill
-  if (nEP > 0)
-    { ring_fill_kernel<0><<<blocks_for(nEP), kThreads, 0, s>>>(Lb, Lo, D, R, eoffP, nEP, K, vposP, regP, mP, SP,
-                                                             slotP, insBaseP, curP, insListP); note_launch(); }
-  if (nEQ > 0)
-    { ring_fill_kernel<1><<<blocks_for(nEQ), kThreads, 0, s>>>(Lb, Lo, D, R, eoffQ, nEQ, K, vposQ, regQ, mQ, SQ,
-                                                             slotQ, insBaseQ, curQ, insListQ); note_launch(); }
+  // ---- G5 ring fill (light edges per thread, heavy edges per block)
+  {
+    int64_t* heavy = A.take_n<int64_t>(std::max(nEP, nEQ));
+    unsigned long long* nHeavy = A.take_n<unsigned long long>(2);
+    const int64_t nIns = std::max(nInsP, nInsQ);
+    uint64_t* gkey = A.take_n<uint64_t>(2 * nIns);
+    uint32_t* gtie = A.take_n<uint32_t>(2 * nIns);
+    uint32_t* gidx = A.take_n<uint32_t>(2 * nIns);
+    if (!heavy || !nHeavy || !gkey || !gtie || !gidx) return ST_OUT_OF_MEMORY;
+    const size_t smem = (size_t)kHeavySmem * (sizeof(uint64_t) + 2 * sizeof(uint32_t));
+    cudaFuncSetAttribute(heavy_fill_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(heavy_fill_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nEP > 0) {
+      cudaMemsetAsync(nHeavy, 0, sizeof(unsigned long long), s);
+      { ring_fill_kernel<0><<<blocks_for(nEP), kThreads, 0, s>>>(Lb, Lo, D, R, eoffP, nEP, K, vposP, regP, mP, SP,
+                                                               slotP, insBaseP, curP, insListP, heavy, nHeavy); note_launch(); }
+      { heavy_fill_kernel<0><<<2 * nsm, kHeavyThreads, smem, s>>>(Lb, Lo, D, R, eoffP, K, vposP, regP, mP, SP, slotP,
+                                                                  insBaseP, curP, insListP, heavy, nHeavy, gkey, gtie,
+                                                                  gidx); note_launch(); }
+    }
+    if (nEQ > 0) {
+      cudaMemsetAsync(nHeavy + 1, 0, sizeof(unsigned long long), s);
+      { ring_fill_kernel<1><<<blocks_for(nEQ), kThreads, 0, s>>>(Lb, Lo, D, R, eoffQ, nEQ, K, vposQ, regQ, mQ, SQ,
+                                                               slotQ, insBaseQ, curQ, insListQ, heavy, nHeavy + 1); note_launch(); }
+      { heavy_fill_kernel<1><<<2 * nsm, kHeavyThreads, smem, s>>>(Lb, Lo, D, R, eoffQ, K, vposQ, regQ, mQ, SQ, slotQ,
+                                                                  insBaseQ, curQ, insListQ, heavy, nHeavy + 1, gkey, gtie,
+                                                                  gidx); note_launch(); }
+    }
+  }
   // ---- G6 links
   if (nR > 0)
     { link_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, D.status, eoffP, eoffQ, vposP, vposQ, regP, regQ,
@@ -992,7 +1605,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int32_t* ocsz = A.take_n<int32_t>(hs[1]);
   if (!oxy || !ocsz) return ST_OUT_OF_MEMORY;
   mk->mark("clip:fill+link", s);
-  { label_trace_kernel<<<(unsigned)((K + 127) / 128), 128, 0, s>>>(D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ,
+  { label_trace_kernel<<<(unsigned)((K + 3) / 4), 128, 0, s>>>(D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ,
                                                                   SP, SQ, oxy, vOff, vcap, ocsz, cOff, ccap, nc,
                                                                   nv, prm, d_err); note_launch(); }
   mk->mark("clip:label+trace", s);
