@@ -308,6 +308,14 @@ gcmfgh_status gcmfgh_set_params(gcmfgh_ctx* c, double eps, double eps_clean, int
   return GCMFGH_OK;
 }
 
+gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* c, int key, int64_t value) {
+  if (!c || value < 0) return GCMFGH_INVALID_ARGUMENT;
+  if (key == GCMFGH_TUNE_BIN_GRID) c->prm.bin_grid = value;
+  else if (key == GCMFGH_TUNE_BIG_LABEL) c->prm.big_label_min = value;
+  else return GCMFGH_INVALID_ARGUMENT;
+  return GCMFGH_OK;
+}
+
 int gcmfgh_last_device_error(gcmfgh_ctx* c) { return c ? c->last_err : -1; }
 
 unsigned long long gcmfgh_launch_count(void) { return launch_counter(); }

@@ -34,6 +34,9 @@
 // labelling may add (one temporary vertex, one duplicate per split vertex): x, y, next,
 // prev, neighbour (pair-local slot on the other side), flags, label, entry/exit.
 #include <algorithm>
+#include <climits>
+#include <cmath>
+#include <vector>
 #include "common.cuh"
 #include "engine.cuh"
 #include "prims.cuh"
@@ -129,12 +132,21 @@ edge_filter_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, int32_t* __re
   }
 }
 
+// Pairs whose filtered edge grid exceeds ClipParams::bin_grid edge pairs are not
+// enumerated pair by pair: their edges are binned on a uniform grid (bin_* kernels).
+
 __global__ void chunk_count_kernel(const int32_t* __restrict__ cP, const int32_t* __restrict__ cQ,
-                                   int64_t K, int64_t* __restrict__ nchunk) {
+                                   int64_t K, int64_t* __restrict__ nchunk, int64_t* __restrict__ bigList,
+                                   unsigned long long* __restrict__ nBig, int64_t binGrid) {
   int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
   if (k >= K) return;
   int64_t W = (int64_t)cP[k] * cQ[k];
-  nchunk[k] = (W + kChunk - 1) / kChunk;
+  if (W > binGrid) {
+    nchunk[k] = 0;
+    bigList[atomicAdd(nBig, 1ull)] = k;
+  } else {
+    nchunk[k] = (W + kChunk - 1) / kChunk;
+  }
 }
 
 // ---------------------------------------------------------------- G2/G3 count + emit
@@ -154,7 +166,7 @@ intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* 
                  const int64_t* __restrict__ offP, const int64_t* __restrict__ offQ,
                  const int32_t* __restrict__ LP, const int32_t* __restrict__ LQ, double eps,
                  int32_t* __restrict__ chunkRec, int32_t* __restrict__ chunkQ,
-                 const int64_t* __restrict__ chunkRecOff, Records R) {
+                 const int64_t* __restrict__ chunkRecOff, const int64_t* __restrict__ recOff, Records R) {
   int64_t c = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
   if (c >= nChunks) return;
   // pair of this chunk: last k with chunkOff[k] <= c (pairs without chunks are skipped)
@@ -169,7 +181,7 @@ intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* 
   const int32_t* lp = LP + offP[k];
   const int32_t* lq = LQ + offQ[k];
   int recs = 0, qhits = 0;
-  int64_t pos = (kMode == 1) ? chunkRecOff[c] : 0;
+  int64_t pos = (kMode == 1) ? recOff[k] + chunkRecOff[c] - chunkRecOff[chunkOff[k]] : 0;
   for (int it = 0; it < kChunk / 32; ++it) {
     int64_t t = t0 + it * 32 + lane_id();
     int tp = 0, tq = 0;
@@ -201,24 +213,160 @@ intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* 
   if (kMode == 0 && lane_id() == 0) { chunkRec[c] = recs; chunkQ[c] = qhits; }
 }
 
-// per pair: record range, validity
+// per pair: record count (chunked + binned), validity
 __global__ void pair_records_kernel(const int64_t* __restrict__ chunkOff, const int64_t* __restrict__ nchunk,
                                     const int64_t* __restrict__ recScan, const int64_t* __restrict__ qScan,
                                     const int32_t* __restrict__ chunkRec, const int32_t* __restrict__ chunkQ,
-                                    int64_t K, int64_t* __restrict__ recOff, int32_t* __restrict__ nrec,
+                                    const int64_t* __restrict__ binRec, const int64_t* __restrict__ binQ,
+                                    int64_t K, int64_t* __restrict__ nrec64, int32_t* __restrict__ nrec,
                                     int64_t* __restrict__ count1, PairDev D) {
   int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
   if (k >= K) return;
   int64_t c0 = chunkOff[k], n = nchunk[k];
-  int64_t r0 = 0, r1 = 0, q0 = 0, q1 = 0;
+  int64_t r = binRec[k], q = binQ[k];
   if (n > 0) {
-    r0 = recScan[c0]; r1 = recScan[c0 + n - 1] + chunkRec[c0 + n - 1];
-    q0 = qScan[c0]; q1 = qScan[c0 + n - 1] + chunkQ[c0 + n - 1];
+    r += recScan[c0 + n - 1] + chunkRec[c0 + n - 1] - recScan[c0];
+    q += qScan[c0 + n - 1] + chunkQ[c0 + n - 1] - qScan[c0];
   }
-  recOff[k] = r0;
-  nrec[k] = (int32_t)(r1 - r0);
-  count1[k] = r1 - r0;
-  if (D.status[k] == 0 && (r1 - r0) != (q1 - q0)) D.status[k] = 1;   // gppolyclip_mDIV512.cu:1461
+  nrec64[k] = r;
+  nrec[k] = (int32_t)r;
+  count1[k] = r;
+  if (D.status[k] == 0 && r != q) D.status[k] = 1;   // gppolyclip_mDIV512.cu:1461
+}
+
+// ---------------------------------------------------------------- G2/G3 binned
+// A uniform grid over the common MBR.  Q edges are listed in every cell their box
+// covers; each P edge visits the cells its box covers and tests a Q edge only in the cell
+// holding the lower-left corner of the two boxes' overlap, so every edge pair whose boxes
+// touch is tested exactly once (cell indices are monotone in the coordinate).
+struct BinGrid { double x0, y0, cw, ch; int gx, gy; };
+
+__device__ __forceinline__ int cell_1d(double v, double c0, double cs, int g) {
+  double t = (v - c0) / cs;
+  if (!(t > 0)) return 0;             // also NaN
+  if (t >= (double)g) return g - 1;
+  return (int)t;
+}
+
+__global__ void bin_count_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LQ,
+                                 int cq, BinGrid G, int32_t* __restrict__ cellCnt) {
+  int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= cq) return;
+  const double2* qv = layer_xy(Lb, Lo, 1 - D.pSide[k]) + D.qS[k];
+  const int nq = D.nQ[k];
+  int q = LQ[i];
+  double2 a = __ldg(qv + q), b = __ldg(qv + (q + 1 < nq ? q + 1 : 0));
+  int x0 = cell_1d(fmin(a.x, b.x), G.x0, G.cw, G.gx), x1 = cell_1d(fmax(a.x, b.x), G.x0, G.cw, G.gx);
+  int y0 = cell_1d(fmin(a.y, b.y), G.y0, G.ch, G.gy), y1 = cell_1d(fmax(a.y, b.y), G.y0, G.ch, G.gy);
+  for (int y = y0; y <= y1; ++y)
+    for (int x = x0; x <= x1; ++x) atomicAdd(&cellCnt[(int64_t)y * G.gx + x], 1);
+}
+
+__global__ void bin_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LQ,
+                                int cq, BinGrid G, const int64_t* __restrict__ cellOff, int32_t* __restrict__ cursor,
+                                int32_t* __restrict__ cellList) {
+  int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= cq) return;
+  const double2* qv = layer_xy(Lb, Lo, 1 - D.pSide[k]) + D.qS[k];
+  const int nq = D.nQ[k];
+  int q = LQ[i];
+  double2 a = __ldg(qv + q), b = __ldg(qv + (q + 1 < nq ? q + 1 : 0));
+  int x0 = cell_1d(fmin(a.x, b.x), G.x0, G.cw, G.gx), x1 = cell_1d(fmax(a.x, b.x), G.x0, G.cw, G.gx);
+  int y0 = cell_1d(fmin(a.y, b.y), G.y0, G.ch, G.gy), y1 = cell_1d(fmax(a.y, b.y), G.y0, G.ch, G.gy);
+  for (int y = y0; y <= y1; ++y)
+    for (int x = x0; x <= x1; ++x) {
+      int64_t c = (int64_t)y * G.gx + x;
+      cellList[cellOff[c] + atomicAdd(&cursor[c], 1)] = q;
+    }
+}
+
+// mode 0: per P edge, records (P side) and the Q-side count; mode 1: write the records of
+// each P edge at its offset, then order them by Q edge.
+template <int kMode>
+__global__ void bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LP,
+                                 int cp, BinGrid G, const int64_t* __restrict__ cellOff,
+                                 const int32_t* __restrict__ cellList, double eps, int32_t* __restrict__ recCnt,
+                                 unsigned long long* __restrict__ qTotal, const int64_t* __restrict__ recPos,
+                                 Records R) {
+  int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= cp) return;
+  const int pside = D.pSide[k];
+  const double2* pv = layer_xy(Lb, Lo, pside) + D.pS[k];
+  const double2* qv = layer_xy(Lb, Lo, 1 - pside) + D.qS[k];
+  const int np_ = D.nP[k], nq = D.nQ[k];
+  const int p = LP[i];
+  const double2 P1 = __ldg(pv + p), P2 = __ldg(pv + (p + 1 < np_ ? p + 1 : 0));
+  const double pminx = fmin(P1.x, P2.x), pmaxx = fmax(P1.x, P2.x);
+  const double pminy = fmin(P1.y, P2.y), pmaxy = fmax(P1.y, P2.y);
+  int x0 = cell_1d(pminx, G.x0, G.cw, G.gx), x1 = cell_1d(pmaxx, G.x0, G.cw, G.gx);
+  int y0 = cell_1d(pminy, G.y0, G.ch, G.gy), y1 = cell_1d(pmaxy, G.y0, G.ch, G.gy);
+  int recs = 0, qhits = 0;
+  int64_t base = (kMode == 1) ? recPos[i] : 0;
+  for (int y = y0; y <= y1; ++y)
+    for (int x = x0; x <= x1; ++x) {
+      int64_t c = (int64_t)y * G.gx + x;
+      for (int64_t e = cellOff[c]; e < cellOff[c + 1]; ++e) {
+        int q = cellList[e];
+        double2 Q1 = __ldg(qv + q), Q2 = __ldg(qv + (q + 1 < nq ? q + 1 : 0));
+        if (!edge_boxes_touch(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y)) continue;
+        double cx = fmax(pminx, fmin(Q1.x, Q2.x)), cy = fmax(pminy, fmin(Q1.y, Q2.y));
+        if (cell_1d(cx, G.x0, G.cw, G.gx) != x || cell_1d(cy, G.y0, G.ch, G.gy) != y) continue;
+        double alpha = 0, beta = 0;
+        int tp = classify_edges(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
+        if (kMode == 0) {
+          double a2, b2;
+          if (classify_edges(Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2)) ++qhits;
+          if (tp) ++recs;
+        } else if (tp) {
+          int64_t r = base + recs++;
+          R.p[r] = p; R.q[r] = q; R.a[r] = alpha; R.b[r] = beta; R.t[r] = (int8_t)tp; R.k[r] = (int32_t)k;
+        }
+      }
+    }
+  if (kMode == 0) {
+    recCnt[i] = recs;
+    if (qhits) atomicAdd(qTotal, (unsigned long long)qhits);
+    return;
+  }
+  // order this edge's records by Q edge (insertion sort; few per edge)
+  for (int a = 1; a < recs; ++a) {
+    int64_t ra = base + a;
+    int qa = R.q[ra]; double aa = R.a[ra], ba = R.b[ra]; int8_t ta = R.t[ra];
+    int j = a - 1;
+    while (j >= 0 && R.q[base + j] > qa) {
+      int64_t rj = base + j;
+      R.q[rj + 1] = R.q[rj]; R.a[rj + 1] = R.a[rj]; R.b[rj + 1] = R.b[rj]; R.t[rj + 1] = R.t[rj];
+      --j;
+    }
+    R.q[base + j + 1] = qa; R.a[base + j + 1] = aa; R.b[base + j + 1] = ba; R.t[base + j + 1] = ta;
+  }
+}
+
+__global__ void add_offset_kernel(int64_t* __restrict__ a, int n, const int64_t* __restrict__ off) {
+  int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i < n) a[i] += *off;
+}
+
+// records binned count for a big pair -> per-pair arrays
+__global__ void bin_total_kernel(const int64_t* __restrict__ recTot, const unsigned long long* __restrict__ qTot,
+                                 int64_t k, int64_t* __restrict__ binRec, int64_t* __restrict__ binQ) {
+  binRec[k] = *recTot;
+  binQ[k] = (int64_t)*qTot;
+}
+
+// big-pair parameters gathered for the host
+struct BigInfo { int64_t k; int32_t cp, cq; int64_t offP, offQ; double cmbr[4]; };
+
+__global__ void big_info_kernel(const int64_t* __restrict__ bigList, int n, const int32_t* __restrict__ cP,
+                                const int32_t* __restrict__ cQ, const int64_t* __restrict__ offP,
+                                const int64_t* __restrict__ offQ, PairDev D, BigInfo* __restrict__ out) {
+  int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  int64_t k = bigList[i];
+  BigInfo b;
+  b.k = k; b.cp = cP[k]; b.cq = cQ[k]; b.offP = offP[k]; b.offQ = offQ[k];
+  for (int j = 0; j < 4; ++j) b.cmbr[j] = D.cmbr[4 * k + j];
+  out[i] = b;
 }
 
 // ---------------------------------------------------------------- G4 ring layout
@@ -1301,12 +1449,14 @@ label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const i
                    RingSet SP, RingSet SQ, double* __restrict__ outXY, const int64_t* __restrict__ outVOff,
                    const int64_t* __restrict__ outVCap, int32_t* __restrict__ outCsz,
                    const int64_t* __restrict__ outCOff, const int32_t* __restrict__ outCCap,
-                   int32_t* __restrict__ outNC, int64_t* __restrict__ outNV, ClipParams prm, int* err) {
+                   int32_t* __restrict__ outNC, int64_t* __restrict__ outNV, ClipParams prm, int* err,
+                   int64_t bigLabelMin) {
   int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (k >= K) return;
   const bool lane0 = lane_id() == 0;
   if (lane0) { outNC[k] = 0; outNV[k] = 0; }
   if (D.status[k] != 0) return;
+  if ((int64_t)mP[k] + mQ[k] > bigLabelMin) return;      // the grid path handles this pair
   PairCtx c;
   c.R[0] = ring_of(SP, regP[k], mP[k], (int)regSizeP[k]);
   c.R[1] = ring_of(SQ, regQ[k], mQ[k], (int)regSizeQ[k]);
@@ -1358,6 +1508,777 @@ label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const i
     return;
   }
   warp_cleanup(c, outNC + k, outNV + k);
+}
+
+// ================================================================ grid path for huge pairs
+// Pairs whose merged rings exceed ClipParams::big_label_min slots are labelled and traced
+// by grid-wide kernels, one phase per launch over the pair's ring slots, with the
+// host reading the few per-pair flags between phases.  The phases give the sequential
+// result under the same conditions as the warp path; otherwise one thread runs the
+// sequential phases from the first one that could differ.
+struct BigPair {
+  int64_t k, regP, regQ, vOff, vCap, cOff;
+  int32_t mP, mQ, capP, capQ, cCap, pad;
+};
+
+struct BigFlags {
+  int bad;
+  int notNone[2];
+  int notAllOn[2];
+  int firstFree[2];
+  int firstMid[2];
+  int anySplit;
+  int pad;
+  unsigned long long wind;
+};
+
+__device__ __forceinline__ Ring big_ring(const RingSet& S, int64_t reg, int m, int cap, int used) {
+  Ring r = ring_of(S, reg, m, cap);
+  r.used = used;
+  return r;
+}
+
+// 0: P, 1: Q of one pair; slot s of ring A; its ring successor/predecessor before any
+// vertex is added
+__device__ __forceinline__ int nxt_slot(int s, int m) { return (s + 1 < m) ? s + 1 : 0; }
+__device__ __forceinline__ int prv_slot(int s, int m) { return (s > 0) ? s - 1 : m - 1; }
+
+__global__ void big_links_kernel(RingSet SP, RingSet SQ, BigPair bp, BigFlags* f) {
+  Ring P = big_ring(SP, bp.regP, bp.mP, bp.capP, bp.mP), Q = big_ring(SQ, bp.regQ, bp.mQ, bp.capQ, bp.mQ);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)P.m + Q.m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    bool bad = false;
+    if (i < P.m) {
+      int s = (int)i;
+      if (P.it[s]) { int nb = P.nb[s]; bad = nb < 0 || nb >= Q.m || Q.nb[nb] != s; }
+    } else {
+      int s = (int)(i - P.m);
+      if (Q.it[s]) { int nb = Q.nb[s]; bad = nb < 0 || nb >= P.m || P.nb[nb] != s; }
+    }
+    if (bad) atomicOr(&f->bad, 1);
+  }
+}
+
+__global__ void big_step1_kernel(RingSet SP, RingSet SQ, BigPair bp) {
+  Ring P = big_ring(SP, bp.regP, bp.mP, bp.capP, bp.mP), Q = big_ring(SQ, bp.regQ, bp.mQ, bp.capQ, bp.mQ);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P.m; s += gridDim.x * blockDim.x) {
+    if (!P.it[s]) continue;
+    int nb = P.nb[s];
+    int pm = prv_slot(s, P.m), pp = nxt_slot(s, P.m);
+    int a = rel_position(P, Q, prv_slot(nb, Q.m), pm, s, pp);
+    int b = rel_position(P, Q, nxt_slot(nb, Q.m), pm, s, pp);
+    int8_t L = initial_label(a, b);
+    if (L != L_NONE) { P.lb[s] = L; Q.lb[nb] = L; }
+  }
+}
+
+// kMode 0: every chain must end at an ON_LEFT/ON_RIGHT intersection vertex; 1: resolve
+template <int kMode>
+__global__ void big_chain_kernel(RingSet SP, RingSet SQ, BigPair bp, BigFlags* f) {
+  Ring P = big_ring(SP, bp.regP, bp.mP, bp.capP, bp.mP), Q = big_ring(SQ, bp.regQ, bp.mQ, bp.capQ, bp.mQ);
+  const int m = P.m;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) {
+    int8_t l0 = P.lb[s];
+    if (!P.it[s] || (l0 != L_LEFT_ON && l0 != L_RIGHT_ON)) continue;
+    int I = nxt_slot(s, m), guard = m;
+    if (kMode == 0) {
+      while (P.lb[I] == L_ON_ON && --guard > 0) I = nxt_slot(I, m);
+      if ((P.lb[I] != L_ON_LEFT && P.lb[I] != L_ON_RIGHT) || !P.it[I]) atomicOr(&f->bad, 1);
+    } else {
+      int x = l0 == L_LEFT_ON ? R_LEFT : R_RIGHT;
+      Q.lb[P.nb[s]] = L_NONE;
+      while (P.lb[I] == L_ON_ON) {
+        P.lb[I] = L_NONE;
+        Q.lb[P.nb[I]] = L_NONE;
+        I = nxt_slot(I, m);
+      }
+      int y = P.lb[I] == L_ON_LEFT ? R_LEFT : R_RIGHT;
+      int8_t ct = (x != y) ? L_DELAYED_CROSSING : L_DELAYED_BOUNCING;
+      P.lb[s] = ct; P.lb[I] = ct;
+      Q.lb[P.nb[s]] = ct; Q.lb[P.nb[I]] = ct;
+    }
+  }
+}
+
+// special-case flags of both rings (polygon.h:453-512 on the rings before any insertion)
+__global__ void big_flags_kernel(RingSet SP, RingSet SQ, BigPair bp, int uni, BigFlags* f) {
+  Ring R[2] = {big_ring(SP, bp.regP, bp.mP, bp.capP, bp.mP), big_ring(SQ, bp.regQ, bp.mQ, bp.capQ, bp.mQ)};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)R[0].m + R[1].m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int sd = i < R[0].m ? 0 : 1;
+    int v = (int)(sd == 0 ? i : i - R[0].m);
+    const Ring& A = R[sd];
+    const Ring& B = R[1 - sd];
+    int8_t l = A.lb[v];
+    if (l != L_ON_ON) atomicOr(&f->notAllOn[sd], 1);
+    if (A.it[v]) {
+      if (l == L_CROSSING || l == L_DELAYED_CROSSING) atomicOr(&f->notNone[sd], 1);
+      if (uni && (l == L_BOUNCING || l == L_DELAYED_BOUNCING)) atomicOr(&f->notNone[sd], 1);
+    } else {
+      atomicMin(&f->firstFree[sd], v);
+    }
+    int nb = A.nb[v], nx = nxt_slot(v, A.m);
+    if (nb >= 0 && A.nb[nx] != prv_slot(nb, B.m) && A.nb[nx] != nxt_slot(nb, B.m)) atomicMin(&f->firstMid[sd], v);
+  }
+}
+
+// first midpoint-rule vertex of ring A against ring B through B's current links (B may
+// hold its temporary vertex)
+__global__ void big_first_mid_kernel(RingSet SA, RingSet SB, int64_t regA, int mA, int capA, int64_t regB, int mB,
+                                     int capB, int usedB, int* out) {
+  Ring A = big_ring(SA, regA, mA, capA, mA), B = big_ring(SB, regB, mB, capB, usedB);
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < A.m; v += gridDim.x * blockDim.x) {
+    int nb = A.nb[v], nx = nxt_slot(v, A.m);
+    if (nb >= 0 && A.nb[nx] != B.pv[nb] && A.nb[nx] != B.nx[nb]) atomicMin(out, v);
+  }
+}
+
+// winding parity test (polygon.h:427-448) of a point of ring A against ring B.
+// point: slot v of A (mode 0), midpoint of v and its successor (mode 1).
+// B's edges are (s, s+1); `after`/`T` splice a temporary vertex of B.
+__global__ void big_wind_kernel(RingSet SA, int64_t regA, int mA, int v, int mode, RingSet SB, int64_t regB, int mB,
+                                int after, int T, unsigned long long* wsum) {
+  const double* ax = SA.x + regA;
+  const double* ay = SA.y + regA;
+  double Rx = ax[v], Ry = ay[v];
+  if (mode == 1) { int n = nxt_slot(v, mA); Rx = 0.5 * (ax[v] + ax[n]); Ry = 0.5 * (ay[v] + ay[n]); }
+  const double* bx = SB.x + regB;
+  const double* by = SB.y + regB;
+  long long w = 0;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < mB; s += gridDim.x * blockDim.x) {
+    int n = nxt_slot(s, mB);
+    if (s == after) {
+      w += wind(bx[s], by[s], bx[T], by[T], Rx, Ry);
+      w += wind(bx[T], by[T], bx[n], by[n], Rx, Ry);
+    } else {
+      w += wind(bx[s], by[s], bx[n], by[n], Rx, Ry);
+    }
+  }
+  w = warp_sum(w);
+  if (lane_id() == 0 && w) atomicAdd(wsum, (unsigned long long)w);
+}
+
+__global__ void big_copy_ring_kernel(RingSet S, int64_t reg, int m, double* __restrict__ oxy, int64_t at,
+                                     int32_t* __restrict__ csz, int comp) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) {
+    oxy[2 * (at + s)] = S.x[reg + s];
+    oxy[2 * (at + s) + 1] = S.y[reg + s];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) csz[comp] = m;
+}
+
+__global__ void big_add_temp_kernel(RingSet S, int64_t reg, int m, int cap, int used, int v) {
+  Ring A = big_ring(S, reg, m, cap, used);
+  int n = A.nx[v];
+  int T = add_vertex(A, 0.5 * (A.x[v] + A.x[n]), 0.5 * (A.y[v] + A.y[n]));
+  if (T >= 0) insert_after(A, T, v);
+}
+
+// step 4 as scans over the ring rotated to start after V0 (see warp_step4)
+__global__ void big_d_kernel(RingSet S, int64_t reg, int m, int V0, int32_t* __restrict__ d) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    int s = V0 + 1 + j;
+    if (s >= m) s -= m;
+    int8_t L = S.lb[reg + s];
+    d[j] = (S.it[reg + s] && (L == L_DELAYED_CROSSING || L == L_DELAYED_BOUNCING)) ? 1 : 0;
+  }
+}
+
+__global__ void big_t_kernel(RingSet S, int64_t reg, int m, int V0, const int64_t* __restrict__ dEx,
+                             int32_t* __restrict__ t) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    int s = V0 + 1 + j;
+    if (s >= m) s -= m;
+    int8_t L = S.lb[reg + s];
+    bool first = (dEx[j] & 1) == 0;
+    t[j] = (S.it[reg + s] && (L == L_CROSSING || L == L_DELAYED_BOUNCING || (L == L_DELAYED_CROSSING && !first))) ? 1 : 0;
+  }
+}
+
+__global__ void big_apply4_kernel(RingSet S, int64_t reg, int m, int V0, const int64_t* __restrict__ dEx,
+                                  const int64_t* __restrict__ tEx, int8_t st0, int uni) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    int s = V0 + 1 + j;
+    if (s >= m) s -= m;
+    const int64_t g = reg + s;
+    if (!S.it[g]) continue;
+    int8_t L = S.lb[g];
+    bool first = (dEx[j] & 1) == 0;
+    int8_t st = (tEx[j] & 1) ? toggled(st0) : st0;
+    if (L == L_CROSSING) S.ee[g] = st;
+    else if (L == L_BOUNCING) { if ((st == E_EXIT) ^ (uni != 0)) S.fl[g] |= 1; }
+    else if (L == L_DELAYED_CROSSING) {
+      S.ee[g] = st;
+      if (first) { if ((st == E_EXIT) ^ (uni != 0)) S.lb[g] = L_CROSSING; }
+      else if ((st == E_ENTRY) ^ (uni != 0)) S.lb[g] = L_CROSSING;
+    } else if (L == L_DELAYED_BOUNCING) {
+      S.ee[g] = st;
+      if (first) { if ((st == E_EXIT) ^ (uni != 0)) S.fl[g] |= 2; }
+      else if ((st == E_ENTRY) ^ (uni != 0)) S.fl[g] |= 2;
+    }
+  }
+}
+
+__global__ void big_split_any_kernel(RingSet SP, RingSet SQ, BigPair bp, BigFlags* f) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < bp.mP; s += gridDim.x * blockDim.x) {
+    if (!(SP.fl[bp.regP + s] & 1)) continue;
+    int nb = SP.nb[bp.regP + s];
+    if (nb >= 0 && (SQ.fl[bp.regQ + nb] & 1)) atomicOr(&f->anySplit, 1);
+  }
+}
+
+__global__ void big_step6_kernel(RingSet SP, RingSet SQ, BigPair bp) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < bp.mP; s += gridDim.x * blockDim.x) {
+    if (!(SP.fl[bp.regP + s] & 2)) continue;
+    int nb = SP.nb[bp.regP + s];
+    if (nb >= 0 && (SQ.fl[bp.regQ + nb] & 2)) { SP.lb[bp.regP + s] = L_CROSSING; SQ.lb[bp.regQ + nb] = L_CROSSING; }
+  }
+}
+
+// the sequential phases from step 5 (split pairs) or from the trace on, one thread
+__global__ void big_seq_tail_kernel(RingSet SP, RingSet SQ, BigPair bp, int usedP, int usedQ, int from_trace,
+                                    double* __restrict__ oxy, int32_t* __restrict__ ocsz, int64_t nv0, int nc0,
+                                    ClipParams prm, int* err, int32_t* status, int32_t* outNC, int64_t* outNV) {
+  PairCtx c;
+  c.R[0] = big_ring(SP, bp.regP, bp.mP, bp.capP, usedP);
+  c.R[1] = big_ring(SQ, bp.regQ, bp.mQ, bp.capQ, usedQ);
+  c.O.xy = oxy + 2 * bp.vOff; c.O.csz = ocsz + bp.cOff; c.O.vcap = bp.vCap; c.O.ccap = bp.cCap;
+  c.O.nv = nv0; c.O.nc = nc0; c.O.overflow = false;
+  c.uni = prm.union_mode != 0;
+  c.eps_clean = prm.eps_clean;
+  c.err = err;
+  c.status = status + bp.k;
+  if (!from_trace) {
+    if (!seq_step5(c)) return;
+    seq_step6(c);
+  }
+  if (!seq_trace(c)) return;
+  seq_cleanup(c, outNC + bp.k, outNV + bp.k);
+}
+
+// the whole pair sequentially from `step` (links not one-to-one, malformed chains)
+__global__ void big_seq_pair_kernel(RingSet SP, RingSet SQ, BigPair bp, int step, double* __restrict__ oxy,
+                                    int32_t* __restrict__ ocsz, ClipParams prm, int* err, int32_t* status,
+                                    int32_t* outNC, int64_t* outNV) {
+  PairCtx c;
+  c.R[0] = big_ring(SP, bp.regP, bp.mP, bp.capP, bp.mP);
+  c.R[1] = big_ring(SQ, bp.regQ, bp.mQ, bp.capQ, bp.mQ);
+  c.O.xy = oxy + 2 * bp.vOff; c.O.csz = ocsz + bp.cOff; c.O.vcap = bp.vCap; c.O.ccap = bp.cCap;
+  c.O.nv = 0; c.O.nc = 0; c.O.overflow = false;
+  c.uni = prm.union_mode != 0;
+  c.eps_clean = prm.eps_clean;
+  c.err = err;
+  c.status = status + bp.k;
+  c.noInter[0] = c.noInter[1] = c.ident[0] = c.ident[1] = false;
+  seq_pair_from(c, step, outNC + bp.k, outNV + bp.k);
+}
+
+// ---- parallel tracing.  With no added vertices, when every vertex carrying an entry/exit
+// flag is an unvisited CROSSING vertex and vice versa, flags alternate along each ring
+// and linked vertices carry opposite flags, a run from a flagged vertex V ends at the
+// next flagged vertex in its direction, W(V), and continues at the twin of W(V).  Runs
+// from ENTRY vertices form cycles (one per result component); the reference traces each
+// component from its smallest-slot flagged P vertex I, forwards if I starts a run of the
+// cycle, else (I ends one) along the reversed cycle.
+__global__ void big_labeled_kernel(RingSet S, int64_t reg, int m, uint8_t* __restrict__ lab, BigFlags* f) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) {
+    int8_t e = S.ee[reg + s];
+    bool flagged = (e == E_ENTRY || e == E_EXIT);
+    bool crossing = S.it[reg + s] && S.lb[reg + s] == L_CROSSING;
+    lab[s] = flagged ? 1 : 0;
+    if (flagged != crossing) atomicOr(&f->bad, 1);
+  }
+}
+
+__global__ void big_lab_list_kernel(const uint8_t* __restrict__ lab, const int64_t* __restrict__ idx, int m,
+                                    int32_t* __restrict__ list) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x)
+    if (lab[s]) list[idx[s]] = s;
+}
+
+// per flagged vertex u (P: [0,nP), Q: [nP,nP+nQ)): checks, run stop, length, successor
+__global__ void big_runs_kernel(RingSet SP, RingSet SQ, BigPair bp, const int32_t* __restrict__ listP,
+                                const int32_t* __restrict__ listQ, const int64_t* __restrict__ idxP,
+                                const int64_t* __restrict__ idxQ, int nP, int nQ, int uni, int32_t* __restrict__ succ,
+                                int32_t* __restrict__ len, int32_t* __restrict__ stop, BigFlags* f) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nP + nQ; u += gridDim.x * blockDim.x) {
+    const bool onP = u < nP;
+    const RingSet& A = onP ? SP : SQ;
+    const RingSet& B = onP ? SQ : SP;
+    const int64_t ra = onP ? bp.regP : bp.regQ, rb = onP ? bp.regQ : bp.regP;
+    const int m = onP ? bp.mP : bp.mQ;
+    const int n = onP ? nP : nQ;
+    const int i = onP ? u : u - nP;
+    const int32_t* list = onP ? listP : listQ;
+    const int s = list[i];
+    const int8_t e = A.ee[ra + s];
+    bool bad = n < 2;
+    int nxt = list[(i + 1 < n) ? i + 1 : 0];
+    if (A.ee[ra + nxt] == e) bad = true;                         // alternation
+    int nb = A.nb[ra + s];
+    if (nb < 0 || B.ee[rb + nb] != toggled(e)) bad = true;        // twin carries the opposite flag
+    const int8_t st = toggled(e);
+    const int dir = ((st == E_EXIT) ^ (uni != 0)) ? 1 : -1;
+    int W = list[(i + dir + n) % n];
+    int L = dir > 0 ? W - s : s - W;
+    if (L <= 0) L += m;
+    int nbW = A.nb[ra + W];
+    if (nbW < 0) bad = true;
+    int v = 0;
+    if (!bad) v = onP ? nP + (int)idxQ[nbW] : (int)idxP[nbW];
+    succ[u] = v;
+    len[u] = L;
+    stop[u] = W;
+    if (bad) atomicOr(&f->bad, 1);
+  }
+}
+
+// pointer jumping over ENTRY-start vertices: cycle minima of the P-start slots (a) and
+// of the P-stop slots (b)
+__global__ void big_cycle_min_kernel(const int32_t* __restrict__ J, const int32_t* __restrict__ a,
+                                     const int32_t* __restrict__ b, int32_t* __restrict__ J2, int32_t* __restrict__ a2,
+                                     int32_t* __restrict__ b2, const uint8_t* __restrict__ isE, int N) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
+    if (!isE[u]) continue;
+    int j = J[u];
+    a2[u] = min(a[u], a[j]);
+    b2[u] = min(b[u], b[j]);
+    J2[u] = J[j];
+  }
+}
+
+__global__ void big_cycle_init_kernel(RingSet SP, RingSet SQ, BigPair bp, const int32_t* __restrict__ listP,
+                                      const int32_t* __restrict__ listQ, int nP, int nQ, const int32_t* __restrict__ succ,
+                                      const int32_t* __restrict__ stop, int32_t* __restrict__ J, int32_t* __restrict__ a,
+                                      int32_t* __restrict__ b, uint8_t* __restrict__ isE) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nP + nQ; u += gridDim.x * blockDim.x) {
+    const bool onP = u < nP;
+    const int s = onP ? listP[u] : listQ[u - nP];
+    const int8_t e = onP ? SP.ee[bp.regP + s] : SQ.ee[bp.regQ + s];
+    isE[u] = e == E_ENTRY ? 1 : 0;
+    J[u] = succ[u];
+    a[u] = onP ? s : INT_MAX;
+    b[u] = onP ? stop[u] : INT_MAX;
+  }
+}
+
+// per ENTRY vertex: the cycle's list-ranking start B and direction; list break
+__global__ void big_cycle_start_kernel(const int32_t* __restrict__ a, const int32_t* __restrict__ b,
+                                       const uint8_t* __restrict__ isE, const int64_t* __restrict__ idxP,
+                                       const int32_t* __restrict__ listP, int nP, int N, int dirE,
+                                       const int32_t* __restrict__ succ, const int32_t* __restrict__ len,
+                                       int32_t* __restrict__ Bst, uint8_t* __restrict__ rev, int32_t* __restrict__ nxt,
+                                       int64_t* __restrict__ sfx) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
+    if (!isE[u]) continue;
+    int B;
+    if (a[u] < b[u]) {
+      B = (int)idxP[a[u]];                       // I starts a run: forwards from I
+      rev[u] = 0;
+    } else {
+      int iI = (int)idxP[b[u]];                  // I ends the run of A
+      int iA = ((iI - dirE) % nP + nP) % nP;
+      B = succ[iA];
+      rev[u] = 1;
+    }
+    Bst[u] = B;
+    nxt[u] = (succ[u] == B) ? -1 : succ[u];
+    sfx[u] = len[u];
+  }
+}
+
+__global__ void big_rank_kernel(const int32_t* __restrict__ nxt, const int64_t* __restrict__ sfx,
+                                int32_t* __restrict__ nxt2, int64_t* __restrict__ sfx2, const uint8_t* __restrict__ isE,
+                                int N) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
+    if (!isE[u]) continue;
+    int j = nxt[u];
+    if (j >= 0) { sfx2[u] = sfx[u] + sfx[j]; nxt2[u] = nxt[j]; }
+    else { sfx2[u] = sfx[u]; nxt2[u] = -1; }
+  }
+}
+
+// one writer per cycle: its length at the slot of I (components in ascending I)
+__global__ void big_comp_len_kernel(const uint8_t* __restrict__ isE, const int32_t* __restrict__ Bst,
+                                    const int64_t* __restrict__ sfx, const int32_t* __restrict__ a,
+                                    const int32_t* __restrict__ b, int N, int64_t* __restrict__ compLen,
+                                    uint8_t* __restrict__ compFlag) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
+    if (!isE[u] || Bst[u] != u) continue;
+    int I = min(a[u], b[u]);
+    compLen[I] = sfx[u];
+    compFlag[I] = 1;
+  }
+}
+
+// warp per run: copies the run's vertices to their places in the component
+__global__ void big_write_kernel(RingSet SP, RingSet SQ, BigPair bp, const int32_t* __restrict__ listP,
+                                 const int32_t* __restrict__ listQ, int nP, int N, const uint8_t* __restrict__ isE,
+                                 const int32_t* __restrict__ len, const int32_t* __restrict__ Bst,
+                                 const uint8_t* __restrict__ rev, const int64_t* __restrict__ sfx,
+                                 const int32_t* __restrict__ a, const int32_t* __restrict__ b,
+                                 const int64_t* __restrict__ compBase, const int64_t* __restrict__ compIdx,
+                                 int64_t nv0, int nc0, int uni, double* __restrict__ oxy, int32_t* __restrict__ ocsz) {
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= N || !isE[w]) return;
+  const int u = (int)w;
+  const bool onP = u < nP;
+  const RingSet& A = onP ? SP : SQ;
+  const int64_t ra = onP ? bp.regP : bp.regQ;
+  const int m = onP ? bp.mP : bp.mQ;
+  const int s = onP ? listP[u] : listQ[u - nP];
+  const int8_t st = toggled(A.ee[ra + s]);
+  const int dir = ((st == E_EXIT) ^ (uni != 0)) ? 1 : -1;
+  const int I = min(a[u], b[u]);
+  const int64_t L = sfx[Bst[u]];
+  const int64_t off = L - sfx[u];
+  const int lu = len[u];
+  const bool r = rev[u];
+  const int64_t base = nv0 + compBase[I];
+  for (int j = lane_id(); j < lu; j += 32) {
+    int v = s + dir * (j + 1);
+    v = ((v % m) + m) % m;
+    int64_t f = off + j;
+    int64_t pos = r ? ((f < L - 1) ? L - 2 - f : L - 1) : f;
+    oxy[2 * (base + pos)] = A.x[ra + v];
+    oxy[2 * (base + pos) + 1] = A.y[ra + v];
+  }
+  if (lane_id() == 0 && Bst[u] == u) ocsz[bp.cOff + nc0 + compIdx[I]] = (int32_t)L;
+}
+
+// warp per component of the pair: clean-up in place (see warp_cleanup)
+__global__ void big_cleanup_kernel(double* __restrict__ xy, const int32_t* __restrict__ csz,
+                                   const int64_t* __restrict__ cstart, int nc, double eps, int32_t* __restrict__ kept) {
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nc) return;
+  const int n = csz[w];
+  double* src = xy + 2 * cstart[w];
+  bool flag = false;
+  for (int j = lane_id(); j < n; j += 32) {
+    int p = (j > 0) ? j - 1 : n - 1, q = (j + 1 < n) ? j + 1 : 0;
+    if (fabs(area2(src[2 * p], src[2 * p + 1], src[2 * j], src[2 * j + 1], src[2 * q], src[2 * q + 1])) < eps)
+      flag = true;
+  }
+  flag = __any_sync(kFull, flag);
+  if (lane_id() == 0) kept[w] = flag ? seq_cleanup_component(src, src, n, eps) : n;
+}
+
+__global__ void big_compact_kernel(const double* __restrict__ xy, const int64_t* __restrict__ cstart,
+                                   const int32_t* __restrict__ kept, const int64_t* __restrict__ kstart, int nc,
+                                   double* __restrict__ tmp) {
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nc) return;
+  const double* src = xy + 2 * cstart[w];
+  double* dst = tmp + 2 * kstart[w];
+  for (int i = lane_id(); i < 2 * kept[w]; i += 32) dst[i] = src[i];
+}
+
+__global__ void big_finish_kernel(const int32_t* __restrict__ kept, const int64_t* __restrict__ cidx, int nc,
+                                  int32_t* __restrict__ csz) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+    if (kept[c] > 0) csz[cidx[c]] = kept[c];
+}
+
+__global__ void big_info_label_kernel(const int64_t* __restrict__ list, int n, const int64_t* __restrict__ regP,
+                                      const int64_t* __restrict__ regQ, const int32_t* __restrict__ mP,
+                                      const int32_t* __restrict__ mQ, const int64_t* __restrict__ regSizeP,
+                                      const int64_t* __restrict__ regSizeQ, const int64_t* __restrict__ vOff,
+                                      const int64_t* __restrict__ vCap, const int64_t* __restrict__ cOff,
+                                      const int32_t* __restrict__ cCap, BigPair* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t k = list[i];
+  BigPair b;
+  b.k = k; b.regP = regP[k]; b.regQ = regQ[k]; b.vOff = vOff[k]; b.vCap = vCap[k]; b.cOff = cOff[k];
+  b.mP = mP[k]; b.mQ = mQ[k]; b.capP = (int32_t)regSizeP[k]; b.capQ = (int32_t)regSizeQ[k]; b.cCap = cCap[k];
+  b.pad = 0;
+  out[i] = b;
+}
+
+__global__ void big_label_list_kernel(const int32_t* __restrict__ mP, const int32_t* __restrict__ mQ,
+                                      const int32_t* __restrict__ status, int64_t K, int64_t minSlots,
+                                      int64_t* __restrict__ list, unsigned long long* __restrict__ n) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K || status[k] != 0) return;
+  if ((int64_t)mP[k] + mQ[k] > minSlots) list[atomicAdd(n, 1ull)] = k;
+}
+
+__global__ void big_kflag_kernel(const int32_t* __restrict__ kept, int nc, uint8_t* __restrict__ f) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) f[c] = kept[c] > 0;
+}
+
+__global__ void big_set_counts_kernel(int32_t* outNC, int64_t* outNV, int nc, int64_t nv) {
+  *outNC = nc;
+  *outNV = nv;
+}
+
+__global__ void big_fail_kernel(int32_t* status, int* err, int code) {
+  *status = 3;
+  raise_error(err, code);
+}
+
+// Host driver of the grid path for one huge pair.
+struct BigCtx {
+  Arena& A;
+  cudaStream_t s;
+  int64_t* hs;
+  int* d_err;
+  RingSet SP, SQ;
+  double* oxy;
+  int32_t* ocsz;
+  int32_t* status;
+  int32_t* outNC;
+  int64_t* outNV;
+  ClipParams prm;
+};
+
+static unsigned grid_for(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 32));
+}
+
+static int run_big_label_pair(BigCtx& c, const BigPair& bp, BigFlags* df) {
+  cudaStream_t s = c.s;
+  const bool uni = c.prm.union_mode != 0;
+  auto sync = [&]() { return cudaStreamSynchronize(s) == cudaSuccess; };
+  BigFlags h{};
+  h.firstFree[0] = h.firstMid[0] = bp.mP;
+  h.firstFree[1] = h.firstMid[1] = bp.mQ;
+  cudaMemcpyAsync(df, &h, sizeof(BigFlags), cudaMemcpyHostToDevice, s);
+  auto read_flags = [&]() {
+    cudaMemcpyAsync(&h, df, sizeof(BigFlags), cudaMemcpyDeviceToHost, s);
+    return sync();
+  };
+  auto seq_pair = [&](int step) {
+    { big_seq_pair_kernel<<<1, 1, 0, s>>>(c.SP, c.SQ, bp, step, c.oxy, c.ocsz, c.prm, c.d_err, c.status, c.outNC,
+                                         c.outNV); note_launch(); }
+    return ST_OK;
+  };
+  const int64_t nAll = (int64_t)bp.mP + bp.mQ;
+  // ---- links one-to-one?
+  { big_links_kernel<<<grid_for(nAll), 256, 0, s>>>(c.SP, c.SQ, bp, df); note_launch(); }
+  if (!read_flags()) return ST_CUDA_ERROR;
+  if (h.bad) return seq_pair(1);
+  // ---- step 1, chains
+  { big_step1_kernel<<<grid_for(bp.mP), 256, 0, s>>>(c.SP, c.SQ, bp); note_launch(); }
+  { big_chain_kernel<0><<<grid_for(bp.mP), 256, 0, s>>>(c.SP, c.SQ, bp, df); note_launch(); }
+  if (!read_flags()) return ST_CUDA_ERROR;
+  if (h.bad) return seq_pair(2);
+  { big_chain_kernel<1><<<grid_for(bp.mP), 256, 0, s>>>(c.SP, c.SQ, bp, df); note_launch(); }
+  // ---- special cases (3.5)
+  { big_flags_kernel<<<grid_for(nAll), 256, 0, s>>>(c.SP, c.SQ, bp, uni ? 1 : 0, df); note_launch(); }
+  if (!read_flags()) return ST_CUDA_ERROR;
+  const int m[2] = {bp.mP, bp.mQ};
+  const int64_t reg[2] = {bp.regP, bp.regQ};
+  const int cap[2] = {bp.capP, bp.capQ};
+  const RingSet* S[2] = {&c.SP, &c.SQ};
+  bool noInter[2], ident[2];
+  for (int sd = 0; sd < 2; ++sd) {
+    noInter[sd] = !h.notNone[sd];
+    ident[sd] = noInter[sd] && !h.notAllOn[sd];
+  }
+  int64_t nv = 0;
+  int nc = 0;
+  unsigned long long* dwind = &df->wind;
+  auto winding = [&](int sa, int v, int mode, int sb, int after, int T, bool& inside) {
+    cudaMemsetAsync(dwind, 0, sizeof(unsigned long long), s);
+    { big_wind_kernel<<<grid_for(m[sb]), 256, 0, s>>>(*S[sa], reg[sa], m[sa], v, mode, *S[sb], reg[sb], m[sb], after, T,
+                                                      dwind); note_launch(); }
+    unsigned long long w = 0;
+    cudaMemcpyAsync(&w, dwind, sizeof(w), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return false;
+    inside = ((long long)w % 2) != 0;
+    return true;
+  };
+  auto push_ring = [&](int sd) {
+    if (nv + m[sd] > bp.vCap || nc >= bp.cCap) return false;
+    { big_copy_ring_kernel<<<grid_for(m[sd]), 256, 0, s>>>(*S[sd], reg[sd], m[sd], c.oxy, bp.vOff + nv,
+                                                           c.ocsz + bp.cOff, nc); note_launch(); }
+    nv += m[sd];
+    ++nc;
+    return true;
+  };
+  auto fail = [&](int code) {
+    { big_fail_kernel<<<1, 1, 0, s>>>(c.status + bp.k, c.d_err, code); note_launch(); }
+    return ST_OK;
+  };
+  for (int sd = 0; sd < 2; ++sd) {
+    if (!noInter[sd] || ident[sd]) continue;
+    int v = -1, mode = 0;
+    if (h.firstFree[sd] < m[sd]) v = h.firstFree[sd];
+    else if (h.firstMid[sd] < m[sd]) { v = h.firstMid[sd]; mode = 1; }
+    if (v < 0) continue;
+    bool inside;
+    if (!winding(sd, v, mode, 1 - sd, -1, -1, inside)) return ST_CUDA_ERROR;
+    if (inside ^ uni)
+      if (!push_ring(sd)) return fail(DEV_CAPACITY);
+  }
+  if (ident[0] && ident[1])
+    if (!push_ring(0)) return fail(DEV_CAPACITY);
+  // ---- step 4 (entry/exit) as device scans over the rotated rings
+  int used[2] = {bp.mP, bp.mQ};
+  int tempAfter[2] = {-1, -1}, tempSlot[2] = {-1, -1};
+  {
+    const int mm = std::max(bp.mP, bp.mQ);
+    int32_t* d = c.A.take_n<int32_t>(mm);
+    int32_t* t = c.A.take_n<int32_t>(mm);
+    int64_t* dEx = c.A.take_n<int64_t>(mm);
+    int64_t* tEx = c.A.take_n<int64_t>(mm);
+    void* st = c.A.take(scan_temp_bytes(mm));
+    if (!d || !t || !dEx || !tEx || !st) return ST_OUT_OF_MEMORY;
+    for (int sd = 0; sd < 2; ++sd) {
+      if (noInter[sd]) continue;
+      int V0 = -1, qslot = -1;
+      if (h.firstFree[sd] < m[sd]) {
+        V0 = qslot = h.firstFree[sd];
+      } else {
+        int mid = h.firstMid[sd];
+        if (sd == 1 && tempSlot[0] >= 0) {        // against P's links including P's temporary vertex
+          int* dm = &df->firstMid[1];
+          cudaMemcpyAsync(dm, &m[1], sizeof(int), cudaMemcpyHostToDevice, s);
+          { big_first_mid_kernel<<<grid_for(m[1]), 256, 0, s>>>(c.SQ, c.SP, reg[1], m[1], cap[1], reg[0], m[0], cap[0],
+                                                                used[0], dm); note_launch(); }
+          if (!read_flags()) return ST_CUDA_ERROR;
+          mid = h.firstMid[1];
+        }
+        if (mid >= m[sd]) continue;
+        if (used[sd] >= cap[sd]) return fail(DEV_CAPACITY);
+        { big_add_temp_kernel<<<1, 1, 0, s>>>(*S[sd], reg[sd], m[sd], cap[sd], used[sd], mid); note_launch(); }
+        tempAfter[sd] = mid;
+        tempSlot[sd] = used[sd]++;
+        V0 = mid;
+        qslot = tempSlot[sd];
+      }
+      bool inside;
+      if (!winding(sd, qslot, 0, 1 - sd, sd == 1 ? tempAfter[0] : -1, sd == 1 ? tempSlot[0] : -1, inside))
+        return ST_CUDA_ERROR;
+      const int8_t st0 = inside ? E_EXIT : E_ENTRY;
+      { big_d_kernel<<<grid_for(m[sd]), 256, 0, s>>>(*S[sd], reg[sd], m[sd], V0, d); note_launch(); }
+      exclusive_scan_i32(d, dEx, m[sd], nullptr, st, c.d_err, s);
+      { big_t_kernel<<<grid_for(m[sd]), 256, 0, s>>>(*S[sd], reg[sd], m[sd], V0, dEx, t); note_launch(); }
+      exclusive_scan_i32(t, tEx, m[sd], nullptr, st, c.d_err, s);
+      { big_apply4_kernel<<<grid_for(m[sd]), 256, 0, s>>>(*S[sd], reg[sd], m[sd], V0, dEx, tEx, st0, uni ? 1 : 0); note_launch(); }
+    }
+  }
+  auto seq_tail = [&](int from_trace) {
+    { big_seq_tail_kernel<<<1, 1, 0, s>>>(c.SP, c.SQ, bp, used[0], used[1], from_trace, c.oxy, c.ocsz, nv, nc, c.prm,
+                                          c.d_err, c.status, c.outNC, c.outNV); note_launch(); }
+    return ST_OK;
+  };
+  // ---- split pairs (sequential), crossing candidates
+  { big_split_any_kernel<<<grid_for(bp.mP), 256, 0, s>>>(c.SP, c.SQ, bp, df); note_launch(); }
+  if (!read_flags()) return ST_CUDA_ERROR;
+  if (h.anySplit) return seq_tail(0);
+  { big_step6_kernel<<<grid_for(bp.mP), 256, 0, s>>>(c.SP, c.SQ, bp); note_launch(); }
+  if (used[0] != bp.mP || used[1] != bp.mQ) return seq_tail(1);
+  // ---- parallel tracing
+  uint8_t* labP = c.A.take_n<uint8_t>(bp.mP);
+  uint8_t* labQ = c.A.take_n<uint8_t>(bp.mQ);
+  int64_t* idxP = c.A.take_n<int64_t>(bp.mP);
+  int64_t* idxQ = c.A.take_n<int64_t>(bp.mQ);
+  int64_t* tots = c.A.take_n<int64_t>(4);
+  void* st = c.A.take(scan_temp_bytes(std::max(bp.mP, bp.mQ)));
+  if (!labP || !labQ || !idxP || !idxQ || !tots || !st) return ST_OUT_OF_MEMORY;
+  { big_labeled_kernel<<<grid_for(bp.mP), 256, 0, s>>>(c.SP, bp.regP, bp.mP, labP, df); note_launch(); }
+  { big_labeled_kernel<<<grid_for(bp.mQ), 256, 0, s>>>(c.SQ, bp.regQ, bp.mQ, labQ, df); note_launch(); }
+  exclusive_scan_u8(labP, idxP, bp.mP, tots + 0, st, c.d_err, s);
+  exclusive_scan_u8(labQ, idxQ, bp.mQ, tots + 1, st, c.d_err, s);
+  cudaMemcpyAsync(c.hs, tots, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (!read_flags()) return ST_CUDA_ERROR;
+  if (h.bad) return seq_tail(1);
+  const int nP = (int)c.hs[0], nQ = (int)c.hs[1], N = nP + nQ;
+  int64_t TV = 0, TC = 0;
+  if (N > 0) {
+    int32_t* listP = c.A.take_n<int32_t>(nP);
+    int32_t* listQ = c.A.take_n<int32_t>(nQ);
+    int32_t* succ = c.A.take_n<int32_t>(N);
+    int32_t* len = c.A.take_n<int32_t>(N);
+    int32_t* stop = c.A.take_n<int32_t>(N);
+    int32_t* J[2] = {c.A.take_n<int32_t>(N), c.A.take_n<int32_t>(N)};
+    int32_t* a[2] = {c.A.take_n<int32_t>(N), c.A.take_n<int32_t>(N)};
+    int32_t* b[2] = {c.A.take_n<int32_t>(N), c.A.take_n<int32_t>(N)};
+    uint8_t* isE = c.A.take_n<uint8_t>(N);
+    int32_t* Bst = c.A.take_n<int32_t>(N);
+    uint8_t* rev = c.A.take_n<uint8_t>(N);
+    int32_t* nx[2] = {c.A.take_n<int32_t>(N), c.A.take_n<int32_t>(N)};
+    int64_t* sf[2] = {c.A.take_n<int64_t>(N), c.A.take_n<int64_t>(N)};
+    int64_t* compLen = c.A.take_n<int64_t>(bp.mP);
+    uint8_t* compFlag = c.A.take_n<uint8_t>(bp.mP);
+    int64_t* compBase = c.A.take_n<int64_t>(bp.mP);
+    int64_t* compIdx = c.A.take_n<int64_t>(bp.mP);
+    if (!listP || !listQ || !succ || !len || !stop || !J[0] || !J[1] || !a[0] || !a[1] || !b[0] || !b[1] || !isE ||
+        !Bst || !rev || !nx[0] || !nx[1] || !sf[0] || !sf[1] || !compLen || !compFlag || !compBase || !compIdx)
+      return ST_OUT_OF_MEMORY;
+    { big_lab_list_kernel<<<grid_for(bp.mP), 256, 0, s>>>(labP, idxP, bp.mP, listP); note_launch(); }
+    { big_lab_list_kernel<<<grid_for(bp.mQ), 256, 0, s>>>(labQ, idxQ, bp.mQ, listQ); note_launch(); }
+    { big_runs_kernel<<<grid_for(N), 256, 0, s>>>(c.SP, c.SQ, bp, listP, listQ, idxP, idxQ, nP, nQ, uni ? 1 : 0, succ,
+                                                  len, stop, df); note_launch(); }
+    if (!read_flags()) return ST_CUDA_ERROR;
+    if (h.bad) return seq_tail(1);
+    { big_cycle_init_kernel<<<grid_for(N), 256, 0, s>>>(c.SP, c.SQ, bp, listP, listQ, nP, nQ, succ, stop, J[0], a[0],
+                                                        b[0], isE); note_launch(); }
+    int rounds = 1;
+    while ((1ll << rounds) < (int64_t)N) ++rounds;
+    int cur = 0;
+    for (int r = 0; r <= rounds; ++r) {
+      { big_cycle_min_kernel<<<grid_for(N), 256, 0, s>>>(J[cur], a[cur], b[cur], J[1 - cur], a[1 - cur], b[1 - cur],
+                                                         isE, N); note_launch(); }
+      cur = 1 - cur;
+    }
+    const int dirE = uni ? -1 : 1;   // ENTRY vertices run forwards in intersection mode
+    { big_cycle_start_kernel<<<grid_for(N), 256, 0, s>>>(a[cur], b[cur], isE, idxP, listP, nP, N, dirE, succ, len, Bst,
+                                                         rev, nx[0], sf[0]); note_launch(); }
+    int rc = 0;
+    for (int r = 0; r <= rounds; ++r) {
+      { big_rank_kernel<<<grid_for(N), 256, 0, s>>>(nx[rc], sf[rc], nx[1 - rc], sf[1 - rc], isE, N); note_launch(); }
+      rc = 1 - rc;
+    }
+    cudaMemsetAsync(compLen, 0, bp.mP * sizeof(int64_t), s);
+    cudaMemsetAsync(compFlag, 0, bp.mP, s);
+    { big_comp_len_kernel<<<grid_for(N), 256, 0, s>>>(isE, Bst, sf[rc], a[cur], b[cur], N, compLen, compFlag); note_launch(); }
+    exclusive_scan_i64(compLen, compBase, bp.mP, tots + 2, st, c.d_err, s);
+    exclusive_scan_u8(compFlag, compIdx, bp.mP, tots + 3, st, c.d_err, s);
+    cudaMemcpyAsync(c.hs, tots + 2, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return ST_CUDA_ERROR;
+    TV = c.hs[0];
+    TC = c.hs[1];
+    if (nv + TV > bp.vCap || nc + TC > bp.cCap) return fail(DEV_CAPACITY);
+    { big_write_kernel<<<(unsigned)(((int64_t)N * 32 + 255) / 256), 256, 0, s>>>(
+        c.SP, c.SQ, bp, listP, listQ, nP, N, isE, len, Bst, rev, sf[rc], a[cur], b[cur], compBase, compIdx, nv, nc,
+        uni ? 1 : 0, c.oxy + 2 * bp.vOff, c.ocsz); note_launch(); }
+  }
+  nv += TV;
+  nc += (int)TC;
+  // ---- clean-up of every component of the pair, then compaction
+  if (nc == 0) {
+    { big_set_counts_kernel<<<1, 1, 0, s>>>(c.outNC + bp.k, c.outNV + bp.k, 0, 0); note_launch(); }
+    return ST_OK;
+  }
+  int32_t* csz = c.ocsz + bp.cOff;
+  double* xy = c.oxy + 2 * bp.vOff;
+  int64_t* cstart = c.A.take_n<int64_t>(nc);
+  int32_t* kept = c.A.take_n<int32_t>(nc);
+  int64_t* kstart = c.A.take_n<int64_t>(nc);
+  uint8_t* kflag = c.A.take_n<uint8_t>(nc);
+  int64_t* cidx = c.A.take_n<int64_t>(nc);
+  double* tmp = c.A.take_n<double>(2 * nv);
+  void* st3 = c.A.take(scan_temp_bytes(nc));
+  if (!cstart || !kept || !kstart || !kflag || !cidx || !tmp || !st3) return ST_OUT_OF_MEMORY;
+  exclusive_scan_i32(csz, cstart, nc, nullptr, st3, c.d_err, s);
+  { big_cleanup_kernel<<<(unsigned)(((int64_t)nc * 32 + 255) / 256), 256, 0, s>>>(xy, csz, cstart, nc, c.prm.eps_clean,
+                                                                                  kept); note_launch(); }
+  exclusive_scan_i32(kept, kstart, nc, tots + 0, st3, c.d_err, s);
+  { big_kflag_kernel<<<grid_for(nc), 256, 0, s>>>(kept, nc, kflag); note_launch(); }
+  exclusive_scan_u8(kflag, cidx, nc, tots + 1, st3, c.d_err, s);
+  { big_compact_kernel<<<(unsigned)(((int64_t)nc * 32 + 255) / 256), 256, 0, s>>>(xy, cstart, kept, kstart, nc, tmp); note_launch(); }
+  cudaMemcpyAsync(c.hs, tots, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (!sync()) return ST_CUDA_ERROR;
+  const int64_t KV = c.hs[0];
+  const int KC = (int)c.hs[1];
+  cudaMemcpyAsync(xy, tmp, 2 * KV * sizeof(double), cudaMemcpyDeviceToDevice, s);
+  { big_finish_kernel<<<grid_for(nc), 256, 0, s>>>(kept, cidx, nc, csz); note_launch(); }
+  { big_set_counts_kernel<<<1, 1, 0, s>>>(c.outNC + bp.k, c.outNV + bp.k, KC, KV); note_launch(); }
+  return ST_OK;
 }
 
 // ---------------------------------------------------------------- G8 compaction
@@ -1433,12 +2354,18 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   exclusive_scan_i32(cQ, offQ, K, tot + 1, stK, d_err, s);
   exclusive_scan_i32(D.nP, eoffP, K, tot + 2, stK, d_err, s);
   exclusive_scan_i32(D.nQ, eoffQ, K, tot + 3, stK, d_err, s);
-  { chunk_count_kernel<<<blocks_for(K), kThreads, 0, s>>>(cP, cQ, K, nchunk); note_launch(); }
+  int64_t* bigList = A.take_n<int64_t>(K);
+  unsigned long long* nBig = A.take_n<unsigned long long>(1);
+  if (!bigList || !nBig) return ST_OUT_OF_MEMORY;
+  cudaMemsetAsync(nBig, 0, sizeof(unsigned long long), s);
+  { chunk_count_kernel<<<blocks_for(K), kThreads, 0, s>>>(cP, cQ, K, nchunk, bigList, nBig, prm.bin_grid); note_launch(); }
   exclusive_scan_i64(nchunk, chunkOff, K, tot + 4, stK, d_err, s);
   mk->mark("clip:setup+filter", s);
   cudaMemcpyAsync(hs, tot, 5 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hs + 5, nBig, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
   const int64_t nLP = hs[0], nLQ = hs[1], nEP = hs[2], nEQ = hs[3], nCh = hs[4];
+  const int nBigPairs = (int)hs[5];
   int32_t* LP = A.take_n<int32_t>(nLP);
   int32_t* LQ = A.take_n<int32_t>(nLQ);
   int32_t* chunkRec = A.take_n<int32_t>(nCh);
@@ -1446,23 +2373,87 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int64_t* recScan = A.take_n<int64_t>(nCh);
   int64_t* qScan = A.take_n<int64_t>(nCh);
   void* stC = A.take(scan_temp_bytes(std::max<int64_t>(nCh, 1)));
-  if (!LP || !LQ || !chunkRec || !chunkQ || !recScan || !qScan || !stC) return ST_OUT_OF_MEMORY;
+  int64_t* binRec = A.take_n<int64_t>(K);
+  int64_t* binQ = A.take_n<int64_t>(K);
+  if (!LP || !LQ || !chunkRec || !chunkQ || !recScan || !qScan || !stC || !binRec || !binQ) return ST_OUT_OF_MEMORY;
+  cudaMemsetAsync(binRec, 0, K * sizeof(int64_t), s);
+  cudaMemsetAsync(binQ, 0, K * sizeof(int64_t), s);
   { edge_filter_kernel<1><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ); note_launch(); }
-  // ---- G2 count
+  // ---- G2 count: chunked pairs
   Records R{};
   if (nCh > 0) {
     { intersect_kernel<0><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, chunkRec, chunkQ, nullptr, R); note_launch(); }
-    exclusive_scan_i32(chunkRec, recScan, nCh, tot + 5, stC, d_err, s);
-    exclusive_scan_i32(chunkQ, qScan, nCh, tot + 6, stC, d_err, s);
-  } else {
-    cudaMemsetAsync(tot + 5, 0, 2 * sizeof(int64_t), s);
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, chunkRec, chunkQ, nullptr, nullptr, R); note_launch(); }
+    exclusive_scan_i32(chunkRec, recScan, nCh, nullptr, stC, d_err, s);
+    exclusive_scan_i32(chunkQ, qScan, nCh, nullptr, stC, d_err, s);
   }
+  // ---- G2 count: binned pairs (host loop; few pairs)
+  struct BigWork { BigInfo info; BinGrid G; int64_t* cellOff; int32_t* cellList; int64_t* recPos; };
+  std::vector<BigWork> bigs(nBigPairs);
+  if (nBigPairs > 0) {
+    BigInfo* dInfo = A.take_n<BigInfo>(nBigPairs);
+    if (!dInfo) return ST_OUT_OF_MEMORY;
+    { big_info_kernel<<<blocks_for(nBigPairs), kThreads, 0, s>>>(bigList, nBigPairs, cP, cQ, offP, offQ, D, dInfo); note_launch(); }
+    std::vector<BigInfo> hInfo(nBigPairs);
+    cudaMemcpyAsync(hInfo.data(), dInfo, nBigPairs * sizeof(BigInfo), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return ST_CUDA_ERROR;
+    std::sort(hInfo.begin(), hInfo.end(), [](const BigInfo& x, const BigInfo& y) { return x.k < y.k; });
+    int64_t* d_t = A.take_n<int64_t>(2);
+    unsigned long long* d_q = A.take_n<unsigned long long>(1);
+    if (!d_t || !d_q) return ST_OUT_OF_MEMORY;
+    for (int bi = 0; bi < nBigPairs; ++bi) {
+      BigWork& W = bigs[bi];
+      W.info = hInfo[bi];
+      const double w = W.info.cmbr[2] - W.info.cmbr[0], h = W.info.cmbr[3] - W.info.cmbr[1];
+      const double target = (double)std::max(1, W.info.cq);
+      int gx = 1, gy = 1;
+      if (w > 0 && h > 0) {
+        gx = (int)std::ceil(std::sqrt(target * w / h));
+        gx = std::min(std::max(gx, 1), 1 << 12);
+        gy = (int)std::ceil(target / gx);
+        gy = std::min(std::max(gy, 1), 1 << 12);
+      } else if (w > 0) {
+        gx = (int)std::min(target, 4096.0);
+      } else if (h > 0) {
+        gy = (int)std::min(target, 4096.0);
+      }
+      W.G = BinGrid{W.info.cmbr[0], W.info.cmbr[1], w > 0 ? w / gx : 1.0, h > 0 ? h / gy : 1.0, gx, gy};
+      const int64_t ncell = (int64_t)gx * gy;
+      int32_t* cellCnt = A.take_n<int32_t>(ncell + 1);
+      W.cellOff = A.take_n<int64_t>(ncell + 1);
+      int32_t* cursor = A.take_n<int32_t>(ncell);
+      void* st = A.take(scan_temp_bytes(ncell + 1));
+      int32_t* recCnt = A.take_n<int32_t>(W.info.cp);
+      W.recPos = A.take_n<int64_t>(W.info.cp);
+      void* st2 = A.take(scan_temp_bytes(std::max(W.info.cp, 1)));
+      if (!cellCnt || !W.cellOff || !cursor || !st || !recCnt || !W.recPos || !st2) return ST_OUT_OF_MEMORY;
+      cudaMemsetAsync(cellCnt, 0, (ncell + 1) * sizeof(int32_t), s);
+      cudaMemsetAsync(cursor, 0, ncell * sizeof(int32_t), s);
+      const int64_t k = W.info.k;
+      { bin_count_kernel<<<blocks_for(W.info.cq), kThreads, 0, s>>>(Lb, Lo, D, k, LQ + W.info.offQ, W.info.cq, W.G,
+                                                                    cellCnt); note_launch(); }
+      exclusive_scan_i32(cellCnt, W.cellOff, ncell + 1, d_t, st, d_err, s);
+      cudaMemcpyAsync(hs, d_t, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+      if (!sync()) return ST_CUDA_ERROR;
+      W.cellList = A.take_n<int32_t>(hs[0]);
+      if (!W.cellList) return ST_OUT_OF_MEMORY;
+      { bin_fill_kernel<<<blocks_for(W.info.cq), kThreads, 0, s>>>(Lb, Lo, D, k, LQ + W.info.offQ, W.info.cq, W.G,
+                                                                   W.cellOff, cursor, W.cellList); note_launch(); }
+      cudaMemsetAsync(d_q, 0, sizeof(unsigned long long), s);
+      { bin_pairs_kernel<0><<<blocks_for(W.info.cp), kThreads, 0, s>>>(Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G,
+                                                                       W.cellOff, W.cellList, prm.eps, recCnt, d_q,
+                                                                       nullptr, R); note_launch(); }
+      exclusive_scan_i32(recCnt, W.recPos, W.info.cp, d_t + 1, st2, d_err, s);
+      { bin_total_kernel<<<1, 1, 0, s>>>(d_t + 1, d_q, k, binRec, binQ); note_launch(); }
+    }
+  }
+  int64_t* nrec64 = A.take_n<int64_t>(K);
   int64_t* recOff = A.take_n<int64_t>(K);
   int32_t* nrec = A.take_n<int32_t>(K);
-  if (!recOff || !nrec) return ST_OUT_OF_MEMORY;
+  if (!nrec64 || !recOff || !nrec) return ST_OUT_OF_MEMORY;
   { pair_records_kernel<<<blocks_for(K), kThreads, 0, s>>>(chunkOff, nchunk, recScan, qScan, chunkRec, chunkQ,
-                                                         K, recOff, nrec, C.count1, D); note_launch(); }
+                                                         binRec, binQ, K, nrec64, nrec, C.count1, D); note_launch(); }
+  exclusive_scan_i64(nrec64, recOff, K, tot + 5, stK, d_err, s);
   mk->mark("clip:count", s);
   cudaMemcpyAsync(hs, tot + 5, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
@@ -1474,7 +2465,14 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (!R.p || !R.q || !R.a || !R.b || !R.t || !R.k) return ST_OUT_OF_MEMORY;
   if (nCh > 0)
     { intersect_kernel<1><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, R); note_launch(); }
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, recOff, R); note_launch(); }
+  for (auto& W : bigs) {
+    const int64_t k = W.info.k;
+    { add_offset_kernel<<<blocks_for(W.info.cp), kThreads, 0, s>>>(W.recPos, W.info.cp, recOff + k); note_launch(); }
+    { bin_pairs_kernel<1><<<blocks_for(W.info.cp), kThreads, 0, s>>>(Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G,
+                                                                     W.cellOff, W.cellList, prm.eps, nullptr, nullptr,
+                                                                     W.recPos, R); note_launch(); }
+  }
   mk->mark("clip:emit", s);
   // ---- G4 ring layout
   int32_t* insP = A.take_n<int32_t>(nEP);
@@ -1607,7 +2605,34 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   mk->mark("clip:fill+link", s);
   { label_trace_kernel<<<(unsigned)((K + 3) / 4), 128, 0, s>>>(D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ,
                                                                   SP, SQ, oxy, vOff, vcap, ocsz, cOff, ccap, nc,
-                                                                  nv, prm, d_err); note_launch(); }
+                                                                  nv, prm, d_err, prm.big_label_min); note_launch(); }
+  // ---- G7 grid path for huge pairs
+  {
+    int64_t* blist = A.take_n<int64_t>(K);
+    unsigned long long* nbl = A.take_n<unsigned long long>(1);
+    BigFlags* dflags = A.take_n<BigFlags>(1);
+    if (!blist || !nbl || !dflags) return ST_OUT_OF_MEMORY;
+    cudaMemsetAsync(nbl, 0, sizeof(unsigned long long), s);
+    { big_label_list_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, D.status, K, prm.big_label_min, blist, nbl); note_launch(); }
+    cudaMemcpyAsync(hs, nbl, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return ST_CUDA_ERROR;
+    const int nbig = (int)hs[0];
+    if (nbig > 0) {
+      BigPair* dbp = A.take_n<BigPair>(nbig);
+      if (!dbp) return ST_OUT_OF_MEMORY;
+      { big_info_label_kernel<<<blocks_for(nbig), kThreads, 0, s>>>(blist, nbig, regP, regQ, mP, mQ, regSizeP, regSizeQ,
+                                                                    vOff, vcap, cOff, ccap, dbp); note_launch(); }
+      std::vector<BigPair> hbp(nbig);
+      cudaMemcpyAsync(hbp.data(), dbp, nbig * sizeof(BigPair), cudaMemcpyDeviceToHost, s);
+      if (!sync()) return ST_CUDA_ERROR;
+      std::sort(hbp.begin(), hbp.end(), [](const BigPair& x, const BigPair& y) { return x.k < y.k; });
+      BigCtx bc{A, s, hs, d_err, SP, SQ, oxy, ocsz, D.status, nc, nv, prm};
+      for (const BigPair& bp : hbp) {
+        int st = run_big_label_pair(bc, bp, dflags);
+        if (st != ST_OK) return st;
+      }
+    }
+  }
   mk->mark("clip:label+trace", s);
   // ---- G8 compaction
   C.ncomp = nc;

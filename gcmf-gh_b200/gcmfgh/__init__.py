@@ -94,6 +94,7 @@ def lib():
         L.gcmfgh_radix_sort_u64.argtypes = [vp, vp, vp, i64, ctypes.c_int]
         L.gcmfgh_launch_count.argtypes = []
         L.gcmfgh_launch_count.restype = ctypes.c_ulonglong
+        L.gcmfgh_set_tuning.argtypes = [vp, ctypes.c_int, i64]
         L.gcmfgh_set_timing.argtypes = [vp, ctypes.c_int]
         L.gcmfgh_get_timing.argtypes = [vp, ctypes.c_int, P(ctypes.c_float), P(ctypes.c_char_p),
                                         ctypes.c_int]
@@ -180,6 +181,13 @@ class Engine:
 
     def last_device_error(self):
         return lib().gcmfgh_last_device_error(self.h)
+
+    def set_tuning(self, bin_grid=None, big_label=None):
+        """Work-distribution thresholds (results do not depend on them)."""
+        if bin_grid is not None:
+            _check(lib().gcmfgh_set_tuning(self.h, 0, int(bin_grid)))
+        if big_label is not None:
+            _check(lib().gcmfgh_set_tuning(self.h, 1, int(big_label)))
 
     def set_timing(self, on=True):
         _check(lib().gcmfgh_set_timing(self.h, 1 if on else 0))

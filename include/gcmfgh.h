@@ -114,6 +114,14 @@ gcmfgh_status gcmfgh_set_stream(gcmfgh_ctx* ctx, void* stream);
  * build); union_mode: polyclip.h:42 UNION. */
 gcmfgh_status gcmfgh_set_params(gcmfgh_ctx* ctx, double eps, double eps_clean, int union_mode);
 const char* gcmfgh_status_string(gcmfgh_status s);
+/* Work-distribution thresholds of the clip (results do not depend on them):
+ * GCMFGH_TUNE_BIN_GRID: a pair whose common-MBR edge grid exceeds this many edge pairs
+ * has its edges binned on a uniform grid instead of enumerated (default 2^24);
+ * GCMFGH_TUNE_BIG_LABEL: a pair whose merged rings exceed this many vertices is labelled
+ * and traced by grid-wide kernels instead of one warp (default 2^18). */
+#define GCMFGH_TUNE_BIN_GRID 0
+#define GCMFGH_TUNE_BIG_LABEL 1
+gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* ctx, int key, int64_t value);
 /* device error word of the last call (0 none, 1 capacity, 2 trace budget, 4 wait limit) */
 int gcmfgh_last_device_error(gcmfgh_ctx* ctx);
 /* Stage timing, replacing the reference's StartTimer/StopTimer pairs around each stage

@@ -293,9 +293,74 @@ struct Clipper {
       for (int i = 0; i < nP; ++i) cmP[i] = edgeTouchesBox(ptP(i), ptP((i + 1) % nP), cmbr);
       for (int j = 0; j < nQ; ++j) cmQ[j] = edgeTouchesBox(ptQ(j), ptQ((j + 1) % nQ), cmbr);
     }
+    // With the box filter on, only Q edges whose boxes can touch P's edge box matter; for
+    // large pairs they are found through a uniform grid of Q-edge boxes (the same set as
+    // testing every j, visited in ascending j).
+    const bool gridded = filters && (double)nP * nQ > 4e6;
+    int gx = 1, gy = 1;
+    double gx0 = cmbr[0], gy0 = cmbr[1], gcw = 1, gch = 1;
+    std::vector<int> cellStart, cellItems;
+    auto cellOf = [](double v, double v0, double cs, int g) {
+      double t = (v - v0) / cs;
+      if (!(t > 0)) return 0;
+      if (t >= g) return g - 1;
+      return (int)t;
+    };
+    if (gridded) {
+      double w = cmbr[2] - cmbr[0], h = cmbr[3] - cmbr[1];
+      int target = std::max(1, nQ);
+      if (w > 0 && h > 0) {
+        gx = std::min(4096, std::max(1, (int)std::ceil(std::sqrt(target * w / h))));
+        gy = std::min(4096, std::max(1, (int)std::ceil((double)target / gx)));
+      }
+      gcw = w > 0 ? w / gx : 1;
+      gch = h > 0 ? h / gy : 1;
+      std::vector<int> cnt((size_t)gx * gy + 1, 0);
+      auto span = [&](int j, int& x0, int& x1, int& y0, int& y1) {
+        Pt a = ptQ(j), b = ptQ((j + 1) % nQ);
+        x0 = cellOf(std::min(a.x, b.x), gx0, gcw, gx); x1 = cellOf(std::max(a.x, b.x), gx0, gcw, gx);
+        y0 = cellOf(std::min(a.y, b.y), gy0, gch, gy); y1 = cellOf(std::max(a.y, b.y), gy0, gch, gy);
+      };
+      for (int j = 0; j < nQ; ++j) {
+        if (!cmQ[j]) continue;
+        int x0, x1, y0, y1;
+        span(j, x0, x1, y0, y1);
+        for (int y = y0; y <= y1; ++y)
+          for (int x = x0; x <= x1; ++x) cnt[(size_t)y * gx + x]++;
+      }
+      cellStart.assign(cnt.size(), 0);
+      for (size_t c = 1; c < cnt.size(); ++c) cellStart[c] = cellStart[c - 1] + cnt[c - 1];
+      cellItems.assign(cellStart.back(), 0);
+      std::vector<int> cur(cellStart.begin(), cellStart.end() - 1);
+      for (int j = 0; j < nQ; ++j) {
+        if (!cmQ[j]) continue;
+        int x0, x1, y0, y1;
+        span(j, x0, x1, y0, y1);
+        for (int y = y0; y <= y1; ++y)
+          for (int x = x0; x <= x1; ++x) cellItems[cur[(size_t)y * gx + x]++] = j;
+      }
+    }
+    std::vector<int> qcand;
     for (int i = 0; i < nP; ++i) {
       Pt P1 = ptP(i), P2 = ptP((i + 1) % nP);
-      for (int j = 0; j < nQ; ++j) {
+      int ncand = nQ;
+      if (gridded) {
+        qcand.clear();
+        if (cmP[i]) {
+          int x0 = cellOf(std::min(P1.x, P2.x), gx0, gcw, gx), x1 = cellOf(std::max(P1.x, P2.x), gx0, gcw, gx);
+          int y0 = cellOf(std::min(P1.y, P2.y), gy0, gch, gy), y1 = cellOf(std::max(P1.y, P2.y), gy0, gch, gy);
+          for (int y = y0; y <= y1; ++y)
+            for (int x = x0; x <= x1; ++x) {
+              size_t c = (size_t)y * gx + x;
+              qcand.insert(qcand.end(), cellItems.begin() + cellStart[c], cellItems.begin() + cellStart[c + 1]);
+            }
+          std::sort(qcand.begin(), qcand.end());
+          qcand.erase(std::unique(qcand.begin(), qcand.end()), qcand.end());
+        }
+        ncand = (int)qcand.size();
+      }
+      for (int jj = 0; jj < ncand; ++jj) {
+        const int j = gridded ? qcand[jj] : jj;
         Pt Q1 = ptQ(j), Q2 = ptQ((j + 1) % nQ);
         double a = 0, b = 0;
         if (filters) {
