@@ -308,6 +308,12 @@ gcmfgh_status gcmfgh_set_params(gcmfgh_ctx* c, double eps, double eps_clean, int
   return GCMFGH_OK;
 }
 
+gcmfgh_status gcmfgh_set_precision(gcmfgh_ctx* c, int mode) {
+  if (!c || (mode != GCMFGH_PRECISION_REFERENCE && mode != GCMFGH_PRECISION_EXACT)) return GCMFGH_INVALID_ARGUMENT;
+  c->prm.exact = mode == GCMFGH_PRECISION_EXACT;
+  return GCMFGH_OK;
+}
+
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* c, int key, int64_t value) {
   if (!c || value < 0) return GCMFGH_INVALID_ARGUMENT;
   if (key == GCMFGH_TUNE_BIN_GRID) c->prm.bin_grid = value;

@@ -79,6 +79,160 @@ GCMFGH_DEV int classify_edges(double p1x, double p1y, double p2x, double p2y,
   return 0;
 }
 
+// ---- exact-predicate mode
+//
+// Signs of u.v-type expressions  (a1 - a0) * (b1 - b0) -/+ (c1 - c0) * (d1 - d0)  over
+// FP64 inputs, exact for every input (no underflow/overflow assumed).  Method: Shewchuk,
+// "Adaptive Precision Floating-Point Arithmetic and Fast Robust Geometric Predicates"
+// (1997): a forward error bound decides the sign from the plain FP64 value whenever it
+// can (stage A of orient2d, bound (3 + 16 e) e (|left| + |right|), e = 2^-53); otherwise
+// every difference is split exactly into two doubles (Two-Diff), every partial product
+// into two (Two-Product, formed here with a fused multiply-add), and the sixteen doubles
+// are summed into a nonoverlapping expansion (Grow-Expansion), whose largest nonzero
+// component carries the sign.
+
+GCMFGH_DEV void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  double bv = s - a;
+  double av = s - bv;
+  e = (a - av) + (b - bv);
+}
+
+GCMFGH_DEV void two_prod(double a, double b, double& p, double& e) {
+  p = a * b;
+  e = fma(a, b, -p);
+}
+
+static __device__ __noinline__ int exact_sign_slow(double a1, double a0, double b1, double b0, double c1, double c0,
+                                            double d1, double d0, int sub) {
+  double ah, al, bh, bl, ch, cl, dh, dl;
+  two_sum(a1, -a0, ah, al);
+  two_sum(b1, -b0, bh, bl);
+  two_sum(c1, -c0, ch, cl);
+  two_sum(d1, -d0, dh, dl);
+  const double sgn = sub ? -1.0 : 1.0;
+  const double fx[4] = {ah, ah, al, al}, fy[4] = {bh, bl, bh, bl};
+  const double gx[4] = {ch, ch, cl, cl}, gy[4] = {dh, dl, dh, dl};
+  double h[16];
+  int n = 0;
+  for (int t = 0; t < 8; ++t) {
+    double p, e;
+    if (t < 4) two_prod(fx[t], fy[t], p, e);
+    else { two_prod(gx[t - 4], gy[t - 4], p, e); p *= sgn; e *= sgn; }
+    const double parts[2] = {e, p};
+    for (int u = 0; u < 2; ++u) {
+      double q = parts[u];
+      for (int i = 0; i < n; ++i) {
+        double s, r;
+        two_sum(q, h[i], s, r);
+        h[i] = r;
+        q = s;
+      }
+      h[n++] = q;
+    }
+  }
+  for (int i = n - 1; i >= 0; --i)
+    if (h[i] != 0.0) return h[i] > 0.0 ? 1 : -1;
+  return 0;
+}
+
+// sign of (a1-a0)(b1-b0) - (c1-c0)(d1-d0)  (sub = 1)  or  ... + ...  (sub = 0)
+GCMFGH_DEV int exact_sign(double a1, double a0, double b1, double b0, double c1, double c0,
+                          double d1, double d0, int sub) {
+  const double left = (a1 - a0) * (b1 - b0);
+  const double right = (c1 - c0) * (d1 - d0);
+  const double r = sub ? right : -right;          // value = left - r
+  const double det = left - r;
+  if (left > 0.0) { if (r <= 0.0) return 1; }
+  else if (left < 0.0) { if (r >= 0.0) return -1; }
+  else return (r > 0.0) ? -1 : (r < 0.0 ? 1 : 0);
+  const double bound = 3.3306690738754716e-16 * (fabs(left) + fabs(r));   // (3 + 16e) e, e = 2^-53
+  if (det >= bound || -det >= bound) return det > 0.0 ? 1 : -1;
+  return exact_sign_slow(a1, a0, b1, b0, c1, c0, d1, d0, sub);
+}
+
+// exact sign of area2(P, Q, R) = (qx - px)(ry - py) - (qy - py)(rx - px)
+GCMFGH_DEV int orient_exact(double px, double py, double qx, double qy, double rx, double ry) {
+  return exact_sign(qx, px, ry, py, qy, py, rx, px, 1);
+}
+
+// sign of area2 in the selected mode: the FP64 value's sign, or the exact sign
+GCMFGH_DEV int orient_sign(int exact, double px, double py, double qx, double qy, double rx, double ry) {
+  if (exact) return orient_exact(px, py, qx, qy, rx, ry);
+  const double v = area2(px, py, qx, qy, rx, ry);
+  return (v > 0.0) - (v < 0.0);
+}
+
+// exact sign of (U1 - U0) . (V1 - V0)
+GCMFGH_DEV int dot_exact(double u1x, double u1y, double u0x, double u0y, double v1x, double v1y, double v0x,
+                         double v0y) {
+  return exact_sign(u1x, u0x, v1x, v0x, u1y, u0y, v1y, v0y, 0);
+}
+
+// FP64 parameter alpha = A1 / (A1 - A2) of a crossing whose exact signs are known to
+// straddle: kept in [0, 1] when rounding of A1, A2 says otherwise.
+GCMFGH_DEV double crossing_param(double A1, double A2) {
+  double t = A1 / (A1 - A2);
+  if (!(t >= 0.0)) t = 0.0;
+  if (t > 1.0) t = 1.0;
+  return t;
+}
+
+// Edge classification with exact predicates (same nine types as classify_edges).
+// Non-collinear edges: alpha in (0,1) iff P1, P2 lie strictly on opposite sides of line
+// Q; alpha == 0 iff P1 lies on it; likewise beta with Q1, Q2 and line P.  Collinear
+// edges: the order of Q1 along P and of P1 along Q from exact dot-product signs;
+// "b0" is Q1 == P1, which is what the tolerance rule reduces to without tolerance.
+// alpha/beta values are the FP64 expressions of the reference, clamped to [0, 1].
+GCMFGH_DEV int classify_exact(double p1x, double p1y, double p2x, double p2y,
+                              double q1x, double q1y, double q2x, double q2y,
+                              double& alpha, double& beta) {
+  const int s1 = orient_exact(p1x, p1y, q1x, q1y, q2x, q2y);
+  const int s2 = orient_exact(p2x, p2y, q1x, q1y, q2x, q2y);
+  if (s1 != 0 || s2 != 0) {
+    if (s1 == s2) return 0;
+    const int t1 = orient_exact(q1x, q1y, p1x, p1y, p2x, p2y);
+    const int t2 = orient_exact(q2x, q2y, p1x, p1y, p2x, p2y);
+    const bool a01 = s1 * s2 < 0, a0 = s1 == 0;
+    const bool b01 = t1 * t2 < 0, b0 = t1 == 0;
+    if (!((a01 || a0) && (b01 || b0))) return 0;
+    const double AP1 = area2(p1x, p1y, q1x, q1y, q2x, q2y), AP2 = area2(p2x, p2y, q1x, q1y, q2x, q2y);
+    const double AQ1 = area2(q1x, q1y, p1x, p1y, p2x, p2y), AQ2 = area2(q2x, q2y, p1x, p1y, p2x, p2y);
+    alpha = a0 ? 0.0 : crossing_param(AP1, AP2);
+    beta = b0 ? 0.0 : crossing_param(AQ1, AQ2);
+    if (a01 && b01) return 1;
+    if (a0 && b01) return 2;
+    if (b0 && a01) return 3;
+    return 4;
+  }
+  const bool same = (p1x == q1x && p1y == q1y);
+  const bool a01 = dot_exact(q1x, q1y, p1x, p1y, p2x, p2y, p1x, p1y) > 0 &&
+                   dot_exact(p2x, p2y, q1x, q1y, p2x, p2y, p1x, p1y) > 0;
+  const bool b01 = dot_exact(p1x, p1y, q1x, q1y, q2x, q2y, q1x, q1y) > 0 &&
+                   dot_exact(q2x, q2y, p1x, p1y, q2x, q2y, q1x, q1y) > 0;
+  const bool a0 = !a01 && same, an = !a01 && !a0;
+  const bool b0 = !b01 && same, bn = !b01 && !b0;
+  const int tp = (a01 && b01) ? 5 : (an && b01) ? 6 : (bn && a01) ? 7 : (a0 && b0) ? 8 : 0;
+  if (tp) {
+    double dPx = p2x - p1x, dPy = p2y - p1y;
+    double dQx = q2x - q1x, dQy = q2y - q1y;
+    double PQx = q1x - p1x, PQy = q1y - p1y;
+    alpha = (PQx * dPx + PQy * dPy) / (dPx * dPx + dPy * dPy);
+    beta = -(PQx * dQx + PQy * dQy) / (dQx * dQx + dQy * dQy);
+    if (a01) alpha = fmin(fmax(alpha, 0.0), 1.0);
+    if (b01) beta = fmin(fmax(beta, 0.0), 1.0);
+    if (a0) alpha = 0.0;
+    if (b0) beta = 0.0;
+  }
+  return tp;
+}
+
+GCMFGH_DEV int classify_mode(int exact, double p1x, double p1y, double p2x, double p2y, double q1x,
+                             double q1y, double q2x, double q2y, double eps, double& alpha, double& beta) {
+  return exact ? classify_exact(p1x, p1y, p2x, p2y, q1x, q1y, q2x, q2y, alpha, beta)
+               : classify_edges(p1x, p1y, p2x, p2y, q1x, q1y, q2x, q2y, eps, alpha, beta);
+}
+
 // closed overlap of the two edges' boxes: gppolyclip_mDIV512.cu:345-371
 GCMFGH_DEV bool edge_boxes_touch(double p1x, double p1y, double p2x, double p2y,
                                  double q1x, double q1y, double q2x, double q2y) {

@@ -74,6 +74,7 @@ struct ClipParams {
   double eps_clean = 1e-7;    // collinear-vertex removal in the clean-up
   int union_mode = 0;         // polyclip.h:42 UNION
   int no_swap = 0;            // 1: clip base as P even when it has fewer vertices
+  int exact = 0;              // 1: exact orientation/classification signs (eps unused there)
   int64_t bin_grid = 1ll << 24;        // edge-pair grid above which a pair's edges are binned
   int64_t big_label_min = 1ll << 18;   // merged-ring slots above which a pair is labelled grid-wide
 };

@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(kThreads)
 intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* __restrict__ chunkOff,
                  int64_t nChunks, const int32_t* __restrict__ cP, const int32_t* __restrict__ cQ,
                  const int64_t* __restrict__ offP, const int64_t* __restrict__ offQ,
-                 const int32_t* __restrict__ LP, const int32_t* __restrict__ LQ, double eps,
+                 const int32_t* __restrict__ LP, const int32_t* __restrict__ LQ, double eps, int exact,
                  int32_t* __restrict__ chunkRec, int32_t* __restrict__ chunkQ,
                  const int64_t* __restrict__ chunkRecOff, const int64_t* __restrict__ recOff, Records R) {
   int64_t c = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
@@ -193,10 +193,10 @@ intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* 
       double2 P1 = __ldg(pv + pe), P2 = __ldg(pv + (pe + 1 < np_ ? pe + 1 : 0));
       double2 Q1 = __ldg(qv + qe), Q2 = __ldg(qv + (qe + 1 < nq_ ? qe + 1 : 0));
       if (edge_boxes_touch(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y)) {
-        tp = classify_edges(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
+        tp = classify_mode(exact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
         if (kMode == 0) {
           double a2, b2;
-          tq = classify_edges(Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2);
+          tq = classify_mode(exact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2);
         }
       }
     }
@@ -262,6 +262,24 @@ __global__ void bin_count_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k,
     for (int x = x0; x <= x1; ++x) atomicAdd(&cellCnt[(int64_t)y * G.gx + x], 1);
 }
 
+// sums of the Q edges' box widths and heights (sizes the grid's cells)
+__global__ void edge_extent_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LQ,
+                                   int cq, double* __restrict__ sums) {
+  int i = blockIdx.x * kThreads + threadIdx.x;
+  double w = 0, h = 0;
+  if (i < cq) {
+    const double2* qv = layer_xy(Lb, Lo, 1 - D.pSide[k]) + D.qS[k];
+    const int nq = D.nQ[k];
+    int q = LQ[i];
+    double2 a = __ldg(qv + q), b = __ldg(qv + (q + 1 < nq ? q + 1 : 0));
+    w = fabs(b.x - a.x);
+    h = fabs(b.y - a.y);
+  }
+  w = warp_sum(w);
+  h = warp_sum(h);
+  if (lane_id() == 0) { atomicAdd(sums, w); atomicAdd(sums + 1, h); }
+}
+
 __global__ void bin_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LQ,
                                 int cq, BinGrid G, const int64_t* __restrict__ cellOff, int32_t* __restrict__ cursor,
                                 int32_t* __restrict__ cellList) {
@@ -281,11 +299,12 @@ __global__ void bin_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, 
 }
 
 // mode 0: per P edge, records (P side) and the Q-side count; mode 1: write the records of
-// each P edge at its offset, then order them by Q edge.
+// each P edge at its offset (in cell order: nothing downstream depends on record order).
 template <int kMode>
 __global__ void bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LP,
                                  int cp, BinGrid G, const int64_t* __restrict__ cellOff,
-                                 const int32_t* __restrict__ cellList, double eps, int32_t* __restrict__ recCnt,
+                                 const int32_t* __restrict__ cellList, double eps, int exact,
+                                 int32_t* __restrict__ recCnt,
                                  unsigned long long* __restrict__ qTotal, const int64_t* __restrict__ recPos,
                                  Records R) {
   int i = blockIdx.x * kThreads + threadIdx.x;
@@ -312,10 +331,10 @@ __global__ void bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k,
         double cx = fmax(pminx, fmin(Q1.x, Q2.x)), cy = fmax(pminy, fmin(Q1.y, Q2.y));
         if (cell_1d(cx, G.x0, G.cw, G.gx) != x || cell_1d(cy, G.y0, G.ch, G.gy) != y) continue;
         double alpha = 0, beta = 0;
-        int tp = classify_edges(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
+        int tp = classify_mode(exact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
         if (kMode == 0) {
           double a2, b2;
-          if (classify_edges(Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2)) ++qhits;
+          if (classify_mode(exact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2)) ++qhits;
           if (tp) ++recs;
         } else if (tp) {
           int64_t r = base + recs++;
@@ -326,19 +345,6 @@ __global__ void bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k,
   if (kMode == 0) {
     recCnt[i] = recs;
     if (qhits) atomicAdd(qTotal, (unsigned long long)qhits);
-    return;
-  }
-  // order this edge's records by Q edge (insertion sort; few per edge)
-  for (int a = 1; a < recs; ++a) {
-    int64_t ra = base + a;
-    int qa = R.q[ra]; double aa = R.a[ra], ba = R.b[ra]; int8_t ta = R.t[ra];
-    int j = a - 1;
-    while (j >= 0 && R.q[base + j] > qa) {
-      int64_t rj = base + j;
-      R.q[rj + 1] = R.q[rj]; R.a[rj + 1] = R.a[rj]; R.b[rj + 1] = R.b[rj]; R.t[rj + 1] = R.t[rj];
-      --j;
-    }
-    R.q[base + j + 1] = qa; R.a[base + j + 1] = aa; R.b[base + j + 1] = ba; R.t[base + j + 1] = ta;
   }
 }
 
@@ -372,6 +378,14 @@ __global__ void big_info_kernel(const int64_t* __restrict__ bigList, int n, cons
 // ---------------------------------------------------------------- G4 ring layout
 // Per record: insertion counts per edge, and the winning (last) record for each source
 // vertex that records link (P: types 2,4,5,6,8; Q: types 3,4,5,7,8).
+// "Last record wins" in the reference's loop order (P edge outer, Q edge inner) is the
+// record with the largest other-side edge, so the winner is the maximum of
+// (other edge, record index): independent of the order records were emitted in.
+constexpr int kLinkKeyShift = 33;             // record indices below 2^33
+__device__ __forceinline__ unsigned long long link_key(int other, int64_t r) {
+  return (((unsigned long long)other << kLinkKeyShift) | (unsigned long long)r) + 1ull;
+}
+
 __global__ void record_count_kernel(Records R, int64_t nR, const int64_t* __restrict__ eoffP,
                                     const int64_t* __restrict__ eoffQ, const int32_t* __restrict__ status,
                                     int32_t* __restrict__ insP, int32_t* __restrict__ insQ,
@@ -385,9 +399,9 @@ __global__ void record_count_kernel(Records R, int64_t nR, const int64_t* __rest
   if (t == 1 || t == 3 || t == 5 || t == 7) atomicAdd(&insP[eP], 1);
   if (t == 1 || t == 2 || t == 5 || t == 6) atomicAdd(&insQ[eQ], 1);
   if (t == 2 || t == 4 || t == 5 || t == 6 || t == 8)
-    atomicMax(reinterpret_cast<unsigned long long*>(&srcLinkP[eP]), (unsigned long long)(r + 1));
+    atomicMax(reinterpret_cast<unsigned long long*>(&srcLinkP[eP]), link_key(R.q[r], r));
   if (t == 3 || t == 4 || t == 5 || t == 7 || t == 8)
-    atomicMax(reinterpret_cast<unsigned long long*>(&srcLinkQ[eQ]), (unsigned long long)(r + 1));
+    atomicMax(reinterpret_cast<unsigned long long*>(&srcLinkQ[eQ]), link_key(R.p[r], r));
 }
 
 __global__ void edge_slots_kernel(const int32_t* __restrict__ ins, int64_t nE, int32_t* __restrict__ sz) {
@@ -402,6 +416,7 @@ struct RingSet {
   int8_t* lb;       // IntersectionLabel
   int8_t* ee;       // EntryExitLabel
   uint8_t* fl;      // bit0 split candidate, bit1 crossing candidate
+  int exact;        // orientation signs exact (ClipParams::exact)
 };
 
 // per pair: ring size, region offset (ring + room for added vertices)
@@ -634,7 +649,8 @@ __global__ void link_kernel(Records R, int64_t nR, const int32_t* __restrict__ s
   const int srcP = (int)(vposP[eP] - vposP[eoffP[k]]);
   const int srcQ = (int)(vposQ[eQ] - vposQ[eoffQ[k]]);
   const int64_t bP = regP[k], bQ = regQ[k];
-  const bool winP = srcLinkP[eP] == r + 1, winQ = srcLinkQ[eQ] == r + 1;
+  const bool winP = (unsigned long long)srcLinkP[eP] == link_key(R.q[r], r);
+  const bool winQ = (unsigned long long)srcLinkQ[eQ] == link_key(R.p[r], r);
   switch (t) {
     case 1: {
       int sp = (int)slotP[r], sq = (int)slotQ[r];
@@ -681,13 +697,14 @@ struct Ring {
   int m;        // slots in the merged ring
   int used;     // slots in use (ring + added vertices)
   int cap;      // region capacity
+  int exact;    // orientation signs exact
 };
 
 __device__ __forceinline__ Ring ring_of(const RingSet& S, int64_t base, int m, int cap) {
   Ring r;
   r.x = S.x + base; r.y = S.y + base; r.nx = S.nx + base; r.pv = S.pv + base; r.nb = S.nb + base;
   r.it = S.it + base; r.lb = S.lb + base; r.ee = S.ee + base; r.fl = S.fl + base;
-  r.m = m; r.used = m; r.cap = cap;
+  r.m = m; r.used = m; r.cap = cap; r.exact = S.exact;
   return r;
 }
 
@@ -716,9 +733,9 @@ __device__ bool point_in_ring(const Ring& R, double Rx, double Ry, int skip) {
     if ((P0y < Ry) != (P1y < Ry)) {
       if (P0x >= Rx) {
         if (P1x > Rx) w = w + 2 * (P1y > P0y) - 1;
-        else if ((area2(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
+        else if ((orient_sign(R.exact, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
       } else if (P1x > Rx) {
-        if ((area2(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
+        if ((orient_sign(R.exact, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
       }
     }
     one = two;
@@ -730,9 +747,10 @@ __device__ bool point_in_ring(const Ring& R, double Rx, double Ry, int skip) {
 __device__ int rel_position(const Ring& P, const Ring& Q, int qv, int p1, int p2, int p3) {
   if (P.it[p1] && P.nb[p1] == qv) return R_IS_P_M;
   if (P.it[p3] && P.nb[p3] == qv) return R_IS_P_P;
-  double s1 = area2(Q.x[qv], Q.y[qv], P.x[p1], P.y[p1], P.x[p2], P.y[p2]);
-  double s2 = area2(Q.x[qv], Q.y[qv], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
-  double s3 = area2(P.x[p1], P.y[p1], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+  const int ex = P.exact;
+  int s1 = orient_sign(ex, Q.x[qv], Q.y[qv], P.x[p1], P.y[p1], P.x[p2], P.y[p2]);
+  int s2 = orient_sign(ex, Q.x[qv], Q.y[qv], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+  int s3 = orient_sign(ex, P.x[p1], P.y[p1], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
   if (s3 > 0) return (s1 > 0 && s2 > 0) ? R_LEFT : R_RIGHT;
   return (s1 < 0 && s2 < 0) ? R_RIGHT : R_LEFT;
 }
@@ -942,9 +960,16 @@ __device__ bool seq_step5(PairCtx& c) {
     int vp = add_vertex(P, P.x[ip], P.y[ip]);
     int vq = add_vertex(Q, Q.x[iq], Q.y[iq]);
     if (vp < 0 || vq < 0) { fail(c, DEV_CAPACITY); return false; }
-    double sP = area2(P.x[P.pv[ip]], P.y[P.pv[ip]], P.x[ip], P.y[ip], P.x[P.nx[ip]], P.y[P.nx[ip]]);
-    double sQ = area2(Q.x[Q.pv[iq]], Q.y[Q.pv[iq]], Q.x[iq], Q.y[iq], Q.x[Q.nx[iq]], Q.y[Q.nx[iq]]);
-    if (sP * sQ > 0) {
+    bool same;
+    if (P.exact) {
+      same = orient_exact(P.x[P.pv[ip]], P.y[P.pv[ip]], P.x[ip], P.y[ip], P.x[P.nx[ip]], P.y[P.nx[ip]]) *
+             orient_exact(Q.x[Q.pv[iq]], Q.y[Q.pv[iq]], Q.x[iq], Q.y[iq], Q.x[Q.nx[iq]], Q.y[Q.nx[iq]]) > 0;
+    } else {
+      double sP = area2(P.x[P.pv[ip]], P.y[P.pv[ip]], P.x[ip], P.y[ip], P.x[P.nx[ip]], P.y[P.nx[ip]]);
+      double sQ = area2(Q.x[Q.pv[iq]], Q.y[Q.pv[iq]], Q.x[iq], Q.y[iq], Q.x[Q.nx[iq]], Q.y[Q.nx[iq]]);
+      same = sP * sQ > 0;
+    }
+    if (same) {
       P.nb[ip] = vq; Q.nb[vq] = ip; P.it[ip] = 1; Q.it[vq] = 1;
       Q.nb[iq] = vp; P.nb[vp] = iq; Q.it[iq] = 1; P.it[vp] = 1;
     } else {
@@ -1074,14 +1099,15 @@ __device__ void seq_pair_from(PairCtx& c, int step, int32_t* outNC, int64_t* out
 constexpr unsigned kFull = 0xffffffffu;
 
 // winding increment of edge (P0,P1) for point R: polygon.h:433-444
-__device__ __forceinline__ int wind(double P0x, double P0y, double P1x, double P1y, double Rx, double Ry) {
+__device__ __forceinline__ int wind(double P0x, double P0y, double P1x, double P1y, double Rx, double Ry,
+                                    int ex) {
   if ((P0y < Ry) == (P1y < Ry)) return 0;
   int d = 2 * (P1y > P0y) - 1;
   if (P0x >= Rx) {
     if (P1x > Rx) return d;
-    return ((area2(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) ? d : 0;
+    return ((orient_sign(ex, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) ? d : 0;
   }
-  if (P1x > Rx) return ((area2(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) ? d : 0;
+  if (P1x > Rx) return ((orient_sign(ex, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) ? d : 0;
   return 0;
 }
 
@@ -1092,10 +1118,10 @@ __device__ bool warp_point_in_ring(const Ring& B, double Rx, double Ry, int afte
   for (int s = lane_id(); s < B.m; s += 32) {
     int n = (s + 1 < B.m) ? s + 1 : 0;
     if (s == after) {
-      w += wind(B.x[s], B.y[s], B.x[T], B.y[T], Rx, Ry);
-      w += wind(B.x[T], B.y[T], B.x[n], B.y[n], Rx, Ry);
+      w += wind(B.x[s], B.y[s], B.x[T], B.y[T], Rx, Ry, B.exact);
+      w += wind(B.x[T], B.y[T], B.x[n], B.y[n], Rx, Ry, B.exact);
     } else {
-      w += wind(B.x[s], B.y[s], B.x[n], B.y[n], Rx, Ry);
+      w += wind(B.x[s], B.y[s], B.x[n], B.y[n], Rx, Ry, B.exact);
     }
   }
   w = warp_sum(w);
@@ -1648,10 +1674,10 @@ __global__ void big_wind_kernel(RingSet SA, int64_t regA, int mA, int v, int mod
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < mB; s += gridDim.x * blockDim.x) {
     int n = nxt_slot(s, mB);
     if (s == after) {
-      w += wind(bx[s], by[s], bx[T], by[T], Rx, Ry);
-      w += wind(bx[T], by[T], bx[n], by[n], Rx, Ry);
+      w += wind(bx[s], by[s], bx[T], by[T], Rx, Ry, SB.exact);
+      w += wind(bx[T], by[T], bx[n], by[n], Rx, Ry, SB.exact);
     } else {
-      w += wind(bx[s], by[s], bx[n], by[n], Rx, Ry);
+      w += wind(bx[s], by[s], bx[n], by[n], Rx, Ry, SB.exact);
     }
   }
   w = warp_sum(w);
@@ -2383,7 +2409,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   Records R{};
   if (nCh > 0) {
     { intersect_kernel<0><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, chunkRec, chunkQ, nullptr, nullptr, R); note_launch(); }
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, prm.exact, chunkRec, chunkQ, nullptr, nullptr, R); note_launch(); }
     exclusive_scan_i32(chunkRec, recScan, nCh, nullptr, stC, d_err, s);
     exclusive_scan_i32(chunkQ, qScan, nCh, nullptr, stC, d_err, s);
   }
@@ -2400,17 +2426,32 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     std::sort(hInfo.begin(), hInfo.end(), [](const BigInfo& x, const BigInfo& y) { return x.k < y.k; });
     int64_t* d_t = A.take_n<int64_t>(2);
     unsigned long long* d_q = A.take_n<unsigned long long>(1);
-    if (!d_t || !d_q) return ST_OUT_OF_MEMORY;
+    double* d_ext = A.take_n<double>(2 * nBigPairs);
+    if (!d_t || !d_q || !d_ext) return ST_OUT_OF_MEMORY;
+    cudaMemsetAsync(d_ext, 0, 2 * nBigPairs * sizeof(double), s);
+    for (int bi = 0; bi < nBigPairs; ++bi)
+      if (hInfo[bi].cq > 0)
+        { edge_extent_kernel<<<blocks_for(hInfo[bi].cq), kThreads, 0, s>>>(Lb, Lo, D, hInfo[bi].k, LQ + hInfo[bi].offQ,
+                                                                          hInfo[bi].cq, d_ext + 2 * bi); note_launch(); }
+    std::vector<double> hExt(2 * nBigPairs);
+    cudaMemcpyAsync(hExt.data(), d_ext, 2 * nBigPairs * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return ST_CUDA_ERROR;
     for (int bi = 0; bi < nBigPairs; ++bi) {
       BigWork& W = bigs[bi];
       W.info = hInfo[bi];
       const double w = W.info.cmbr[2] - W.info.cmbr[0], h = W.info.cmbr[3] - W.info.cmbr[1];
       const double target = (double)std::max(1, W.info.cq);
+      // Cells: about one Q edge per cell, but never smaller than the Q edges' mean box
+      // (long edges would otherwise be listed in many cells and each P edge would scan
+      // them all again); at most 4096 per axis.
+      const double mw = hExt[2 * bi] / target, mh = hExt[2 * bi + 1] / target;
       int gx = 1, gy = 1;
       if (w > 0 && h > 0) {
         gx = (int)std::ceil(std::sqrt(target * w / h));
-        gx = std::min(std::max(gx, 1), 1 << 12);
         gy = (int)std::ceil(target / gx);
+        if (mw > 0) gx = std::min(gx, (int)std::ceil(w / mw));
+        if (mh > 0) gy = std::min(gy, (int)std::ceil(h / mh));
+        gx = std::min(std::max(gx, 1), 1 << 12);
         gy = std::min(std::max(gy, 1), 1 << 12);
       } else if (w > 0) {
         gx = (int)std::min(target, 4096.0);
@@ -2441,7 +2482,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
                                                                    W.cellOff, cursor, W.cellList); note_launch(); }
       cudaMemsetAsync(d_q, 0, sizeof(unsigned long long), s);
       { bin_pairs_kernel<0><<<blocks_for(W.info.cp), kThreads, 0, s>>>(Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G,
-                                                                       W.cellOff, W.cellList, prm.eps, recCnt, d_q,
+                                                                       W.cellOff, W.cellList, prm.eps, prm.exact, recCnt, d_q,
                                                                        nullptr, R); note_launch(); }
       exclusive_scan_i32(recCnt, W.recPos, W.info.cp, d_t + 1, st2, d_err, s);
       { bin_total_kernel<<<1, 1, 0, s>>>(d_t + 1, d_q, k, binRec, binQ); note_launch(); }
@@ -2458,6 +2499,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   cudaMemcpyAsync(hs, tot + 5, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
   const int64_t nR = hs[0];
+  if (nR >= (1ll << kLinkKeyShift)) return ST_OUT_OF_MEMORY;
   // ---- G3 emit
   R.p = A.take_n<int32_t>(nR); R.q = A.take_n<int32_t>(nR);
   R.a = A.take_n<double>(nR); R.b = A.take_n<double>(nR);
@@ -2465,12 +2507,12 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (!R.p || !R.q || !R.a || !R.b || !R.t || !R.k) return ST_OUT_OF_MEMORY;
   if (nCh > 0)
     { intersect_kernel<1><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, recOff, R); note_launch(); }
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, prm.exact, nullptr, nullptr, recScan, recOff, R); note_launch(); }
   for (auto& W : bigs) {
     const int64_t k = W.info.k;
     { add_offset_kernel<<<blocks_for(W.info.cp), kThreads, 0, s>>>(W.recPos, W.info.cp, recOff + k); note_launch(); }
     { bin_pairs_kernel<1><<<blocks_for(W.info.cp), kThreads, 0, s>>>(Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G,
-                                                                     W.cellOff, W.cellList, prm.eps, nullptr, nullptr,
+                                                                     W.cellOff, W.cellList, prm.eps, prm.exact, nullptr, nullptr,
                                                                      W.recPos, R); note_launch(); }
   }
   mk->mark("clip:emit", s);
@@ -2549,6 +2591,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   };
   RingSet SP, SQ;
   if (!take_ring(regTotP, SP) || !take_ring(regTotQ, SQ)) return ST_OUT_OF_MEMORY;
+  SP.exact = SQ.exact = prm.exact;
   mk->mark("clip:layout", s);
   // ---- G5 ring fill (light edges per thread, heavy edges per block)
   {

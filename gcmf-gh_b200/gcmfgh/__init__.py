@@ -78,6 +78,7 @@ def lib():
         L.gcmfgh_destroy.argtypes = [vp]
         L.gcmfgh_set_stream.argtypes = [vp, vp]
         L.gcmfgh_set_params.argtypes = [vp, d, d, ctypes.c_int]
+        L.gcmfgh_set_precision.argtypes = [vp, ctypes.c_int]
         L.gcmfgh_status_string.argtypes = [ctypes.c_int]
         L.gcmfgh_status_string.restype = ctypes.c_char_p
         L.gcmfgh_last_device_error.argtypes = [vp]
@@ -175,6 +176,10 @@ class Engine:
 
     def set_params(self, eps=1e-7, eps_clean=1e-7, union=False):
         _check(lib().gcmfgh_set_params(self.h, eps, eps_clean, 1 if union else 0))
+
+    def set_precision(self, exact=False):
+        """exact=True: exact orientation/classification signs (eps unused there)."""
+        _check(lib().gcmfgh_set_precision(self.h, 1 if exact else 0))
 
     def set_stream(self, stream_ptr):
         _check(lib().gcmfgh_set_stream(self.h, ctypes.c_void_p(stream_ptr)))

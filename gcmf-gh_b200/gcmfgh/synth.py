@@ -129,3 +129,52 @@ def random_star_pairs(seed: int, npairs: int, vmin: int = 3, vmax: int = 40,
             ps.append(np.stack([c[0] + r * np.cos(ang), c[1] + r * np.sin(ang)], axis=1))
         pairs.append((ps[0], ps[1]))
     return pairs
+
+
+def _star(rng, n, cx, cy, R, rlo=0.6, rhi=1.0):
+    ang = np.sort(rng.uniform(0.0, 2 * np.pi, size=n))
+    r = R * rng.uniform(rlo, rhi, size=n)
+    return np.stack([cx + r * np.cos(ang), cy + r * np.sin(ang)], axis=1)
+
+
+def degeneracy_pairs(seed: int = 3, npairs: int = 1_000_000, vmin: int = 4, vmax: int = 10_000,
+                     quantum: float = 2.0 ** -20):
+    """Independent pairs for the precision path, as (classes, [(P, Q), ...]).
+
+    Vertex counts are log-uniform on [vmin, vmax] per polygon; centres uniform on
+    [0, 1000]^2, radius 10 * U(0.6, 1.0) per vertex, counter-clockwise.  Classes (drawn
+    per pair): 1 (2%) the overlay shares one vertex exactly with the base; 2 (1%) the
+    overlay is the base translated along one of its edges by a quarter of that edge, so
+    the two copies of the edge are collinear and overlap; 3 (1%) the overlay is the base
+    translated by 1e-12 relative to its coordinates; 0 the rest, generic overlaps.  Classes
+    1 and 2 use coordinates that are multiples of `quantum`, which makes both
+    constructions exact in FP64."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(vmin), np.log(vmax + 1)
+    classes = np.zeros(npairs, np.int8)
+    pairs = []
+    for k in range(npairs):
+        nP, nQ = (int(v) for v in np.exp(rng.uniform(lo, hi, size=2)))
+        nP, nQ = min(max(nP, vmin), vmax), min(max(nQ, vmin), vmax)
+        u = rng.uniform()
+        c = rng.uniform(0.0, 1000.0, size=2)
+        P = _star(rng, nP, c[0], c[1], 10.0)
+        if u < 0.02:
+            classes[k] = 1
+            P = np.round(P / quantum) * quantum
+            Q = _star(rng, nQ, c[0] + rng.uniform(-8, 8), c[1] + rng.uniform(-8, 8), 10.0)
+            Q = np.round(Q / quantum) * quantum
+            i, j = int(rng.integers(nP)), int(rng.integers(nQ))
+            Q = Q + (P[i] - Q[j])
+        elif u < 0.03:
+            classes[k] = 2
+            P = np.round(P / quantum) * quantum
+            i = int(rng.integers(nP))
+            Q = P + 0.25 * (P[(i + 1) % nP] - P[i])
+        elif u < 0.04:
+            classes[k] = 3
+            Q = P + 1e-12 * np.abs(P).max()
+        else:
+            Q = _star(rng, nQ, c[0] + rng.uniform(-10, 10), c[1] + rng.uniform(-10, 10), 10.0)
+        pairs.append((P, Q))
+    return classes, pairs

@@ -113,6 +113,16 @@ gcmfgh_status gcmfgh_set_stream(gcmfgh_ctx* ctx, void* stream);
  * tolerance (polyclip.h:795; 1e-12 where Constants.h:29 overrides it in the merged
  * build); union_mode: polyclip.h:42 UNION. */
 gcmfgh_status gcmfgh_set_params(gcmfgh_ctx* ctx, double eps, double eps_clean, int union_mode);
+/* Predicate precision of the clip.  GCMFGH_PRECISION_REFERENCE (default): FP64 values
+ * compared against eps, as gppolyclip_mDIV512.cu:95-169 and polyclip.h:297-326 do.
+ * GCMFGH_PRECISION_EXACT: every orientation/order sign of the classification, labelling,
+ * inside tests and split rule is exact (error-bounded FP64 filter, exact expansion
+ * arithmetic when the filter cannot decide); eps is unused there, eps_clean still sets
+ * the clean-up tolerance.  In exact mode P-side and Q-side counts agree by construction,
+ * so no pair is invalid. */
+#define GCMFGH_PRECISION_REFERENCE 0
+#define GCMFGH_PRECISION_EXACT 1
+gcmfgh_status gcmfgh_set_precision(gcmfgh_ctx* ctx, int mode);
 const char* gcmfgh_status_string(gcmfgh_status s);
 /* Work-distribution thresholds of the clip (results do not depend on them):
  * GCMFGH_TUNE_BIN_GRID: a pair whose common-MBR edge grid exceeds this many edge pairs

@@ -95,6 +95,123 @@ int classify(Pt P1, Pt P2, Pt Q1, Pt Q2, double eps, double& alpha, double& beta
   return 0;
 }
 
+// ---- exact-predicate mode (the engine's precision option, not a reference behaviour)
+//
+// Exact signs of (a1-a0)(b1-b0) -/+ (c1-c0)(d1-d0), always through exact arithmetic:
+// Two-Diff for the differences, Dekker's split-based Two-Product for the partial
+// products, Grow-Expansion for the sum (Shewchuk 1997); the largest nonzero component
+// of the nonoverlapping expansion carries the sign.  No error-bound shortcut here, so the
+// engine's filtered evaluation is checked against the unconditional one.
+inline void twoSum(double a, double b, double& s, double& e) {
+  s = a + b;
+  double bv = s - a, av = s - bv;
+  e = (a - av) + (b - bv);
+}
+inline void dekkerSplit(double a, double& hi, double& lo) {      // Dekker: 2^27 + 1
+  double c = 134217729.0 * a;
+  double big = c - a;
+  hi = c - big;
+  lo = a - hi;
+}
+inline void twoProd(double a, double b, double& p, double& e) {
+  p = a * b;
+  double ah, al, bh, bl;
+  dekkerSplit(a, ah, al);
+  dekkerSplit(b, bh, bl);
+  e = al * bl - (((p - ah * bh) - al * bh) - ah * bl);
+}
+int exactSign(double a1, double a0, double b1, double b0, double c1, double c0, double d1, double d0, bool sub) {
+  double d[8];
+  twoSum(a1, -a0, d[0], d[1]);
+  twoSum(b1, -b0, d[2], d[3]);
+  twoSum(c1, -c0, d[4], d[5]);
+  twoSum(d1, -d0, d[6], d[7]);
+  double h[16];
+  int n = 0;
+  auto grow = [&](double q) {
+    for (int i = 0; i < n; ++i) { double s, r; twoSum(q, h[i], s, r); h[i] = r; q = s; }
+    h[n++] = q;
+  };
+  for (int u = 0; u < 2; ++u)
+    for (int v = 0; v < 2; ++v) {
+      double p, e;
+      twoProd(d[u], d[2 + v], p, e);
+      grow(p); grow(e);
+      twoProd(d[4 + u], d[6 + v], p, e);
+      if (sub) { p = -p; e = -e; }
+      grow(p); grow(e);
+    }
+  for (int i = n - 1; i >= 0; --i)
+    if (h[i] != 0.0) return h[i] > 0 ? 1 : -1;
+  return 0;
+}
+inline int orientExact(double px, double py, double qx, double qy, double rx, double ry) {
+  return exactSign(qx, px, ry, py, qy, py, rx, px, true);   // sign of A3(P, Q, R)
+}
+inline int dotExact(Pt U1, Pt U0, Pt V1, Pt V0) {            // sign of (U1-U0).(V1-V0)
+  return exactSign(U1.x, U0.x, V1.x, V0.x, U1.y, U0.y, V1.y, V0.y, false);
+}
+inline double crossingParam(double A1, double A2) {
+  double t = A1 / (A1 - A2);
+  if (!(t >= 0.0)) t = 0.0;
+  if (t > 1.0) t = 1.0;
+  return t;
+}
+
+// Edge classification with exact signs: the nine types of classify() with every
+// tolerance test replaced by its exact counterpart (alpha in (0,1) <=> P1, P2 strictly on
+// opposite sides of line Q; alpha == 0 <=> P1 on it; collinear order from exact dot
+// signs; Q1 == P1 for the coincident-start cases).  alpha/beta are the FP64 expressions,
+// clamped to [0,1].
+int classifyExact(Pt P1, Pt P2, Pt Q1, Pt Q2, double& alpha, double& beta) {
+  int s1 = orientExact(P1.x, P1.y, Q1.x, Q1.y, Q2.x, Q2.y);
+  int s2 = orientExact(P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y);
+  if (s1 != 0 || s2 != 0) {
+    if (s1 == s2) return 0;
+    int t1 = orientExact(Q1.x, Q1.y, P1.x, P1.y, P2.x, P2.y);
+    int t2 = orientExact(Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y);
+    bool a01 = s1 * s2 < 0, a0 = s1 == 0, b01 = t1 * t2 < 0, b0 = t1 == 0;
+    if (!(a01 || a0) || !(b01 || b0)) return 0;
+    double AP1 = A3(P1.x, P1.y, Q1.x, Q1.y, Q2.x, Q2.y), AP2 = A3(P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y);
+    double AQ1 = A3(Q1.x, Q1.y, P1.x, P1.y, P2.x, P2.y), AQ2 = A3(Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y);
+    alpha = a0 ? 0.0 : crossingParam(AP1, AP2);
+    beta = b0 ? 0.0 : crossingParam(AQ1, AQ2);
+    if (a01 && b01) return 1;
+    if (a0 && b01) return 2;
+    if (b0 && a01) return 3;
+    return 4;
+  }
+  bool same = P1.x == Q1.x && P1.y == Q1.y;
+  bool a01 = dotExact(Q1, P1, P2, P1) > 0 && dotExact(P2, Q1, P2, P1) > 0;
+  bool b01 = dotExact(P1, Q1, Q2, Q1) > 0 && dotExact(Q2, P1, Q2, Q1) > 0;
+  bool a0 = !a01 && same, an = !a01 && !same;
+  bool b0 = !b01 && same, bn = !b01 && !same;
+  int tp = 0;
+  if (a01 && b01) tp = 5;
+  else if (an && b01) tp = 6;
+  else if (bn && a01) tp = 7;
+  else if (a0 && b0) tp = 8;
+  if (tp) {
+    double dPx = P2.x - P1.x, dPy = P2.y - P1.y;
+    double dQx = Q2.x - Q1.x, dQy = Q2.y - Q1.y;
+    double PQx = Q1.x - P1.x, PQy = Q1.y - P1.y;
+    alpha = (PQx * dPx + PQy * dPy) / (dPx * dPx + dPy * dPy);
+    beta = -(PQx * dQx + PQy * dQy) / (dQx * dQx + dQy * dQy);
+    if (a01) alpha = std::min(std::max(alpha, 0.0), 1.0);
+    if (b01) beta = std::min(std::max(beta, 0.0), 1.0);
+    if (a0) alpha = 0.0;
+    if (b0) beta = 0.0;
+  }
+  return tp;
+}
+
+// sign of A3 in the selected mode
+inline int orientSign(bool exact, double px, double py, double qx, double qy, double rx, double ry) {
+  if (exact) return orientExact(px, py, qx, qy, rx, ry);
+  double v = A3(px, py, qx, qy, rx, ry);
+  return (v > 0) - (v < 0);
+}
+
 // gppolyclip_mDIV512.cu:345-371
 inline bool edgeBoxesTouch(Pt P1, Pt P2, Pt Q1, Pt Q2) {
   double minPX = std::min(P1.x, P2.x), maxPX = std::max(P1.x, P2.x);
@@ -138,6 +255,7 @@ struct Ring {
 struct Clipper {
   double eps, epsClean;
   bool uni, filters;
+  bool exact = false;                          // exact-predicate mode
   Ring R[2];                                   // R[0] = P, R[1] = Q
   std::vector<std::vector<Pt>> out;            // result components
   long long count1P = 0, count1Q = 0, typeCount[9] = {0};
@@ -148,7 +266,7 @@ struct Clipper {
   }
 
   // polygon.h:427-448 over the ring's current vertices (edges(ALL)).
-  static bool pointInPoly(const Ring& Rg, double Rx, double Ry) {
+  static bool pointInPoly(const Ring& Rg, double Rx, double Ry, bool ex) {
     int w = 0;
     int one = Rg.root;
     do {
@@ -157,9 +275,9 @@ struct Clipper {
       if ((P0y < Ry) != (P1y < Ry)) {
         if (P0x >= Rx) {
           if (P1x > Rx) w = w + 2 * (P1y > P0y) - 1;
-          else if ((A3(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
+          else if ((orientSign(ex, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
         } else if (P1x > Rx) {
-          if ((A3(P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
+          if ((orientSign(ex, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
         }
       }
       one = two;
@@ -171,9 +289,9 @@ struct Clipper {
     const Ring& Q = R[1];
     if (P.inter[p1] && P.nbr[p1] == qv) return IS_P_m;
     if (P.inter[p3] && P.nbr[p3] == qv) return IS_P_p;
-    double s1 = A3(Q.x[qv], Q.y[qv], P.x[p1], P.y[p1], P.x[p2], P.y[p2]);
-    double s2 = A3(Q.x[qv], Q.y[qv], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
-    double s3 = A3(P.x[p1], P.y[p1], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+    int s1 = orientSign(exact, Q.x[qv], Q.y[qv], P.x[p1], P.y[p1], P.x[p2], P.y[p2]);
+    int s2 = orientSign(exact, Q.x[qv], Q.y[qv], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+    int s3 = orientSign(exact, P.x[p1], P.y[p1], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
     if (s3 > 0) return (s1 > 0 && s2 > 0) ? LEFT : RIGHT;
     return (s1 < 0 && s2 < 0) ? RIGHT : LEFT;
   }
@@ -340,6 +458,9 @@ struct Clipper {
           for (int x = x0; x <= x1; ++x) cellItems[cur[(size_t)y * gx + x]++] = j;
       }
     }
+    auto cls = [&](Pt A1, Pt A2, Pt B1, Pt B2, double& al, double& be) {
+      return exact ? classifyExact(A1, A2, B1, B2, al, be) : classify(A1, A2, B1, B2, eps, al, be);
+    };
     std::vector<int> qcand;
     for (int i = 0; i < nP; ++i) {
       Pt P1 = ptP(i), P2 = ptP((i + 1) % nP);
@@ -365,15 +486,15 @@ struct Clipper {
         double a = 0, b = 0;
         if (filters) {
           if (!edgeBoxesTouch(P1, P2, Q1, Q2)) continue;
-          int tp = (cmP[i] || cmQ[j]) ? classify(P1, P2, Q1, Q2, eps, a, b) : 0;
+          int tp = (cmP[i] || cmQ[j]) ? cls(P1, P2, Q1, Q2, a, b) : 0;
           if (cmP[i] && tp) count1P++;
           if (cmQ[j]) {
             double a2, b2;
-            if (classify(Q1, Q2, P1, P2, eps, a2, b2)) count1Q++;
+            if (cls(Q1, Q2, P1, P2, a2, b2)) count1Q++;
           }
           if (tp && cmP[i] && cmQ[j]) { recs.push_back({i, j, a, b, tp}); typeCount[tp]++; }
         } else {
-          int tp = classify(P1, P2, Q1, Q2, eps, a, b);
+          int tp = cls(P1, P2, Q1, Q2, a, b);
           if (tp) { recs.push_back({i, j, a, b, tp}); typeCount[tp]++; count1P++; count1Q++; }
         }
       }
@@ -482,7 +603,7 @@ struct Clipper {
         else {
           double px = 0, py = 0;
           nonIntersectionPoint(A, B, px, py);
-          bool inside = pointInPoly(B, px, py);
+          bool inside = pointInPoly(B, px, py, exact);
           if (inside ^ uni) out.push_back(ringPoints(A));
         }
       }
@@ -498,7 +619,7 @@ struct Clipper {
       int V = nonIntersectionVertex(A, B);
       if (V < 0) continue;
       int st = ENTRY;
-      if (pointInPoly(B, A.x[V], A.y[V])) st = EXIT;
+      if (pointInPoly(B, A.x[V], A.y[V], exact)) st = EXIT;
       bool first = true;
       auto toggle = [&]() { st = (st == ENTRY) ? EXIT : ENTRY; };
       forIntersections(A, V, [&](int I) {
@@ -530,7 +651,12 @@ struct Clipper {
         int VQ = RQ.add(RQ.x[IQ], RQ.y[IQ], false);
         double sP = A3(RP.x[RP.prev[IP]], RP.y[RP.prev[IP]], RP.x[IP], RP.y[IP], RP.x[RP.next[IP]], RP.y[RP.next[IP]]);
         double sQ = A3(RQ.x[RQ.prev[IQ]], RQ.y[RQ.prev[IQ]], RQ.x[IQ], RQ.y[IQ], RQ.x[RQ.next[IQ]], RQ.y[RQ.next[IQ]]);
-        if (sP * sQ > 0) { link(RP, IP, RQ, VQ); link(RP, VP, RQ, IQ); }
+        bool same = exact ? orientSign(true, RP.x[RP.prev[IP]], RP.y[RP.prev[IP]], RP.x[IP], RP.y[IP],
+                                       RP.x[RP.next[IP]], RP.y[RP.next[IP]]) *
+                                orientSign(true, RQ.x[RQ.prev[IQ]], RQ.y[RQ.prev[IQ]], RQ.x[IQ], RQ.y[IQ],
+                                       RQ.x[RQ.next[IQ]], RQ.y[RQ.next[IQ]]) > 0
+                          : sP * sQ > 0;
+        if (same) { link(RP, IP, RQ, VQ); link(RP, VP, RQ, IQ); }
         else link(RP, VP, RQ, VQ);
         RP.insertAfter(VP, IP);
         RQ.insertAfter(VQ, IQ);
@@ -658,10 +784,12 @@ extern "C" {
 // Clip one pair.  P, Q: open rings (no closing vertex), interleaved x,y.
 // flags bit0: union instead of intersection.  bit1: GPU-path semantics (CMBR and edge-box
 // filters, P/Q count cross-check); without it, the reference's CPU path (every edge pair).
+// bit2: exact-predicate mode (eps unused for classification; epsClean still applies).
 int orc_clip_pair(const double* P, int nP, const double* Q, int nQ, double eps, double epsClean, int flags) {
   g_store.clear();
   Clipper c;
   c.eps = eps; c.epsClean = epsClean; c.uni = flags & 1; c.filters = (flags >> 1) & 1;
+  c.exact = (flags >> 2) & 1;
   c.run(P, nP, Q, nQ);
   storeResult(c);
   return c.status;
@@ -683,6 +811,7 @@ int64_t orc_clip_batch(const double* bxy, const int32_t* bvnum, const int64_t* b
     const double* po = oxy + 2 * (ovps[o] - ovnum[o]);
     Clipper c;
     c.eps = eps; c.epsClean = epsClean; c.uni = flags & 1; c.filters = (flags >> 1) & 1;
+    c.exact = (flags >> 2) & 1;
     if (nb < no) c.run(po, no, pb, nb);
     else c.run(pb, nb, po, no);
     storeResult(c);
@@ -705,6 +834,20 @@ void orc_result_copy(int32_t* status, int32_t* ncomp, int64_t* count1, int64_t* 
   if (nrec) std::copy(g_store.nrec.begin(), g_store.nrec.end(), nrec);
   if (compSize) std::copy(g_store.compSize.begin(), g_store.compSize.end(), compSize);
   if (xy) std::copy(g_store.xy.begin(), g_store.xy.end(), xy);
+}
+
+// exact sign of A3(P, Q, R) for n point triples (v: 6 doubles per triple), and of the
+// dot product (U1-U0).(V1-V0) when dot != 0 (v: 8 doubles per entry)
+void orc_exact_signs(const double* v, int64_t n, int dot, int32_t* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    if (dot) {
+      const double* w = v + 8 * i;
+      out[i] = dotExact(Pt{w[0], w[1]}, Pt{w[2], w[3]}, Pt{w[4], w[5]}, Pt{w[6], w[7]});
+    } else {
+      const double* w = v + 6 * i;
+      out[i] = orientExact(w[0], w[1], w[2], w[3], w[4], w[5]);
+    }
+  }
 }
 
 }  // extern "C"

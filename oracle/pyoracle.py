@@ -20,6 +20,7 @@ REF_BIN = os.path.join(HERE, "_ref", "ghclip_ref")
 
 FLAG_UNION = 1
 FLAG_GPU_SEMANTICS = 2
+FLAG_EXACT = 4
 
 _lib = None
 
@@ -44,9 +45,8 @@ def lib():
         L.orc_result_sizes.restype = i64
         L.orc_result_copy.argtypes = [vp] * 6
         L.orc_result_copy.restype = None
-        for name in ("orc_join",):
-            if hasattr(L, name):
-                pass
+        L.orc_exact_signs.argtypes = [vp, i64, i32, vp]
+        L.orc_exact_signs.restype = None
         _lib = L
     return _lib
 
@@ -91,21 +91,37 @@ def _collect():
     return ClipResult(status, ncmp, count1, nrec, csz, xy)
 
 
-def clip_pair(P, Q, eps=1e-7, eps_clean=None, union=False, gpu_semantics=True):
+def _flags(union, gpu_semantics, exact):
+    return ((FLAG_UNION if union else 0) | (FLAG_GPU_SEMANTICS if gpu_semantics else 0)
+            | (FLAG_EXACT if exact else 0))
+
+
+def exact_signs(v, dot=False):
+    """Exact signs of A3 over rows (px,py,qx,qy,rx,ry), or of (U1-U0).(V1-V0) over rows
+    (u1x,u1y,u0x,u0y,v1x,v1y,v0x,v0y) when dot."""
+    v = np.ascontiguousarray(v, np.float64)
+    n = v.shape[0]
+    out = np.zeros(n, np.int32)
+    lib().orc_exact_signs(_p(v), n, 1 if dot else 0, _p(out))
+    return out
+
+
+def clip_pair(P, Q, eps=1e-7, eps_clean=None, union=False, gpu_semantics=True, exact=False):
     P = np.ascontiguousarray(P, np.float64).reshape(-1)
     Q = np.ascontiguousarray(Q, np.float64).reshape(-1)
-    flags = (FLAG_UNION if union else 0) | (FLAG_GPU_SEMANTICS if gpu_semantics else 0)
+    flags = _flags(union, gpu_semantics, exact)
     lib().orc_clip_pair(_p(P), len(P) // 2, _p(Q), len(Q) // 2, eps,
                         eps if eps_clean is None else eps_clean, flags)
     return _collect()
 
 
 def clip_batch(base, overlay, pid, qid, eps=1e-7, eps_clean=None, union=False,
-               gpu_semantics=True):
-    """Clip the listed (base, overlay) pairs with the reference's swap rule."""
+               gpu_semantics=True, exact=False):
+    """Clip the listed (base, overlay) pairs with the reference's swap rule.  exact=True
+    selects the exact-predicate mode (classification and orientation signs exact)."""
     pid = np.ascontiguousarray(pid, np.int32)
     qid = np.ascontiguousarray(qid, np.int32)
-    flags = (FLAG_UNION if union else 0) | (FLAG_GPU_SEMANTICS if gpu_semantics else 0)
+    flags = _flags(union, gpu_semantics, exact)
     lib().orc_clip_batch(_p(base.xy), _p(base.vnum), _p(base.vps),
                          _p(overlay.xy), _p(overlay.vnum), _p(overlay.vps),
                          _p(pid), _p(qid), len(pid), eps,
