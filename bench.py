@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--sample-bases", type=int, default=0,
                     help="reference arm: base polygons per step sample (0: auto)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving latency section")
     return ap.parse_args()
 
 
@@ -218,6 +219,73 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+# ----------------------------------------------------------------------------- serving
+
+SERVE_WORKLOAD = ("serving: resident layer of 1,000,000 FP64 stars (batched workload's distributions, "
+                  "seed 4) with its MBR grid index in HBM; open-loop Poisson arrivals of query stars "
+                  "(vertex counts log-uniform [16, 50000], pool of 512) joined against the layer and "
+                  "clipped against every hit")
+
+
+def _open_loop(srv, queries, rate, seconds, rng, max_requests=None):
+    """Submits queries at Poisson arrival times (open loop; latency counts from the
+    scheduled arrival, so client lag is charged to the server, never hidden) and returns
+    per-request results."""
+    n = int(rate * seconds)
+    if max_requests:
+        n = min(n, max_requests)
+    gaps = rng.exponential(1.0 / rate, size=n)
+    t0 = time.monotonic_ns() + 2_000_000
+    arrivals = t0 + np.cumsum(gaps * 1e9).astype(np.int64)
+    pick = rng.integers(0, len(queries), size=n)
+    tickets = []
+    i = 0
+    while i < n:
+        now = time.monotonic_ns()
+        while i < n and arrivals[i] <= now:
+            tickets.append(srv.submit(queries[pick[i]], arrival_ns=int(arrivals[i])))
+            i += 1
+        if i < n and arrivals[i] > now + 200_000:
+            time.sleep(max(0.0, (arrivals[i] - now) * 1e-9 - 1e-4))
+    infos = [srv.wait(t, 600_000) for t in tickets]
+    for t, inf in zip(tickets, infos):
+        srv.take(t, inf)
+    return infos, arrivals
+
+
+def _latency_summary(infos, arrivals, rate):
+    lat = np.array([inf["done_ns"] - inf["arrival_ns"] for inf in infos], dtype=np.float64) * 1e-6
+    hits = sum(inf["n_hits"] for inf in infos)
+    span = (max(inf["done_ns"] for inf in infos) - int(arrivals[0])) * 1e-9
+    bad = sum(1 for inf in infos if inf["status"] != 0)
+    return {"rate_req_s": rate, "requests": len(infos), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "pairs_per_s": hits / span,
+            "queries_per_s": len(infos) / span, "mean_batch": float(np.mean([inf["batch_queries"] for inf in infos])),
+            "errors": bad}
+
+
+def serve_measure(local, seconds=0.5):
+    """p50/p99 latency and pairs/s of the continuous-batching server at 2k/10k/50k req/s,
+    and of the plain one-query-per-launch form (one worker, batches of one query)."""
+    import gcmfgh
+    from gcmfgh import synth
+    resident, queries = synth.serving_workload(seed=4)
+    rng = np.random.default_rng(44)
+    out = {"workload": SERVE_WORKLOAD, "batched": [], "plain": []}
+    with gcmfgh.Server(resident, device=local, workers=2) as srv:
+        _open_loop(srv, queries, 2000, 0.1, rng)                     # warm-up
+        for rate in (2000, 10000, 50000):
+            infos, arr = _open_loop(srv, queries, rate, seconds, rng)
+            out["batched"].append(_latency_summary(infos, arr, rate))
+        out["batched_stats"] = srv.stats()
+    with gcmfgh.Server(resident, device=local, workers=1, max_batch_queries=1) as srv:
+        _open_loop(srv, queries, 500, 0.1, rng)
+        for rate in (2000, 10000, 50000):
+            infos, arr = _open_loop(srv, queries, rate, seconds, rng, max_requests=2000)
+            out["plain"].append(_latency_summary(infos, arr, rate))
+    return out
+
+
 # ----------------------------------------------------------------------------- our arm
 
 def run_ours(args, rank, world, local):
@@ -348,6 +416,8 @@ def run_ours(args, rank, world, local):
             "clocks": clocks,
             "gpu_launches": launches,
         }
+        if not args.no_serve:
+            line["serving"] = serve_measure(local)
         if world == 1:
             nb = args.sample_bases or 20000
             p, s, cores = reference_cpu_sample(base, ovl, nb, 7)

@@ -114,6 +114,10 @@ int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s);
 int run_join(const LayerDev& base, const LayerDev& ovl, Arena& arena, JoinDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);
 
+int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys, int64_t K, int obits,
+                   Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,
+                   int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);
+
 int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, const int32_t* d_qid,
              int64_t n_pairs, const ClipParams& prm, Arena& arena, ClipDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);

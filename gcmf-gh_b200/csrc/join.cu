@@ -429,6 +429,19 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   { sweep_kernel<1><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs, pkeys, obits); note_launch(); }
   radix_sort_pairs(pkeys, pvals, pkAlt, pvAlt, K, ((obits + bbits + 7) / 8) * 8, rtmp, d_err, s);
   mk->mark("join:sweep-emit+sort", s);
+  return join_from_keys(Lb, Lo, pkeys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, mk);
+}
+
+// Stages J3-J6 and the clip set over candidate pairs given as packed keys
+// (b << obits | o) sorted ascending; J.mbr_b/J.mbr_o hold the layers' MBRs.  d_total
+// (4 entries) and d_cnt (8 entries, zeroed) are device scratch counters.
+int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys, int64_t K, int obits,
+                   Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,
+                   int64_t* h_scratch, cudaStream_t s, Marks* mk) {
+  Marks dummy;
+  if (!mk) mk = &dummy;
+  J.n_pairs = K;
+  if (K == 0) return ST_OK;
   // ---- J3 CMBR + containment candidates
   J.b = A.take_n<int32_t>(K); J.o = A.take_n<int32_t>(K);
   J.cmbr = A.take_n<double>(4 * K);

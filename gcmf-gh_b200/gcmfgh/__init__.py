@@ -63,6 +63,23 @@ class ClipInfo(ctypes.Structure):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
+class ServeOptions(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_int),
+                ("max_batch_queries", ctypes.c_int64), ("max_batch_vertices", ctypes.c_int64),
+                ("reserve_bytes", ctypes.c_int64), ("bytes_per_vertex", ctypes.c_int64),
+                ("eps", ctypes.c_double), ("eps_clean", ctypes.c_double),
+                ("union_mode", ctypes.c_int), ("exact", ctypes.c_int)]
+
+
+class ServeResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32)] + [(n, ctypes.c_int64) for n in
+                ("n_hits", "n_components", "n_vertices", "n_candidates", "arrival_ns", "admitted_ns",
+                 "done_ns", "batch_id", "batch_queries")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -100,6 +117,14 @@ def lib():
         L.gcmfgh_get_timing.argtypes = [vp, ctypes.c_int, P(ctypes.c_float), P(ctypes.c_char_p),
                                         ctypes.c_int]
         L.gcmfgh_get_timing.restype = ctypes.c_int
+        L.gcmfgh_serve_default_options.argtypes = [P(ServeOptions)]
+        L.gcmfgh_serve_open.argtypes = [P(Layer), P(ServeOptions), P(vp)]
+        L.gcmfgh_serve_submit.argtypes = [vp, vp, i32, i64, P(ctypes.c_uint64)]
+        L.gcmfgh_serve_poll.argtypes = [vp, ctypes.c_uint64, P(ServeResult)]
+        L.gcmfgh_serve_wait.argtypes = [vp, ctypes.c_uint64, i64, P(ServeResult)]
+        L.gcmfgh_serve_take.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp]
+        L.gcmfgh_serve_stats.argtypes = [vp, P(i64), P(i64), P(i64)]
+        L.gcmfgh_serve_close.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -282,3 +307,85 @@ class Engine:
         _check(lib().gcmfgh_join_clip_host(self.h, ctypes.byref(jb), ctypes.byref(jo), ctypes.byref(ji),
                                            ctypes.byref(ci)))
         return ji.as_dict(), ci.as_dict()
+
+
+class QueryResult:
+    """One served query: per hit the resident polygon id, clip status and components."""
+
+    def __init__(self, info, hit_ids, hit_status, hit_ncomp, comp_size, xy):
+        self.info = info
+        self.hit_ids, self.hit_status, self.hit_ncomp = hit_ids, hit_status, hit_ncomp
+        self.comp_size, self.xy = comp_size, xy
+
+    def latency_ns(self):
+        return self.info["done_ns"] - self.info["arrival_ns"]
+
+
+class Server:
+    """Continuous-batching join+clip server over a resident (host numpy) layer."""
+
+    def __init__(self, resident, device=0, workers=2, max_batch_queries=4096,
+                 max_batch_vertices=1 << 22, reserve_bytes=2 << 30, bytes_per_vertex=4096,
+                 eps=1e-7, eps_clean=1e-7, union=False, exact=False):
+        o = ServeOptions()
+        _check(lib().gcmfgh_serve_default_options(ctypes.byref(o)))
+        o.device, o.workers = device, workers
+        o.max_batch_queries, o.max_batch_vertices = max_batch_queries, max_batch_vertices
+        o.reserve_bytes, o.bytes_per_vertex = reserve_bytes, bytes_per_vertex
+        o.eps, o.eps_clean, o.union_mode, o.exact = eps, eps_clean, int(union), int(exact)
+        self._resident = resident
+        self.h = ctypes.c_void_p()
+        L = host_layer(resident)
+        _check(lib().gcmfgh_serve_open(ctypes.byref(L), ctypes.byref(o), ctypes.byref(self.h)))
+
+    def submit(self, ring, arrival_ns=0):
+        r = np.ascontiguousarray(ring, np.float64).reshape(-1)
+        t = ctypes.c_uint64()
+        _check(lib().gcmfgh_serve_submit(self.h, _np_ptr(r), len(r) // 2, int(arrival_ns), ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket):
+        info = ServeResult()
+        st = lib().gcmfgh_serve_poll(self.h, ticket, ctypes.byref(info))
+        if st == 5:
+            return None
+        _check(st)
+        return info.as_dict()
+
+    def wait(self, ticket, timeout_ms=-1):
+        info = ServeResult()
+        st = lib().gcmfgh_serve_wait(self.h, ticket, int(timeout_ms), ctypes.byref(info))
+        if st == 5:
+            return None
+        _check(st)
+        return info.as_dict()
+
+    def take(self, ticket, info):
+        nh, nc, nv = info["n_hits"], info["n_components"], info["n_vertices"]
+        ids, hst, hnc = (np.zeros(nh, np.int32) for _ in range(3))
+        csz, xy = np.zeros(nc, np.int32), np.zeros(2 * nv, np.float64)
+        _check(lib().gcmfgh_serve_take(self.h, ticket, _np_ptr(ids), _np_ptr(hst), _np_ptr(hnc),
+                                       _np_ptr(csz), _np_ptr(xy)))
+        return QueryResult(info, ids, hst, hnc, csz, xy)
+
+    def result(self, ticket, timeout_ms=-1):
+        info = self.wait(ticket, timeout_ms)
+        if info is None:
+            raise GcmfghError("query not finished within the timeout")
+        return self.take(ticket, info)
+
+    def stats(self):
+        b, q, p = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().gcmfgh_serve_stats(self.h, ctypes.byref(b), ctypes.byref(q), ctypes.byref(p)))
+        return {"batches": b.value, "queries": q.value, "peak_batch": p.value}
+
+    def close(self):
+        if self.h:
+            _check(lib().gcmfgh_serve_close(self.h))
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

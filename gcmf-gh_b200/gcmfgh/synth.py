@@ -178,3 +178,27 @@ def degeneracy_pairs(seed: int = 3, npairs: int = 1_000_000, vmin: int = 4, vmax
             Q = _star(rng, nQ, c[0] + rng.uniform(-10, 10), c[1] + rng.uniform(-10, 10), 10.0)
         pairs.append((P, Q))
     return classes, pairs
+
+
+def serving_workload(seed: int = 4, n: int = 1_000_000, n_queries: int = 512, components: int = 64,
+                     extent: float = 1e5, sigma: float = 2000.0, cap: int = 100_000,
+                     qmin: int = 16, qmax: int = 50_000):
+    """Resident layer of n stars with the batched workload's distributions (Pareto(1.5, 4)
+    vertex counts capped at `cap`, 64-component GMM centres, log-normal(ln 50, 0.7) radius),
+    and a pool of query stars whose vertex counts are log-uniform on [qmin, qmax], centred
+    by the same mixture with the same radius law.  Returns (resident Layer, [query rings])."""
+    rng = np.random.default_rng(seed)
+    means = rng.uniform(0.0, extent, size=(components, 2))
+    counts = np.minimum(np.floor(4.0 * (1.0 + rng.pareto(1.5, size=n))), cap).astype(np.int64)
+    comp = rng.integers(0, components, size=n)
+    centres = means[comp] + rng.normal(0.0, sigma, size=(n, 2))
+    base = rng.lognormal(np.log(50.0), 0.7, size=n)
+    resident = star_layer(rng, counts, centres, base)
+    qcounts = np.exp(rng.uniform(np.log(qmin), np.log(qmax + 1), size=n_queries)).astype(np.int64)
+    qcounts = np.clip(qcounts, qmin, qmax)
+    qcomp = rng.integers(0, components, size=n_queries)
+    qcentres = means[qcomp] + rng.normal(0.0, sigma, size=(n_queries, 2))
+    qbase = rng.lognormal(np.log(50.0), 0.7, size=n_queries)
+    ql = star_layer(rng, qcounts, qcentres, qbase)
+    queries = [np.ascontiguousarray(ql.ring(i)) for i in range(n_queries)]
+    return resident, queries

@@ -204,6 +204,65 @@ gcmfgh_status gcmfgh_join_clip_host(gcmfgh_ctx* ctx, const gcmfgh_layer* base_ho
                                     const gcmfgh_layer* overlay_host, gcmfgh_join_info* jinfo,
                                     gcmfgh_clip_info* cinfo);
 
+/* ---- serving: continuous batching of join+clip queries against a resident layer.
+ * No counterpart in the reference (its main() runs one join and one clip over two whole
+ * layers, main.cpp:15-29).  The resident layer is copied to the device once and indexed
+ * by an MBR grid.  Each submitted query polygon is joined against it (the same MBR
+ * candidate predicate, containment, common-MBR and segment filters as gcmf_join, with the
+ * query as base polygon) and clipped against every hit (as gh_clip_batch, swap rule
+ * included).  Worker threads, each with its own stream and device workspace, take the
+ * queries waiting at that moment as one batch: FIFO, at most max_batch_queries queries and
+ * max_batch_vertices query vertices, and no more vertices than
+ * (free device memory - reserve_bytes) / bytes_per_vertex (at least one query).  While one
+ * batch is on the GPU the next worker admits what arrived meanwhile.  A query's result
+ * does not depend on the other queries of its batch.  workers = 1 with
+ * max_batch_queries = 1 is the plain one-query-per-launch form. */
+typedef struct gcmfgh_server gcmfgh_server;
+typedef struct {
+  int device;
+  int workers;                 /* batches in flight at once (default 2) */
+  int64_t max_batch_queries;   /* default 4096 */
+  int64_t max_batch_vertices;  /* default 2^22 */
+  int64_t reserve_bytes;       /* device memory left free when admitting (default 2 GiB) */
+  int64_t bytes_per_vertex;    /* working-set estimate per query vertex (default 4096) */
+  double eps, eps_clean;       /* as gcmfgh_set_params */
+  int union_mode;
+  int exact;                   /* GCMFGH_PRECISION_EXACT semantics when nonzero */
+} gcmfgh_serve_options;
+typedef struct {
+  int32_t status;              /* gcmfgh_status of the query's batch */
+  int64_t n_hits;              /* clipped pairs (resident polygons in the clip set) */
+  int64_t n_components;
+  int64_t n_vertices;
+  int64_t n_candidates;        /* MBR candidates */
+  int64_t arrival_ns;          /* CLOCK_MONOTONIC nanoseconds */
+  int64_t admitted_ns;         /* taken into a batch */
+  int64_t done_ns;             /* results on the host */
+  int64_t batch_id;
+  int64_t batch_queries;       /* queries in that batch */
+} gcmfgh_serve_result;
+gcmfgh_status gcmfgh_serve_default_options(gcmfgh_serve_options* opt);
+/* resident: HOST layer in the layout above; opt may be NULL (defaults) */
+gcmfgh_status gcmfgh_serve_open(const gcmfgh_layer* resident, const gcmfgh_serve_options* opt,
+                                gcmfgh_server** out);
+/* one query: host open ring (no closing vertex) of n vertices, copied before returning;
+ * arrival_ns: when the request arrived (CLOCK_MONOTONIC ns; <= 0 = now).  Thread-safe. */
+gcmfgh_status gcmfgh_serve_submit(gcmfgh_server* srv, const double* xy, int32_t n, int64_t arrival_ns,
+                                  uint64_t* ticket);
+/* GCMFGH_NOT_READY until the query's batch has completed, then fills *info */
+gcmfgh_status gcmfgh_serve_poll(gcmfgh_server* srv, uint64_t ticket, gcmfgh_serve_result* info);
+/* blocks until completed or timeout_ms elapsed (< 0: no limit) */
+gcmfgh_status gcmfgh_serve_wait(gcmfgh_server* srv, uint64_t ticket, int64_t timeout_ms,
+                                gcmfgh_serve_result* info);
+/* copies a completed result and releases the ticket: per hit its resident polygon id,
+ * clip status and component count [n_hits]; component sizes [n_components]; vertices
+ * [2 n_vertices].  Hits are in ascending resident id; NULL skips a field. */
+gcmfgh_status gcmfgh_serve_take(gcmfgh_server* srv, uint64_t ticket, int32_t* hit_ids, int32_t* hit_status,
+                                int32_t* hit_ncomp, int32_t* comp_size, double* xy);
+gcmfgh_status gcmfgh_serve_stats(gcmfgh_server* srv, int64_t* batches, int64_t* queries, int64_t* peak_batch);
+/* finishes the queued queries, stops the workers and frees the device state */
+gcmfgh_status gcmfgh_serve_close(gcmfgh_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

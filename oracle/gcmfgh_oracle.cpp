@@ -39,6 +39,8 @@
 #include <vector>
 #include <algorithm>
 #include <numeric>
+#include <thread>
+#include <functional>
 
 namespace {
 
@@ -403,7 +405,6 @@ struct Clipper {
                       std::min(mb[0][2], mb[1][2]), std::min(mb[0][3], mb[1][3])};
 
     // ---- intersection records (gpuCountIntersections / polyclip.h:202-268)
-    std::vector<Rec> recs;
     std::vector<uint8_t> cmP(nP, 1), cmQ(nQ, 1);
     auto ptP = [&](int i) { return Pt{P[2 * i], P[2 * i + 1]}; };
     auto ptQ = [&](int i) { return Pt{Q[2 * i], Q[2 * i + 1]}; };
@@ -413,7 +414,10 @@ struct Clipper {
     }
     // With the box filter on, only Q edges whose boxes can touch P's edge box matter; for
     // large pairs they are found through a uniform grid of Q-edge boxes (the same set as
-    // testing every j, visited in ascending j).
+    // testing every j, visited in ascending j).  Cells hold about one Q edge each but are
+    // never smaller than the Q edges' mean box.  P edges are processed in contiguous
+    // blocks by worker threads; blocks are concatenated in P-edge order, so records and
+    // counts are the same as one sequential pass.
     const bool gridded = filters && (double)nP * nQ > 4e6;
     int gx = 1, gy = 1;
     double gx0 = cmbr[0], gy0 = cmbr[1], gcw = 1, gch = 1;
@@ -427,9 +431,18 @@ struct Clipper {
     if (gridded) {
       double w = cmbr[2] - cmbr[0], h = cmbr[3] - cmbr[1];
       int target = std::max(1, nQ);
+      double sw = 0, sh = 0;
+      for (int j = 0; j < nQ; ++j) {
+        Pt a = ptQ(j), b = ptQ((j + 1) % nQ);
+        sw += std::fabs(b.x - a.x); sh += std::fabs(b.y - a.y);
+      }
       if (w > 0 && h > 0) {
-        gx = std::min(4096, std::max(1, (int)std::ceil(std::sqrt(target * w / h))));
-        gy = std::min(4096, std::max(1, (int)std::ceil((double)target / gx)));
+        gx = std::max(1, (int)std::ceil(std::sqrt(target * w / h)));
+        gy = std::max(1, (int)std::ceil((double)target / gx));
+        if (sw > 0) gx = std::min(gx, (int)std::ceil(w / (sw / target)));
+        if (sh > 0) gy = std::min(gy, (int)std::ceil(h / (sh / target)));
+        gx = std::min(4096, std::max(1, gx));
+        gy = std::min(4096, std::max(1, gy));
       }
       gcw = w > 0 ? w / gx : 1;
       gch = h > 0 ? h / gy : 1;
@@ -461,42 +474,75 @@ struct Clipper {
     auto cls = [&](Pt A1, Pt A2, Pt B1, Pt B2, double& al, double& be) {
       return exact ? classifyExact(A1, A2, B1, B2, al, be) : classify(A1, A2, B1, B2, eps, al, be);
     };
-    std::vector<int> qcand;
-    for (int i = 0; i < nP; ++i) {
-      Pt P1 = ptP(i), P2 = ptP((i + 1) % nP);
-      int ncand = nQ;
-      if (gridded) {
-        qcand.clear();
-        if (cmP[i]) {
-          int x0 = cellOf(std::min(P1.x, P2.x), gx0, gcw, gx), x1 = cellOf(std::max(P1.x, P2.x), gx0, gcw, gx);
-          int y0 = cellOf(std::min(P1.y, P2.y), gy0, gch, gy), y1 = cellOf(std::max(P1.y, P2.y), gy0, gch, gy);
-          for (int y = y0; y <= y1; ++y)
-            for (int x = x0; x <= x1; ++x) {
-              size_t c = (size_t)y * gx + x;
-              qcand.insert(qcand.end(), cellItems.begin() + cellStart[c], cellItems.begin() + cellStart[c + 1]);
-            }
-          std::sort(qcand.begin(), qcand.end());
-          qcand.erase(std::unique(qcand.begin(), qcand.end()), qcand.end());
-        }
-        ncand = (int)qcand.size();
-      }
-      for (int jj = 0; jj < ncand; ++jj) {
-        const int j = gridded ? qcand[jj] : jj;
-        Pt Q1 = ptQ(j), Q2 = ptQ((j + 1) % nQ);
-        double a = 0, b = 0;
-        if (filters) {
-          if (!edgeBoxesTouch(P1, P2, Q1, Q2)) continue;
-          int tp = (cmP[i] || cmQ[j]) ? cls(P1, P2, Q1, Q2, a, b) : 0;
-          if (cmP[i] && tp) count1P++;
-          if (cmQ[j]) {
-            double a2, b2;
-            if (cls(Q1, Q2, P1, P2, a2, b2)) count1Q++;
+    struct Part { std::vector<Rec> recs; long long c1P = 0, c1Q = 0, tc[9] = {0}; };
+    auto runBlock = [&](int i0, int i1, Part& out) {
+      std::vector<int> qcand;
+      for (int i = i0; i < i1; ++i) {
+        Pt P1 = ptP(i), P2 = ptP((i + 1) % nP);
+        int ncand = nQ;
+        if (gridded) {
+          qcand.clear();
+          if (cmP[i]) {
+            int x0 = cellOf(std::min(P1.x, P2.x), gx0, gcw, gx), x1 = cellOf(std::max(P1.x, P2.x), gx0, gcw, gx);
+            int y0 = cellOf(std::min(P1.y, P2.y), gy0, gch, gy), y1 = cellOf(std::max(P1.y, P2.y), gy0, gch, gy);
+            for (int y = y0; y <= y1; ++y)
+              for (int x = x0; x <= x1; ++x) {
+                size_t c = (size_t)y * gx + x;
+                qcand.insert(qcand.end(), cellItems.begin() + cellStart[c], cellItems.begin() + cellStart[c + 1]);
+              }
+            std::sort(qcand.begin(), qcand.end());
+            qcand.erase(std::unique(qcand.begin(), qcand.end()), qcand.end());
           }
-          if (tp && cmP[i] && cmQ[j]) { recs.push_back({i, j, a, b, tp}); typeCount[tp]++; }
-        } else {
-          int tp = cls(P1, P2, Q1, Q2, a, b);
-          if (tp) { recs.push_back({i, j, a, b, tp}); typeCount[tp]++; count1P++; count1Q++; }
+          ncand = (int)qcand.size();
         }
+        for (int jj = 0; jj < ncand; ++jj) {
+          const int j = gridded ? qcand[jj] : jj;
+          Pt Q1 = ptQ(j), Q2 = ptQ((j + 1) % nQ);
+          double a = 0, b = 0;
+          if (filters) {
+            if (!edgeBoxesTouch(P1, P2, Q1, Q2)) continue;
+            int tp = (cmP[i] || cmQ[j]) ? cls(P1, P2, Q1, Q2, a, b) : 0;
+            if (cmP[i] && tp) out.c1P++;
+            if (cmQ[j]) {
+              double a2, b2;
+              if (cls(Q1, Q2, P1, P2, a2, b2)) out.c1Q++;
+            }
+            if (tp && cmP[i] && cmQ[j]) { out.recs.push_back({i, j, a, b, tp}); out.tc[tp]++; }
+          } else {
+            int tp = cls(P1, P2, Q1, Q2, a, b);
+            if (tp) { out.recs.push_back({i, j, a, b, tp}); out.tc[tp]++; out.c1P++; out.c1Q++; }
+          }
+        }
+      }
+    };
+    std::vector<Rec> recs;
+    {
+      int nth = 1;
+      if ((double)nP * nQ > 4e7) {
+        unsigned hc = std::thread::hardware_concurrency();
+        nth = (int)std::max(1u, std::min(hc ? hc : 1u, 64u));
+        if (const char* e = std::getenv("GCMFGH_ORACLE_THREADS")) nth = std::max(1, std::atoi(e));
+      }
+      nth = std::min(nth, std::max(1, nP));
+      std::vector<Part> parts(nth);
+      if (nth == 1) {
+        runBlock(0, nP, parts[0]);
+      } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nth; ++t) {
+          int i0 = (int)((int64_t)nP * t / nth), i1 = (int)((int64_t)nP * (t + 1) / nth);
+          th.emplace_back(runBlock, i0, i1, std::ref(parts[t]));
+        }
+        for (auto& x : th) x.join();
+      }
+      size_t tot = 0;
+      for (auto& pt : parts) tot += pt.recs.size();
+      recs.reserve(tot);
+      for (auto& pt : parts) {
+        recs.insert(recs.end(), pt.recs.begin(), pt.recs.end());
+        std::vector<Rec>().swap(pt.recs);
+        count1P += pt.c1P; count1Q += pt.c1Q;
+        for (int t = 0; t < 9; ++t) typeCount[t] += pt.tc[t];
       }
     }
     if (filters && count1P != count1Q) { status = 1; return; }   // gppolyclip_mDIV512.cu:1461
