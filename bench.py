@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--sample-bases", type=int, default=0,
                     help="reference arm: base polygons per step sample (0: auto)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving latency section")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the host-core reference sample")
     return ap.parse_args()
 
 
@@ -418,7 +419,7 @@ def run_ours(args, rank, world, local):
         }
         if not args.no_serve:
             line["serving"] = serve_measure(local)
-        if world == 1:
+        if world == 1 and not args.no_cpu_baseline:
             nb = args.sample_bases or 20000
             p, s, cores = reference_cpu_sample(base, ovl, nb, 7)
             line["cpu_baseline"] = {"value": p / s, "unit": "pairs/s", "cores": cores, "kind": "reference",

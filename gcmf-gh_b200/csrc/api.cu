@@ -1,15 +1,28 @@
 // api.cu -- the C ABI (include/gcmfgh.h): contexts, device arenas, argument checks and
 // result export.  The reference's entry points exit the process on errors
 // (GPU_Manage.h:25-44, ghcuda.cpp:109-116); these return a status instead.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 #include "common.cuh"
 #include "engine.cuh"
 #include "prims.cuh"
 #include "../../include/gcmfgh.h"
 
 namespace gcmfgh {
+
+cudaStream_t create_priority_stream() {
+  int lo = 0, hi = 0;
+  cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, hi) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return s;
+}
 
 unsigned long long& launch_counter() {
   static unsigned long long n = 0;
@@ -75,6 +88,7 @@ struct gcmfgh_ctx {
   int device = 0;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t aux = nullptr;     // high-priority stream for the long pairs' labelling
   Arena join_arena, clip_arena, layer_arena, pair_arena;
   int* d_err = nullptr;
   int64_t* h_scratch = nullptr;   // pinned
@@ -89,6 +103,7 @@ struct gcmfgh_ctx {
   const double* join_o = nullptr;
   int64_t join_nb = 0, join_no = 0;
   Marks marks[2];                 // stage timing of the last join / clip
+  std::vector<void*> uploads;     // gcmfgh_upload_layer copies, freed by gcmfgh_destroy
 };
 
 namespace {
@@ -150,7 +165,7 @@ gcmfgh_status run_clip_ctx(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_la
   c->marks[1].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   int st = run_clip(to_dev(b), to_dev(o), pid, qid, n, c->prm, c->clip_arena, c->clip, c->d_err,
-                    c->h_scratch, c->stream, &c->marks[1]);
+                    c->h_scratch, c->stream, &c->marks[1], c->aux);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_clip = true;
@@ -249,6 +264,7 @@ gcmfgh_status gcmfgh_create(int device, gcmfgh_ctx** out) {
     return GCMFGH_CUDA_ERROR;
   }
   c->stream = c->own;
+  c->aux = create_priority_stream();
   cudaMemset(c->d_err, 0, 64);
   for (auto& m : c->marks)
     for (int i = 0; i < Marks::kMax; ++i) cudaEventCreate(&m.ev[i]);
@@ -283,10 +299,12 @@ gcmfgh_status gcmfgh_destroy(gcmfgh_ctx* c) {
   c->clip_arena.release();
   c->layer_arena.release();
   c->pair_arena.release();
+  for (void* p : c->uploads) cudaFree(p);
   if (c->d_err) cudaFree(c->d_err);
   if (c->d_stats) cudaFree(c->d_stats);
   if (c->h_scratch) cudaFreeHost(c->h_scratch);
   if (c->own) cudaStreamDestroy(c->own);
+  if (c->aux) cudaStreamDestroy(c->aux);
   for (auto& m : c->marks)
     for (int i = 0; i < Marks::kMax; ++i)
       if (m.ev[i]) cudaEventDestroy(m.ev[i]);
@@ -308,6 +326,29 @@ gcmfgh_status gcmfgh_set_params(gcmfgh_ctx* c, double eps, double eps_clean, int
   return GCMFGH_OK;
 }
 
+gcmfgh_status gcmfgh_upload_layer(gcmfgh_ctx* c, const gcmfgh_layer* h, gcmfgh_layer* d) {
+  if (!c || !h || !d || h->n_polys < 0) return GCMFGH_INVALID_ARGUMENT;
+  if (h->n_polys > 0 && (!h->coords || !h->vnum || !h->vps)) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  const int64_t n = h->n_polys;
+  const int64_t nv = n > 0 ? (h->n_vertices > 0 ? h->n_vertices : h->vps[n - 1]) : 0;
+  const size_t bxy = ((sizeof(double) * 2 * nv + 255) / 256) * 256;
+  const size_t bvn = ((sizeof(int32_t) * n + 255) / 256) * 256;
+  char* p = nullptr;
+  if (cudaMalloc(&p, bxy + bvn + sizeof(int64_t) * n + 256) != cudaSuccess) { cudaGetLastError(); return GCMFGH_OUT_OF_MEMORY; }
+  c->uploads.push_back(p);
+  cudaMemcpyAsync(p, h->coords, sizeof(double) * 2 * nv, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(p + bxy, h->vnum, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(p + bxy + bvn, h->vps, sizeof(int64_t) * n, cudaMemcpyHostToDevice, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  d->coords = reinterpret_cast<const double*>(p);
+  d->vnum = reinterpret_cast<const int32_t*>(p + bxy);
+  d->vps = reinterpret_cast<const int64_t*>(p + bxy + bvn);
+  d->n_polys = n;
+  d->n_vertices = nv;
+  return GCMFGH_OK;
+}
+
 gcmfgh_status gcmfgh_set_precision(gcmfgh_ctx* c, int mode) {
   if (!c || (mode != GCMFGH_PRECISION_REFERENCE && mode != GCMFGH_PRECISION_EXACT)) return GCMFGH_INVALID_ARGUMENT;
   c->prm.exact = mode == GCMFGH_PRECISION_EXACT;
@@ -318,6 +359,7 @@ gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* c, int key, int64_t value) {
   if (!c || value < 0) return GCMFGH_INVALID_ARGUMENT;
   if (key == GCMFGH_TUNE_BIN_GRID) c->prm.bin_grid = value;
   else if (key == GCMFGH_TUNE_BIG_LABEL) c->prm.big_label_min = value;
+  else if (key == GCMFGH_TUNE_MID_LABEL) c->prm.mid_label_min = value;
   else return GCMFGH_INVALID_ARGUMENT;
   return GCMFGH_OK;
 }
@@ -375,6 +417,21 @@ gcmfgh_status gh_clip_batch(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_l
   cudaSetDevice(c->device);
   c->prm.no_swap = 0;
   return run_clip_ctx(c, b, o, pid, qid, n, info);
+}
+
+gcmfgh_status gh_clip_batch_host_ids(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o,
+                                     const int32_t* pid, const int32_t* qid, int64_t n, gcmfgh_clip_info* info) {
+  if (!c || !layer_ok(b) || !layer_ok(o) || n < 0 || (n > 0 && (!pid || !qid))) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->pair_arena.reset();
+  int32_t* d = c->pair_arena.take_n<int32_t>(2 * std::max<int64_t>(n, 1));
+  if (!d) return GCMFGH_OUT_OF_MEMORY;
+  if (n > 0) {
+    cudaMemcpyAsync(d, pid, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(d + n, qid, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream);
+  }
+  c->prm.no_swap = 0;
+  return run_clip_ctx(c, b, o, d, d + n, n, info);
 }
 
 gcmfgh_status gh_clip_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, gcmfgh_clip_info* info) {

@@ -103,7 +103,7 @@ GCMFGH_DEV void two_prod(double a, double b, double& p, double& e) {
   e = fma(a, b, -p);
 }
 
-static __device__ __noinline__ int exact_sign_slow(double a1, double a0, double b1, double b0, double c1, double c0,
+GCMFGH_DEV int exact_sign_slow(double a1, double a0, double b1, double b0, double c1, double c0,
                                             double d1, double d0, int sub) {
   double ah, al, bh, bl, ch, cl, dh, dl;
   two_sum(a1, -a0, ah, al);
@@ -114,26 +114,30 @@ static __device__ __noinline__ int exact_sign_slow(double a1, double a0, double 
   const double fx[4] = {ah, ah, al, al}, fy[4] = {bh, bl, bh, bl};
   const double gx[4] = {ch, ch, cl, cl}, gy[4] = {dh, dl, dh, dl};
   double h[16];
-  int n = 0;
+#pragma unroll
   for (int t = 0; t < 8; ++t) {
     double p, e;
     if (t < 4) two_prod(fx[t], fy[t], p, e);
     else { two_prod(gx[t - 4], gy[t - 4], p, e); p *= sgn; e *= sgn; }
-    const double parts[2] = {e, p};
+#pragma unroll
     for (int u = 0; u < 2; ++u) {
-      double q = parts[u];
+      double q = u == 0 ? e : p;
+      const int n = 2 * t + u;            // components so far (compile-time after unrolling)
+#pragma unroll
       for (int i = 0; i < n; ++i) {
         double s, r;
         two_sum(q, h[i], s, r);
         h[i] = r;
         q = s;
       }
-      h[n++] = q;
+      h[n] = q;
     }
   }
-  for (int i = n - 1; i >= 0; --i)
-    if (h[i] != 0.0) return h[i] > 0.0 ? 1 : -1;
-  return 0;
+  int sg = 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i)
+    if (h[i] != 0.0) sg = h[i] > 0.0 ? 1 : -1;   // the last nonzero component is the largest
+  return sg;
 }
 
 // sign of (a1-a0)(b1-b0) - (c1-c0)(d1-d0)  (sub = 1)  or  ... + ...  (sub = 0)
@@ -156,9 +160,13 @@ GCMFGH_DEV int orient_exact(double px, double py, double qx, double qy, double r
   return exact_sign(qx, px, ry, py, qy, py, rx, px, 1);
 }
 
+GCMFGH_DEV int orient_exact_call(double px, double py, double qx, double qy, double rx, double ry) {
+  return orient_exact(px, py, qx, qy, rx, ry);
+}
+
 // sign of area2 in the selected mode: the FP64 value's sign, or the exact sign
 GCMFGH_DEV int orient_sign(int exact, double px, double py, double qx, double qy, double rx, double ry) {
-  if (exact) return orient_exact(px, py, qx, qy, rx, ry);
+  if (exact) return orient_exact_call(px, py, qx, qy, rx, ry);
   const double v = area2(px, py, qx, qy, rx, ry);
   return (v > 0.0) - (v < 0.0);
 }
@@ -227,10 +235,21 @@ GCMFGH_DEV int classify_exact(double p1x, double p1y, double p2x, double p2y,
   return tp;
 }
 
+GCMFGH_DEV int classify_exact_call(double p1x, double p1y, double p2x, double p2y, double q1x,
+                                   double q1y, double q2x, double q2y, double* ab) {
+  return classify_exact(p1x, p1y, p2x, p2y, q1x, q1y, q2x, q2y, ab[0], ab[1]);
+}
+
 GCMFGH_DEV int classify_mode(int exact, double p1x, double p1y, double p2x, double p2y, double q1x,
                              double q1y, double q2x, double q2y, double eps, double& alpha, double& beta) {
-  return exact ? classify_exact(p1x, p1y, p2x, p2y, q1x, q1y, q2x, q2y, alpha, beta)
-               : classify_edges(p1x, p1y, p2x, p2y, q1x, q1y, q2x, q2y, eps, alpha, beta);
+  if (exact) {
+    double ab[2] = {alpha, beta};
+    int t = classify_exact_call(p1x, p1y, p2x, p2y, q1x, q1y, q2x, q2y, ab);
+    alpha = ab[0];
+    beta = ab[1];
+    return t;
+  }
+  return classify_edges(p1x, p1y, p2x, p2y, q1x, q1y, q2x, q2y, eps, alpha, beta);
 }
 
 // closed overlap of the two edges' boxes: gppolyclip_mDIV512.cu:345-371

@@ -76,6 +76,7 @@ struct ClipParams {
   int no_swap = 0;            // 1: clip base as P even when it has fewer vertices
   int exact = 0;              // 1: exact orientation/classification signs (eps unused there)
   int64_t bin_grid = 1ll << 24;        // edge-pair grid above which a pair's edges are binned
+  int64_t mid_label_min = 1ll << 13;   // merged-ring slots above which a block labels a pair
   int64_t big_label_min = 1ll << 18;   // merged-ring slots above which a pair is labelled grid-wide
 };
 
@@ -118,8 +119,14 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
                    Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,
                    int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);
 
+// aux: optional second stream (ideally of higher priority); long pairs are labelled on it
+// while the warp-per-pair kernel runs on s.  Without it everything runs on s.
 int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, const int32_t* d_qid,
              int64_t n_pairs, const ClipParams& prm, Arena& arena, ClipDev& out,
-             int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);
+             int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
+             cudaStream_t aux = nullptr);
+
+// a non-blocking stream at the device's highest priority (nullptr on failure)
+cudaStream_t create_priority_stream();
 
 }  // namespace gcmfgh

@@ -159,12 +159,12 @@ struct Records {
   int32_t* k;       // pair
 };
 
-template <int kMode>
+template <int kMode, int kExact>
 __global__ void __launch_bounds__(kThreads)
 intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* __restrict__ chunkOff,
                  int64_t nChunks, const int32_t* __restrict__ cP, const int32_t* __restrict__ cQ,
                  const int64_t* __restrict__ offP, const int64_t* __restrict__ offQ,
-                 const int32_t* __restrict__ LP, const int32_t* __restrict__ LQ, double eps, int exact,
+                 const int32_t* __restrict__ LP, const int32_t* __restrict__ LQ, double eps,
                  int32_t* __restrict__ chunkRec, int32_t* __restrict__ chunkQ,
                  const int64_t* __restrict__ chunkRecOff, const int64_t* __restrict__ recOff, Records R) {
   int64_t c = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
@@ -193,10 +193,10 @@ intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* 
       double2 P1 = __ldg(pv + pe), P2 = __ldg(pv + (pe + 1 < np_ ? pe + 1 : 0));
       double2 Q1 = __ldg(qv + qe), Q2 = __ldg(qv + (qe + 1 < nq_ ? qe + 1 : 0));
       if (edge_boxes_touch(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y)) {
-        tp = classify_mode(exact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
+        tp = classify_mode(kExact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
         if (kMode == 0) {
           double a2, b2;
-          tq = classify_mode(exact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2);
+          tq = classify_mode(kExact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2);
         }
       }
     }
@@ -300,10 +300,10 @@ __global__ void bin_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, 
 
 // mode 0: per P edge, records (P side) and the Q-side count; mode 1: write the records of
 // each P edge at its offset (in cell order: nothing downstream depends on record order).
-template <int kMode>
+template <int kMode, int kExact>
 __global__ void bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LP,
                                  int cp, BinGrid G, const int64_t* __restrict__ cellOff,
-                                 const int32_t* __restrict__ cellList, double eps, int exact,
+                                 const int32_t* __restrict__ cellList, double eps,
                                  int32_t* __restrict__ recCnt,
                                  unsigned long long* __restrict__ qTotal, const int64_t* __restrict__ recPos,
                                  Records R) {
@@ -331,10 +331,10 @@ __global__ void bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k,
         double cx = fmax(pminx, fmin(Q1.x, Q2.x)), cy = fmax(pminy, fmin(Q1.y, Q2.y));
         if (cell_1d(cx, G.x0, G.cw, G.gx) != x || cell_1d(cy, G.y0, G.ch, G.gy) != y) continue;
         double alpha = 0, beta = 0;
-        int tp = classify_mode(exact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
+        int tp = classify_mode(kExact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
         if (kMode == 0) {
           double a2, b2;
-          if (classify_mode(exact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2)) ++qhits;
+          if (classify_mode(kExact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2)) ++qhits;
           if (tp) ++recs;
         } else if (tp) {
           int64_t r = base + recs++;
@@ -722,6 +722,7 @@ __device__ __forceinline__ void insert_after(Ring& R, int v, int after) {
 }
 
 // polygon.h:427-448 (winding parity) over the ring reached from slot 0, skipping `skip`
+template <int EX>
 __device__ bool point_in_ring(const Ring& R, double Rx, double Ry, int skip) {
   int w = 0;
   int one = 0;
@@ -733,9 +734,9 @@ __device__ bool point_in_ring(const Ring& R, double Rx, double Ry, int skip) {
     if ((P0y < Ry) != (P1y < Ry)) {
       if (P0x >= Rx) {
         if (P1x > Rx) w = w + 2 * (P1y > P0y) - 1;
-        else if ((orient_sign(R.exact, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
+        else if ((orient_sign(EX, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
       } else if (P1x > Rx) {
-        if ((orient_sign(R.exact, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
+        if ((orient_sign(EX, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
       }
     }
     one = two;
@@ -744,10 +745,11 @@ __device__ bool point_in_ring(const Ring& R, double Rx, double Ry, int skip) {
 }
 
 // relative position of Q w.r.t. the chain (P1, P2, P3): polyclip.h:297-326
+template <int EX>
 __device__ int rel_position(const Ring& P, const Ring& Q, int qv, int p1, int p2, int p3) {
   if (P.it[p1] && P.nb[p1] == qv) return R_IS_P_M;
   if (P.it[p3] && P.nb[p3] == qv) return R_IS_P_P;
-  const int ex = P.exact;
+  const int ex = EX;
   int s1 = orient_sign(ex, Q.x[qv], Q.y[qv], P.x[p1], P.y[p1], P.x[p2], P.y[p2]);
   int s2 = orient_sign(ex, Q.x[qv], Q.y[qv], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
   int s3 = orient_sign(ex, P.x[p1], P.y[p1], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
@@ -834,6 +836,7 @@ __device__ __forceinline__ void fail(PairCtx& c, int code) {
 // split vertices, tracing through added vertices).
 
 // step 1: initial labels (computed on P, copied to the neighbour on Q)
+template <int EX>
 __device__ void seq_step1(PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
@@ -842,8 +845,8 @@ __device__ void seq_step1(PairCtx& c) {
     int nb = P.nb[s];
     if (nb < 0) continue;
     int pm = P.pv[s], pp = P.nx[s];
-    int a = rel_position(P, Q, Q.pv[nb], pm, s, pp);
-    int b = rel_position(P, Q, Q.nx[nb], pm, s, pp);
+    int a = rel_position<EX>(P, Q, Q.pv[nb], pm, s, pp);
+    int b = rel_position<EX>(P, Q, Q.nx[nb], pm, s, pp);
     int8_t L = initial_label(a, b);
     if (L != L_NONE) { P.lb[s] = L; Q.lb[nb] = L; }
   }
@@ -871,6 +874,7 @@ __device__ void seq_step2(PairCtx& c) {
 }
 
 // step 3.5: components without crossings (polyclip.h:474-541)
+template <int EX>
 __device__ void seq_step35(PairCtx& c) {
   for (int sd = 0; sd < 2; ++sd) {
     Ring& A = c.R[sd];
@@ -895,13 +899,14 @@ __device__ void seq_step35(PairCtx& c) {
     if (v < 0) continue;
     double px = A.x[v], py = A.y[v];
     if (mid) { int n = A.nx[v]; px = 0.5 * (A.x[v] + A.x[n]); py = 0.5 * (A.y[v] + A.y[n]); }
-    bool inside = point_in_ring(B, px, py, -1);
+    bool inside = point_in_ring<EX>(B, px, py, -1);
     if (inside ^ c.uni) push_ring(c.O, A);
   }
   if (c.ident[0] && c.ident[1]) push_ring(c.O, c.R[0]);
 }
 
 // step 4: entry/exit flags (polyclip.h:549-655)
+template <int EX>
 __device__ bool seq_step4(PairCtx& c) {
   for (int sd = 0; sd < 2; ++sd) {
     if (c.noInter[sd]) continue;
@@ -918,7 +923,7 @@ __device__ bool seq_step4(PairCtx& c) {
       V = T;
     }
     // the Q pass sees P's temporary vertex; P's pass cannot see Q's (not yet added)
-    int8_t st = point_in_ring(B, A.x[V], A.y[V], -1) ? E_EXIT : E_ENTRY;
+    int8_t st = point_in_ring<EX>(B, A.x[V], A.y[V], -1) ? E_EXIT : E_ENTRY;
     bool first = true;
     int I = A.nx[V], guard = A.used + 1;
     while (I != V && --guard > 0) {
@@ -949,6 +954,7 @@ __device__ bool seq_step4(PairCtx& c) {
 }
 
 // step 5: split vertex pairs (polyclip.h:661-714)
+template <int EX>
 __device__ bool seq_step5(PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
@@ -961,9 +967,9 @@ __device__ bool seq_step5(PairCtx& c) {
     int vq = add_vertex(Q, Q.x[iq], Q.y[iq]);
     if (vp < 0 || vq < 0) { fail(c, DEV_CAPACITY); return false; }
     bool same;
-    if (P.exact) {
-      same = orient_exact(P.x[P.pv[ip]], P.y[P.pv[ip]], P.x[ip], P.y[ip], P.x[P.nx[ip]], P.y[P.nx[ip]]) *
-             orient_exact(Q.x[Q.pv[iq]], Q.y[Q.pv[iq]], Q.x[iq], Q.y[iq], Q.x[Q.nx[iq]], Q.y[Q.nx[iq]]) > 0;
+    if (EX) {
+      same = orient_exact_call(P.x[P.pv[ip]], P.y[P.pv[ip]], P.x[ip], P.y[ip], P.x[P.nx[ip]], P.y[P.nx[ip]]) *
+             orient_exact_call(Q.x[Q.pv[iq]], Q.y[Q.pv[iq]], Q.x[iq], Q.y[iq], Q.x[Q.nx[iq]], Q.y[Q.nx[iq]]) > 0;
     } else {
       double sP = area2(P.x[P.pv[ip]], P.y[P.pv[ip]], P.x[ip], P.y[ip], P.x[P.nx[ip]], P.y[P.nx[ip]]);
       double sQ = area2(Q.x[Q.pv[iq]], Q.y[Q.pv[iq]], Q.x[iq], Q.y[iq], Q.x[Q.nx[iq]], Q.y[Q.nx[iq]]);
@@ -1085,11 +1091,12 @@ __device__ void seq_cleanup(PairCtx& c, int32_t* outNC, int64_t* outNV) {
 }
 
 // the whole pair from `step` on (1: everything, 2: after the initial labels)
+template <int EX>
 __device__ void seq_pair_from(PairCtx& c, int step, int32_t* outNC, int64_t* outNV) {
-  if (step <= 1) seq_step1(c);
+  if (step <= 1) seq_step1<EX>(c);
   seq_step2(c);
-  seq_step35(c);
-  if (!seq_step4(c) || !seq_step5(c)) return;
+  seq_step35<EX>(c);
+  if (!seq_step4<EX>(c) || !seq_step5<EX>(c)) return;
   seq_step6(c);
   if (!seq_trace(c)) return;
   seq_cleanup(c, outNC, outNV);
@@ -1111,74 +1118,154 @@ __device__ __forceinline__ int wind(double P0x, double P0y, double P1x, double P
   return 0;
 }
 
+// ---- cooperative groups for the parallel labelling and tracing of one pair.  The same
+// code runs with a warp per pair (WarpGroup) or, for pairs with long rings, a whole block
+// per pair (BlockGroup); every member executes every group call (uniform control flow).
+struct WarpGroup {
+  __device__ __forceinline__ int rank() const { return (int)lane_id(); }
+  __device__ __forceinline__ int size() const { return 32; }
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+  __device__ __forceinline__ bool all(bool v) const { return __all_sync(kFull, v); }
+  __device__ __forceinline__ bool any(bool v) const { return __any_sync(kFull, v); }
+  __device__ __forceinline__ int sum(int v) const { return warp_sum(v); }
+  template <class T>
+  __device__ __forceinline__ T bcast0(T v) const { return __shfl_sync(kFull, v, 0); }
+  // smallest member index whose flag is set, -1 if none
+  __device__ __forceinline__ int first(bool hit) const {
+    unsigned m = __ballot_sync(kFull, hit);
+    return m ? __ffs(m) - 1 : -1;
+  }
+  __device__ __forceinline__ int incl_scan(int v, int& total) const {
+    int x = warp_incl_scan(v);
+    total = __shfl_sync(kFull, x, 31);
+    return x;
+  }
+};
+
+// Block-wide versions over shared scratch (kBlockLabelThreads / 32 warps); each call
+// begins with a barrier so the scratch of the previous call is free.
+constexpr int kBlockLabelThreads = 256;
+struct BlockGroup {
+  long long* sm;        // kBlockLabelThreads / 32 + 1 entries
+  __device__ __forceinline__ int rank() const { return (int)threadIdx.x; }
+  __device__ __forceinline__ int size() const { return kBlockLabelThreads; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  __device__ __forceinline__ bool all(bool v) const { return __syncthreads_and(v) != 0; }
+  __device__ __forceinline__ bool any(bool v) const { return __syncthreads_or(v) != 0; }
+  __device__ __forceinline__ int sum(int v) const {
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane_id() == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    long long t = 0;
+    for (int w = 0; w < kBlockLabelThreads / 32; ++w) t += sm[w];
+    return (int)t;
+  }
+  template <class T>
+  __device__ __forceinline__ T bcast0(T v) const {
+    static_assert(sizeof(T) <= sizeof(long long), "bcast0: scalar types only");
+    __syncthreads();
+    if (threadIdx.x == 0) { long long x = 0; memcpy(&x, &v, sizeof(T)); sm[kBlockLabelThreads / 32] = x; }
+    __syncthreads();
+    long long x = sm[kBlockLabelThreads / 32];
+    T r;
+    memcpy(&r, &x, sizeof(T));
+    return r;
+  }
+  __device__ __forceinline__ int first(bool hit) const {
+    unsigned m = __ballot_sync(kFull, hit);
+    __syncthreads();
+    if (lane_id() == 0) sm[threadIdx.x >> 5] = m ? (long long)((threadIdx.x & ~31u) + __ffs(m) - 1) : -1;
+    __syncthreads();
+    for (int w = 0; w < kBlockLabelThreads / 32; ++w)
+      if (sm[w] >= 0) return (int)sm[w];
+    return -1;
+  }
+  __device__ __forceinline__ int incl_scan(int v, int& total) const {
+    int x = warp_incl_scan(v);
+    __syncthreads();
+    if (lane_id() == 31) sm[threadIdx.x >> 5] = x;
+    __syncthreads();
+    long long before = 0, all = 0;
+    const int me = (int)(threadIdx.x >> 5);
+    for (int w = 0; w < kBlockLabelThreads / 32; ++w) { if (w < me) before += sm[w]; all += sm[w]; }
+    total = (int)all;
+    return (int)(before + x);
+  }
+};
+
 // polygon.h:427-448 over ring B in slot order; `after`/`T`: a temporary vertex T inserted
 // after slot `after` (or -1)
-__device__ bool warp_point_in_ring(const Ring& B, double Rx, double Ry, int after, int T) {
+template <int EX, class G>
+__device__ bool grp_point_in_ring(const G& g, const Ring& B, double Rx, double Ry, int after, int T) {
   int w = 0;
-  for (int s = lane_id(); s < B.m; s += 32) {
+  for (int s = g.rank(); s < B.m; s += g.size()) {
     int n = (s + 1 < B.m) ? s + 1 : 0;
     if (s == after) {
-      w += wind(B.x[s], B.y[s], B.x[T], B.y[T], Rx, Ry, B.exact);
-      w += wind(B.x[T], B.y[T], B.x[n], B.y[n], Rx, Ry, B.exact);
+      w += wind(B.x[s], B.y[s], B.x[T], B.y[T], Rx, Ry, EX);
+      w += wind(B.x[T], B.y[T], B.x[n], B.y[n], Rx, Ry, EX);
     } else {
-      w += wind(B.x[s], B.y[s], B.x[n], B.y[n], Rx, Ry, B.exact);
+      w += wind(B.x[s], B.y[s], B.x[n], B.y[n], Rx, Ry, EX);
     }
   }
-  w = warp_sum(w);
+  w = g.sum(w);
   return (w % 2) != 0;
 }
 
 // first slot s >= from (slot order, s < n) where pred(s); n if none
-template <class F>
-__device__ int warp_find_first(int from, int n, F pred) {
-  for (int b = from; b < n; b += 32) {
-    int s = b + lane_id();
-    unsigned m = __ballot_sync(kFull, s < n && pred(s));
-    if (m) return b + __ffs(m) - 1;
+template <class G, class F>
+__device__ int grp_find_first(const G& g, int from, int n, F pred) {
+  for (int b = from; b < n; b += g.size()) {
+    int s = b + g.rank();
+    int f = g.first(s < n && pred(s));
+    if (f >= 0) return b + f;
   }
   return n;
 }
 
-__device__ bool warp_links_one_to_one(const Ring& P, const Ring& Q) {
+template <class G>
+__device__ bool grp_links_one_to_one(const G& g, const Ring& P, const Ring& Q) {
   bool ok = true;
-  for (int s = lane_id(); s < P.m; s += 32)
+  for (int s = g.rank(); s < P.m; s += g.size())
     if (P.it[s]) { int nb = P.nb[s]; if (nb < 0 || nb >= Q.m || Q.nb[nb] != s) ok = false; }
-  for (int s = lane_id(); s < Q.m; s += 32)
+  for (int s = g.rank(); s < Q.m; s += g.size())
     if (Q.it[s]) { int nb = Q.nb[s]; if (nb < 0 || nb >= P.m || P.nb[nb] != s) ok = false; }
-  return __all_sync(kFull, ok);
+  return g.all(ok);
 }
 
-__device__ void warp_step1(PairCtx& c) {
+template <int EX, class G>
+__device__ void grp_step1(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
-  for (int s = lane_id(); s < P.m; s += 32) {
+  for (int s = g.rank(); s < P.m; s += g.size()) {
     if (!P.it[s]) continue;
     int nb = P.nb[s];
     int pm = (s > 0) ? s - 1 : P.m - 1, pp = (s + 1 < P.m) ? s + 1 : 0;
-    int a = rel_position(P, Q, (nb > 0) ? nb - 1 : Q.m - 1, pm, s, pp);
-    int b = rel_position(P, Q, (nb + 1 < Q.m) ? nb + 1 : 0, pm, s, pp);
+    int a = rel_position<EX>(P, Q, (nb > 0) ? nb - 1 : Q.m - 1, pm, s, pp);
+    int b = rel_position<EX>(P, Q, (nb + 1 < Q.m) ? nb + 1 : 0, pm, s, pp);
     int8_t L = initial_label(a, b);
     if (L != L_NONE) { P.lb[s] = L; Q.lb[nb] = L; }
   }
-  __syncwarp();
+  g.sync();
 }
 
 // Chains run from a LEFT_ON/RIGHT_ON vertex over ON_ON vertices to an ON_LEFT/ON_RIGHT
 // vertex.  When every chain ends so, chains are disjoint and can be resolved in parallel
 // with the sequential result; otherwise returns false and nothing is changed.
-__device__ bool warp_step2(PairCtx& c) {
+template <class G>
+__device__ bool grp_step2(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
   const int m = P.m;
   bool ok = true;
-  for (int s = lane_id(); s < m; s += 32) {
+  for (int s = g.rank(); s < m; s += g.size()) {
     if (!P.it[s] || (P.lb[s] != L_LEFT_ON && P.lb[s] != L_RIGHT_ON)) continue;
     int I = (s + 1 < m) ? s + 1 : 0, guard = m;
     while (P.lb[I] == L_ON_ON && --guard > 0) I = (I + 1 < m) ? I + 1 : 0;
     if ((P.lb[I] != L_ON_LEFT && P.lb[I] != L_ON_RIGHT) || !P.it[I]) ok = false;
   }
-  if (!__all_sync(kFull, ok)) return false;
-  for (int s = lane_id(); s < m; s += 32) {
+  if (!g.all(ok)) return false;
+  for (int s = g.rank(); s < m; s += g.size()) {
     int8_t l0 = P.lb[s];
     if (!P.it[s] || (l0 != L_LEFT_ON && l0 != L_RIGHT_ON)) continue;
     int x = l0 == L_LEFT_ON ? R_LEFT : R_RIGHT;
@@ -1194,31 +1281,33 @@ __device__ bool warp_step2(PairCtx& c) {
     P.lb[s] = ct; P.lb[I] = ct;
     Q.lb[P.nb[s]] = ct; Q.lb[P.nb[I]] = ct;
   }
-  __syncwarp();
+  g.sync();
   return true;
 }
 
 // copies ring A (slot order, no added vertices) as one output component
-__device__ void warp_push_ring(OutRegion& O, const Ring& A) {
+template <class G>
+__device__ void grp_push_ring(const G& g, OutRegion& O, const Ring& A) {
   O.begin();
   if (O.overflow) return;
   if (O.nv + A.m > O.vcap) { O.overflow = true; return; }
-  for (int s = lane_id(); s < A.m; s += 32) { O.xy[2 * (O.nv + s)] = A.x[s]; O.xy[2 * (O.nv + s) + 1] = A.y[s]; }
-  if (lane_id() == 0) O.csz[O.nc] = A.m;
+  for (int s = g.rank(); s < A.m; s += g.size()) { O.xy[2 * (O.nv + s)] = A.x[s]; O.xy[2 * (O.nv + s) + 1] = A.y[s]; }
+  if (g.rank() == 0) O.csz[O.nc] = A.m;
   O.nv += A.m;
   O.end();
-  __syncwarp();
+  g.sync();
 }
 
 // first non-intersection slot (slot order = ring order before any insertion), else the
 // first vertex whose edge to the next one is not collinear with the other polygon
 // (polygon.h:480-512); returns -1 if none
-__device__ int warp_first_non_intersection(const Ring& A, const Ring& B, bool& mid) {
+template <class G>
+__device__ int grp_first_non_intersection(const G& g, const Ring& A, const Ring& B, bool& mid) {
   mid = false;
-  int v = warp_find_first(0, A.m, [&](int s) { return !A.it[s]; });
+  int v = grp_find_first(g, 0, A.m, [&](int s) { return !A.it[s]; });
   if (v < A.m) return v;
   // B's own links: B may already hold its temporary vertex when A is Q
-  v = warp_find_first(0, A.m, [&](int s) {
+  v = grp_find_first(g, 0, A.m, [&](int s) {
     int nb = A.nb[s], nx = A.nx[s];
     return nb >= 0 && A.nb[nx] != B.pv[nb] && A.nb[nx] != B.nx[nb];
   });
@@ -1226,11 +1315,12 @@ __device__ int warp_first_non_intersection(const Ring& A, const Ring& B, bool& m
   return -1;
 }
 
-__device__ void warp_step35(PairCtx& c) {
+template <int EX, class G>
+__device__ void grp_step35(const G& g, PairCtx& c) {
   for (int sd = 0; sd < 2; ++sd) {
     Ring& A = c.R[sd];
     bool none = true, allOn = true;
-    for (int v = lane_id(); v < A.m; v += 32) {
+    for (int v = g.rank(); v < A.m; v += g.size()) {
       int8_t l = A.lb[v];
       if (l != L_ON_ON) allOn = false;
       if (A.it[v]) {
@@ -1238,8 +1328,8 @@ __device__ void warp_step35(PairCtx& c) {
         if (c.uni && (l == L_BOUNCING || l == L_DELAYED_BOUNCING)) none = false;
       }
     }
-    none = __all_sync(kFull, none);
-    allOn = __all_sync(kFull, allOn);
+    none = g.all(none);
+    allOn = g.all(allOn);
     c.noInter[sd] = none;
     c.ident[sd] = none && allOn;
   }
@@ -1248,21 +1338,22 @@ __device__ void warp_step35(PairCtx& c) {
     Ring& A = c.R[sd];
     Ring& B = c.R[1 - sd];
     bool mid;
-    int v = warp_first_non_intersection(A, B, mid);
+    int v = grp_first_non_intersection(g, A, B, mid);
     if (v < 0) continue;
     double px = A.x[v], py = A.y[v];
     if (mid) { int n = (v + 1 < A.m) ? v + 1 : 0; px = 0.5 * (A.x[v] + A.x[n]); py = 0.5 * (A.y[v] + A.y[n]); }
-    bool inside = warp_point_in_ring(B, px, py, -1, -1);
-    if (inside ^ c.uni) warp_push_ring(c.O, A);
+    bool inside = grp_point_in_ring<EX>(g, B, px, py, -1, -1);
+    if (inside ^ c.uni) grp_push_ring(g, c.O, A);
   }
-  if (c.ident[0] && c.ident[1]) warp_push_ring(c.O, c.R[0]);
+  if (c.ident[0] && c.ident[1]) grp_push_ring(g, c.O, c.R[0]);
 }
 
 // Entry/exit flags as a warp prefix scan over the ring from the start vertex: the status
 // at a vertex is the start status toggled once per earlier CROSSING, DELAYED_BOUNCING and
 // second-of-a-chain DELAYED_CROSSING; "first chain vertex" alternates over the DELAYED
 // vertices met (polyclip.h:582-653).
-__device__ bool warp_step4(PairCtx& c, int tempAfter[2], int tempSlot[2]) {
+template <int EX, class G>
+__device__ bool grp_step4(const G& g, PairCtx& c, int tempAfter[2], int tempSlot[2]) {
   for (int sd = 0; sd < 2; ++sd) {
     tempAfter[sd] = -1;
     tempSlot[sd] = -1;
@@ -1272,32 +1363,32 @@ __device__ bool warp_step4(PairCtx& c, int tempAfter[2], int tempSlot[2]) {
     Ring& A = c.R[sd];
     Ring& B = c.R[1 - sd];
     bool mid;
-    int V0 = warp_first_non_intersection(A, B, mid);
+    int V0 = grp_first_non_intersection(g, A, B, mid);
     if (V0 < 0) continue;
     double qx = A.x[V0], qy = A.y[V0];
     if (mid) {
       int T = -1;
-      if (lane_id() == 0) {
+      if (g.rank() == 0) {
         T = add_vertex(A, 0.5 * (A.x[V0] + A.x[(V0 + 1 < A.m) ? V0 + 1 : 0]),
                        0.5 * (A.y[V0] + A.y[(V0 + 1 < A.m) ? V0 + 1 : 0]));
         if (T >= 0) insert_after(A, T, V0);
       }
-      T = __shfl_sync(kFull, T, 0);
-      A.used = __shfl_sync(kFull, A.used, 0);
-      __syncwarp();
-      if (T < 0) { if (lane_id() == 0) fail(c, DEV_CAPACITY); return false; }
+      T = g.bcast0(T);
+      A.used = g.bcast0(A.used);
+      g.sync();
+      if (T < 0) { if (g.rank() == 0) fail(c, DEV_CAPACITY); return false; }
       tempAfter[sd] = V0;
       tempSlot[sd] = T;
       qx = A.x[T];
       qy = A.y[T];
     }
     // the Q pass tests against P's ring including P's temporary vertex
-    int8_t st0 = (sd == 1 ? warp_point_in_ring(B, qx, qy, tempAfter[0], tempSlot[0])
-                          : warp_point_in_ring(B, qx, qy, -1, -1)) ? E_EXIT : E_ENTRY;
+    int8_t st0 = (sd == 1 ? grp_point_in_ring<EX>(g, B, qx, qy, tempAfter[0], tempSlot[0])
+                          : grp_point_in_ring<EX>(g, B, qx, qy, -1, -1)) ? E_EXIT : E_ENTRY;
     int carryD = 0, carryT = 0;
     const int m = A.m;
-    for (int b = 0; b < m; b += 32) {
-      int j = b + lane_id();
+    for (int b = 0; b < m; b += g.size()) {
+      int j = b + g.rank();
       int s = -1;
       int8_t L = L_NONE;
       bool inter = false;
@@ -1308,10 +1399,11 @@ __device__ bool warp_step4(PairCtx& c, int tempAfter[2], int tempSlot[2]) {
         L = inter ? A.lb[s] : L_NONE;
       }
       int d = inter && (L == L_DELAYED_CROSSING || L == L_DELAYED_BOUNCING);
-      int dIncl = warp_incl_scan(d);
+      int dTot, tTot;
+      int dIncl = g.incl_scan(d, dTot);
       bool first = ((carryD + dIncl - d) & 1) == 0;
       int t = inter && (L == L_CROSSING || L == L_DELAYED_BOUNCING || (L == L_DELAYED_CROSSING && !first));
-      int tIncl = warp_incl_scan(t);
+      int tIncl = g.incl_scan(t, tTot);
       int8_t st = ((carryT + tIncl - t) & 1) ? toggled(st0) : st0;
       if (inter) {
         if (L == L_CROSSING) A.ee[s] = st;
@@ -1326,71 +1418,74 @@ __device__ bool warp_step4(PairCtx& c, int tempAfter[2], int tempSlot[2]) {
           else if ((st == E_ENTRY) ^ c.uni) A.fl[s] |= 2;
         }
       }
-      carryD += __shfl_sync(kFull, dIncl, 31);
-      carryT += __shfl_sync(kFull, tIncl, 31);
+      carryD += dTot;
+      carryT += tTot;
     }
-    __syncwarp();
+    g.sync();
   }
   return true;
 }
 
-__device__ bool warp_any_split(const Ring& P, const Ring& Q) {
+template <class G>
+__device__ bool grp_any_split(const G& g, const Ring& P, const Ring& Q) {
   bool any = false;
-  for (int s = lane_id(); s < P.m; s += 32)
+  for (int s = g.rank(); s < P.m; s += g.size())
     if (P.fl[s] & 1) { int nb = P.nb[s]; if (nb >= 0 && (Q.fl[nb] & 1)) any = true; }
-  return __any_sync(kFull, any);
+  return g.any(any);
 }
 
-__device__ void warp_step6(PairCtx& c) {
+template <class G>
+__device__ void grp_step6(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
-  for (int ip = lane_id(); ip < P.m; ip += 32) {
+  for (int ip = g.rank(); ip < P.m; ip += g.size()) {
     if (!(P.fl[ip] & 2)) continue;
     int iq = P.nb[ip];
     if (iq >= 0 && (Q.fl[iq] & 2)) { P.lb[ip] = L_CROSSING; Q.lb[iq] = L_CROSSING; }
   }
-  __syncwarp();
+  g.sync();
 }
 
 // Tracing when neither ring has added vertices (rings in slot order): each run from V to
 // the next vertex with the target entry/exit flag (or back at the start) is found with a
 // warp ballot and copied with coalesced stores.
-__device__ bool warp_trace(PairCtx& c) {
+template <class G>
+__device__ bool grp_trace(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
   OutRegion& O = c.O;
   long long budget = 4ll * (c.R[0].used + c.R[1].used) + 16;
   int from = 0;
   for (;;) {
-    int I = warp_find_first(from, P.m, [&](int s) { return P.it[s] && P.lb[s] == L_CROSSING; });
+    int I = grp_find_first(g, from, P.m, [&](int s) { return P.it[s] && P.lb[s] == L_CROSSING; });
     if (I >= P.m) break;
     O.begin();
-    if (O.overflow) { if (lane_id() == 0) fail(c, DEV_CAPACITY); return false; }
+    if (O.overflow) { if (g.rank() == 0) fail(c, DEV_CAPACITY); return false; }
     int side = 0, V = I;
-    if (lane_id() == 0) P.it[V] = 0;
-    __syncwarp();
+    if (g.rank() == 0) P.it[V] = 0;
+    g.sync();
     do {
       Ring& C = c.R[side];
       const int m = C.m;
       int8_t st = toggled(C.ee[V]);
       const int dir = ((st == E_EXIT) ^ c.uni) ? 1 : -1;
       int L = -1;
-      for (int j0 = 1; j0 <= m && L < 0; j0 += 32) {
-        int j = j0 + lane_id();
+      for (int j0 = 1; j0 <= m && L < 0; j0 += g.size()) {
+        int j = j0 + g.rank();
         bool hit = false;
         if (j <= m) {
           int w = V + dir * (j % m);
           w = (w % m + m) % m;
           hit = (C.ee[w] == st) || (side == 0 && w == I);
         }
-        unsigned msk = __ballot_sync(kFull, hit);
-        if (msk) L = j0 + __ffs(msk) - 1;
+        int f = g.first(hit);
+        if (f >= 0) L = j0 + f;
       }
-      if (L < 0) { if (lane_id() == 0) fail(c, DEV_TRACE); return false; }
+      if (L < 0) { if (g.rank() == 0) fail(c, DEV_TRACE); return false; }
       budget -= L;
-      if (budget < 0) { if (lane_id() == 0) fail(c, DEV_TRACE); return false; }
-      if (O.nv + L > O.vcap) { if (lane_id() == 0) fail(c, DEV_CAPACITY); return false; }
-      for (int j0 = 1; j0 <= L; j0 += 32) {
-        int j = j0 + lane_id();
+      if (budget < 0) { if (g.rank() == 0) fail(c, DEV_TRACE); return false; }
+      if (O.nv + L > O.vcap) { if (g.rank() == 0) fail(c, DEV_CAPACITY); return false; }
+      for (int j0 = 1; j0 <= L; j0 += g.size()) {
+        int j = j0 + g.rank();
         if (j <= L) {
           int w = V + dir * (j % m);
           w = (w % m + m) % m;
@@ -1400,17 +1495,17 @@ __device__ bool warp_trace(PairCtx& c) {
         }
       }
       O.nv += L;
-      if (lane_id() == 0) O.csz[O.nc] += L;
+      if (g.rank() == 0) O.csz[O.nc] += L;
       int W = V + dir * (L % m);
       V = (W % m + m) % m;
-      __syncwarp();
+      g.sync();
       if (!(side == 0 && V == I)) {
         int nb = C.nb[V];
-        if (nb < 0) { if (lane_id() == 0) fail(c, DEV_TRACE); return false; }
+        if (nb < 0) { if (g.rank() == 0) fail(c, DEV_TRACE); return false; }
         V = nb;
         side = 1 - side;
-        if (lane_id() == 0) c.R[side].it[V] = 0;
-        __syncwarp();
+        if (g.rank() == 0) c.R[side].it[V] = 0;
+        g.sync();
       }
     } while (!(side == 0 && V == I));
     O.end();
@@ -1422,7 +1517,8 @@ __device__ bool warp_trace(PairCtx& c) {
 // Clean-up: a component where no vertex is collinear with its two ring neighbours keeps
 // every vertex (the sequential pass would remove nothing), so it is only moved into place;
 // any other component is cleaned by one lane with the sequential pass.
-__device__ void warp_cleanup(PairCtx& c, int32_t* outNC, int64_t* outNV) {
+template <class G>
+__device__ void grp_cleanup(const G& g, PairCtx& c, int32_t* outNC, int64_t* outNV) {
   OutRegion& O = c.O;
   int64_t vin = 0, vout = 0;
   int nc = 0;
@@ -1431,109 +1527,186 @@ __device__ void warp_cleanup(PairCtx& c, int32_t* outNC, int64_t* outNV) {
     const double* src = O.xy + 2 * vin;
     double* dst = O.xy + 2 * vout;
     bool flag = false;
-    for (int j = lane_id(); j < n; j += 32) {
+    for (int j = g.rank(); j < n; j += g.size()) {
       int p = (j > 0) ? j - 1 : n - 1, q = (j + 1 < n) ? j + 1 : 0;
       if (fabs(area2(src[2 * p], src[2 * p + 1], src[2 * j], src[2 * j + 1], src[2 * q], src[2 * q + 1])) <
           c.eps_clean)
         flag = true;
     }
-    flag = __any_sync(kFull, flag);
+    flag = g.any(flag);
     int kept;
     if (!flag) {
       if (dst != src) {
-        for (int b = 0; b < 2 * n; b += 32) {
-          int i = b + lane_id();
+        for (int b = 0; b < 2 * n; b += g.size()) {
+          int i = b + g.rank();
           double v = (i < 2 * n) ? src[i] : 0.0;
-          __syncwarp();
+          g.sync();
           if (i < 2 * n) dst[i] = v;
         }
       }
       kept = n;
     } else {
       kept = 0;
-      if (lane_id() == 0) kept = seq_cleanup_component(src, dst, n, c.eps_clean);
-      kept = __shfl_sync(kFull, kept, 0);
+      if (g.rank() == 0) kept = seq_cleanup_component(src, dst, n, c.eps_clean);
+      kept = g.bcast0(kept);
     }
-    __syncwarp();
+    g.sync();
     vin += n;
     if (kept == 0) continue;
-    if (lane_id() == 0) O.csz[nc] = kept;
+    if (g.rank() == 0) O.csz[nc] = kept;
     ++nc;
     vout += kept;
-    __syncwarp();
+    g.sync();
   }
-  if (lane_id() == 0) { *outNC = nc; *outNV = vout; }
+  if (g.rank() == 0) { *outNC = nc; *outNV = vout; }
 }
 
-// One warp per pair.  The warp phases give the sequential result whenever neighbour links
-// are one-to-one (then labels written through a link never collide) and chains are well
-// formed; otherwise lane 0 runs the sequential phases from the first one that could differ.
-__global__ void __launch_bounds__(128)
-label_trace_kernel(PairDev D, int64_t K, const int32_t* __restrict__ mP, const int32_t* __restrict__ mQ,
-                   const int64_t* __restrict__ regP, const int64_t* __restrict__ regQ,
-                   const int64_t* __restrict__ regSizeP, const int64_t* __restrict__ regSizeQ,
-                   RingSet SP, RingSet SQ, double* __restrict__ outXY, const int64_t* __restrict__ outVOff,
-                   const int64_t* __restrict__ outVCap, int32_t* __restrict__ outCsz,
-                   const int64_t* __restrict__ outCOff, const int32_t* __restrict__ outCCap,
-                   int32_t* __restrict__ outNC, int64_t* __restrict__ outNV, ClipParams prm, int* err,
-                   int64_t bigLabelMin) {
-  int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (k >= K) return;
-  const bool lane0 = lane_id() == 0;
-  if (lane0) { outNC[k] = 0; outNV[k] = 0; }
-  if (D.status[k] != 0) return;
-  if ((int64_t)mP[k] + mQ[k] > bigLabelMin) return;      // the grid path handles this pair
-  PairCtx c;
-  c.R[0] = ring_of(SP, regP[k], mP[k], (int)regSizeP[k]);
-  c.R[1] = ring_of(SQ, regQ[k], mQ[k], (int)regSizeQ[k]);
-  c.O.xy = outXY + 2 * outVOff[k]; c.O.csz = outCsz + outCOff[k]; c.O.vcap = outVCap[k]; c.O.ccap = outCCap[k];
-  c.O.nv = 0; c.O.nc = 0; c.O.overflow = false;
-  c.uni = prm.union_mode != 0;
-  c.eps_clean = prm.eps_clean;
-  c.err = err;
-  c.status = D.status + k;
-  c.noInter[0] = c.noInter[1] = c.ident[0] = c.ident[1] = false;
+// Pulls a pair's ring arrays into L1 in one burst, one request per 128-byte line, so the
+// labelling phases (each of which touches some of the arrays first) do not pay a DRAM
+// round trip each.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 
-  if (!warp_links_one_to_one(c.R[0], c.R[1])) {
-    if (lane0) seq_pair_from(c, 1, outNC + k, outNV + k);
+template <class G>
+__device__ void prefetch_ring(const G& g, const Ring& R) {
+  for (int s = g.rank() * 16; s < R.m; s += g.size() * 16) {
+    prefetch_l1(R.x + s);
+    prefetch_l1(R.y + s);
+    if ((s & 31) == 0) { prefetch_l1(R.nx + s); prefetch_l1(R.pv + s); prefetch_l1(R.nb + s); }
+    if ((s & 127) == 0) { prefetch_l1(R.it + s); prefetch_l1(R.lb + s); prefetch_l1(R.ee + s); prefetch_l1(R.fl + s); }
+  }
+}
+
+// Arguments of the labelling kernels (one struct so the warp and block kernels agree).
+struct LabelArgs {
+  PairDev D;
+  int64_t K;
+  const int32_t* mP; const int32_t* mQ;
+  const int64_t* regP; const int64_t* regQ;
+  const int64_t* regSizeP; const int64_t* regSizeQ;
+  RingSet SP, SQ;
+  double* outXY; const int64_t* outVOff; const int64_t* outVCap;
+  int32_t* outCsz; const int64_t* outCOff; const int32_t* outCCap;
+  int32_t* outNC; int64_t* outNV;
+  ClipParams prm;
+  int* err;
+  int64_t midLabelMin;        // rings above: a block per pair
+  int64_t bigLabelMin;        // rings above: the grid path
+  const int64_t* midList;     // pairs for the block kernel
+  const unsigned long long* midCount;
+  unsigned long long* midNext; // work-stealing cursor of the block kernel
+};
+
+// One pair labelled and traced by group g.  The group phases give the sequential result
+// whenever neighbour links are one-to-one (then labels written through a link never
+// collide) and chains are well formed; otherwise member 0 runs the sequential phases from
+// the first one that could differ.
+template <int EX, class G>
+__device__ void label_trace_pair(const G& g, const LabelArgs& a, int64_t k) {
+  const bool lead = g.rank() == 0;
+  int32_t* outNC = a.outNC + k;
+  int64_t* outNV = a.outNV + k;
+  PairCtx c;
+  c.R[0] = ring_of(a.SP, a.regP[k], a.mP[k], (int)a.regSizeP[k]);
+  c.R[1] = ring_of(a.SQ, a.regQ[k], a.mQ[k], (int)a.regSizeQ[k]);
+  c.O.xy = a.outXY + 2 * a.outVOff[k]; c.O.csz = a.outCsz + a.outCOff[k];
+  c.O.vcap = a.outVCap[k]; c.O.ccap = a.outCCap[k];
+  c.O.nv = 0; c.O.nc = 0; c.O.overflow = false;
+  c.uni = a.prm.union_mode != 0;
+  c.eps_clean = a.prm.eps_clean;
+  c.err = a.err;
+  c.status = a.D.status + k;
+  c.noInter[0] = c.noInter[1] = c.ident[0] = c.ident[1] = false;
+  prefetch_ring(g, c.R[0]);
+  prefetch_ring(g, c.R[1]);
+
+  if (!grp_links_one_to_one(g, c.R[0], c.R[1])) {
+    if (lead) seq_pair_from<EX>(c, 1, outNC, outNV);
+    g.sync();
     return;
   }
-  warp_step1(c);
-  if (!warp_step2(c)) {
-    if (lane0) seq_pair_from(c, 2, outNC + k, outNV + k);
+  grp_step1<EX>(g, c);
+  if (!grp_step2(g, c)) {
+    if (lead) seq_pair_from<EX>(c, 2, outNC, outNV);
+    g.sync();
     return;
   }
-  warp_step35(c);
+  grp_step35<EX>(g, c);
   int tempAfter[2], tempSlot[2];
-  if (!warp_step4(c, tempAfter, tempSlot)) return;
-  if (warp_any_split(c.R[0], c.R[1])) {
+  if (!grp_step4<EX>(g, c, tempAfter, tempSlot)) return;
+  if (grp_any_split(g, c.R[0], c.R[1])) {
     bool ok = true;
-    if (lane0) ok = seq_step5(c);
-    ok = __shfl_sync(kFull, (int)ok, 0);
-    c.R[0].used = __shfl_sync(kFull, c.R[0].used, 0);
-    c.R[1].used = __shfl_sync(kFull, c.R[1].used, 0);
-    __syncwarp();
+    if (lead) ok = seq_step5<EX>(c);
+    ok = g.bcast0((int)ok);
+    c.R[0].used = g.bcast0(c.R[0].used);
+    c.R[1].used = g.bcast0(c.R[1].used);
+    g.sync();
     if (!ok) return;
   }
-  warp_step6(c);
+  grp_step6(g, c);
   const bool added = c.R[0].used != c.R[0].m || c.R[1].used != c.R[1].m;
   if (added) {
-    // vertices were added to a ring: trace through the next/prev links on one lane
+    // vertices were added to a ring: trace through the next/prev links on one member
     int ok = 1;
-    if (lane0) ok = seq_trace(c) ? 1 : 0;
-    ok = __shfl_sync(kFull, ok, 0);
-    c.O.nv = __shfl_sync(kFull, (long long)c.O.nv, 0);
-    c.O.nc = __shfl_sync(kFull, c.O.nc, 0);
-    __syncwarp();
+    if (lead) ok = seq_trace(c) ? 1 : 0;
+    ok = g.bcast0(ok);
+    c.O.nv = g.bcast0((long long)c.O.nv);
+    c.O.nc = g.bcast0(c.O.nc);
+    c.O.overflow = g.bcast0((int)c.O.overflow) != 0;
+    g.sync();
     if (!ok) return;
-  } else if (!warp_trace(c)) {
+  } else if (!grp_trace(g, c)) {
     return;
   }
   if (c.O.overflow) {
-    if (lane0) fail(c, DEV_CAPACITY);
+    if (lead) fail(c, DEV_CAPACITY);
     return;
   }
-  warp_cleanup(c, outNC + k, outNV + k);
+  grp_cleanup(g, c, outNC, outNV);
+}
+
+// A warp per pair for pairs whose merged rings have at most midLabelMin slots.
+template <int EX>
+__global__ void __launch_bounds__(128)
+label_trace_kernel(LabelArgs a) {
+  int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (k >= a.K) return;
+  if (a.D.status[k] != 0) return;
+  const int64_t slots = (int64_t)a.mP[k] + a.mQ[k];
+  if (slots > a.midLabelMin) return;                       // block or grid path
+  WarpGroup g;
+  label_trace_pair<EX>(g, a, k);
+}
+
+// Pairs with midLabelMin < slots <= bigLabelMin: persistent blocks take pairs from the
+// list through an atomic cursor (work stealing), one block of kBlockLabelThreads per pair.
+template <int EX>
+__global__ void __launch_bounds__(kBlockLabelThreads)
+label_trace_block_kernel(LabelArgs a) {
+  __shared__ long long sm[kBlockLabelThreads / 32 + 1];
+  __shared__ long long next;
+  BlockGroup g{sm};
+  const unsigned long long n = *a.midCount;
+  for (;;) {
+    if (threadIdx.x == 0) next = (long long)atomicAdd(a.midNext, 1ull);
+    __syncthreads();
+    const long long i = next;
+    __syncthreads();
+    if (i >= (long long)n) return;
+    label_trace_pair<EX>(g, a, a.midList[i]);
+    __syncthreads();
+  }
+}
+
+// pairs for the block kernel (order does not matter: each pair has its own output region)
+__global__ void mid_label_list_kernel(const int32_t* __restrict__ mP, const int32_t* __restrict__ mQ,
+                                      const int32_t* __restrict__ status, int64_t K, int64_t midMin, int64_t bigMin,
+                                      int64_t* __restrict__ list, unsigned long long* __restrict__ n) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K || status[k] != 0) return;
+  const int64_t slots = (int64_t)mP[k] + mQ[k];
+  if (slots > midMin && slots <= bigMin) list[atomicAdd(n, 1ull)] = k;
 }
 
 // ================================================================ grid path for huge pairs
@@ -1585,14 +1758,15 @@ __global__ void big_links_kernel(RingSet SP, RingSet SQ, BigPair bp, BigFlags* f
   }
 }
 
+template <int EX>
 __global__ void big_step1_kernel(RingSet SP, RingSet SQ, BigPair bp) {
   Ring P = big_ring(SP, bp.regP, bp.mP, bp.capP, bp.mP), Q = big_ring(SQ, bp.regQ, bp.mQ, bp.capQ, bp.mQ);
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P.m; s += gridDim.x * blockDim.x) {
     if (!P.it[s]) continue;
     int nb = P.nb[s];
     int pm = prv_slot(s, P.m), pp = nxt_slot(s, P.m);
-    int a = rel_position(P, Q, prv_slot(nb, Q.m), pm, s, pp);
-    int b = rel_position(P, Q, nxt_slot(nb, Q.m), pm, s, pp);
+    int a = rel_position<EX>(P, Q, prv_slot(nb, Q.m), pm, s, pp);
+    int b = rel_position<EX>(P, Q, nxt_slot(nb, Q.m), pm, s, pp);
     int8_t L = initial_label(a, b);
     if (L != L_NONE) { P.lb[s] = L; Q.lb[nb] = L; }
   }
@@ -1762,6 +1936,7 @@ __global__ void big_step6_kernel(RingSet SP, RingSet SQ, BigPair bp) {
 }
 
 // the sequential phases from step 5 (split pairs) or from the trace on, one thread
+template <int EX>
 __global__ void big_seq_tail_kernel(RingSet SP, RingSet SQ, BigPair bp, int usedP, int usedQ, int from_trace,
                                     double* __restrict__ oxy, int32_t* __restrict__ ocsz, int64_t nv0, int nc0,
                                     ClipParams prm, int* err, int32_t* status, int32_t* outNC, int64_t* outNV) {
@@ -1775,7 +1950,7 @@ __global__ void big_seq_tail_kernel(RingSet SP, RingSet SQ, BigPair bp, int used
   c.err = err;
   c.status = status + bp.k;
   if (!from_trace) {
-    if (!seq_step5(c)) return;
+    if (!seq_step5<EX>(c)) return;
     seq_step6(c);
   }
   if (!seq_trace(c)) return;
@@ -1783,6 +1958,7 @@ __global__ void big_seq_tail_kernel(RingSet SP, RingSet SQ, BigPair bp, int used
 }
 
 // the whole pair sequentially from `step` (links not one-to-one, malformed chains)
+template <int EX>
 __global__ void big_seq_pair_kernel(RingSet SP, RingSet SQ, BigPair bp, int step, double* __restrict__ oxy,
                                     int32_t* __restrict__ ocsz, ClipParams prm, int* err, int32_t* status,
                                     int32_t* outNC, int64_t* outNV) {
@@ -1796,7 +1972,7 @@ __global__ void big_seq_pair_kernel(RingSet SP, RingSet SQ, BigPair bp, int step
   c.err = err;
   c.status = status + bp.k;
   c.noInter[0] = c.noInter[1] = c.ident[0] = c.ident[1] = false;
-  seq_pair_from(c, step, outNC + bp.k, outNV + bp.k);
+  seq_pair_from<EX>(c, step, outNC + bp.k, outNV + bp.k);
 }
 
 // ---- parallel tracing.  With no added vertices, when every vertex carrying an entry/exit
@@ -2076,7 +2252,7 @@ static int run_big_label_pair(BigCtx& c, const BigPair& bp, BigFlags* df) {
     return sync();
   };
   auto seq_pair = [&](int step) {
-    { big_seq_pair_kernel<<<1, 1, 0, s>>>(c.SP, c.SQ, bp, step, c.oxy, c.ocsz, c.prm, c.d_err, c.status, c.outNC,
+    { (c.prm.exact ? big_seq_pair_kernel<1> : big_seq_pair_kernel<0>)<<<1, 1, 0, s>>>(c.SP, c.SQ, bp, step, c.oxy, c.ocsz, c.prm, c.d_err, c.status, c.outNC,
                                          c.outNV); note_launch(); }
     return ST_OK;
   };
@@ -2086,7 +2262,7 @@ static int run_big_label_pair(BigCtx& c, const BigPair& bp, BigFlags* df) {
   if (!read_flags()) return ST_CUDA_ERROR;
   if (h.bad) return seq_pair(1);
   // ---- step 1, chains
-  { big_step1_kernel<<<grid_for(bp.mP), 256, 0, s>>>(c.SP, c.SQ, bp); note_launch(); }
+  { (c.prm.exact ? big_step1_kernel<1> : big_step1_kernel<0>)<<<grid_for(bp.mP), 256, 0, s>>>(c.SP, c.SQ, bp); note_launch(); }
   { big_chain_kernel<0><<<grid_for(bp.mP), 256, 0, s>>>(c.SP, c.SQ, bp, df); note_launch(); }
   if (!read_flags()) return ST_CUDA_ERROR;
   if (h.bad) return seq_pair(2);
@@ -2187,7 +2363,7 @@ static int run_big_label_pair(BigCtx& c, const BigPair& bp, BigFlags* df) {
     }
   }
   auto seq_tail = [&](int from_trace) {
-    { big_seq_tail_kernel<<<1, 1, 0, s>>>(c.SP, c.SQ, bp, used[0], used[1], from_trace, c.oxy, c.ocsz, nv, nc, c.prm,
+    { (c.prm.exact ? big_seq_tail_kernel<1> : big_seq_tail_kernel<0>)<<<1, 1, 0, s>>>(c.SP, c.SQ, bp, used[0], used[1], from_trace, c.oxy, c.ocsz, nv, nc, c.prm,
                                           c.d_err, c.status, c.outNC, c.outNV); note_launch(); }
     return ST_OK;
   };
@@ -2337,7 +2513,7 @@ out_compact_kernel(int64_t K, const double* __restrict__ xy, const int64_t* __re
 
 int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const int32_t* d_qid,
              int64_t K, const ClipParams& prm, Arena& A, ClipDev& C, int* d_err, int64_t* hs,
-             cudaStream_t s, Marks* mk) {
+             cudaStream_t s, Marks* mk, cudaStream_t aux) {
   Marks dummy;
   if (!mk) mk = &dummy;
   C = ClipDev();
@@ -2408,8 +2584,8 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   // ---- G2 count: chunked pairs
   Records R{};
   if (nCh > 0) {
-    { intersect_kernel<0><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, prm.exact, chunkRec, chunkQ, nullptr, nullptr, R); note_launch(); }
+    { (prm.exact ? intersect_kernel<0, 1> : intersect_kernel<0, 0>)<<<blocks_for_warps(nCh), kThreads, 0, s>>>(
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, chunkRec, chunkQ, nullptr, nullptr, R); note_launch(); }
     exclusive_scan_i32(chunkRec, recScan, nCh, nullptr, stC, d_err, s);
     exclusive_scan_i32(chunkQ, qScan, nCh, nullptr, stC, d_err, s);
   }
@@ -2481,8 +2657,8 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
       { bin_fill_kernel<<<blocks_for(W.info.cq), kThreads, 0, s>>>(Lb, Lo, D, k, LQ + W.info.offQ, W.info.cq, W.G,
                                                                    W.cellOff, cursor, W.cellList); note_launch(); }
       cudaMemsetAsync(d_q, 0, sizeof(unsigned long long), s);
-      { bin_pairs_kernel<0><<<blocks_for(W.info.cp), kThreads, 0, s>>>(Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G,
-                                                                       W.cellOff, W.cellList, prm.eps, prm.exact, recCnt, d_q,
+      { (prm.exact ? bin_pairs_kernel<0, 1> : bin_pairs_kernel<0, 0>)<<<blocks_for(W.info.cp), kThreads, 0, s>>>(
+            Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G, W.cellOff, W.cellList, prm.eps, recCnt, d_q,
                                                                        nullptr, R); note_launch(); }
       exclusive_scan_i32(recCnt, W.recPos, W.info.cp, d_t + 1, st2, d_err, s);
       { bin_total_kernel<<<1, 1, 0, s>>>(d_t + 1, d_q, k, binRec, binQ); note_launch(); }
@@ -2506,13 +2682,13 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   R.t = A.take_n<int8_t>(nR); R.k = A.take_n<int32_t>(nR);
   if (!R.p || !R.q || !R.a || !R.b || !R.t || !R.k) return ST_OUT_OF_MEMORY;
   if (nCh > 0)
-    { intersect_kernel<1><<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, prm.exact, nullptr, nullptr, recScan, recOff, R); note_launch(); }
+    { (prm.exact ? intersect_kernel<1, 1> : intersect_kernel<1, 0>)<<<blocks_for_warps(nCh), kThreads, 0, s>>>(
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, recOff, R); note_launch(); }
   for (auto& W : bigs) {
     const int64_t k = W.info.k;
     { add_offset_kernel<<<blocks_for(W.info.cp), kThreads, 0, s>>>(W.recPos, W.info.cp, recOff + k); note_launch(); }
-    { bin_pairs_kernel<1><<<blocks_for(W.info.cp), kThreads, 0, s>>>(Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G,
-                                                                     W.cellOff, W.cellList, prm.eps, prm.exact, nullptr, nullptr,
+    { (prm.exact ? bin_pairs_kernel<1, 1> : bin_pairs_kernel<1, 0>)<<<blocks_for(W.info.cp), kThreads, 0, s>>>(
+          Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G, W.cellOff, W.cellList, prm.eps, nullptr, nullptr,
                                                                      W.recPos, R); note_launch(); }
   }
   mk->mark("clip:emit", s);
@@ -2646,9 +2822,39 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int32_t* ocsz = A.take_n<int32_t>(hs[1]);
   if (!oxy || !ocsz) return ST_OUT_OF_MEMORY;
   mk->mark("clip:fill+link", s);
-  { label_trace_kernel<<<(unsigned)((K + 3) / 4), 128, 0, s>>>(D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ,
-                                                                  SP, SQ, oxy, vOff, vcap, ocsz, cOff, ccap, nc,
-                                                                  nv, prm, d_err, prm.big_label_min); note_launch(); }
+  {
+    int64_t* mlist = A.take_n<int64_t>(K);
+    unsigned long long* mcnt = A.take_n<unsigned long long>(2);
+    if (!mlist || !mcnt) return ST_OUT_OF_MEMORY;
+    cudaMemsetAsync(mcnt, 0, 2 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(nc, 0, K * sizeof(int32_t), s);
+    cudaMemsetAsync(nv, 0, K * sizeof(int64_t), s);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    LabelArgs la{D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ, SP, SQ, oxy, vOff, vcap, ocsz, cOff, ccap, nc, nv,
+                 prm, d_err, std::min(prm.mid_label_min, prm.big_label_min), prm.big_label_min, mlist, mcnt, mcnt + 1};
+    // long pairs: a block each, on the auxiliary stream when there is one, so they start
+    // first and overlap the warp-per-pair kernel instead of trailing it
+    cudaStream_t ls = s;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    if (aux && cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) == cudaSuccess &&
+        cudaEventCreateWithFlags(&join, cudaEventDisableTiming) == cudaSuccess) {
+      cudaEventRecord(fork, s);
+      cudaStreamWaitEvent(aux, fork, 0);
+      ls = aux;
+    }
+    { mid_label_list_kernel<<<blocks_for(K), kThreads, 0, ls>>>(mP, mQ, D.status, K, la.midLabelMin, la.bigLabelMin,
+                                                               mlist, mcnt); note_launch(); }
+    { (prm.exact ? label_trace_block_kernel<1> : label_trace_block_kernel<0>)<<<2 * nsm, kBlockLabelThreads, 0, ls>>>(la); note_launch(); }
+    { (prm.exact ? label_trace_kernel<1> : label_trace_kernel<0>)<<<(unsigned)((K + 3) / 4), 128, 0, s>>>(la); note_launch(); }
+    if (ls != s) {
+      cudaEventRecord(join, ls);
+      cudaStreamWaitEvent(s, join, 0);
+    }
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+  }
   // ---- G7 grid path for huge pairs
   {
     int64_t* blist = A.take_n<int64_t>(K);

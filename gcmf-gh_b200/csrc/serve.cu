@@ -207,7 +207,8 @@ struct gcmfgh_server {
 
   LayerDev resident() const { return LayerDev{r_xy, r_vnum, r_vps, r_n}; }
   void worker_main(int wid);
-  int run_batch(std::vector<std::shared_ptr<Request>>& batch, int64_t batch_id, cudaStream_t s, Arena& A,
+  int run_batch(std::vector<std::shared_ptr<Request>>& batch, int64_t batch_id, cudaStream_t s, cudaStream_t aux,
+                Arena& A,
                 Arena& C, int* d_err, int64_t* h_scratch, Pinned<char>& hin, Pinned<char>& hout);
 };
 
@@ -220,6 +221,7 @@ size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 // One batch: queries -> device layer, MBR candidates from the grid index, join stages
 // J3-J6, clip of the clip set, results back to the host and split per query.
 int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64_t batch_id, cudaStream_t s,
+                             cudaStream_t aux,
                              Arena& A, Arena& C, int* d_err, int64_t* h_scratch, Pinned<char>& hin,
                              Pinned<char>& hout) {
   A.reset();
@@ -292,7 +294,7 @@ int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64
       prm.eps_clean = opt.eps_clean;
       prm.union_mode = opt.union_mode ? 1 : 0;
       prm.exact = opt.exact ? 1 : 0;
-      st = run_clip(Lq, resident(), J.clip_b, J.clip_o, J.n_clip, prm, C, CD, d_err, h_scratch, s);
+      st = run_clip(Lq, resident(), J.clip_b, J.clip_o, J.n_clip, prm, C, CD, d_err, h_scratch, s, nullptr, aux);
       if (st != ST_OK) return st;
     }
   }
@@ -355,6 +357,7 @@ void gcmfgh_server::worker_main(int wid) {
   cudaSetDevice(device);
   cudaStream_t s = nullptr;
   cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaStream_t aux = create_priority_stream();
   Arena A, C;
   int* d_err = nullptr;
   int64_t* h_scratch = nullptr;
@@ -392,14 +395,14 @@ void gcmfgh_server::worker_main(int wid) {
       if (!queue.empty()) cv_work.notify_one();
     }
     if (batch.empty()) continue;
-    int st = run_batch(batch, bid, s, A, C, d_err, h_scratch, hin, hout);
+    int st = run_batch(batch, bid, s, aux, A, C, d_err, h_scratch, hin, hout);
     if (st == ST_OUT_OF_MEMORY && batch.size() > 1) {
       // split the batch until it fits; a single query that does not fit fails alone
       A.release(); C.release();
       std::vector<std::shared_ptr<Request>> half(batch.begin() + batch.size() / 2, batch.end());
       batch.resize(batch.size() / 2);
-      st = run_batch(batch, bid, s, A, C, d_err, h_scratch, hin, hout);
-      int st2 = run_batch(half, bid, s, A, C, d_err, h_scratch, hin, hout);
+      st = run_batch(batch, bid, s, aux, A, C, d_err, h_scratch, hin, hout);
+      int st2 = run_batch(half, bid, s, aux, A, C, d_err, h_scratch, hin, hout);
       if (st2 != ST_OK) for (auto& r : half) { r->status = st2; r->done_ns = now_ns(); }
       std::lock_guard<std::mutex> lk(mu);
       for (auto& r : half) r->done = true;
@@ -425,6 +428,7 @@ void gcmfgh_server::worker_main(int wid) {
   cudaFree(d_err);
   cudaFreeHost(h_scratch);
   cudaStreamDestroy(s);
+  if (aux) cudaStreamDestroy(aux);
 }
 
 extern "C" {

@@ -212,12 +212,14 @@ class Engine:
     def last_device_error(self):
         return lib().gcmfgh_last_device_error(self.h)
 
-    def set_tuning(self, bin_grid=None, big_label=None):
+    def set_tuning(self, bin_grid=None, big_label=None, mid_label=None):
         """Work-distribution thresholds (results do not depend on them)."""
         if bin_grid is not None:
             _check(lib().gcmfgh_set_tuning(self.h, 0, int(bin_grid)))
         if big_label is not None:
             _check(lib().gcmfgh_set_tuning(self.h, 1, int(big_label)))
+        if mid_label is not None:
+            _check(lib().gcmfgh_set_tuning(self.h, 2, int(mid_label)))
 
     def set_timing(self, on=True):
         _check(lib().gcmfgh_set_timing(self.h, 1 if on else 0))
@@ -389,3 +391,35 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class TextLayer(ctypes.Structure):
+    _fields_ = [("coords", ctypes.c_void_p), ("vnum", ctypes.c_void_p), ("vps", ctypes.c_void_p),
+                ("ids", ctypes.c_void_p), ("n_polys", ctypes.c_int64), ("n_vertices", ctypes.c_int64)]
+
+
+def read_text_layer(path, threads=0):
+    """Parses a GCMF text layer file with the engine's parallel reader; returns
+    (synth.Layer, ids)."""
+    L = lib()
+    L.gcmfgh_read_text_layer.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(TextLayer)]
+    L.gcmfgh_free_text_layer.argtypes = [ctypes.POINTER(TextLayer)]
+    L.gcmfgh_free_text_layer.restype = None
+    t = TextLayer()
+    _check(L.gcmfgh_read_text_layer(os.fsencode(path), int(threads), ctypes.byref(t)))
+    try:
+        n, nv = t.n_polys, t.n_vertices
+        xy = np.ctypeslib.as_array(ctypes.cast(t.coords, ctypes.POINTER(ctypes.c_double)), (2 * max(nv, 1),))[:2 * nv].copy()
+        vnum = np.ctypeslib.as_array(ctypes.cast(t.vnum, ctypes.POINTER(ctypes.c_int32)), (max(n, 1),))[:n].copy()
+        ids = np.ctypeslib.as_array(ctypes.cast(t.ids, ctypes.POINTER(ctypes.c_int64)), (max(n, 1),))[:n].copy()
+    finally:
+        L.gcmfgh_free_text_layer(ctypes.byref(t))
+    return synth.Layer(xy, vnum), ids
+
+
+def write_text_layer(path, layer):
+    """Writes a (host) layer in the GCMF text format."""
+    L = lib()
+    L.gcmfgh_write_text_layer.argtypes = [ctypes.c_char_p, ctypes.POINTER(Layer)]
+    h = host_layer(layer)
+    _check(L.gcmfgh_write_text_layer(os.fsencode(path), ctypes.byref(h)))

@@ -127,10 +127,14 @@ const char* gcmfgh_status_string(gcmfgh_status s);
 /* Work-distribution thresholds of the clip (results do not depend on them):
  * GCMFGH_TUNE_BIN_GRID: a pair whose common-MBR edge grid exceeds this many edge pairs
  * has its edges binned on a uniform grid instead of enumerated (default 2^24);
+ * GCMFGH_TUNE_MID_LABEL: a pair whose merged rings exceed this many vertices is labelled
+ * and traced by one thread block (persistent, work-stealing) instead of one warp
+ * (default 2^13);
  * GCMFGH_TUNE_BIG_LABEL: a pair whose merged rings exceed this many vertices is labelled
- * and traced by grid-wide kernels instead of one warp (default 2^18). */
+ * and traced by grid-wide kernels (default 2^18). */
 #define GCMFGH_TUNE_BIN_GRID 0
 #define GCMFGH_TUNE_BIG_LABEL 1
+#define GCMFGH_TUNE_MID_LABEL 2
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* ctx, int key, int64_t value);
 /* device error word of the last call (0 none, 1 capacity, 2 trace budget, 4 wait limit) */
 int gcmfgh_last_device_error(gcmfgh_ctx* ctx);
@@ -158,6 +162,10 @@ gcmfgh_status gcmf_join_ptr(gcmfgh_ctx* ctx, int field, const void** dev_ptr, in
 gcmfgh_status gh_clip_batch(gcmfgh_ctx* ctx, const gcmfgh_layer* base, const gcmfgh_layer* overlay,
                             const int32_t* pid, const int32_t* qid, int64_t n_pairs,
                             gcmfgh_clip_info* info);
+/* as gh_clip_batch with the pair ids in HOST memory (copied in) */
+gcmfgh_status gh_clip_batch_host_ids(gcmfgh_ctx* ctx, const gcmfgh_layer* base, const gcmfgh_layer* overlay,
+                                     const int32_t* pid, const int32_t* qid, int64_t n_pairs,
+                                     gcmfgh_clip_info* info);
 /* clip the clip set of the last gcmf_join on the same layers (no host round trip) */
 gcmfgh_status gh_clip_joined(gcmfgh_ctx* ctx, const gcmfgh_layer* base, const gcmfgh_layer* overlay,
                              gcmfgh_clip_info* info);
@@ -203,6 +211,30 @@ gcmfgh_status gcmfgh_exclusive_scan_i32_noalloc(const int32_t* d_in, int64_t* d_
 gcmfgh_status gcmfgh_join_clip_host(gcmfgh_ctx* ctx, const gcmfgh_layer* base_host,
                                     const gcmfgh_layer* overlay_host, gcmfgh_join_info* jinfo,
                                     gcmfgh_clip_info* cinfo);
+
+/* ---- the GCMF text layer format (dataConverter.py:95-111; reader
+ * ReadTextFormatPolygon2WithVector, SEQ_Overlay.h:285-390): a header line, then per
+ * polygon "id minx miny maxx maxy x0 y0 ... x0 y0".  gcmfgh_read_text_layer parses it on
+ * `threads` host threads (<= 0: all cores) with the reference reader's rules (tokens of
+ * 0-9 . -, MBR over every pair read, zero-width MBR polygons skipped) into malloc'ed
+ * host arrays in the layer layout above; ids holds each stored polygon's file id.
+ * gcmfgh_write_text_layer writes a host layer in the format, 17 significant digits in
+ * fixed-point notation (the reference tokenizer has no exponents). */
+typedef struct {
+  double* coords;
+  int32_t* vnum;
+  int64_t* vps;
+  int64_t* ids;
+  int64_t n_polys;
+  int64_t n_vertices;
+} gcmfgh_text_layer;
+gcmfgh_status gcmfgh_read_text_layer(const char* path, int threads, gcmfgh_text_layer* out);
+void gcmfgh_free_text_layer(gcmfgh_text_layer* layer);
+gcmfgh_status gcmfgh_write_text_layer(const char* path, const gcmfgh_layer* host_layer);
+
+/* copy a host layer to the device; the copy belongs to the context and lives until
+ * gcmfgh_destroy.  dev_out receives the device view. */
+gcmfgh_status gcmfgh_upload_layer(gcmfgh_ctx* ctx, const gcmfgh_layer* host_layer, gcmfgh_layer* dev_out);
 
 /* ---- serving: continuous batching of join+clip queries against a resident layer.
  * No counterpart in the reference (its main() runs one join and one clip over two whole

@@ -20,7 +20,8 @@ def pytest_configure(config):
 
 def build_library():
     lib = os.path.join(ROOT, "gcmf-gh_b200", "lib", "libgcmfgh.so")
-    if not os.path.exists(lib):
+    shims = os.path.join(ROOT, "gcmf-gh_b200", "lib", "libgcmfgh_shims.so")
+    if not os.path.exists(lib) or not os.path.exists(shims):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "gcmf-gh_b200")], check=True)
     return lib
 

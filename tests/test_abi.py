@@ -9,9 +9,9 @@ import subprocess
 from conftest import ROOT, build_library
 
 
-def declared_functions():
+def declared_functions(header="gcmfgh.h"):
     names = set()
-    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+    for h in glob.glob(os.path.join(ROOT, "include", header)):
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         text = re.sub(r"^\s*#.*$", "", text, flags=re.M)
@@ -35,6 +35,17 @@ def test_library_exports_every_declared_symbol():
     exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
     missing = declared_functions() - exported
     assert not missing, missing
+
+
+def test_shim_library_exports_the_reference_signatures():
+    """include/gcmfgh_shims.h: C++ symbols whose mangled names equal the reference's
+    declarations (main.h:5-11, coord_t = double), so its main.cpp links unchanged."""
+    build_library()
+    lib = os.path.join(ROOT, "gcmf-gh_b200", "lib", "libgcmfgh_shims.so")
+    out = subprocess.run(["nm", "-DC", "--defined-only", lib], capture_output=True, text=True, check=True).stdout
+    assert "spatialJoin(int, char**, int**, int**, long*, double**, double**, int**, long**, int**, long**)" in out
+    assert "ghcuda(int*, int*, int, double*, double*, int*, long*, int*, long*)" in out
+    assert declared_functions("gcmfgh_shims.h") == {"spatialJoin", "ghcuda"}
 
 
 def test_library_loads_and_reports_status_strings():

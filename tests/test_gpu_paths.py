@@ -10,20 +10,23 @@ from gcmfgh import synth
 
 pytestmark = pytest.mark.gpu
 
-BIN_DEFAULT, BIG_DEFAULT = 1 << 24, 1 << 18
+BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT = 1 << 24, 1 << 18, 1 << 13
 
 
-def _run(engine, base, ovl, pid, qid, union=False, bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT):
+def _run(engine, base, ovl, pid, qid, union=False, bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT,
+         mid_label=MID_DEFAULT, exact=False):
     import gcmfgh
     db, do = gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl)
-    engine.set_tuning(bin_grid=bin_grid, big_label=big_label)
+    engine.set_tuning(bin_grid=bin_grid, big_label=big_label, mid_label=mid_label)
     engine.set_params(1e-7, 1e-7, union)
+    engine.set_precision(exact)
     try:
         info = engine.clip_batch(db, do, pid, qid)
         r = engine.clip_result()
     finally:
-        engine.set_tuning(bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT)
+        engine.set_tuning(bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT, mid_label=MID_DEFAULT)
         engine.set_params(1e-7, 1e-7, False)
+        engine.set_precision(False)
     return info, r
 
 
@@ -54,6 +57,30 @@ def test_grid_labelling_every_pair(engine, union):
     base, ovl, ids = _pairs_layers(synth.random_star_pairs(22, 250, 3, 60, spread=0.8))
     _, r = _run(engine, base, ovl, ids, ids, union=union, big_label=0)
     _assert_equal(r, pyoracle.clip_batch(base, ovl, ids, ids, union=union))
+
+
+@pytest.mark.parametrize("union", [False, True])
+@pytest.mark.parametrize("exact", [False, True])
+def test_block_labelling_every_pair(engine, union, exact):
+    """Every pair labelled and traced by a whole thread block (persistent, work-stealing)."""
+    base, ovl, ids = _pairs_layers(synth.random_star_pairs(23, 1200, 3, 120, spread=0.8))
+    _, r = _run(engine, base, ovl, ids, ids, union=union, mid_label=0, exact=exact)
+    _assert_equal(r, pyoracle.clip_batch(base, ovl, ids, ids, union=union, exact=exact))
+
+
+def test_block_labelling_degenerate_cases(engine):
+    from test_gpu_clip import degenerate_pairs
+    base, ovl, ids = _pairs_layers(degenerate_pairs())
+    for union in (False, True):
+        _, r = _run(engine, base, ovl, ids, ids, union=union, mid_label=0)
+        _assert_equal(r, pyoracle.clip_batch(base, ovl, ids, ids, union=union))
+
+
+def test_block_labelling_medium_pair(engine):
+    s, c = synth.large_pair(1, 20000, 10000)
+    one = np.array([0], np.int32)
+    _, r = _run(engine, s, c, one, one, mid_label=0)
+    _assert_equal(r, pyoracle.clip_batch(s, c, one, one))
 
 
 def test_grid_labelling_degenerate_cases(engine):
