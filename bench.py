@@ -287,6 +287,41 @@ def serve_measure(local, seconds=0.5):
     return out
 
 
+# ----------------------------------------------------------------------------- plain form
+
+def plain_measure(eng, db, do, stream, n=2000, seed=9):
+    """The plain one-pair-per-launch form on the same GPU: a seeded sample of the clip set
+    of the last join, each pair clipped by its own gh_clip_batch_host_ids call (its own
+    launch sequence, host synchronisations included), same kernels and arithmetic."""
+    import ctypes
+    import torch
+    import gcmfgh
+    cb, co = eng.join_field("clip_b"), eng.join_field("clip_o")
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(len(cb), size=min(n, len(cb)), replace=False)
+    L = gcmfgh.lib()
+    info = gcmfgh.ClipInfo()
+    pids = [np.ascontiguousarray(cb[i:i + 1]) for i in idx]
+    qids = [np.ascontiguousarray(co[i:i + 1]) for i in idx]
+
+    def one(k):
+        gcmfgh._check(L.gh_clip_batch_host_ids(eng.h, ctypes.byref(db.c), ctypes.byref(do.c),
+                                               ctypes.c_void_p(pids[k].ctypes.data),
+                                               ctypes.c_void_p(qids[k].ctypes.data), 1, ctypes.byref(info)))
+    for k in range(min(50, len(idx))):
+        one(k)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(len(idx)):
+        one(k)
+    e1.record(stream)
+    e1.synchronize()
+    secs = e0.elapsed_time(e1) * 1e-3
+    return {"value": len(idx) / secs, "unit": "pairs/s",
+            "sample": f"{len(idx)} seeded pairs of the clip set, one gh_clip_batch call each"}
+
+
 # ----------------------------------------------------------------------------- our arm
 
 def run_ours(args, rank, world, local):
@@ -417,6 +452,9 @@ def run_ours(args, rank, world, local):
             "clocks": clocks,
             "gpu_launches": launches,
         }
+        plain = plain_measure(eng, db, do, stream)
+        plain["batched_over_plain"] = line["value"] / world / plain["value"]
+        line["plain"] = plain
         if not args.no_serve:
             line["serving"] = serve_measure(local)
         if world == 1 and not args.no_cpu_baseline:

@@ -104,6 +104,7 @@ def lib():
         L.gcmf_join_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
         L.gh_clip_batch.argtypes = [vp, P(Layer), P(Layer), vp, vp, i64, P(ClipInfo)]
         L.gh_clip_joined.argtypes = [vp, P(Layer), P(Layer), P(ClipInfo)]
+        L.gh_clip_batch_host_ids.argtypes = [vp, P(Layer), P(Layer), vp, vp, i64, P(ClipInfo)]
         L.gh_clip_get.argtypes = [vp, ctypes.c_int, vp, i64, ctypes.c_int, P(i64)]
         L.gh_clip_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
         L.gh_clip_pair.argtypes = [vp, vp, i32, vp, i32, P(ClipInfo)]
