@@ -416,6 +416,10 @@ struct RingSet {
   int8_t* lb;       // IntersectionLabel
   int8_t* ee;       // EntryExitLabel
   uint8_t* fl;      // bit0 split candidate, bit1 crossing candidate
+  int32_t* tn;      // tracing scratch: next run start (other ring), run length, output
+  int32_t* tl;      //   offset, and the slots of the flagged vertices in ring order
+  int32_t* to;
+  int32_t* ls;
   int exact;        // orientation signs exact (ClipParams::exact)
 };
 
@@ -694,6 +698,7 @@ __global__ void link_kernel(Records R, int64_t nR, const int32_t* __restrict__ s
 struct Ring {
   double* x; double* y; int32_t* nx; int32_t* pv; int32_t* nb;
   uint8_t* it; int8_t* lb; int8_t* ee; uint8_t* fl;
+  int32_t* tn; int32_t* tl; int32_t* to; int32_t* ls;
   int m;        // slots in the merged ring
   int used;     // slots in use (ring + added vertices)
   int cap;      // region capacity
@@ -704,6 +709,7 @@ __device__ __forceinline__ Ring ring_of(const RingSet& S, int64_t base, int m, i
   Ring r;
   r.x = S.x + base; r.y = S.y + base; r.nx = S.nx + base; r.pv = S.pv + base; r.nb = S.nb + base;
   r.it = S.it + base; r.lb = S.lb + base; r.ee = S.ee + base; r.fl = S.fl + base;
+  r.tn = S.tn + base; r.tl = S.tl + base; r.to = S.to + base; r.ls = S.ls + base;
   r.m = m; r.used = m; r.cap = cap; r.exact = S.exact;
   return r;
 }
@@ -1449,6 +1455,128 @@ __device__ void grp_step6(const G& g, PairCtx& c) {
 // Tracing when neither ring has added vertices (rings in slot order): each run from V to
 // the next vertex with the target entry/exit flag (or back at the start) is found with a
 // warp ballot and copied with coalesced stores.
+// Tracing from a run table.  With entry/exit flags alternating along both rings (checked
+// here), every run of the sequential walk goes from a flagged vertex to the adjacent
+// flagged vertex in its direction, and the next run starts at that vertex's neighbour.
+// Phase 1 (parallel) lists the flagged slots of each ring and gives each its run: the
+// length (signed by direction) and the next run's start.  Phase 2 (one member) follows the
+// runs in the order of the sequential walk -- components from the first unvisited crossing
+// of P, in P's slot order -- and assigns each run its output offset.  Phase 3 (parallel)
+// copies the runs.  Returns 0 when done, 1 when the flags do not alternate (the caller
+// then runs the general walk), -1 on a capacity or trace error.
+template <class G>
+__device__ int grp_trace_runs(const G& g, PairCtx& c) {
+  int nF[2];
+  bool mismatch = false;     // a flagged vertex that is not a crossing, or the reverse
+  for (int sd = 0; sd < 2; ++sd) {
+    Ring& A = c.R[sd];
+    int carry = 0;
+    for (int b = 0; b < A.m; b += g.size()) {
+      const int s = b + g.rank();
+      const int f = (s < A.m && (A.ee[s] == E_ENTRY || A.ee[s] == E_EXIT)) ? 1 : 0;
+      if (s < A.m && (f != 0) != (A.it[s] && A.lb[s] == L_CROSSING)) mismatch = true;
+      int tot;
+      const int incl = g.incl_scan(f, tot);
+      if (f) A.ls[carry + incl - 1] = s;
+      carry += tot;
+    }
+    nF[sd] = carry;
+  }
+  if (g.any(mismatch)) return 1;
+  if (nF[0] == 0 && nF[1] == 0) return 0;
+  bool bad = nF[0] < 2 || nF[1] < 2;
+  for (int sd = 0; sd < 2 && !bad; ++sd) {
+    Ring& A = c.R[sd];
+    const Ring& B = c.R[1 - sd];
+    const int n = nF[sd], m = A.m;
+    for (int i = g.rank(); i < n; i += g.size()) {
+      const int s = A.ls[i];
+      const int8_t e = A.ee[s];
+      if (!A.it[s] || A.lb[s] != L_CROSSING) { bad = true; continue; }
+      if (A.ee[A.ls[(i + 1 < n) ? i + 1 : 0]] == e) { bad = true; continue; }   // alternation
+      const int nb = A.nb[s];
+      if (nb < 0 || nb >= B.m || B.ee[nb] != toggled(e)) { bad = true; continue; }
+      const int8_t st = toggled(e);
+      const int dir = ((st == E_EXIT) ^ c.uni) ? 1 : -1;
+      const int W = A.ls[(i + dir + n) % n];
+      int L = dir > 0 ? W - s : s - W;
+      if (L <= 0) L += m;
+      const int nbW = A.nb[W];
+      if (nbW < 0 || nbW >= B.m) { bad = true; continue; }
+      A.tl[s] = dir * L;
+      A.tn[s] = nbW;
+      A.to[s] = -1;
+    }
+  }
+  if (g.any(bad)) return 1;
+  // ---- phase 2: the walk over the run table, one member
+  OutRegion& O = c.O;
+  int status = 0;
+  int64_t nv = O.nv;
+  int nc = O.nc;
+  if (g.rank() == 0) {
+    Ring& P = c.R[0];
+    const int64_t nv0 = O.nv;
+    long long budget = (long long)nF[0] + nF[1] + 4;
+    for (int i = 0; i < nF[0] && status == 0; ++i) {
+      const int I = P.ls[i];
+      if (!P.it[I]) continue;
+      if (nc >= O.ccap) { status = -1; fail(c, DEV_CAPACITY); break; }
+      P.it[I] = 0;
+      int side = 0, V = I;
+      int64_t csz = 0;
+      for (;;) {
+        Ring& C = c.R[side];
+        const int t = C.tl[V], L = t < 0 ? -t : t, m = C.m;
+        int W = V + t % m;
+        W = (W % m + m) % m;
+        C.to[V] = (int32_t)(nv - nv0);
+        nv += L;
+        csz += L;
+        C.it[W] = 0;
+        if (side == 0 && W == I) break;
+        const int V2 = C.tn[V];
+        side ^= 1;
+        if (side == 0 && V2 == I) break;
+        c.R[side].it[V2] = 0;
+        V = V2;
+        if (--budget < 0) { status = -1; fail(c, DEV_TRACE); break; }
+      }
+      if (status == 0) {
+        if (nv > O.vcap) { status = -1; fail(c, DEV_CAPACITY); break; }
+        O.csz[nc++] = (int32_t)csz;
+      }
+    }
+  }
+  status = g.bcast0(status);
+  if (status != 0) return -1;
+  const int64_t nv0 = O.nv;
+  O.nv = g.bcast0((long long)nv);
+  O.nc = g.bcast0(nc);
+  // ---- phase 3: copy every run to its place
+  for (int sd = 0; sd < 2; ++sd) {
+    const Ring& A = c.R[sd];
+    const int m = A.m;
+    for (int i = g.rank(); i < nF[sd]; i += g.size()) {
+      const int s = A.ls[i];
+      const int off = A.to[s];
+      if (off < 0) continue;
+      const int t = A.tl[s], L = t < 0 ? -t : t, dir = t < 0 ? -1 : 1;
+      double* dst = O.xy + 2 * (nv0 + off);
+      int w = s;
+      for (int j = 0; j < L; ++j) {
+        w += dir;
+        if (w >= m) w -= m;
+        if (w < 0) w += m;
+        dst[2 * j] = A.x[w];
+        dst[2 * j + 1] = A.y[w];
+      }
+    }
+  }
+  g.sync();
+  return 0;
+}
+
 template <class G>
 __device__ bool grp_trace(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
@@ -1656,8 +1784,10 @@ __device__ void label_trace_pair(const G& g, const LabelArgs& a, int64_t k) {
     c.O.overflow = g.bcast0((int)c.O.overflow) != 0;
     g.sync();
     if (!ok) return;
-  } else if (!grp_trace(g, c)) {
-    return;
+  } else {
+    const int r = grp_trace_runs(g, c);
+    if (r < 0) return;
+    if (r > 0 && !grp_trace(g, c)) return;
   }
   if (c.O.overflow) {
     if (lead) fail(c, DEV_CAPACITY);
@@ -1668,7 +1798,7 @@ __device__ void label_trace_pair(const G& g, const LabelArgs& a, int64_t k) {
 
 // A warp per pair for pairs whose merged rings have at most midLabelMin slots.
 template <int EX>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
 label_trace_kernel(LabelArgs a) {
   int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (k >= a.K) return;
@@ -2763,7 +2893,8 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     S.nx = A.take_n<int32_t>(n); S.pv = A.take_n<int32_t>(n); S.nb = A.take_n<int32_t>(n);
     S.it = A.take_n<uint8_t>(n); S.lb = A.take_n<int8_t>(n); S.ee = A.take_n<int8_t>(n);
     S.fl = A.take_n<uint8_t>(n);
-    return S.x && S.y && S.nx && S.pv && S.nb && S.it && S.lb && S.ee && S.fl;
+    S.tn = A.take_n<int32_t>(n); S.tl = A.take_n<int32_t>(n); S.to = A.take_n<int32_t>(n); S.ls = A.take_n<int32_t>(n);
+    return S.x && S.y && S.nx && S.pv && S.nb && S.it && S.lb && S.ee && S.fl && S.tn && S.tl && S.to && S.ls;
   };
   RingSet SP, SQ;
   if (!take_ring(regTotP, SP) || !take_ring(regTotQ, SQ)) return ST_OUT_OF_MEMORY;

@@ -129,7 +129,7 @@ const char* gcmfgh_status_string(gcmfgh_status s);
  * has its edges binned on a uniform grid instead of enumerated (default 2^24);
  * GCMFGH_TUNE_MID_LABEL: a pair whose merged rings exceed this many vertices is labelled
  * and traced by one thread block (persistent, work-stealing) instead of one warp
- * (default 2^13);
+ * (default 2^10);
  * GCMFGH_TUNE_BIG_LABEL: a pair whose merged rings exceed this many vertices is labelled
  * and traced by grid-wide kernels (default 2^18). */
 #define GCMFGH_TUNE_BIN_GRID 0

@@ -10,7 +10,7 @@ from gcmfgh import synth
 
 pytestmark = pytest.mark.gpu
 
-BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT = 1 << 24, 1 << 18, 1 << 13
+BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT = 1 << 24, 1 << 18, 1 << 10
 
 
 def _run(engine, base, ovl, pid, qid, union=False, bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT,
