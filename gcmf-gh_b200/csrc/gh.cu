@@ -1553,7 +1553,9 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
   const int64_t nv0 = O.nv;
   O.nv = g.bcast0((long long)nv);
   O.nc = g.bcast0(nc);
-  // ---- phase 3: copy every run to its place
+  // ---- phase 3: copy every run to its place; short runs one member each, long runs by
+  // the whole group (no barrier between runs: runs write disjoint ranges)
+  constexpr int kShortRun = 32;
   for (int sd = 0; sd < 2; ++sd) {
     const Ring& A = c.R[sd];
     const int m = A.m;
@@ -1562,11 +1564,27 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
       const int off = A.to[s];
       if (off < 0) continue;
       const int t = A.tl[s], L = t < 0 ? -t : t, dir = t < 0 ? -1 : 1;
+      if (L > kShortRun) continue;
       double* dst = O.xy + 2 * (nv0 + off);
       int w = s;
       for (int j = 0; j < L; ++j) {
         w += dir;
         if (w >= m) w -= m;
+        if (w < 0) w += m;
+        dst[2 * j] = A.x[w];
+        dst[2 * j + 1] = A.y[w];
+      }
+    }
+    for (int i = 0; i < nF[sd]; ++i) {
+      const int s = A.ls[i];
+      const int off = A.to[s];
+      const int t = A.tl[s], L = t < 0 ? -t : t;
+      if (off < 0 || L <= kShortRun) continue;
+      const int dir = t < 0 ? -1 : 1;
+      double* dst = O.xy + 2 * (nv0 + off);
+      for (int j = g.rank(); j < L; j += g.size()) {
+        int w = s + dir * (j + 1);
+        w %= m;
         if (w < 0) w += m;
         dst[2 * j] = A.x[w];
         dst[2 * j + 1] = A.y[w];
