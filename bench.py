@@ -322,6 +322,67 @@ def plain_measure(eng, db, do, stream, n=2000, seed=9):
             "sample": f"{len(idx)} seeded pairs of the clip set, one gh_clip_batch call each"}
 
 
+# ----------------------------------------------------------------------------- precision
+
+def precision_measure(local, n=2000, n_check=150):
+    """The degeneracy-stressed batch (independent pairs, vertex counts log-uniform on
+    [4, 10000]; 2% share a vertex exactly, 1% have collinear overlapping edges, 1% are
+    translated by 1e-12 relative; seed 3), a seeded sample of n pairs: clipped in exact
+    mode and in the reference's tolerance mode, timed with CUDA events; the exact results
+    of n_check pairs (every degenerate one among them) compared with the oracle."""
+    import torch
+    import gcmfgh
+    import pyoracle
+    from gcmfgh import synth
+    classes, pairs = synth.degeneracy_pairs(3, n, 4, 10_000)
+    base = synth.Layer.from_rings([p for p, _ in pairs])
+    ovl = synth.Layer.from_rings([q for _, q in pairs])
+    ids = np.arange(n, dtype=np.int32)
+    eng = gcmfgh.Engine(local)
+    db, do = gcmfgh.DeviceLayer(base, f"cuda:{local}"), gcmfgh.DeviceLayer(ovl, f"cuda:{local}")
+    out = {"workload": "degeneracy batch: %d pairs, vertex counts log-uniform [4, 10000], classes "
+                       "shared-vertex / collinear-overlap / 1e-12-translated at 2%%/1%%/1%%, seed 3" % n}
+    for exact in (True, False):
+        eng.set_precision(exact)
+        eng.clip_batch(db, do, ids, ids)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        info = eng.clip_batch(db, do, ids, ids)
+        e1.record()
+        e1.synchronize()
+        key = "exact" if exact else "reference_mode"
+        out[key] = {"pairs_per_s": n / (e0.elapsed_time(e1) * 1e-3), "invalid_pairs": info["n_invalid"],
+                    "errors": info["n_error"]}
+        if exact:
+            r = eng.clip_result()
+    eng.set_precision(False)
+    rng = np.random.default_rng(33)
+    degenerate = np.flatnonzero(classes > 0)
+    rest = np.setdiff1d(np.arange(n), degenerate)
+    chk = np.sort(np.concatenate([degenerate, rng.choice(rest, size=max(0, n_check - len(degenerate)), replace=False)]))
+    sub_b = synth.Layer.from_rings([pairs[i][0] for i in chk])
+    sub_o = synth.Layer.from_rings([pairs[i][1] for i in chk])
+    sid = np.arange(len(chk), dtype=np.int32)
+    o = pyoracle.clip_batch(sub_b, sub_o, sid, sid, exact=True)
+    comps_gpu = [r.components(int(i)) for i in chk]
+    comps_orc = [o.components(k) for k in range(len(chk))]
+    maxrel = 0.0
+    same = True
+    for a, b in zip(comps_gpu, comps_orc):
+        if len(a) != len(b) or any(x.shape != y.shape for x, y in zip(a, b)):
+            same = False
+            continue
+        for x, y in zip(a, b):
+            if x.size:
+                maxrel = max(maxrel, float(np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-300))))
+    out["oracle_check"] = {"pairs": int(len(chk)), "degenerate_pairs": int(len(degenerate)),
+                           "identical_structure": same, "max_rel_vertex_error": maxrel,
+                           "status_equal": bool(np.array_equal(r.status[chk], o.status))}
+    eng.close()
+    return out
+
+
 # ----------------------------------------------------------------------------- our arm
 
 def run_ours(args, rank, world, local):
@@ -457,6 +518,7 @@ def run_ours(args, rank, world, local):
         line["plain"] = plain
         if not args.no_serve:
             line["serving"] = serve_measure(local)
+            line["precision"] = precision_measure(local)
         if world == 1 and not args.no_cpu_baseline:
             nb = args.sample_bases or 20000
             p, s, cores = reference_cpu_sample(base, ovl, nb, 7)

@@ -961,7 +961,7 @@ __device__ bool seq_step4(PairCtx& c) {
 
 // step 5: split vertex pairs (polyclip.h:661-714)
 template <int EX>
-__device__ bool seq_step5(PairCtx& c) {
+__device__ __noinline__ bool seq_step5(PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
   const int pm0 = P.used;
@@ -1009,7 +1009,7 @@ __device__ void seq_step6(PairCtx& c) {
 
 // tracing (polyclip.h:743-783): starts at unvisited CROSSING vertices of P in ring order
 // from slot 0; visited vertices are marked by clearing their intersection flag.
-__device__ bool seq_trace(PairCtx& c) {
+__device__ __noinline__ bool seq_trace(PairCtx& c) {
   Ring& P = c.R[0];
   OutRegion& O = c.O;
   long long budget = 4ll * (c.R[0].used + c.R[1].used) + 16;
@@ -1098,7 +1098,7 @@ __device__ void seq_cleanup(PairCtx& c, int32_t* outNC, int64_t* outNV) {
 
 // the whole pair from `step` on (1: everything, 2: after the initial labels)
 template <int EX>
-__device__ void seq_pair_from(PairCtx& c, int step, int32_t* outNC, int64_t* outNV) {
+__device__ __noinline__ void seq_pair_from(PairCtx& c, int step, int32_t* outNC, int64_t* outNV) {
   if (step <= 1) seq_step1<EX>(c);
   seq_step2(c);
   seq_step35<EX>(c);
@@ -1596,7 +1596,7 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
 }
 
 template <class G>
-__device__ bool grp_trace(const G& g, PairCtx& c) {
+__device__ __noinline__ bool grp_trace(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
   OutRegion& O = c.O;
   long long budget = 4ll * (c.R[0].used + c.R[1].used) + 16;
@@ -1666,6 +1666,50 @@ __device__ bool grp_trace(const G& g, PairCtx& c) {
 template <class G>
 __device__ void grp_cleanup(const G& g, PairCtx& c, int32_t* outNC, int64_t* outNV) {
   OutRegion& O = c.O;
+  // Fast pass: test every vertex of every component at once (short components one member
+  // each, long ones by the whole group).  When nothing is removable, the output stands as
+  // traced; otherwise the per-component pass below removes and compacts.
+  {
+    int32_t* start = c.R[0].tn;          // the trace's scratch is free now
+    int carry = 0;
+    for (int b = 0; b < O.nc; b += g.size()) {
+      const int k = b + g.rank();
+      const int v = (k < O.nc) ? O.csz[k] : 0;
+      int tot;
+      const int incl = g.incl_scan(v, tot);
+      if (k < O.nc) start[k] = carry + incl - v;
+      carry += tot;
+    }
+    g.sync();
+    constexpr int kShortComp = 64;
+    bool any = false;
+    for (int k = g.rank(); k < O.nc; k += g.size()) {
+      const int n = O.csz[k];
+      if (n > kShortComp) continue;
+      const double* src = O.xy + 2 * (int64_t)start[k];
+      for (int j = 0; j < n && !any; ++j) {
+        int p = (j > 0) ? j - 1 : n - 1, q = (j + 1 < n) ? j + 1 : 0;
+        if (fabs(area2(src[2 * p], src[2 * p + 1], src[2 * j], src[2 * j + 1], src[2 * q], src[2 * q + 1])) <
+            c.eps_clean)
+          any = true;
+      }
+    }
+    for (int k = 0; k < O.nc; ++k) {
+      const int n = O.csz[k];
+      if (n <= kShortComp) continue;
+      const double* src = O.xy + 2 * (int64_t)start[k];
+      for (int j = g.rank(); j < n && !any; j += g.size()) {
+        int p = (j > 0) ? j - 1 : n - 1, q = (j + 1 < n) ? j + 1 : 0;
+        if (fabs(area2(src[2 * p], src[2 * p + 1], src[2 * j], src[2 * j + 1], src[2 * q], src[2 * q + 1])) <
+            c.eps_clean)
+          any = true;
+      }
+    }
+    if (!g.any(any)) {
+      if (g.rank() == 0) { *outNC = O.nc; *outNV = O.nv; }
+      return;
+    }
+  }
   int64_t vin = 0, vout = 0;
   int nc = 0;
   for (int k = 0; k < O.nc; ++k) {
