@@ -961,7 +961,7 @@ __device__ bool seq_step4(PairCtx& c) {
 
 // step 5: split vertex pairs (polyclip.h:661-714)
 template <int EX>
-__device__ __noinline__ bool seq_step5(PairCtx& c) {
+__device__ bool seq_step5(PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
   const int pm0 = P.used;
@@ -1009,7 +1009,7 @@ __device__ void seq_step6(PairCtx& c) {
 
 // tracing (polyclip.h:743-783): starts at unvisited CROSSING vertices of P in ring order
 // from slot 0; visited vertices are marked by clearing their intersection flag.
-__device__ __noinline__ bool seq_trace(PairCtx& c) {
+__device__ bool seq_trace(PairCtx& c) {
   Ring& P = c.R[0];
   OutRegion& O = c.O;
   long long budget = 4ll * (c.R[0].used + c.R[1].used) + 16;
@@ -1098,7 +1098,7 @@ __device__ void seq_cleanup(PairCtx& c, int32_t* outNC, int64_t* outNV) {
 
 // the whole pair from `step` on (1: everything, 2: after the initial labels)
 template <int EX>
-__device__ __noinline__ void seq_pair_from(PairCtx& c, int step, int32_t* outNC, int64_t* outNV) {
+__device__ void seq_pair_from(PairCtx& c, int step, int32_t* outNC, int64_t* outNV) {
   if (step <= 1) seq_step1<EX>(c);
   seq_step2(c);
   seq_step35<EX>(c);
@@ -1485,6 +1485,7 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
   if (g.any(mismatch)) return 1;
   if (nF[0] == 0 && nF[1] == 0) return 0;
   bool bad = nF[0] < 2 || nF[1] < 2;
+  bool longRun = false;
   for (int sd = 0; sd < 2 && !bad; ++sd) {
     Ring& A = c.R[sd];
     const Ring& B = c.R[1 - sd];
@@ -1506,9 +1507,11 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
       A.tl[s] = dir * L;
       A.tn[s] = nbW;
       A.to[s] = -1;
+      if (L > 32) longRun = true;
     }
   }
   if (g.any(bad)) return 1;
+  const bool anyLong = g.any(longRun);
   // ---- phase 2: the walk over the run table, one member
   OutRegion& O = c.O;
   int status = 0;
@@ -1555,7 +1558,7 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
   O.nc = g.bcast0(nc);
   // ---- phase 3: copy every run to its place; short runs one member each, long runs by
   // the whole group (no barrier between runs: runs write disjoint ranges)
-  constexpr int kShortRun = 32;
+  constexpr int kShortRun = 32;      // the run-length threshold of phase 1's longRun
   for (int sd = 0; sd < 2; ++sd) {
     const Ring& A = c.R[sd];
     const int m = A.m;
@@ -1564,7 +1567,7 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
       const int off = A.to[s];
       if (off < 0) continue;
       const int t = A.tl[s], L = t < 0 ? -t : t, dir = t < 0 ? -1 : 1;
-      if (L > kShortRun) continue;
+      if (anyLong && L > kShortRun) continue;
       double* dst = O.xy + 2 * (nv0 + off);
       int w = s;
       for (int j = 0; j < L; ++j) {
@@ -1575,7 +1578,7 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
         dst[2 * j + 1] = A.y[w];
       }
     }
-    for (int i = 0; i < nF[sd]; ++i) {
+    for (int i = 0; anyLong && i < nF[sd]; ++i) {
       const int s = A.ls[i];
       const int off = A.to[s];
       const int t = A.tl[s], L = t < 0 ? -t : t;
@@ -1596,7 +1599,7 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
 }
 
 template <class G>
-__device__ __noinline__ bool grp_trace(const G& g, PairCtx& c) {
+__device__ bool grp_trace(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
   OutRegion& O = c.O;
   long long budget = 4ll * (c.R[0].used + c.R[1].used) + 16;
@@ -1666,10 +1669,11 @@ __device__ __noinline__ bool grp_trace(const G& g, PairCtx& c) {
 template <class G>
 __device__ void grp_cleanup(const G& g, PairCtx& c, int32_t* outNC, int64_t* outNV) {
   OutRegion& O = c.O;
-  // Fast pass: test every vertex of every component at once (short components one member
-  // each, long ones by the whole group).  When nothing is removable, the output stands as
-  // traced; otherwise the per-component pass below removes and compacts.
-  {
+  // Fast pass for pairs with many components: test every vertex of every component at
+  // once (short components one member each, long ones by the whole group).  When nothing
+  // is removable, the output stands as traced; otherwise (and for pairs with few
+  // components) the per-component pass below removes and compacts.
+  if (O.nc > 4) {
     int32_t* start = c.R[0].tn;          // the trace's scratch is free now
     int carry = 0;
     for (int b = 0; b < O.nc; b += g.size()) {
