@@ -1128,6 +1128,7 @@ __device__ __forceinline__ int wind(double P0x, double P0y, double P1x, double P
 // code runs with a warp per pair (WarpGroup) or, for pairs with long rings, a whole block
 // per pair (BlockGroup); every member executes every group call (uniform control flow).
 struct WarpGroup {
+  static constexpr bool kBlock = false;
   __device__ __forceinline__ int rank() const { return (int)lane_id(); }
   __device__ __forceinline__ int size() const { return 32; }
   __device__ __forceinline__ void sync() const { __syncwarp(); }
@@ -1152,6 +1153,7 @@ struct WarpGroup {
 // begins with a barrier so the scratch of the previous call is free.
 constexpr int kBlockLabelThreads = 256;
 struct BlockGroup {
+  static constexpr bool kBlock = true;
   long long* sm;        // kBlockLabelThreads / 32 + 1 entries
   __device__ __forceinline__ int rank() const { return (int)threadIdx.x; }
   __device__ __forceinline__ int size() const { return kBlockLabelThreads; }
@@ -1452,20 +1454,11 @@ __device__ void grp_step6(const G& g, PairCtx& c) {
   g.sync();
 }
 
-// Tracing when neither ring has added vertices (rings in slot order): each run from V to
-// the next vertex with the target entry/exit flag (or back at the start) is found with a
-// warp ballot and copied with coalesced stores.
-// Tracing from a run table.  With entry/exit flags alternating along both rings (checked
-// here), every run of the sequential walk goes from a flagged vertex to the adjacent
-// flagged vertex in its direction, and the next run starts at that vertex's neighbour.
-// Phase 1 (parallel) lists the flagged slots of each ring and gives each its run: the
-// length (signed by direction) and the next run's start.  Phase 2 (one member) follows the
-// runs in the order of the sequential walk -- components from the first unvisited crossing
-// of P, in P's slot order -- and assigns each run its output offset.  Phase 3 (parallel)
-// copies the runs.  Returns 0 when done, 1 when the flags do not alternate (the caller
-// then runs the general walk), -1 on a capacity or trace error.
+// Run-table tracing for warp-sized pairs: the table is kept per ring slot (tl, tn, to),
+// which saves the slot-to-index translation of the indexed variant below; the walk marks
+// visited vertices in the rings' intersection flags.  Same phases and results.
 template <class G>
-__device__ int grp_trace_runs(const G& g, PairCtx& c) {
+__device__ int grp_trace_runs_slots(const G& g, PairCtx& c) {
   int nF[2];
   bool mismatch = false;     // a flagged vertex that is not a crossing, or the reverse
   for (int sd = 0; sd < 2; ++sd) {
@@ -1598,6 +1591,165 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
   return 0;
 }
 
+// Tracing from a run table.  With entry/exit flags alternating along both rings (checked
+// here), every run of the sequential walk goes from a flagged vertex to the adjacent
+// flagged vertex in its direction, and the next run starts at that vertex's neighbour.
+// Phase 1 (parallel) lists the flagged slots of each ring and gives each flagged vertex
+// (by its index in that list) its run: the length, signed by direction, and the index of
+// the next run's start on the other ring.  Phase 2 (one member) follows the runs in the
+// order of the sequential walk -- components from the first unvisited crossing of P, in
+// P's slot order -- and assigns each run its output offset.  Phase 3 (parallel) copies
+// the runs.  Indexing the table by flagged vertex keeps the walk's visited marks in the
+// table itself, so the walk touches no ring array.  Returns 0 when done, 1
+// when the flags do not alternate (the caller then runs the general walk), -1 on a
+// capacity or trace error.
+template <class G>
+__device__ int grp_trace_runs(const G& g, PairCtx& c) {
+  int nF[2];
+  bool mismatch = false;     // a flagged vertex that is not a crossing, or the reverse
+  for (int sd = 0; sd < 2; ++sd) {
+    Ring& A = c.R[sd];
+    int carry = 0;
+    for (int b = 0; b < A.m; b += g.size()) {
+      const int s = b + g.rank();
+      const int f = (s < A.m && (A.ee[s] == E_ENTRY || A.ee[s] == E_EXIT)) ? 1 : 0;
+      if (s < A.m && (f != 0) != (A.it[s] && A.lb[s] == L_CROSSING)) mismatch = true;
+      int tot;
+      const int incl = g.incl_scan(f, tot);
+      if (f) { A.ls[carry + incl - 1] = s; A.to[s] = carry + incl - 1; }   // slot -> index
+      carry += tot;
+    }
+    nF[sd] = carry;
+  }
+  if (g.any(mismatch)) return 1;
+  if (nF[0] == 0 && nF[1] == 0) return 0;
+  // run table by list index, in the rings' scratch arrays: length RL, next start RN (sign
+  // bit = visited), output offset RO.  The slot -> index map in `to` is read until phase 1
+  // ends; the offsets take its place then.  (Pointers are selected per side in registers.)
+  int32_t* const RL0 = c.R[0].tl; int32_t* const RL1 = c.R[1].tl;
+  int32_t* const RN0 = c.R[0].tn; int32_t* const RN1 = c.R[1].tn;
+  int32_t* const RO0 = c.R[0].to; int32_t* const RO1 = c.R[1].to;
+#define RL_(sd) ((sd) ? RL1 : RL0)
+#define RN_(sd) ((sd) ? RN1 : RN0)
+#define RO_(sd) ((sd) ? RO1 : RO0)
+  bool bad = nF[0] < 2 || nF[1] < 2;
+  bool longRun = false;
+  for (int sd = 0; sd < 2 && !bad; ++sd) {
+    Ring& A = c.R[sd];
+    const Ring& B = c.R[1 - sd];
+    const int n = nF[sd], m = A.m;
+    for (int i = g.rank(); i < n; i += g.size()) {
+      const int s = A.ls[i];
+      const int8_t e = A.ee[s];
+      if (A.ee[A.ls[(i + 1 < n) ? i + 1 : 0]] == e) { bad = true; continue; }   // alternation
+      const int nb = A.nb[s];
+      if (nb < 0 || nb >= B.m || B.ee[nb] != toggled(e)) { bad = true; continue; }
+      const int8_t st = toggled(e);
+      const int dir = ((st == E_EXIT) ^ c.uni) ? 1 : -1;
+      const int W = A.ls[(i + dir + n) % n];
+      int L = dir > 0 ? W - s : s - W;
+      if (L <= 0) L += m;
+      const int nbW = A.nb[W];
+      if (nbW < 0 || nbW >= B.m) { bad = true; continue; }
+      RL_(sd)[i] = dir * L;
+      RN_(sd)[i] = B.to[nbW];          // a flagged twin (checked): its index in B's list
+      if (L > 32) longRun = true;
+    }
+  }
+  if (g.any(bad)) return 1;
+  for (int sd = 0; sd < 2; ++sd)
+    for (int i = g.rank(); i < nF[sd]; i += g.size()) RO_(sd)[i] = -1;
+  const bool anyLong = g.any(longRun);
+  // ---- phase 2: the walk over the run table, one member
+  constexpr int32_t kSeen = (int32_t)0x80000000u;
+  OutRegion& O = c.O;
+  int status = 0;
+  int64_t nv = O.nv;
+  int nc = O.nc;
+  if (g.rank() == 0) {
+    const int64_t nv0 = O.nv;
+    const int nFP = nF[0], nFQ = nF[1];
+    long long budget = (long long)nFP + nFQ + 4;
+    for (int I = 0; I < nFP && status == 0; ++I) {
+      if (RN_(0)[I] < 0) continue;                       // visited
+      if (nc >= O.ccap) { status = -1; fail(c, DEV_CAPACITY); break; }
+      RN_(0)[I] |= kSeen;
+      int side = 0, V = I;
+      int64_t csz = 0;
+      for (;;) {
+        const int t = RL_(side)[V], L = t < 0 ? -t : t, n = side ? nFQ : nFP;
+        int W = V + (t < 0 ? -1 : 1);
+        if (W >= n) W -= n;
+        if (W < 0) W += n;
+        RO_(side)[V] = (int32_t)(nv - nv0);
+        nv += L;
+        csz += L;
+        const int V2 = RN_(side)[V] & 0x7fffffff;
+        RN_(side)[W] |= kSeen;
+        if (side == 0 && W == I) break;
+        side ^= 1;
+        if (side == 0 && V2 == I) break;
+        RN_(side)[V2] |= kSeen;
+        V = V2;
+        if (--budget < 0) { status = -1; fail(c, DEV_TRACE); break; }
+      }
+      if (status == 0) {
+        if (nv > O.vcap) { status = -1; fail(c, DEV_CAPACITY); break; }
+        O.csz[nc++] = (int32_t)csz;
+      }
+    }
+  }
+  status = g.bcast0(status);
+  if (status != 0) return -1;
+  const int64_t nv0 = O.nv;
+  O.nv = g.bcast0((long long)nv);
+  O.nc = g.bcast0(nc);
+  // ---- phase 3: copy every run to its place; short runs one member each, long runs by
+  // the whole group (no barrier between runs: runs write disjoint ranges)
+  constexpr int kShortRun = 32;      // the run-length threshold of phase 1's longRun
+  for (int sd = 0; sd < 2; ++sd) {
+    const Ring& A = c.R[sd];
+    const int m = A.m;
+    for (int i = g.rank(); i < nF[sd]; i += g.size()) {
+      const int off = RO_(sd)[i];
+      if (off < 0) continue;
+      const int t = RL_(sd)[i], L = t < 0 ? -t : t, dir = t < 0 ? -1 : 1;
+      if (anyLong && L > kShortRun) continue;
+      double* dst = O.xy + 2 * (nv0 + off);
+      int w = A.ls[i];
+      for (int j = 0; j < L; ++j) {
+        w += dir;
+        if (w >= m) w -= m;
+        if (w < 0) w += m;
+        dst[2 * j] = A.x[w];
+        dst[2 * j + 1] = A.y[w];
+      }
+    }
+    for (int i = 0; anyLong && i < nF[sd]; ++i) {
+      const int off = RO_(sd)[i];
+      const int t = RL_(sd)[i], L = t < 0 ? -t : t;
+      if (off < 0 || L <= kShortRun) continue;
+      const int dir = t < 0 ? -1 : 1, s0 = A.ls[i];
+      double* dst = O.xy + 2 * (nv0 + off);
+      for (int j = g.rank(); j < L; j += g.size()) {
+        int w = s0 + dir * (j + 1);
+        w %= m;
+        if (w < 0) w += m;
+        dst[2 * j] = A.x[w];
+        dst[2 * j + 1] = A.y[w];
+      }
+    }
+  }
+  g.sync();
+  return 0;
+#undef RL_
+#undef RN_
+#undef RO_
+}
+
+// Tracing when neither ring has added vertices (rings in slot order): each run from V to
+// the next vertex with the target entry/exit flag (or back at the start) is found with a
+// group ballot and copied with coalesced stores.
 template <class G>
 __device__ bool grp_trace(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
@@ -1851,7 +2003,9 @@ __device__ void label_trace_pair(const G& g, const LabelArgs& a, int64_t k) {
     g.sync();
     if (!ok) return;
   } else {
-    const int r = grp_trace_runs(g, c);
+    int r;
+    if constexpr (G::kBlock) r = grp_trace_runs(g, c);
+    else r = grp_trace_runs_slots(g, c);
     if (r < 0) return;
     if (r > 0 && !grp_trace(g, c)) return;
   }
