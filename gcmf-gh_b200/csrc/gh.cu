@@ -135,6 +135,25 @@ edge_filter_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, int32_t* __re
 // Pairs whose filtered edge grid exceeds ClipParams::bin_grid edge pairs are not
 // enumerated pair by pair: their edges are binned on a uniform grid (bin_* kernels).
 
+// edge -> pair: a warp per pair fills the entries of its cnt[k] edges starting at off[k]
+__global__ void range_owner_kernel(const int64_t* __restrict__ off, const int32_t* __restrict__ cnt, int64_t K,
+                                   int32_t* __restrict__ owner) {
+  const int64_t k = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  if (k >= K) return;
+  const int64_t o = off[k];
+  const int n = cnt[k];
+  for (int j = lane_id(); j < n; j += 32) owner[o + j] = (int32_t)k;
+}
+
+// chunk -> pair: a warp per pair fills its chunks' entries
+__global__ void chunk_pair_kernel(const int64_t* __restrict__ chunkOff, const int64_t* __restrict__ nchunk, int64_t K,
+                                  int32_t* __restrict__ chunkPair) {
+  const int64_t k = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  if (k >= K) return;
+  const int64_t o = chunkOff[k], n = nchunk[k];
+  for (int64_t j = lane_id(); j < n; j += 32) chunkPair[o + j] = (int32_t)k;
+}
+
 __global__ void chunk_count_kernel(const int32_t* __restrict__ cP, const int32_t* __restrict__ cQ,
                                    int64_t K, int64_t* __restrict__ nchunk, int64_t* __restrict__ bigList,
                                    unsigned long long* __restrict__ nBig, int64_t binGrid) {
@@ -166,11 +185,11 @@ intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* 
                  const int64_t* __restrict__ offP, const int64_t* __restrict__ offQ,
                  const int32_t* __restrict__ LP, const int32_t* __restrict__ LQ, double eps,
                  int32_t* __restrict__ chunkRec, int32_t* __restrict__ chunkQ,
-                 const int64_t* __restrict__ chunkRecOff, const int64_t* __restrict__ recOff, Records R) {
+                 const int64_t* __restrict__ chunkRecOff, const int64_t* __restrict__ recOff, Records R,
+                 const int32_t* __restrict__ chunkPair) {
   int64_t c = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
   if (c >= nChunks) return;
-  // pair of this chunk: last k with chunkOff[k] <= c (pairs without chunks are skipped)
-  int64_t k = upper_index(chunkOff, K, c);
+  const int64_t k = chunkPair[c];                  // the pair this chunk belongs to
   const int nq = cQ[k];
   const int64_t W = (int64_t)cP[k] * nq;
   const int64_t t0 = (c - chunkOff[k]) * kChunk;
@@ -188,8 +207,14 @@ intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* 
     int pe = 0, qe = 0;
     double alpha = 0, beta = 0;
     if (t < W) {
-      pe = lp[t / nq];
-      qe = lq[t % nq];
+      if (W <= INT32_MAX) {                         // 32-bit division when it suffices
+        const int tt = (int)t, r = tt / nq;
+        pe = lp[r];
+        qe = lq[tt - r * nq];
+      } else {
+        pe = lp[t / nq];
+        qe = lq[t % nq];
+      }
       double2 P1 = __ldg(pv + pe), P2 = __ldg(pv + (pe + 1 < np_ ? pe + 1 : 0));
       double2 Q1 = __ldg(qv + qe), Q2 = __ldg(qv + (qe + 1 < nq_ ? qe + 1 : 0));
       if (edge_boxes_touch(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y)) {
@@ -481,9 +506,9 @@ __device__ __forceinline__ void write_inserted(const EdgeFill& f, const Records&
 
 template <int kSide>
 __device__ __forceinline__ bool edge_fill_info(const LayerDev& Lb, const LayerDev& Lo, const PairDev& D,
-                                               const int64_t* eoff, int64_t K, const int64_t* vpos,
+                                               const int64_t* eoff, const int32_t* edgePair, const int64_t* vpos,
                                                const int64_t* regOff, const int32_t* m, int64_t e, EdgeFill& f) {
-  int64_t k = upper_index(eoff, K, e);
+  const int64_t k = edgePair[e];
   if (D.status[k] != 0) return false;
   const int n = kSide == 0 ? D.nP[k] : D.nQ[k];
   if ((int)(e - eoff[k]) >= n) return false;
@@ -500,7 +525,7 @@ __device__ __forceinline__ bool edge_fill_info(const LayerDev& Lb, const LayerDe
 
 template <int kSide>
 __global__ void ring_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R,
-                                 const int64_t* __restrict__ eoff, int64_t nE, int64_t K,
+                                 const int64_t* __restrict__ eoff, int64_t nE, const int32_t* __restrict__ edgePair,
                                  const int64_t* __restrict__ vpos, const int64_t* __restrict__ regOff,
                                  const int32_t* __restrict__ m, RingSet S, int64_t* __restrict__ slotOfRec,
                                  const int64_t* __restrict__ insCursorBase, int32_t* __restrict__ insCursor,
@@ -509,7 +534,7 @@ __global__ void ring_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R,
   int64_t e = (int64_t)blockIdx.x * kThreads + threadIdx.x;
   if (e >= nE) return;
   EdgeFill f;
-  if (!edge_fill_info<kSide>(Lb, Lo, D, eoff, K, vpos, regOff, m, e, f)) return;
+  if (!edge_fill_info<kSide>(Lb, Lo, D, eoff, edgePair, vpos, regOff, m, e, f)) return;
   const int le = (int)(e - eoff[f.k]);
   const double2 A = __ldg((kSide == 0 ? f.pvx : f.qvx) + le);
   const int64_t g = f.base + f.s0;
@@ -573,7 +598,8 @@ __device__ void bitonic_sort(uint64_t* key, uint32_t* tie, uint32_t* idx, int np
 
 template <int kSide>
 __global__ void __launch_bounds__(kHeavyThreads)
-heavy_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R, const int64_t* __restrict__ eoff, int64_t K,
+heavy_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R, const int64_t* __restrict__ eoff,
+                  const int32_t* __restrict__ edgePair,
                   const int64_t* __restrict__ vpos, const int64_t* __restrict__ regOff,
                   const int32_t* __restrict__ m, RingSet S, int64_t* __restrict__ slotOfRec,
                   const int64_t* __restrict__ insCursorBase, const int32_t* __restrict__ insCursor,
@@ -587,7 +613,7 @@ heavy_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R, const int64_t*
   const unsigned long long nh = *nHeavy;
   for (unsigned long long h = blockIdx.x; h < nh; h += gridDim.x) {
     const int64_t e = heavy[h];
-    if (threadIdx.x == 0) edge_fill_info<kSide>(Lb, Lo, D, eoff, K, vpos, regOff, m, e, f);
+    if (threadIdx.x == 0) edge_fill_info<kSide>(Lb, Lo, D, eoff, edgePair, vpos, regOff, m, e, f);
     __syncthreads();
     const int64_t l0 = insCursorBase[e];
     const int cnt = insCursor[e];
@@ -2921,13 +2947,16 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int32_t* LP = A.take_n<int32_t>(nLP);
   int32_t* LQ = A.take_n<int32_t>(nLQ);
   int32_t* chunkRec = A.take_n<int32_t>(nCh);
+  int32_t* chunkPair = A.take_n<int32_t>(nCh);
   int32_t* chunkQ = A.take_n<int32_t>(nCh);
   int64_t* recScan = A.take_n<int64_t>(nCh);
   int64_t* qScan = A.take_n<int64_t>(nCh);
   void* stC = A.take(scan_temp_bytes(std::max<int64_t>(nCh, 1)));
   int64_t* binRec = A.take_n<int64_t>(K);
   int64_t* binQ = A.take_n<int64_t>(K);
-  if (!LP || !LQ || !chunkRec || !chunkQ || !recScan || !qScan || !stC || !binRec || !binQ) return ST_OUT_OF_MEMORY;
+  if (!LP || !LQ || !chunkRec || !chunkPair || !chunkQ || !recScan || !qScan || !stC || !binRec || !binQ)
+    return ST_OUT_OF_MEMORY;
+  if (nCh > 0) { chunk_pair_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(chunkOff, nchunk, K, chunkPair); note_launch(); }
   cudaMemsetAsync(binRec, 0, K * sizeof(int64_t), s);
   cudaMemsetAsync(binQ, 0, K * sizeof(int64_t), s);
   { edge_filter_kernel<1><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ); note_launch(); }
@@ -2935,7 +2964,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   Records R{};
   if (nCh > 0) {
     { (prm.exact ? intersect_kernel<0, 1> : intersect_kernel<0, 0>)<<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, chunkRec, chunkQ, nullptr, nullptr, R); note_launch(); }
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, chunkRec, chunkQ, nullptr, nullptr, R, chunkPair); note_launch(); }
     exclusive_scan_i32(chunkRec, recScan, nCh, nullptr, stC, d_err, s);
     exclusive_scan_i32(chunkQ, qScan, nCh, nullptr, stC, d_err, s);
   }
@@ -3033,7 +3062,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (!R.p || !R.q || !R.a || !R.b || !R.t || !R.k) return ST_OUT_OF_MEMORY;
   if (nCh > 0)
     { (prm.exact ? intersect_kernel<1, 1> : intersect_kernel<1, 0>)<<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, recOff, R); note_launch(); }
+        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, recOff, R, chunkPair); note_launch(); }
   for (auto& W : bigs) {
     const int64_t k = W.info.k;
     { add_offset_kernel<<<blocks_for(W.info.cp), kThreads, 0, s>>>(W.recPos, W.info.cp, recOff + k); note_launch(); }
@@ -3135,19 +3164,25 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // edge -> pair tables for the fill kernels
+    int32_t* edgeP = A.take_n<int32_t>(nEP);
+    int32_t* edgeQ = A.take_n<int32_t>(nEQ);
+    if (!edgeP || !edgeQ) return ST_OUT_OF_MEMORY;
+    { range_owner_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(eoffP, D.nP, K, edgeP); note_launch(); }
+    { range_owner_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(eoffQ, D.nQ, K, edgeQ); note_launch(); }
     if (nEP > 0) {
       cudaMemsetAsync(nHeavy, 0, sizeof(unsigned long long), s);
-      { ring_fill_kernel<0><<<blocks_for(nEP), kThreads, 0, s>>>(Lb, Lo, D, R, eoffP, nEP, K, vposP, regP, mP, SP,
+      { ring_fill_kernel<0><<<blocks_for(nEP), kThreads, 0, s>>>(Lb, Lo, D, R, eoffP, nEP, edgeP, vposP, regP, mP, SP,
                                                                slotP, insBaseP, curP, insListP, heavy, nHeavy); note_launch(); }
-      { heavy_fill_kernel<0><<<2 * nsm, kHeavyThreads, smem, s>>>(Lb, Lo, D, R, eoffP, K, vposP, regP, mP, SP, slotP,
+      { heavy_fill_kernel<0><<<2 * nsm, kHeavyThreads, smem, s>>>(Lb, Lo, D, R, eoffP, edgeP, vposP, regP, mP, SP, slotP,
                                                                   insBaseP, curP, insListP, heavy, nHeavy, gkey, gtie,
                                                                   gidx); note_launch(); }
     }
     if (nEQ > 0) {
       cudaMemsetAsync(nHeavy + 1, 0, sizeof(unsigned long long), s);
-      { ring_fill_kernel<1><<<blocks_for(nEQ), kThreads, 0, s>>>(Lb, Lo, D, R, eoffQ, nEQ, K, vposQ, regQ, mQ, SQ,
+      { ring_fill_kernel<1><<<blocks_for(nEQ), kThreads, 0, s>>>(Lb, Lo, D, R, eoffQ, nEQ, edgeQ, vposQ, regQ, mQ, SQ,
                                                                slotQ, insBaseQ, curQ, insListQ, heavy, nHeavy + 1); note_launch(); }
-      { heavy_fill_kernel<1><<<2 * nsm, kHeavyThreads, smem, s>>>(Lb, Lo, D, R, eoffQ, K, vposQ, regQ, mQ, SQ, slotQ,
+      { heavy_fill_kernel<1><<<2 * nsm, kHeavyThreads, smem, s>>>(Lb, Lo, D, R, eoffQ, edgeQ, vposQ, regQ, mQ, SQ, slotQ,
                                                                   insBaseQ, curQ, insListQ, heavy, nHeavy + 1, gkey, gtie,
                                                                   gidx); note_launch(); }
     }
