@@ -68,18 +68,34 @@ __global__ void gather_sorted_kernel(const double* __restrict__ mbr, const uint3
   S.x1[i] = m.x; S.y1[i] = m.y; S.x2[i] = m.z; S.y2[i] = m.w; S.id[i] = id;
 }
 
-// first index with a[i] >= x
-__device__ __forceinline__ int64_t lower_bound_d(const double* a, int64_t n, double x) {
-  int64_t lo = 0, hi = n;
-  while (lo < hi) { int64_t m = (lo + hi) >> 1; if (a[m] < x) lo = m + 1; else hi = m; }
-  return lo;
+// Warp-cooperative search in an ascending array (all 32 lanes call it with the same
+// arguments): the first index whose element is not "before" x, where before means
+// a[i] < x (lower bound) or a[i] <= x (upper bound).  Each round the lanes probe 32
+// evenly spaced elements at once and the range shrinks 32-fold, so a search costs
+// log32(n) dependent loads instead of log2(n).
+template <bool kUpper>
+__device__ __forceinline__ int64_t warp_bound(const double* a, int64_t n, double x) {
+  int64_t lo = 0, hi = n;                       // the answer lies in [lo, hi]
+  const int l = (int)lane_id();
+  while (hi - lo > 32) {
+    const int64_t seg = (hi - lo + 31) / 32;
+    int64_t p = lo + (int64_t)(l + 1) * seg - 1;
+    const bool in = p < hi;
+    const double v = in ? a[p] : 0.0;
+    const bool before = in && (kUpper ? v <= x : v < x);
+    const int c = __popc(__ballot_sync(0xffffffffu, before));
+    const int64_t plo = lo + (int64_t)c * seg - 1;            // last probe that is before
+    const int64_t phi = lo + (int64_t)(c + 1) * seg - 1;      // first probe that is not
+    if (c > 0) lo = plo + 1;
+    if (c < 32 && phi < hi) hi = phi;
+  }
+  const int64_t q = lo + l;
+  const bool before = q < hi && (kUpper ? a[q] <= x : a[q] < x);
+  return lo + __popc(__ballot_sync(0xffffffffu, before));
 }
-// first index with a[i] > x
-__device__ __forceinline__ int64_t upper_bound_d(const double* a, int64_t n, double x) {
-  int64_t lo = 0, hi = n;
-  while (lo < hi) { int64_t m = (lo + hi) >> 1; if (a[m] <= x) lo = m + 1; else hi = m; }
-  return lo;
-}
+// first index with a[i] >= x / with a[i] > x
+__device__ __forceinline__ int64_t lower_bound_d(const double* a, int64_t n, double x) { return warp_bound<false>(a, n, x); }
+__device__ __forceinline__ int64_t upper_bound_d(const double* a, int64_t n, double x) { return warp_bound<true>(a, n, x); }
 
 // ---------------------------------------------------------------- J2: sweep
 // The reference sorts all x endpoints (stable on endpoint index, base before overlay)
