@@ -304,7 +304,15 @@ refine_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const in
     int64_t t = t0 + lane_id();
     bool hit = false;
     if (t < total) {
-      int be = bl[t / no], oe = ol[t % no];
+      int be, oe;
+      if (total <= INT32_MAX) {                    // 32-bit division when it suffices
+        const int tt = (int)t, r = tt / no;
+        be = bl[r];
+        oe = ol[tt - r * no];
+      } else {
+        be = bl[t / no];
+        oe = ol[t % no];
+      }
       double2 b1 = __ldg(bv + be), b2 = __ldg(bv + ((be < bV - 1) ? be + 1 : 0));
       double2 o1 = __ldg(ov + oe), o2 = __ldg(ov + ((oe < oV - 1) ? oe + 1 : 0));
       hit = segment_hit(b1.x, b1.y, b2.x, b2.y, o1.x, o1.y, o2.x, o2.y);
