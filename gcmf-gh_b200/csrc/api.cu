@@ -360,6 +360,7 @@ gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* c, int key, int64_t value) {
   if (key == GCMFGH_TUNE_BIN_GRID) c->prm.bin_grid = value;
   else if (key == GCMFGH_TUNE_BIG_LABEL) c->prm.big_label_min = value;
   else if (key == GCMFGH_TUNE_MID_LABEL) c->prm.mid_label_min = value;
+  else if (key == GCMFGH_TUNE_TILE_LABEL) c->prm.tile_label_max = value;
   else return GCMFGH_INVALID_ARGUMENT;
   return GCMFGH_OK;
 }

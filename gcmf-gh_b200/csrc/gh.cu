@@ -1175,6 +1175,44 @@ struct WarpGroup {
   }
 };
 
+// A tile of W lanes (W = 8 or 16) of one warp: the warp's tiles work on different pairs
+// side by side, each with its own lane mask.
+template <int W>
+struct TileGroup {
+  static constexpr bool kBlock = false;
+  unsigned mask;
+  int base;
+  __device__ __forceinline__ TileGroup() {
+    base = (int)(lane_id() & ~(unsigned)(W - 1));
+    mask = ((1u << W) - 1u) << base;
+  }
+  __device__ __forceinline__ int rank() const { return (int)lane_id() - base; }
+  __device__ __forceinline__ int size() const { return W; }
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+  __device__ __forceinline__ bool all(bool v) const { return (__ballot_sync(mask, v) & mask) == mask; }
+  __device__ __forceinline__ bool any(bool v) const { return (__ballot_sync(mask, v) & mask) != 0u; }
+  __device__ __forceinline__ int sum(int v) const {
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, W);
+    return v;
+  }
+  template <class T>
+  __device__ __forceinline__ T bcast0(T v) const { return __shfl_sync(mask, v, 0, W); }
+  __device__ __forceinline__ int first(bool hit) const {
+    const unsigned m = (__ballot_sync(mask, hit) & mask) >> base;
+    return m ? __ffs(m) - 1 : -1;
+  }
+  __device__ __forceinline__ int incl_scan(int v, int& total) const {
+#pragma unroll
+    for (int o = 1; o < W; o <<= 1) {
+      const int w = __shfl_up_sync(mask, v, o, W);
+      if (rank() >= o) v += w;
+    }
+    total = __shfl_sync(mask, v, W - 1, W);
+    return v;
+  }
+};
+
 // Block-wide versions over shared scratch (kBlockLabelThreads / 32 warps); each call
 // begins with a barrier so the scratch of the previous call is free.
 constexpr int kBlockLabelThreads = 256;
@@ -1963,6 +2001,7 @@ struct LabelArgs {
   int32_t* outNC; int64_t* outNV;
   ClipParams prm;
   int* err;
+  int64_t tileLabelMax;       // rings up to: a tile of lanes per pair
   int64_t midLabelMin;        // rings above: a block per pair
   int64_t bigLabelMin;        // rings above: the grid path
   const int64_t* midList;     // pairs for the block kernel
@@ -2051,7 +2090,23 @@ label_trace_kernel(LabelArgs a) {
   if (a.D.status[k] != 0) return;
   const int64_t slots = (int64_t)a.mP[k] + a.mQ[k];
   if (slots > a.midLabelMin) return;                       // block or grid path
+  if (slots <= a.tileLabelMax) return;                     // tile path
   WarpGroup g;
+  label_trace_pair<EX>(g, a, k);
+}
+
+// Pairs whose merged rings have at most tileLabelMax slots: a tile of kTileLanes lanes per
+// pair, 32 / kTileLanes consecutive pairs per warp.
+constexpr int kTileLanes = 8;
+template <int EX>
+__global__ void __launch_bounds__(128, 4)
+label_trace_tile_kernel(LabelArgs a) {
+  const int64_t k = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / kTileLanes) +
+                    (lane_id() / kTileLanes);
+  if (k >= a.K || a.D.status[k] != 0) return;
+  const int64_t slots = (int64_t)a.mP[k] + a.mQ[k];
+  if (slots > a.tileLabelMax || slots > a.midLabelMin) return;
+  TileGroup<kTileLanes> g;
   label_trace_pair<EX>(g, a, k);
 }
 
@@ -3219,7 +3274,8 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     LabelArgs la{D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ, SP, SQ, oxy, vOff, vcap, ocsz, cOff, ccap, nc, nv,
-                 prm, d_err, std::min(prm.mid_label_min, prm.big_label_min), prm.big_label_min, mlist, mcnt, mcnt + 1};
+                 prm, d_err, prm.tile_label_max, std::min(prm.mid_label_min, prm.big_label_min), prm.big_label_min,
+                 mlist, mcnt, mcnt + 1};
     // long pairs: a block each, on the auxiliary stream when there is one, so they start
     // first and overlap the warp-per-pair kernel instead of trailing it
     cudaStream_t ls = s;
@@ -3234,6 +3290,10 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
                                                                mlist, mcnt); note_launch(); }
     { (prm.exact ? label_trace_block_kernel<1> : label_trace_block_kernel<0>)<<<2 * nsm, kBlockLabelThreads, 0, ls>>>(la); note_launch(); }
     { (prm.exact ? label_trace_kernel<1> : label_trace_kernel<0>)<<<(unsigned)((K + 3) / 4), 128, 0, s>>>(la); note_launch(); }
+    if (prm.tile_label_max > 0) {
+      const int64_t pairsPerBlock = 4 * (32 / kTileLanes);
+      { (prm.exact ? label_trace_tile_kernel<1> : label_trace_tile_kernel<0>)<<<(unsigned)((K + pairsPerBlock - 1) / pairsPerBlock), 128, 0, s>>>(la); note_launch(); }
+    }
     if (ls != s) {
       cudaEventRecord(join, ls);
       cudaStreamWaitEvent(s, join, 0);

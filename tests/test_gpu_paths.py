@@ -10,21 +10,22 @@ from gcmfgh import synth
 
 pytestmark = pytest.mark.gpu
 
-BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT = 1 << 24, 1 << 18, 1 << 10
+BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT, TILE_DEFAULT = 1 << 24, 1 << 18, 1 << 10, 128
 
 
 def _run(engine, base, ovl, pid, qid, union=False, bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT,
-         mid_label=MID_DEFAULT, exact=False):
+         mid_label=MID_DEFAULT, exact=False, tile_label=TILE_DEFAULT):
     import gcmfgh
     db, do = gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl)
-    engine.set_tuning(bin_grid=bin_grid, big_label=big_label, mid_label=mid_label)
+    engine.set_tuning(bin_grid=bin_grid, big_label=big_label, mid_label=mid_label, tile_label=tile_label)
     engine.set_params(1e-7, 1e-7, union)
     engine.set_precision(exact)
     try:
         info = engine.clip_batch(db, do, pid, qid)
         r = engine.clip_result()
     finally:
-        engine.set_tuning(bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT, mid_label=MID_DEFAULT)
+        engine.set_tuning(bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT, mid_label=MID_DEFAULT,
+                          tile_label=TILE_DEFAULT)
         engine.set_params(1e-7, 1e-7, False)
         engine.set_precision(False)
     return info, r
@@ -66,6 +67,25 @@ def test_block_labelling_every_pair(engine, union, exact):
     base, ovl, ids = _pairs_layers(synth.random_star_pairs(23, 1200, 3, 120, spread=0.8))
     _, r = _run(engine, base, ovl, ids, ids, union=union, mid_label=0, exact=exact)
     _assert_equal(r, pyoracle.clip_batch(base, ovl, ids, ids, union=union, exact=exact))
+
+
+@pytest.mark.parametrize("union", [False, True])
+@pytest.mark.parametrize("exact", [False, True])
+@pytest.mark.parametrize("tile_label", [0, 1 << 10])
+def test_tile_and_warp_labelling_every_pair(engine, union, exact, tile_label):
+    """Every warp-sized pair labelled by a tile of 8 lanes (tile_label 2^10), or by a whole
+    warp with tiles switched off (0)."""
+    base, ovl, ids = _pairs_layers(synth.random_star_pairs(24, 1500, 3, 90, spread=0.8))
+    _, r = _run(engine, base, ovl, ids, ids, union=union, tile_label=tile_label, exact=exact)
+    _assert_equal(r, pyoracle.clip_batch(base, ovl, ids, ids, union=union, exact=exact))
+
+
+def test_tile_labelling_degenerate_cases(engine):
+    from test_gpu_clip import degenerate_pairs
+    base, ovl, ids = _pairs_layers(degenerate_pairs())
+    for union in (False, True):
+        _, r = _run(engine, base, ovl, ids, ids, union=union, tile_label=1 << 10)
+        _assert_equal(r, pyoracle.clip_batch(base, ovl, ids, ids, union=union))
 
 
 def test_block_labelling_degenerate_cases(engine):
