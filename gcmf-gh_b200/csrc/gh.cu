@@ -1175,7 +1175,7 @@ struct WarpGroup {
   }
 };
 
-// A tile of W lanes (W = 8 or 16) of one warp: the warp's tiles work on different pairs
+// A tile of W lanes (a power of two below 32) of one warp: the tiles work on different pairs
 // side by side, each with its own lane mask.
 template <int W>
 struct TileGroup {
@@ -2097,7 +2097,7 @@ label_trace_kernel(LabelArgs a) {
 
 // Pairs whose merged rings have at most tileLabelMax slots: a tile of kTileLanes lanes per
 // pair, 32 / kTileLanes consecutive pairs per warp.
-constexpr int kTileLanes = 8;
+constexpr int kTileLanes = 2;
 template <int EX>
 __global__ void __launch_bounds__(128, 4)
 label_trace_tile_kernel(LabelArgs a) {

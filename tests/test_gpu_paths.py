@@ -10,7 +10,7 @@ from gcmfgh import synth
 
 pytestmark = pytest.mark.gpu
 
-BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT, TILE_DEFAULT = 1 << 24, 1 << 18, 1 << 10, 128
+BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT, TILE_DEFAULT = 1 << 24, 1 << 18, 1 << 10, 96
 
 
 def _run(engine, base, ovl, pid, qid, union=False, bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT,
@@ -73,7 +73,7 @@ def test_block_labelling_every_pair(engine, union, exact):
 @pytest.mark.parametrize("exact", [False, True])
 @pytest.mark.parametrize("tile_label", [0, 1 << 10])
 def test_tile_and_warp_labelling_every_pair(engine, union, exact, tile_label):
-    """Every warp-sized pair labelled by a tile of 8 lanes (tile_label 2^10), or by a whole
+    """Every warp-sized pair labelled by a tile of 2 lanes (tile_label 2^10), or by a whole
     warp with tiles switched off (0)."""
     base, ovl, ids = _pairs_layers(synth.random_star_pairs(24, 1500, 3, 90, spread=0.8))
     _, r = _run(engine, base, ovl, ids, ids, union=union, tile_label=tile_label, exact=exact)
