@@ -26,6 +26,32 @@ inline unsigned blocks_for_warps(int64_t warps) {
   return (unsigned)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
 }
 inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+inline unsigned blocks_for_tiles(int64_t units, int w) {
+  const int64_t per = (int64_t)kThreads / w;
+  return (unsigned)((units + per - 1) / per);
+}
+
+// W lanes of a warp working on one pair (W = 32: the whole warp).  Pairs are small in the
+// bulk of a join, so narrow tiles put more pairs in flight per warp; the launches split
+// pairs by size between a narrow-tile pass and a whole-warp pass.
+template <int W>
+struct JTile {
+  int lane, base;
+  unsigned mask;
+  __device__ __forceinline__ JTile() {
+    lane = (int)(threadIdx.x & (W - 1));
+    base = (int)(lane_id() & ~(unsigned)(W - 1));
+    mask = (W == 32) ? 0xffffffffu : (((1u << W) - 1u) << base);
+  }
+  __device__ __forceinline__ unsigned ballot(bool v) const {
+    const unsigned b = __ballot_sync(mask, v);
+    return (W == 32) ? b : ((b >> base) & ((1u << W) - 1u));
+  }
+  __device__ __forceinline__ unsigned lanes_below() const { return (1u << lane) - 1u; }
+  static __device__ __forceinline__ int64_t unit() {
+    return ((int64_t)blockIdx.x * kThreads + threadIdx.x) / W;
+  }
+};
 
 // ---------------------------------------------------------------- J0: MBRs
 // One warp per polygon, 128-bit vertex loads.  The MBR covers every stored vertex,
@@ -169,15 +195,17 @@ __global__ void cmbr_kernel(const uint64_t* __restrict__ keys, int64_t K, int ob
 // Crossing parity of the contained candidate's first vertex against the other polygon's
 // stored ring, edges (i, i-1) for every stored vertex i (GPU_Join.h:856-939).  A warp per
 // candidate pair; the parity of the per-lane parities equals the reference's XOR scan.
+template <int W>
 __global__ void __launch_bounds__(kThreads)
 pip_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32_t* __restrict__ po,
            const int8_t* __restrict__ pip_type, int64_t K, int8_t* __restrict__ pip_flag,
-           int8_t* __restrict__ join_flag) {
-  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+           int8_t* __restrict__ join_flag, int64_t lo, int64_t hi) {
+  const JTile<W> T;
+  const int64_t w = JTile<W>::unit();
   if (w >= K) return;
   int t = pip_type[w];
   if (t == 0) {
-    if (lane_id() == 0) { pip_flag[w] = 0; join_flag[w] = 1; }
+    if (W != 32 && T.lane == 0) { pip_flag[w] = 0; join_flag[w] = 1; }
     return;
   }
   int b = pb[w], o = po[w];
@@ -187,17 +215,18 @@ pip_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32
   const double2* pt = reinterpret_cast<const double2*>(Lp.xy) + (Lp.vps[ip] - Lp.vnum[ip]);
   const double2 P = pt[0];
   const int nv = Lr.vnum[ir];
+  if (nv <= lo || nv > hi) return;                 // the other pass takes this pair
   const double2* v = reinterpret_cast<const double2*>(Lr.xy) + (Lr.vps[ir] - nv);
   int par = 0;
-  for (int i = lane_id(); i < nv; i += 32) {
+  for (int i = T.lane; i < nv; i += W) {
     int j = (i == 0) ? nv - 1 : i - 1;
     double2 a = __ldg(v + i), c = __ldg(v + j);
     double Y1 = a.y, Y2 = c.y, X1 = a.x, X2 = c.x;
     if ((Y1 > P.y) == (Y2 > P.y)) continue;
     if (P.x < (X2 - X1) * (P.y - Y1) / (Y2 - Y1) + X1) par ^= 1;
   }
-  int inside = __popc(__ballot_sync(0xffffffffu, par)) & 1;
-  if (lane_id() == 0) { pip_flag[w] = (int8_t)inside; join_flag[w] = inside ? 0 : 1; }
+  int inside = __popc(T.ballot(par)) & 1;
+  if (T.lane == 0) { pip_flag[w] = (int8_t)inside; join_flag[w] = inside ? 0 : 1; }
 }
 
 // ---------------------------------------------------------------- J5: common-MBR filter
@@ -205,20 +234,25 @@ pip_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32
 // from vertex k to k+1 and the last one from the closing vertex back to vertex 0.
 // mode 0 counts (and drops pairs with an empty side, :604-613), mode 1 writes the
 // surviving edge ids in ascending order (Apply_CMF :676-733, 32-bit ids here).
-template <int kMode>
+template <int kMode, int W>
 __global__ void __launch_bounds__(kThreads)
 cmf_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32_t* __restrict__ po,
            const double* __restrict__ cmbr, int64_t K, int8_t* __restrict__ join_flag,
            int32_t* __restrict__ bE, int32_t* __restrict__ oE,
            const int64_t* __restrict__ bOff, const int64_t* __restrict__ oOff,
-           int32_t* __restrict__ bList, int32_t* __restrict__ oList) {
-  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+           int32_t* __restrict__ bList, int32_t* __restrict__ oList, int64_t lo, int64_t hi) {
+  const JTile<W> T;
+  const int64_t w = JTile<W>::unit();
   if (w >= K) return;
   if (!join_flag[w]) {
-    if (kMode == 0 && lane_id() == 0) { bE[w] = 0; oE[w] = 0; }
+    if (kMode == 0 && W != 32 && T.lane == 0) { bE[w] = 0; oE[w] = 0; }
     return;
   }
   if (kMode == 1 && bE[w] == 0) return;
+  {
+    const int64_t size = (int64_t)Lb.vnum[pb[w]] + Lo.vnum[po[w]];
+    if (size <= lo || size > hi) return;             // the other pass takes this pair
+  }
   double4 c = reinterpret_cast<const double4*>(cmbr)[w];
   int counts[2];
   for (int side = 0; side < 2; ++side) {
@@ -230,20 +264,20 @@ cmf_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32
     int32_t* list = nullptr;
     if (kMode == 1) { pos = side == 0 ? bOff[w] : oOff[w]; list = side == 0 ? bList : oList; }
     int cnt = 0;
-    for (int k0 = 0; k0 < nv; k0 += 32) {
-      int k = k0 + lane_id();
+    for (int k0 = 0; k0 < nv; k0 += W) {
+      int k = k0 + T.lane;
       bool hit = false;
       if (k < nv) {
         double2 a = __ldg(v + k), b = __ldg(v + ((k < nv - 1) ? k + 1 : 0));
         hit = edge_touches_box(a.x, a.y, b.x, b.y, c.x, c.y, c.z, c.w);
       }
-      unsigned m = __ballot_sync(0xffffffffu, hit);
-      if (kMode == 1 && hit) list[pos + cnt + __popc(m & lanemask_lt())] = k;
+      unsigned m = T.ballot(hit);
+      if (kMode == 1 && hit) list[pos + cnt + __popc(m & T.lanes_below())] = k;
       cnt += __popc(m);
     }
     counts[side] = cnt;
   }
-  if (kMode == 0 && lane_id() == 0) {
+  if (kMode == 0 && T.lane == 0) {
     if (counts[0] == 0 || counts[1] == 0) { join_flag[w] = 0; bE[w] = 0; oE[w] = 0; }
     else { bE[w] = counts[0]; oE[w] = counts[1]; }
   }
@@ -281,17 +315,20 @@ __device__ __forceinline__ bool segment_hit(double bX1, double bY1, double bX2, 
   return true;
 }
 
+template <int W>
 __global__ void __launch_bounds__(kThreads)
 refine_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32_t* __restrict__ po,
               int64_t K, const int8_t* __restrict__ join_flag,
               const int32_t* __restrict__ bE, const int32_t* __restrict__ oE,
               const int64_t* __restrict__ bOff, const int64_t* __restrict__ oOff,
               const int32_t* __restrict__ bList, const int32_t* __restrict__ oList,
-              int8_t* __restrict__ seg_flag) {
-  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+              int8_t* __restrict__ seg_flag, int64_t lo, int64_t hi) {
+  const JTile<W> T;
+  const int64_t w = JTile<W>::unit();
   if (w >= K) return;
-  if (!join_flag[w]) { if (lane_id() == 0) seg_flag[w] = 0; return; }
+  if (!join_flag[w]) { if (W != 32 && T.lane == 0) seg_flag[w] = 0; return; }
   const int nb = bE[w], no = oE[w];
+  if ((int64_t)nb * no <= lo || (int64_t)nb * no > hi) return;   // the other pass takes this pair
   const int b = pb[w], o = po[w];
   const int bV = Lb.vnum[b], oV = Lo.vnum[o];
   const double2* bv = reinterpret_cast<const double2*>(Lb.xy) + (Lb.vps[b] - bV);
@@ -300,8 +337,8 @@ refine_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const in
   const int32_t* ol = oList + oOff[w];
   const int64_t total = (int64_t)nb * no;
   int found = 0;
-  for (int64_t t0 = 0; t0 < total && !found; t0 += 32) {
-    int64_t t = t0 + lane_id();
+  for (int64_t t0 = 0; t0 < total && !found; t0 += W) {
+    int64_t t = t0 + T.lane;
     bool hit = false;
     if (t < total) {
       int be, oe;
@@ -317,9 +354,9 @@ refine_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const in
       double2 o1 = __ldg(ov + oe), o2 = __ldg(ov + ((oe < oV - 1) ? oe + 1 : 0));
       hit = segment_hit(b1.x, b1.y, b2.x, b2.y, o1.x, o1.y, o2.x, o2.y);
     }
-    found = __any_sync(0xffffffffu, hit);
+    found = T.ballot(hit) != 0u;
   }
-  if (lane_id() == 0) seg_flag[w] = (int8_t)found;
+  if (T.lane == 0) seg_flag[w] = (int8_t)found;
 }
 
 // ---------------------------------------------------------------- clip set + stats
@@ -459,6 +496,10 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
 // Stages J3-J6 and the clip set over candidate pairs given as packed keys
 // (b << obits | o) sorted ascending; J.mbr_b/J.mbr_o hold the layers' MBRs.  d_total
 // (4 entries) and d_cnt (8 entries, zeroed) are device scratch counters.
+// lanes per pair of the narrow-tile passes, and the pair size up to which they are used
+constexpr int kJoinTile = 4;
+constexpr int64_t kJoinTileMax = 64;
+
 int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys, int64_t K, int obits,
                    Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,
                    int64_t* h_scratch, cudaStream_t s, Marks* mk) {
@@ -483,12 +524,20 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
   { cmbr_kernel<<<blocks_for(K), kThreads, 0, s>>>(pkeys, K, obits, J.mbr_b, J.mbr_o, J.b, J.o, J.cmbr,
                                                  J.pip_type); note_launch(); }
   // ---- J4 point in polygon
-  { pip_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.pip_type, K, J.pip_flag,
-                                                      J.join_flag); note_launch(); }
+  // narrow tiles for small pairs first (they also set the flags of pairs with nothing to
+  // test), then whole warps for the rest
+  { pip_kernel<kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
+        Lb, Lo, J.b, J.o, J.pip_type, K, J.pip_flag, J.join_flag, -1, kJoinTileMax); note_launch(); }
+  { pip_kernel<32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.pip_type, K, J.pip_flag,
+                                                          J.join_flag, kJoinTileMax, INT64_MAX); note_launch(); }
   mk->mark("join:cmbr+pip", s);
   // ---- J5 common-MBR edge filter: count, offsets, lists
-  { cmf_kernel<0><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
-                                                         J.oE, nullptr, nullptr, nullptr, nullptr); note_launch(); }
+  { cmf_kernel<0, kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
+        Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, nullptr, nullptr, nullptr, nullptr, -1,
+        kJoinTileMax); note_launch(); }
+  { cmf_kernel<0, 32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                             J.oE, nullptr, nullptr, nullptr, nullptr, kJoinTileMax,
+                                                             INT64_MAX); note_launch(); }
   exclusive_scan_i32(J.bE, bOff, K, d_total + 1, stmpK, d_err, s);
   exclusive_scan_i32(J.oE, oOff, K, d_total + 2, stmpK, d_err, s);
   cudaMemcpyAsync(h_scratch, d_total + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
@@ -497,12 +546,19 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
   int32_t* bList = A.take_n<int32_t>(nBl);
   int32_t* oList = A.take_n<int32_t>(nOl);
   if (!bList || !oList) return ST_OUT_OF_MEMORY;
-  { cmf_kernel<1><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
-                                                         J.oE, bOff, oOff, bList, oList); note_launch(); }
+  { cmf_kernel<1, kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
+        Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, bOff, oOff, bList, oList, -1, kJoinTileMax); note_launch(); }
+  { cmf_kernel<1, 32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                             J.oE, bOff, oOff, bList, oList, kJoinTileMax,
+                                                             INT64_MAX); note_launch(); }
   mk->mark("join:cmf", s);
   // ---- J6 refine
-  { refine_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, K, J.join_flag, J.bE, J.oE,
-                                                         bOff, oOff, bList, oList, J.seg_flag); note_launch(); }
+  { refine_kernel<kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
+        Lb, Lo, J.b, J.o, K, J.join_flag, J.bE, J.oE, bOff, oOff, bList, oList, J.seg_flag, -1,
+        kJoinTileMax * 4); note_launch(); }
+  { refine_kernel<32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, K, J.join_flag, J.bE, J.oE,
+                                                             bOff, oOff, bList, oList, J.seg_flag, kJoinTileMax * 4,
+                                                             INT64_MAX); note_launch(); }
   mk->mark("join:refine", s);
   // ---- clip set = containment pairs + pairs with intersecting edges
   { clip_flag_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.pip_type, J.pip_flag, J.join_flag, J.seg_flag, K,
