@@ -48,6 +48,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarpsPerBlock = kThreads / 32;
 constexpr int kChunk = 256;            // edge pairs per warp work unit (8 x 32 lanes)
+constexpr int kFilterTile = 4;         // lanes per small pair in the edge filter
+constexpr int64_t kFilterTileMax = 64; // ring size up to which the narrow tiles take a pair
 
 inline unsigned blocks_for_warps(int64_t warps) {
   return (unsigned)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
@@ -100,14 +102,26 @@ __global__ void setup_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict
 }
 
 // ---------------------------------------------------------------- G1 edge filter
-template <int kMode>
+// W lanes per pair (W = 32: a warp).  Two passes split the pairs by ring size: narrow
+// tiles for small pairs (they also zero the counts of pairs with nothing to test), whole
+// warps for the rest.
+template <int kMode, int W>
 __global__ void __launch_bounds__(kThreads)
 edge_filter_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, int32_t* __restrict__ cP,
                    int32_t* __restrict__ cQ, const int64_t* __restrict__ offP,
-                   const int64_t* __restrict__ offQ, int32_t* __restrict__ LP, int32_t* __restrict__ LQ) {
-  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+                   const int64_t* __restrict__ offQ, int32_t* __restrict__ LP, int32_t* __restrict__ LQ,
+                   int64_t lo, int64_t hi) {
+  constexpr unsigned kBits = (W == 32) ? 0xffffffffu : ((1u << (W & 31)) - 1u);
+  const int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) / W;
+  const int tl = (int)(threadIdx.x & (W - 1));
+  const int tbase = (int)(lane_id() & ~(unsigned)(W - 1));
+  const unsigned tmask = kBits << tbase;
   if (w >= K) return;
-  if (D.status[w] != 0) { if (kMode == 0 && lane_id() == 0) { cP[w] = 0; cQ[w] = 0; } return; }
+  if (D.status[w] != 0) { if (kMode == 0 && W != 32 && tl == 0) { cP[w] = 0; cQ[w] = 0; } return; }
+  {
+    const int64_t size = (int64_t)D.nP[w] + D.nQ[w];
+    if (size <= lo || size > hi) return;             // the other pass takes this pair
+  }
   double4 c = reinterpret_cast<const double4*>(D.cmbr)[w];
   const int pside = D.pSide[w];
   for (int side = 0; side < 2; ++side) {
@@ -117,18 +131,19 @@ edge_filter_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, int32_t* __re
     int64_t pos = 0;
     int32_t* list = nullptr;
     if (kMode == 1) { pos = side == 0 ? offP[w] : offQ[w]; list = side == 0 ? LP : LQ; }
-    for (int k0 = 0; k0 < n; k0 += 32) {
-      int k = k0 + lane_id();
+    for (int k0 = 0; k0 < n; k0 += W) {
+      int k = k0 + tl;
       bool hit = false;
       if (k < n) {
         double2 a = __ldg(v + k), b = __ldg(v + (k + 1 < n ? k + 1 : 0));
         hit = edge_touches_box(a.x, a.y, b.x, b.y, c.x, c.y, c.z, c.w);
       }
-      unsigned m = __ballot_sync(0xffffffffu, hit);
-      if (kMode == 1 && hit) list[pos + cnt + __popc(m & lanemask_lt())] = k;
+      unsigned m = __ballot_sync(tmask, hit);
+      if (W != 32) m = (m >> tbase) & kBits;
+      if (kMode == 1 && hit) list[pos + cnt + __popc(m & ((1u << tl) - 1u))] = k;
       cnt += __popc(m);
     }
-    if (kMode == 0 && lane_id() == 0) { if (side == 0) cP[w] = cnt; else cQ[w] = cnt; }
+    if (kMode == 0 && tl == 0) { if (side == 0) cP[w] = cnt; else cQ[w] = cnt; }
   }
 }
 
@@ -2981,8 +2996,11 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     return ST_OUT_OF_MEMORY;
   { setup_kernel<<<blocks_for(K), kThreads, 0, s>>>(Lb, Lo, d_pid, d_qid, K, mb, mo, D, C.swapped, prm.no_swap); note_launch(); }
   // ---- G1 edge filter
-  { edge_filter_kernel<0><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, nullptr, nullptr,
-                                                                 nullptr, nullptr); note_launch(); }
+  { edge_filter_kernel<0, kFilterTile><<<(unsigned)((K * kFilterTile + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+        Lb, Lo, D, K, cP, cQ, nullptr, nullptr, nullptr, nullptr, -1, kFilterTileMax); note_launch(); }
+  { edge_filter_kernel<0, 32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, nullptr, nullptr,
+                                                                      nullptr, nullptr, kFilterTileMax,
+                                                                      INT64_MAX); note_launch(); }
   exclusive_scan_i32(cP, offP, K, tot + 0, stK, d_err, s);
   exclusive_scan_i32(cQ, offQ, K, tot + 1, stK, d_err, s);
   exclusive_scan_i32(D.nP, eoffP, K, tot + 2, stK, d_err, s);
@@ -3014,7 +3032,10 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (nCh > 0) { chunk_pair_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(chunkOff, nchunk, K, chunkPair); note_launch(); }
   cudaMemsetAsync(binRec, 0, K * sizeof(int64_t), s);
   cudaMemsetAsync(binQ, 0, K * sizeof(int64_t), s);
-  { edge_filter_kernel<1><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ); note_launch(); }
+  { edge_filter_kernel<1, kFilterTile><<<(unsigned)((K * kFilterTile + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+        Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ, -1, kFilterTileMax); note_launch(); }
+  { edge_filter_kernel<1, 32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ,
+                                                                      kFilterTileMax, INT64_MAX); note_launch(); }
   // ---- G2 count: chunked pairs
   Records R{};
   if (nCh > 0) {

@@ -36,16 +36,17 @@ inline unsigned blocks_for_tiles(int64_t units, int w) {
 // pairs by size between a narrow-tile pass and a whole-warp pass.
 template <int W>
 struct JTile {
+  static constexpr unsigned kBits = (W == 32) ? 0xffffffffu : ((1u << (W & 31)) - 1u);
   int lane, base;
   unsigned mask;
   __device__ __forceinline__ JTile() {
     lane = (int)(threadIdx.x & (W - 1));
     base = (int)(lane_id() & ~(unsigned)(W - 1));
-    mask = (W == 32) ? 0xffffffffu : (((1u << W) - 1u) << base);
+    mask = kBits << base;
   }
   __device__ __forceinline__ unsigned ballot(bool v) const {
     const unsigned b = __ballot_sync(mask, v);
-    return (W == 32) ? b : ((b >> base) & ((1u << W) - 1u));
+    return (W == 32) ? b : ((b >> base) & kBits);
   }
   __device__ __forceinline__ unsigned lanes_below() const { return (1u << lane) - 1u; }
   static __device__ __forceinline__ int64_t unit() {
