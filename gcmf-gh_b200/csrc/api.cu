@@ -495,6 +495,92 @@ gcmfgh_status gh_clip_pair(gcmfgh_ctx* c, const double* P, int32_t nP, const dou
   return r;
 }
 
+gcmfgh_status gh_calculate_intersections(gcmfgh_ctx* c, const gcmfgh_layer* pl, int32_t p_id,
+                                         const gcmfgh_layer* ql, int32_t q_id, gcmfgh_intersections* out) {
+  if (!out) return GCMFGH_INVALID_ARGUMENT;
+  std::memset(out, 0, sizeof(*out));
+  if (!c || !layer_ok(pl) || !layer_ok(ql) || p_id < 0 || q_id < 0 || p_id >= pl->n_polys || q_id >= ql->n_polys)
+    return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->pair_arena.reset();
+  int32_t* ids = c->pair_arena.take_n<int32_t>(2);
+  if (!ids) return GCMFGH_OUT_OF_MEMORY;
+  const int32_t hid[2] = {p_id, q_id};
+  if (cudaMemcpy(ids, hid, sizeof(hid), cudaMemcpyHostToDevice) != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  c->clip_arena.reset();
+  c->have_clip = false;
+  c->marks[1].n = 0;
+  cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  ClipParams prm = c->prm;
+  prm.no_swap = 1;
+  RingExport ex;
+  int st = run_clip(to_dev(pl), to_dev(ql), ids, ids + 1, 1, prm, c->clip_arena, c->clip, c->d_err, c->h_scratch,
+                    c->stream, nullptr, nullptr, &ex);
+  gcmfgh_status r = finish(c, st);
+  if (r != GCMFGH_OK) return r;
+  out->n_p = ex.n_p;
+  out->n_q = ex.n_q;
+  out->invalid = ex.status == 1 ? 1 : 0;
+  if (ex.status == 1) return GCMFGH_OK;
+  if (ex.status == 2) {
+    // disjoint MBRs: no edge meets the (empty) common MBR, so the rings come back as they
+    // are, every vertex plain
+    const gcmfgh_layer* L[2] = {pl, ql};
+    const int32_t id[2] = {p_id, q_id};
+    std::vector<double>* dst[2] = {&ex.xy_p, &ex.xy_q};
+    int64_t n[2];
+    for (int side = 0; side < 2; ++side) {
+      int32_t vn = 0;
+      int64_t vp = 0;
+      if (cudaMemcpy(&vn, L[side]->vnum + id[side], sizeof(vn), cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(&vp, L[side]->vps + id[side], sizeof(vp), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return GCMFGH_CUDA_ERROR;
+      n[side] = std::max<int64_t>(vn - 1, 0);
+      dst[side]->resize(2 * n[side]);
+      if (n[side] > 0 && cudaMemcpy(dst[side]->data(), L[side]->coords + 2 * (vp - vn),
+                                    2 * n[side] * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return GCMFGH_CUDA_ERROR;
+    }
+    out->n_p = n[0];
+    out->n_q = n[1];
+    ex.alpha_p.assign(n[0], -100); ex.label_p.assign(n[0], -100); ex.nb_p.assign(n[0], 0);
+    ex.alpha_q.assign(n[1], -100); ex.label_q.assign(n[1], -100); ex.nb_q.assign(n[1], 0);
+  } else if (ex.status != 0) {
+    return GCMFGH_DEVICE_ERROR;
+  }
+  const int64_t np = out->n_p, nq = out->n_q;
+  out->xy_p = static_cast<double*>(malloc(sizeof(double) * 2 * std::max<int64_t>(np, 1)));
+  out->xy_q = static_cast<double*>(malloc(sizeof(double) * 2 * std::max<int64_t>(nq, 1)));
+  int32_t** arr[6] = {&out->alpha_p, &out->label_p, &out->neighbor_p, &out->alpha_q, &out->label_q, &out->neighbor_q};
+  const std::vector<int32_t>* src[6] = {&ex.alpha_p, &ex.label_p, &ex.nb_p, &ex.alpha_q, &ex.label_q, &ex.nb_q};
+  bool ok = out->xy_p && out->xy_q;
+  for (int i = 0; i < 6; ++i) {
+    const int64_t n = i < 3 ? np : nq;
+    *arr[i] = static_cast<int32_t*>(malloc(sizeof(int32_t) * std::max<int64_t>(n, 1)));
+    ok = ok && *arr[i];
+    if (*arr[i] && n > 0) memcpy(*arr[i], src[i]->data(), sizeof(int32_t) * n);
+  }
+  if (!ok) {
+    gh_free_intersections(out);
+    return GCMFGH_OUT_OF_MEMORY;
+  }
+  if (np > 0) memcpy(out->xy_p, ex.xy_p.data(), sizeof(double) * 2 * np);
+  if (nq > 0) memcpy(out->xy_q, ex.xy_q.data(), sizeof(double) * 2 * nq);
+  return GCMFGH_OK;
+}
+
+void gh_free_intersections(gcmfgh_intersections* x) {
+  if (!x) return;
+  free(x->xy_p); free(x->xy_q);
+  free(x->alpha_p); free(x->alpha_q);
+  free(x->label_p); free(x->label_q);
+  free(x->neighbor_p); free(x->neighbor_q);
+  const int64_t np = x->n_p, nq = x->n_q;
+  const int32_t inv = x->invalid;
+  std::memset(x, 0, sizeof(*x));
+  x->n_p = np; x->n_q = nq; x->invalid = inv;
+}
+
 gcmfgh_status gcmfgh_exclusive_scan_i32(gcmfgh_ctx* c, const int32_t* d_in, int64_t* d_out, int64_t n,
                                         int64_t* total) {
   if (!c || n < 0 || (n > 0 && (!d_in || !d_out))) return GCMFGH_INVALID_ARGUMENT;

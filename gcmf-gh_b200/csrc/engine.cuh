@@ -120,12 +120,27 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
                    Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,
                    int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);
 
+// Merged rings of pair 0 after the neighbour links, as the reference's
+// calculateIntersections hands them back (gppolyclip_mDIV512.cu:1298-1640): vertices in
+// ring order, the integer parameter key (int)(1e7 * alpha) of every vertex that carries an
+// intersection (-100 at plain vertices), the initial label (-100 where no key), and the
+// 1-based slot of the neighbour in the other ring (0 = none).
+struct RingExport {
+  int status = 0;                    // pair status: 0 ok, 1 invalid, 2 disjoint MBRs
+  int64_t n_p = 0, n_q = 0;          // merged ring sizes
+  int64_t edges_p = 0, edges_q = 0;  // ring edges (vertices without the closing one)
+  std::vector<double> xy_p, xy_q;
+  std::vector<int32_t> alpha_p, alpha_q, label_p, label_q, nb_p, nb_q;
+};
+
 // aux: optional second stream (ideally of higher priority); long pairs are labelled on it
 // while the warp-per-pair kernel runs on s.  Without it everything runs on s.
+// ex: when given, the clip stops after the neighbour links and pair 0's merged rings are
+// exported into it instead of being labelled and traced.
 int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, const int32_t* d_qid,
              int64_t n_pairs, const ClipParams& prm, Arena& arena, ClipDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
-             cudaStream_t aux = nullptr);
+             cudaStream_t aux = nullptr, RingExport* ex = nullptr);
 
 // a non-blocking stream at the device's highest priority (nullptr on failure)
 cudaStream_t create_priority_stream();

@@ -735,6 +735,133 @@ __global__ void link_kernel(Records R, int64_t nR, const int32_t* __restrict__ s
   }
 }
 
+// ---------------------------------------------------------------- ring export
+// The reference's calculateIntersections (gppolyclip_mDIV512.cu:1298-1640) returns the
+// merged rings with an integer parameter key per vertex: (int)(1e7 * alpha) where the
+// vertex carries an intersection, -100 at plain vertices (:926).  Inserted vertices get
+// the key of their one record (:997-1053).  The source vertex of an edge gets the key of
+// its degenerate records (P: types 2/4/6/8, Q: types 3/4/7/8).  The P side is written by
+// the P edge's loop over ascending Q edges, so the largest Q edge wins.  The Q side is
+// written by concurrent P-edge threads (a race in the reference); here the largest P edge
+// wins.  Keys are packed as (other edge + 1) << 32 | key and combined with atomicMax.
+// Per pair it also counts the records that insert a vertex on each ring.
+__device__ __forceinline__ uint32_t alpha_key(double a) {
+  return (uint32_t)(int32_t)(10000000.0 * a);      // (int)pow(10, EPSILON_POSITIONS)*alpha
+}
+
+__global__ void export_key_kernel(Records R, int64_t nR, const int32_t* __restrict__ status,
+                                  const int64_t* __restrict__ eoffP, const int64_t* __restrict__ eoffQ,
+                                  const int64_t* __restrict__ vposP, const int64_t* __restrict__ vposQ,
+                                  const int64_t* __restrict__ regP, const int64_t* __restrict__ regQ,
+                                  const int64_t* __restrict__ slotP, const int64_t* __restrict__ slotQ,
+                                  unsigned long long* __restrict__ keyP, unsigned long long* __restrict__ keyQ,
+                                  int32_t* __restrict__ cntP, int32_t* __restrict__ cntQ) {
+  int64_t r = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  if (r >= nR) return;
+  const int k = R.k[r];
+  const int t = R.t[r];
+  const bool insOnP = t == 1 || t == 3 || t == 5 || t == 7;
+  const bool insOnQ = t == 1 || t == 2 || t == 5 || t == 6;
+  if (insOnP) atomicAdd(&cntP[k], 1);
+  if (insOnQ) atomicAdd(&cntQ[k], 1);
+  if (status[k] != 0) return;
+  const int64_t eP = eoffP[k] + R.p[r], eQ = eoffQ[k] + R.q[r];
+  const uint32_t kp = alpha_key(R.a[r]), kq = alpha_key(R.b[r]);
+  if (insOnP) {
+    keyP[regP[k] + slotP[r]] = (1ull << 32) | kp;
+  } else {
+    const int64_t src = vposP[eP] - vposP[eoffP[k]];
+    atomicMax(&keyP[regP[k] + src], ((unsigned long long)(R.q[r] + 1) << 32) | kp);
+  }
+  if (insOnQ) {
+    keyQ[regQ[k] + slotQ[r]] = (1ull << 32) | kq;
+  } else {
+    const int64_t src = vposQ[eQ] - vposQ[eoffQ[k]];
+    atomicMax(&keyQ[regQ[k] + src], ((unsigned long long)(R.p[r] + 1) << 32) | kq);
+  }
+}
+
+__device__ __forceinline__ int32_t unpack_key(unsigned long long v) {
+  return v == 0 ? -100 : (int32_t)(uint32_t)v;
+}
+
+// oracle() of gppolyclip_mDIV512.cu:195-215: Q's position relative to the chain
+// (P1, P2, P3), or which of P1 / P3 it is linked to
+__device__ int export_rel(int exact, int pMN, int pPN, int qId, const RingSet& SQ, int64_t bQ,
+                          const RingSet& SP, int64_t bP, int p1, int p2, int p3) {
+  if (pMN != -100 && pMN == qId) return R_IS_P_M;
+  if (pPN != -100 && pPN == qId) return R_IS_P_P;
+  const double qx = SQ.x[bQ + qId], qy = SQ.y[bQ + qId];
+  const double x1 = SP.x[bP + p1], y1 = SP.y[bP + p1], x2 = SP.x[bP + p2], y2 = SP.y[bP + p2];
+  const double x3 = SP.x[bP + p3], y3 = SP.y[bP + p3];
+  const int s1 = orient_sign(exact, qx, qy, x1, y1, x2, y2);
+  const int s2 = orient_sign(exact, qx, qy, x2, y2, x3, y3);
+  const int s3 = orient_sign(exact, x1, y1, x2, y2, x3, y3);
+  if (s3 > 0) return (s1 > 0 && s2 > 0) ? R_LEFT : R_RIGHT;
+  return (s1 < 0 && s2 < 0) ? R_RIGHT : R_LEFT;
+}
+
+// getInitialLabel of gppolyclip_mDIV512.cu:237-252, including its -102 for combinations
+// that name no label
+__device__ int32_t export_label(int m, int p) {
+  auto is = [&](int a, int b) { return (m == a && p == b) || (m == b && p == a); };
+  if (is(R_LEFT, R_RIGHT)) return L_CROSSING;
+  if ((m == R_LEFT && p == R_LEFT) || (m == R_RIGHT && p == R_RIGHT)) return L_BOUNCING;
+  if (is(R_IS_P_P, R_RIGHT)) return L_LEFT_ON;
+  if (is(R_IS_P_P, R_LEFT)) return L_RIGHT_ON;
+  if (is(R_IS_P_P, R_IS_P_M)) return L_ON_ON;
+  if (is(R_IS_P_M, R_RIGHT)) return L_ON_LEFT;
+  if (is(R_IS_P_M, R_LEFT)) return L_ON_RIGHT;
+  return -102;
+}
+
+// Block per pair: the merged rings in ring order (slot order before any labelling), their
+// keys and 1-based neighbours; then the initial labels of gpuCalculateInitLabel
+// (gppolyclip_mDIV512.cu:1171-1223), computed at the P vertices that carry a key and
+// copied to their Q neighbours.  Output arrays are indexed like the ring regions.
+__global__ void export_ring_kernel(int64_t K, const int32_t* __restrict__ status, const int32_t* __restrict__ mP,
+                                   const int32_t* __restrict__ mQ, const int64_t* __restrict__ regP,
+                                   const int64_t* __restrict__ regQ, RingSet SP, RingSet SQ,
+                                   const unsigned long long* __restrict__ keyP,
+                                   const unsigned long long* __restrict__ keyQ, double* __restrict__ xyP,
+                                   double* __restrict__ xyQ, int32_t* __restrict__ alP, int32_t* __restrict__ alQ,
+                                   int32_t* __restrict__ lbP, int32_t* __restrict__ lbQ, int32_t* __restrict__ nbP,
+                                   int32_t* __restrict__ nbQ) {
+  const int64_t k = blockIdx.x;
+  if (k >= K || status[k] != 0) return;
+  const int np = mP[k], nq = mQ[k];
+  const int64_t bP = regP[k], bQ = regQ[k];
+  for (int s = threadIdx.x; s < np; s += blockDim.x) {
+    const int64_t g = bP + s;
+    xyP[2 * g] = SP.x[g]; xyP[2 * g + 1] = SP.y[g];
+    alP[g] = unpack_key(keyP[g]);
+    lbP[g] = -100;
+    nbP[g] = SP.nb[g] + 1;
+  }
+  for (int s = threadIdx.x; s < nq; s += blockDim.x) {
+    const int64_t g = bQ + s;
+    xyQ[2 * g] = SQ.x[g]; xyQ[2 * g + 1] = SQ.y[g];
+    alQ[g] = unpack_key(keyQ[g]);
+    lbQ[g] = -100;
+    nbQ[g] = SQ.nb[g] + 1;
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < np; s += blockDim.x) {
+    if (keyP[bP + s] == 0) continue;
+    const int nId = SP.nb[bP + s];
+    if (nId < 0 || nId >= nq) continue;
+    const int pm = s > 0 ? s - 1 : np - 1, pp = s + 1 < np ? s + 1 : 0;
+    const int pMN = keyP[bP + pm] != 0 ? SP.nb[bP + pm] : -100;
+    const int pPN = keyP[bP + pp] != 0 ? SP.nb[bP + pp] : -100;
+    const int qm = nId > 0 ? nId - 1 : nq - 1, qp = nId + 1 < nq ? nId + 1 : 0;
+    const int a = export_rel(SP.exact, pMN, pPN, qm, SQ, bQ, SP, bP, pm, s, pp);
+    const int b = export_rel(SP.exact, pMN, pPN, qp, SQ, bQ, SP, bP, pm, s, pp);
+    const int32_t L = export_label(a, b);
+    lbP[bP + s] = L;
+    lbQ[bQ + nId] = L;
+  }
+}
+
 // ---------------------------------------------------------------- G7 label + trace
 struct Ring {
   double* x; double* y; int32_t* nx; int32_t* pv; int32_t* nb;
@@ -2959,7 +3086,7 @@ out_compact_kernel(int64_t K, const double* __restrict__ xy, const int64_t* __re
 
 int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const int32_t* d_qid,
              int64_t K, const ClipParams& prm, Arena& A, ClipDev& C, int* d_err, int64_t* hs,
-             cudaStream_t s, Marks* mk, cudaStream_t aux) {
+             cudaStream_t s, Marks* mk, cudaStream_t aux, RingExport* ex) {
   Marks dummy;
   if (!mk) mk = &dummy;
   C = ClipDev();
@@ -3267,6 +3394,61 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (nR > 0)
     { link_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, D.status, eoffP, eoffQ, vposP, vposQ, regP, regQ,
                                                     slotP, slotQ, srcLinkP, srcLinkQ, SP, SQ); note_launch(); }
+  // ---- export of the merged rings instead of labelling (calculateIntersections)
+  if (ex) {
+    unsigned long long* keyP = A.take_n<unsigned long long>(std::max<int64_t>(regTotP, 1));
+    unsigned long long* keyQ = A.take_n<unsigned long long>(std::max<int64_t>(regTotQ, 1));
+    int32_t* cnt = A.take_n<int32_t>(2 * K);
+    double* xyP = A.take_n<double>(2 * std::max<int64_t>(regTotP, 1));
+    double* xyQ = A.take_n<double>(2 * std::max<int64_t>(regTotQ, 1));
+    int32_t* iP = A.take_n<int32_t>(3 * std::max<int64_t>(regTotP, 1));
+    int32_t* iQ = A.take_n<int32_t>(3 * std::max<int64_t>(regTotQ, 1));
+    if (!keyP || !keyQ || !cnt || !xyP || !xyQ || !iP || !iQ) return ST_OUT_OF_MEMORY;
+    cudaMemsetAsync(keyP, 0, std::max<int64_t>(regTotP, 1) * sizeof(unsigned long long), s);
+    cudaMemsetAsync(keyQ, 0, std::max<int64_t>(regTotQ, 1) * sizeof(unsigned long long), s);
+    cudaMemsetAsync(cnt, 0, 2 * K * sizeof(int32_t), s);
+    if (nR > 0)
+      { export_key_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, D.status, eoffP, eoffQ, vposP, vposQ, regP,
+                                                              regQ, slotP, slotQ, keyP, keyQ, cnt, cnt + K); note_launch(); }
+    const int64_t rP = std::max<int64_t>(regTotP, 1), rQ = std::max<int64_t>(regTotQ, 1);
+    { export_ring_kernel<<<(unsigned)K, kThreads, 0, s>>>(K, D.status, mP, mQ, regP, regQ, SP, SQ, keyP, keyQ, xyP,
+                                                         xyQ, iP, iQ, iP + rP, iQ + rQ, iP + 2 * rP,
+                                                         iQ + 2 * rQ); note_launch(); }
+    // pair 0: status, record counts per ring, edges, merged sizes, region offsets
+    int32_t h32[6];
+    int64_t h64[2];
+    cudaMemcpyAsync(h32 + 0, D.status, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h32 + 1, cnt, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h32 + 2, cnt + K, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h32 + 3, D.nP, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h32 + 4, D.nQ, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h32 + 5, mP, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h64 + 0, regP, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h64 + 1, regQ, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return ST_CUDA_ERROR;
+    ex->status = h32[0];
+    ex->edges_p = h32[3];
+    ex->edges_q = h32[4];
+    ex->n_p = (int64_t)h32[3] + h32[1];
+    ex->n_q = (int64_t)h32[4] + h32[2];
+    if (ex->status == 0) {
+      if (h32[5] != ex->n_p) return ST_DEVICE_ERROR;   // the ring layout disagrees with the records
+      const int64_t np = ex->n_p, nq = ex->n_q, oP = h64[0], oQ = h64[1];
+      ex->xy_p.resize(2 * np); ex->xy_q.resize(2 * nq);
+      ex->alpha_p.resize(np); ex->label_p.resize(np); ex->nb_p.resize(np);
+      ex->alpha_q.resize(nq); ex->label_q.resize(nq); ex->nb_q.resize(nq);
+      cudaMemcpyAsync(ex->xy_p.data(), xyP + 2 * oP, 2 * np * sizeof(double), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(ex->xy_q.data(), xyQ + 2 * oQ, 2 * nq * sizeof(double), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(ex->alpha_p.data(), iP + oP, np * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(ex->label_p.data(), iP + rP + oP, np * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(ex->nb_p.data(), iP + 2 * rP + oP, np * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(ex->alpha_q.data(), iQ + oQ, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(ex->label_q.data(), iQ + rQ + oQ, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(ex->nb_q.data(), iQ + 2 * rQ + oQ, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      if (!sync()) return ST_CUDA_ERROR;
+    }
+    return ST_OK;
+  }
   // ---- G7 label + trace into per-pair output regions
   int64_t* vcap = A.take_n<int64_t>(K);
   int32_t* ccap = A.take_n<int32_t>(K);

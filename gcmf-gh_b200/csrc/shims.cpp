@@ -121,3 +121,44 @@ int ghcuda(int pIDList[], int qIDList[], int totalNumPairs, coord_t* bCoords, co
   }
   return 0;
 }
+
+void calculateIntersections(coord_t* baseCoord, coord_t* overlayCoords, int sizeP, int sizeQ, coord_t* cmbr,
+                            int* dbVNum, long* dbVPSNum, int* doVNum, long* doVPSNum, int bPID, int oPID,
+                            int* countNonDegenIntP, int* countNonDegenIntQ,
+                            coord_t** intersectionsP, coord_t** intersectionsQ, int** alphaValuesP,
+                            int** alphaValuesQ, int** initLabelsP, int** initLabelsQ,
+                            int** neighborP, int** neighborQ, int* invalid) {
+  (void)sizeP;
+  (void)sizeQ;
+  (void)cmbr;
+  int** outs[6] = {alphaValuesP, alphaValuesQ, initLabelsP, initLabelsQ, neighborP, neighborQ};
+  for (int** o : outs)
+    if (o) *o = nullptr;
+  if (intersectionsP) *intersectionsP = nullptr;
+  if (intersectionsQ) *intersectionsQ = nullptr;
+  if (countNonDegenIntP) *countNonDegenIntP = 0;
+  if (countNonDegenIntQ) *countNonDegenIntQ = 0;
+  if (!invalid) return;
+  *invalid = -1;
+  if (!countNonDegenIntP || !countNonDegenIntQ || !intersectionsP || !intersectionsQ || !alphaValuesP ||
+      !alphaValuesQ || !initLabelsP || !initLabelsQ || !neighborP || !neighborQ || bPID < 0 || oPID < 0 ||
+      !ensure_ctx())
+    return;
+  ShimState& S = state();
+  gcmfgh_layer b{baseCoord, dbVNum, reinterpret_cast<const int64_t*>(dbVPSNum), (int64_t)bPID + 1, 0};
+  gcmfgh_layer o{overlayCoords, doVNum, reinterpret_cast<const int64_t*>(doVPSNum), (int64_t)oPID + 1, 0};
+  gcmfgh_intersections x;
+  if (gh_calculate_intersections(S.ctx, &b, bPID, &o, oPID, &x) != GCMFGH_OK) return;
+  *countNonDegenIntP = (int)x.n_p;
+  *countNonDegenIntQ = (int)x.n_q;
+  *invalid = x.invalid;
+  // ownership of the malloc'ed arrays passes to the caller, as in the reference
+  *intersectionsP = x.xy_p;
+  *intersectionsQ = x.xy_q;
+  *alphaValuesP = x.alpha_p;
+  *alphaValuesQ = x.alpha_q;
+  *initLabelsP = x.label_p;
+  *initLabelsQ = x.label_q;
+  *neighborP = x.neighbor_p;
+  *neighborQ = x.neighbor_q;
+}

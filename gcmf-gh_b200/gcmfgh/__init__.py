@@ -63,6 +63,14 @@ class ClipInfo(ctypes.Structure):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
+class Intersections(ctypes.Structure):
+    _fields_ = [("n_p", ctypes.c_int64), ("n_q", ctypes.c_int64), ("invalid", ctypes.c_int32),
+                ("xy_p", ctypes.c_void_p), ("xy_q", ctypes.c_void_p),
+                ("alpha_p", ctypes.c_void_p), ("alpha_q", ctypes.c_void_p),
+                ("label_p", ctypes.c_void_p), ("label_q", ctypes.c_void_p),
+                ("neighbor_p", ctypes.c_void_p), ("neighbor_q", ctypes.c_void_p)]
+
+
 class ServeOptions(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_int),
                 ("max_batch_queries", ctypes.c_int64), ("max_batch_vertices", ctypes.c_int64),
@@ -108,6 +116,9 @@ def lib():
         L.gh_clip_get.argtypes = [vp, ctypes.c_int, vp, i64, ctypes.c_int, P(i64)]
         L.gh_clip_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
         L.gh_clip_pair.argtypes = [vp, vp, i32, vp, i32, P(ClipInfo)]
+        L.gh_calculate_intersections.argtypes = [vp, P(Layer), i32, P(Layer), i32, P(Intersections)]
+        L.gh_free_intersections.argtypes = [P(Intersections)]
+        L.gh_free_intersections.restype = None
         L.gcmfgh_join_clip_host.argtypes = [vp, P(Layer), P(Layer), P(JoinInfo), P(ClipInfo)]
         L.gcmfgh_exclusive_scan_i32.argtypes = [vp, vp, vp, i64, P(i64)]
         L.gcmfgh_radix_sort_u64.argtypes = [vp, vp, vp, i64, ctypes.c_int]
@@ -285,6 +296,32 @@ class Engine:
         _check(lib().gh_clip_pair(self.h, _np_ptr(P), len(P) // 2, _np_ptr(Q), len(Q) // 2,
                                   ctypes.byref(info)))
         return info.as_dict()
+
+    def calculate_intersections(self, p_layer: DeviceLayer, p_id, q_layer: DeviceLayer, q_id):
+        """The reference's calculateIntersections for polygon p_id of p_layer (P, not swapped)
+        against polygon q_id of q_layer: dict with n_p, n_q, invalid and, unless invalid,
+        numpy copies of the merged rings (xy_*), keys (alpha_*), initial labels (label_*)
+        and 1-based neighbours (neighbor_*)."""
+        x = Intersections()
+        _check(lib().gh_calculate_intersections(self.h, ctypes.byref(p_layer.c), int(p_id), ctypes.byref(q_layer.c),
+                                                int(q_id), ctypes.byref(x)))
+        try:
+            r = {"n_p": int(x.n_p), "n_q": int(x.n_q), "invalid": int(x.invalid)}
+            if not x.invalid:
+                for name, n, ct, dt in (("xy_p", 2 * x.n_p, ctypes.c_double, np.float64),
+                                        ("xy_q", 2 * x.n_q, ctypes.c_double, np.float64),
+                                        ("alpha_p", x.n_p, ctypes.c_int32, np.int32),
+                                        ("alpha_q", x.n_q, ctypes.c_int32, np.int32),
+                                        ("label_p", x.n_p, ctypes.c_int32, np.int32),
+                                        ("label_q", x.n_q, ctypes.c_int32, np.int32),
+                                        ("neighbor_p", x.n_p, ctypes.c_int32, np.int32),
+                                        ("neighbor_q", x.n_q, ctypes.c_int32, np.int32)):
+                    ptr = getattr(x, name)
+                    r[name] = (np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ct)), shape=(n,)).astype(dt)
+                               if n > 0 else np.zeros(0, dt))
+            return r
+        finally:
+            lib().gh_free_intersections(ctypes.byref(x))
 
     def clip_result(self):
         return ClipResult(self.clip_field("status"), self.clip_field("ncomp"), self.clip_field("count1"),

@@ -181,6 +181,38 @@ gcmfgh_status gh_clip_ptr(gcmfgh_ctx* ctx, int field, const void** dev_ptr, int6
 gcmfgh_status gh_clip_pair(gcmfgh_ctx* ctx, const double* P, int32_t nP, const double* Q, int32_t nQ,
                            gcmfgh_clip_info* info);
 
+/* ---- the intersection phase of one pair: replaces calculateIntersections
+ * (ghcuda.h:6-14, gppolyclip_mDIV512.cu:1298-1640), which hands the merged rings to the
+ * host list builder (ghcuda.cpp:239-322).  Arrays are host malloc'ed, freed by
+ * gh_free_intersections; they are NULL when the pair is invalid. */
+typedef struct {
+  int64_t n_p, n_q;        /* countNonDegenIntP / Q: ring vertices plus inserted vertices */
+  int32_t invalid;         /* 1 when the P-side and Q-side intersection counts differ (:1460-1476) */
+  double* xy_p;            /* merged rings in ring order, interleaved x,y (intersectionsP / Q) */
+  double* xy_q;
+  int32_t* alpha_p;        /* (int)(1e7 * alpha) where the vertex carries an intersection, -100
+                              at plain vertices (alphaValuesP / Q) */
+  int32_t* alpha_q;
+  int32_t* label_p;        /* initial label (IntersectionLabel, polygon.h:21-32) at P vertices
+                              with a key and at their Q neighbours, -100 elsewhere, -102 where
+                              the two positions name no label (initLabelsP / Q) */
+  int32_t* label_q;
+  int32_t* neighbor_p;     /* 1-based index of the linked vertex in the other ring, 0 = none */
+  int32_t* neighbor_q;
+} gcmfgh_intersections;
+
+/* P = polygon p_id of p_layer, Q = polygon q_id of q_layer (device layers in the reference
+ * layout, as spatialJoin hands them out); P is not swapped with Q.  The common MBR is the
+ * intersection of the two polygons' MBRs, as the caller computes it (ghcuda.cpp:94-125).
+ * Differences from the reference: the per-edge vertex order is by exact FP64 parameter (the
+ * reference sorts the integer keys), ties on the Q side's source-vertex keys go to the
+ * largest P edge (a race in the reference), neighbour entries of plain vertices are 0 (left
+ * uninitialised there), and for an invalid pair n_q counts the Q vertices inserted by the
+ * P-side records (the reference counts its Q-side pass). */
+gcmfgh_status gh_calculate_intersections(gcmfgh_ctx* ctx, const gcmfgh_layer* p_layer, int32_t p_id,
+                                         const gcmfgh_layer* q_layer, int32_t q_id, gcmfgh_intersections* out);
+void gh_free_intersections(gcmfgh_intersections* x);
+
 /* ---- the device primitives the path is built on.  Replace PrefixSum (GPU_Utility.h:128,
  * a multi-pass inclusive scan, GPU_PrefixSum.h:355) and RadixSort (GPU_Utility.h:242, a
  * 16-digit decimal LSD sort, GPU_RadixSort.h:27-148).  d_* are device pointers.

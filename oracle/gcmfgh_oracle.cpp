@@ -260,6 +260,14 @@ struct Clipper {
   bool exact = false;                          // exact-predicate mode
   Ring R[2];                                   // R[0] = P, R[1] = Q
   std::vector<std::vector<Pt>> out;            // result components
+  // When set, run() stops after the neighbour links and fills this with what the
+  // reference's calculateIntersections returns (gppolyclip_mDIV512.cu:1298-1640).
+  struct Export {
+    int64_t np = 0, nq = 0;
+    std::vector<double> xyP, xyQ;
+    std::vector<int32_t> alP, alQ, lbP, lbQ, nbP, nbQ;
+  };
+  Export* ex = nullptr;
   long long count1P = 0, count1Q = 0, typeCount[9] = {0};
   int status = 0;                              // 0 ok, 1 invalid, 2 disjoint MBRs
 
@@ -378,6 +386,80 @@ struct Clipper {
     return pts;
   }
 
+  // ---- calculateIntersections outputs
+  void exportPlain(const double* P, int nP, const double* Q, int nQ) {
+    ex->np = nP; ex->nq = nQ;
+    ex->xyP.assign(P, P + 2 * nP); ex->xyQ.assign(Q, Q + 2 * nQ);
+    ex->alP.assign(nP, -100); ex->lbP.assign(nP, -100); ex->nbP.assign(nP, 0);
+    ex->alQ.assign(nQ, -100); ex->lbQ.assign(nQ, -100); ex->nbQ.assign(nQ, 0);
+  }
+  static int32_t alphaKey(double a) { return (int32_t)(10000000.0 * a); }   // (int)pow(10,7)*alpha
+  // oracle(), gppolyclip_mDIV512.cu:195-215, with linked-ness read from the keys
+  int relKeyed(int pMN, int pPN, int qId, int p1, int p2, int p3) const {
+    const Ring& P = R[0];
+    const Ring& Q = R[1];
+    if (pMN != -100 && pMN == qId) return IS_P_m;
+    if (pPN != -100 && pPN == qId) return IS_P_p;
+    int s1 = orientSign(exact, Q.x[qId], Q.y[qId], P.x[p1], P.y[p1], P.x[p2], P.y[p2]);
+    int s2 = orientSign(exact, Q.x[qId], Q.y[qId], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+    int s3 = orientSign(exact, P.x[p1], P.y[p1], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+    if (s3 > 0) return (s1 > 0 && s2 > 0) ? LEFT : RIGHT;
+    return (s1 < 0 && s2 < 0) ? RIGHT : LEFT;
+  }
+  // getInitialLabel, gppolyclip_mDIV512.cu:237-252
+  static int32_t labelKeyed(int m, int p) {
+    auto has = [&](int a, int b) { return (m == a && p == b) || (m == b && p == a); };
+    if (has(LEFT, RIGHT)) return CROSSING;
+    if ((m == LEFT && p == LEFT) || (m == RIGHT && p == RIGHT)) return BOUNCING;
+    if (has(IS_P_p, RIGHT)) return LEFT_ON;
+    if (has(IS_P_p, LEFT)) return RIGHT_ON;
+    if (has(IS_P_p, IS_P_m)) return ON_ON;
+    if (has(IS_P_m, RIGHT)) return ON_LEFT;
+    if (has(IS_P_m, LEFT)) return ON_RIGHT;
+    return -102;
+  }
+  // Rings in slot order (= ring order before labelling).  Keys follow the reference's
+  // writes (gppolyclip_mDIV512.cu:926-1053): an inserted vertex gets its record's key; a
+  // source vertex gets the key of its last degenerate record in (P edge, Q edge) order --
+  // P: types 2/4/6/8, Q: types 3/4/7/8; type 5 keys only its inserted vertices.  Labels
+  // as gpuCalculateInitLabel (:1171-1223), in slot order.
+  void exportRings(const std::vector<Rec>& recs, const std::vector<int>& srcP, const std::vector<int>& srcQ,
+                   const std::vector<int>& insP, const std::vector<int>& insQ) {
+    const Ring& RP = R[0];
+    const Ring& RQ = R[1];
+    const int np = (int)RP.x.size(), nq = (int)RQ.x.size();
+    ex->np = np; ex->nq = nq;
+    ex->xyP.resize(2 * np); ex->xyQ.resize(2 * nq);
+    for (int v = 0; v < np; ++v) { ex->xyP[2 * v] = RP.x[v]; ex->xyP[2 * v + 1] = RP.y[v]; }
+    for (int v = 0; v < nq; ++v) { ex->xyQ[2 * v] = RQ.x[v]; ex->xyQ[2 * v + 1] = RQ.y[v]; }
+    ex->alP.assign(np, -100); ex->alQ.assign(nq, -100);
+    for (size_t r = 0; r < recs.size(); ++r) {
+      const Rec& rc = recs[r];
+      const int t = rc.type;
+      if (t == 1 || t == 3 || t == 5 || t == 7) ex->alP[insP[r]] = alphaKey(rc.a);
+      else ex->alP[srcP[rc.p]] = alphaKey(rc.a);
+      if (t == 1 || t == 2 || t == 5 || t == 6) ex->alQ[insQ[r]] = alphaKey(rc.b);
+      else ex->alQ[srcQ[rc.q]] = alphaKey(rc.b);
+    }
+    ex->nbP.resize(np); ex->nbQ.resize(nq);
+    for (int v = 0; v < np; ++v) ex->nbP[v] = RP.nbr[v] + 1;
+    for (int v = 0; v < nq; ++v) ex->nbQ[v] = RQ.nbr[v] + 1;
+    ex->lbP.assign(np, -100); ex->lbQ.assign(nq, -100);
+    for (int i = 0; i < np; ++i) {
+      if (ex->alP[i] == -100) continue;
+      const int nId = RP.nbr[i];
+      if (nId < 0 || nId >= nq) continue;
+      const int pm = (i + np - 1) % np, pp = (i + 1) % np;
+      const int pMN = ex->alP[pm] != -100 ? RP.nbr[pm] : -100;
+      const int pPN = ex->alP[pp] != -100 ? RP.nbr[pp] : -100;
+      const int a = relKeyed(pMN, pPN, (nId + nq - 1) % nq, pm, i, pp);
+      const int b = relKeyed(pMN, pPN, (nId + 1) % nq, pm, i, pp);
+      const int32_t L = labelKeyed(a, b);
+      ex->lbP[i] = L;
+      ex->lbQ[nId] = L;
+    }
+  }
+
   void run(const double* P, int nP, const double* Q, int nQ) {
     out.clear();
     // ---- MBRs and CMBR (ghcuda.cpp:94-125, readShapefile.h:304-330)
@@ -398,6 +480,7 @@ struct Clipper {
     if (filters) {
       if (mb[0][0] > mb[1][2] || mb[0][2] < mb[1][0] || mb[0][1] > mb[1][3] || mb[0][3] < mb[1][1]) {
         status = 2;
+        if (ex) exportPlain(P, nP, Q, nQ);
         return;
       }
     }
@@ -545,7 +628,17 @@ struct Clipper {
         for (int t = 0; t < 9; ++t) typeCount[t] += pt.tc[t];
       }
     }
-    if (filters && count1P != count1Q) { status = 1; return; }   // gppolyclip_mDIV512.cu:1461
+    if (filters && count1P != count1Q) {                         // gppolyclip_mDIV512.cu:1461
+      status = 1;
+      if (ex) {
+        ex->np = nP; ex->nq = nQ;
+        for (const Rec& rc : recs) {
+          if (rc.type == 1 || rc.type == 3 || rc.type == 5 || rc.type == 7) ex->np++;
+          if (rc.type == 1 || rc.type == 2 || rc.type == 5 || rc.type == 6) ex->nq++;
+        }
+      }
+      return;
+    }
 
     // ---- merged rings: source vertex of each edge followed by inserted vertices in
     // ascending parameter; equal parameters keep the later-inserted vertex first
@@ -611,6 +704,8 @@ struct Clipper {
         case 4: case 8: link(RP, srcP[rc.p], RQ, srcQ[rc.q]); break;
       }
     }
+
+    if (ex) { exportRings(recs, srcP, srcQ, insP, insQ); return; }
 
     // ---- step 1: initial labels on P, copied to the neighbour on Q
     forIntersections(RP, RP.root, [&](int I) {
@@ -880,6 +975,39 @@ void orc_result_copy(int32_t* status, int32_t* ncomp, int64_t* count1, int64_t* 
   if (nrec) std::copy(g_store.nrec.begin(), g_store.nrec.end(), nrec);
   if (compSize) std::copy(g_store.compSize.begin(), g_store.compSize.end(), compSize);
   if (xy) std::copy(g_store.xy.begin(), g_store.xy.end(), xy);
+}
+
+static Clipper::Export g_export;
+static int32_t g_export_status = 0;
+
+// The reference's calculateIntersections for one pair (GPU-path semantics: CMBR and
+// edge-box filters, P/Q count cross-check).  P, Q: open rings; P is not swapped.
+// flags bit2: exact-predicate mode.  out3 = merged sizes n_p, n_q and the invalid flag.
+// Returns the pair status (0 ok, 1 invalid, 2 disjoint MBRs).
+int orc_pair_intersections(const double* P, int nP, const double* Q, int nQ, double eps, int flags,
+                           int64_t* out3) {
+  Clipper c;
+  c.eps = eps; c.epsClean = 0; c.uni = false; c.filters = true; c.exact = (flags >> 2) & 1;
+  g_export = Clipper::Export();
+  c.ex = &g_export;
+  c.run(P, nP, Q, nQ);
+  g_export_status = c.status;
+  out3[0] = g_export.np;
+  out3[1] = g_export.nq;
+  out3[2] = c.status == 1 ? 1 : 0;
+  return c.status;
+}
+
+// arrays of the last orc_pair_intersections (sizes 2 n_p, 2 n_q, then n_p / n_q each);
+// nothing is written for an invalid pair
+void orc_pair_intersections_copy(double* xyP, double* xyQ, int32_t* alP, int32_t* alQ, int32_t* lbP,
+                                 int32_t* lbQ, int32_t* nbP, int32_t* nbQ) {
+  if (g_export_status == 1) return;
+  const Clipper::Export& e = g_export;
+  std::copy(e.xyP.begin(), e.xyP.end(), xyP); std::copy(e.xyQ.begin(), e.xyQ.end(), xyQ);
+  std::copy(e.alP.begin(), e.alP.end(), alP); std::copy(e.alQ.begin(), e.alQ.end(), alQ);
+  std::copy(e.lbP.begin(), e.lbP.end(), lbP); std::copy(e.lbQ.begin(), e.lbQ.end(), lbQ);
+  std::copy(e.nbP.begin(), e.nbP.end(), nbP); std::copy(e.nbQ.begin(), e.nbQ.end(), nbQ);
 }
 
 // exact sign of A3(P, Q, R) for n point triples (v: 6 doubles per triple), and of the

@@ -47,6 +47,10 @@ def lib():
         L.orc_result_copy.restype = None
         L.orc_exact_signs.argtypes = [vp, i64, i32, vp]
         L.orc_exact_signs.restype = None
+        L.orc_pair_intersections.argtypes = [vp, i32, vp, i32, d, i32, vp]
+        L.orc_pair_intersections.restype = i32
+        L.orc_pair_intersections_copy.argtypes = [vp] * 8
+        L.orc_pair_intersections_copy.restype = None
         _lib = L
     return _lib
 
@@ -115,6 +119,29 @@ def clip_pair(P, Q, eps=1e-7, eps_clean=None, union=False, gpu_semantics=True, e
     return _collect()
 
 
+INTERSECTION_FIELDS = ("xy_p", "xy_q", "alpha_p", "alpha_q", "label_p", "label_q", "neighbor_p", "neighbor_q")
+
+
+def pair_intersections(P, Q, eps=1e-7, exact=False):
+    """What the reference's calculateIntersections returns for P (not swapped) against Q:
+    dict with status, n_p, n_q, invalid and, unless invalid, the merged rings (xy_*), keys
+    (alpha_*), initial labels (label_*) and 1-based neighbours (neighbor_*)."""
+    P = np.ascontiguousarray(P, np.float64).reshape(-1)
+    Q = np.ascontiguousarray(Q, np.float64).reshape(-1)
+    out3 = np.zeros(3, np.int64)
+    st = lib().orc_pair_intersections(_p(P), len(P) // 2, _p(Q), len(Q) // 2, eps,
+                                      FLAG_EXACT if exact else 0, _p(out3))
+    r = {"status": int(st), "n_p": int(out3[0]), "n_q": int(out3[1]), "invalid": int(out3[2])}
+    if r["invalid"]:
+        return r
+    np_, nq = r["n_p"], r["n_q"]
+    arrs = [np.zeros(2 * np_), np.zeros(2 * nq)] + [np.zeros(n, np.int32) for n in (np_, nq) * 3]
+    arrs = [arrs[0], arrs[1], arrs[2], arrs[3], arrs[4], arrs[5], arrs[6], arrs[7]]
+    lib().orc_pair_intersections_copy(*[_p(a) for a in arrs])
+    r.update(zip(INTERSECTION_FIELDS, arrs))
+    return r
+
+
 def clip_batch(base, overlay, pid, qid, eps=1e-7, eps_clean=None, union=False,
                gpu_semantics=True, exact=False):
     """Clip the listed (base, overlay) pairs with the reference's swap rule.  exact=True
@@ -174,6 +201,34 @@ def ref_clip_pairs(pairs, union=False):
         cmd = [REF_BIN, "batch", fin, fout] + (["union"] if union else [])
         subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
         return read_result_batch(fout)
+
+
+RING_FIELDS = ("x", "y", "alpha", "source", "inter", "label", "nb")
+
+
+def ref_rings(pairs):
+    """The reference's own merged vertex lists after computeIntersections plus the step-1
+    labels, per pair: a (P list, Q list) tuple of dicts of arrays named RING_FIELDS."""
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        fout = os.path.join(td, "out.bin")
+        write_pair_batch(fin, pairs)
+        subprocess.run([REF_BIN, "rings", fin, fout], check=True, stdout=subprocess.DEVNULL)
+        data = open(fout, "rb").read()
+    rec = np.dtype([("x", "<f8"), ("y", "<f8"), ("alpha", "<f8"), ("source", "<i4"), ("inter", "<i4"),
+                    ("label", "<i4"), ("nb", "<i4")])
+    off = 8
+    out = []
+    for _ in range(struct.unpack_from("<q", data, 0)[0]):
+        n_p, n_q = struct.unpack_from("<ii", data, off)
+        off += 8
+        sides = []
+        for n in (n_p, n_q):
+            a = np.frombuffer(data, rec, n, off)
+            off += n * rec.itemsize
+            sides.append({f: a[f].copy() for f in RING_FIELDS})
+        out.append(tuple(sides))
+    return out
 
 
 def ref_time_pairs(pairs, reps=1, union=False):

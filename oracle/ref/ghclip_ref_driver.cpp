@@ -23,6 +23,7 @@
 //   ghclip_ref text P.poly Q.poly R.poly [union]   (reference .poly text format)
 //   ghclip_ref batch in.bin out.bin [union]          (binary pair batch, see readBatch)
 //   ghclip_ref time  in.bin reps [union]             (times the batch, prints seconds)
+//   ghclip_ref rings in.bin out.bin                  (merged lists + step-1 labels, see below)
 
 #include <iostream>
 #include <fstream>
@@ -151,6 +152,43 @@ int main(int argc, char** argv) {
         int32_t nv = (int32_t)(xy.size() / 2);
         fwrite(&nv, 4, 1, f);
         fwrite(xy.data(), 8, xy.size(), f);
+      }
+      resetGlobals();
+    }
+    fclose(f);
+    return 0;
+  }
+  if (mode == "rings") {
+    // The reference's merged lists after computeIntersections and the step-1 labels, for
+    // each pair: int32 nP, nQ (list lengths), then per list and vertex in list order from
+    // the root: f64 x, y, alpha; int32 source, intersection, label, neighbour position in
+    // the other list (-1 = none).
+    std::vector<Pair> pairs = readBatch(argv[2]);
+    FILE* f = fopen(argv[3], "wb");
+    if (!f) { perror(argv[3]); return 2; }
+    int64_t n = (int64_t)pairs.size();
+    fwrite(&n, 8, 1, f);
+    for (auto& pr : pairs) {
+      pPolygon.push_back(makePolygon(pr.p.data(), (int)(pr.p.size() / 2)));
+      qPolygon.push_back(makePolygon(pr.q.data(), (int)(pr.q.size() / 2)));
+      computeIntersections();
+      initialLabels();
+      std::vector<vertex*> lists[2];
+      for (vertex* V : pPolygon[0].vertices(ALL)) lists[0].push_back(V);
+      for (vertex* V : qPolygon[0].vertices(ALL)) lists[1].push_back(V);
+      int32_t sz[2] = {(int32_t)lists[0].size(), (int32_t)lists[1].size()};
+      fwrite(sz, 4, 2, f);
+      for (int side = 0; side < 2; ++side) {
+        const std::vector<vertex*>& other = lists[1 - side];
+        for (vertex* V : lists[side]) {
+          double d[3] = {V->p.x, V->p.y, V->alpha};
+          int32_t nb = -1;
+          for (size_t j = 0; V->neighbour && j < other.size(); ++j)
+            if (other[j] == V->neighbour) { nb = (int32_t)j; break; }
+          int32_t w[4] = {V->source ? 1 : 0, V->intersection ? 1 : 0, (int32_t)V->label, nb};
+          fwrite(d, 8, 3, f);
+          fwrite(w, 4, 4, f);
+        }
       }
       resetGlobals();
     }

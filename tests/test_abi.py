@@ -25,6 +25,7 @@ def declared_functions(header="gcmfgh.h"):
 def test_header_declares_the_entry_points():
     names = declared_functions()
     for n in ("gcmf_join", "gh_clip_batch", "gh_clip_pair", "gh_clip_joined", "gcmfgh_create",
+              "gh_calculate_intersections", "gh_free_intersections",
               "gcmfgh_join_clip_host", "gcmfgh_exclusive_scan_i32", "gcmfgh_radix_sort_u64"):
         assert n in names
 
@@ -45,7 +46,9 @@ def test_shim_library_exports_the_reference_signatures():
     out = subprocess.run(["nm", "-DC", "--defined-only", lib], capture_output=True, text=True, check=True).stdout
     assert "spatialJoin(int, char**, int**, int**, long*, double**, double**, int**, long**, int**, long**)" in out
     assert "ghcuda(int*, int*, int, double*, double*, int*, long*, int*, long*)" in out
-    assert declared_functions("gcmfgh_shims.h") == {"spatialJoin", "ghcuda"}
+    assert ("calculateIntersections(double*, double*, int, int, double*, int*, long*, int*, long*, int, int, "
+            "int*, int*, double**, double**, int**, int**, int**, int**, int**, int**, int*)") in out
+    assert declared_functions("gcmfgh_shims.h") == {"spatialJoin", "ghcuda", "calculateIntersections"}
 
 
 def test_library_loads_and_reports_status_strings():

@@ -124,3 +124,65 @@ def test_containment_and_disjoint_boundaries():
     res = pyoracle.clip_batch(base, ovl, r.b, r.o)
     assert list(res.ncomp) == [1, 1]
     assert same_components(res.components(0), [_box(2, 2, 3, 3)])
+
+
+def _ring_pairs():
+    d = np.load(os.path.join(GOLDEN, "ring_pairs.npz"))
+    op = oq = lp = lq = 0
+    for k in range(len(d["nP"])):
+        P = d["P"][2 * op:2 * (op + d["nP"][k])].reshape(-1, 2)
+        Q = d["Q"][2 * oq:2 * (oq + d["nQ"][k])].reshape(-1, 2)
+        ref = ({f: d[f"p_{f}"][lp:lp + d["lenP"][k]] for f in pyoracle.RING_FIELDS},
+               {f: d[f"q_{f}"][lq:lq + d["lenQ"][k]] for f in pyoracle.RING_FIELDS})
+        op += d["nP"][k]; oq += d["nQ"][k]; lp += d["lenP"][k]; lq += d["lenQ"][k]
+        yield P, Q, ref
+
+
+def test_pair_intersections_match_reference_lists():
+    """The oracle's calculateIntersections outputs against the reference's own merged lists
+    (computeIntersections + step-1 labels of GH-CUDA/lib/polyclip.h, fixture made by
+    tests/golden/make_ring_goldens.py): same vertices in the same order, same links, the
+    inserted vertices' keys equal (int)(1e7 * alpha), same initial labels.  Labels are
+    compared where the GPU's rule for 'linked neighbour' (key != -100,
+    gppolyclip_mDIV512.cu:1190-1201) agrees with the list's intersection flag: the source
+    vertex of an X-overlap (type 5) is linked but keeps the key -100 on the GPU."""
+    n = 0
+    for P, Q, ref in _ring_pairs():
+        r = pyoracle.pair_intersections(P, Q)
+        assert r["status"] == 0
+        quirkP = (r["neighbor_p"] != 0) & (r["alpha_p"] == -100)
+        for tag, R in (("p", ref[0]), ("q", ref[1])):
+            assert r["n_" + tag] == len(R["x"])
+            xy = r["xy_" + tag].reshape(-1, 2)
+            assert np.array_equal(xy[:, 0], R["x"]) and np.array_equal(xy[:, 1], R["y"])
+            nb = r["neighbor_" + tag]
+            assert np.array_equal(nb != 0, R["inter"] == 1)
+            m = R["inter"] == 1
+            assert np.array_equal(nb[m] - 1, R["nb"][m])
+            ins = R["source"] == 0
+            assert np.array_equal(r["alpha_" + tag][ins], (1e7 * R["alpha"][ins]).astype(np.int64))
+        lbP = r["label_p"]
+        npv = len(lbP)
+        keyed = np.flatnonzero(lbP != -100)
+        clean = keyed[~(quirkP[(keyed - 1) % npv] | quirkP[(keyed + 1) % npv])]
+        got = np.where(lbP[clean] == -102, 0, lbP[clean])
+        assert np.array_equal(got, ref[0]["label"][clean])
+        qn = r["neighbor_p"][clean] - 1
+        assert np.array_equal(np.where(r["label_q"][qn] == -102, 0, r["label_q"][qn]), ref[1]["label"][qn])
+        n += 1
+    assert n == 128
+
+
+def test_pair_intersections_invalid_and_disjoint():
+    # disjoint MBRs: the rings come back unchanged, every vertex plain
+    P = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], float)
+    r = pyoracle.pair_intersections(P, P + 5)
+    assert r["status"] == 2 and r["n_p"] == 4 and r["n_q"] == 4
+    assert np.array_equal(r["xy_p"], P.reshape(-1)) and (r["alpha_p"] == -100).all()
+    assert (r["neighbor_q"] == 0).all() and (r["label_q"] == -100).all()
+    # stars scaled to 1e-3: every area falls under the absolute tolerance, so the P-side and
+    # Q-side counts differ and the pair is invalid (no arrays)
+    P, Q = synth.random_star_pairs(7, 1, 4, 12, spread=1.0)[0]
+    r = pyoracle.pair_intersections(P * 1e-3, Q * 1e-3)
+    assert r["invalid"] == 1 and r["status"] == 1
+    assert "xy_p" not in r and r["n_p"] >= len(P) and r["n_q"] >= len(Q)
