@@ -26,6 +26,13 @@ GCMFGH_DEV void raise_error(int* err, int code) {
   if (err) atomicCAS(err, 0, code);
 }
 
+// GH vertex labels (IntersectionLabel, polygon.h:21-32), entry/exit flags
+// (EntryExitLabel) and relative positions (RelativePositionType, polyclip.h:290-295)
+enum : int8_t { L_NONE = 0, L_CROSSING, L_BOUNCING, L_LEFT_ON, L_RIGHT_ON, L_ON_ON, L_ON_LEFT,
+                L_ON_RIGHT, L_DELAYED_CROSSING, L_DELAYED_BOUNCING };
+enum : int8_t { E_EXIT = 0, E_ENTRY = 1, E_NEITHER = 2 };
+enum : int { R_LEFT = 0, R_RIGHT = 1, R_IS_P_M = 2, R_IS_P_P = 3 };
+
 // host-side count of kernel launches issued by the library (gcmfgh_launch_count)
 unsigned long long& launch_counter();
 inline void note_launch() { ++launch_counter(); }

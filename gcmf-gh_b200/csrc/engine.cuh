@@ -125,7 +125,18 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
 // ring order, the integer parameter key (int)(1e7 * alpha) of every vertex that carries an
 // intersection (-100 at plain vertices), the initial label (-100 where no key), and the
 // 1-based slot of the neighbour in the other ring (0 = none).
+//
+// With records_only set, the clip instead stops after the emit stage (G3) and hands back
+// the device arrays of every pair's intersection records, valid until the arena is reset.
 struct RingExport {
+  bool records_only = false;
+  int64_t n_records = 0;
+  const int32_t* rec_p = nullptr;    // pair-local P edge
+  const int32_t* rec_q = nullptr;    // pair-local Q edge
+  const double* rec_a = nullptr;     // alpha (on P)
+  const double* rec_b = nullptr;     // beta (on Q)
+  const int8_t* rec_t = nullptr;     // intersection type 1..8
+  const int32_t* rec_k = nullptr;    // pair
   int status = 0;                    // pair status: 0 ok, 1 invalid, 2 disjoint MBRs
   int64_t n_p = 0, n_q = 0;          // merged ring sizes
   int64_t edges_p = 0, edges_q = 0;  // ring edges (vertices without the closing one)
@@ -141,6 +152,12 @@ int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, co
              int64_t n_pairs, const ClipParams& prm, Arena& arena, ClipDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
              cudaStream_t aux = nullptr, RingExport* ex = nullptr);
+
+// One pair of multi-component polygons (rings: host, interleaved, open; ring c has
+// sizes[c] >= 3 vertices), P clipped against Q as given.  Result as one pair of ClipDev.
+int run_clip_multi(const double* P, const int32_t* sizesP, int kP, const double* Q, const int32_t* sizesQ, int kQ,
+                   const ClipParams& prm, Arena& arena, ClipDev& out, int* d_err, int64_t* h_scratch,
+                   cudaStream_t s);
 
 // a non-blocking stream at the device's highest priority (nullptr on failure)
 cudaStream_t create_priority_stream();

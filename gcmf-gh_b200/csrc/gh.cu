@@ -56,10 +56,6 @@ inline unsigned blocks_for_warps(int64_t warps) {
 }
 inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
-enum : int8_t { L_NONE = 0, L_CROSSING, L_BOUNCING, L_LEFT_ON, L_RIGHT_ON, L_ON_ON, L_ON_LEFT,
-                L_ON_RIGHT, L_DELAYED_CROSSING, L_DELAYED_BOUNCING };
-enum : int8_t { E_EXIT = 0, E_ENTRY = 1, E_NEITHER = 2 };
-enum : int { R_LEFT = 0, R_RIGHT = 1, R_IS_P_M = 2, R_IS_P_P = 3 };
 
 // ---------------------------------------------------------------- pair setup
 struct PairDev {
@@ -3274,6 +3270,12 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
                                                                      W.recPos, R); note_launch(); }
   }
   mk->mark("clip:emit", s);
+  if (ex && ex->records_only) {
+    ex->n_records = nR;
+    ex->rec_p = R.p; ex->rec_q = R.q; ex->rec_a = R.a; ex->rec_b = R.b; ex->rec_t = R.t; ex->rec_k = R.k;
+    C.n_records = nR;
+    return ST_OK;
+  }
   // ---- G4 ring layout
   int32_t* insP = A.take_n<int32_t>(nEP);
   int32_t* insQ = A.take_n<int32_t>(nEQ);

@@ -116,6 +116,7 @@ def lib():
         L.gh_clip_get.argtypes = [vp, ctypes.c_int, vp, i64, ctypes.c_int, P(i64)]
         L.gh_clip_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
         L.gh_clip_pair.argtypes = [vp, vp, i32, vp, i32, P(ClipInfo)]
+        L.gh_clip_multi.argtypes = [vp, vp, vp, i32, vp, vp, i32, P(ClipInfo)]
         L.gh_calculate_intersections.argtypes = [vp, P(Layer), i32, P(Layer), i32, P(Intersections)]
         L.gh_free_intersections.argtypes = [P(Intersections)]
         L.gh_free_intersections.restype = None
@@ -295,6 +296,18 @@ class Engine:
         info = ClipInfo()
         _check(lib().gh_clip_pair(self.h, _np_ptr(P), len(P) // 2, _np_ptr(Q), len(Q) // 2,
                                   ctypes.byref(info)))
+        return info.as_dict()
+
+    def clip_multi(self, P_rings, Q_rings):
+        """Clip one pair of multi-component polygons (lists of open rings, holes by
+        even-odd); read the result with clip_result()."""
+        P = np.ascontiguousarray(np.concatenate([np.asarray(r, np.float64).reshape(-1) for r in P_rings]))
+        Q = np.ascontiguousarray(np.concatenate([np.asarray(r, np.float64).reshape(-1) for r in Q_rings]))
+        sp = np.array([len(np.asarray(r).reshape(-1)) // 2 for r in P_rings], np.int32)
+        sq = np.array([len(np.asarray(r).reshape(-1)) // 2 for r in Q_rings], np.int32)
+        info = ClipInfo()
+        _check(lib().gh_clip_multi(self.h, _np_ptr(P), _np_ptr(sp), len(sp), _np_ptr(Q), _np_ptr(sq), len(sq),
+                                   ctypes.byref(info)))
         return info.as_dict()
 
     def calculate_intersections(self, p_layer: DeviceLayer, p_id, q_layer: DeviceLayer, q_id):

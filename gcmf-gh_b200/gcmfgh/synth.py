@@ -202,3 +202,35 @@ def serving_workload(seed: int = 4, n: int = 1_000_000, n_queries: int = 512, co
     ql = star_layer(rng, qcounts, qcentres, qbase)
     queries = [np.ascontiguousarray(ql.ring(i)) for i in range(n_queries)]
     return resident, queries
+
+
+def holed_polygon(rng, cx, cy, vmin=5, vmax=30, max_holes=3, max_islands=2):
+    """A multi-component polygon as a list of open rings: 1..max_islands disjoint star
+    islands (radius 1), each with 0..max_holes star holes placed on a circle of radius 0.35
+    around the island centre (hole radius <= 0.15, so holes are disjoint and inside).
+    Holes are clockwise half of the time."""
+    rings = []
+    islands = int(rng.integers(1, max_islands + 1))
+    for k in range(islands):
+        ox = cx + 2.2 * k
+        rings.append(_star(rng, int(rng.integers(vmin, vmax + 1)), ox, cy, 1.0, 0.6, 1.0))
+        h = int(rng.integers(0, max_holes + 1))
+        for t in range(h):
+            ang = 2 * np.pi * t / max(h, 1) + rng.uniform(-0.3, 0.3)
+            hole = _star(rng, int(rng.integers(max(3, vmin // 2), max(4, vmax // 2) + 1)),
+                         ox + 0.35 * np.cos(ang), cy + 0.35 * np.sin(ang), 0.15, 0.5, 1.0)
+            rings.append(hole[::-1].copy() if rng.random() < 0.5 else hole)
+    return rings
+
+
+def holed_pairs(seed: int, npairs: int, vmin: int = 5, vmax: int = 30):
+    """Seeded pairs of multi-component polygons (islands with holes) whose centres are at
+    most 0.8 apart, for the multi-component clip."""
+    rng = np.random.default_rng(seed)
+    pairs = []
+    for _ in range(npairs):
+        P = holed_polygon(rng, 0.0, 0.0, vmin, vmax)
+        d = rng.uniform(0.0, 0.8, size=2)
+        Q = holed_polygon(rng, d[0], d[1], vmin, vmax)
+        pairs.append((P, Q))
+    return pairs

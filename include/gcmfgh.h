@@ -181,6 +181,17 @@ gcmfgh_status gh_clip_ptr(gcmfgh_ctx* ctx, int field, const void** dev_ptr, int6
 gcmfgh_status gh_clip_pair(gcmfgh_ctx* ctx, const double* P, int32_t nP, const double* Q, int32_t nQ,
                            gcmfgh_clip_info* info);
 
+/* ---- one pair of multi-component polygons (outer rings and holes, even-odd; the
+ * reference's CPU clipper over component lists, GH-CUDA/lib/polyclip.h, whose GPU form
+ * calculateIntersectionsMultipleComponents is declared in ghcuda.h:15 and never defined).
+ * P, Q: host rings, interleaved and open (no closing vertex), ring c of p_sizes[c] (or
+ * q_sizes[c]) >= 3 vertices, one after the other.  P is clipped against Q as given.
+ * Every (P ring, Q ring) pair gets the GPU path's filters and P/Q count check; one failing
+ * ring pair makes the pair invalid (status 1).  The result is read like one pair of
+ * gh_clip_batch (gh_clip_get / gh_clip_ptr). */
+gcmfgh_status gh_clip_multi(gcmfgh_ctx* ctx, const double* P, const int32_t* p_sizes, int32_t p_rings,
+                            const double* Q, const int32_t* q_sizes, int32_t q_rings, gcmfgh_clip_info* info);
+
 /* ---- the intersection phase of one pair: replaces calculateIntersections
  * (ghcuda.h:6-14, gppolyclip_mDIV512.cu:1298-1640), which hands the merged rings to the
  * host list builder (ghcuda.cpp:239-322).  Arrays are host malloc'ed, freed by

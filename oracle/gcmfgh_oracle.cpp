@@ -37,6 +37,7 @@
 #include <cstring>
 #include <cmath>
 #include <vector>
+#include <array>
 #include <algorithm>
 #include <numeric>
 #include <thread>
@@ -232,6 +233,44 @@ inline bool edgeTouchesBox(Pt P1, Pt P2, const double* c) {
   if (minX > c[2] || maxX < c[0]) return false;
   if (minY > c[3] || maxY < c[1]) return false;
   return true;
+}
+
+// ---- clean-up (polyclip.h:791-807): drop the root while it is collinear, then one
+// forward pass over the remaining vertices; components left empty are dropped.
+void cleanUp(std::vector<std::vector<Pt>>& out, double epsClean) {
+    for (auto& comp : out) {
+      int m = (int)comp.size();
+      if (m == 0) continue;
+      std::vector<int> nx(m), pv(m);
+      for (int i = 0; i < m; ++i) { nx[i] = (i + 1) % m; pv[i] = (i + m - 1) % m; }
+      int root = 0, alive = m;
+      auto area = [&](int v) {
+        return std::fabs(A3(comp[pv[v]].x, comp[pv[v]].y, comp[v].x, comp[v].y, comp[nx[v]].x, comp[nx[v]].y));
+      };
+      auto remove = [&](int v) {
+        if (root == v) { root = nx[v]; if (nx[root] == root) root = -1; }
+        nx[pv[v]] = nx[v]; pv[nx[v]] = pv[v];
+        --alive;
+      };
+      while (root >= 0 && area(root) < epsClean) remove(root);
+      std::vector<Pt> res;
+      if (root >= 0) {
+        int start = root, v = root;
+        do {
+          int nxt = nx[v];
+          if (area(v) < epsClean) remove(v);
+          v = nxt;
+        } while (v != start && root >= 0);
+        if (root >= 0) {
+          v = root;
+          do { res.push_back(comp[v]); v = nx[v]; } while (v != root);
+        }
+      }
+      comp.swap(res);
+    }
+    std::vector<std::vector<Pt>> kept;
+    for (auto& c : out) if (!c.empty()) kept.push_back(std::move(c));
+    out.swap(kept);
 }
 
 struct Rec { int p, q; double a, b; int type; };
@@ -858,41 +897,422 @@ struct Clipper {
       }
     }
 
-    // ---- clean-up (polyclip.h:791-807): drop the root while it is collinear, then
-    // one forward pass over the remaining vertices.
-    for (auto& comp : out) {
-      int m = (int)comp.size();
-      if (m == 0) continue;
-      std::vector<int> nx(m), pv(m);
-      for (int i = 0; i < m; ++i) { nx[i] = (i + 1) % m; pv[i] = (i + m - 1) % m; }
-      int root = 0, alive = m;
-      auto area = [&](int v) {
-        return std::fabs(A3(comp[pv[v]].x, comp[pv[v]].y, comp[v].x, comp[v].y, comp[nx[v]].x, comp[nx[v]].y));
-      };
-      auto remove = [&](int v) {
-        if (root == v) { root = nx[v]; if (nx[root] == root) root = -1; }
-        nx[pv[v]] = nx[v]; pv[nx[v]] = pv[v];
-        --alive;
-      };
-      while (root >= 0 && area(root) < epsClean) remove(root);
-      std::vector<Pt> res;
-      if (root >= 0) {
-        int start = root, v = root;
-        do {
-          int nxt = nx[v];
-          if (area(v) < epsClean) remove(v);
-          v = nxt;
-        } while (v != start && root >= 0);
-        if (root >= 0) {
-          v = root;
-          do { res.push_back(comp[v]); v = nx[v]; } while (v != root);
+    cleanUp(out, epsClean);
+  }
+};
+
+// ------------------------------------------------------------------ multi-component pairs
+// P and Q each made of several rings (outer boundaries and holes, even-odd).  The
+// reference's CPU clipper handles them by looping over components in every phase
+// (GH-CUDA/lib/polyclip.h: computeIntersections :202-268 over all component pairs, step 1
+// and the chains per component, special cases :474-541 per component with the inside
+// test's parity over all components of the other polygon and the hole test for identical
+// components, entry/exit :549-655 per component, split pairs and crossing candidates over
+// all components, tracing :743-783 from every component of P).  The GPU intersection
+// phase has no multi-component form (calculateIntersectionsMultipleComponents is declared
+// in GH-CUDA/ghcuda.h:15 and defined nowhere).  With filters on, every (P ring, Q ring)
+// pair gets the GPU path's common-MBR edge filter, edge-box test and P/Q count check; a
+// failing ring pair makes the whole pair invalid.
+struct MultiClipper {
+  double eps, epsClean;
+  bool uni, filters, exact = false;
+  Ring R[2];
+  std::vector<int> roots[2];                   // root slot of every component
+  std::vector<std::vector<Pt>> out;
+  long long count1P = 0, nrec = 0;
+  int status = 0;
+
+  static void link(Ring& a, int i, Ring& b, int j) { a.nbr[i] = j; b.nbr[j] = i; a.inter[i] = 1; b.inter[j] = 1; }
+
+  bool pointInComp(const Ring& Rg, int root, double Rx, double Ry) const {   // polygon.h:427-448
+    int w = 0, one = root;
+    do {
+      int two = Rg.next[one];
+      double P0x = Rg.x[one], P0y = Rg.y[one], P1x = Rg.x[two], P1y = Rg.y[two];
+      if ((P0y < Ry) != (P1y < Ry)) {
+        if (P0x >= Rx) {
+          if (P1x > Rx) w = w + 2 * (P1y > P0y) - 1;
+          else if ((orientSign(exact, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
+        } else if (P1x > Rx) {
+          if ((orientSign(exact, P0x, P0y, P1x, P1y, Rx, Ry) > 0) == (P1y > P0y)) w = w + 2 * (P1y > P0y) - 1;
         }
       }
-      comp.swap(res);
+      one = two;
+    } while (one != root);
+    return (w % 2) != 0;
+  }
+  RelPos rel(int qv, int p1, int p2, int p3) const {                      // polyclip.h:297-326
+    const Ring& P = R[0];
+    const Ring& Q = R[1];
+    if (P.inter[p1] && P.nbr[p1] == qv) return IS_P_m;
+    if (P.inter[p3] && P.nbr[p3] == qv) return IS_P_p;
+    int s1 = orientSign(exact, Q.x[qv], Q.y[qv], P.x[p1], P.y[p1], P.x[p2], P.y[p2]);
+    int s2 = orientSign(exact, Q.x[qv], Q.y[qv], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+    int s3 = orientSign(exact, P.x[p1], P.y[p1], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+    if (s3 > 0) return (s1 > 0 && s2 > 0) ? LEFT : RIGHT;
+    return (s1 < 0 && s2 < 0) ? RIGHT : LEFT;
+  }
+  template <class F> static void forInter(const Ring& rg, int start, F f) {   // vertexIterator
+    int V = start;
+    if (!rg.inter[V]) {
+      do { V = rg.next[V]; } while (!rg.inter[V] && V != start);
+      if (V == start) return;
     }
-    std::vector<std::vector<Pt>> kept;
-    for (auto& c : out) if (!c.empty()) kept.push_back(std::move(c));
-    out.swap(kept);
+    for (;;) {
+      f(V);
+      do { V = rg.next[V]; } while (!rg.inter[V] && V != start);
+      if (V == start) return;
+    }
+  }
+  bool noCrossing(const Ring& rg, int root) const {                      // polygon.h:465-475
+    int v = root;
+    do {
+      if (rg.inter[v]) {
+        if (rg.label[v] == CROSSING || rg.label[v] == DELAYED_CROSSING) return false;
+        if (uni && (rg.label[v] == BOUNCING || rg.label[v] == DELAYED_BOUNCING)) return false;
+      }
+      v = rg.next[v];
+    } while (v != root);
+    return true;
+  }
+  static bool allOnOn(const Ring& rg, int root) {                       // polygon.h:453-458
+    int v = root;
+    do { if (rg.label[v] != ON_ON) return false; v = rg.next[v]; } while (v != root);
+    return true;
+  }
+  static bool nonInterPoint(const Ring& rg, int root, const Ring& other, double& px, double& py) {
+    int v = root;                                                       // polygon.h:480-491
+    do { if (!rg.inter[v]) { px = rg.x[v]; py = rg.y[v]; return true; } v = rg.next[v]; } while (v != root);
+    v = root;
+    do {
+      int nb = rg.nbr[v], nx = rg.next[v];
+      if (nb >= 0 && rg.nbr[nx] != other.prev[nb] && rg.nbr[nx] != other.next[nb]) {
+        px = 0.5 * (rg.x[v] + rg.x[nx]); py = 0.5 * (rg.y[v] + rg.y[nx]); return true;
+      }
+      v = rg.next[v];
+    } while (v != root);
+    return false;
+  }
+  static int nonInterVertex(Ring& rg, int root, const Ring& other) {    // polygon.h:496-512
+    int v = root;
+    do { if (!rg.inter[v]) return v; v = rg.next[v]; } while (v != root);
+    v = root;
+    do {
+      int nb = rg.nbr[v], nx = rg.next[v];
+      if (nb >= 0 && rg.nbr[nx] != other.prev[nb] && rg.nbr[nx] != other.next[nb]) {
+        int t = rg.add(0.5 * (rg.x[v] + rg.x[nx]), 0.5 * (rg.y[v] + rg.y[nx]), false);
+        rg.insertAfter(t, v);
+        return t;
+      }
+      v = rg.next[v];
+    } while (v != root);
+    return -1;
+  }
+  std::vector<Pt> compPoints(const Ring& rg, int root) const {
+    std::vector<Pt> pts;
+    int v = root;
+    do { pts.push_back({rg.x[v], rg.y[v]}); v = rg.next[v]; } while (v != root);
+    return pts;
+  }
+
+  // rings: interleaved open rings, ring k has sizes[k] vertices
+  void run(const double* P, const int32_t* sizesP, int kP, const double* Q, const int32_t* sizesQ, int kQ) {
+    out.clear();
+    std::vector<int64_t> offP(kP + 1, 0), offQ(kQ + 1, 0);
+    for (int i = 0; i < kP; ++i) offP[i + 1] = offP[i] + sizesP[i];
+    for (int j = 0; j < kQ; ++j) offQ[j + 1] = offQ[j] + sizesQ[j];
+    auto vP = [&](int i, int e) { int n = sizesP[i]; e %= n; return Pt{P[2 * (offP[i] + e)], P[2 * (offP[i] + e) + 1]}; };
+    auto vQ = [&](int j, int e) { int n = sizesQ[j]; e %= n; return Pt{Q[2 * (offQ[j] + e)], Q[2 * (offQ[j] + e) + 1]}; };
+    auto mbrOf = [&](const double* xy, int64_t o, int n, double* m) {
+      m[0] = m[2] = xy[2 * o]; m[1] = m[3] = xy[2 * o + 1];
+      for (int k = 0; k < n; ++k) {
+        double X = xy[2 * (o + k)], Y = xy[2 * (o + k) + 1];
+        m[0] = std::min(m[0], X); m[2] = std::max(m[2], X); m[1] = std::min(m[1], Y); m[3] = std::max(m[3], Y);
+      }
+    };
+    std::vector<std::array<double, 4>> mbP(kP), mbQ(kQ);
+    for (int i = 0; i < kP; ++i) mbrOf(P, offP[i], sizesP[i], mbP[i].data());
+    for (int j = 0; j < kQ; ++j) mbrOf(Q, offQ[j], sizesQ[j], mbQ[j].data());
+    auto cls = [&](Pt A1, Pt A2, Pt B1, Pt B2, double& al, double& be) {
+      return exact ? classifyExact(A1, A2, B1, B2, al, be) : classify(A1, A2, B1, B2, eps, al, be);
+    };
+    // ---- records in the reference's loop order: P component, P edge, Q component, Q edge
+    struct MRec { int i, p, j, q; double a, b; int type; };
+    std::vector<MRec> recs;
+    std::vector<long long> c1P((size_t)kP * kQ, 0), c1Q((size_t)kP * kQ, 0);
+    for (int i = 0; i < kP; ++i)
+      for (int e = 0; e < sizesP[i]; ++e) {
+        Pt P1 = vP(i, e), P2 = vP(i, e + 1);
+        for (int j = 0; j < kQ; ++j) {
+          const double* a = mbP[i].data();
+          const double* b = mbQ[j].data();
+          bool disjoint = a[0] > b[2] || a[2] < b[0] || a[1] > b[3] || a[3] < b[1];
+          if (filters && disjoint) continue;                       // ghcuda.cpp:109-116 per ring pair
+          double cm[4] = {std::max(a[0], b[0]), std::max(a[1], b[1]), std::min(a[2], b[2]), std::min(a[3], b[3])};
+          bool cmP = !filters || edgeTouchesBox(P1, P2, cm);
+          for (int q = 0; q < sizesQ[j]; ++q) {
+            Pt Q1 = vQ(j, q), Q2 = vQ(j, q + 1);
+            double al = 0, be = 0;
+            int tp;
+            if (filters) {
+              if (!edgeBoxesTouch(P1, P2, Q1, Q2)) continue;
+              bool cmQ = edgeTouchesBox(Q1, Q2, cm);
+              tp = (cmP || cmQ) ? cls(P1, P2, Q1, Q2, al, be) : 0;
+              if (cmP && tp) c1P[(size_t)i * kQ + j]++;
+              if (cmQ) { double a2, b2; if (cls(Q1, Q2, P1, P2, a2, b2)) c1Q[(size_t)i * kQ + j]++; }
+              if (!(tp && cmP && cmQ)) continue;
+            } else {
+              tp = cls(P1, P2, Q1, Q2, al, be);
+              if (!tp) continue;
+              c1P[(size_t)i * kQ + j]++; c1Q[(size_t)i * kQ + j]++;
+            }
+            recs.push_back({i, e, j, q, al, be, tp});
+          }
+        }
+      }
+    bool counts_differ = false;
+    for (size_t k = 0; k < c1P.size(); ++k) {
+      count1P += c1P[k];
+      if (c1P[k] != c1Q[k]) counts_differ = true;
+    }
+    if (filters && counts_differ) { status = 1; return; }     // per ring pair, gppolyclip_mDIV512.cu:1461
+    nrec = (long long)recs.size();
+    // ---- merged rings, component by component
+    Ring& RP = R[0];
+    Ring& RQ = R[1];
+    RP = Ring(); RQ = Ring();
+    roots[0].clear(); roots[1].clear();
+    std::vector<std::vector<int>> onP(offP[kP]), onQ(offQ[kQ]);
+    for (int r = 0; r < (int)recs.size(); ++r) {
+      int t = recs[r].type;
+      if (t == 1 || t == 3 || t == 5 || t == 7) onP[offP[recs[r].i] + recs[r].p].push_back(r);
+      if (t == 1 || t == 2 || t == 5 || t == 6) onQ[offQ[recs[r].j] + recs[r].q].push_back(r);
+    }
+    std::vector<int> srcP(offP[kP]), srcQ(offQ[kQ]), insP(recs.size(), -1), insQ(recs.size(), -1);
+    for (int i = 0; i < kP; ++i) {
+      int first = (int)RP.x.size();
+      roots[0].push_back(first);
+      for (int e = 0; e < sizesP[i]; ++e) {
+        srcP[offP[i] + e] = RP.add(vP(i, e).x, vP(i, e).y, true);
+        std::vector<int>& L = onP[offP[i] + e];
+        // ascending parameter; equal parameters: the later-inserted record (larger
+        // (Q component, Q edge)) first, as insertVertex does (polygon.h:101-113)
+        std::stable_sort(L.begin(), L.end(), [&](int u, int v) {
+          if (recs[u].a != recs[v].a) return recs[u].a < recs[v].a;
+          return std::make_pair(recs[u].j, recs[u].q) > std::make_pair(recs[v].j, recs[v].q);
+        });
+        for (int r : L) {
+          const MRec& rc = recs[r];
+          double X, Y;
+          if (rc.type == 1) {
+            Pt P1 = vP(i, e), P2 = vP(i, e + 1);
+            X = (1.0 - rc.a) * P1.x + rc.a * P2.x;
+            Y = (1.0 - rc.a) * P1.y + rc.a * P2.y;
+          } else {
+            X = vQ(rc.j, rc.q).x; Y = vQ(rc.j, rc.q).y;
+          }
+          insP[r] = RP.add(X, Y, false);
+        }
+      }
+      int last = (int)RP.x.size();
+      for (int v = first; v < last; ++v) { RP.next[v] = v + 1 < last ? v + 1 : first; RP.prev[v] = v > first ? v - 1 : last - 1; }
+    }
+    for (int j = 0; j < kQ; ++j) {
+      int first = (int)RQ.x.size();
+      roots[1].push_back(first);
+      for (int e = 0; e < sizesQ[j]; ++e) {
+        srcQ[offQ[j] + e] = RQ.add(vQ(j, e).x, vQ(j, e).y, true);
+        std::vector<int>& L = onQ[offQ[j] + e];
+        std::stable_sort(L.begin(), L.end(), [&](int u, int v) {
+          if (recs[u].b != recs[v].b) return recs[u].b < recs[v].b;
+          return std::make_pair(recs[u].i, recs[u].p) > std::make_pair(recs[v].i, recs[v].p);
+        });
+        for (int r : L) {
+          const MRec& rc = recs[r];
+          double X, Y;
+          if (rc.type == 1) { X = RP.x[insP[r]]; Y = RP.y[insP[r]]; }
+          else { X = vP(rc.i, rc.p).x; Y = vP(rc.i, rc.p).y; }
+          insQ[r] = RQ.add(X, Y, false);
+        }
+      }
+      int last = (int)RQ.x.size();
+      for (int v = first; v < last; ++v) { RQ.next[v] = v + 1 < last ? v + 1 : first; RQ.prev[v] = v > first ? v - 1 : last - 1; }
+    }
+    for (int r = 0; r < (int)recs.size(); ++r) {                  // polyclip.h:215-267
+      const MRec& rc = recs[r];
+      const int sp = srcP[offP[rc.i] + rc.p], sq = srcQ[offQ[rc.j] + rc.q];
+      switch (rc.type) {
+        case 1: link(RP, insP[r], RQ, insQ[r]); break;
+        case 5: link(RP, sp, RQ, insQ[r]); link(RP, insP[r], RQ, sq); break;
+        case 2: case 6: link(RP, sp, RQ, insQ[r]); break;
+        case 3: case 7: link(RP, insP[r], RQ, sq); break;
+        case 4: case 8: link(RP, sp, RQ, sq); break;
+      }
+    }
+    // ---- step 1 and step 2, per component of P
+    for (int root : roots[0])
+      forInter(RP, root, [&](int I) {
+        int nb = RP.nbr[I];
+        Label L = Clipper::initialLabel(rel(RQ.prev[nb], RP.prev[I], I, RP.next[I]),
+                                        rel(RQ.next[nb], RP.prev[I], I, RP.next[I]));
+        if (L != NONE) { RP.label[I] = L; RQ.label[nb] = L; }
+      });
+    for (int root : roots[0])
+      forInter(RP, root, [&](int I0) {
+        if (RP.label[I0] == LEFT_ON || RP.label[I0] == RIGHT_ON) {
+          RelPos x = RP.label[I0] == LEFT_ON ? LEFT : RIGHT;
+          int X = I0, I = I0;
+          do {
+            RP.label[I] = NONE;
+            RQ.label[RP.nbr[I]] = NONE;
+            I = RP.next[I];
+          } while (RP.label[I] == ON_ON);
+          RelPos y = RP.label[I] == ON_LEFT ? LEFT : RIGHT;
+          Label ct = (x != y) ? DELAYED_CROSSING : DELAYED_BOUNCING;
+          RP.label[X] = ct; RP.label[I] = ct;
+          RQ.label[RP.nbr[X]] = ct; RQ.label[RP.nbr[I]] = ct;
+        }
+      });
+    // ---- step 3.5, per component (polyclip.h:474-541)
+    std::vector<uint8_t> noInter[2], ident[2];
+    for (int s = 0; s < 2; ++s) {
+      noInter[s].assign(roots[s].size(), 0);
+      ident[s].assign(roots[s].size(), 0);
+      Ring& A = R[s];
+      Ring& B = R[1 - s];
+      for (size_t c = 0; c < roots[s].size(); ++c) {
+        int root = roots[s][c];
+        if (!noCrossing(A, root)) continue;
+        noInter[s][c] = 1;
+        if (allOnOn(A, root)) { ident[s][c] = 1; continue; }
+        double px = 0, py = 0;
+        nonInterPoint(A, root, B, px, py);
+        bool inside = false;
+        for (int rb : roots[1 - s]) if (pointInComp(B, rb, px, py)) inside = !inside;
+        if (inside ^ uni) out.push_back(compPoints(A, root));
+      }
+    }
+    for (size_t c = 0; c < roots[0].size(); ++c) {                  // identical components
+      if (!ident[0][c]) continue;
+      const int pr = roots[0][c];
+      bool pHole = false;
+      for (int r2 : roots[0]) if (r2 != pr && pointInComp(RP, r2, RP.x[pr], RP.y[pr])) pHole = !pHole;
+      for (size_t d = 0; d < roots[1].size(); ++d) {
+        if (!ident[1][d]) continue;
+        const int qr = roots[1][d];
+        bool match = false;
+        int v = qr;
+        do { if (v == RP.nbr[pr]) { match = true; break; } v = RQ.next[v]; } while (v != qr);
+        if (!match) continue;
+        bool qHole = false;
+        for (int r2 : roots[1]) if (r2 != qr && pointInComp(RQ, r2, RQ.x[qr], RQ.y[qr])) qHole = !qHole;
+        if (pHole == qHole) out.push_back(compPoints(RP, pr));
+        break;
+      }
+    }
+    // ---- step 4, per component (polyclip.h:549-655)
+    std::vector<int> split[2], cand[2];
+    for (int s = 0; s < 2; ++s) {
+      Ring& A = R[s];
+      Ring& B = R[1 - s];
+      for (size_t c = 0; c < roots[s].size(); ++c) {
+        if (noInter[s][c]) continue;
+        int V = nonInterVertex(A, roots[s][c], B);
+        if (V < 0) continue;
+        int st = ENTRY;
+        for (int rb : roots[1 - s]) if (pointInComp(B, rb, A.x[V], A.y[V])) st = (st == ENTRY) ? EXIT : ENTRY;
+        bool first = true;
+        auto toggle = [&]() { st = (st == ENTRY) ? EXIT : ENTRY; };
+        forInter(A, V, [&](int I) {
+          if (A.label[I] == CROSSING) { A.enex[I] = st; toggle(); }
+          if (A.label[I] == BOUNCING && ((st == EXIT) ^ uni)) split[s].push_back(I);
+          if (A.label[I] == DELAYED_CROSSING) {
+            A.enex[I] = st;
+            if (first) { if ((st == EXIT) ^ uni) A.label[I] = CROSSING; first = false; }
+            else { if ((st == ENTRY) ^ uni) A.label[I] = CROSSING; first = true; toggle(); }
+          }
+          if (A.label[I] == DELAYED_BOUNCING) {
+            A.enex[I] = st;
+            if (first) { if ((st == EXIT) ^ uni) cand[s].push_back(I); first = false; }
+            else { if ((st == ENTRY) ^ uni) cand[s].push_back(I); first = true; }
+            toggle();
+          }
+        });
+      }
+    }
+    // ---- step 5: split vertex pairs, in the order P's components found them
+    {
+      std::vector<uint8_t> inSplitQ(RQ.x.size(), 0);
+      for (int v : split[1]) inSplitQ[v] = 1;
+      std::vector<int> order = split[0];
+      for (int IP : order) {
+        int IQ = RP.nbr[IP];
+        if (IQ < 0 || IQ >= (int)inSplitQ.size() || !inSplitQ[IQ]) continue;
+        int VP = RP.add(RP.x[IP], RP.y[IP], false);
+        int VQ = RQ.add(RQ.x[IQ], RQ.y[IQ], false);
+        double sP = A3(RP.x[RP.prev[IP]], RP.y[RP.prev[IP]], RP.x[IP], RP.y[IP], RP.x[RP.next[IP]], RP.y[RP.next[IP]]);
+        double sQ = A3(RQ.x[RQ.prev[IQ]], RQ.y[RQ.prev[IQ]], RQ.x[IQ], RQ.y[IQ], RQ.x[RQ.next[IQ]], RQ.y[RQ.next[IQ]]);
+        bool same = exact ? orientSign(true, RP.x[RP.prev[IP]], RP.y[RP.prev[IP]], RP.x[IP], RP.y[IP],
+                                       RP.x[RP.next[IP]], RP.y[RP.next[IP]]) *
+                                orientSign(true, RQ.x[RQ.prev[IQ]], RQ.y[RQ.prev[IQ]], RQ.x[IQ], RQ.y[IQ],
+                                       RQ.x[RQ.next[IQ]], RQ.y[RQ.next[IQ]]) > 0
+                          : sP * sQ > 0;
+        if (same) { link(RP, IP, RQ, VQ); link(RP, VP, RQ, IQ); }
+        else link(RP, VP, RQ, VQ);
+        RP.insertAfter(VP, IP);
+        RQ.insertAfter(VQ, IQ);
+        int8_t e1 = uni ? ENTRY : EXIT, e2 = uni ? EXIT : ENTRY;
+        RP.enex[IP] = e1; RP.enex[VP] = e2; RQ.enex[IQ] = e1; RQ.enex[VQ] = e2;
+        RP.label[IP] = CROSSING; RP.label[VP] = CROSSING; RQ.label[IQ] = CROSSING; RQ.label[VQ] = CROSSING;
+      }
+    }
+    // ---- step 6: crossing candidates
+    {
+      std::vector<uint8_t> inCandQ(RQ.x.size(), 0);
+      for (int v : cand[1]) inCandQ[v] = 1;
+      for (int IP : cand[0]) {
+        int IQ = RP.nbr[IP];
+        if (IQ >= 0 && inCandQ[IQ]) { RP.label[IP] = CROSSING; RQ.label[IQ] = CROSSING; }
+      }
+    }
+    // ---- tracing from every component of P (polyclip.h:743-783)
+    long long budget = 4 * (long long)(RP.x.size() + RQ.x.size()) + 16;
+    for (int V0 : roots[0]) {
+      auto isStart = [&](int v) { return RP.inter[v] && RP.label[v] == CROSSING; };
+      int I = V0;
+      bool have = isStart(I);
+      if (!have) {
+        do { I = RP.next[I]; } while (!isStart(I) && I != V0);
+        have = (I != V0);
+      }
+      while (have) {
+        std::vector<Pt> comp;
+        int side = 0, V = I;
+        RP.inter[V] = 0;
+        do {
+          if (--budget < 0) { status = 3; out.clear(); return; }
+          Ring* cur = &R[side];
+          int st = cur->enex[V];
+          if (st == ENTRY) st = EXIT; else if (st == EXIT) st = ENTRY;
+          do {
+            if (--budget < 0) { status = 3; out.clear(); return; }
+            if ((st == EXIT) ^ uni) V = cur->next[V]; else V = cur->prev[V];
+            cur->inter[V] = 0;
+            comp.push_back({cur->x[V], cur->y[V]});
+          } while (!(cur->enex[V] == st) && !(side == 0 && V == I));
+          if (!(side == 0 && V == I)) {
+            if (cur->nbr[V] < 0) { status = 3; out.clear(); return; }
+            V = cur->nbr[V];
+            side = 1 - side;
+            R[side].inter[V] = 0;
+          }
+        } while (!(side == 0 && V == I));
+        out.push_back(comp);
+        do { I = RP.next[I]; } while (!isStart(I) && I != V0);
+        have = (I != V0);
+      }
+    }
+    cleanUp(out, epsClean);
   }
 };
 
@@ -975,6 +1395,26 @@ void orc_result_copy(int32_t* status, int32_t* ncomp, int64_t* count1, int64_t* 
   if (nrec) std::copy(g_store.nrec.begin(), g_store.nrec.end(), nrec);
   if (compSize) std::copy(g_store.compSize.begin(), g_store.compSize.end(), compSize);
   if (xy) std::copy(g_store.xy.begin(), g_store.xy.end(), xy);
+}
+
+// Multi-component pair: P and Q as interleaved open rings, ring k of sizes[k] vertices,
+// P clipped against Q as given.  flags as orc_clip_pair.  Returns the status.
+int orc_clip_multi(const double* P, const int32_t* sizesP, int kP, const double* Q, const int32_t* sizesQ, int kQ,
+                   double eps, double epsClean, int flags) {
+  g_store.clear();
+  MultiClipper c;
+  c.eps = eps; c.epsClean = epsClean; c.uni = flags & 1; c.filters = (flags >> 1) & 1;
+  c.exact = (flags >> 2) & 1;
+  c.run(P, sizesP, kP, Q, sizesQ, kQ);
+  g_store.status.push_back(c.status);
+  g_store.ncomp.push_back((int32_t)c.out.size());
+  g_store.count1.push_back(c.count1P);
+  g_store.nrec.push_back(c.nrec);
+  for (auto& comp : c.out) {
+    g_store.compSize.push_back((int32_t)comp.size());
+    for (auto& p : comp) { g_store.xy.push_back(p.x); g_store.xy.push_back(p.y); }
+  }
+  return c.status;
 }
 
 static Clipper::Export g_export;

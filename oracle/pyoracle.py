@@ -47,6 +47,8 @@ def lib():
         L.orc_result_copy.restype = None
         L.orc_exact_signs.argtypes = [vp, i64, i32, vp]
         L.orc_exact_signs.restype = None
+        L.orc_clip_multi.argtypes = [vp, vp, i32, vp, vp, i32, d, d, i32]
+        L.orc_clip_multi.restype = i32
         L.orc_pair_intersections.argtypes = [vp, i32, vp, i32, d, i32, vp]
         L.orc_pair_intersections.restype = i32
         L.orc_pair_intersections_copy.argtypes = [vp] * 8
@@ -116,6 +118,18 @@ def clip_pair(P, Q, eps=1e-7, eps_clean=None, union=False, gpu_semantics=True, e
     flags = _flags(union, gpu_semantics, exact)
     lib().orc_clip_pair(_p(P), len(P) // 2, _p(Q), len(Q) // 2, eps,
                         eps if eps_clean is None else eps_clean, flags)
+    return _collect()
+
+
+def clip_multi(P_rings, Q_rings, eps=1e-7, eps_clean=None, union=False, gpu_semantics=True, exact=False):
+    """Clip a pair of multi-component polygons (lists of open rings; holes by even-odd)."""
+    P = np.ascontiguousarray(np.concatenate([np.asarray(r, np.float64).reshape(-1) for r in P_rings]))
+    Q = np.ascontiguousarray(np.concatenate([np.asarray(r, np.float64).reshape(-1) for r in Q_rings]))
+    sp = np.array([len(np.asarray(r).reshape(-1)) // 2 for r in P_rings], np.int32)
+    sq = np.array([len(np.asarray(r).reshape(-1)) // 2 for r in Q_rings], np.int32)
+    flags = _flags(union, gpu_semantics, exact)
+    lib().orc_clip_multi(_p(P), _p(sp), len(sp), _p(Q), _p(sq), len(sq), eps,
+                         eps if eps_clean is None else eps_clean, flags)
     return _collect()
 
 
@@ -199,6 +213,26 @@ def ref_clip_pairs(pairs, union=False):
         fout = os.path.join(td, "out.bin")
         write_pair_batch(fin, pairs)
         cmd = [REF_BIN, "batch", fin, fout] + (["union"] if union else [])
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+        return read_result_batch(fout)
+
+
+def ref_clip_multi(pairs, union=False):
+    """The reference's own sequential clipper on multi-component pairs: pairs is a list of
+    (P rings, Q rings), each a list of open rings."""
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        fout = os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(struct.pack("<q", len(pairs)))
+            for Ps, Qs in pairs:
+                for rings in (Ps, Qs):
+                    f.write(struct.pack("<i", len(rings)))
+                    f.write(np.array([len(np.asarray(r).reshape(-1, 2)) for r in rings], np.int32).tobytes())
+                for rings in (Ps, Qs):
+                    for r in rings:
+                        f.write(np.ascontiguousarray(r, np.float64).reshape(-1).tobytes())
+        cmd = [REF_BIN, "mbatch", fin, fout] + (["union"] if union else [])
         subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
         return read_result_batch(fout)
 

@@ -24,6 +24,7 @@
 //   ghclip_ref batch in.bin out.bin [union]          (binary pair batch, see readBatch)
 //   ghclip_ref time  in.bin reps [union]             (times the batch, prints seconds)
 //   ghclip_ref rings in.bin out.bin                  (merged lists + step-1 labels, see below)
+//   ghclip_ref mbatch in.bin out.bin [union]         (multi-component pairs, see below)
 
 #include <iostream>
 #include <fstream>
@@ -155,6 +156,49 @@ int main(int argc, char** argv) {
       }
       resetGlobals();
     }
+    fclose(f);
+    return 0;
+  }
+  if (mode == "mbatch") {
+    // multi-component pairs: int64 npairs; per pair: int32 kP, int32 sizes[kP], int32 kQ,
+    // int32 sizes[kQ], then f64 coordinates of P's rings and of Q's rings (open rings).
+    // Output as "batch".
+    UNION = (argc > 4 && std::string(argv[4]) == "union");
+    FILE* fi = fopen(argv[2], "rb");
+    FILE* f = fopen(argv[3], "wb");
+    if (!fi || !f) { perror("mbatch"); return 2; }
+    int64_t n = 0;
+    if (fread(&n, 8, 1, fi) != 1) return 2;
+    fwrite(&n, 8, 1, f);
+    for (int64_t k = 0; k < n; ++k) {
+      std::vector<int32_t> sz[2];
+      for (int side = 0; side < 2; ++side) {
+        int32_t kk = 0;
+        if (fread(&kk, 4, 1, fi) != 1) return 2;
+        sz[side].resize(kk);
+        if (kk > 0 && fread(sz[side].data(), 4, kk, fi) != (size_t)kk) return 2;
+      }
+      for (int side = 0; side < 2; ++side)
+        for (int32_t m : sz[side]) {
+          std::vector<double> xy(2 * (size_t)m);
+          if (fread(xy.data(), 8, xy.size(), fi) != xy.size()) return 2;
+          (side == 0 ? pPolygon : qPolygon).push_back(makePolygon(xy.data(), m));
+        }
+      runClip();
+      int32_t nc = 0;
+      for (polygon& R : resultPolygon) if (R.root != NULL) ++nc;
+      fwrite(&nc, 4, 1, f);
+      for (polygon& R : resultPolygon) {
+        if (R.root == NULL) continue;
+        std::vector<double> xy;
+        for (vertex* V : R.vertices(ALL)) { xy.push_back(V->p.x); xy.push_back(V->p.y); }
+        int32_t nv = (int32_t)(xy.size() / 2);
+        fwrite(&nv, 4, 1, f);
+        fwrite(xy.data(), 8, xy.size(), f);
+      }
+      resetGlobals();
+    }
+    fclose(fi);
     fclose(f);
     return 0;
   }

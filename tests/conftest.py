@@ -78,3 +78,33 @@ def unpack_pairs(path):
             oc += 1
         results.append(comps)
     return pairs, results
+
+
+def unpack_multi(path):
+    """(pairs, intersection results, union results) of a multi-component fixture made by
+    tests/golden/make_multi_goldens.py; a pair is (P rings, Q rings)."""
+    d = np.load(path)
+    pairs, res = [], {"i_": [], "u_": []}
+    si = so = 0
+    for k in range(len(d["kP"])):
+        sides = []
+        for cnt in (d["kP"][k], d["kQ"][k]):
+            rings = []
+            for _ in range(cnt):
+                m = int(d["sizes"][si])
+                rings.append(d["xy"][2 * so:2 * (so + m)].reshape(-1, 2))
+                si += 1
+                so += m
+            sides.append(rings)
+        pairs.append(tuple(sides))
+    for tag in res:
+        oc = ov = 0
+        for k in range(len(d["kP"])):
+            comps = []
+            for _ in range(int(d[tag + "ncomp"][k])):
+                m = int(d[tag + "comp_size"][oc])
+                comps.append(d[tag + "xy"][2 * ov:2 * (ov + m)].reshape(-1, 2))
+                oc += 1
+                ov += m
+            res[tag].append(comps)
+    return pairs, res["i_"], res["u_"]

@@ -186,3 +186,39 @@ def test_pair_intersections_invalid_and_disjoint():
     r = pyoracle.pair_intersections(P * 1e-3, Q * 1e-3)
     assert r["invalid"] == 1 and r["status"] == 1
     assert "xy_p" not in r and r["n_p"] >= len(P) and r["n_q"] >= len(Q)
+
+
+@pytest.mark.parametrize("name", ["Fig18", "Fig19"])
+@pytest.mark.parametrize("gpu_semantics", [False, True])
+def test_multi_component_figs_byte_identical(name, gpu_semantics):
+    """Fig18 (6 x 10 rings, holes) and Fig19 (5 rings): every component of both inputs,
+    against the reference's own clipper run here."""
+    P = load_poly(_fig(name, "P.poly"))
+    Q = load_poly(_fig(name, "Q.poly"))
+    assert len(P) > 1
+    r = pyoracle.clip_multi(P, Q, gpu_semantics=gpu_semantics)
+    assert r.status[0] == 0
+    assert format_reference(r.components(0)) == open(_fig(name, "R.run.poly")).read()
+
+
+@pytest.mark.parametrize("union", [False, True])
+def test_multi_component_matches_reference_clipper(union):
+    from conftest import unpack_multi
+    pairs, inter, uni = unpack_multi(os.path.join(GOLDEN, "holed_pairs.npz"))
+    assert len(pairs) == 150 and sum(len(p) for p, _ in pairs) > 300
+    for (P, Q), exp in zip(pairs, uni if union else inter):
+        for gs in (False, True):
+            r = pyoracle.clip_multi(P, Q, union=union, gpu_semantics=gs)
+            assert r.status[0] == 0
+            assert same_components(r.components(0), exp)
+
+
+def test_multi_component_single_rings_equal_single_pair():
+    """One ring per side: the multi-component clipper gives what the single-pair one does."""
+    pairs, expect = unpack_pairs(os.path.join(GOLDEN, "random_pairs.npz"))
+    for (P, Q), _ in list(zip(pairs, expect))[:150]:
+        a = pyoracle.clip_pair(P, Q)
+        b = pyoracle.clip_multi([P], [Q])
+        assert a.status[0] == b.status[0]
+        if a.status[0] == 0:
+            assert same_components(a.components(0), b.components(0))
