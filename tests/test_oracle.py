@@ -9,9 +9,9 @@ import pyoracle
 from conftest import GOLDEN, format_reference, load_poly, same_components, unpack_pairs
 from gcmfgh import synth
 
-# Fig18 has several components per input (a polygon with holes); the join-and-clip path
-# clips single-component layer polygons (GH-CUDA/ghcuda.cpp:64-91 takes one polygon per
-# side), so it is not among the single-pair golden cases.
+# Single-pair cases take the first component of each input, as the join-and-clip path
+# does (GH-CUDA/ghcuda.cpp:64-91 takes one polygon per side).  Fig18 (holes) and all of
+# Fig19's components are the multi-component cases further down.
 FIGS = ["Fig1", "Fig8", "Fig14", "Fig14cw", "Fig15", "Fig16", "Fig17", "Fig19"]
 
 
