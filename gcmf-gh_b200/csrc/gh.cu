@@ -127,17 +127,27 @@ edge_filter_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, int32_t* __re
     int64_t pos = 0;
     int32_t* list = nullptr;
     if (kMode == 1) { pos = side == 0 ? offP[w] : offQ[w]; list = side == 0 ? LP : LQ; }
-    for (int k0 = 0; k0 < n; k0 += W) {
-      int k = k0 + tl;
-      bool hit = false;
-      if (k < n) {
-        double2 a = __ldg(v + k), b = __ldg(v + (k + 1 < n ? k + 1 : 0));
-        hit = edge_touches_box(a.x, a.y, b.x, b.y, c.x, c.y, c.z, c.w);
+    // whole warps take kUnroll groups of W edges per step: every group's loads are issued
+    // before the first ballot
+    constexpr int kUnroll = (W == 32) ? 4 : 1;
+    for (int k0 = 0; k0 < n; k0 += W * kUnroll) {
+      bool hit[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int k = k0 + u * W + tl;
+        hit[u] = false;
+        if (k < n) {
+          double2 a = __ldg(v + k), b = __ldg(v + (k + 1 < n ? k + 1 : 0));
+          hit[u] = edge_touches_box(a.x, a.y, b.x, b.y, c.x, c.y, c.z, c.w);
+        }
       }
-      unsigned m = __ballot_sync(tmask, hit);
-      if (W != 32) m = (m >> tbase) & kBits;
-      if (kMode == 1 && hit) list[pos + cnt + __popc(m & ((1u << tl) - 1u))] = k;
-      cnt += __popc(m);
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        unsigned m = __ballot_sync(tmask, hit[u]);
+        if (W != 32) m = (m >> tbase) & kBits;
+        if (kMode == 1 && hit[u]) list[pos + cnt + __popc(m & ((1u << tl) - 1u))] = k0 + u * W + tl;
+        cnt += __popc(m);
+      }
     }
     if (kMode == 0 && tl == 0) { if (side == 0) cP[w] = cnt; else cQ[w] = cnt; }
   }
@@ -189,8 +199,11 @@ struct Records {
   int32_t* k;       // pair
 };
 
+// Occupancy over registers: the count pass at most 80 registers (3 blocks per SM; count
+// stage 1.29 -> 1.07 ms), the emit pass 64 (4 blocks; 0.55 -> 0.45 ms).  The
+// exact-predicate instances keep 128 registers (their expansions would spill).
 template <int kMode, int kExact>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kExact ? 2 : (kMode == 1 ? 4 : 3))
 intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* __restrict__ chunkOff,
                  int64_t nChunks, const int32_t* __restrict__ cP, const int32_t* __restrict__ cQ,
                  const int64_t* __restrict__ offP, const int64_t* __restrict__ offQ,
@@ -534,8 +547,10 @@ __device__ __forceinline__ bool edge_fill_info(const LayerDev& Lb, const LayerDe
   return true;
 }
 
+// At most 64 registers (4 blocks per SM): the kernel is latency-bound and the extra
+// occupancy outweighs a few spilled values (measured 1.35 -> 1.03 ms for the fill stage).
 template <int kSide>
-__global__ void ring_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R,
+__global__ void __launch_bounds__(kThreads, 4) ring_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, Records R,
                                  const int64_t* __restrict__ eoff, int64_t nE, const int32_t* __restrict__ edgePair,
                                  const int64_t* __restrict__ vpos, const int64_t* __restrict__ regOff,
                                  const int32_t* __restrict__ m, RingSet S, int64_t* __restrict__ slotOfRec,
@@ -1350,6 +1365,24 @@ struct TileGroup {
     return v;
   }
 };
+
+// One thread per pair: every collective is the identity, nothing synchronises.
+struct SoloGroup {
+  static constexpr bool kBlock = false;
+  __device__ __forceinline__ int rank() const { return 0; }
+  __device__ __forceinline__ int size() const { return 1; }
+  __device__ __forceinline__ void sync() const {}
+  __device__ __forceinline__ bool all(bool v) const { return v; }
+  __device__ __forceinline__ bool any(bool v) const { return v; }
+  __device__ __forceinline__ int sum(int v) const { return v; }
+  template <class T>
+  __device__ __forceinline__ T bcast0(T v) const { return v; }
+  __device__ __forceinline__ int first(bool hit) const { return hit ? 0 : -1; }
+  __device__ __forceinline__ int incl_scan(int v, int& total) const { total = v; return v; }
+};
+
+template <int W> struct TileOf { using type = TileGroup<W>; };
+template <> struct TileOf<1> { using type = SoloGroup; };
 
 // Block-wide versions over shared scratch (kBlockLabelThreads / 32 warps); each call
 // begins with a barrier so the scratch of the previous call is free.
@@ -2219,9 +2252,13 @@ __device__ void label_trace_pair(const G& g, const LabelArgs& a, int64_t k) {
   grp_cleanup(g, c, outNC, outNV);
 }
 
-// A warp per pair for pairs whose merged rings have at most midLabelMin slots.
+// A warp per pair for pairs whose merged rings have at most midLabelMin slots.  Launch
+// bounds of 6 blocks (at most 80 registers) and, for the one-thread tiles below, 12 blocks
+// (40 registers): both kernels wait on dependent loads, and the occupancy pays for the
+// spills (label stage 2.59 -> 2.15 ms from the tile kernel, -0.07 ms from this one).  The
+// exact-predicate instances keep 4 blocks: their expansion arithmetic would spill.
 template <int EX>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, EX ? 4 : 6)
 label_trace_kernel(LabelArgs a) {
   int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (k >= a.K) return;
@@ -2234,17 +2271,18 @@ label_trace_kernel(LabelArgs a) {
 }
 
 // Pairs whose merged rings have at most tileLabelMax slots: a tile of kTileLanes lanes per
-// pair, 32 / kTileLanes consecutive pairs per warp.
-constexpr int kTileLanes = 2;
+// pair, 32 / kTileLanes consecutive pairs per warp (one lane: SoloGroup, measured slightly
+// faster than 2-lane tiles on the batched workload).
+constexpr int kTileLanes = 1;
 template <int EX>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, EX ? 4 : 12)
 label_trace_tile_kernel(LabelArgs a) {
   const int64_t k = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / kTileLanes) +
                     (lane_id() / kTileLanes);
   if (k >= a.K || a.D.status[k] != 0) return;
   const int64_t slots = (int64_t)a.mP[k] + a.mQ[k];
   if (slots > a.tileLabelMax || slots > a.midLabelMin) return;
-  TileGroup<kTileLanes> g;
+  typename TileOf<kTileLanes>::type g;
   label_trace_pair<EX>(g, a, k);
 }
 

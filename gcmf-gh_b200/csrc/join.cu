@@ -317,7 +317,7 @@ __device__ __forceinline__ bool segment_hit(double bX1, double bY1, double bX2, 
 }
 
 template <int W>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)   // 64 registers: occupancy for a latency-bound loop
 refine_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32_t* __restrict__ po,
               int64_t K, const int8_t* __restrict__ join_flag,
               const int32_t* __restrict__ bE, const int32_t* __restrict__ oE,

@@ -136,7 +136,7 @@ const char* gcmfgh_status_string(gcmfgh_status s);
 #define GCMFGH_TUNE_BIG_LABEL 1
 #define GCMFGH_TUNE_MID_LABEL 2
 /* GCMFGH_TUNE_TILE_LABEL: a pair whose merged rings have at most this many vertices is
- * labelled and traced by a tile of 2 lanes, 16 pairs per warp (default 96; 0: never) */
+ * labelled and traced by one thread, 32 pairs per warp (default 96; 0: never) */
 #define GCMFGH_TUNE_TILE_LABEL 3
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* ctx, int key, int64_t value);
 /* device error word of the last call (0 none, 1 capacity, 2 trace budget, 4 wait limit) */
