@@ -102,7 +102,7 @@ __global__ void setup_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict
 // tiles for small pairs (they also zero the counts of pairs with nothing to test), whole
 // warps for the rest.
 template <int kMode, int W>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 6)
 edge_filter_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, int32_t* __restrict__ cP,
                    int32_t* __restrict__ cQ, const int64_t* __restrict__ offP,
                    const int64_t* __restrict__ offQ, int32_t* __restrict__ LP, int32_t* __restrict__ LQ,
@@ -2253,9 +2253,9 @@ __device__ void label_trace_pair(const G& g, const LabelArgs& a, int64_t k) {
 }
 
 // A warp per pair for pairs whose merged rings have at most midLabelMin slots.  Launch
-// bounds of 6 blocks (at most 80 registers) and, for the one-thread tiles below, 12 blocks
-// (40 registers): both kernels wait on dependent loads, and the occupancy pays for the
-// spills (label stage 2.59 -> 2.15 ms from the tile kernel, -0.07 ms from this one).  The
+// bounds of 6 blocks (at most 80 registers) and, for the one-thread tiles below, 16 blocks
+// (32 registers): both kernels wait on dependent loads, and the occupancy pays for the
+// spills (label stage 2.59 -> 2.11 ms from the tile kernel, -0.07 ms from this one).  The
 // exact-predicate instances keep 4 blocks: their expansion arithmetic would spill.
 template <int EX>
 __global__ void __launch_bounds__(128, EX ? 4 : 6)
@@ -2275,7 +2275,7 @@ label_trace_kernel(LabelArgs a) {
 // faster than 2-lane tiles on the batched workload).
 constexpr int kTileLanes = 1;
 template <int EX>
-__global__ void __launch_bounds__(128, EX ? 4 : 12)
+__global__ void __launch_bounds__(128, EX ? 4 : 16)
 label_trace_tile_kernel(LabelArgs a) {
   const int64_t k = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / kTileLanes) +
                     (lane_id() / kTileLanes);
@@ -2289,7 +2289,7 @@ label_trace_tile_kernel(LabelArgs a) {
 // Pairs with midLabelMin < slots <= bigLabelMin: persistent blocks take pairs from the
 // list through an atomic cursor (work stealing), one block of kBlockLabelThreads per pair.
 template <int EX>
-__global__ void __launch_bounds__(kBlockLabelThreads)
+__global__ void __launch_bounds__(kBlockLabelThreads, EX ? 1 : 3)
 label_trace_block_kernel(LabelArgs a) {
   __shared__ long long sm[kBlockLabelThreads / 32 + 1];
   __shared__ long long next;
@@ -3102,7 +3102,7 @@ __global__ void out_sizes_kernel(const int32_t* __restrict__ mP, const int32_t* 
   ccap[k] = mP[k] + 2 * nrec[k] + 8;
 }
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 8)   // 32 registers: compact 0.33 -> 0.20 ms
 out_compact_kernel(int64_t K, const double* __restrict__ xy, const int64_t* __restrict__ vOff,
                    const int32_t* __restrict__ csz, const int64_t* __restrict__ cOff,
                    const int32_t* __restrict__ nc, const int64_t* __restrict__ nv,
