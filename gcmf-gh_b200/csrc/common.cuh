@@ -86,6 +86,57 @@ GCMFGH_DEV int classify_edges(double p1x, double p1y, double p2x, double p2y,
   return 0;
 }
 
+// Both sides' classification of one edge pair in one pass: the P-side type of
+// classify_edges(P1,P2,Q1,Q2) (returned, with alpha and beta) and whether the Q side's
+// own call classify_edges(Q1,Q2,P1,P2) finds an intersection (*qhit), the check behind the
+// reference's invalid-pair test (gppolyclip_mDIV512.cu:1461).  The Q-side call evaluates
+// the same four areas with the same operands (its AP1, AP2 are AQ1, AQ2 here and the other
+// way round) and the same two quotients with alpha and beta swapped, so they are computed
+// once; only its collinear branch, which is rare, runs separately.  Bit-identical to the
+// two calls.
+GCMFGH_DEV int classify_edges_both(double p1x, double p1y, double p2x, double p2y,
+                                   double q1x, double q1y, double q2x, double q2y,
+                                   double eps, double& alpha, double& beta, bool& qhit) {
+  const double AP1 = area2(p1x, p1y, q1x, q1y, q2x, q2y);
+  const double AP2 = area2(p2x, p2y, q1x, q1y, q2x, q2y);
+  const double AQ1 = area2(q1x, q1y, p1x, p1y, p2x, p2y);
+  const double AQ2 = area2(q2x, q2y, p1x, p1y, p2x, p2y);
+  const bool pCross = fabs(AP1 - AP2) > eps, qCross = fabs(AQ1 - AQ2) > eps;
+  double qa = 0.0, qb = 0.0;
+  if (pCross || qCross) {
+    qa = AP1 / (AP1 - AP2);
+    qb = AQ1 / (AQ1 - AQ2);
+  }
+  auto crossing_type = [eps](double a, double b) {
+    const bool a01 = (a > eps && a < 1.0 - eps);
+    const bool a0 = !a01 && fabs(a) <= eps;
+    const bool b01 = (b > eps && b < 1.0 - eps);
+    const bool b0 = !b01 && fabs(b) <= eps;
+    if (a01 && b01) return 1;
+    if (a0 && b01) return 2;
+    if (b0 && a01) return 3;
+    if (a0 && b0) return 4;
+    return 0;
+  };
+  int tp = 0;
+  if (pCross) {
+    alpha = qa;
+    beta = qb;
+    tp = crossing_type(qa, qb);
+  } else if (fabs(AP1) < eps) {
+    tp = classify_edges(p1x, p1y, p2x, p2y, q1x, q1y, q2x, q2y, eps, alpha, beta);
+  }
+  if (qCross) {
+    qhit = crossing_type(qb, qa) != 0;
+  } else if (fabs(AQ1) < eps) {
+    double a2, b2;
+    qhit = classify_edges(q1x, q1y, q2x, q2y, p1x, p1y, p2x, p2y, eps, a2, b2) != 0;
+  } else {
+    qhit = false;
+  }
+  return tp;
+}
+
 // ---- exact-predicate mode
 //
 // Signs of u.v-type expressions  (a1 - a0) * (b1 - b0) -/+ (c1 - c0) * (d1 - d0)  over

@@ -242,10 +242,16 @@ intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* 
       double2 P1 = __ldg(pv + pe), P2 = __ldg(pv + (pe + 1 < np_ ? pe + 1 : 0));
       double2 Q1 = __ldg(qv + qe), Q2 = __ldg(qv + (qe + 1 < nq_ ? qe + 1 : 0));
       if (edge_boxes_touch(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y)) {
-        tp = classify_mode(kExact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
-        if (kMode == 0) {
-          double a2, b2;
-          tq = classify_mode(kExact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2);
+        if (kMode == 0 && !kExact) {
+          bool qhit;
+          tp = classify_edges_both(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta, qhit);
+          tq = qhit ? 1 : 0;
+        } else {
+          tp = classify_mode(kExact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
+          if (kMode == 0) {
+            double a2, b2;
+            tq = classify_mode(kExact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2);
+          }
         }
       }
     }
