@@ -361,6 +361,7 @@ gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* c, int key, int64_t value) {
   else if (key == GCMFGH_TUNE_BIG_LABEL) c->prm.big_label_min = value;
   else if (key == GCMFGH_TUNE_MID_LABEL) c->prm.mid_label_min = value;
   else if (key == GCMFGH_TUNE_TILE_LABEL) c->prm.tile_label_max = value;
+  else if (key == GCMFGH_TUNE_WIDE_LABEL) c->prm.wide_label_min = value;
   else return GCMFGH_INVALID_ARGUMENT;
   return GCMFGH_OK;
 }

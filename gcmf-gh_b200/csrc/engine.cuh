@@ -76,7 +76,9 @@ struct ClipParams {
   int no_swap = 0;            // 1: clip base as P even when it has fewer vertices
   int exact = 0;              // 1: exact orientation/classification signs (eps unused there)
   int64_t bin_grid = 1ll << 24;        // edge-pair grid above which a pair's edges are binned
-  int64_t tile_label_max = 96;         // merged-ring slots up to which a tile of 2 lanes labels a pair
+  int64_t tile_label_max = 96;         // merged-ring slots up to which one thread labels a pair
+  int64_t wide_label_min = 1 << 16;    // clip batches of at least this many pairs use the
+                                       // high-occupancy labelling kernels
   int64_t mid_label_min = 1ll << 10;   // merged-ring slots above which a block labels a pair
   int64_t big_label_min = 1ll << 18;   // merged-ring slots above which a pair is labelled grid-wide
 };

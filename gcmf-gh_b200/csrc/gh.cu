@@ -2258,13 +2258,15 @@ __device__ void label_trace_pair(const G& g, const LabelArgs& a, int64_t k) {
   grp_cleanup(g, c, outNC, outNV);
 }
 
-// A warp per pair for pairs whose merged rings have at most midLabelMin slots.  Launch
-// bounds of 6 blocks (at most 80 registers) and, for the one-thread tiles below, 16 blocks
-// (32 registers): both kernels wait on dependent loads, and the occupancy pays for the
-// spills (label stage 2.59 -> 2.11 ms from the tile kernel, -0.07 ms from this one).  The
-// exact-predicate instances keep 4 blocks: their expansion arithmetic would spill.
-template <int EX>
-__global__ void __launch_bounds__(128, EX ? 4 : 6)
+// Two register budgets for the warp and one-thread kernels.  kWide (batches of at least
+// ClipParams::wide_label_min pairs): 6 blocks of 128 (at most 80 registers) here and 16 blocks (32
+// registers) for the tiles below -- both kernels wait on dependent loads, and on a full
+// GPU the occupancy pays for the spills (label stage 2.59 -> 2.11 ms from the tile kernel,
+// -0.07 ms from this one).  Small batches (serving) leave most SMs idle, so there the
+// kernels keep 4 blocks and spill nothing.  Exact-predicate instances always keep 4
+// blocks: their expansion arithmetic would spill.
+template <int EX, int kWide>
+__global__ void __launch_bounds__(128, (kWide && !EX) ? 6 : 4)
 label_trace_kernel(LabelArgs a) {
   int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (k >= a.K) return;
@@ -2280,8 +2282,8 @@ label_trace_kernel(LabelArgs a) {
 // pair, 32 / kTileLanes consecutive pairs per warp (one lane: SoloGroup, measured slightly
 // faster than 2-lane tiles on the batched workload).
 constexpr int kTileLanes = 1;
-template <int EX>
-__global__ void __launch_bounds__(128, EX ? 4 : 16)
+template <int EX, int kWide>
+__global__ void __launch_bounds__(128, (kWide && !EX) ? 16 : 4)
 label_trace_tile_kernel(LabelArgs a) {
   const int64_t k = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / kTileLanes) +
                     (lane_id() / kTileLanes);
@@ -2295,7 +2297,7 @@ label_trace_tile_kernel(LabelArgs a) {
 // Pairs with midLabelMin < slots <= bigLabelMin: persistent blocks take pairs from the
 // list through an atomic cursor (work stealing), one block of kBlockLabelThreads per pair.
 template <int EX>
-__global__ void __launch_bounds__(kBlockLabelThreads, EX ? 1 : 3)
+__global__ void __launch_bounds__(kBlockLabelThreads)
 label_trace_block_kernel(LabelArgs a) {
   __shared__ long long sm[kBlockLabelThreads / 32 + 1];
   __shared__ long long next;
@@ -3538,10 +3540,13 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     { mid_label_list_kernel<<<blocks_for(K), kThreads, 0, ls>>>(mP, mQ, D.status, K, la.midLabelMin, la.bigLabelMin,
                                                                mlist, mcnt); note_launch(); }
     { (prm.exact ? label_trace_block_kernel<1> : label_trace_block_kernel<0>)<<<2 * nsm, kBlockLabelThreads, 0, ls>>>(la); note_launch(); }
-    { (prm.exact ? label_trace_kernel<1> : label_trace_kernel<0>)<<<(unsigned)((K + 3) / 4), 128, 0, s>>>(la); note_launch(); }
+    const bool wide = K >= prm.wide_label_min;
+    { (prm.exact ? label_trace_kernel<1, 0>
+                 : (wide ? label_trace_kernel<0, 1> : label_trace_kernel<0, 0>))<<<(unsigned)((K + 3) / 4), 128, 0, s>>>(la); note_launch(); }
     if (prm.tile_label_max > 0) {
       const int64_t pairsPerBlock = 4 * (32 / kTileLanes);
-      { (prm.exact ? label_trace_tile_kernel<1> : label_trace_tile_kernel<0>)<<<(unsigned)((K + pairsPerBlock - 1) / pairsPerBlock), 128, 0, s>>>(la); note_launch(); }
+      { (prm.exact ? label_trace_tile_kernel<1, 0>
+                   : (wide ? label_trace_tile_kernel<0, 1> : label_trace_tile_kernel<0, 0>))<<<(unsigned)((K + pairsPerBlock - 1) / pairsPerBlock), 128, 0, s>>>(la); note_launch(); }
     }
     if (ls != s) {
       cudaEventRecord(join, ls);

@@ -225,7 +225,7 @@ class Engine:
     def last_device_error(self):
         return lib().gcmfgh_last_device_error(self.h)
 
-    def set_tuning(self, bin_grid=None, big_label=None, mid_label=None, tile_label=None):
+    def set_tuning(self, bin_grid=None, big_label=None, mid_label=None, tile_label=None, wide_label=None):
         """Work-distribution thresholds (results do not depend on them)."""
         if bin_grid is not None:
             _check(lib().gcmfgh_set_tuning(self.h, 0, int(bin_grid)))
@@ -235,6 +235,8 @@ class Engine:
             _check(lib().gcmfgh_set_tuning(self.h, 2, int(mid_label)))
         if tile_label is not None:
             _check(lib().gcmfgh_set_tuning(self.h, 3, int(tile_label)))
+        if wide_label is not None:
+            _check(lib().gcmfgh_set_tuning(self.h, 4, int(wide_label)))
 
     def set_timing(self, on=True):
         _check(lib().gcmfgh_set_timing(self.h, 1 if on else 0))

@@ -138,6 +138,10 @@ const char* gcmfgh_status_string(gcmfgh_status s);
 /* GCMFGH_TUNE_TILE_LABEL: a pair whose merged rings have at most this many vertices is
  * labelled and traced by one thread, 32 pairs per warp (default 96; 0: never) */
 #define GCMFGH_TUNE_TILE_LABEL 3
+/* GCMFGH_TUNE_WIDE_LABEL: clip batches of at least this many pairs are labelled by the
+ * kernels built for a full GPU (fewer registers, more resident warps); smaller batches
+ * by the ones built for per-pair latency (default 65536) */
+#define GCMFGH_TUNE_WIDE_LABEL 4
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* ctx, int key, int64_t value);
 /* device error word of the last call (0 none, 1 capacity, 2 trace budget, 4 wait limit) */
 int gcmfgh_last_device_error(gcmfgh_ctx* ctx);

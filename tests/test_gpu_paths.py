@@ -10,14 +10,15 @@ from gcmfgh import synth
 
 pytestmark = pytest.mark.gpu
 
-BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT, TILE_DEFAULT = 1 << 24, 1 << 18, 1 << 10, 96
+BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT, TILE_DEFAULT, WIDE_DEFAULT = 1 << 24, 1 << 18, 1 << 10, 96, 1 << 16
 
 
 def _run(engine, base, ovl, pid, qid, union=False, bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT,
-         mid_label=MID_DEFAULT, exact=False, tile_label=TILE_DEFAULT):
+         mid_label=MID_DEFAULT, exact=False, tile_label=TILE_DEFAULT, wide_label=WIDE_DEFAULT):
     import gcmfgh
     db, do = gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl)
-    engine.set_tuning(bin_grid=bin_grid, big_label=big_label, mid_label=mid_label, tile_label=tile_label)
+    engine.set_tuning(bin_grid=bin_grid, big_label=big_label, mid_label=mid_label, tile_label=tile_label,
+                      wide_label=wide_label)
     engine.set_params(1e-7, 1e-7, union)
     engine.set_precision(exact)
     try:
@@ -25,7 +26,7 @@ def _run(engine, base, ovl, pid, qid, union=False, bin_grid=BIN_DEFAULT, big_lab
         r = engine.clip_result()
     finally:
         engine.set_tuning(bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT, mid_label=MID_DEFAULT,
-                          tile_label=TILE_DEFAULT)
+                          tile_label=TILE_DEFAULT, wide_label=WIDE_DEFAULT)
         engine.set_params(1e-7, 1e-7, False)
         engine.set_precision(False)
     return info, r
@@ -72,19 +73,23 @@ def test_block_labelling_every_pair(engine, union, exact):
 @pytest.mark.parametrize("union", [False, True])
 @pytest.mark.parametrize("exact", [False, True])
 @pytest.mark.parametrize("tile_label", [0, 1 << 10])
-def test_tile_and_warp_labelling_every_pair(engine, union, exact, tile_label):
-    """Every warp-sized pair labelled by a tile of 2 lanes (tile_label 2^10), or by a whole
-    warp with tiles switched off (0)."""
+@pytest.mark.parametrize("wide_label", [0, WIDE_DEFAULT])
+def test_tile_and_warp_labelling_every_pair(engine, union, exact, tile_label, wide_label):
+    """Every warp-sized pair labelled by one thread (tile_label 2^10), or by a whole warp
+    with the one-thread path switched off (0); with the full-GPU register budget forced
+    (wide_label 0) and with the per-pair-latency one this batch size gets by default."""
     base, ovl, ids = _pairs_layers(synth.random_star_pairs(24, 1500, 3, 90, spread=0.8))
-    _, r = _run(engine, base, ovl, ids, ids, union=union, tile_label=tile_label, exact=exact)
+    _, r = _run(engine, base, ovl, ids, ids, union=union, tile_label=tile_label, exact=exact,
+                wide_label=wide_label)
     _assert_equal(r, pyoracle.clip_batch(base, ovl, ids, ids, union=union, exact=exact))
 
 
-def test_tile_labelling_degenerate_cases(engine):
+@pytest.mark.parametrize("wide_label", [0, WIDE_DEFAULT])
+def test_tile_labelling_degenerate_cases(engine, wide_label):
     from test_gpu_clip import degenerate_pairs
     base, ovl, ids = _pairs_layers(degenerate_pairs())
     for union in (False, True):
-        _, r = _run(engine, base, ovl, ids, ids, union=union, tile_label=1 << 10)
+        _, r = _run(engine, base, ovl, ids, ids, union=union, tile_label=1 << 10, wide_label=wide_label)
         _assert_equal(r, pyoracle.clip_batch(base, ovl, ids, ids, union=union))
 
 
