@@ -378,7 +378,7 @@ gcmfgh_status gcmf_join(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer
   c->marks[0].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   int st = run_join(to_dev(b), to_dev(o), c->join_arena, c->join, c->d_err, c->h_scratch, c->stream,
-                    &c->marks[0]);
+                    &c->marks[0], c->aux);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_join = true;

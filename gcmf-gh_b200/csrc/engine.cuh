@@ -115,12 +115,16 @@ struct Marks {
 
 int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s);
 
+// aux: optional second stream; the overlay layer's MBRs and sort run on it, beside the
+// base layer's on s.
 int run_join(const LayerDev& base, const LayerDev& ovl, Arena& arena, JoinDev& out,
-             int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);
+             int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
+             cudaStream_t aux = nullptr);
 
 int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys, int64_t K, int obits,
                    Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,
-                   int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr);
+                   int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
+                   cudaStream_t aux = nullptr);
 
 // Merged rings of pair 0 after the neighbour links, as the reference's
 // calculateIntersections hands them back (gppolyclip_mDIV512.cu:1298-1640): vertices in

@@ -3164,12 +3164,23 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
       !cP || !cQ || !offP || !offQ || !nchunk || !chunkOff || !eoffP || !eoffQ || !tot || !stK)
     return ST_OUT_OF_MEMORY;
   { setup_kernel<<<blocks_for(K), kThreads, 0, s>>>(Lb, Lo, d_pid, d_qid, K, mb, mo, D, C.swapped, prm.no_swap); note_launch(); }
+  // The narrow-tile and whole-warp passes of the edge filter take disjoint pairs (by size):
+  // with an auxiliary stream the warp pass runs beside the tile pass.
+  cudaEvent_t fev[2] = {nullptr, nullptr};
+  const bool two = aux && cudaEventCreateWithFlags(&fev[0], cudaEventDisableTiming) == cudaSuccess &&
+                   cudaEventCreateWithFlags(&fev[1], cudaEventDisableTiming) == cudaSuccess;
+  struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 2; ++i) if (e[i]) cudaEventDestroy(e[i]); } } fguard{fev};
+  cudaStream_t sw = two ? aux : s;
+  auto fork_aux = [&]() { if (two) { cudaEventRecord(fev[0], s); cudaStreamWaitEvent(aux, fev[0], 0); } };
+  auto join_aux = [&]() { if (two) { cudaEventRecord(fev[1], aux); cudaStreamWaitEvent(s, fev[1], 0); } };
   // ---- G1 edge filter
+  fork_aux();
   { edge_filter_kernel<0, kFilterTile><<<(unsigned)((K * kFilterTile + kThreads - 1) / kThreads), kThreads, 0, s>>>(
         Lb, Lo, D, K, cP, cQ, nullptr, nullptr, nullptr, nullptr, -1, kFilterTileMax); note_launch(); }
-  { edge_filter_kernel<0, 32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, nullptr, nullptr,
-                                                                      nullptr, nullptr, kFilterTileMax,
-                                                                      INT64_MAX); note_launch(); }
+  { edge_filter_kernel<0, 32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, D, K, cP, cQ, nullptr, nullptr,
+                                                                       nullptr, nullptr, kFilterTileMax,
+                                                                       INT64_MAX); note_launch(); }
+  join_aux();
   exclusive_scan_i32(cP, offP, K, tot + 0, stK, d_err, s);
   exclusive_scan_i32(cQ, offQ, K, tot + 1, stK, d_err, s);
   exclusive_scan_i32(D.nP, eoffP, K, tot + 2, stK, d_err, s);
@@ -3201,10 +3212,12 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (nCh > 0) { chunk_pair_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(chunkOff, nchunk, K, chunkPair); note_launch(); }
   cudaMemsetAsync(binRec, 0, K * sizeof(int64_t), s);
   cudaMemsetAsync(binQ, 0, K * sizeof(int64_t), s);
+  fork_aux();
   { edge_filter_kernel<1, kFilterTile><<<(unsigned)((K * kFilterTile + kThreads - 1) / kThreads), kThreads, 0, s>>>(
         Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ, -1, kFilterTileMax); note_launch(); }
-  { edge_filter_kernel<1, 32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ,
-                                                                      kFilterTileMax, INT64_MAX); note_launch(); }
+  { edge_filter_kernel<1, 32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ,
+                                                                       kFilterTileMax, INT64_MAX); note_launch(); }
+  join_aux();
   // ---- G2 count: chunked pairs
   Records R{};
   if (nCh > 0) {
@@ -3400,43 +3413,63 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (!take_ring(regTotP, SP) || !take_ring(regTotQ, SQ)) return ST_OUT_OF_MEMORY;
   SP.exact = SQ.exact = prm.exact;
   mk->mark("clip:layout", s);
-  // ---- G5 ring fill (light edges per thread, heavy edges per block)
+  // ---- G5 ring fill (light edges per thread, heavy edges per block).  The P and Q rings
+  // are independent, and each side's latency-bound fill leaves room on the GPU for the
+  // other, so the Q side runs on the auxiliary stream when there is one.
   {
-    int64_t* heavy = A.take_n<int64_t>(std::max(nEP, nEQ));
-    unsigned long long* nHeavy = A.take_n<unsigned long long>(2);
-    const int64_t nIns = std::max(nInsP, nInsQ);
-    uint64_t* gkey = A.take_n<uint64_t>(2 * nIns);
-    uint32_t* gtie = A.take_n<uint32_t>(2 * nIns);
-    uint32_t* gidx = A.take_n<uint32_t>(2 * nIns);
-    if (!heavy || !nHeavy || !gkey || !gtie || !gidx) return ST_OUT_OF_MEMORY;
     const size_t smem = (size_t)kHeavySmem * (sizeof(uint64_t) + 2 * sizeof(uint32_t));
     cudaFuncSetAttribute(heavy_fill_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(heavy_fill_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    // edge -> pair tables for the fill kernels
-    int32_t* edgeP = A.take_n<int32_t>(nEP);
-    int32_t* edgeQ = A.take_n<int32_t>(nEQ);
-    if (!edgeP || !edgeQ) return ST_OUT_OF_MEMORY;
-    { range_owner_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(eoffP, D.nP, K, edgeP); note_launch(); }
-    { range_owner_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(eoffQ, D.nQ, K, edgeQ); note_launch(); }
-    if (nEP > 0) {
-      cudaMemsetAsync(nHeavy, 0, sizeof(unsigned long long), s);
-      { ring_fill_kernel<0><<<blocks_for(nEP), kThreads, 0, s>>>(Lb, Lo, D, R, eoffP, nEP, edgeP, vposP, regP, mP, SP,
-                                                               slotP, insBaseP, curP, insListP, heavy, nHeavy); note_launch(); }
-      { heavy_fill_kernel<0><<<2 * nsm, kHeavyThreads, smem, s>>>(Lb, Lo, D, R, eoffP, edgeP, vposP, regP, mP, SP, slotP,
-                                                                  insBaseP, curP, insListP, heavy, nHeavy, gkey, gtie,
-                                                                  gidx); note_launch(); }
+    unsigned long long* nHeavy = A.take_n<unsigned long long>(2);
+    if (!nHeavy) return ST_OUT_OF_MEMORY;
+    cudaMemsetAsync(nHeavy, 0, 2 * sizeof(unsigned long long), s);
+    cudaStream_t sq = s;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    if (aux && cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) == cudaSuccess &&
+        cudaEventCreateWithFlags(&join, cudaEventDisableTiming) == cudaSuccess) {
+      cudaEventRecord(fork, s);
+      cudaStreamWaitEvent(aux, fork, 0);
+      sq = aux;
     }
-    if (nEQ > 0) {
-      cudaMemsetAsync(nHeavy + 1, 0, sizeof(unsigned long long), s);
-      { ring_fill_kernel<1><<<blocks_for(nEQ), kThreads, 0, s>>>(Lb, Lo, D, R, eoffQ, nEQ, edgeQ, vposQ, regQ, mQ, SQ,
-                                                               slotQ, insBaseQ, curQ, insListQ, heavy, nHeavy + 1); note_launch(); }
-      { heavy_fill_kernel<1><<<2 * nsm, kHeavyThreads, smem, s>>>(Lb, Lo, D, R, eoffQ, edgeQ, vposQ, regQ, mQ, SQ, slotQ,
-                                                                  insBaseQ, curQ, insListQ, heavy, nHeavy + 1, gkey, gtie,
-                                                                  gidx); note_launch(); }
+    int st = ST_OK;
+    for (int side = 0; side < 2 && st == ST_OK; ++side) {
+      cudaStream_t ss = side == 0 ? s : sq;
+      const int64_t nE = side == 0 ? nEP : nEQ, nIns = side == 0 ? nInsP : nInsQ;
+      int64_t* heavy = A.take_n<int64_t>(nE);
+      uint64_t* gkey = A.take_n<uint64_t>(2 * nIns);
+      uint32_t* gtie = A.take_n<uint32_t>(2 * nIns);
+      uint32_t* gidx = A.take_n<uint32_t>(2 * nIns);
+      int32_t* edgePair = A.take_n<int32_t>(nE);                    // edge -> pair
+      if (!heavy || !gkey || !gtie || !gidx || !edgePair) { st = ST_OUT_OF_MEMORY; break; }
+      if (nE == 0) continue;
+      if (side == 0) {
+        { range_owner_kernel<<<blocks_for_warps(K), kThreads, 0, ss>>>(eoffP, D.nP, K, edgePair); note_launch(); }
+        { ring_fill_kernel<0><<<blocks_for(nEP), kThreads, 0, ss>>>(Lb, Lo, D, R, eoffP, nEP, edgePair, vposP, regP, mP,
+                                                                  SP, slotP, insBaseP, curP, insListP, heavy,
+                                                                  nHeavy); note_launch(); }
+        { heavy_fill_kernel<0><<<2 * nsm, kHeavyThreads, smem, ss>>>(Lb, Lo, D, R, eoffP, edgePair, vposP, regP, mP, SP,
+                                                                     slotP, insBaseP, curP, insListP, heavy, nHeavy,
+                                                                     gkey, gtie, gidx); note_launch(); }
+      } else {
+        { range_owner_kernel<<<blocks_for_warps(K), kThreads, 0, ss>>>(eoffQ, D.nQ, K, edgePair); note_launch(); }
+        { ring_fill_kernel<1><<<blocks_for(nEQ), kThreads, 0, ss>>>(Lb, Lo, D, R, eoffQ, nEQ, edgePair, vposQ, regQ, mQ,
+                                                                  SQ, slotQ, insBaseQ, curQ, insListQ, heavy,
+                                                                  nHeavy + 1); note_launch(); }
+        { heavy_fill_kernel<1><<<2 * nsm, kHeavyThreads, smem, ss>>>(Lb, Lo, D, R, eoffQ, edgePair, vposQ, regQ, mQ, SQ,
+                                                                     slotQ, insBaseQ, curQ, insListQ, heavy, nHeavy + 1,
+                                                                     gkey, gtie, gidx); note_launch(); }
+      }
     }
+    if (sq != s) {
+      cudaEventRecord(join, sq);
+      cudaStreamWaitEvent(s, join, 0);
+    }
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (st != ST_OK) return st;
   }
   // ---- G6 links
   if (nR > 0)

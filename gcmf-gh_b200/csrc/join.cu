@@ -422,7 +422,7 @@ int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s) {
 }
 
 int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* d_err,
-             int64_t* h_scratch, cudaStream_t s, Marks* mk) {
+             int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux) {
   Marks dummy;
   if (!mk) mk = &dummy;
   J = JoinDev();
@@ -432,24 +432,42 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   // ---- J0 MBRs + sort keys
   J.mbr_b = A.take_n<double>(4 * nb); J.mbr_o = A.take_n<double>(4 * no);
   J.valid_b = A.take_n<uint8_t>(nb); J.valid_o = A.take_n<uint8_t>(no);
-  const int64_t nmax = std::max(nb, no);
   uint64_t* keyB = A.take_n<uint64_t>(nb);
   uint64_t* keyO = A.take_n<uint64_t>(no);
   uint32_t* idB = A.take_n<uint32_t>(nb);
   uint32_t* idO = A.take_n<uint32_t>(no);
-  uint64_t* kAlt = A.take_n<uint64_t>(nmax);
-  uint32_t* vAlt = A.take_n<uint32_t>(nmax);
+  uint64_t* kAlt = A.take_n<uint64_t>(nb);
+  uint32_t* vAlt = A.take_n<uint32_t>(nb);
+  uint64_t* kAltO = A.take_n<uint64_t>(no);
+  uint32_t* vAltO = A.take_n<uint32_t>(no);
   unsigned long long* d_cnt = A.take_n<unsigned long long>(8);
-  void* tmp = A.take(std::max(radix_temp_bytes(nmax), scan_temp_bytes(nmax)));
+  void* tmp = A.take(std::max(radix_temp_bytes(nb), scan_temp_bytes(nb)));
+  void* tmpO = A.take(std::max(radix_temp_bytes(no), scan_temp_bytes(no)));
   if (!J.mbr_b || !J.mbr_o || !J.valid_b || !J.valid_o || !keyB || !keyO || !idB || !idO || !kAlt ||
-      !vAlt || !d_cnt || !tmp)
+      !vAlt || !kAltO || !vAltO || !d_cnt || !tmp || !tmpO)
     return ST_OUT_OF_MEMORY;
   cudaMemsetAsync(d_cnt, 0, 8 * sizeof(unsigned long long), s);
+  // The two layers' MBRs and sorts are independent and each fills under half of the GPU
+  // (about 100 blocks per pass), so the overlay's run on the auxiliary stream.
+  cudaStream_t so = s;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  if (aux && cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) == cudaSuccess &&
+      cudaEventCreateWithFlags(&join, cudaEventDisableTiming) == cudaSuccess) {
+    cudaEventRecord(fork, s);
+    cudaStreamWaitEvent(aux, fork, 0);
+    so = aux;
+  }
   { mbr_kernel<<<blocks_for_warps(nb), kThreads, 0, s>>>(Lb, J.mbr_b, J.valid_b, keyB, idB, d_cnt + 0); note_launch(); }
-  { mbr_kernel<<<blocks_for_warps(no), kThreads, 0, s>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1); note_launch(); }
+  { mbr_kernel<<<blocks_for_warps(no), kThreads, 0, so>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1); note_launch(); }
   // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
   radix_sort_pairs(keyB, idB, kAlt, vAlt, nb, 64, tmp, d_err, s);
-  radix_sort_pairs(keyO, idO, kAlt, vAlt, no, 64, tmp, d_err, s);
+  radix_sort_pairs(keyO, idO, kAltO, vAltO, no, 64, tmpO, d_err, so);
+  if (so != s) {
+    cudaEventRecord(join, so);
+    cudaStreamWaitEvent(s, join, 0);
+  }
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
   mk->mark("join:mbr+sort", s);
   cudaMemcpyAsync(h_scratch, d_cnt, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
@@ -494,7 +512,7 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   { sweep_kernel<1><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs, pkeys, obits); note_launch(); }
   radix_sort_pairs(pkeys, pvals, pkAlt, pvAlt, K, ((obits + bbits + 7) / 8) * 8, rtmp, d_err, s);
   mk->mark("join:sweep-emit+sort", s);
-  return join_from_keys(Lb, Lo, pkeys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, mk);
+  return join_from_keys(Lb, Lo, pkeys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, mk, aux);
 }
 
 // Stages J3-J6 and the clip set over candidate pairs given as packed keys
@@ -506,11 +524,21 @@ constexpr int64_t kJoinTileMax = 64;
 
 int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys, int64_t K, int obits,
                    Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,
-                   int64_t* h_scratch, cudaStream_t s, Marks* mk) {
+                   int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux) {
   Marks dummy;
   if (!mk) mk = &dummy;
   J.n_pairs = K;
   if (K == 0) return ST_OK;
+  // The narrow-tile and whole-warp passes of each stage take disjoint pairs (by size), so
+  // with an auxiliary stream the warp pass, whose few large pairs make the tail, runs
+  // beside the tile pass; both are joined back into s before the stage's results are used.
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  const bool two = aux && cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) == cudaSuccess &&
+                   cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) == cudaSuccess;
+  struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 2; ++i) if (e[i]) cudaEventDestroy(e[i]); } } guard{ev};
+  cudaStream_t sw = two ? aux : s;
+  auto fork_aux = [&]() { if (two) { cudaEventRecord(ev[0], s); cudaStreamWaitEvent(aux, ev[0], 0); } };
+  auto join_aux = [&]() { if (two) { cudaEventRecord(ev[1], aux); cudaStreamWaitEvent(s, ev[1], 0); } };
   // ---- J3 CMBR + containment candidates
   J.b = A.take_n<int32_t>(K); J.o = A.take_n<int32_t>(K);
   J.cmbr = A.take_n<double>(4 * K);
@@ -530,18 +558,22 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
   // ---- J4 point in polygon
   // narrow tiles for small pairs first (they also set the flags of pairs with nothing to
   // test), then whole warps for the rest
+  fork_aux();
   { pip_kernel<kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
         Lb, Lo, J.b, J.o, J.pip_type, K, J.pip_flag, J.join_flag, -1, kJoinTileMax); note_launch(); }
-  { pip_kernel<32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.pip_type, K, J.pip_flag,
-                                                          J.join_flag, kJoinTileMax, INT64_MAX); note_launch(); }
+  { pip_kernel<32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.pip_type, K, J.pip_flag,
+                                                           J.join_flag, kJoinTileMax, INT64_MAX); note_launch(); }
+  join_aux();
   mk->mark("join:cmbr+pip", s);
   // ---- J5 common-MBR edge filter: count, offsets, lists
+  fork_aux();
   { cmf_kernel<0, kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
         Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, nullptr, nullptr, nullptr, nullptr, -1,
         kJoinTileMax); note_launch(); }
-  { cmf_kernel<0, 32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
-                                                             J.oE, nullptr, nullptr, nullptr, nullptr, kJoinTileMax,
-                                                             INT64_MAX); note_launch(); }
+  { cmf_kernel<0, 32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                              J.oE, nullptr, nullptr, nullptr, nullptr, kJoinTileMax,
+                                                              INT64_MAX); note_launch(); }
+  join_aux();
   exclusive_scan_i32(J.bE, bOff, K, d_total + 1, stmpK, d_err, s);
   exclusive_scan_i32(J.oE, oOff, K, d_total + 2, stmpK, d_err, s);
   cudaMemcpyAsync(h_scratch, d_total + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
@@ -550,19 +582,23 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
   int32_t* bList = A.take_n<int32_t>(nBl);
   int32_t* oList = A.take_n<int32_t>(nOl);
   if (!bList || !oList) return ST_OUT_OF_MEMORY;
+  fork_aux();
   { cmf_kernel<1, kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
         Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, bOff, oOff, bList, oList, -1, kJoinTileMax); note_launch(); }
-  { cmf_kernel<1, 32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
-                                                             J.oE, bOff, oOff, bList, oList, kJoinTileMax,
-                                                             INT64_MAX); note_launch(); }
+  { cmf_kernel<1, 32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                              J.oE, bOff, oOff, bList, oList, kJoinTileMax,
+                                                              INT64_MAX); note_launch(); }
+  join_aux();
   mk->mark("join:cmf", s);
   // ---- J6 refine
+  fork_aux();
   { refine_kernel<kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
         Lb, Lo, J.b, J.o, K, J.join_flag, J.bE, J.oE, bOff, oOff, bList, oList, J.seg_flag, -1,
         kJoinTileMax * 4); note_launch(); }
-  { refine_kernel<32><<<blocks_for_warps(K), kThreads, 0, s>>>(Lb, Lo, J.b, J.o, K, J.join_flag, J.bE, J.oE,
-                                                             bOff, oOff, bList, oList, J.seg_flag, kJoinTileMax * 4,
-                                                             INT64_MAX); note_launch(); }
+  { refine_kernel<32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, K, J.join_flag, J.bE, J.oE,
+                                                              bOff, oOff, bList, oList, J.seg_flag, kJoinTileMax * 4,
+                                                              INT64_MAX); note_launch(); }
+  join_aux();
   mk->mark("join:refine", s);
   // ---- clip set = containment pairs + pairs with intersecting edges
   { clip_flag_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.pip_type, J.pip_flag, J.join_flag, J.seg_flag, K,

@@ -286,7 +286,7 @@ int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64
     { candidate_kernel<1><<<blocks_for_warps(nq), kThreads, 0, s>>>(qmbr, qvalid, nq, r_mbr, grid, nullptr, qoff,
                                                                      keys, obits); note_launch(); }
     radix_sort_pairs(keys, vals, kAlt, vAlt, K, ((obits + qbits + 7) / 8) * 8, rtmp, d_err, s);
-    st = join_from_keys(Lq, resident(), keys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s);
+    st = join_from_keys(Lq, resident(), keys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, nullptr, aux);
     if (st != ST_OK) return st;
     if (J.n_clip > 0) {
       ClipParams prm;
