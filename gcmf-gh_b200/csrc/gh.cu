@@ -3218,6 +3218,17 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   { edge_filter_kernel<1, 32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ,
                                                                        kFilterTileMax, INT64_MAX); note_launch(); }
   join_aux();
+  // The binned pairs (below) go to the auxiliary stream when there is one: fork here, before
+  // the chunked count is queued on s, so that the two run side by side.
+  cudaStream_t sb = s;
+  cudaEvent_t bev[2] = {nullptr, nullptr};
+  struct BinEvGuard { cudaEvent_t* e; ~BinEvGuard() { for (int i = 0; i < 2; ++i) if (e[i]) cudaEventDestroy(e[i]); } } bguard{bev};
+  if (nBigPairs > 0 && aux && cudaEventCreateWithFlags(&bev[0], cudaEventDisableTiming) == cudaSuccess &&
+      cudaEventCreateWithFlags(&bev[1], cudaEventDisableTiming) == cudaSuccess) {
+    cudaEventRecord(bev[0], s);
+    cudaStreamWaitEvent(aux, bev[0], 0);
+    sb = aux;
+  }
   // ---- G2 count: chunked pairs
   Records R{};
   if (nCh > 0) {
@@ -3226,29 +3237,32 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     exclusive_scan_i32(chunkRec, recScan, nCh, nullptr, stC, d_err, s);
     exclusive_scan_i32(chunkQ, qScan, nCh, nullptr, stC, d_err, s);
   }
-  // ---- G2 count: binned pairs (host loop; few pairs)
+  // ---- G2 count: binned pairs (host loop; few pairs).  It is driven from the host with a
+  // read-back per pair, so with an auxiliary stream it runs there, beside the chunked
+  // count; s waits for it before the per-pair totals.
+  auto syncb = [&]() { return cudaStreamSynchronize(sb) == cudaSuccess; };
   struct BigWork { BigInfo info; BinGrid G; int64_t* cellOff; int32_t* cellList; int64_t* recPos; };
   std::vector<BigWork> bigs(nBigPairs);
   if (nBigPairs > 0) {
     BigInfo* dInfo = A.take_n<BigInfo>(nBigPairs);
     if (!dInfo) return ST_OUT_OF_MEMORY;
-    { big_info_kernel<<<blocks_for(nBigPairs), kThreads, 0, s>>>(bigList, nBigPairs, cP, cQ, offP, offQ, D, dInfo); note_launch(); }
+    { big_info_kernel<<<blocks_for(nBigPairs), kThreads, 0, sb>>>(bigList, nBigPairs, cP, cQ, offP, offQ, D, dInfo); note_launch(); }
     std::vector<BigInfo> hInfo(nBigPairs);
-    cudaMemcpyAsync(hInfo.data(), dInfo, nBigPairs * sizeof(BigInfo), cudaMemcpyDeviceToHost, s);
-    if (!sync()) return ST_CUDA_ERROR;
+    cudaMemcpyAsync(hInfo.data(), dInfo, nBigPairs * sizeof(BigInfo), cudaMemcpyDeviceToHost, sb);
+    if (!syncb()) return ST_CUDA_ERROR;
     std::sort(hInfo.begin(), hInfo.end(), [](const BigInfo& x, const BigInfo& y) { return x.k < y.k; });
     int64_t* d_t = A.take_n<int64_t>(2);
     unsigned long long* d_q = A.take_n<unsigned long long>(1);
     double* d_ext = A.take_n<double>(2 * nBigPairs);
     if (!d_t || !d_q || !d_ext) return ST_OUT_OF_MEMORY;
-    cudaMemsetAsync(d_ext, 0, 2 * nBigPairs * sizeof(double), s);
+    cudaMemsetAsync(d_ext, 0, 2 * nBigPairs * sizeof(double), sb);
     for (int bi = 0; bi < nBigPairs; ++bi)
       if (hInfo[bi].cq > 0)
-        { edge_extent_kernel<<<blocks_for(hInfo[bi].cq), kThreads, 0, s>>>(Lb, Lo, D, hInfo[bi].k, LQ + hInfo[bi].offQ,
+        { edge_extent_kernel<<<blocks_for(hInfo[bi].cq), kThreads, 0, sb>>>(Lb, Lo, D, hInfo[bi].k, LQ + hInfo[bi].offQ,
                                                                           hInfo[bi].cq, d_ext + 2 * bi); note_launch(); }
     std::vector<double> hExt(2 * nBigPairs);
-    cudaMemcpyAsync(hExt.data(), d_ext, 2 * nBigPairs * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (!sync()) return ST_CUDA_ERROR;
+    cudaMemcpyAsync(hExt.data(), d_ext, 2 * nBigPairs * sizeof(double), cudaMemcpyDeviceToHost, sb);
+    if (!syncb()) return ST_CUDA_ERROR;
     for (int bi = 0; bi < nBigPairs; ++bi) {
       BigWork& W = bigs[bi];
       W.info = hInfo[bi];
@@ -3281,25 +3295,29 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
       W.recPos = A.take_n<int64_t>(W.info.cp);
       void* st2 = A.take(scan_temp_bytes(std::max(W.info.cp, 1)));
       if (!cellCnt || !W.cellOff || !cursor || !st || !recCnt || !W.recPos || !st2) return ST_OUT_OF_MEMORY;
-      cudaMemsetAsync(cellCnt, 0, (ncell + 1) * sizeof(int32_t), s);
-      cudaMemsetAsync(cursor, 0, ncell * sizeof(int32_t), s);
+      cudaMemsetAsync(cellCnt, 0, (ncell + 1) * sizeof(int32_t), sb);
+      cudaMemsetAsync(cursor, 0, ncell * sizeof(int32_t), sb);
       const int64_t k = W.info.k;
-      { bin_count_kernel<<<blocks_for(W.info.cq), kThreads, 0, s>>>(Lb, Lo, D, k, LQ + W.info.offQ, W.info.cq, W.G,
+      { bin_count_kernel<<<blocks_for(W.info.cq), kThreads, 0, sb>>>(Lb, Lo, D, k, LQ + W.info.offQ, W.info.cq, W.G,
                                                                     cellCnt); note_launch(); }
-      exclusive_scan_i32(cellCnt, W.cellOff, ncell + 1, d_t, st, d_err, s);
-      cudaMemcpyAsync(hs, d_t, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-      if (!sync()) return ST_CUDA_ERROR;
+      exclusive_scan_i32(cellCnt, W.cellOff, ncell + 1, d_t, st, d_err, sb);
+      cudaMemcpyAsync(hs, d_t, sizeof(int64_t), cudaMemcpyDeviceToHost, sb);
+      if (!syncb()) return ST_CUDA_ERROR;
       W.cellList = A.take_n<int32_t>(hs[0]);
       if (!W.cellList) return ST_OUT_OF_MEMORY;
-      { bin_fill_kernel<<<blocks_for(W.info.cq), kThreads, 0, s>>>(Lb, Lo, D, k, LQ + W.info.offQ, W.info.cq, W.G,
+      { bin_fill_kernel<<<blocks_for(W.info.cq), kThreads, 0, sb>>>(Lb, Lo, D, k, LQ + W.info.offQ, W.info.cq, W.G,
                                                                    W.cellOff, cursor, W.cellList); note_launch(); }
-      cudaMemsetAsync(d_q, 0, sizeof(unsigned long long), s);
-      { (prm.exact ? bin_pairs_kernel<0, 1> : bin_pairs_kernel<0, 0>)<<<blocks_for(W.info.cp), kThreads, 0, s>>>(
+      cudaMemsetAsync(d_q, 0, sizeof(unsigned long long), sb);
+      { (prm.exact ? bin_pairs_kernel<0, 1> : bin_pairs_kernel<0, 0>)<<<blocks_for(W.info.cp), kThreads, 0, sb>>>(
             Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G, W.cellOff, W.cellList, prm.eps, recCnt, d_q,
                                                                        nullptr, R); note_launch(); }
-      exclusive_scan_i32(recCnt, W.recPos, W.info.cp, d_t + 1, st2, d_err, s);
-      { bin_total_kernel<<<1, 1, 0, s>>>(d_t + 1, d_q, k, binRec, binQ); note_launch(); }
+      exclusive_scan_i32(recCnt, W.recPos, W.info.cp, d_t + 1, st2, d_err, sb);
+      { bin_total_kernel<<<1, 1, 0, sb>>>(d_t + 1, d_q, k, binRec, binQ); note_launch(); }
     }
+  }
+  if (sb != s) {
+    cudaEventRecord(bev[1], sb);
+    cudaStreamWaitEvent(s, bev[1], 0);
   }
   int64_t* nrec64 = A.take_n<int64_t>(K);
   int64_t* recOff = A.take_n<int64_t>(K);
@@ -3318,15 +3336,23 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   R.a = A.take_n<double>(nR); R.b = A.take_n<double>(nR);
   R.t = A.take_n<int8_t>(nR); R.k = A.take_n<int32_t>(nR);
   if (!R.p || !R.q || !R.a || !R.b || !R.t || !R.k) return ST_OUT_OF_MEMORY;
+  if (sb != s && !bigs.empty()) {                   // the binned pairs' emit beside the chunked one
+    cudaEventRecord(bev[0], s);
+    cudaStreamWaitEvent(sb, bev[0], 0);
+  }
   if (nCh > 0)
     { (prm.exact ? intersect_kernel<1, 1> : intersect_kernel<1, 0>)<<<blocks_for_warps(nCh), kThreads, 0, s>>>(
         Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, recOff, R, chunkPair); note_launch(); }
   for (auto& W : bigs) {
     const int64_t k = W.info.k;
-    { add_offset_kernel<<<blocks_for(W.info.cp), kThreads, 0, s>>>(W.recPos, W.info.cp, recOff + k); note_launch(); }
-    { (prm.exact ? bin_pairs_kernel<1, 1> : bin_pairs_kernel<1, 0>)<<<blocks_for(W.info.cp), kThreads, 0, s>>>(
+    { add_offset_kernel<<<blocks_for(W.info.cp), kThreads, 0, sb>>>(W.recPos, W.info.cp, recOff + k); note_launch(); }
+    { (prm.exact ? bin_pairs_kernel<1, 1> : bin_pairs_kernel<1, 0>)<<<blocks_for(W.info.cp), kThreads, 0, sb>>>(
           Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G, W.cellOff, W.cellList, prm.eps, nullptr, nullptr,
-                                                                     W.recPos, R); note_launch(); }
+                                                                      W.recPos, R); note_launch(); }
+  }
+  if (sb != s && !bigs.empty()) {
+    cudaEventRecord(bev[1], sb);
+    cudaStreamWaitEvent(s, bev[1], 0);
   }
   mk->mark("clip:emit", s);
   if (ex && ex->records_only) {
