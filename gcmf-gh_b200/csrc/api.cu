@@ -89,6 +89,7 @@ struct gcmfgh_ctx {
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   cudaStream_t aux = nullptr;     // high-priority stream for the long pairs' labelling
+  cudaStream_t aux2 = nullptr;    // third stream: the warp-per-pair labelling beside the tiles
   Arena join_arena, clip_arena, layer_arena, pair_arena;
   int* d_err = nullptr;
   int64_t* h_scratch = nullptr;   // pinned
@@ -165,7 +166,7 @@ gcmfgh_status run_clip_ctx(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_la
   c->marks[1].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   int st = run_clip(to_dev(b), to_dev(o), pid, qid, n, c->prm, c->clip_arena, c->clip, c->d_err,
-                    c->h_scratch, c->stream, &c->marks[1], c->aux);
+                    c->h_scratch, c->stream, &c->marks[1], c->aux, nullptr, c->aux2);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_clip = true;
@@ -265,6 +266,10 @@ gcmfgh_status gcmfgh_create(int device, gcmfgh_ctx** out) {
   }
   c->stream = c->own;
   c->aux = create_priority_stream();
+  if (cudaStreamCreateWithFlags(&c->aux2, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    c->aux2 = nullptr;
+  }
   cudaMemset(c->d_err, 0, 64);
   for (auto& m : c->marks)
     for (int i = 0; i < Marks::kMax; ++i) cudaEventCreate(&m.ev[i]);
@@ -305,6 +310,7 @@ gcmfgh_status gcmfgh_destroy(gcmfgh_ctx* c) {
   if (c->h_scratch) cudaFreeHost(c->h_scratch);
   if (c->own) cudaStreamDestroy(c->own);
   if (c->aux) cudaStreamDestroy(c->aux);
+  if (c->aux2) cudaStreamDestroy(c->aux2);
   for (auto& m : c->marks)
     for (int i = 0; i < Marks::kMax; ++i)
       if (m.ev[i]) cudaEventDestroy(m.ev[i]);

@@ -152,12 +152,14 @@ struct RingExport {
 
 // aux: optional second stream (ideally of higher priority); long pairs are labelled on it
 // while the warp-per-pair kernel runs on s.  Without it everything runs on s.
+// aux2: optional third stream; the warp-per-pair labelling runs on it beside the one-thread
+// labelling on s.
 // ex: when given, the clip stops after the neighbour links and pair 0's merged rings are
 // exported into it instead of being labelled and traced.
 int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, const int32_t* d_qid,
              int64_t n_pairs, const ClipParams& prm, Arena& arena, ClipDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
-             cudaStream_t aux = nullptr, RingExport* ex = nullptr);
+             cudaStream_t aux = nullptr, RingExport* ex = nullptr, cudaStream_t aux2 = nullptr);
 
 // One pair of multi-component polygons (rings: host, interleaved, open; ring c has
 // sizes[c] >= 3 vertices), P clipped against Q as given.  Result as one pair of ClipDev.

@@ -459,9 +459,11 @@ __global__ void record_count_kernel(Records R, int64_t nR, const int64_t* __rest
     atomicMax(reinterpret_cast<unsigned long long*>(&srcLinkQ[eQ]), link_key(R.p[r], r));
 }
 
-__global__ void edge_slots_kernel(const int32_t* __restrict__ ins, int64_t nE, int32_t* __restrict__ sz) {
+// slot of each edge's source vertex in the concatenated merged rings: the exclusive scan
+// of (1 + insertions) over the edges, i.e. the edge index plus the scan of the insertions
+__global__ void edge_slots_kernel(const int64_t* __restrict__ insBase, int64_t nE, int64_t* __restrict__ vpos) {
   int64_t e = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-  if (e < nE) sz[e] = 1 + ins[e];
+  if (e < nE) vpos[e] = e + insBase[e];
 }
 
 struct RingSet {
@@ -482,14 +484,19 @@ struct RingSet {
 __global__ void pair_ring_kernel(const int64_t* __restrict__ eoff, const int64_t* __restrict__ vpos,
                                  const int32_t* __restrict__ n, const int32_t* __restrict__ nrec,
                                  const int32_t* __restrict__ status, int64_t K, int64_t nE, int64_t vtot,
-                                 int32_t* __restrict__ m, int64_t* __restrict__ regSize) {
+                                 int32_t* __restrict__ m, int64_t* __restrict__ regSize,
+                                 unsigned long long* __restrict__ ringTot) {
   int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-  if (k >= K) return;
-  int64_t e0 = eoff[k], e1 = e0 + (status[k] == 2 ? 0 : n[k]);
-  int64_t v0 = e0 < nE ? vpos[e0] : vtot, v1 = e1 < nE ? vpos[e1] : vtot;
-  int mm = status[k] == 0 ? (int)(v1 - v0) : 0;
-  m[k] = mm;
-  regSize[k] = status[k] == 0 ? (int64_t)mm + 2 + 2 * (int64_t)nrec[k] : 0;
+  unsigned long long mm = 0;
+  if (k < K) {
+    int64_t e0 = eoff[k], e1 = e0 + (status[k] == 2 ? 0 : n[k]);
+    int64_t v0 = e0 < nE ? vpos[e0] : vtot, v1 = e1 < nE ? vpos[e1] : vtot;
+    mm = status[k] == 0 ? (unsigned long long)(v1 - v0) : 0ull;
+    m[k] = (int)mm;
+    regSize[k] = status[k] == 0 ? (int64_t)mm + 2 + 2 * (int64_t)nrec[k] : 0;
+  }
+  mm = warp_sum(mm);                                        // merged-ring vertices, all pairs
+  if (lane_id() == 0 && mm) atomicAdd(ringTot, mm);
 }
 
 // ---------------------------------------------------------------- G5 ring fill
@@ -3128,7 +3135,7 @@ out_compact_kernel(int64_t K, const double* __restrict__ xy, const int64_t* __re
 
 int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const int32_t* d_qid,
              int64_t K, const ClipParams& prm, Arena& A, ClipDev& C, int* d_err, int64_t* hs,
-             cudaStream_t s, Marks* mk, cudaStream_t aux, RingExport* ex) {
+             cudaStream_t s, Marks* mk, cudaStream_t aux, RingExport* ex, cudaStream_t aux2) {
   Marks dummy;
   if (!mk) mk = &dummy;
   C = ClipDev();
@@ -3366,8 +3373,6 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int32_t* insQ = A.take_n<int32_t>(nEQ);
   int64_t* srcLinkP = A.take_n<int64_t>(nEP);
   int64_t* srcLinkQ = A.take_n<int64_t>(nEQ);
-  int32_t* szP = A.take_n<int32_t>(nEP);
-  int32_t* szQ = A.take_n<int32_t>(nEQ);
   int64_t* vposP = A.take_n<int64_t>(nEP);
   int64_t* vposQ = A.take_n<int64_t>(nEQ);
   int64_t* insBaseP = A.take_n<int64_t>(nEP);
@@ -3377,7 +3382,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int64_t* slotP = A.take_n<int64_t>(nR);
   int64_t* slotQ = A.take_n<int64_t>(nR);
   void* stE = A.take(scan_temp_bytes(std::max<int64_t>(std::max(nEP, nEQ), 1)));
-  if (!insP || !insQ || !srcLinkP || !srcLinkQ || !szP || !szQ || !vposP || !vposQ || !insBaseP ||
+  if (!insP || !insQ || !srcLinkP || !srcLinkQ || !vposP || !vposQ || !insBaseP ||
       !insBaseQ || !curP || !curQ || !slotP || !slotQ || !stE)
     return ST_OUT_OF_MEMORY;
   cudaMemsetAsync(insP, 0, nEP * sizeof(int32_t), s);
@@ -3389,15 +3394,13 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (nR > 0)
     { record_count_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, eoffP, eoffQ, D.status, insP, insQ,
                                                             srcLinkP, srcLinkQ); note_launch(); }
-  { edge_slots_kernel<<<blocks_for(nEP), kThreads, 0, s>>>(insP, nEP, szP); note_launch(); }
-  { edge_slots_kernel<<<blocks_for(nEQ), kThreads, 0, s>>>(insQ, nEQ, szQ); note_launch(); }
-  exclusive_scan_i32(szP, vposP, nEP, tot + 7, stE, d_err, s);
-  exclusive_scan_i32(szQ, vposQ, nEQ, tot + 8, stE, d_err, s);
   exclusive_scan_i32(insP, insBaseP, nEP, tot + 9, stE, d_err, s);
   exclusive_scan_i32(insQ, insBaseQ, nEQ, tot + 10, stE, d_err, s);
-  cudaMemcpyAsync(hs, tot + 7, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  { edge_slots_kernel<<<blocks_for(nEP), kThreads, 0, s>>>(insBaseP, nEP, vposP); note_launch(); }
+  { edge_slots_kernel<<<blocks_for(nEQ), kThreads, 0, s>>>(insBaseQ, nEQ, vposQ); note_launch(); }
+  cudaMemcpyAsync(hs + 2, tot + 9, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
-  const int64_t vtotP = hs[0], vtotQ = hs[1], nInsP = hs[2], nInsQ = hs[3];
+  const int64_t nInsP = hs[2], nInsQ = hs[3], vtotP = nEP + nInsP, vtotQ = nEQ + nInsQ;
   int64_t* insListP = A.take_n<int64_t>(nInsP);
   int64_t* insListQ = A.take_n<int64_t>(nInsQ);
   int32_t* mP = A.take_n<int32_t>(K);
@@ -3410,22 +3413,18 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (nR > 0)
     { record_scatter_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, eoffP, eoffQ, D.status, insBaseP, curP,
                                                               insListP, insBaseQ, curQ, insListQ); note_launch(); }
+  unsigned long long* ringTot = reinterpret_cast<unsigned long long*>(tot + 13);
+  cudaMemsetAsync(ringTot, 0, sizeof(unsigned long long), s);
   { pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffP, vposP, D.nP, nrec, D.status, K, nEP, vtotP, mP,
-                                                      regSizeP); note_launch(); }
+                                                      regSizeP, ringTot); note_launch(); }
   { pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffQ, vposQ, D.nQ, nrec, D.status, K, nEQ, vtotQ, mQ,
-                                                      regSizeQ); note_launch(); }
+                                                      regSizeQ, ringTot); note_launch(); }
   exclusive_scan_i64(regSizeP, regP, K, tot + 11, stK, d_err, s);
   exclusive_scan_i64(regSizeQ, regQ, K, tot + 12, stK, d_err, s);
-  {
-    int64_t* junk = A.take_n<int64_t>(K);
-    if (!junk) return ST_OUT_OF_MEMORY;
-    exclusive_scan_i32(mP, junk, K, tot + 13, stK, d_err, s);
-    exclusive_scan_i32(mQ, junk, K, tot + 14, stK, d_err, s);
-  }
-  cudaMemcpyAsync(hs, tot + 11, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hs, tot + 11, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
   const int64_t regTotP = hs[0], regTotQ = hs[1];
-  C.n_ring_vertices = hs[2] + hs[3];
+  C.n_ring_vertices = hs[2];
   C.n_records = nR;
   auto take_ring = [&](int64_t n, RingSet& S) {
     S.x = A.take_n<double>(n); S.y = A.take_n<double>(n);
@@ -3600,13 +3599,28 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
                                                                mlist, mcnt); note_launch(); }
     { (prm.exact ? label_trace_block_kernel<1> : label_trace_block_kernel<0>)<<<2 * nsm, kBlockLabelThreads, 0, ls>>>(la); note_launch(); }
     const bool wide = K >= prm.wide_label_min;
+    // the warp-per-pair pairs on the third stream, beside the one-thread pairs on s
+    cudaStream_t ws = s;
+    cudaEvent_t wfork = nullptr, wjoin = nullptr;
+    if (aux2 && cudaEventCreateWithFlags(&wfork, cudaEventDisableTiming) == cudaSuccess &&
+        cudaEventCreateWithFlags(&wjoin, cudaEventDisableTiming) == cudaSuccess) {
+      cudaEventRecord(wfork, s);
+      cudaStreamWaitEvent(aux2, wfork, 0);
+      ws = aux2;
+    }
     { (prm.exact ? label_trace_kernel<1, 0>
-                 : (wide ? label_trace_kernel<0, 1> : label_trace_kernel<0, 0>))<<<(unsigned)((K + 3) / 4), 128, 0, s>>>(la); note_launch(); }
+                 : (wide ? label_trace_kernel<0, 1> : label_trace_kernel<0, 0>))<<<(unsigned)((K + 3) / 4), 128, 0, ws>>>(la); note_launch(); }
     if (prm.tile_label_max > 0) {
       const int64_t pairsPerBlock = 4 * (32 / kTileLanes);
       { (prm.exact ? label_trace_tile_kernel<1, 0>
                    : (wide ? label_trace_tile_kernel<0, 1> : label_trace_tile_kernel<0, 0>))<<<(unsigned)((K + pairsPerBlock - 1) / pairsPerBlock), 128, 0, s>>>(la); note_launch(); }
     }
+    if (ws != s) {
+      cudaEventRecord(wjoin, ws);
+      cudaStreamWaitEvent(s, wjoin, 0);
+    }
+    if (wfork) cudaEventDestroy(wfork);
+    if (wjoin) cudaEventDestroy(wjoin);
     if (ls != s) {
       cudaEventRecord(join, ls);
       cudaStreamWaitEvent(s, join, 0);
