@@ -199,11 +199,11 @@ struct Records {
   int32_t* k;       // pair
 };
 
-// Occupancy over registers: the count pass at most 80 registers (3 blocks per SM; count
-// stage 1.29 -> 1.07 ms), the emit pass 64 (4 blocks; 0.55 -> 0.45 ms).  The
+// Occupancy over registers: the count pass at most 64 registers (4 blocks per SM; count
+// stage 1.29 -> 0.81 ms), the emit pass 40 (6 blocks; 0.55 -> 0.39 ms).  The
 // exact-predicate instances keep 128 registers (their expansions would spill).
 template <int kMode, int kExact>
-__global__ void __launch_bounds__(kThreads, kExact ? 2 : (kMode == 1 ? 4 : 3))
+__global__ void __launch_bounds__(kThreads, kExact ? 2 : (kMode == 1 ? 6 : 4))
 intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* __restrict__ chunkOff,
                  int64_t nChunks, const int32_t* __restrict__ cP, const int32_t* __restrict__ cQ,
                  const int64_t* __restrict__ offP, const int64_t* __restrict__ offQ,
