@@ -160,13 +160,14 @@ gcmfgh_status clip_info(gcmfgh_ctx* c, gcmfgh_clip_info* info) {
 }
 
 gcmfgh_status run_clip_ctx(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o,
-                           const int32_t* pid, const int32_t* qid, int64_t n, gcmfgh_clip_info* info) {
+                           const int32_t* pid, const int32_t* qid, int64_t n, gcmfgh_clip_info* info,
+                           const double* mbrB = nullptr, const double* mbrO = nullptr) {
   c->clip_arena.reset();
   c->have_clip = false;
   c->marks[1].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   int st = run_clip(to_dev(b), to_dev(o), pid, qid, n, c->prm, c->clip_arena, c->clip, c->d_err,
-                    c->h_scratch, c->stream, &c->marks[1], c->aux, nullptr, c->aux2);
+                    c->h_scratch, c->stream, &c->marks[1], c->aux, nullptr, c->aux2, mbrB, mbrO);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_clip = true;
@@ -448,7 +449,9 @@ gcmfgh_status gh_clip_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_
   if (b->coords != c->join_b || o->coords != c->join_o) return GCMFGH_INVALID_ARGUMENT;
   cudaSetDevice(c->device);
   c->prm.no_swap = 0;
-  return run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, c->join.n_clip, info);
+  // the join's polygon MBRs of the same layers (mbr_kernel computes what the clip would)
+  return run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, c->join.n_clip, info, c->join.mbr_b,
+                      c->join.mbr_o);
 }
 
 gcmfgh_status gh_clip_get(gcmfgh_ctx* c, int f, void* dst, int64_t cap, int on_dev, int64_t* bytes) {

@@ -154,12 +154,15 @@ struct RingExport {
 // while the warp-per-pair kernel runs on s.  Without it everything runs on s.
 // aux2: optional third stream; the warp-per-pair labelling runs on it beside the one-thread
 // labelling on s.
+// mbrB / mbrO: the layers' polygon MBRs when the caller already has them (the join
+// computes the same ones), else they are computed here.
 // ex: when given, the clip stops after the neighbour links and pair 0's merged rings are
 // exported into it instead of being labelled and traced.
 int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, const int32_t* d_qid,
              int64_t n_pairs, const ClipParams& prm, Arena& arena, ClipDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
-             cudaStream_t aux = nullptr, RingExport* ex = nullptr, cudaStream_t aux2 = nullptr);
+             cudaStream_t aux = nullptr, RingExport* ex = nullptr, cudaStream_t aux2 = nullptr,
+             const double* mbrB = nullptr, const double* mbrO = nullptr);
 
 // One pair of multi-component polygons (rings: host, interleaved, open; ring c has
 // sizes[c] >= 3 vertices), P clipped against Q as given.  Result as one pair of ClipDev.

@@ -3135,7 +3135,8 @@ out_compact_kernel(int64_t K, const double* __restrict__ xy, const int64_t* __re
 
 int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const int32_t* d_qid,
              int64_t K, const ClipParams& prm, Arena& A, ClipDev& C, int* d_err, int64_t* hs,
-             cudaStream_t s, Marks* mk, cudaStream_t aux, RingExport* ex, cudaStream_t aux2) {
+             cudaStream_t s, Marks* mk, cudaStream_t aux, RingExport* ex, cudaStream_t aux2,
+             const double* mbrB, const double* mbrO) {
   Marks dummy;
   if (!mk) mk = &dummy;
   C = ClipDev();
@@ -3144,11 +3145,20 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (K <= 0) return ST_OK;
   auto sync = [&]() { return cudaStreamSynchronize(s) == cudaSuccess; };
   // layer MBRs (same definition as the join's)
-  double* mb = A.take_n<double>(4 * Lb.n);
-  double* mo = A.take_n<double>(4 * Lo.n);
-  if (!mb || !mo) return ST_OUT_OF_MEMORY;
-  layer_mbrs(Lb, mb, s);
-  layer_mbrs(Lo, mo, s);
+  const double* mb = mbrB;
+  const double* mo = mbrO;
+  if (!mb) {
+    double* m = A.take_n<double>(4 * Lb.n);
+    if (!m) return ST_OUT_OF_MEMORY;
+    layer_mbrs(Lb, m, s);
+    mb = m;
+  }
+  if (!mo) {
+    double* m = A.take_n<double>(4 * Lo.n);
+    if (!m) return ST_OUT_OF_MEMORY;
+    layer_mbrs(Lo, m, s);
+    mo = m;
+  }
   // ---- G0 setup
   PairDev D;
   D.pS = A.take_n<int64_t>(K); D.qS = A.take_n<int64_t>(K);
