@@ -114,9 +114,11 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def stage_bytes(stage, ji, ci, nb, no, vb, vo):
+def stage_bytes(stage, ji, ci, nb, no, vb, vo, cand_vertices=0):
     """Algorithmic bytes of one stage (reads of what it must read once + writes of what it
-    must produce), from the step's counts."""
+    must produce), from the step's counts.  cand_vertices is the sum over candidate pairs
+    of both polygons' vertex counts: the common-MBR filter reads every edge of both
+    polygons of each candidate once."""
     K, C = ji["n_pairs"], ci["n_pairs"]
     ring, out_v, recs = ci["n_ring_vertices"], ci["n_vertices"], ci["n_records"]
     table = {
@@ -129,7 +131,7 @@ def stage_bytes(stage, ji, ci, nb, no, vb, vo):
         "join:mbr+sort": 16 * (vb + vo) + 40 * (nb + no),
         "join:sweep-count": 36 * (nb + no),
         "join:sweep-emit+sort": 36 * (nb + no) + 16 * K,
-        "join:cmf": 16 * (vb + vo) * 0 + 40 * K,
+        "join:cmf": 16 * cand_vertices + 40 * K,
     }
     return table.get(stage)
 
@@ -494,8 +496,20 @@ def run_ours(args, rank, world, local):
         stage_ms = {k: statistics.mean(v) for k, v in stages.items()}
         dom = max(stage_ms, key=stage_ms.get)
         peak, peak_kind = measured_peaks()
-        alg = stage_bytes(dom, ji, ci, base.n_polys, ovl.n_polys, base.n_vertices, ovl.n_vertices)
+        jb, jo = eng.join_field("b"), eng.join_field("o")
+        cand_v = int(base.vnum[jb].astype(np.int64).sum() + ovl.vnum[jo].astype(np.int64).sum())
+        counts = (ji, ci, base.n_polys, ovl.n_polys, base.n_vertices, ovl.n_vertices, cand_v)
+        alg = stage_bytes(dom, *counts)
         achieved = (alg / (stage_ms[dom] * 1e-3) / 1e9) if alg else None
+        # every stage with a byte model, and the whole step: sum of algorithmic bytes / step time
+        per_stage = {}
+        for k, v in stage_ms.items():
+            b = stage_bytes(k, *counts)
+            if b:
+                per_stage[k] = {"ms": round(v, 4), "algorithmic_bytes": b,
+                                "frac": round(b / (v * 1e-3) / 1e9 / peak, 5)}
+        step_bytes = (32 * (base.n_polys + ovl.n_polys) + 8 * ji["n_pairs"] + 16 * cand_v
+                      + 16 * ci["n_ring_vertices"] + 16 * ci["n_vertices"] + 8 * pairs)
         line = {
             "metric": METRIC, "value": total_pairs / (ms * 1e-3), "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -510,6 +524,12 @@ def run_ours(args, rank, world, local):
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic_from_profiles(dom),
                          "algorithmic_bytes": alg, "kernel_ms": stage_ms[dom], "peak_source": peak_kind},
             "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+            "stage_roofline": per_stage,
+            "step_roofline": {"algorithmic_bytes": step_bytes, "achieved": step_bytes / (ms * 1e-3) / 1e9,
+                              "peak": peak, "unit": "GB/s", "frac": step_bytes / (ms * 1e-3) / 1e9 / peak,
+                              "bytes": "32 B per layer MBR + 8 B per candidate pair + 16 B per vertex of "
+                                       "both polygons of every candidate (CMF edge scan) + 16 B per merged "
+                                       "ring vertex + 16 B per result vertex + 8 B per clipped pair"},
             "clocks": clocks,
             "gpu_launches": launches,
         }

@@ -654,9 +654,12 @@ gcmfgh_status gcmfgh_join_clip_host(gcmfgh_ctx* c, const gcmfgh_layer* bh, const
     if (!xy || !vn || !vp) return GCMFGH_OUT_OF_MEMORY;
     if (h->n_polys > 0) {
       if (!h->coords || !h->vnum || !h->vps) return GCMFGH_INVALID_ARGUMENT;
-      cudaMemcpyAsync(xy, h->coords, sizeof(double) * 2 * h->n_vertices, cudaMemcpyHostToDevice, c->stream);
-      cudaMemcpyAsync(vn, h->vnum, sizeof(int32_t) * h->n_polys, cudaMemcpyHostToDevice, c->stream);
-      cudaMemcpyAsync(vp, h->vps, sizeof(int64_t) * h->n_polys, cudaMemcpyHostToDevice, c->stream);
+      if (cudaMemcpyAsync(xy, h->coords, sizeof(double) * 2 * h->n_vertices, cudaMemcpyHostToDevice, c->stream) !=
+              cudaSuccess ||
+          cudaMemcpyAsync(vn, h->vnum, sizeof(int32_t) * h->n_polys, cudaMemcpyHostToDevice, c->stream) !=
+              cudaSuccess ||
+          cudaMemcpyAsync(vp, h->vps, sizeof(int64_t) * h->n_polys, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        return GCMFGH_CUDA_ERROR;
     }
     dl[i] = gcmfgh_layer{xy, vn, vp, h->n_polys, h->n_vertices};
   }

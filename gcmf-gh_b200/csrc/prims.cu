@@ -10,7 +10,8 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;   // 2048 elements per tile
 // look-back status word: bits 62-63 flag (0 pending, 1 tile aggregate, 2 inclusive
-// prefix), bits 0-61 the value (sums stay below 2^62).
+// prefix), bits 0-61 the value in two's complement (|sums| stay below 2^61, so the
+// reader sign-extends bit 61).
 constexpr uint64_t kFlagAgg = 1ull << 62;
 constexpr uint64_t kFlagPrefix = 2ull << 62;
 constexpr uint64_t kValueMask = (1ull << 62) - 1;
@@ -76,7 +77,8 @@ scan_kernel(const T* __restrict__ in, int64_t* __restrict__ out, int64_t n, int6
         unsigned prefix = __ballot_sync(0xffffffffu, (word >> 62) == 2);
         // lanes up to and including the first (lowest lane) inclusive prefix contribute
         int stop = prefix ? __ffs(prefix) - 1 : 31;
-        int64_t val = ((int)lane_id() <= stop && idx >= 0) ? (int64_t)(word & kValueMask) : 0;
+        // the value field holds the low 62 bits of a signed sum: sign-extend it
+        int64_t val = ((int)lane_id() <= stop && idx >= 0) ? ((int64_t)(word << 2) >> 2) : 0;
         excl += warp_sum(val);
         if (prefix) done = true;
         else look -= 32;
@@ -307,9 +309,11 @@ extern "C" gcmfgh_status gcmfgh_exclusive_scan_i32_noalloc(const int32_t* d_in, 
     gcmfgh::scan_kernel<int32_t><<<(unsigned)tiles, gcmfgh::kScanThreads, 0, s>>>(
         d_in, d_out, n, d_total, reinterpret_cast<gcmfgh::ScanState*>(scratch), err);
     gcmfgh::note_launch();
+    // the launch's own status, taken right after it
+    if (cudaGetLastError() != cudaSuccess) return GCMFGH_CUDA_ERROR;
   }
   int h_err = 0;
   if (cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return GCMFGH_CUDA_ERROR;
-  if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return GCMFGH_CUDA_ERROR;
   return h_err ? GCMFGH_DEVICE_ERROR : GCMFGH_OK;
 }

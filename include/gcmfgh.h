@@ -249,6 +249,8 @@ gcmfgh_status gcmfgh_radix_sort_u64(gcmfgh_ctx* ctx, uint64_t* d_keys, uint32_t*
  * current device; stream is a cudaStream_t (NULL = legacy default stream).  The call
  * returns when the result is ready.  The first call on a device looks the scratch array's
  * address up (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * The looked-up address is kept for the life of the process, so cudaDeviceReset on a
+ * device after its first call here is not supported.  Input values may be negative.
  * All calls share the one array: calls that overlap on the GPU (other threads, other
  * streams of the same device) race and must be serialised by the caller. */
 #define GCMFGH_NOALLOC_SCAN_MAX_ELEMENTS (1LL << 24)

@@ -1,9 +1,9 @@
 """Regenerates the golden fixtures in tests/golden/ from the reference repository.
 
-Run in a container where the reference is mounted (its path below) and after
-`make -C oracle` has built oracle/_ref/ghclip_ref from the reference's own sources:
+Run where the reference's sources are present, after
+`make -C oracle REF_ROOT=<reference root>` has built oracle/_ref/ghclip_ref from them:
 
-    python tests/golden/make_goldens.py
+    GCMFGH_REFERENCE=<reference root> python tests/golden/make_goldens.py
 
 Writes
   figs/<Name>-P.poly, figs/<Name>-Q.poly   the reference's GH test inputs
@@ -26,7 +26,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("GCMFGH_REFERENCE", "/root/reference")
+REF = os.environ.get("GCMFGH_REFERENCE")
+if not REF:
+    sys.exit("set GCMFGH_REFERENCE to the directory that holds the reference's sources")
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "gcmf-gh_b200"))
 

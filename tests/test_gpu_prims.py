@@ -19,6 +19,18 @@ def test_exclusive_scan(engine, n):
     assert np.array_equal(out.cpu().numpy(), ref[:-1])
 
 
+@pytest.mark.parametrize("lo,hi", [(-1000, 0), (-2_000_000_000, 2_000_000_000)])
+def test_exclusive_scan_signed(engine, lo, hi):
+    """Negative tile aggregates and prefixes cross the look-back as signed values."""
+    import torch
+    rng = np.random.default_rng(7)
+    a = rng.integers(lo, hi, size=3_000_017).astype(np.int32)
+    out, tot = engine.exclusive_scan_i32(torch.from_numpy(a).cuda())
+    ref = np.concatenate([[0], np.cumsum(a, dtype=np.int64)])
+    assert tot == int(ref[-1])
+    assert np.array_equal(out.cpu().numpy(), ref[:-1])
+
+
 def test_exclusive_scan_large_values(engine):
     import torch
     a = np.full(5_000_000, 2_000_000_000, dtype=np.int32)

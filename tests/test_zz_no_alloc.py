@@ -41,8 +41,10 @@ def test_noalloc_scan_equals_allocating_scan_twice():
         rng = np.random.default_rng(1234)
         # two calls in a row; the second is smaller, so stale status words of the first
         # call would corrupt it if the scratch were not cleared
-        for n in (3_000_017, 1_234_567):
-            a = torch.from_numpy(rng.integers(-1000, 100000, size=n).astype(np.int32)).cuda()
+        # the third call is all negative, so every tile aggregate and running prefix
+        # that the look-back passes between tiles is negative
+        for n, lo, hi in ((3_000_017, -1000, 100000), (1_234_567, -1000, 100000), (3_000_017, -1000, 0)):
+            a = torch.from_numpy(rng.integers(lo, hi, size=n).astype(np.int32)).cuda()
             ref = torch.empty(n, dtype=torch.int64, device="cuda")
             ref_total = ctypes.c_int64()
             assert L.gcmfgh_exclusive_scan_i32(ctx, ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(ref.data_ptr()),
