@@ -74,9 +74,12 @@ def coord_to_mbr(tok: str) -> int:
     return sign * num + 9000000000000000
 
 
-def read_text_layer(path):
-    """Returns (coords (V,2), vnum, ids) of the stored polygons."""
-    coords, vnum, ids = [], [], []
+def read_text_layer(path, with_mbrs=False):
+    """Returns (coords (V,2), vnum, ids) of the stored polygons; with_mbrs adds the
+    reader's two MBR forms per polygon (SEQ_Overlay.h:327-334): the decimal keys
+    CoordToMBR(token) (n,4) uint64 and atof(token) (n,4) float64, both over the header
+    pairs and the vertices, in (x1, y1, x2, y2) order."""
+    coords, vnum, ids, keys, mbrs = [], [], [], [], []
     with open(path) as f:
         content = f.read()
     lines = re.findall(r"[^\n]*\n|[^\n]+$", content)  # fgets: each line with its newline
@@ -111,4 +114,9 @@ def read_text_layer(path):
         coords.extend(body)
         vnum.append(len(body))
         ids.append(int(pid))
-    return np.array(coords, np.float64).reshape(-1, 2), np.array(vnum, np.int32), np.array(ids, np.int64)
+        keys.append([coord_to_mbr(t) for t in (cx1, cy1, cx2, cy2)])
+        mbrs.append([_atof(t) for t in (cx1, cy1, cx2, cy2)])
+    out = (np.array(coords, np.float64).reshape(-1, 2), np.array(vnum, np.int32), np.array(ids, np.int64))
+    if with_mbrs:
+        out += (np.array(keys, np.uint64).reshape(-1, 4), np.array(mbrs, np.float64).reshape(-1, 4))
+    return out

@@ -114,3 +114,26 @@ def test_host_entry_point_equals_device_path(engine):
     ji2, ci2 = engine.join_clip_host(base, ovl)
     assert ji == ji2 and ci == ci2
     assert np.array_equal(engine.clip_field("xy"), xy)
+
+
+@pytest.mark.parametrize("name", ["small_join", "dense"])
+def test_join_matches_reference_gpu_join(engine, name, tmp_path):
+    """The engine's join on the layers of tests/golden/join_ref_<name>.npz (read through
+    the engine's text reader) against the reference's own GPU join stages run on the
+    same text: candidates, common MBRs, containment, edge-filter counts, refine flags."""
+    import os
+    import gcmfgh
+    from conftest import GOLDEN
+    from golden import make_join_goldens as mjg
+    fx = np.load(os.path.join(GOLDEN, f"join_ref_{name}.npz"))
+    if "gpu_jxy" not in fx.files:
+        pytest.skip("fixture made without the reference's GPU stages")
+    pb, po = mjg.write_case_text(name, str(tmp_path))
+    assert mjg.sha256(pb) == str(fx["text_sha_b"]) and mjg.sha256(po) == str(fx["text_sha_o"])
+    base, _ = gcmfgh.read_text_layer(pb)
+    ovl, _ = gcmfgh.read_text_layer(po)
+    engine.join(gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl))
+    r = mjg.reference_join_by_pair(fx)
+    for f in ("b", "o", "pip_type", "pip_flag", "join_flag", "bE", "oE", "seg_flag"):
+        assert np.array_equal(engine.join_field(f).astype(np.int64), r[f].astype(np.int64)), f
+    assert np.array_equal(engine.join_field("cmbr").reshape(-1, 4), r["cmbr"])
