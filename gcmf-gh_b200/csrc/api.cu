@@ -31,33 +31,40 @@ unsigned long long& launch_counter() {
 
 void* Arena::take(size_t bytes) {
   bytes = (bytes + 255) & ~size_t(255);
-  while (cur_ < chunks_.size()) {
-    Chunk& c = chunks_[cur_];
+  for (auto& c : chunks_) {                       // first fit: earlier chunks' leftover room too
     if (c.off + bytes <= c.cap) {
       void* p = c.base + c.off;
       c.off += bytes;
       return p;
     }
-    ++cur_;
   }
-  size_t last = chunks_.empty() ? 0 : chunks_.back().cap;
+  size_t last = 0;
+  for (auto& c : chunks_) last = c.cap > last ? c.cap : last;
   size_t cap = bytes > 2 * last ? bytes : 2 * last;
   if (cap < (size_t(64) << 20)) cap = size_t(64) << 20;
   char* p = nullptr;
   if (cudaMalloc(&p, cap) != cudaSuccess) {
     cudaGetLastError();
-    cap = bytes;                                  // retry with the exact size
+    // Chunks not touched since the last reset() hold nothing: give them back (cudaFree
+    // waits for the device), then retry with the exact size.
+    for (size_t i = 0; i < chunks_.size();) {
+      if (chunks_[i].off == 0) {
+        cudaFree(chunks_[i].base);
+        chunks_.erase(chunks_.begin() + (std::ptrdiff_t)i);
+      } else {
+        ++i;
+      }
+    }
+    cap = bytes;
     if (cudaMalloc(&p, cap) != cudaSuccess) { cudaGetLastError(); return nullptr; }
   }
   chunks_.push_back({p, cap, bytes});
-  cur_ = chunks_.size() - 1;
   return p;
 }
 
 void Arena::release() {
   for (auto& c : chunks_) cudaFree(c.base);
   chunks_.clear();
-  cur_ = 0;
 }
 
 namespace {

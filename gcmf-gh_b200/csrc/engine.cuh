@@ -21,12 +21,12 @@ enum Status : int {
 };
 
 // Bump allocator over device chunks.  Chunks are kept across calls and reused after
-// reset(); a request that does not fit opens a new chunk (cudaMalloc), so pointers
-// handed out since the last reset() stay valid.
+// reset(); a request goes to the first chunk with room, else opens a new chunk
+// (cudaMalloc), so pointers handed out since the last reset() stay valid.
 class Arena {
  public:
   ~Arena() { release(); }
-  void reset() { cur_ = 0; if (!chunks_.empty()) chunks_[0].off = 0; for (auto& c : chunks_) c.off = 0; }
+  void reset() { for (auto& c : chunks_) c.off = 0; }
   void* take(size_t bytes);           // nullptr on allocation failure
   template <class T> T* take_n(int64_t n) { return static_cast<T*>(take(sizeof(T) * (size_t)(n > 0 ? n : 1))); }
   void release();
@@ -34,7 +34,6 @@ class Arena {
  private:
   struct Chunk { char* base; size_t cap; size_t off; };
   std::vector<Chunk> chunks_;
-  size_t cur_ = 0;
 };
 
 // A polygon layer in the reference's join layout, device pointers:

@@ -466,18 +466,67 @@ __global__ void edge_slots_kernel(const int64_t* __restrict__ insBase, int64_t n
   if (e < nE) vpos[e] = e + insBase[e];
 }
 
+// The merged rings of one side live in one buffer of n slots, column by column:
+//   xy (double2) | nx pv nb (int32) | tn tl to ls (int32) | it lb ee fl (byte)
+// 48 bytes per slot.  A ring is then the buffer, n and its first slot: a thread that
+// walks a pair keeps three words per ring instead of a pointer per column, and each
+// column stays dense for the scans over one field.
+//   nx, pv, nb  next, previous, neighbour (slot on the other ring, -1 none)
+//   tn tl to ls tracing scratch: next run start (other ring), run length, output offset,
+//               and (by list index) the slots of the flagged vertices
+//   it          intersection flag (cleared when visited by the trace)
+//   lb, ee      IntersectionLabel, EntryExitLabel
+//   fl          bit0 split candidate, bit1 crossing candidate
+#define GCMFGH_RING_COLUMNS(IDX)                                                                   \
+  __device__ __forceinline__ double2& xy(int64_t i) const { return reinterpret_cast<double2*>(b)[IDX]; } \
+  __device__ __forceinline__ double& x(int64_t i) const { return xy(i).x; }                         \
+  __device__ __forceinline__ double& y(int64_t i) const { return xy(i).y; }                         \
+  __device__ __forceinline__ int32_t& nx(int64_t i) const { return reinterpret_cast<int32_t*>(b + 16 * n)[IDX]; } \
+  __device__ __forceinline__ int32_t& pv(int64_t i) const { return reinterpret_cast<int32_t*>(b + 20 * n)[IDX]; } \
+  __device__ __forceinline__ int32_t& nb(int64_t i) const { return reinterpret_cast<int32_t*>(b + 24 * n)[IDX]; } \
+  __device__ __forceinline__ int32_t& tn(int64_t i) const { return reinterpret_cast<int32_t*>(b + 28 * n)[IDX]; } \
+  __device__ __forceinline__ int32_t& tl(int64_t i) const { return reinterpret_cast<int32_t*>(b + 32 * n)[IDX]; } \
+  __device__ __forceinline__ int32_t& to(int64_t i) const { return reinterpret_cast<int32_t*>(b + 36 * n)[IDX]; } \
+  __device__ __forceinline__ int32_t& ls(int64_t i) const { return reinterpret_cast<int32_t*>(b + 40 * n)[IDX]; } \
+  __device__ __forceinline__ uint8_t& it(int64_t i) const { return reinterpret_cast<uint8_t*>(b + 44 * n)[IDX]; } \
+  __device__ __forceinline__ int8_t& lb(int64_t i) const { return reinterpret_cast<int8_t*>(b + 45 * n)[IDX]; } \
+  __device__ __forceinline__ int8_t& ee(int64_t i) const { return reinterpret_cast<int8_t*>(b + 46 * n)[IDX]; } \
+  __device__ __forceinline__ uint8_t& fl(int64_t i) const { return reinterpret_cast<uint8_t*>(b + 47 * n)[IDX]; }
+
+constexpr int64_t kRingSlotBytes = 48;
+
+// Kernels that take a RingSet by value keep its column pointers in the parameter space,
+// so the side-wide kernels (fill, links, export, grid path) index columns directly.
 struct RingSet {
-  double* x; double* y;
-  int32_t* nx; int32_t* pv; int32_t* nb;
-  uint8_t* it;      // intersection flag (cleared when visited by the trace)
-  int8_t* lb;       // IntersectionLabel
-  int8_t* ee;       // EntryExitLabel
-  uint8_t* fl;      // bit0 split candidate, bit1 crossing candidate
-  int32_t* tn;      // tracing scratch: next run start (other ring), run length, output
-  int32_t* tl;      //   offset, and the slots of the flagged vertices in ring order
-  int32_t* to;
-  int32_t* ls;
+  char* b;          // column buffer
+  int64_t n;        // slots per column (a multiple of 16, so every column stays aligned)
   int exact;        // orientation signs exact (ClipParams::exact)
+  double2* cxy; int32_t* cnx; int32_t* cpv; int32_t* cnb; int32_t* ctn; int32_t* ctl; int32_t* cto; int32_t* cls;
+  uint8_t* cit; int8_t* clb; int8_t* cee; uint8_t* cfl;
+  void set(char* buf, int64_t slots) {
+    b = buf; n = slots;
+    cxy = reinterpret_cast<double2*>(b);
+    cnx = reinterpret_cast<int32_t*>(b + 16 * n); cpv = reinterpret_cast<int32_t*>(b + 20 * n);
+    cnb = reinterpret_cast<int32_t*>(b + 24 * n); ctn = reinterpret_cast<int32_t*>(b + 28 * n);
+    ctl = reinterpret_cast<int32_t*>(b + 32 * n); cto = reinterpret_cast<int32_t*>(b + 36 * n);
+    cls = reinterpret_cast<int32_t*>(b + 40 * n); cit = reinterpret_cast<uint8_t*>(b + 44 * n);
+    clb = reinterpret_cast<int8_t*>(b + 45 * n); cee = reinterpret_cast<int8_t*>(b + 46 * n);
+    cfl = reinterpret_cast<uint8_t*>(b + 47 * n);
+  }
+  __device__ __forceinline__ double2& xy(int64_t i) const { return cxy[i]; }
+  __device__ __forceinline__ double& x(int64_t i) const { return cxy[i].x; }
+  __device__ __forceinline__ double& y(int64_t i) const { return cxy[i].y; }
+  __device__ __forceinline__ int32_t& nx(int64_t i) const { return cnx[i]; }
+  __device__ __forceinline__ int32_t& pv(int64_t i) const { return cpv[i]; }
+  __device__ __forceinline__ int32_t& nb(int64_t i) const { return cnb[i]; }
+  __device__ __forceinline__ int32_t& tn(int64_t i) const { return ctn[i]; }
+  __device__ __forceinline__ int32_t& tl(int64_t i) const { return ctl[i]; }
+  __device__ __forceinline__ int32_t& to(int64_t i) const { return cto[i]; }
+  __device__ __forceinline__ int32_t& ls(int64_t i) const { return cls[i]; }
+  __device__ __forceinline__ uint8_t& it(int64_t i) const { return cit[i]; }
+  __device__ __forceinline__ int8_t& lb(int64_t i) const { return clb[i]; }
+  __device__ __forceinline__ int8_t& ee(int64_t i) const { return cee[i]; }
+  __device__ __forceinline__ uint8_t& fl(int64_t i) const { return cfl[i]; }
 };
 
 // per pair: ring size, region offset (ring + room for added vertices)
@@ -535,9 +584,9 @@ __device__ __forceinline__ void write_inserted(const EdgeFill& f, const Records&
   }
   int sl = f.s0 + 1 + i;
   int64_t gs = f.base + sl;
-  S.x[gs] = X; S.y[gs] = Y;
-  S.nx[gs] = (sl + 1) % f.mm; S.pv[gs] = (sl + f.mm - 1) % f.mm; S.nb[gs] = -1;
-  S.it[gs] = 0; S.lb[gs] = L_NONE; S.ee[gs] = E_NEITHER; S.fl[gs] = 0;
+  S.x(gs) = X; S.y(gs) = Y;
+  S.nx(gs) = (sl + 1) % f.mm; S.pv(gs) = (sl + f.mm - 1) % f.mm; S.nb(gs) = -1;
+  S.it(gs) = 0; S.lb(gs) = L_NONE; S.ee(gs) = E_NEITHER; S.fl(gs) = 0;
   slotOfRec[r] = sl;
 }
 
@@ -577,9 +626,9 @@ __global__ void __launch_bounds__(kThreads, 4) ring_fill_kernel(LayerDev Lb, Lay
   const int le = (int)(e - eoff[f.k]);
   const double2 A = __ldg((kSide == 0 ? f.pvx : f.qvx) + le);
   const int64_t g = f.base + f.s0;
-  S.x[g] = A.x; S.y[g] = A.y;
-  S.nx[g] = (f.s0 + 1) % f.mm; S.pv[g] = (f.s0 + f.mm - 1) % f.mm; S.nb[g] = -1;
-  S.it[g] = 0; S.lb[g] = L_NONE; S.ee[g] = E_NEITHER; S.fl[g] = 0;
+  S.x(g) = A.x; S.y(g) = A.y;
+  S.nx(g) = (f.s0 + 1) % f.mm; S.pv(g) = (f.s0 + f.mm - 1) % f.mm; S.nb(g) = -1;
+  S.it(g) = 0; S.lb(g) = L_NONE; S.ee(g) = E_NEITHER; S.fl(g) = 0;
   // inserted records of this edge, gathered by record_scatter_kernel into insList
   const int64_t l0 = insCursorBase[e];
   const int cnt = insCursor[e];
@@ -698,8 +747,8 @@ __global__ void record_scatter_kernel(Records R, int64_t nR, const int64_t* __re
 
 // ---------------------------------------------------------------- G6 links
 __device__ __forceinline__ void set_link(RingSet& S, int64_t base, int slot, int target) {
-  S.nb[base + slot] = target;
-  S.it[base + slot] = 1;
+  S.nb(base + slot) = target;
+  S.it(base + slot) = 1;
 }
 
 __global__ void link_kernel(Records R, int64_t nR, const int32_t* __restrict__ status,
@@ -729,31 +778,31 @@ __global__ void link_kernel(Records R, int64_t nR, const int32_t* __restrict__ s
     case 2: case 6: {
       int sq = (int)slotQ[r];
       set_link(SQ, bQ, sq, srcP);
-      SP.it[bP + srcP] = 1;
-      if (winP) SP.nb[bP + srcP] = sq;
+      SP.it(bP + srcP) = 1;
+      if (winP) SP.nb(bP + srcP) = sq;
       break;
     }
     case 3: case 7: {
       int sp = (int)slotP[r];
       set_link(SP, bP, sp, srcQ);
-      SQ.it[bQ + srcQ] = 1;
-      if (winQ) SQ.nb[bQ + srcQ] = sp;
+      SQ.it(bQ + srcQ) = 1;
+      if (winQ) SQ.nb(bQ + srcQ) = sp;
       break;
     }
     case 4: case 8: {
-      SP.it[bP + srcP] = 1; SQ.it[bQ + srcQ] = 1;
-      if (winP) SP.nb[bP + srcP] = srcQ;
-      if (winQ) SQ.nb[bQ + srcQ] = srcP;
+      SP.it(bP + srcP) = 1; SQ.it(bQ + srcQ) = 1;
+      if (winP) SP.nb(bP + srcP) = srcQ;
+      if (winQ) SQ.nb(bQ + srcQ) = srcP;
       break;
     }
     case 5: {
       int sp = (int)slotP[r], sq = (int)slotQ[r];
       set_link(SQ, bQ, sq, srcP);
-      SP.it[bP + srcP] = 1;
-      if (winP) SP.nb[bP + srcP] = sq;
+      SP.it(bP + srcP) = 1;
+      if (winP) SP.nb(bP + srcP) = sq;
       set_link(SP, bP, sp, srcQ);
-      SQ.it[bQ + srcQ] = 1;
-      if (winQ) SQ.nb[bQ + srcQ] = sp;
+      SQ.it(bQ + srcQ) = 1;
+      if (winQ) SQ.nb(bQ + srcQ) = sp;
       break;
     }
   }
@@ -815,9 +864,9 @@ __device__ int export_rel(int exact, int pMN, int pPN, int qId, const RingSet& S
                           const RingSet& SP, int64_t bP, int p1, int p2, int p3) {
   if (pMN != -100 && pMN == qId) return R_IS_P_M;
   if (pPN != -100 && pPN == qId) return R_IS_P_P;
-  const double qx = SQ.x[bQ + qId], qy = SQ.y[bQ + qId];
-  const double x1 = SP.x[bP + p1], y1 = SP.y[bP + p1], x2 = SP.x[bP + p2], y2 = SP.y[bP + p2];
-  const double x3 = SP.x[bP + p3], y3 = SP.y[bP + p3];
+  const double qx = SQ.x(bQ + qId), qy = SQ.y(bQ + qId);
+  const double x1 = SP.x(bP + p1), y1 = SP.y(bP + p1), x2 = SP.x(bP + p2), y2 = SP.y(bP + p2);
+  const double x3 = SP.x(bP + p3), y3 = SP.y(bP + p3);
   const int s1 = orient_sign(exact, qx, qy, x1, y1, x2, y2);
   const int s2 = orient_sign(exact, qx, qy, x2, y2, x3, y3);
   const int s3 = orient_sign(exact, x1, y1, x2, y2, x3, y3);
@@ -857,26 +906,26 @@ __global__ void export_ring_kernel(int64_t K, const int32_t* __restrict__ status
   const int64_t bP = regP[k], bQ = regQ[k];
   for (int s = threadIdx.x; s < np; s += blockDim.x) {
     const int64_t g = bP + s;
-    xyP[2 * g] = SP.x[g]; xyP[2 * g + 1] = SP.y[g];
+    xyP[2 * g] = SP.x(g); xyP[2 * g + 1] = SP.y(g);
     alP[g] = unpack_key(keyP[g]);
     lbP[g] = -100;
-    nbP[g] = SP.nb[g] + 1;
+    nbP[g] = SP.nb(g) + 1;
   }
   for (int s = threadIdx.x; s < nq; s += blockDim.x) {
     const int64_t g = bQ + s;
-    xyQ[2 * g] = SQ.x[g]; xyQ[2 * g + 1] = SQ.y[g];
+    xyQ[2 * g] = SQ.x(g); xyQ[2 * g + 1] = SQ.y(g);
     alQ[g] = unpack_key(keyQ[g]);
     lbQ[g] = -100;
-    nbQ[g] = SQ.nb[g] + 1;
+    nbQ[g] = SQ.nb(g) + 1;
   }
   __syncthreads();
   for (int s = threadIdx.x; s < np; s += blockDim.x) {
     if (keyP[bP + s] == 0) continue;
-    const int nId = SP.nb[bP + s];
+    const int nId = SP.nb(bP + s);
     if (nId < 0 || nId >= nq) continue;
     const int pm = s > 0 ? s - 1 : np - 1, pp = s + 1 < np ? s + 1 : 0;
-    const int pMN = keyP[bP + pm] != 0 ? SP.nb[bP + pm] : -100;
-    const int pPN = keyP[bP + pp] != 0 ? SP.nb[bP + pp] : -100;
+    const int pMN = keyP[bP + pm] != 0 ? SP.nb(bP + pm) : -100;
+    const int pPN = keyP[bP + pp] != 0 ? SP.nb(bP + pp) : -100;
     const int qm = nId > 0 ? nId - 1 : nq - 1, qp = nId + 1 < nq ? nId + 1 : 0;
     const int a = export_rel(SP.exact, pMN, pPN, qm, SQ, bQ, SP, bP, pm, s, pp);
     const int b = export_rel(SP.exact, pMN, pPN, qp, SQ, bQ, SP, bP, pm, s, pp);
@@ -888,20 +937,18 @@ __global__ void export_ring_kernel(int64_t K, const int32_t* __restrict__ status
 
 // ---------------------------------------------------------------- G7 label + trace
 struct Ring {
-  double* x; double* y; int32_t* nx; int32_t* pv; int32_t* nb;
-  uint8_t* it; int8_t* lb; int8_t* ee; uint8_t* fl;
-  int32_t* tn; int32_t* tl; int32_t* to; int32_t* ls;
+  char* b; int64_t n;   // the side's column buffer (RingSet)
+  int64_t o;            // first slot of this ring
   int m;        // slots in the merged ring
   int used;     // slots in use (ring + added vertices)
   int cap;      // region capacity
   int exact;    // orientation signs exact
+  GCMFGH_RING_COLUMNS(o + i)
 };
 
 __device__ __forceinline__ Ring ring_of(const RingSet& S, int64_t base, int m, int cap) {
   Ring r;
-  r.x = S.x + base; r.y = S.y + base; r.nx = S.nx + base; r.pv = S.pv + base; r.nb = S.nb + base;
-  r.it = S.it + base; r.lb = S.lb + base; r.ee = S.ee + base; r.fl = S.fl + base;
-  r.tn = S.tn + base; r.tl = S.tl + base; r.to = S.to + base; r.ls = S.ls + base;
+  r.b = S.b; r.n = S.n; r.o = base;
   r.m = m; r.used = m; r.cap = cap; r.exact = S.exact;
   return r;
 }
@@ -909,14 +956,14 @@ __device__ __forceinline__ Ring ring_of(const RingSet& S, int64_t base, int m, i
 __device__ int add_vertex(Ring& R, double X, double Y) {
   if (R.used >= R.cap) return -1;
   int v = R.used++;
-  R.x[v] = X; R.y[v] = Y; R.nx[v] = v; R.pv[v] = v; R.nb[v] = -1;
-  R.it[v] = 0; R.lb[v] = L_NONE; R.ee[v] = E_NEITHER; R.fl[v] = 0;
+  R.x(v) = X; R.y(v) = Y; R.nx(v) = v; R.pv(v) = v; R.nb(v) = -1;
+  R.it(v) = 0; R.lb(v) = L_NONE; R.ee(v) = E_NEITHER; R.fl(v) = 0;
   return v;
 }
 
 __device__ __forceinline__ void insert_after(Ring& R, int v, int after) {
-  int c = R.nx[after];
-  R.nx[R.pv[c]] = v; R.pv[v] = R.pv[c]; R.nx[v] = c; R.pv[c] = v;
+  int c = R.nx(after);
+  R.nx(R.pv(c)) = v; R.pv(v) = R.pv(c); R.nx(v) = c; R.pv(c) = v;
 }
 
 // polygon.h:427-448 (winding parity) over the ring reached from slot 0, skipping `skip`
@@ -926,9 +973,9 @@ __device__ bool point_in_ring(const Ring& R, double Rx, double Ry, int skip) {
   int one = 0;
   int guard = R.used + 2;
   do {
-    int two = R.nx[one];
-    if (two == skip) two = R.nx[two];
-    double P0x = R.x[one], P0y = R.y[one], P1x = R.x[two], P1y = R.y[two];
+    int two = R.nx(one);
+    if (two == skip) two = R.nx(two);
+    double P0x = R.x(one), P0y = R.y(one), P1x = R.x(two), P1y = R.y(two);
     if ((P0y < Ry) != (P1y < Ry)) {
       if (P0x >= Rx) {
         if (P1x > Rx) w = w + 2 * (P1y > P0y) - 1;
@@ -945,12 +992,12 @@ __device__ bool point_in_ring(const Ring& R, double Rx, double Ry, int skip) {
 // relative position of Q w.r.t. the chain (P1, P2, P3): polyclip.h:297-326
 template <int EX>
 __device__ int rel_position(const Ring& P, const Ring& Q, int qv, int p1, int p2, int p3) {
-  if (P.it[p1] && P.nb[p1] == qv) return R_IS_P_M;
-  if (P.it[p3] && P.nb[p3] == qv) return R_IS_P_P;
+  if (P.it(p1) && P.nb(p1) == qv) return R_IS_P_M;
+  if (P.it(p3) && P.nb(p3) == qv) return R_IS_P_P;
   const int ex = EX;
-  int s1 = orient_sign(ex, Q.x[qv], Q.y[qv], P.x[p1], P.y[p1], P.x[p2], P.y[p2]);
-  int s2 = orient_sign(ex, Q.x[qv], Q.y[qv], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
-  int s3 = orient_sign(ex, P.x[p1], P.y[p1], P.x[p2], P.y[p2], P.x[p3], P.y[p3]);
+  int s1 = orient_sign(ex, Q.x(qv), Q.y(qv), P.x(p1), P.y(p1), P.x(p2), P.y(p2));
+  int s2 = orient_sign(ex, Q.x(qv), Q.y(qv), P.x(p2), P.y(p2), P.x(p3), P.y(p3));
+  int s3 = orient_sign(ex, P.x(p1), P.y(p1), P.x(p2), P.y(p2), P.x(p3), P.y(p3));
   if (s3 > 0) return (s1 > 0 && s2 > 0) ? R_LEFT : R_RIGHT;
   return (s1 < 0 && s2 < 0) ? R_RIGHT : R_LEFT;
 }
@@ -990,12 +1037,12 @@ struct OutRegion {
 __device__ int first_non_intersection(const Ring& A, const Ring& B, bool& midpoint) {
   midpoint = false;
   int v = 0, guard = A.used + 1;
-  do { if (!A.it[v]) return v; v = A.nx[v]; } while (v != 0 && --guard > 0);
+  do { if (!A.it(v)) return v; v = A.nx(v); } while (v != 0 && --guard > 0);
   v = 0; guard = A.used + 1;
   do {
-    int nb = A.nb[v], nx = A.nx[v];
-    if (nb >= 0 && A.nb[nx] != B.pv[nb] && A.nb[nx] != B.nx[nb]) { midpoint = true; return v; }
-    v = A.nx[v];
+    int nb = A.nb(v), nx = A.nx(v);
+    if (nb >= 0 && A.nb(nx) != B.pv(nb) && A.nb(nx) != B.nx(nb)) { midpoint = true; return v; }
+    v = A.nx(v);
   } while (v != 0 && --guard > 0);
   return -1;
 }
@@ -1003,7 +1050,7 @@ __device__ int first_non_intersection(const Ring& A, const Ring& B, bool& midpoi
 __device__ void push_ring(OutRegion& O, const Ring& A) {
   O.begin();
   int v = 0, guard = A.used + 1;
-  do { O.push(A.x[v], A.y[v]); v = A.nx[v]; } while (v != 0 && --guard > 0);
+  do { O.push(A.x(v), A.y(v)); v = A.nx(v); } while (v != 0 && --guard > 0);
   O.end();
 }
 
@@ -1039,14 +1086,14 @@ __device__ void seq_step1(PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
   for (int s = 0; s < P.m; ++s) {
-    if (!P.it[s]) continue;
-    int nb = P.nb[s];
+    if (!P.it(s)) continue;
+    int nb = P.nb(s);
     if (nb < 0) continue;
-    int pm = P.pv[s], pp = P.nx[s];
-    int a = rel_position<EX>(P, Q, Q.pv[nb], pm, s, pp);
-    int b = rel_position<EX>(P, Q, Q.nx[nb], pm, s, pp);
+    int pm = P.pv(s), pp = P.nx(s);
+    int a = rel_position<EX>(P, Q, Q.pv(nb), pm, s, pp);
+    int b = rel_position<EX>(P, Q, Q.nx(nb), pm, s, pp);
     int8_t L = initial_label(a, b);
-    if (L != L_NONE) { P.lb[s] = L; Q.lb[nb] = L; }
+    if (L != L_NONE) { P.lb(s) = L; Q.lb(nb) = L; }
   }
 }
 
@@ -1055,19 +1102,19 @@ __device__ void seq_step2(PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
   for (int s = 0; s < P.m; ++s) {
-    if (!P.it[s] || (P.lb[s] != L_LEFT_ON && P.lb[s] != L_RIGHT_ON)) continue;
-    int x = P.lb[s] == L_LEFT_ON ? R_LEFT : R_RIGHT;
+    if (!P.it(s) || (P.lb(s) != L_LEFT_ON && P.lb(s) != L_RIGHT_ON)) continue;
+    int x = P.lb(s) == L_LEFT_ON ? R_LEFT : R_RIGHT;
     int X = s, I = s, guard = P.m + 1;
     do {
-      P.lb[I] = L_NONE;
-      if (P.nb[I] >= 0) Q.lb[P.nb[I]] = L_NONE;
-      I = P.nx[I];
-    } while (P.lb[I] == L_ON_ON && --guard > 0);
-    int y = P.lb[I] == L_ON_LEFT ? R_LEFT : R_RIGHT;
+      P.lb(I) = L_NONE;
+      if (P.nb(I) >= 0) Q.lb(P.nb(I)) = L_NONE;
+      I = P.nx(I);
+    } while (P.lb(I) == L_ON_ON && --guard > 0);
+    int y = P.lb(I) == L_ON_LEFT ? R_LEFT : R_RIGHT;
     int8_t ct = (x != y) ? L_DELAYED_CROSSING : L_DELAYED_BOUNCING;
-    P.lb[X] = ct; P.lb[I] = ct;
-    if (P.nb[X] >= 0) Q.lb[P.nb[X]] = ct;
-    if (P.nb[I] >= 0) Q.lb[P.nb[I]] = ct;
+    P.lb(X) = ct; P.lb(I) = ct;
+    if (P.nb(X) >= 0) Q.lb(P.nb(X)) = ct;
+    if (P.nb(I) >= 0) Q.lb(P.nb(I)) = ct;
   }
 }
 
@@ -1078,9 +1125,9 @@ __device__ void seq_step35(PairCtx& c) {
     Ring& A = c.R[sd];
     bool none = true, allOn = true;
     for (int v = 0; v < A.m; ++v) {
-      int8_t l = A.lb[v];
+      int8_t l = A.lb(v);
       if (l != L_ON_ON) allOn = false;
-      if (A.it[v]) {
+      if (A.it(v)) {
         if (l == L_CROSSING || l == L_DELAYED_CROSSING) none = false;
         if (c.uni && (l == L_BOUNCING || l == L_DELAYED_BOUNCING)) none = false;
       }
@@ -1095,8 +1142,8 @@ __device__ void seq_step35(PairCtx& c) {
     bool mid;
     int v = first_non_intersection(A, B, mid);
     if (v < 0) continue;
-    double px = A.x[v], py = A.y[v];
-    if (mid) { int n = A.nx[v]; px = 0.5 * (A.x[v] + A.x[n]); py = 0.5 * (A.y[v] + A.y[n]); }
+    double px = A.x(v), py = A.y(v);
+    if (mid) { int n = A.nx(v); px = 0.5 * (A.x(v) + A.x(n)); py = 0.5 * (A.y(v) + A.y(n)); }
     bool inside = point_in_ring<EX>(B, px, py, -1);
     if (inside ^ c.uni) push_ring(c.O, A);
   }
@@ -1114,38 +1161,38 @@ __device__ bool seq_step4(PairCtx& c) {
     int V = first_non_intersection(A, B, mid);
     if (V < 0) continue;
     if (mid) {
-      int n = A.nx[V];
-      int T = add_vertex(A, 0.5 * (A.x[V] + A.x[n]), 0.5 * (A.y[V] + A.y[n]));
+      int n = A.nx(V);
+      int T = add_vertex(A, 0.5 * (A.x(V) + A.x(n)), 0.5 * (A.y(V) + A.y(n)));
       if (T < 0) { fail(c, DEV_CAPACITY); return false; }
       insert_after(A, T, V);
       V = T;
     }
     // the Q pass sees P's temporary vertex; P's pass cannot see Q's (not yet added)
-    int8_t st = point_in_ring<EX>(B, A.x[V], A.y[V], -1) ? E_EXIT : E_ENTRY;
+    int8_t st = point_in_ring<EX>(B, A.x(V), A.y(V), -1) ? E_EXIT : E_ENTRY;
     bool first = true;
-    int I = A.nx[V], guard = A.used + 1;
+    int I = A.nx(V), guard = A.used + 1;
     while (I != V && --guard > 0) {
-      if (A.it[I]) {
-        int8_t l = A.lb[I];
-        if (l == L_CROSSING) { A.ee[I] = st; st = toggled(st); }
-        if (A.lb[I] == L_BOUNCING && ((st == E_EXIT) ^ c.uni)) A.fl[I] |= 1;
-        if (A.lb[I] == L_DELAYED_CROSSING) {
-          A.ee[I] = st;
-          if (first) { if ((st == E_EXIT) ^ c.uni) A.lb[I] = L_CROSSING; first = false; }
+      if (A.it(I)) {
+        int8_t l = A.lb(I);
+        if (l == L_CROSSING) { A.ee(I) = st; st = toggled(st); }
+        if (A.lb(I) == L_BOUNCING && ((st == E_EXIT) ^ c.uni)) A.fl(I) |= 1;
+        if (A.lb(I) == L_DELAYED_CROSSING) {
+          A.ee(I) = st;
+          if (first) { if ((st == E_EXIT) ^ c.uni) A.lb(I) = L_CROSSING; first = false; }
           else {
-            if ((st == E_ENTRY) ^ c.uni) A.lb[I] = L_CROSSING;
+            if ((st == E_ENTRY) ^ c.uni) A.lb(I) = L_CROSSING;
             first = true;
             st = toggled(st);
           }
         }
-        if (A.lb[I] == L_DELAYED_BOUNCING) {
-          A.ee[I] = st;
-          if (first) { if ((st == E_EXIT) ^ c.uni) A.fl[I] |= 2; first = false; }
-          else { if ((st == E_ENTRY) ^ c.uni) A.fl[I] |= 2; first = true; }
+        if (A.lb(I) == L_DELAYED_BOUNCING) {
+          A.ee(I) = st;
+          if (first) { if ((st == E_EXIT) ^ c.uni) A.fl(I) |= 2; first = false; }
+          else { if ((st == E_ENTRY) ^ c.uni) A.fl(I) |= 2; first = true; }
           st = toggled(st);
         }
       }
-      I = A.nx[I];
+      I = A.nx(I);
     }
   }
   return true;
@@ -1158,32 +1205,32 @@ __device__ bool seq_step5(PairCtx& c) {
   Ring& Q = c.R[1];
   const int pm0 = P.used;
   for (int ip = 0; ip < pm0; ++ip) {
-    if (!(P.fl[ip] & 1)) continue;
-    int iq = P.nb[ip];
-    if (iq < 0 || !(Q.fl[iq] & 1)) continue;
-    int vp = add_vertex(P, P.x[ip], P.y[ip]);
-    int vq = add_vertex(Q, Q.x[iq], Q.y[iq]);
+    if (!(P.fl(ip) & 1)) continue;
+    int iq = P.nb(ip);
+    if (iq < 0 || !(Q.fl(iq) & 1)) continue;
+    int vp = add_vertex(P, P.x(ip), P.y(ip));
+    int vq = add_vertex(Q, Q.x(iq), Q.y(iq));
     if (vp < 0 || vq < 0) { fail(c, DEV_CAPACITY); return false; }
     bool same;
     if (EX) {
-      same = orient_exact_call(P.x[P.pv[ip]], P.y[P.pv[ip]], P.x[ip], P.y[ip], P.x[P.nx[ip]], P.y[P.nx[ip]]) *
-             orient_exact_call(Q.x[Q.pv[iq]], Q.y[Q.pv[iq]], Q.x[iq], Q.y[iq], Q.x[Q.nx[iq]], Q.y[Q.nx[iq]]) > 0;
+      same = orient_exact_call(P.x(P.pv(ip)), P.y(P.pv(ip)), P.x(ip), P.y(ip), P.x(P.nx(ip)), P.y(P.nx(ip))) *
+             orient_exact_call(Q.x(Q.pv(iq)), Q.y(Q.pv(iq)), Q.x(iq), Q.y(iq), Q.x(Q.nx(iq)), Q.y(Q.nx(iq))) > 0;
     } else {
-      double sP = area2(P.x[P.pv[ip]], P.y[P.pv[ip]], P.x[ip], P.y[ip], P.x[P.nx[ip]], P.y[P.nx[ip]]);
-      double sQ = area2(Q.x[Q.pv[iq]], Q.y[Q.pv[iq]], Q.x[iq], Q.y[iq], Q.x[Q.nx[iq]], Q.y[Q.nx[iq]]);
+      double sP = area2(P.x(P.pv(ip)), P.y(P.pv(ip)), P.x(ip), P.y(ip), P.x(P.nx(ip)), P.y(P.nx(ip)));
+      double sQ = area2(Q.x(Q.pv(iq)), Q.y(Q.pv(iq)), Q.x(iq), Q.y(iq), Q.x(Q.nx(iq)), Q.y(Q.nx(iq)));
       same = sP * sQ > 0;
     }
     if (same) {
-      P.nb[ip] = vq; Q.nb[vq] = ip; P.it[ip] = 1; Q.it[vq] = 1;
-      Q.nb[iq] = vp; P.nb[vp] = iq; Q.it[iq] = 1; P.it[vp] = 1;
+      P.nb(ip) = vq; Q.nb(vq) = ip; P.it(ip) = 1; Q.it(vq) = 1;
+      Q.nb(iq) = vp; P.nb(vp) = iq; Q.it(iq) = 1; P.it(vp) = 1;
     } else {
-      P.nb[vp] = vq; Q.nb[vq] = vp; P.it[vp] = 1; Q.it[vq] = 1;
+      P.nb(vp) = vq; Q.nb(vq) = vp; P.it(vp) = 1; Q.it(vq) = 1;
     }
     insert_after(P, vp, ip);
     insert_after(Q, vq, iq);
     int8_t e1 = c.uni ? E_ENTRY : E_EXIT, e2 = c.uni ? E_EXIT : E_ENTRY;
-    P.ee[ip] = e1; P.ee[vp] = e2; Q.ee[iq] = e1; Q.ee[vq] = e2;
-    P.lb[ip] = L_CROSSING; P.lb[vp] = L_CROSSING; Q.lb[iq] = L_CROSSING; Q.lb[vq] = L_CROSSING;
+    P.ee(ip) = e1; P.ee(vp) = e2; Q.ee(iq) = e1; Q.ee(vq) = e2;
+    P.lb(ip) = L_CROSSING; P.lb(vp) = L_CROSSING; Q.lb(iq) = L_CROSSING; Q.lb(vq) = L_CROSSING;
   }
   return true;
 }
@@ -1193,9 +1240,9 @@ __device__ void seq_step6(PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
   for (int ip = 0; ip < P.m; ++ip) {
-    if (!(P.fl[ip] & 2)) continue;
-    int iq = P.nb[ip];
-    if (iq >= 0 && (Q.fl[iq] & 2)) { P.lb[ip] = L_CROSSING; Q.lb[iq] = L_CROSSING; }
+    if (!(P.fl(ip) & 2)) continue;
+    int iq = P.nb(ip);
+    if (iq >= 0 && (Q.fl(iq) & 2)) { P.lb(ip) = L_CROSSING; Q.lb(iq) = L_CROSSING; }
   }
 }
 
@@ -1206,36 +1253,36 @@ __device__ bool seq_trace(PairCtx& c) {
   OutRegion& O = c.O;
   long long budget = 4ll * (c.R[0].used + c.R[1].used) + 16;
   int I = 0;
-  bool have = P.it[I] && P.lb[I] == L_CROSSING;
+  bool have = P.it(I) && P.lb(I) == L_CROSSING;
   if (!have) {
     int guard = P.used + 1;
-    do { I = P.nx[I]; } while (!(P.it[I] && P.lb[I] == L_CROSSING) && I != 0 && --guard > 0);
+    do { I = P.nx(I); } while (!(P.it(I) && P.lb(I) == L_CROSSING) && I != 0 && --guard > 0);
     have = I != 0 && guard > 0;
   }
   while (have) {
     O.begin();
     int side = 0, V = I;
-    P.it[V] = 0;
+    P.it(V) = 0;
     do {
       Ring& C = c.R[side];
-      int8_t st = toggled(C.ee[V]);
+      int8_t st = toggled(C.ee(V));
       do {
         if (--budget < 0) { fail(c, DEV_TRACE); return false; }
-        V = ((st == E_EXIT) ^ c.uni) ? C.nx[V] : C.pv[V];
-        C.it[V] = 0;
-        O.push(C.x[V], C.y[V]);
-      } while (!(C.ee[V] == st) && !(side == 0 && V == I));
+        V = ((st == E_EXIT) ^ c.uni) ? C.nx(V) : C.pv(V);
+        C.it(V) = 0;
+        O.push(C.x(V), C.y(V));
+      } while (!(C.ee(V) == st) && !(side == 0 && V == I));
       if (!(side == 0 && V == I)) {
-        int nb = C.nb[V];
+        int nb = C.nb(V);
         if (nb < 0) { fail(c, DEV_TRACE); return false; }
         V = nb;
         side = 1 - side;
-        c.R[side].it[V] = 0;
+        c.R[side].it(V) = 0;
       }
     } while (!(side == 0 && V == I));
     O.end();
     int guard = P.used + 1;
-    do { I = P.nx[I]; } while (!(P.it[I] && P.lb[I] == L_CROSSING) && I != 0 && --guard > 0);
+    do { I = P.nx(I); } while (!(P.it(I) && P.lb(I) == L_CROSSING) && I != 0 && --guard > 0);
     have = I != 0 && guard > 0;
   }
   if (O.overflow) { fail(c, DEV_CAPACITY); return false; }
@@ -1458,10 +1505,10 @@ __device__ bool grp_point_in_ring(const G& g, const Ring& B, double Rx, double R
   for (int s = g.rank(); s < B.m; s += g.size()) {
     int n = (s + 1 < B.m) ? s + 1 : 0;
     if (s == after) {
-      w += wind(B.x[s], B.y[s], B.x[T], B.y[T], Rx, Ry, EX);
-      w += wind(B.x[T], B.y[T], B.x[n], B.y[n], Rx, Ry, EX);
+      w += wind(B.x(s), B.y(s), B.x(T), B.y(T), Rx, Ry, EX);
+      w += wind(B.x(T), B.y(T), B.x(n), B.y(n), Rx, Ry, EX);
     } else {
-      w += wind(B.x[s], B.y[s], B.x[n], B.y[n], Rx, Ry, EX);
+      w += wind(B.x(s), B.y(s), B.x(n), B.y(n), Rx, Ry, EX);
     }
   }
   w = g.sum(w);
@@ -1483,9 +1530,9 @@ template <class G>
 __device__ bool grp_links_one_to_one(const G& g, const Ring& P, const Ring& Q) {
   bool ok = true;
   for (int s = g.rank(); s < P.m; s += g.size())
-    if (P.it[s]) { int nb = P.nb[s]; if (nb < 0 || nb >= Q.m || Q.nb[nb] != s) ok = false; }
+    if (P.it(s)) { int nb = P.nb(s); if (nb < 0 || nb >= Q.m || Q.nb(nb) != s) ok = false; }
   for (int s = g.rank(); s < Q.m; s += g.size())
-    if (Q.it[s]) { int nb = Q.nb[s]; if (nb < 0 || nb >= P.m || P.nb[nb] != s) ok = false; }
+    if (Q.it(s)) { int nb = Q.nb(s); if (nb < 0 || nb >= P.m || P.nb(nb) != s) ok = false; }
   return g.all(ok);
 }
 
@@ -1494,13 +1541,13 @@ __device__ void grp_step1(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
   for (int s = g.rank(); s < P.m; s += g.size()) {
-    if (!P.it[s]) continue;
-    int nb = P.nb[s];
+    if (!P.it(s)) continue;
+    int nb = P.nb(s);
     int pm = (s > 0) ? s - 1 : P.m - 1, pp = (s + 1 < P.m) ? s + 1 : 0;
     int a = rel_position<EX>(P, Q, (nb > 0) ? nb - 1 : Q.m - 1, pm, s, pp);
     int b = rel_position<EX>(P, Q, (nb + 1 < Q.m) ? nb + 1 : 0, pm, s, pp);
     int8_t L = initial_label(a, b);
-    if (L != L_NONE) { P.lb[s] = L; Q.lb[nb] = L; }
+    if (L != L_NONE) { P.lb(s) = L; Q.lb(nb) = L; }
   }
   g.sync();
 }
@@ -1515,27 +1562,27 @@ __device__ bool grp_step2(const G& g, PairCtx& c) {
   const int m = P.m;
   bool ok = true;
   for (int s = g.rank(); s < m; s += g.size()) {
-    if (!P.it[s] || (P.lb[s] != L_LEFT_ON && P.lb[s] != L_RIGHT_ON)) continue;
+    if (!P.it(s) || (P.lb(s) != L_LEFT_ON && P.lb(s) != L_RIGHT_ON)) continue;
     int I = (s + 1 < m) ? s + 1 : 0, guard = m;
-    while (P.lb[I] == L_ON_ON && --guard > 0) I = (I + 1 < m) ? I + 1 : 0;
-    if ((P.lb[I] != L_ON_LEFT && P.lb[I] != L_ON_RIGHT) || !P.it[I]) ok = false;
+    while (P.lb(I) == L_ON_ON && --guard > 0) I = (I + 1 < m) ? I + 1 : 0;
+    if ((P.lb(I) != L_ON_LEFT && P.lb(I) != L_ON_RIGHT) || !P.it(I)) ok = false;
   }
   if (!g.all(ok)) return false;
   for (int s = g.rank(); s < m; s += g.size()) {
-    int8_t l0 = P.lb[s];
-    if (!P.it[s] || (l0 != L_LEFT_ON && l0 != L_RIGHT_ON)) continue;
+    int8_t l0 = P.lb(s);
+    if (!P.it(s) || (l0 != L_LEFT_ON && l0 != L_RIGHT_ON)) continue;
     int x = l0 == L_LEFT_ON ? R_LEFT : R_RIGHT;
     int I = (s + 1 < m) ? s + 1 : 0;
-    Q.lb[P.nb[s]] = L_NONE;
-    while (P.lb[I] == L_ON_ON) {
-      P.lb[I] = L_NONE;
-      Q.lb[P.nb[I]] = L_NONE;
+    Q.lb(P.nb(s)) = L_NONE;
+    while (P.lb(I) == L_ON_ON) {
+      P.lb(I) = L_NONE;
+      Q.lb(P.nb(I)) = L_NONE;
       I = (I + 1 < m) ? I + 1 : 0;
     }
-    int y = P.lb[I] == L_ON_LEFT ? R_LEFT : R_RIGHT;
+    int y = P.lb(I) == L_ON_LEFT ? R_LEFT : R_RIGHT;
     int8_t ct = (x != y) ? L_DELAYED_CROSSING : L_DELAYED_BOUNCING;
-    P.lb[s] = ct; P.lb[I] = ct;
-    Q.lb[P.nb[s]] = ct; Q.lb[P.nb[I]] = ct;
+    P.lb(s) = ct; P.lb(I) = ct;
+    Q.lb(P.nb(s)) = ct; Q.lb(P.nb(I)) = ct;
   }
   g.sync();
   return true;
@@ -1547,7 +1594,7 @@ __device__ void grp_push_ring(const G& g, OutRegion& O, const Ring& A) {
   O.begin();
   if (O.overflow) return;
   if (O.nv + A.m > O.vcap) { O.overflow = true; return; }
-  for (int s = g.rank(); s < A.m; s += g.size()) { O.xy[2 * (O.nv + s)] = A.x[s]; O.xy[2 * (O.nv + s) + 1] = A.y[s]; }
+  for (int s = g.rank(); s < A.m; s += g.size()) { O.xy[2 * (O.nv + s)] = A.x(s); O.xy[2 * (O.nv + s) + 1] = A.y(s); }
   if (g.rank() == 0) O.csz[O.nc] = A.m;
   O.nv += A.m;
   O.end();
@@ -1560,12 +1607,12 @@ __device__ void grp_push_ring(const G& g, OutRegion& O, const Ring& A) {
 template <class G>
 __device__ int grp_first_non_intersection(const G& g, const Ring& A, const Ring& B, bool& mid) {
   mid = false;
-  int v = grp_find_first(g, 0, A.m, [&](int s) { return !A.it[s]; });
+  int v = grp_find_first(g, 0, A.m, [&](int s) { return !A.it(s); });
   if (v < A.m) return v;
   // B's own links: B may already hold its temporary vertex when A is Q
   v = grp_find_first(g, 0, A.m, [&](int s) {
-    int nb = A.nb[s], nx = A.nx[s];
-    return nb >= 0 && A.nb[nx] != B.pv[nb] && A.nb[nx] != B.nx[nb];
+    int nb = A.nb(s), nx = A.nx(s);
+    return nb >= 0 && A.nb(nx) != B.pv(nb) && A.nb(nx) != B.nx(nb);
   });
   if (v < A.m) { mid = true; return v; }
   return -1;
@@ -1577,9 +1624,9 @@ __device__ void grp_step35(const G& g, PairCtx& c) {
     Ring& A = c.R[sd];
     bool none = true, allOn = true;
     for (int v = g.rank(); v < A.m; v += g.size()) {
-      int8_t l = A.lb[v];
+      int8_t l = A.lb(v);
       if (l != L_ON_ON) allOn = false;
-      if (A.it[v]) {
+      if (A.it(v)) {
         if (l == L_CROSSING || l == L_DELAYED_CROSSING) none = false;
         if (c.uni && (l == L_BOUNCING || l == L_DELAYED_BOUNCING)) none = false;
       }
@@ -1596,8 +1643,8 @@ __device__ void grp_step35(const G& g, PairCtx& c) {
     bool mid;
     int v = grp_first_non_intersection(g, A, B, mid);
     if (v < 0) continue;
-    double px = A.x[v], py = A.y[v];
-    if (mid) { int n = (v + 1 < A.m) ? v + 1 : 0; px = 0.5 * (A.x[v] + A.x[n]); py = 0.5 * (A.y[v] + A.y[n]); }
+    double px = A.x(v), py = A.y(v);
+    if (mid) { int n = (v + 1 < A.m) ? v + 1 : 0; px = 0.5 * (A.x(v) + A.x(n)); py = 0.5 * (A.y(v) + A.y(n)); }
     bool inside = grp_point_in_ring<EX>(g, B, px, py, -1, -1);
     if (inside ^ c.uni) grp_push_ring(g, c.O, A);
   }
@@ -1621,12 +1668,12 @@ __device__ bool grp_step4(const G& g, PairCtx& c, int tempAfter[2], int tempSlot
     bool mid;
     int V0 = grp_first_non_intersection(g, A, B, mid);
     if (V0 < 0) continue;
-    double qx = A.x[V0], qy = A.y[V0];
+    double qx = A.x(V0), qy = A.y(V0);
     if (mid) {
       int T = -1;
       if (g.rank() == 0) {
-        T = add_vertex(A, 0.5 * (A.x[V0] + A.x[(V0 + 1 < A.m) ? V0 + 1 : 0]),
-                       0.5 * (A.y[V0] + A.y[(V0 + 1 < A.m) ? V0 + 1 : 0]));
+        T = add_vertex(A, 0.5 * (A.x(V0) + A.x((V0 + 1 < A.m) ? V0 + 1 : 0)),
+                       0.5 * (A.y(V0) + A.y((V0 + 1 < A.m) ? V0 + 1 : 0)));
         if (T >= 0) insert_after(A, T, V0);
       }
       T = g.bcast0(T);
@@ -1635,8 +1682,8 @@ __device__ bool grp_step4(const G& g, PairCtx& c, int tempAfter[2], int tempSlot
       if (T < 0) { if (g.rank() == 0) fail(c, DEV_CAPACITY); return false; }
       tempAfter[sd] = V0;
       tempSlot[sd] = T;
-      qx = A.x[T];
-      qy = A.y[T];
+      qx = A.x(T);
+      qy = A.y(T);
     }
     // the Q pass tests against P's ring including P's temporary vertex
     int8_t st0 = (sd == 1 ? grp_point_in_ring<EX>(g, B, qx, qy, tempAfter[0], tempSlot[0])
@@ -1651,8 +1698,8 @@ __device__ bool grp_step4(const G& g, PairCtx& c, int tempAfter[2], int tempSlot
       if (j < m) {
         s = V0 + 1 + j;
         if (s >= m) s -= m;
-        inter = A.it[s];
-        L = inter ? A.lb[s] : L_NONE;
+        inter = A.it(s);
+        L = inter ? A.lb(s) : L_NONE;
       }
       int d = inter && (L == L_DELAYED_CROSSING || L == L_DELAYED_BOUNCING);
       int dTot, tTot;
@@ -1662,16 +1709,16 @@ __device__ bool grp_step4(const G& g, PairCtx& c, int tempAfter[2], int tempSlot
       int tIncl = g.incl_scan(t, tTot);
       int8_t st = ((carryT + tIncl - t) & 1) ? toggled(st0) : st0;
       if (inter) {
-        if (L == L_CROSSING) A.ee[s] = st;
-        else if (L == L_BOUNCING) { if ((st == E_EXIT) ^ c.uni) A.fl[s] |= 1; }
+        if (L == L_CROSSING) A.ee(s) = st;
+        else if (L == L_BOUNCING) { if ((st == E_EXIT) ^ c.uni) A.fl(s) |= 1; }
         else if (L == L_DELAYED_CROSSING) {
-          A.ee[s] = st;
-          if (first) { if ((st == E_EXIT) ^ c.uni) A.lb[s] = L_CROSSING; }
-          else if ((st == E_ENTRY) ^ c.uni) A.lb[s] = L_CROSSING;
+          A.ee(s) = st;
+          if (first) { if ((st == E_EXIT) ^ c.uni) A.lb(s) = L_CROSSING; }
+          else if ((st == E_ENTRY) ^ c.uni) A.lb(s) = L_CROSSING;
         } else if (L == L_DELAYED_BOUNCING) {
-          A.ee[s] = st;
-          if (first) { if ((st == E_EXIT) ^ c.uni) A.fl[s] |= 2; }
-          else if ((st == E_ENTRY) ^ c.uni) A.fl[s] |= 2;
+          A.ee(s) = st;
+          if (first) { if ((st == E_EXIT) ^ c.uni) A.fl(s) |= 2; }
+          else if ((st == E_ENTRY) ^ c.uni) A.fl(s) |= 2;
         }
       }
       carryD += dTot;
@@ -1686,7 +1733,7 @@ template <class G>
 __device__ bool grp_any_split(const G& g, const Ring& P, const Ring& Q) {
   bool any = false;
   for (int s = g.rank(); s < P.m; s += g.size())
-    if (P.fl[s] & 1) { int nb = P.nb[s]; if (nb >= 0 && (Q.fl[nb] & 1)) any = true; }
+    if (P.fl(s) & 1) { int nb = P.nb(s); if (nb >= 0 && (Q.fl(nb) & 1)) any = true; }
   return g.any(any);
 }
 
@@ -1695,9 +1742,9 @@ __device__ void grp_step6(const G& g, PairCtx& c) {
   Ring& P = c.R[0];
   Ring& Q = c.R[1];
   for (int ip = g.rank(); ip < P.m; ip += g.size()) {
-    if (!(P.fl[ip] & 2)) continue;
-    int iq = P.nb[ip];
-    if (iq >= 0 && (Q.fl[iq] & 2)) { P.lb[ip] = L_CROSSING; Q.lb[iq] = L_CROSSING; }
+    if (!(P.fl(ip) & 2)) continue;
+    int iq = P.nb(ip);
+    if (iq >= 0 && (Q.fl(iq) & 2)) { P.lb(ip) = L_CROSSING; Q.lb(iq) = L_CROSSING; }
   }
   g.sync();
 }
@@ -1714,11 +1761,11 @@ __device__ int grp_trace_runs_slots(const G& g, PairCtx& c) {
     int carry = 0;
     for (int b = 0; b < A.m; b += g.size()) {
       const int s = b + g.rank();
-      const int f = (s < A.m && (A.ee[s] == E_ENTRY || A.ee[s] == E_EXIT)) ? 1 : 0;
-      if (s < A.m && (f != 0) != (A.it[s] && A.lb[s] == L_CROSSING)) mismatch = true;
+      const int f = (s < A.m && (A.ee(s) == E_ENTRY || A.ee(s) == E_EXIT)) ? 1 : 0;
+      if (s < A.m && (f != 0) != (A.it(s) && A.lb(s) == L_CROSSING)) mismatch = true;
       int tot;
       const int incl = g.incl_scan(f, tot);
-      if (f) A.ls[carry + incl - 1] = s;
+      if (f) A.ls(carry + incl - 1) = s;
       carry += tot;
     }
     nF[sd] = carry;
@@ -1732,22 +1779,22 @@ __device__ int grp_trace_runs_slots(const G& g, PairCtx& c) {
     const Ring& B = c.R[1 - sd];
     const int n = nF[sd], m = A.m;
     for (int i = g.rank(); i < n; i += g.size()) {
-      const int s = A.ls[i];
-      const int8_t e = A.ee[s];
-      if (!A.it[s] || A.lb[s] != L_CROSSING) { bad = true; continue; }
-      if (A.ee[A.ls[(i + 1 < n) ? i + 1 : 0]] == e) { bad = true; continue; }   // alternation
-      const int nb = A.nb[s];
-      if (nb < 0 || nb >= B.m || B.ee[nb] != toggled(e)) { bad = true; continue; }
+      const int s = A.ls(i);
+      const int8_t e = A.ee(s);
+      if (!A.it(s) || A.lb(s) != L_CROSSING) { bad = true; continue; }
+      if (A.ee(A.ls((i + 1 < n) ? i + 1 : 0)) == e) { bad = true; continue; }   // alternation
+      const int nb = A.nb(s);
+      if (nb < 0 || nb >= B.m || B.ee(nb) != toggled(e)) { bad = true; continue; }
       const int8_t st = toggled(e);
       const int dir = ((st == E_EXIT) ^ c.uni) ? 1 : -1;
-      const int W = A.ls[(i + dir + n) % n];
+      const int W = A.ls((i + dir + n) % n);
       int L = dir > 0 ? W - s : s - W;
       if (L <= 0) L += m;
-      const int nbW = A.nb[W];
+      const int nbW = A.nb(W);
       if (nbW < 0 || nbW >= B.m) { bad = true; continue; }
-      A.tl[s] = dir * L;
-      A.tn[s] = nbW;
-      A.to[s] = -1;
+      A.tl(s) = dir * L;
+      A.tn(s) = nbW;
+      A.to(s) = -1;
       if (L > 32) longRun = true;
     }
   }
@@ -1763,26 +1810,26 @@ __device__ int grp_trace_runs_slots(const G& g, PairCtx& c) {
     const int64_t nv0 = O.nv;
     long long budget = (long long)nF[0] + nF[1] + 4;
     for (int i = 0; i < nF[0] && status == 0; ++i) {
-      const int I = P.ls[i];
-      if (!P.it[I]) continue;
+      const int I = P.ls(i);
+      if (!P.it(I)) continue;
       if (nc >= O.ccap) { status = -1; fail(c, DEV_CAPACITY); break; }
-      P.it[I] = 0;
+      P.it(I) = 0;
       int side = 0, V = I;
       int64_t csz = 0;
       for (;;) {
         Ring& C = c.R[side];
-        const int t = C.tl[V], L = t < 0 ? -t : t, m = C.m;
+        const int t = C.tl(V), L = t < 0 ? -t : t, m = C.m;
         int W = V + t % m;
         W = (W % m + m) % m;
-        C.to[V] = (int32_t)(nv - nv0);
+        C.to(V) = (int32_t)(nv - nv0);
         nv += L;
         csz += L;
-        C.it[W] = 0;
+        C.it(W) = 0;
         if (side == 0 && W == I) break;
-        const int V2 = C.tn[V];
+        const int V2 = C.tn(V);
         side ^= 1;
         if (side == 0 && V2 == I) break;
-        c.R[side].it[V2] = 0;
+        c.R[side].it(V2) = 0;
         V = V2;
         if (--budget < 0) { status = -1; fail(c, DEV_TRACE); break; }
       }
@@ -1804,10 +1851,10 @@ __device__ int grp_trace_runs_slots(const G& g, PairCtx& c) {
     const Ring& A = c.R[sd];
     const int m = A.m;
     for (int i = g.rank(); i < nF[sd]; i += g.size()) {
-      const int s = A.ls[i];
-      const int off = A.to[s];
+      const int s = A.ls(i);
+      const int off = A.to(s);
       if (off < 0) continue;
-      const int t = A.tl[s], L = t < 0 ? -t : t, dir = t < 0 ? -1 : 1;
+      const int t = A.tl(s), L = t < 0 ? -t : t, dir = t < 0 ? -1 : 1;
       if (anyLong && L > kShortRun) continue;
       double* dst = O.xy + 2 * (nv0 + off);
       int w = s;
@@ -1815,14 +1862,14 @@ __device__ int grp_trace_runs_slots(const G& g, PairCtx& c) {
         w += dir;
         if (w >= m) w -= m;
         if (w < 0) w += m;
-        dst[2 * j] = A.x[w];
-        dst[2 * j + 1] = A.y[w];
+        dst[2 * j] = A.x(w);
+        dst[2 * j + 1] = A.y(w);
       }
     }
     for (int i = 0; anyLong && i < nF[sd]; ++i) {
-      const int s = A.ls[i];
-      const int off = A.to[s];
-      const int t = A.tl[s], L = t < 0 ? -t : t;
+      const int s = A.ls(i);
+      const int off = A.to(s);
+      const int t = A.tl(s), L = t < 0 ? -t : t;
       if (off < 0 || L <= kShortRun) continue;
       const int dir = t < 0 ? -1 : 1;
       double* dst = O.xy + 2 * (nv0 + off);
@@ -1830,8 +1877,8 @@ __device__ int grp_trace_runs_slots(const G& g, PairCtx& c) {
         int w = s + dir * (j + 1);
         w %= m;
         if (w < 0) w += m;
-        dst[2 * j] = A.x[w];
-        dst[2 * j + 1] = A.y[w];
+        dst[2 * j] = A.x(w);
+        dst[2 * j + 1] = A.y(w);
       }
     }
   }
@@ -1860,11 +1907,11 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
     int carry = 0;
     for (int b = 0; b < A.m; b += g.size()) {
       const int s = b + g.rank();
-      const int f = (s < A.m && (A.ee[s] == E_ENTRY || A.ee[s] == E_EXIT)) ? 1 : 0;
-      if (s < A.m && (f != 0) != (A.it[s] && A.lb[s] == L_CROSSING)) mismatch = true;
+      const int f = (s < A.m && (A.ee(s) == E_ENTRY || A.ee(s) == E_EXIT)) ? 1 : 0;
+      if (s < A.m && (f != 0) != (A.it(s) && A.lb(s) == L_CROSSING)) mismatch = true;
       int tot;
       const int incl = g.incl_scan(f, tot);
-      if (f) { A.ls[carry + incl - 1] = s; A.to[s] = carry + incl - 1; }   // slot -> index
+      if (f) { A.ls(carry + incl - 1) = s; A.to(s) = carry + incl - 1; }   // slot -> index
       carry += tot;
     }
     nF[sd] = carry;
@@ -1874,9 +1921,9 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
   // run table by list index, in the rings' scratch arrays: length RL, next start RN (sign
   // bit = visited), output offset RO.  The slot -> index map in `to` is read until phase 1
   // ends; the offsets take its place then.  (Pointers are selected per side in registers.)
-  int32_t* const RL0 = c.R[0].tl; int32_t* const RL1 = c.R[1].tl;
-  int32_t* const RN0 = c.R[0].tn; int32_t* const RN1 = c.R[1].tn;
-  int32_t* const RO0 = c.R[0].to; int32_t* const RO1 = c.R[1].to;
+  int32_t* const RL0 = &c.R[0].tl(0); int32_t* const RL1 = &c.R[1].tl(0);
+  int32_t* const RN0 = &c.R[0].tn(0); int32_t* const RN1 = &c.R[1].tn(0);
+  int32_t* const RO0 = &c.R[0].to(0); int32_t* const RO1 = &c.R[1].to(0);
 #define RL_(sd) ((sd) ? RL1 : RL0)
 #define RN_(sd) ((sd) ? RN1 : RN0)
 #define RO_(sd) ((sd) ? RO1 : RO0)
@@ -1887,20 +1934,20 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
     const Ring& B = c.R[1 - sd];
     const int n = nF[sd], m = A.m;
     for (int i = g.rank(); i < n; i += g.size()) {
-      const int s = A.ls[i];
-      const int8_t e = A.ee[s];
-      if (A.ee[A.ls[(i + 1 < n) ? i + 1 : 0]] == e) { bad = true; continue; }   // alternation
-      const int nb = A.nb[s];
-      if (nb < 0 || nb >= B.m || B.ee[nb] != toggled(e)) { bad = true; continue; }
+      const int s = A.ls(i);
+      const int8_t e = A.ee(s);
+      if (A.ee(A.ls((i + 1 < n) ? i + 1 : 0)) == e) { bad = true; continue; }   // alternation
+      const int nb = A.nb(s);
+      if (nb < 0 || nb >= B.m || B.ee(nb) != toggled(e)) { bad = true; continue; }
       const int8_t st = toggled(e);
       const int dir = ((st == E_EXIT) ^ c.uni) ? 1 : -1;
-      const int W = A.ls[(i + dir + n) % n];
+      const int W = A.ls((i + dir + n) % n);
       int L = dir > 0 ? W - s : s - W;
       if (L <= 0) L += m;
-      const int nbW = A.nb[W];
+      const int nbW = A.nb(W);
       if (nbW < 0 || nbW >= B.m) { bad = true; continue; }
       RL_(sd)[i] = dir * L;
-      RN_(sd)[i] = B.to[nbW];          // a flagged twin (checked): its index in B's list
+      RN_(sd)[i] = B.to(nbW);          // a flagged twin (checked): its index in B's list
       if (L > 32) longRun = true;
     }
   }
@@ -1964,27 +2011,27 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
       const int t = RL_(sd)[i], L = t < 0 ? -t : t, dir = t < 0 ? -1 : 1;
       if (anyLong && L > kShortRun) continue;
       double* dst = O.xy + 2 * (nv0 + off);
-      int w = A.ls[i];
+      int w = A.ls(i);
       for (int j = 0; j < L; ++j) {
         w += dir;
         if (w >= m) w -= m;
         if (w < 0) w += m;
-        dst[2 * j] = A.x[w];
-        dst[2 * j + 1] = A.y[w];
+        dst[2 * j] = A.x(w);
+        dst[2 * j + 1] = A.y(w);
       }
     }
     for (int i = 0; anyLong && i < nF[sd]; ++i) {
       const int off = RO_(sd)[i];
       const int t = RL_(sd)[i], L = t < 0 ? -t : t;
       if (off < 0 || L <= kShortRun) continue;
-      const int dir = t < 0 ? -1 : 1, s0 = A.ls[i];
+      const int dir = t < 0 ? -1 : 1, s0 = A.ls(i);
       double* dst = O.xy + 2 * (nv0 + off);
       for (int j = g.rank(); j < L; j += g.size()) {
         int w = s0 + dir * (j + 1);
         w %= m;
         if (w < 0) w += m;
-        dst[2 * j] = A.x[w];
-        dst[2 * j + 1] = A.y[w];
+        dst[2 * j] = A.x(w);
+        dst[2 * j + 1] = A.y(w);
       }
     }
   }
@@ -2005,17 +2052,17 @@ __device__ bool grp_trace(const G& g, PairCtx& c) {
   long long budget = 4ll * (c.R[0].used + c.R[1].used) + 16;
   int from = 0;
   for (;;) {
-    int I = grp_find_first(g, from, P.m, [&](int s) { return P.it[s] && P.lb[s] == L_CROSSING; });
+    int I = grp_find_first(g, from, P.m, [&](int s) { return P.it(s) && P.lb(s) == L_CROSSING; });
     if (I >= P.m) break;
     O.begin();
     if (O.overflow) { if (g.rank() == 0) fail(c, DEV_CAPACITY); return false; }
     int side = 0, V = I;
-    if (g.rank() == 0) P.it[V] = 0;
+    if (g.rank() == 0) P.it(V) = 0;
     g.sync();
     do {
       Ring& C = c.R[side];
       const int m = C.m;
-      int8_t st = toggled(C.ee[V]);
+      int8_t st = toggled(C.ee(V));
       const int dir = ((st == E_EXIT) ^ c.uni) ? 1 : -1;
       int L = -1;
       for (int j0 = 1; j0 <= m && L < 0; j0 += g.size()) {
@@ -2024,7 +2071,7 @@ __device__ bool grp_trace(const G& g, PairCtx& c) {
         if (j <= m) {
           int w = V + dir * (j % m);
           w = (w % m + m) % m;
-          hit = (C.ee[w] == st) || (side == 0 && w == I);
+          hit = (C.ee(w) == st) || (side == 0 && w == I);
         }
         int f = g.first(hit);
         if (f >= 0) L = j0 + f;
@@ -2038,9 +2085,9 @@ __device__ bool grp_trace(const G& g, PairCtx& c) {
         if (j <= L) {
           int w = V + dir * (j % m);
           w = (w % m + m) % m;
-          C.it[w] = 0;
-          O.xy[2 * (O.nv + j - 1)] = C.x[w];
-          O.xy[2 * (O.nv + j - 1) + 1] = C.y[w];
+          C.it(w) = 0;
+          O.xy[2 * (O.nv + j - 1)] = C.x(w);
+          O.xy[2 * (O.nv + j - 1) + 1] = C.y(w);
         }
       }
       O.nv += L;
@@ -2049,11 +2096,11 @@ __device__ bool grp_trace(const G& g, PairCtx& c) {
       V = (W % m + m) % m;
       g.sync();
       if (!(side == 0 && V == I)) {
-        int nb = C.nb[V];
+        int nb = C.nb(V);
         if (nb < 0) { if (g.rank() == 0) fail(c, DEV_TRACE); return false; }
         V = nb;
         side = 1 - side;
-        if (g.rank() == 0) c.R[side].it[V] = 0;
+        if (g.rank() == 0) c.R[side].it(V) = 0;
         g.sync();
       }
     } while (!(side == 0 && V == I));
@@ -2074,7 +2121,7 @@ __device__ void grp_cleanup(const G& g, PairCtx& c, int32_t* outNC, int64_t* out
   // is removable, the output stands as traced; otherwise (and for pairs with few
   // components) the per-component pass below removes and compacts.
   if (O.nc > 4) {
-    int32_t* start = c.R[0].tn;          // the trace's scratch is free now
+    int32_t* start = &c.R[0].tn(0);      // the trace's scratch is free now
     int carry = 0;
     for (int b = 0; b < O.nc; b += g.size()) {
       const int k = b + g.rank();
@@ -2164,11 +2211,10 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
 
 template <class G>
 __device__ void prefetch_ring(const G& g, const Ring& R) {
-  for (int s = g.rank() * 16; s < R.m; s += g.size() * 16) {
-    prefetch_l1(R.x + s);
-    prefetch_l1(R.y + s);
-    if ((s & 31) == 0) { prefetch_l1(R.nx + s); prefetch_l1(R.pv + s); prefetch_l1(R.nb + s); }
-    if ((s & 127) == 0) { prefetch_l1(R.it + s); prefetch_l1(R.lb + s); prefetch_l1(R.ee + s); prefetch_l1(R.fl + s); }
+  for (int s = g.rank() * 8; s < R.m; s += g.size() * 8) {
+    prefetch_l1(&R.xy(s));
+    if ((s & 31) == 0) { prefetch_l1(&R.nx(s)); prefetch_l1(&R.pv(s)); prefetch_l1(&R.nb(s)); }
+    if ((s & 127) == 0) { prefetch_l1(&R.it(s)); prefetch_l1(&R.lb(s)); prefetch_l1(&R.ee(s)); prefetch_l1(&R.fl(s)); }
   }
 }
 
@@ -2266,10 +2312,11 @@ __device__ void label_trace_pair(const G& g, const LabelArgs& a, int64_t k) {
 }
 
 // Two register budgets for the warp and one-thread kernels.  kWide (batches of at least
-// ClipParams::wide_label_min pairs): 6 blocks of 128 (at most 80 registers) here and 16 blocks (32
+// ClipParams::wide_label_min pairs): 6 blocks of 128 (at most 80 registers) here and 12 blocks (40
 // registers) for the tiles below -- both kernels wait on dependent loads, and on a full
 // GPU the occupancy pays for the spills (label stage 2.59 -> 2.11 ms from the tile kernel,
-// -0.07 ms from this one).  Small batches (serving) leave most SMs idle, so there the
+// -0.07 ms from this one; with the column-buffer rings, 12 tile blocks measured 2.00 ms
+// against 2.08 ms for 16).  Small batches (serving) leave most SMs idle, so there the
 // kernels keep 4 blocks and spill nothing.  Exact-predicate instances always keep 4
 // blocks: their expansion arithmetic would spill.
 template <int EX, int kWide>
@@ -2290,7 +2337,7 @@ label_trace_kernel(LabelArgs a) {
 // faster than 2-lane tiles on the batched workload).
 constexpr int kTileLanes = 1;
 template <int EX, int kWide>
-__global__ void __launch_bounds__(128, (kWide && !EX) ? 16 : 4)
+__global__ void __launch_bounds__(128, (kWide && !EX) ? 12 : 4)
 label_trace_tile_kernel(LabelArgs a) {
   const int64_t k = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / kTileLanes) +
                     (lane_id() / kTileLanes);
@@ -2371,10 +2418,10 @@ __global__ void big_links_kernel(RingSet SP, RingSet SQ, BigPair bp, BigFlags* f
     bool bad = false;
     if (i < P.m) {
       int s = (int)i;
-      if (P.it[s]) { int nb = P.nb[s]; bad = nb < 0 || nb >= Q.m || Q.nb[nb] != s; }
+      if (P.it(s)) { int nb = P.nb(s); bad = nb < 0 || nb >= Q.m || Q.nb(nb) != s; }
     } else {
       int s = (int)(i - P.m);
-      if (Q.it[s]) { int nb = Q.nb[s]; bad = nb < 0 || nb >= P.m || P.nb[nb] != s; }
+      if (Q.it(s)) { int nb = Q.nb(s); bad = nb < 0 || nb >= P.m || P.nb(nb) != s; }
     }
     if (bad) atomicOr(&f->bad, 1);
   }
@@ -2384,13 +2431,13 @@ template <int EX>
 __global__ void big_step1_kernel(RingSet SP, RingSet SQ, BigPair bp) {
   Ring P = big_ring(SP, bp.regP, bp.mP, bp.capP, bp.mP), Q = big_ring(SQ, bp.regQ, bp.mQ, bp.capQ, bp.mQ);
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P.m; s += gridDim.x * blockDim.x) {
-    if (!P.it[s]) continue;
-    int nb = P.nb[s];
+    if (!P.it(s)) continue;
+    int nb = P.nb(s);
     int pm = prv_slot(s, P.m), pp = nxt_slot(s, P.m);
     int a = rel_position<EX>(P, Q, prv_slot(nb, Q.m), pm, s, pp);
     int b = rel_position<EX>(P, Q, nxt_slot(nb, Q.m), pm, s, pp);
     int8_t L = initial_label(a, b);
-    if (L != L_NONE) { P.lb[s] = L; Q.lb[nb] = L; }
+    if (L != L_NONE) { P.lb(s) = L; Q.lb(nb) = L; }
   }
 }
 
@@ -2400,24 +2447,24 @@ __global__ void big_chain_kernel(RingSet SP, RingSet SQ, BigPair bp, BigFlags* f
   Ring P = big_ring(SP, bp.regP, bp.mP, bp.capP, bp.mP), Q = big_ring(SQ, bp.regQ, bp.mQ, bp.capQ, bp.mQ);
   const int m = P.m;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) {
-    int8_t l0 = P.lb[s];
-    if (!P.it[s] || (l0 != L_LEFT_ON && l0 != L_RIGHT_ON)) continue;
+    int8_t l0 = P.lb(s);
+    if (!P.it(s) || (l0 != L_LEFT_ON && l0 != L_RIGHT_ON)) continue;
     int I = nxt_slot(s, m), guard = m;
     if (kMode == 0) {
-      while (P.lb[I] == L_ON_ON && --guard > 0) I = nxt_slot(I, m);
-      if ((P.lb[I] != L_ON_LEFT && P.lb[I] != L_ON_RIGHT) || !P.it[I]) atomicOr(&f->bad, 1);
+      while (P.lb(I) == L_ON_ON && --guard > 0) I = nxt_slot(I, m);
+      if ((P.lb(I) != L_ON_LEFT && P.lb(I) != L_ON_RIGHT) || !P.it(I)) atomicOr(&f->bad, 1);
     } else {
       int x = l0 == L_LEFT_ON ? R_LEFT : R_RIGHT;
-      Q.lb[P.nb[s]] = L_NONE;
-      while (P.lb[I] == L_ON_ON) {
-        P.lb[I] = L_NONE;
-        Q.lb[P.nb[I]] = L_NONE;
+      Q.lb(P.nb(s)) = L_NONE;
+      while (P.lb(I) == L_ON_ON) {
+        P.lb(I) = L_NONE;
+        Q.lb(P.nb(I)) = L_NONE;
         I = nxt_slot(I, m);
       }
-      int y = P.lb[I] == L_ON_LEFT ? R_LEFT : R_RIGHT;
+      int y = P.lb(I) == L_ON_LEFT ? R_LEFT : R_RIGHT;
       int8_t ct = (x != y) ? L_DELAYED_CROSSING : L_DELAYED_BOUNCING;
-      P.lb[s] = ct; P.lb[I] = ct;
-      Q.lb[P.nb[s]] = ct; Q.lb[P.nb[I]] = ct;
+      P.lb(s) = ct; P.lb(I) = ct;
+      Q.lb(P.nb(s)) = ct; Q.lb(P.nb(I)) = ct;
     }
   }
 }
@@ -2431,16 +2478,16 @@ __global__ void big_flags_kernel(RingSet SP, RingSet SQ, BigPair bp, int uni, Bi
     int v = (int)(sd == 0 ? i : i - R[0].m);
     const Ring& A = R[sd];
     const Ring& B = R[1 - sd];
-    int8_t l = A.lb[v];
+    int8_t l = A.lb(v);
     if (l != L_ON_ON) atomicOr(&f->notAllOn[sd], 1);
-    if (A.it[v]) {
+    if (A.it(v)) {
       if (l == L_CROSSING || l == L_DELAYED_CROSSING) atomicOr(&f->notNone[sd], 1);
       if (uni && (l == L_BOUNCING || l == L_DELAYED_BOUNCING)) atomicOr(&f->notNone[sd], 1);
     } else {
       atomicMin(&f->firstFree[sd], v);
     }
-    int nb = A.nb[v], nx = nxt_slot(v, A.m);
-    if (nb >= 0 && A.nb[nx] != prv_slot(nb, B.m) && A.nb[nx] != nxt_slot(nb, B.m)) atomicMin(&f->firstMid[sd], v);
+    int nb = A.nb(v), nx = nxt_slot(v, A.m);
+    if (nb >= 0 && A.nb(nx) != prv_slot(nb, B.m) && A.nb(nx) != nxt_slot(nb, B.m)) atomicMin(&f->firstMid[sd], v);
   }
 }
 
@@ -2450,8 +2497,8 @@ __global__ void big_first_mid_kernel(RingSet SA, RingSet SB, int64_t regA, int m
                                      int capB, int usedB, int* out) {
   Ring A = big_ring(SA, regA, mA, capA, mA), B = big_ring(SB, regB, mB, capB, usedB);
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < A.m; v += gridDim.x * blockDim.x) {
-    int nb = A.nb[v], nx = nxt_slot(v, A.m);
-    if (nb >= 0 && A.nb[nx] != B.pv[nb] && A.nb[nx] != B.nx[nb]) atomicMin(out, v);
+    int nb = A.nb(v), nx = nxt_slot(v, A.m);
+    if (nb >= 0 && A.nb(nx) != B.pv(nb) && A.nb(nx) != B.nx(nb)) atomicMin(out, v);
   }
 }
 
@@ -2460,20 +2507,18 @@ __global__ void big_first_mid_kernel(RingSet SA, RingSet SB, int64_t regA, int m
 // B's edges are (s, s+1); `after`/`T` splice a temporary vertex of B.
 __global__ void big_wind_kernel(RingSet SA, int64_t regA, int mA, int v, int mode, RingSet SB, int64_t regB, int mB,
                                 int after, int T, unsigned long long* wsum) {
-  const double* ax = SA.x + regA;
-  const double* ay = SA.y + regA;
-  double Rx = ax[v], Ry = ay[v];
-  if (mode == 1) { int n = nxt_slot(v, mA); Rx = 0.5 * (ax[v] + ax[n]); Ry = 0.5 * (ay[v] + ay[n]); }
-  const double* bx = SB.x + regB;
-  const double* by = SB.y + regB;
+  const double2* a = &SA.xy(regA);
+  double Rx = a[v].x, Ry = a[v].y;
+  if (mode == 1) { int n = nxt_slot(v, mA); Rx = 0.5 * (a[v].x + a[n].x); Ry = 0.5 * (a[v].y + a[n].y); }
+  const double2* q = &SB.xy(regB);
   long long w = 0;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < mB; s += gridDim.x * blockDim.x) {
     int n = nxt_slot(s, mB);
     if (s == after) {
-      w += wind(bx[s], by[s], bx[T], by[T], Rx, Ry, SB.exact);
-      w += wind(bx[T], by[T], bx[n], by[n], Rx, Ry, SB.exact);
+      w += wind(q[s].x, q[s].y, q[T].x, q[T].y, Rx, Ry, SB.exact);
+      w += wind(q[T].x, q[T].y, q[n].x, q[n].y, Rx, Ry, SB.exact);
     } else {
-      w += wind(bx[s], by[s], bx[n], by[n], Rx, Ry, SB.exact);
+      w += wind(q[s].x, q[s].y, q[n].x, q[n].y, Rx, Ry, SB.exact);
     }
   }
   w = warp_sum(w);
@@ -2483,16 +2528,16 @@ __global__ void big_wind_kernel(RingSet SA, int64_t regA, int mA, int v, int mod
 __global__ void big_copy_ring_kernel(RingSet S, int64_t reg, int m, double* __restrict__ oxy, int64_t at,
                                      int32_t* __restrict__ csz, int comp) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) {
-    oxy[2 * (at + s)] = S.x[reg + s];
-    oxy[2 * (at + s) + 1] = S.y[reg + s];
+    oxy[2 * (at + s)] = S.x(reg + s);
+    oxy[2 * (at + s) + 1] = S.y(reg + s);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) csz[comp] = m;
 }
 
 __global__ void big_add_temp_kernel(RingSet S, int64_t reg, int m, int cap, int used, int v) {
   Ring A = big_ring(S, reg, m, cap, used);
-  int n = A.nx[v];
-  int T = add_vertex(A, 0.5 * (A.x[v] + A.x[n]), 0.5 * (A.y[v] + A.y[n]));
+  int n = A.nx(v);
+  int T = add_vertex(A, 0.5 * (A.x(v) + A.x(n)), 0.5 * (A.y(v) + A.y(n)));
   if (T >= 0) insert_after(A, T, v);
 }
 
@@ -2501,8 +2546,8 @@ __global__ void big_d_kernel(RingSet S, int64_t reg, int m, int V0, int32_t* __r
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
     int s = V0 + 1 + j;
     if (s >= m) s -= m;
-    int8_t L = S.lb[reg + s];
-    d[j] = (S.it[reg + s] && (L == L_DELAYED_CROSSING || L == L_DELAYED_BOUNCING)) ? 1 : 0;
+    int8_t L = S.lb(reg + s);
+    d[j] = (S.it(reg + s) && (L == L_DELAYED_CROSSING || L == L_DELAYED_BOUNCING)) ? 1 : 0;
   }
 }
 
@@ -2511,9 +2556,9 @@ __global__ void big_t_kernel(RingSet S, int64_t reg, int m, int V0, const int64_
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
     int s = V0 + 1 + j;
     if (s >= m) s -= m;
-    int8_t L = S.lb[reg + s];
+    int8_t L = S.lb(reg + s);
     bool first = (dEx[j] & 1) == 0;
-    t[j] = (S.it[reg + s] && (L == L_CROSSING || L == L_DELAYED_BOUNCING || (L == L_DELAYED_CROSSING && !first))) ? 1 : 0;
+    t[j] = (S.it(reg + s) && (L == L_CROSSING || L == L_DELAYED_BOUNCING || (L == L_DELAYED_CROSSING && !first))) ? 1 : 0;
   }
 }
 
@@ -2523,37 +2568,37 @@ __global__ void big_apply4_kernel(RingSet S, int64_t reg, int m, int V0, const i
     int s = V0 + 1 + j;
     if (s >= m) s -= m;
     const int64_t g = reg + s;
-    if (!S.it[g]) continue;
-    int8_t L = S.lb[g];
+    if (!S.it(g)) continue;
+    int8_t L = S.lb(g);
     bool first = (dEx[j] & 1) == 0;
     int8_t st = (tEx[j] & 1) ? toggled(st0) : st0;
-    if (L == L_CROSSING) S.ee[g] = st;
-    else if (L == L_BOUNCING) { if ((st == E_EXIT) ^ (uni != 0)) S.fl[g] |= 1; }
+    if (L == L_CROSSING) S.ee(g) = st;
+    else if (L == L_BOUNCING) { if ((st == E_EXIT) ^ (uni != 0)) S.fl(g) |= 1; }
     else if (L == L_DELAYED_CROSSING) {
-      S.ee[g] = st;
-      if (first) { if ((st == E_EXIT) ^ (uni != 0)) S.lb[g] = L_CROSSING; }
-      else if ((st == E_ENTRY) ^ (uni != 0)) S.lb[g] = L_CROSSING;
+      S.ee(g) = st;
+      if (first) { if ((st == E_EXIT) ^ (uni != 0)) S.lb(g) = L_CROSSING; }
+      else if ((st == E_ENTRY) ^ (uni != 0)) S.lb(g) = L_CROSSING;
     } else if (L == L_DELAYED_BOUNCING) {
-      S.ee[g] = st;
-      if (first) { if ((st == E_EXIT) ^ (uni != 0)) S.fl[g] |= 2; }
-      else if ((st == E_ENTRY) ^ (uni != 0)) S.fl[g] |= 2;
+      S.ee(g) = st;
+      if (first) { if ((st == E_EXIT) ^ (uni != 0)) S.fl(g) |= 2; }
+      else if ((st == E_ENTRY) ^ (uni != 0)) S.fl(g) |= 2;
     }
   }
 }
 
 __global__ void big_split_any_kernel(RingSet SP, RingSet SQ, BigPair bp, BigFlags* f) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < bp.mP; s += gridDim.x * blockDim.x) {
-    if (!(SP.fl[bp.regP + s] & 1)) continue;
-    int nb = SP.nb[bp.regP + s];
-    if (nb >= 0 && (SQ.fl[bp.regQ + nb] & 1)) atomicOr(&f->anySplit, 1);
+    if (!(SP.fl(bp.regP + s) & 1)) continue;
+    int nb = SP.nb(bp.regP + s);
+    if (nb >= 0 && (SQ.fl(bp.regQ + nb) & 1)) atomicOr(&f->anySplit, 1);
   }
 }
 
 __global__ void big_step6_kernel(RingSet SP, RingSet SQ, BigPair bp) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < bp.mP; s += gridDim.x * blockDim.x) {
-    if (!(SP.fl[bp.regP + s] & 2)) continue;
-    int nb = SP.nb[bp.regP + s];
-    if (nb >= 0 && (SQ.fl[bp.regQ + nb] & 2)) { SP.lb[bp.regP + s] = L_CROSSING; SQ.lb[bp.regQ + nb] = L_CROSSING; }
+    if (!(SP.fl(bp.regP + s) & 2)) continue;
+    int nb = SP.nb(bp.regP + s);
+    if (nb >= 0 && (SQ.fl(bp.regQ + nb) & 2)) { SP.lb(bp.regP + s) = L_CROSSING; SQ.lb(bp.regQ + nb) = L_CROSSING; }
   }
 }
 
@@ -2606,9 +2651,9 @@ __global__ void big_seq_pair_kernel(RingSet SP, RingSet SQ, BigPair bp, int step
 // cycle, else (I ends one) along the reversed cycle.
 __global__ void big_labeled_kernel(RingSet S, int64_t reg, int m, uint8_t* __restrict__ lab, BigFlags* f) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) {
-    int8_t e = S.ee[reg + s];
+    int8_t e = S.ee(reg + s);
     bool flagged = (e == E_ENTRY || e == E_EXIT);
-    bool crossing = S.it[reg + s] && S.lb[reg + s] == L_CROSSING;
+    bool crossing = S.it(reg + s) && S.lb(reg + s) == L_CROSSING;
     lab[s] = flagged ? 1 : 0;
     if (flagged != crossing) atomicOr(&f->bad, 1);
   }
@@ -2635,18 +2680,18 @@ __global__ void big_runs_kernel(RingSet SP, RingSet SQ, BigPair bp, const int32_
     const int i = onP ? u : u - nP;
     const int32_t* list = onP ? listP : listQ;
     const int s = list[i];
-    const int8_t e = A.ee[ra + s];
+    const int8_t e = A.ee(ra + s);
     bool bad = n < 2;
     int nxt = list[(i + 1 < n) ? i + 1 : 0];
-    if (A.ee[ra + nxt] == e) bad = true;                         // alternation
-    int nb = A.nb[ra + s];
-    if (nb < 0 || B.ee[rb + nb] != toggled(e)) bad = true;        // twin carries the opposite flag
+    if (A.ee(ra + nxt) == e) bad = true;                         // alternation
+    int nb = A.nb(ra + s);
+    if (nb < 0 || B.ee(rb + nb) != toggled(e)) bad = true;        // twin carries the opposite flag
     const int8_t st = toggled(e);
     const int dir = ((st == E_EXIT) ^ (uni != 0)) ? 1 : -1;
     int W = list[(i + dir + n) % n];
     int L = dir > 0 ? W - s : s - W;
     if (L <= 0) L += m;
-    int nbW = A.nb[ra + W];
+    int nbW = A.nb(ra + W);
     if (nbW < 0) bad = true;
     int v = 0;
     if (!bad) v = onP ? nP + (int)idxQ[nbW] : (int)idxP[nbW];
@@ -2678,7 +2723,7 @@ __global__ void big_cycle_init_kernel(RingSet SP, RingSet SQ, BigPair bp, const 
   for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nP + nQ; u += gridDim.x * blockDim.x) {
     const bool onP = u < nP;
     const int s = onP ? listP[u] : listQ[u - nP];
-    const int8_t e = onP ? SP.ee[bp.regP + s] : SQ.ee[bp.regQ + s];
+    const int8_t e = onP ? SP.ee(bp.regP + s) : SQ.ee(bp.regQ + s);
     isE[u] = e == E_ENTRY ? 1 : 0;
     J[u] = succ[u];
     a[u] = onP ? s : INT_MAX;
@@ -2751,7 +2796,7 @@ __global__ void big_write_kernel(RingSet SP, RingSet SQ, BigPair bp, const int32
   const int64_t ra = onP ? bp.regP : bp.regQ;
   const int m = onP ? bp.mP : bp.mQ;
   const int s = onP ? listP[u] : listQ[u - nP];
-  const int8_t st = toggled(A.ee[ra + s]);
+  const int8_t st = toggled(A.ee(ra + s));
   const int dir = ((st == E_EXIT) ^ (uni != 0)) ? 1 : -1;
   const int I = min(a[u], b[u]);
   const int64_t L = sfx[Bst[u]];
@@ -2764,8 +2809,8 @@ __global__ void big_write_kernel(RingSet SP, RingSet SQ, BigPair bp, const int32
     v = ((v % m) + m) % m;
     int64_t f = off + j;
     int64_t pos = r ? ((f < L - 1) ? L - 2 - f : L - 1) : f;
-    oxy[2 * (base + pos)] = A.x[ra + v];
-    oxy[2 * (base + pos) + 1] = A.y[ra + v];
+    oxy[2 * (base + pos)] = A.x(ra + v);
+    oxy[2 * (base + pos) + 1] = A.y(ra + v);
   }
   if (lane_id() == 0 && Bst[u] == u) ocsz[bp.cOff + nc0 + compIdx[I]] = (int32_t)L;
 }
@@ -3437,12 +3482,10 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   C.n_ring_vertices = hs[2];
   C.n_records = nR;
   auto take_ring = [&](int64_t n, RingSet& S) {
-    S.x = A.take_n<double>(n); S.y = A.take_n<double>(n);
-    S.nx = A.take_n<int32_t>(n); S.pv = A.take_n<int32_t>(n); S.nb = A.take_n<int32_t>(n);
-    S.it = A.take_n<uint8_t>(n); S.lb = A.take_n<int8_t>(n); S.ee = A.take_n<int8_t>(n);
-    S.fl = A.take_n<uint8_t>(n);
-    S.tn = A.take_n<int32_t>(n); S.tl = A.take_n<int32_t>(n); S.to = A.take_n<int32_t>(n); S.ls = A.take_n<int32_t>(n);
-    return S.x && S.y && S.nx && S.pv && S.nb && S.it && S.lb && S.ee && S.fl && S.tn && S.tl && S.to && S.ls;
+    const int64_t slots = (std::max<int64_t>(n, 1) + 15) & ~int64_t(15);
+    char* buf = static_cast<char*>(A.take((size_t)(kRingSlotBytes * slots)));
+    S.set(buf, slots);
+    return buf != nullptr;
   };
   RingSet SP, SQ;
   if (!take_ring(regTotP, SP) || !take_ring(regTotQ, SQ)) return ST_OUT_OF_MEMORY;
