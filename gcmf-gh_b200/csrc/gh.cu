@@ -290,10 +290,14 @@ __global__ void pair_records_kernel(const int64_t* __restrict__ chunkOff, const 
 }
 
 // ---------------------------------------------------------------- G2/G3 binned
-// A uniform grid over the common MBR.  Q edges are listed in every cell their box
-// covers; each P edge visits the cells its box covers and tests a Q edge only in the cell
-// holding the lower-left corner of the two boxes' overlap, so every edge pair whose boxes
-// touch is tested exactly once (cell indices are monotone in the coordinate).
+// Pairs whose filtered edge grid exceeds ClipParams::bin_grid edge pairs are not
+// enumerated edge pair by edge pair.  Each gets a uniform grid over its common MBR
+// (about one Q edge per cell); its Q edges are listed in every cell their box covers;
+// each P edge visits the cells its box covers and tests a Q edge only in the cell holding
+// the lower-left corner of the two boxes' overlap, so every edge pair whose boxes touch
+// is tested exactly once (cell indices are monotone in the coordinate).  All binned pairs
+// go through the same launches: their P and Q edges are numbered consecutively (pair by
+// pair) and each edge finds its pair through an owner table.
 struct BinGrid { double x0, y0, cw, ch; int gx, gy; };
 
 __device__ __forceinline__ int cell_1d(double v, double c0, double cs, int g) {
@@ -303,131 +307,183 @@ __device__ __forceinline__ int cell_1d(double v, double c0, double cs, int g) {
   return (int)t;
 }
 
-__global__ void bin_count_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LQ,
-                                 int cq, BinGrid G, int32_t* __restrict__ cellCnt) {
+// The binned pairs, i = 0..B-1 (pair k = list[i]).
+struct BinSet {
+  const int64_t* list;
+  int32_t* cp; int32_t* cq;           // filtered edges per side
+  int64_t* pBase; int64_t* qBase;     // first binned P / Q edge of pair i
+  int32_t* ownP; int32_t* ownQ;       // binned edge -> i
+  double* ext;                        // per pair: sums of the Q edges' box widths, heights
+  BinGrid* grid;
+  int64_t* cellBase;                  // first cell of pair i (cells of all pairs in one array)
+  int32_t* ncell;
+};
+
+__global__ void bin_sizes_kernel(BinSet S, int n, const int32_t* __restrict__ cP, const int32_t* __restrict__ cQ) {
   int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i >= cq) return;
-  const double2* qv = layer_xy(Lb, Lo, 1 - D.pSide[k]) + D.qS[k];
-  const int nq = D.nQ[k];
-  int q = LQ[i];
-  double2 a = __ldg(qv + q), b = __ldg(qv + (q + 1 < nq ? q + 1 : 0));
-  int x0 = cell_1d(fmin(a.x, b.x), G.x0, G.cw, G.gx), x1 = cell_1d(fmax(a.x, b.x), G.x0, G.cw, G.gx);
-  int y0 = cell_1d(fmin(a.y, b.y), G.y0, G.ch, G.gy), y1 = cell_1d(fmax(a.y, b.y), G.y0, G.ch, G.gy);
-  for (int y = y0; y <= y1; ++y)
-    for (int x = x0; x <= x1; ++x) atomicAdd(&cellCnt[(int64_t)y * G.gx + x], 1);
+  if (i >= n) return;
+  const int64_t k = S.list[i];
+  S.cp[i] = cP[k];
+  S.cq[i] = cQ[k];
 }
 
-// sums of the Q edges' box widths and heights (sizes the grid's cells)
-__global__ void edge_extent_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LQ,
-                                   int cq, double* __restrict__ sums) {
-  int i = blockIdx.x * kThreads + threadIdx.x;
+// the pair-local Q (P) edge of binned edge j
+__device__ __forceinline__ int binned_q(const BinSet& S, int64_t j, int i, const int64_t* offQ, const int32_t* LQ) {
+  return LQ[offQ[S.list[i]] + (j - S.qBase[i])];
+}
+__device__ __forceinline__ int binned_p(const BinSet& S, int64_t j, int i, const int64_t* offP, const int32_t* LP) {
+  return LP[offP[S.list[i]] + (j - S.pBase[i])];
+}
+
+// Sums of the Q edges' box widths and heights per pair (they size the cells).  Edges of
+// one pair are consecutive, so a warp reduces each run of equal owners and one lane per
+// run adds it.
+__global__ void bin_extent_kernel(LayerDev Lb, LayerDev Lo, PairDev D, BinSet S, int64_t nq,
+                                  const int64_t* __restrict__ offQ, const int32_t* __restrict__ LQ) {
+  const int64_t j = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  int i = -1;
   double w = 0, h = 0;
-  if (i < cq) {
+  if (j < nq) {
+    i = S.ownQ[j];
+    const int64_t k = S.list[i];
     const double2* qv = layer_xy(Lb, Lo, 1 - D.pSide[k]) + D.qS[k];
-    const int nq = D.nQ[k];
-    int q = LQ[i];
-    double2 a = __ldg(qv + q), b = __ldg(qv + (q + 1 < nq ? q + 1 : 0));
+    const int n = D.nQ[k];
+    const int q = binned_q(S, j, i, offQ, LQ);
+    const double2 a = __ldg(qv + q), b = __ldg(qv + (q + 1 < n ? q + 1 : 0));
     w = fabs(b.x - a.x);
     h = fabs(b.y - a.y);
   }
-  w = warp_sum(w);
-  h = warp_sum(h);
-  if (lane_id() == 0) { atomicAdd(sums, w); atomicAdd(sums + 1, h); }
+  const int lane = (int)lane_id();
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {          // segmented inclusive scan over equal owners
+    const double uw = __shfl_up_sync(0xffffffffu, w, d), uh = __shfl_up_sync(0xffffffffu, h, d);
+    const int ui = __shfl_up_sync(0xffffffffu, i, d);
+    if (lane >= d && ui == i) { w += uw; h += uh; }
+  }
+  const int ni = __shfl_down_sync(0xffffffffu, i, 1);
+  if (i >= 0 && (lane == 31 || ni != i)) {
+    atomicAdd(S.ext + 2 * i, w);
+    atomicAdd(S.ext + 2 * i + 1, h);
+  }
 }
 
-__global__ void bin_fill_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LQ,
-                                int cq, BinGrid G, const int64_t* __restrict__ cellOff, int32_t* __restrict__ cursor,
-                                int32_t* __restrict__ cellList) {
+// Grid of each binned pair: about one Q edge per cell, but never cells smaller than the
+// Q edges' mean box (long edges would otherwise be listed in many cells and each P edge
+// would scan them all again); at most 4096 cells per axis.
+__global__ void bin_grid_kernel(PairDev D, BinSet S, int n) {
   int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i >= cq) return;
+  if (i >= n) return;
+  const double4 c = reinterpret_cast<const double4*>(D.cmbr)[S.list[i]];
+  const double w = c.z - c.x, h = c.w - c.y;
+  const double target = (double)max(1, S.cq[i]);
+  const double mw = S.ext[2 * i] / target, mh = S.ext[2 * i + 1] / target;
+  double gx = 1, gy = 1;
+  if (w > 0 && h > 0) {
+    gx = ceil(sqrt(target * w / h));
+    gx = fmin(fmax(gx, 1.0), 4096.0);
+    gy = ceil(target / gx);
+    if (mw > 0) gx = fmin(gx, ceil(w / mw));
+    if (mh > 0) gy = fmin(gy, ceil(h / mh));
+    gx = fmin(fmax(gx, 1.0), 4096.0);
+    gy = fmin(fmax(gy, 1.0), 4096.0);
+  } else if (w > 0) {
+    gx = fmin(target, 4096.0);
+  } else if (h > 0) {
+    gy = fmin(target, 4096.0);
+  }
+  BinGrid G{c.x, c.y, w > 0 ? w / gx : 1.0, h > 0 ? h / gy : 1.0, (int)gx, (int)gy};
+  S.grid[i] = G;
+  S.ncell[i] = G.gx * G.gy;
+}
+
+// kMode 0: count the listings per cell; kMode 1: list every Q edge in the cells its box covers
+template <int kMode>
+__global__ void bin_cells_kernel(LayerDev Lb, LayerDev Lo, PairDev D, BinSet S, int64_t nq,
+                                 const int64_t* __restrict__ offQ, const int32_t* __restrict__ LQ,
+                                 int32_t* __restrict__ cellCnt, const int64_t* __restrict__ cellOff,
+                                 int32_t* __restrict__ cursor, int32_t* __restrict__ cellList) {
+  const int64_t j = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  if (j >= nq) return;
+  const int i = S.ownQ[j];
+  const int64_t k = S.list[i];
   const double2* qv = layer_xy(Lb, Lo, 1 - D.pSide[k]) + D.qS[k];
-  const int nq = D.nQ[k];
-  int q = LQ[i];
-  double2 a = __ldg(qv + q), b = __ldg(qv + (q + 1 < nq ? q + 1 : 0));
-  int x0 = cell_1d(fmin(a.x, b.x), G.x0, G.cw, G.gx), x1 = cell_1d(fmax(a.x, b.x), G.x0, G.cw, G.gx);
-  int y0 = cell_1d(fmin(a.y, b.y), G.y0, G.ch, G.gy), y1 = cell_1d(fmax(a.y, b.y), G.y0, G.ch, G.gy);
+  const int n = D.nQ[k];
+  const int q = binned_q(S, j, i, offQ, LQ);
+  const double2 a = __ldg(qv + q), b = __ldg(qv + (q + 1 < n ? q + 1 : 0));
+  const BinGrid G = S.grid[i];
+  const int64_t cb = S.cellBase[i];
+  const int x0 = cell_1d(fmin(a.x, b.x), G.x0, G.cw, G.gx), x1 = cell_1d(fmax(a.x, b.x), G.x0, G.cw, G.gx);
+  const int y0 = cell_1d(fmin(a.y, b.y), G.y0, G.ch, G.gy), y1 = cell_1d(fmax(a.y, b.y), G.y0, G.ch, G.gy);
   for (int y = y0; y <= y1; ++y)
     for (int x = x0; x <= x1; ++x) {
-      int64_t c = (int64_t)y * G.gx + x;
-      cellList[cellOff[c] + atomicAdd(&cursor[c], 1)] = q;
+      const int64_t c = cb + (int64_t)y * G.gx + x;
+      if (kMode == 0) atomicAdd(&cellCnt[c], 1);
+      else cellList[cellOff[c] + atomicAdd(&cursor[c], 1)] = q;
     }
 }
 
-// mode 0: per P edge, records (P side) and the Q-side count; mode 1: write the records of
-// each P edge at its offset (in cell order: nothing downstream depends on record order).
+// kMode 0: per binned P edge, its records (P side) into recCnt, and the pair's Q-side
+// count into binQ; kMode 1: write the records of each P edge at its offset (in cell
+// order: nothing downstream depends on record order).
 template <int kMode, int kExact>
-__global__ void bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t k, const int32_t* __restrict__ LP,
-                                 int cp, BinGrid G, const int64_t* __restrict__ cellOff,
-                                 const int32_t* __restrict__ cellList, double eps,
-                                 int32_t* __restrict__ recCnt,
-                                 unsigned long long* __restrict__ qTotal, const int64_t* __restrict__ recPos,
-                                 Records R) {
-  int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i >= cp) return;
+__global__ void __launch_bounds__(kThreads, kExact ? 2 : 4)
+bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, BinSet S, int64_t np,
+                 const int64_t* __restrict__ offP, const int32_t* __restrict__ LP,
+                 const int64_t* __restrict__ cellOff, const int32_t* __restrict__ cellList, double eps,
+                 int32_t* __restrict__ recCnt, int64_t* __restrict__ binQ,
+                 const int64_t* __restrict__ recPos, const int64_t* __restrict__ recOff, Records R) {
+  const int64_t j = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  if (j >= np) return;
+  const int i = S.ownP[j];
+  const int64_t k = S.list[i];
   const int pside = D.pSide[k];
   const double2* pv = layer_xy(Lb, Lo, pside) + D.pS[k];
   const double2* qv = layer_xy(Lb, Lo, 1 - pside) + D.qS[k];
   const int np_ = D.nP[k], nq = D.nQ[k];
-  const int p = LP[i];
+  const int p = binned_p(S, j, i, offP, LP);
   const double2 P1 = __ldg(pv + p), P2 = __ldg(pv + (p + 1 < np_ ? p + 1 : 0));
   const double pminx = fmin(P1.x, P2.x), pmaxx = fmax(P1.x, P2.x);
   const double pminy = fmin(P1.y, P2.y), pmaxy = fmax(P1.y, P2.y);
-  int x0 = cell_1d(pminx, G.x0, G.cw, G.gx), x1 = cell_1d(pmaxx, G.x0, G.cw, G.gx);
-  int y0 = cell_1d(pminy, G.y0, G.ch, G.gy), y1 = cell_1d(pmaxy, G.y0, G.ch, G.gy);
+  const BinGrid G = S.grid[i];
+  const int64_t cb = S.cellBase[i];
+  const int x0 = cell_1d(pminx, G.x0, G.cw, G.gx), x1 = cell_1d(pmaxx, G.x0, G.cw, G.gx);
+  const int y0 = cell_1d(pminy, G.y0, G.ch, G.gy), y1 = cell_1d(pmaxy, G.y0, G.ch, G.gy);
   int recs = 0, qhits = 0;
-  int64_t base = (kMode == 1) ? recPos[i] : 0;
+  const int64_t base = (kMode == 1) ? recOff[k] + recPos[j] - recPos[S.pBase[i]] : 0;
   for (int y = y0; y <= y1; ++y)
     for (int x = x0; x <= x1; ++x) {
-      int64_t c = (int64_t)y * G.gx + x;
+      const int64_t c = cb + (int64_t)y * G.gx + x;
       for (int64_t e = cellOff[c]; e < cellOff[c + 1]; ++e) {
-        int q = cellList[e];
-        double2 Q1 = __ldg(qv + q), Q2 = __ldg(qv + (q + 1 < nq ? q + 1 : 0));
+        const int q = cellList[e];
+        const double2 Q1 = __ldg(qv + q), Q2 = __ldg(qv + (q + 1 < nq ? q + 1 : 0));
         if (!edge_boxes_touch(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y)) continue;
-        double cx = fmax(pminx, fmin(Q1.x, Q2.x)), cy = fmax(pminy, fmin(Q1.y, Q2.y));
+        const double cx = fmax(pminx, fmin(Q1.x, Q2.x)), cy = fmax(pminy, fmin(Q1.y, Q2.y));
         if (cell_1d(cx, G.x0, G.cw, G.gx) != x || cell_1d(cy, G.y0, G.ch, G.gy) != y) continue;
         double alpha = 0, beta = 0;
-        int tp = classify_mode(kExact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
+        const int tp = classify_mode(kExact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
         if (kMode == 0) {
           double a2, b2;
           if (classify_mode(kExact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2)) ++qhits;
           if (tp) ++recs;
         } else if (tp) {
-          int64_t r = base + recs++;
+          const int64_t r = base + recs++;
           R.p[r] = p; R.q[r] = q; R.a[r] = alpha; R.b[r] = beta; R.t[r] = (int8_t)tp; R.k[r] = (int32_t)k;
         }
       }
     }
   if (kMode == 0) {
-    recCnt[i] = recs;
-    if (qhits) atomicAdd(qTotal, (unsigned long long)qhits);
+    recCnt[j] = recs;
+    if (qhits) atomicAdd(reinterpret_cast<unsigned long long*>(binQ + k), (unsigned long long)qhits);
   }
 }
 
-__global__ void add_offset_kernel(int64_t* __restrict__ a, int n, const int64_t* __restrict__ off) {
-  int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i < n) a[i] += *off;
-}
-
-// records binned count for a big pair -> per-pair arrays
-__global__ void bin_total_kernel(const int64_t* __restrict__ recTot, const unsigned long long* __restrict__ qTot,
-                                 int64_t k, int64_t* __restrict__ binRec, int64_t* __restrict__ binQ) {
-  binRec[k] = *recTot;
-  binQ[k] = (int64_t)*qTot;
-}
-
-// big-pair parameters gathered for the host
-struct BigInfo { int64_t k; int32_t cp, cq; int64_t offP, offQ; double cmbr[4]; };
-
-__global__ void big_info_kernel(const int64_t* __restrict__ bigList, int n, const int32_t* __restrict__ cP,
-                                const int32_t* __restrict__ cQ, const int64_t* __restrict__ offP,
-                                const int64_t* __restrict__ offQ, PairDev D, BigInfo* __restrict__ out) {
+// per binned pair: its records (the P edges' counts summed through their scan)
+__global__ void bin_rec_total_kernel(BinSet S, int n, const int64_t* __restrict__ recPos,
+                                     int64_t* __restrict__ binRec) {
   int i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= n) return;
-  int64_t k = bigList[i];
-  BigInfo b;
-  b.k = k; b.cp = cP[k]; b.cq = cQ[k]; b.offP = offP[k]; b.offQ = offQ[k];
-  for (int j = 0; j < 4; ++j) b.cmbr[j] = D.cmbr[4 * k + j];
-  out[i] = b;
+  const int64_t b = S.pBase[i];
+  binRec[S.list[i]] = recPos[b + S.cp[i]] - recPos[b];
 }
 
 // ---------------------------------------------------------------- G4 ring layout
@@ -501,15 +557,13 @@ struct RingSet {
   char* b;          // column buffer
   int64_t n;        // slots per column (a multiple of 16, so every column stays aligned)
   int exact;        // orientation signs exact (ClipParams::exact)
-  double2* cxy; int32_t* cnx; int32_t* cpv; int32_t* cnb; int32_t* ctn; int32_t* ctl; int32_t* cto; int32_t* cls;
+  double2* cxy; int32_t* cnx; int32_t* cpv; int32_t* cnb;
   uint8_t* cit; int8_t* clb; int8_t* cee; uint8_t* cfl;
   void set(char* buf, int64_t slots) {
     b = buf; n = slots;
     cxy = reinterpret_cast<double2*>(b);
     cnx = reinterpret_cast<int32_t*>(b + 16 * n); cpv = reinterpret_cast<int32_t*>(b + 20 * n);
-    cnb = reinterpret_cast<int32_t*>(b + 24 * n); ctn = reinterpret_cast<int32_t*>(b + 28 * n);
-    ctl = reinterpret_cast<int32_t*>(b + 32 * n); cto = reinterpret_cast<int32_t*>(b + 36 * n);
-    cls = reinterpret_cast<int32_t*>(b + 40 * n); cit = reinterpret_cast<uint8_t*>(b + 44 * n);
+    cnb = reinterpret_cast<int32_t*>(b + 24 * n); cit = reinterpret_cast<uint8_t*>(b + 44 * n);
     clb = reinterpret_cast<int8_t*>(b + 45 * n); cee = reinterpret_cast<int8_t*>(b + 46 * n);
     cfl = reinterpret_cast<uint8_t*>(b + 47 * n);
   }
@@ -519,10 +573,6 @@ struct RingSet {
   __device__ __forceinline__ int32_t& nx(int64_t i) const { return cnx[i]; }
   __device__ __forceinline__ int32_t& pv(int64_t i) const { return cpv[i]; }
   __device__ __forceinline__ int32_t& nb(int64_t i) const { return cnb[i]; }
-  __device__ __forceinline__ int32_t& tn(int64_t i) const { return ctn[i]; }
-  __device__ __forceinline__ int32_t& tl(int64_t i) const { return ctl[i]; }
-  __device__ __forceinline__ int32_t& to(int64_t i) const { return cto[i]; }
-  __device__ __forceinline__ int32_t& ls(int64_t i) const { return cls[i]; }
   __device__ __forceinline__ uint8_t& it(int64_t i) const { return cit[i]; }
   __device__ __forceinline__ int8_t& lb(int64_t i) const { return clb[i]; }
   __device__ __forceinline__ int8_t& ee(int64_t i) const { return cee[i]; }
@@ -1368,6 +1418,7 @@ __device__ __forceinline__ int wind(double P0x, double P0y, double P1x, double P
 // per pair (BlockGroup); every member executes every group call (uniform control flow).
 struct WarpGroup {
   static constexpr bool kBlock = false;
+  static constexpr bool kSolo = false;
   __device__ __forceinline__ int rank() const { return (int)lane_id(); }
   __device__ __forceinline__ int size() const { return 32; }
   __device__ __forceinline__ void sync() const { __syncwarp(); }
@@ -1393,6 +1444,7 @@ struct WarpGroup {
 template <int W>
 struct TileGroup {
   static constexpr bool kBlock = false;
+  static constexpr bool kSolo = false;
   unsigned mask;
   int base;
   __device__ __forceinline__ TileGroup() {
@@ -1429,6 +1481,7 @@ struct TileGroup {
 // One thread per pair: every collective is the identity, nothing synchronises.
 struct SoloGroup {
   static constexpr bool kBlock = false;
+  static constexpr bool kSolo = true;
   __device__ __forceinline__ int rank() const { return 0; }
   __device__ __forceinline__ int size() const { return 1; }
   __device__ __forceinline__ void sync() const {}
@@ -1447,9 +1500,15 @@ template <> struct TileOf<1> { using type = SoloGroup; };
 // Block-wide versions over shared scratch (kBlockLabelThreads / 32 warps); each call
 // begins with a barrier so the scratch of the previous call is free.
 constexpr int kBlockLabelThreads = 256;
+// Dynamic shared memory of the block labelling kernel: the trace's run table of pairs with
+// up to 8,192 runs (two blocks per SM at its register budget).
+constexpr int kBlockRunTableBytes = 96 * 1024;
 struct BlockGroup {
   static constexpr bool kBlock = true;
+  static constexpr bool kSolo = false;
   long long* sm;        // kBlockLabelThreads / 32 + 1 entries
+  int32_t* runs;        // shared memory for the trace's run table (3 words per run)
+  int runsCap;          // runs that fit
   __device__ __forceinline__ int rank() const { return (int)threadIdx.x; }
   __device__ __forceinline__ int size() const { return kBlockLabelThreads; }
   __device__ __forceinline__ void sync() const { __syncthreads(); }
@@ -1921,9 +1980,9 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
   // run table by list index, in the rings' scratch arrays: length RL, next start RN (sign
   // bit = visited), output offset RO.  The slot -> index map in `to` is read until phase 1
   // ends; the offsets take its place then.  (Pointers are selected per side in registers.)
-  int32_t* const RL0 = &c.R[0].tl(0); int32_t* const RL1 = &c.R[1].tl(0);
-  int32_t* const RN0 = &c.R[0].tn(0); int32_t* const RN1 = &c.R[1].tn(0);
-  int32_t* const RO0 = &c.R[0].to(0); int32_t* const RO1 = &c.R[1].to(0);
+  int32_t* RL0 = &c.R[0].tl(0); int32_t* RL1 = &c.R[1].tl(0);
+  int32_t* RN0 = &c.R[0].tn(0); int32_t* RN1 = &c.R[1].tn(0);
+  int32_t* RO0 = &c.R[0].to(0); int32_t* RO1 = &c.R[1].to(0);
 #define RL_(sd) ((sd) ? RL1 : RL0)
 #define RN_(sd) ((sd) ? RN1 : RN0)
 #define RO_(sd) ((sd) ? RO1 : RO0)
@@ -1952,6 +2011,22 @@ __device__ int grp_trace_runs(const G& g, PairCtx& c) {
     }
   }
   if (g.any(bad)) return 1;
+  if constexpr (G::kBlock) {
+    // The walk below is one long chain of dependent loads: with the table in shared
+    // memory each step costs tens of cycles instead of an L2 round trip.
+    if (nF[0] + nF[1] <= g.runsCap) {
+      int32_t* sh = g.runs;
+      int32_t* dst[6] = {sh, sh + nF[0], sh + 2 * nF[0], sh + 3 * nF[0], sh + 3 * nF[0] + nF[1],
+                         sh + 3 * nF[0] + 2 * nF[1]};
+      for (int sd = 0; sd < 2; ++sd)
+        for (int i = g.rank(); i < nF[sd]; i += g.size()) {
+          dst[3 * sd][i] = RL_(sd)[i];
+          dst[3 * sd + 1][i] = RN_(sd)[i];
+        }
+      RL0 = dst[0]; RN0 = dst[1]; RO0 = dst[2];
+      RL1 = dst[3]; RN1 = dst[4]; RO1 = dst[5];
+    }
+  }
   for (int sd = 0; sd < 2; ++sd)
     for (int i = g.rank(); i < nF[sd]; i += g.size()) RO_(sd)[i] = -1;
   const bool anyLong = g.any(longRun);
@@ -2160,6 +2235,74 @@ __device__ void grp_cleanup(const G& g, PairCtx& c, int32_t* outNC, int64_t* out
       if (g.rank() == 0) { *outNC = O.nc; *outNV = O.nv; }
       return;
     }
+    if constexpr (!G::kSolo) {
+      // Removal with many components: each member cleans whole components in place (a
+      // component's kept vertices move to the front of its own range), then the kept
+      // vertices are compacted, through ring P's coordinate column (free after the
+      // trace) when they fit there.  Per component this is the sequential pass.
+      int32_t* keptA = &c.R[0].ls(0);
+      int32_t* dstA = &c.R[0].tl(0);
+      for (int k = g.rank(); k < O.nc; k += g.size()) {
+        double* src = O.xy + 2 * (int64_t)start[k];
+        keptA[k] = seq_cleanup_component(src, src, O.csz[k], c.eps_clean);
+      }
+      g.sync();
+      long long total = 0;
+      for (int b = 0; b < O.nc; b += g.size()) {
+        const int k = b + g.rank();
+        const int v = (k < O.nc) ? keptA[k] : 0;
+        int tot;
+        const int incl = g.incl_scan(v, tot);
+        if (k < O.nc) dstA[k] = (int32_t)(total + incl - v);
+        total += tot;
+      }
+      g.sync();
+      if (total <= (long long)c.R[0].cap) {
+        double2* stage = &c.R[0].xy(0);
+        for (int k = g.rank(); k < O.nc; k += g.size()) {
+          const int kept = keptA[k];
+          const double* src = O.xy + 2 * (int64_t)start[k];
+          double2* dst = stage + dstA[k];
+          for (int j = 0; j < kept; ++j) dst[j] = make_double2(src[2 * j], src[2 * j + 1]);
+        }
+        g.sync();
+        for (long long t = g.rank(); t < total; t += g.size()) {
+          const double2 v = stage[t];
+          O.xy[2 * t] = v.x;
+          O.xy[2 * t + 1] = v.y;
+        }
+      } else {
+        long long vout = 0;
+        for (int k = 0; k < O.nc; ++k) {
+          const int kept = keptA[k];
+          const double* src = O.xy + 2 * (int64_t)start[k];
+          double* dst = O.xy + 2 * vout;
+          if (kept > 0 && dst != src) {
+            for (int b = 0; b < 2 * kept; b += g.size()) {
+              const int i = b + g.rank();
+              const double v = (i < 2 * kept) ? src[i] : 0.0;
+              g.sync();
+              if (i < 2 * kept) dst[i] = v;
+            }
+          }
+          g.sync();
+          vout += kept;
+        }
+      }
+      g.sync();
+      int cc = 0;
+      for (int b = 0; b < O.nc; b += g.size()) {
+        const int k = b + g.rank();
+        const int f = (k < O.nc && keptA[k] > 0) ? 1 : 0;
+        int tot;
+        const int incl = g.incl_scan(f, tot);
+        if (f) O.csz[cc + incl - 1] = keptA[k];
+        cc += tot;
+      }
+      if (g.rank() == 0) { *outNC = cc; *outNV = (int64_t)total; }
+      g.sync();
+      return;
+    }
   }
   int64_t vin = 0, vout = 0;
   int nc = 0;
@@ -2237,6 +2380,7 @@ struct LabelArgs {
   const int64_t* midList;     // pairs for the block kernel
   const unsigned long long* midCount;
   unsigned long long* midNext; // work-stealing cursor of the block kernel
+  int blockRunCap;            // runs the block kernel's shared run table holds (0: none)
 };
 
 // One pair labelled and traced by group g.  The group phases give the sequential result
@@ -2355,7 +2499,8 @@ __global__ void __launch_bounds__(kBlockLabelThreads)
 label_trace_block_kernel(LabelArgs a) {
   __shared__ long long sm[kBlockLabelThreads / 32 + 1];
   __shared__ long long next;
-  BlockGroup g{sm};
+  extern __shared__ int32_t runTable[];
+  BlockGroup g{sm, runTable, a.blockRunCap};
   const unsigned long long n = *a.midCount;
   for (;;) {
     if (threadIdx.x == 0) next = (long long)atomicAdd(a.midNext, 1ull);
@@ -3299,83 +3444,73 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     exclusive_scan_i32(chunkRec, recScan, nCh, nullptr, stC, d_err, s);
     exclusive_scan_i32(chunkQ, qScan, nCh, nullptr, stC, d_err, s);
   }
-  // ---- G2 count: binned pairs (host loop; few pairs).  It is driven from the host with a
-  // read-back per pair, so with an auxiliary stream it runs there, beside the chunked
-  // count; s waits for it before the per-pair totals.
+  // ---- G2 count: binned pairs, all in the same launches.  With an auxiliary stream they
+  // run there, beside the chunked count; s waits for them before the per-pair totals.
   auto syncb = [&]() { return cudaStreamSynchronize(sb) == cudaSuccess; };
-  struct BigWork { BigInfo info; BinGrid G; int64_t* cellOff; int32_t* cellList; int64_t* recPos; };
-  std::vector<BigWork> bigs(nBigPairs);
+  BinSet BS{};
+  int64_t nBinP = 0, nBinQ = 0;
+  int64_t* cellOff = nullptr;
+  int32_t* cellList = nullptr;
+  int64_t* binRecPos = nullptr;
   if (nBigPairs > 0) {
-    BigInfo* dInfo = A.take_n<BigInfo>(nBigPairs);
-    if (!dInfo) return ST_OUT_OF_MEMORY;
-    { big_info_kernel<<<blocks_for(nBigPairs), kThreads, 0, sb>>>(bigList, nBigPairs, cP, cQ, offP, offQ, D, dInfo); note_launch(); }
-    std::vector<BigInfo> hInfo(nBigPairs);
-    cudaMemcpyAsync(hInfo.data(), dInfo, nBigPairs * sizeof(BigInfo), cudaMemcpyDeviceToHost, sb);
+    const int B = nBigPairs;
+    BS.list = bigList;
+    BS.cp = A.take_n<int32_t>(B); BS.cq = A.take_n<int32_t>(B);
+    BS.pBase = A.take_n<int64_t>(B); BS.qBase = A.take_n<int64_t>(B);
+    BS.ext = A.take_n<double>(2 * B); BS.grid = A.take_n<BinGrid>(B);
+    BS.cellBase = A.take_n<int64_t>(B); BS.ncell = A.take_n<int32_t>(B);
+    int64_t* d_t = A.take_n<int64_t>(4);
+    void* stB = A.take(scan_temp_bytes(B));
+    if (!BS.cp || !BS.cq || !BS.pBase || !BS.qBase || !BS.ext || !BS.grid || !BS.cellBase || !BS.ncell || !d_t ||
+        !stB)
+      return ST_OUT_OF_MEMORY;
+    { bin_sizes_kernel<<<blocks_for(B), kThreads, 0, sb>>>(BS, B, cP, cQ); note_launch(); }
+    exclusive_scan_i32(BS.cp, BS.pBase, B, d_t + 0, stB, d_err, sb);
+    exclusive_scan_i32(BS.cq, BS.qBase, B, d_t + 1, stB, d_err, sb);
+    cudaMemsetAsync(BS.ext, 0, 2 * (size_t)B * sizeof(double), sb);
+    cudaMemcpyAsync(hs + 40, d_t, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, sb);
     if (!syncb()) return ST_CUDA_ERROR;
-    std::sort(hInfo.begin(), hInfo.end(), [](const BigInfo& x, const BigInfo& y) { return x.k < y.k; });
-    int64_t* d_t = A.take_n<int64_t>(2);
-    unsigned long long* d_q = A.take_n<unsigned long long>(1);
-    double* d_ext = A.take_n<double>(2 * nBigPairs);
-    if (!d_t || !d_q || !d_ext) return ST_OUT_OF_MEMORY;
-    cudaMemsetAsync(d_ext, 0, 2 * nBigPairs * sizeof(double), sb);
-    for (int bi = 0; bi < nBigPairs; ++bi)
-      if (hInfo[bi].cq > 0)
-        { edge_extent_kernel<<<blocks_for(hInfo[bi].cq), kThreads, 0, sb>>>(Lb, Lo, D, hInfo[bi].k, LQ + hInfo[bi].offQ,
-                                                                          hInfo[bi].cq, d_ext + 2 * bi); note_launch(); }
-    std::vector<double> hExt(2 * nBigPairs);
-    cudaMemcpyAsync(hExt.data(), d_ext, 2 * nBigPairs * sizeof(double), cudaMemcpyDeviceToHost, sb);
+    nBinP = hs[40];
+    nBinQ = hs[41];
+    BS.ownP = A.take_n<int32_t>(nBinP);
+    BS.ownQ = A.take_n<int32_t>(nBinQ);
+    if (!BS.ownP || !BS.ownQ) return ST_OUT_OF_MEMORY;
+    { range_owner_kernel<<<blocks_for_warps(B), kThreads, 0, sb>>>(BS.pBase, BS.cp, B, BS.ownP); note_launch(); }
+    { range_owner_kernel<<<blocks_for_warps(B), kThreads, 0, sb>>>(BS.qBase, BS.cq, B, BS.ownQ); note_launch(); }
+    if (nBinQ > 0)
+      { bin_extent_kernel<<<blocks_for(nBinQ), kThreads, 0, sb>>>(Lb, Lo, D, BS, nBinQ, offQ, LQ); note_launch(); }
+    { bin_grid_kernel<<<blocks_for(B), kThreads, 0, sb>>>(D, BS, B); note_launch(); }
+    exclusive_scan_i32(BS.ncell, BS.cellBase, B, d_t + 2, stB, d_err, sb);
+    cudaMemcpyAsync(hs + 42, d_t + 2, sizeof(int64_t), cudaMemcpyDeviceToHost, sb);
     if (!syncb()) return ST_CUDA_ERROR;
-    for (int bi = 0; bi < nBigPairs; ++bi) {
-      BigWork& W = bigs[bi];
-      W.info = hInfo[bi];
-      const double w = W.info.cmbr[2] - W.info.cmbr[0], h = W.info.cmbr[3] - W.info.cmbr[1];
-      const double target = (double)std::max(1, W.info.cq);
-      // Cells: about one Q edge per cell, but never smaller than the Q edges' mean box
-      // (long edges would otherwise be listed in many cells and each P edge would scan
-      // them all again); at most 4096 per axis.
-      const double mw = hExt[2 * bi] / target, mh = hExt[2 * bi + 1] / target;
-      int gx = 1, gy = 1;
-      if (w > 0 && h > 0) {
-        gx = (int)std::ceil(std::sqrt(target * w / h));
-        gy = (int)std::ceil(target / gx);
-        if (mw > 0) gx = std::min(gx, (int)std::ceil(w / mw));
-        if (mh > 0) gy = std::min(gy, (int)std::ceil(h / mh));
-        gx = std::min(std::max(gx, 1), 1 << 12);
-        gy = std::min(std::max(gy, 1), 1 << 12);
-      } else if (w > 0) {
-        gx = (int)std::min(target, 4096.0);
-      } else if (h > 0) {
-        gy = (int)std::min(target, 4096.0);
-      }
-      W.G = BinGrid{W.info.cmbr[0], W.info.cmbr[1], w > 0 ? w / gx : 1.0, h > 0 ? h / gy : 1.0, gx, gy};
-      const int64_t ncell = (int64_t)gx * gy;
-      int32_t* cellCnt = A.take_n<int32_t>(ncell + 1);
-      W.cellOff = A.take_n<int64_t>(ncell + 1);
-      int32_t* cursor = A.take_n<int32_t>(ncell);
-      void* st = A.take(scan_temp_bytes(ncell + 1));
-      int32_t* recCnt = A.take_n<int32_t>(W.info.cp);
-      W.recPos = A.take_n<int64_t>(W.info.cp);
-      void* st2 = A.take(scan_temp_bytes(std::max(W.info.cp, 1)));
-      if (!cellCnt || !W.cellOff || !cursor || !st || !recCnt || !W.recPos || !st2) return ST_OUT_OF_MEMORY;
-      cudaMemsetAsync(cellCnt, 0, (ncell + 1) * sizeof(int32_t), sb);
-      cudaMemsetAsync(cursor, 0, ncell * sizeof(int32_t), sb);
-      const int64_t k = W.info.k;
-      { bin_count_kernel<<<blocks_for(W.info.cq), kThreads, 0, sb>>>(Lb, Lo, D, k, LQ + W.info.offQ, W.info.cq, W.G,
-                                                                    cellCnt); note_launch(); }
-      exclusive_scan_i32(cellCnt, W.cellOff, ncell + 1, d_t, st, d_err, sb);
-      cudaMemcpyAsync(hs, d_t, sizeof(int64_t), cudaMemcpyDeviceToHost, sb);
-      if (!syncb()) return ST_CUDA_ERROR;
-      W.cellList = A.take_n<int32_t>(hs[0]);
-      if (!W.cellList) return ST_OUT_OF_MEMORY;
-      { bin_fill_kernel<<<blocks_for(W.info.cq), kThreads, 0, sb>>>(Lb, Lo, D, k, LQ + W.info.offQ, W.info.cq, W.G,
-                                                                   W.cellOff, cursor, W.cellList); note_launch(); }
-      cudaMemsetAsync(d_q, 0, sizeof(unsigned long long), sb);
-      { (prm.exact ? bin_pairs_kernel<0, 1> : bin_pairs_kernel<0, 0>)<<<blocks_for(W.info.cp), kThreads, 0, sb>>>(
-            Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G, W.cellOff, W.cellList, prm.eps, recCnt, d_q,
-                                                                       nullptr, R); note_launch(); }
-      exclusive_scan_i32(recCnt, W.recPos, W.info.cp, d_t + 1, st2, d_err, sb);
-      { bin_total_kernel<<<1, 1, 0, sb>>>(d_t + 1, d_q, k, binRec, binQ); note_launch(); }
-    }
+    const int64_t nCells = hs[42];
+    int32_t* cellCnt = A.take_n<int32_t>(nCells + 1);
+    cellOff = A.take_n<int64_t>(nCells + 1);
+    int32_t* cursor = A.take_n<int32_t>(nCells);
+    void* stCell = A.take(scan_temp_bytes(nCells + 1));
+    if (!cellCnt || !cellOff || !cursor || !stCell) return ST_OUT_OF_MEMORY;
+    cudaMemsetAsync(cellCnt, 0, (nCells + 1) * sizeof(int32_t), sb);
+    cudaMemsetAsync(cursor, 0, nCells * sizeof(int32_t), sb);
+    if (nBinQ > 0)
+      { bin_cells_kernel<0><<<blocks_for(nBinQ), kThreads, 0, sb>>>(Lb, Lo, D, BS, nBinQ, offQ, LQ, cellCnt, nullptr,
+                                                                   nullptr, nullptr); note_launch(); }
+    exclusive_scan_i32(cellCnt, cellOff, nCells + 1, d_t + 3, stCell, d_err, sb);
+    cudaMemcpyAsync(hs + 43, d_t + 3, sizeof(int64_t), cudaMemcpyDeviceToHost, sb);
+    if (!syncb()) return ST_CUDA_ERROR;
+    cellList = A.take_n<int32_t>(hs[43]);
+    int32_t* binRecCnt = A.take_n<int32_t>(nBinP + 1);
+    binRecPos = A.take_n<int64_t>(nBinP + 1);
+    void* stP = A.take(scan_temp_bytes(nBinP + 1));
+    if (!cellList || !binRecCnt || !binRecPos || !stP) return ST_OUT_OF_MEMORY;
+    if (nBinQ > 0)
+      { bin_cells_kernel<1><<<blocks_for(nBinQ), kThreads, 0, sb>>>(Lb, Lo, D, BS, nBinQ, offQ, LQ, nullptr, cellOff,
+                                                                   cursor, cellList); note_launch(); }
+    cudaMemsetAsync(binRecCnt + nBinP, 0, sizeof(int32_t), sb);     // so the scan's last entry is the total
+    if (nBinP > 0)
+      { (prm.exact ? bin_pairs_kernel<0, 1> : bin_pairs_kernel<0, 0>)<<<blocks_for(nBinP), kThreads, 0, sb>>>(
+            Lb, Lo, D, BS, nBinP, offP, LP, cellOff, cellList, prm.eps, binRecCnt, binQ, nullptr, nullptr, R); note_launch(); }
+    exclusive_scan_i32(binRecCnt, binRecPos, nBinP + 1, nullptr, stP, d_err, sb);
+    { bin_rec_total_kernel<<<blocks_for(B), kThreads, 0, sb>>>(BS, B, binRecPos, binRec); note_launch(); }
   }
   if (sb != s) {
     cudaEventRecord(bev[1], sb);
@@ -3398,21 +3533,17 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   R.a = A.take_n<double>(nR); R.b = A.take_n<double>(nR);
   R.t = A.take_n<int8_t>(nR); R.k = A.take_n<int32_t>(nR);
   if (!R.p || !R.q || !R.a || !R.b || !R.t || !R.k) return ST_OUT_OF_MEMORY;
-  if (sb != s && !bigs.empty()) {                   // the binned pairs' emit beside the chunked one
+  if (sb != s && nBigPairs > 0) {                   // the binned pairs' emit beside the chunked one
     cudaEventRecord(bev[0], s);
     cudaStreamWaitEvent(sb, bev[0], 0);
   }
   if (nCh > 0)
     { (prm.exact ? intersect_kernel<1, 1> : intersect_kernel<1, 0>)<<<blocks_for_warps(nCh), kThreads, 0, s>>>(
         Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, recOff, R, chunkPair); note_launch(); }
-  for (auto& W : bigs) {
-    const int64_t k = W.info.k;
-    { add_offset_kernel<<<blocks_for(W.info.cp), kThreads, 0, sb>>>(W.recPos, W.info.cp, recOff + k); note_launch(); }
-    { (prm.exact ? bin_pairs_kernel<1, 1> : bin_pairs_kernel<1, 0>)<<<blocks_for(W.info.cp), kThreads, 0, sb>>>(
-          Lb, Lo, D, k, LP + W.info.offP, W.info.cp, W.G, W.cellOff, W.cellList, prm.eps, nullptr, nullptr,
-                                                                      W.recPos, R); note_launch(); }
-  }
-  if (sb != s && !bigs.empty()) {
+  if (nBinP > 0)
+    { (prm.exact ? bin_pairs_kernel<1, 1> : bin_pairs_kernel<1, 0>)<<<blocks_for(nBinP), kThreads, 0, sb>>>(
+        Lb, Lo, D, BS, nBinP, offP, LP, cellOff, cellList, prm.eps, nullptr, nullptr, binRecPos, recOff, R); note_launch(); }
+  if (sb != s && nBigPairs > 0) {
     cudaEventRecord(bev[1], sb);
     cudaStreamWaitEvent(s, bev[1], 0);
   }
@@ -3619,25 +3750,30 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   { out_sizes_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, nrec, D.status, K, vcap, ccap); note_launch(); }
   exclusive_scan_i64(vcap, vOff, K, tot + 13, stK, d_err, s);
   exclusive_scan_i32(ccap, cOff, K, tot + 14, stK, d_err, s);
+  // the pairs for the block kernel (their count is read with the output sizes)
+  int64_t* mlist = A.take_n<int64_t>(K);
+  unsigned long long* mcnt = A.take_n<unsigned long long>(2);
+  if (!mlist || !mcnt) return ST_OUT_OF_MEMORY;
+  cudaMemsetAsync(mcnt, 0, 2 * sizeof(unsigned long long), s);
+  const int64_t midMin = std::min(prm.mid_label_min, prm.big_label_min);
+  { mid_label_list_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, D.status, K, midMin, prm.big_label_min,
+                                                            mlist, mcnt); note_launch(); }
   cudaMemcpyAsync(hs, tot + 13, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hs + 2, mcnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
   double* oxy = A.take_n<double>(2 * hs[0]);
   int32_t* ocsz = A.take_n<int32_t>(hs[1]);
+  const int64_t nMid = hs[2];
   if (!oxy || !ocsz) return ST_OUT_OF_MEMORY;
   mk->mark("clip:fill+link", s);
   {
-    int64_t* mlist = A.take_n<int64_t>(K);
-    unsigned long long* mcnt = A.take_n<unsigned long long>(2);
-    if (!mlist || !mcnt) return ST_OUT_OF_MEMORY;
-    cudaMemsetAsync(mcnt, 0, 2 * sizeof(unsigned long long), s);
     cudaMemsetAsync(nc, 0, K * sizeof(int32_t), s);
     cudaMemsetAsync(nv, 0, K * sizeof(int64_t), s);
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     LabelArgs la{D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ, SP, SQ, oxy, vOff, vcap, ocsz, cOff, ccap, nc, nv,
-                 prm, d_err, prm.tile_label_max, std::min(prm.mid_label_min, prm.big_label_min), prm.big_label_min,
-                 mlist, mcnt, mcnt + 1};
+                 prm, d_err, prm.tile_label_max, midMin, prm.big_label_min, mlist, mcnt, mcnt + 1};
     // long pairs: a block each, on the auxiliary stream when there is one, so they start
     // first and overlap the warp-per-pair kernel instead of trailing it
     cudaStream_t ls = s;
@@ -3648,9 +3784,17 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
       cudaStreamWaitEvent(aux, fork, 0);
       ls = aux;
     }
-    { mid_label_list_kernel<<<blocks_for(K), kThreads, 0, ls>>>(mP, mQ, D.status, K, la.midLabelMin, la.bigLabelMin,
-                                                               mlist, mcnt); note_launch(); }
-    { (prm.exact ? label_trace_block_kernel<1> : label_trace_block_kernel<0>)<<<2 * nsm, kBlockLabelThreads, 0, ls>>>(la); note_launch(); }
+    if (nMid > 0) {
+      // The run table goes to shared memory only when block pairs make up at least a
+      // quarter of the batch: otherwise the one-thread and warp kernels beside this one
+      // need the SMs' L1 more (batched workload: label stage 2.02 -> 2.52 ms with it).
+      const int smem = (4 * nMid >= K) ? kBlockRunTableBytes : 0;
+      auto kern = prm.exact ? label_trace_block_kernel<1> : label_trace_block_kernel<0>;
+      if (smem) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      la.blockRunCap = smem / 12;
+      kern<<<(unsigned)std::min<int64_t>(2 * nsm, nMid), kBlockLabelThreads, smem, ls>>>(la);
+      note_launch();
+    }
     const bool wide = K >= prm.wide_label_min;
     // the warp-per-pair pairs on the third stream, beside the one-thread pairs on s
     cudaStream_t ws = s;
