@@ -49,6 +49,11 @@ def parse():
                     help="reference arm: base polygons per step sample (0: auto)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving latency section")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the host-core reference sample")
+    ap.add_argument("--precision-pairs", type=int, default=1_000_000, help="pairs of the degeneracy batch")
+    ap.add_argument("--precision-chunk", type=int, default=50_000, help="pairs generated and clipped at once")
+    ap.add_argument("--precision-check-all", action="store_true",
+                    help="compare every degenerate pair (not a sample) with the oracle")
+    ap.add_argument("--no-precision", action="store_true", help="skip the degeneracy batch")
     return ap.parse_args()
 
 
@@ -326,62 +331,133 @@ def plain_measure(eng, db, do, stream, n=2000, seed=9):
 
 # ----------------------------------------------------------------------------- precision
 
-def precision_measure(local, n=2000, n_check=150):
-    """The degeneracy-stressed batch (independent pairs, vertex counts log-uniform on
-    [4, 10000]; 2% share a vertex exactly, 1% have collinear overlapping edges, 1% are
-    translated by 1e-12 relative; seed 3), a seeded sample of n pairs: clipped in exact
-    mode and in the reference's tolerance mode, timed with CUDA events; the exact results
-    of n_check pairs (every degenerate one among them) compared with the oracle."""
+def _area(comps):
+    """Total signed shoelace area of a result's components."""
+    a = 0.0
+    for c in comps:
+        if len(c) >= 3:
+            x, y = c[:, 0], c[:, 1]
+            a += 0.5 * float(np.dot(x, np.roll(y, -1)) - np.dot(np.roll(x, -1), y))
+    return a
+
+
+def _compare(gpu_st, gpu_comps, orc):
+    """Parity of GPU results against the oracle's: status and component structure equal,
+    max relative vertex error, max relative area error."""
+    same_status = bool(np.array_equal(gpu_st, orc.status))
+    same_structure = True
+    max_v = max_a = 0.0
+    for k, a in enumerate(gpu_comps):
+        b = orc.components(k)
+        if len(a) != len(b) or any(x.shape != y.shape for x, y in zip(a, b)):
+            same_structure = False
+            continue
+        for x, y in zip(a, b):
+            if x.size:
+                max_v = max(max_v, float(np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-300))))
+        aa, ab = _area(a), _area(b)
+        if aa != ab:
+            max_a = max(max_a, abs(aa - ab) / max(abs(ab), 1e-300))
+    return {"status_equal": same_status, "identical_structure": same_structure,
+            "max_rel_vertex_error": max_v, "max_rel_area_error": max_a}
+
+
+def precision_measure(local, total=1_000_000, chunk=50_000, check_degenerate=1200, check_generic=600,
+                      check_all_degenerate=False):
+    """The degeneracy-stressed batch at its full size: `total` independent pairs (vertex
+    counts log-uniform on [4, 10000]; 2% share a vertex exactly, 1% have collinear
+    overlapping edges, 1% are translated by 1e-12 relative; seed 3), generated on the GPU
+    in chunks of `chunk` pairs and clipped chunk by chunk in exact mode and in the
+    reference's tolerance mode (eps 1e-7), each clip timed with CUDA events.  A stratified
+    sample -- `check_degenerate` degenerate and `check_generic` generic pairs spread over
+    the chunks (every degenerate pair with check_all_degenerate) -- is compared with the
+    FP64 oracle in both modes: status, component structure, relative vertex and area
+    error.  Pairs that end in status 3 are the ones whose trace does not close: the
+    reference's own clipper loops on them (its trace appends vertices without end), the
+    engine and the oracle stop the walk and report the pair."""
     import torch
     import gcmfgh
     import pyoracle
     from gcmfgh import synth
-    classes, pairs = synth.degeneracy_pairs(3, n, 4, 10_000)
-    base = synth.Layer.from_rings([p for p, _ in pairs])
-    ovl = synth.Layer.from_rings([q for _, q in pairs])
-    ids = np.arange(n, dtype=np.int32)
+    dev = torch.device("cuda", local)
     eng = gcmfgh.Engine(local)
-    db, do = gcmfgh.DeviceLayer(base, f"cuda:{local}"), gcmfgh.DeviceLayer(ovl, f"cuda:{local}")
-    out = {"workload": "degeneracy batch: %d pairs, vertex counts log-uniform [4, 10000], classes "
-                       "shared-vertex / collinear-overlap / 1e-12-translated at 2%%/1%%/1%%, seed 3" % n}
-    for exact in (True, False):
-        eng.set_precision(exact)
-        eng.clip_batch(db, do, ids, ids)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        info = eng.clip_batch(db, do, ids, ids)
-        e1.record()
-        e1.synchronize()
-        key = "exact" if exact else "reference_mode"
-        out[key] = {"pairs_per_s": n / (e0.elapsed_time(e1) * 1e-3), "invalid_pairs": info["n_invalid"],
-                    "errors": info["n_error"]}
-        if exact:
-            r = eng.clip_result()
-    eng.set_precision(False)
+    nchunks = (total + chunk - 1) // chunk
+    modes = {"exact": True, "reference_mode": False}
+    agg = {m: {"pairs": 0, "ms": 0.0, "invalid_pairs": 0, "errors": 0, "disjoint_pairs": 0, "components": 0,
+               "vertices": 0, "records": 0} for m in modes}
+    classes_all = np.zeros(4, np.int64)
     rng = np.random.default_rng(33)
-    degenerate = np.flatnonzero(classes > 0)
-    rest = np.setdiff1d(np.arange(n), degenerate)
-    chk = np.sort(np.concatenate([degenerate, rng.choice(rest, size=max(0, n_check - len(degenerate)), replace=False)]))
-    sub_b = synth.Layer.from_rings([pairs[i][0] for i in chk])
-    sub_o = synth.Layer.from_rings([pairs[i][1] for i in chk])
-    sid = np.arange(len(chk), dtype=np.int32)
-    o = pyoracle.clip_batch(sub_b, sub_o, sid, sid, exact=True)
-    comps_gpu = [r.components(int(i)) for i in chk]
-    comps_orc = [o.components(k) for k in range(len(chk))]
-    maxrel = 0.0
-    same = True
-    for a, b in zip(comps_gpu, comps_orc):
-        if len(a) != len(b) or any(x.shape != y.shape for x, y in zip(a, b)):
-            same = False
-            continue
-        for x, y in zip(a, b):
-            if x.size:
-                maxrel = max(maxrel, float(np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-300))))
-    out["oracle_check"] = {"pairs": int(len(chk)), "degenerate_pairs": int(len(degenerate)),
-                           "identical_structure": same, "max_rel_vertex_error": maxrel,
-                           "status_equal": bool(np.array_equal(r.status[chk], o.status))}
+    samples = {m: [] for m in modes}          # (P ring, Q ring, status, components)
+    per_deg = (check_degenerate + nchunks - 1) // nchunks
+    per_gen = (check_generic + nchunks - 1) // nchunks
+    for c in range(nchunks):
+        n = min(chunk, total - c * chunk)
+        cls, B, O = synth.degeneracy_chunk_device(3, c, n, device=dev)
+        classes_all += np.bincount(cls, minlength=4)
+        db, do = gcmfgh.DeviceLayer.from_tensors(*B), gcmfgh.DeviceLayer.from_tensors(*O)
+        ids = torch.arange(n, dtype=torch.int32, device=dev)
+        deg = np.flatnonzero(cls > 0)
+        gen = np.flatnonzero(cls == 0)
+        if not check_all_degenerate:
+            deg = rng.choice(deg, size=min(per_deg, len(deg)), replace=False)
+        sel = np.sort(np.concatenate([deg, rng.choice(gen, size=min(per_gen, len(gen)), replace=False)]))
+        bv, bp = B[1].cpu().numpy(), B[2].cpu().numpy()
+        ov, op = O[1].cpu().numpy(), O[2].cpu().numpy()
+        rings = []
+        for k in sel:
+            k = int(k)
+            pb = B[0][2 * (bp[k] - bv[k]):2 * (bp[k] - 1)].cpu().numpy().reshape(-1, 2)
+            pq = O[0][2 * (op[k] - ov[k]):2 * (op[k] - 1)].cpu().numpy().reshape(-1, 2)
+            rings.append((pb, pq, int(cls[k])))
+        for m, exact in modes.items():
+            eng.set_precision(exact)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            info = eng.clip_batch(db, do, ids, ids)
+            e1.record()
+            e1.synchronize()
+            a = agg[m]
+            a["pairs"] += n
+            a["ms"] += e0.elapsed_time(e1)
+            a["invalid_pairs"] += info["n_invalid"]
+            a["errors"] += info["n_error"]
+            a["disjoint_pairs"] += info["n_disjoint"]
+            a["components"] += info["n_components"]
+            a["vertices"] += info["n_vertices"]
+            a["records"] += info["n_records"]
+            if info["n_error"]:
+                stat = eng.clip_field("status")
+                a.setdefault("errors_by_class", np.zeros(4, np.int64))
+                a["errors_by_class"] += np.bincount(cls[stat == 3], minlength=4)
+            st, comps = eng.clip_result_pairs(sel)
+            samples[m].extend((r[0], r[1], s_, cc, r[2]) for r, s_, cc in zip(rings, st, comps))
+        del db, do, B, O
+    eng.set_precision(False)
     eng.close()
+    out = {"workload": "degeneracy batch: %d pairs generated on the GPU in chunks of %d, vertex counts "
+                       "log-uniform [4, 10000], classes shared-vertex / collinear-overlap / "
+                       "1e-12-translated at 2%%/1%%/1%%, seed 3" % (total, chunk),
+           "pairs": total, "classes": {"generic": int(classes_all[0]), "shared_vertex": int(classes_all[1]),
+                                       "collinear_overlap": int(classes_all[2]),
+                                       "translated_1e-12": int(classes_all[3])}}
+    for m, exact in modes.items():
+        a = agg[m]
+        sub_b = synth.Layer.from_rings([r[0] for r in samples[m]])
+        sub_o = synth.Layer.from_rings([r[1] for r in samples[m]])
+        sid = np.arange(len(samples[m]), dtype=np.int32)
+        t0 = time.perf_counter()
+        o = pyoracle.clip_batch(sub_b, sub_o, sid, sid, exact=exact)
+        t_orc = time.perf_counter() - t0
+        chk = _compare(np.array([s_[2] for s_ in samples[m]]), [s_[3] for s_ in samples[m]], o)
+        chk.update({"pairs": len(sid), "degenerate_pairs": int(sum(1 for x in samples[m] if x[4] > 0)),
+                    "oracle_s": round(t_orc, 2), "status3_pairs_in_sample": int(np.sum(o.status == 3))})
+        out[m] = {"pairs_per_s": a["pairs"] / (a["ms"] * 1e-3), "ms_total": a["ms"],
+                  "invalid_pairs": a["invalid_pairs"], "errors": a["errors"], "disjoint_pairs": a["disjoint_pairs"],
+                  "components": a["components"], "vertices": a["vertices"], "records": a["records"],
+                  "errors_by_class": dict(zip(("generic", "shared_vertex", "collinear_overlap", "translated_1e-12"),
+                                              [int(x) for x in a.get("errors_by_class", np.zeros(4))])),
+                  "oracle_check": chk}
     return out
 
 
@@ -538,7 +614,9 @@ def run_ours(args, rank, world, local):
         line["plain"] = plain
         if not args.no_serve:
             line["serving"] = serve_measure(local)
-            line["precision"] = precision_measure(local)
+        if not args.no_precision:
+            line["precision"] = precision_measure(local, total=args.precision_pairs, chunk=args.precision_chunk,
+                                                  check_all_degenerate=args.precision_check_all)
         if world == 1 and not args.no_cpu_baseline:
             nb = args.sample_bases or 20000
             p, s, cores = reference_cpu_sample(base, ovl, nb, 7)

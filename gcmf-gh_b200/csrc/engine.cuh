@@ -74,7 +74,7 @@ struct ClipParams {
   int union_mode = 0;         // polyclip.h:42 UNION
   int no_swap = 0;            // 1: clip base as P even when it has fewer vertices
   int exact = 0;              // 1: exact orientation/classification signs (eps unused there)
-  int64_t bin_grid = 1ll << 24;        // edge-pair grid above which a pair's edges are binned
+  int64_t bin_grid = 1ll << 16;        // edge-pair grid above which a pair's edges are binned
   int64_t tile_label_max = 96;         // merged-ring slots up to which one thread labels a pair
   int64_t wide_label_min = 1 << 16;    // clip batches of at least this many pairs use the
                                        // high-occupancy labelling kernels

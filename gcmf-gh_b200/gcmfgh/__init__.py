@@ -164,6 +164,21 @@ class DeviceLayer:
                        layer.n_polys, layer.n_vertices)
 
 
+def _device_layer_from_tensors(xy, vnum, vps):
+    """DeviceLayer over device tensors already in the layer layout (xy f64 interleaved
+    with closing vertices, vnum i32, vps i64 inclusive)."""
+    d = DeviceLayer.__new__(DeviceLayer)
+    d.layer = None
+    d.xy, d.vnum, d.vps = xy.contiguous(), vnum.contiguous(), vps.contiguous()
+    n = int(d.vnum.numel())
+    nv = int(d.vps[-1].item()) if n else 0
+    d.c = Layer(d.xy.data_ptr(), d.vnum.data_ptr(), d.vps.data_ptr(), n, nv)
+    return d
+
+
+DeviceLayer.from_tensors = staticmethod(_device_layer_from_tensors)
+
+
 def host_layer(layer):
     """C view of a host (numpy) layer for the host-buffer entry point."""
     return Layer(layer.xy.ctypes.data, layer.vnum.ctypes.data, layer.vps.ctypes.data,
@@ -279,8 +294,12 @@ class Engine:
     def clip_batch(self, dbase: DeviceLayer, dovl: DeviceLayer, pid, qid):
         import torch
         dev = dbase.xy.device
-        p = torch.as_tensor(np.ascontiguousarray(pid, np.int32)).to(dev)
-        q = torch.as_tensor(np.ascontiguousarray(qid, np.int32)).to(dev)
+        if isinstance(pid, torch.Tensor):
+            p = pid.to(device=dev, dtype=torch.int32).contiguous()
+            q = qid.to(device=dev, dtype=torch.int32).contiguous()
+        else:
+            p = torch.as_tensor(np.ascontiguousarray(pid, np.int32)).to(dev)
+            q = torch.as_tensor(np.ascontiguousarray(qid, np.int32)).to(dev)
         info = ClipInfo()
         _check(lib().gh_clip_batch(self.h, ctypes.byref(dbase.c), ctypes.byref(dovl.c),
                                    ctypes.c_void_p(p.data_ptr()), ctypes.c_void_p(q.data_ptr()),
@@ -337,6 +356,40 @@ class Engine:
             return r
         finally:
             lib().gh_free_intersections(ctypes.byref(x))
+
+    def clip_result_pairs(self, pairs):
+        """Host copies of the results of the listed pairs only (the rest stays on the
+        device): (status, [components per pair])."""
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+
+        def field(name):
+            fid, dt = CLIP_FIELDS[name]
+            p = ctypes.c_void_p()
+            n = ctypes.c_int64()
+            _check(lib().gh_clip_ptr(self.h, fid, ctypes.byref(p), ctypes.byref(n)))
+            out = torch.empty(max(n.value, 1), dtype={np.int32: torch.int32, np.int64: torch.int64,
+                                                      np.float64: torch.float64}[dt], device=dev)
+            nb = ctypes.c_int64()
+            _check(lib().gh_clip_get(self.h, fid, ctypes.c_void_p(out.data_ptr()),
+                                     out.numel() * out.element_size(), 1, ctypes.byref(nb)))
+            return out[:n.value]
+
+        pairs = np.asarray(pairs, np.int64)
+        status, ncomp = field("status"), field("ncomp")
+        coff, voff, csz, xy = field("comp_off"), field("vert_off"), field("comp_size"), field("xy")
+        sel = torch.as_tensor(pairs, device=dev)
+        st = status[sel].cpu().numpy()
+        nc = ncomp[sel].cpu().numpy()
+        c0 = coff[sel].cpu().numpy()
+        v0 = voff[sel].cpu().numpy()
+        comps = []
+        for k in range(len(pairs)):
+            sizes = csz[int(c0[k]):int(c0[k]) + int(nc[k])].cpu().numpy() if nc[k] else np.zeros(0, np.int32)
+            n = int(sizes.sum())
+            v = xy[2 * int(v0[k]):2 * (int(v0[k]) + n)].cpu().numpy().reshape(-1, 2)
+            comps.append(np.split(v, np.cumsum(sizes)[:-1]) if n else [])
+        return st, comps
 
     def clip_result(self):
         return ClipResult(self.clip_field("status"), self.clip_field("ncomp"), self.clip_field("count1"),

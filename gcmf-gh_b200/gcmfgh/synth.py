@@ -234,3 +234,89 @@ def holed_pairs(seed: int, npairs: int, vmin: int = 5, vmax: int = 30):
         Q = holed_polygon(rng, d[0], d[1], vmin, vmax)
         pairs.append((P, Q))
     return pairs
+
+
+def degeneracy_chunk_device(seed: int, chunk: int, npairs: int, device="cuda:0", vmin: int = 4,
+                            vmax: int = 10_000, quantum: float = 2.0 ** -20):
+    """One chunk of the degeneracy-stressed batch, generated on the GPU with torch (the
+    million-pair batch does not fit the host loop of degeneracy_pairs): the same
+    distributions and classes as degeneracy_pairs, from the seeded stream (seed, chunk).
+
+    Vertex counts log-uniform on [vmin, vmax]; centres uniform on [0, 1000]^2; radius
+    10 * U(0.6, 1.0) per vertex at sorted uniform angles (counter-clockwise); class 1 (2%):
+    both polygons on the `quantum` lattice and the overlay translated so that one of its
+    vertices equals one of the base's; class 2 (1%): the base on the lattice and the
+    overlay = base translated along one of its edges by a quarter of that edge (collinear
+    overlapping edges, same vertex count); class 3 (1%): overlay = base translated by
+    1e-12 x max |coordinate|; class 0: an independent star centred within +-10.
+    Returns (classes int8 numpy, base (xy, vnum, vps), overlay (xy, vnum, vps)) with the
+    layers as device tensors in the layer layout (closing vertex stored)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed) * 1_000_003 + int(chunk))
+    f64 = dict(dtype=torch.float64, device=device)
+    lo, hi = np.log(vmin), np.log(vmax + 1)
+
+    def U(*shape):
+        return torch.rand(*shape, generator=g, **f64)
+
+    n = npairs
+    cnt = torch.exp(lo + (hi - lo) * U(n, 2)).floor().clamp_(vmin, vmax).to(torch.int64)
+    u = U(n)
+    cls = torch.zeros(n, dtype=torch.int8, device=device)
+    cls[u < 0.04] = 3
+    cls[u < 0.03] = 2
+    cls[u < 0.02] = 1
+    cnt[:, 1] = torch.where((cls == 2) | (cls == 3), cnt[:, 0], cnt[:, 1])
+    centre = 1000.0 * U(n, 2)
+    off = torch.where((cls == 1).unsqueeze(1), 16.0 * U(n, 2) - 8.0, 20.0 * U(n, 2) - 10.0)
+
+    def stars(counts, centres):
+        tot = int(counts.sum())
+        pid = torch.repeat_interleave(torch.arange(counts.numel(), device=device), counts)
+        ang = 2.0 * np.pi * U(tot)
+        order = torch.argsort(pid.to(torch.float64) + ang / (2.0 * np.pi + 1e-9))
+        ang = ang[order]
+        rad = 10.0 * (0.6 + 0.4 * U(tot))
+        x = centres[pid, 0] + rad * torch.cos(ang)
+        y = centres[pid, 1] + rad * torch.sin(ang)
+        return torch.stack([x, y], 1), pid
+
+    P, pidP = stars(cnt[:, 0], centre)
+    Q, pidQ = stars(cnt[:, 1], centre + off)
+    startP = torch.cumsum(cnt[:, 0], 0) - cnt[:, 0]
+    startQ = torch.cumsum(cnt[:, 1], 0) - cnt[:, 1]
+    lat = ((cls == 1) | (cls == 2))
+    P = torch.where(lat[pidP].unsqueeze(1), torch.round(P / quantum) * quantum, P)
+    Q = torch.where((cls == 1)[pidQ].unsqueeze(1), torch.round(Q / quantum) * quantum, Q)
+    # class 1: translate Q so that Q[j] == P[i]
+    i1 = (U(n) * cnt[:, 0]).floor().to(torch.int64).clamp_(max=cnt[:, 0] - 1)
+    j1 = (U(n) * cnt[:, 1]).floor().to(torch.int64).clamp_(max=cnt[:, 1] - 1)
+    shift1 = P[startP + i1] - Q[startQ + j1]
+    # class 2: Q = P + 0.25 (P[i+1] - P[i]) (P's vertex count)
+    i2 = (U(n) * cnt[:, 0]).floor().to(torch.int64).clamp_(max=cnt[:, 0] - 1)
+    i2n = torch.where(i2 + 1 < cnt[:, 0], i2 + 1, torch.zeros_like(i2))
+    shift2 = 0.25 * (P[startP + i2n] - P[startP + i2])
+    # class 3: Q = P + 1e-12 max|P|
+    amax = torch.zeros(n, **f64).scatter_reduce(0, pidP, P.abs().amax(1), reduce="amax", include_self=True)
+    samePQ = ((cls == 2) | (cls == 3))[pidQ].unsqueeze(1)
+    # for classes 2 and 3 the overlay's vertices are the base's, vertex for vertex
+    local = torch.arange(Q.shape[0], device=device) - startQ[pidQ]
+    Pfor = P[startP[pidQ] + torch.minimum(local, cnt[pidQ, 0] - 1)]
+    Q = torch.where(samePQ, Pfor, Q)
+    c = cls[pidQ].unsqueeze(1)
+    Q = torch.where(c == 1, Q + shift1[pidQ], Q)
+    Q = torch.where(c == 2, Q + shift2[pidQ], Q)
+    Q = torch.where(c == 3, Q + (1e-12 * amax)[pidQ].unsqueeze(1), Q)
+
+    def layer(V, counts, start):
+        vnum = counts + 1
+        ends = torch.cumsum(vnum, 0)
+        xy = torch.empty(int(ends[-1]) if n else 0, 2, **f64)
+        pos = torch.arange(V.shape[0], device=device)
+        pid = torch.repeat_interleave(torch.arange(n, device=device), counts)
+        xy[pos + pid] = V                                   # each polygon shifted by its closing vertices
+        xy[ends - 1] = V[start]
+        return xy.reshape(-1).contiguous(), vnum.to(torch.int32), ends.to(torch.int64)
+
+    return cls.cpu().numpy(), layer(P, cnt[:, 0], startP), layer(Q, cnt[:, 1], startQ)

@@ -126,7 +126,7 @@ gcmfgh_status gcmfgh_set_precision(gcmfgh_ctx* ctx, int mode);
 const char* gcmfgh_status_string(gcmfgh_status s);
 /* Work-distribution thresholds of the clip (results do not depend on them):
  * GCMFGH_TUNE_BIN_GRID: a pair whose common-MBR edge grid exceeds this many edge pairs
- * has its edges binned on a uniform grid instead of enumerated (default 2^24);
+ * has its edges binned on a uniform grid instead of enumerated (default 2^16);
  * GCMFGH_TUNE_MID_LABEL: a pair whose merged rings exceed this many vertices is labelled
  * and traced by one thread block (persistent, work-stealing) instead of one warp
  * (default 2^10);

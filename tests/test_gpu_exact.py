@@ -10,7 +10,7 @@ from gcmfgh import synth
 
 pytestmark = pytest.mark.gpu
 
-BIN_DEFAULT, BIG_DEFAULT = 1 << 24, 1 << 18
+BIN_DEFAULT, BIG_DEFAULT = 1 << 16, 1 << 18
 
 
 def _run(engine, base, ovl, ids_p, ids_q, union=False, bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT):

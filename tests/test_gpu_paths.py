@@ -10,7 +10,7 @@ from gcmfgh import synth
 
 pytestmark = pytest.mark.gpu
 
-BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT, TILE_DEFAULT, WIDE_DEFAULT = 1 << 24, 1 << 18, 1 << 10, 96, 1 << 16
+BIN_DEFAULT, BIG_DEFAULT, MID_DEFAULT, TILE_DEFAULT, WIDE_DEFAULT = 1 << 16, 1 << 18, 1 << 10, 96, 1 << 16
 
 
 def _run(engine, base, ovl, pid, qid, union=False, bin_grid=BIN_DEFAULT, big_label=BIG_DEFAULT,
