@@ -5,11 +5,12 @@
 
 Workload (one step): the GCMF join of two layers of 200,000 FP64 star polygons (vertex
 counts floor(Pareto(1.5, 4)) capped at 100,000; centres from a 64-component Gaussian
-mixture over [0,1e5]^2, sigma 2,000; base radius log-normal(ln 50, 0.7); seed 2 on rank
-0, 2+r on rank r), followed by the Greiner-Hormann clip of every pair in the clip set.
-The unit is one clipped polygon pair.  Under torchrun every rank processes its own
-instance (weak scaling, no data-path collective); value = all ranks' pairs / the
-slowest rank's step time.
+mixture over [0,1e5]^2, sigma 2,000; base radius log-normal(ln 50, 0.7); seed 2),
+followed by the Greiner-Hormann clip of every pair in the clip set.
+The unit is one clipped polygon pair.  Under torchrun the ranks split that one workload:
+rank r joins and clips its x-slab of base polygons (equal counts by MBR x1) against the
+whole overlay layer, with no data-path collective (strong scaling); value = all ranks'
+pairs / the slowest rank's step time.
 
 --impl reference times the reference's CPU path on the host cores instead: the GH clip by
 the reference's own sequential clipper built from its sources (oracle/_ref), the join by
@@ -54,6 +55,7 @@ def parse():
     ap.add_argument("--precision-check-all", action="store_true",
                     help="compare every degenerate pair (not a sample) with the oracle")
     ap.add_argument("--no-precision", action="store_true", help="skip the degeneracy batch")
+    ap.add_argument("--no-large-pair", action="store_true", help="skip the single large pair")
     return ap.parse_args()
 
 
@@ -297,9 +299,12 @@ def serve_measure(local, seconds=0.5):
 # ----------------------------------------------------------------------------- plain form
 
 def plain_measure(eng, db, do, stream, n=2000, seed=9):
-    """The plain one-pair-per-launch form on the same GPU: a seeded sample of the clip set
-    of the last join, each pair clipped by its own gh_clip_batch_host_ids call (its own
-    launch sequence, host synchronisations included), same kernels and arithmetic."""
+    """The plain one-pair-per-launch form on the same GPU and the same resident context: a
+    seeded sample of the clip set of the last join, each pair run through the whole join +
+    clip pipeline on its own (gcmf_join over one-polygon views of the two device layers,
+    then gh_clip_joined: every launch sequence and host synchronisation of the batched
+    step, for one pair), same kernels and arithmetic.  Pairs/s of that form is the
+    denominator of batched_over_plain."""
     import ctypes
     import torch
     import gcmfgh
@@ -307,26 +312,97 @@ def plain_measure(eng, db, do, stream, n=2000, seed=9):
     rng = np.random.default_rng(seed)
     idx = rng.choice(len(cb), size=min(n, len(cb)), replace=False)
     L = gcmfgh.lib()
-    info = gcmfgh.ClipInfo()
-    pids = [np.ascontiguousarray(cb[i:i + 1]) for i in idx]
-    qids = [np.ascontiguousarray(co[i:i + 1]) for i in idx]
+    dev = db.xy.device
+    views = []
+    for lay, ids in ((db, cb[idx]), (do, co[idx])):
+        vnum = lay.layer.vnum[ids].astype(np.int32)
+        start = (lay.layer.vps[ids] - lay.layer.vnum[ids]).astype(np.int64)
+        dv = torch.from_numpy(vnum).to(dev)             # one polygon per view: vps = vnum
+        dp = torch.from_numpy(vnum.astype(np.int64)).to(dev)
+        views.append((dv, dp, start, vnum))
+    (bv, bp, bs, bn), (ov, op, os_, on) = views
+    esz = db.xy.element_size()
+    lb = [gcmfgh.Layer(db.xy.data_ptr() + 2 * esz * int(bs[k]), bv.data_ptr() + 4 * k, bp.data_ptr() + 8 * k, 1,
+                       int(bn[k])) for k in range(len(idx))]
+    lo = [gcmfgh.Layer(do.xy.data_ptr() + 2 * esz * int(os_[k]), ov.data_ptr() + 4 * k, op.data_ptr() + 8 * k, 1,
+                       int(on[k])) for k in range(len(idx))]
+    ji, ci = gcmfgh.JoinInfo(), gcmfgh.ClipInfo()
+    clipped = 0
 
     def one(k):
-        gcmfgh._check(L.gh_clip_batch_host_ids(eng.h, ctypes.byref(db.c), ctypes.byref(do.c),
-                                               ctypes.c_void_p(pids[k].ctypes.data),
-                                               ctypes.c_void_p(qids[k].ctypes.data), 1, ctypes.byref(info)))
+        gcmfgh._check(L.gcmf_join(eng.h, ctypes.byref(lb[k]), ctypes.byref(lo[k]), ctypes.byref(ji)))
+        gcmfgh._check(L.gh_clip_joined(eng.h, ctypes.byref(lb[k]), ctypes.byref(lo[k]), ctypes.byref(ci)))
+        return ci.n_pairs
+
     for k in range(min(50, len(idx))):
         one(k)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for k in range(len(idx)):
-        one(k)
+        clipped += one(k)
     e1.record(stream)
     e1.synchronize()
     secs = e0.elapsed_time(e1) * 1e-3
-    return {"value": len(idx) / secs, "unit": "pairs/s",
-            "sample": f"{len(idx)} seeded pairs of the clip set, one gh_clip_batch call each"}
+    # restore the batched join's state for the caller
+    eng.join(db, do)
+    return {"value": clipped / secs, "unit": "pairs/s", "pairs_clipped": int(clipped),
+            "sample": f"{len(idx)} seeded pairs of the clip set, each run alone through gcmf_join + "
+                      f"gh_clip_joined on one-polygon views of the resident layers"}
+
+
+# ----------------------------------------------------------------------------- single large pair
+
+def large_pair_measure(local, nP=1_000_000, nQ=500_000, reps=2, cpu_div=64):
+    """The single large pair (star of nP vertices, radius U(0.8,1.2), at the origin, clipped
+    by a star of nQ vertices, radius U(0.7,1.3), centred at (0.05, 0.03); seed 1) in exact
+    mode, timed with CUDA events after one warm-up clip.  The reference's sequential
+    clipper tests every edge pair (O(nP nQ), 5e11 tests here) and inserts each intersection
+    into linked lists, so its time is taken on the same distribution at nP/cpu_div x
+    nQ/cpu_div vertices and scaled by cpu_div^2 -- an extrapolation and a lower bound, as
+    the sample times grow faster than quadratically."""
+    import torch
+    import gcmfgh
+    import pyoracle
+    from gcmfgh import synth
+    s, c = synth.large_pair(1, nP, nQ)
+    eng = gcmfgh.Engine(local)
+    eng.set_timing(True)
+    ds, dc = gcmfgh.DeviceLayer(s, f"cuda:{local}"), gcmfgh.DeviceLayer(c, f"cuda:{local}")
+    one = np.array([0], np.int32)
+    eng.set_precision(True)
+    info = eng.clip_batch(ds, dc, one, one)
+    times = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        info = eng.clip_batch(ds, dc, one, one)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    stages = {k: round(v, 2) for k, v in eng.timing(1)}
+    st = eng.clip_field("status")
+    eng.set_precision(False)
+    eng.close()
+    out = {"workload": f"single large pair: {nP} x {nQ} vertex stars (seed 1), exact mode",
+           "gpu_s": min(times) * 1e-3, "status": int(st[0]), "intersection_records": info["n_records"],
+           "components": info["n_components"], "vertices": info["n_vertices"], "stages_ms": stages}
+    if pyoracle.ref_available():
+        sp, cp = synth.large_pair(1, nP // cpu_div, nQ // cpu_div)
+        P, Q = sp.ring(0), cp.ring(0)
+        with tempfile.TemporaryDirectory() as td:
+            fn = os.path.join(td, "lp.bin")
+            pyoracle.write_pair_batch(fn, [(P, Q)])
+            r = subprocess.run([pyoracle.REF_BIN, "time", fn, "1"], stdout=subprocess.PIPE, text=True, check=True)
+            t = float(r.stdout.split()[0])
+        out["cpu_reference"] = {"sample_s": t, "sample": f"{len(P)} x {len(Q)} vertices, one core",
+                                "extrapolated_s": t * cpu_div * cpu_div,
+                                "method": f"lower bound: sample time x {cpu_div}^2 for the O(nP nQ) edge "
+                                          f"tests (the sample times grow faster than that: 0.85 s at "
+                                          f"half these sizes)"}
+        out["gpu_over_cpu_extrapolated"] = out["cpu_reference"]["extrapolated_s"] / out["gpu_s"]
+    return out
 
 
 # ----------------------------------------------------------------------------- precision
@@ -473,7 +549,11 @@ def run_ours(args, rank, world, local):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    base, ovl = synth.batched_join(seed=2 + rank)
+    from gcmfgh import shard
+    full_base, ovl = synth.batched_join(seed=2)
+    # one workload split across the ranks: rank r joins and clips its x-slab of base
+    # polygons against the whole overlay layer (every pair is found by exactly one rank)
+    base, _ = shard.shard_base(full_base, world, rank) if world > 1 else (full_base, None)
     eng = gcmfgh.Engine(local)
     stream = torch.cuda.current_stream()
     eng.set_stream(stream.cuda_stream)
@@ -589,9 +669,10 @@ def run_ours(args, rank, world, local):
         line = {
             "metric": METRIC, "value": total_pairs / (ms * 1e-3), "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "pairs_per_step_per_gpu": pairs,
-                       "candidates_per_step_per_gpu": ji["n_pairs"], "parallelism": f"replicas{world}",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "pairs_per_step_rank0": pairs, "pairs_per_step": int(total_pairs),
+                       "candidates_per_step_rank0": ji["n_pairs"],
+                       "parallelism": f"x-slabs of the base layer over {world} GPU(s), overlay layer replicated",
                        "l2": "flushed between steps (256 MiB write, outside the step events)",
                        "inputs_resident": True},
             "e2e": {"value": total_pairs / (e2e_ms * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": h2d,
@@ -614,6 +695,8 @@ def run_ours(args, rank, world, local):
         line["plain"] = plain
         if not args.no_serve:
             line["serving"] = serve_measure(local)
+        if not args.no_large_pair:
+            line["large_pair"] = large_pair_measure(local)
         if not args.no_precision:
             line["precision"] = precision_measure(local, total=args.precision_pairs, chunk=args.precision_chunk,
                                                   check_all_degenerate=args.precision_check_all)

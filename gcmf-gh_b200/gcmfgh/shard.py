@@ -38,6 +38,26 @@ def slab_edges(x1: np.ndarray, world: int) -> np.ndarray:
     return np.concatenate([[-np.inf], qs, [np.inf]])
 
 
+def ranges_to_index(starts: np.ndarray, lens: np.ndarray) -> np.ndarray:
+    """Concatenation of the index ranges [starts[i], starts[i] + lens[i])."""
+    starts = np.asarray(starts, np.int64)
+    lens = np.asarray(lens, np.int64)
+    total = int(lens.sum())
+    if total == 0:
+        return np.zeros(0, np.int64)
+    first = np.cumsum(lens) - lens
+    return np.arange(total, dtype=np.int64) - np.repeat(first, lens) + np.repeat(starts, lens)
+
+
+def subset_layer(layer: synth.Layer, ids: np.ndarray) -> synth.Layer:
+    """The listed polygons of a layer, in the given order, as a layer of their own."""
+    ids = np.asarray(ids, np.int64)
+    vn = layer.vnum[ids].astype(np.int64)
+    v = ranges_to_index(layer.vps[ids] - vn, vn)
+    xy = layer.xy.reshape(-1, 2)[v]
+    return synth.Layer(xy, vn.astype(np.int32))
+
+
 def shard_base(layer: synth.Layer, world: int, rank: int):
     """(sub-layer of this rank's base polygons, their global ids)."""
     x1 = layer_mbr_x1(layer)
@@ -45,8 +65,32 @@ def shard_base(layer: synth.Layer, world: int, rank: int):
     owner = np.searchsorted(edges, x1, side="right") - 1
     owner = np.clip(owner, 0, world - 1)
     ids = np.flatnonzero(owner == rank).astype(np.int32)
-    sub = synth.Layer.from_rings([layer.ring(int(i)) for i in ids])
-    return sub, ids
+    return subset_layer(layer, ids), ids
+
+
+def merge_results(parts):
+    """Merges per-rank results [(b, o, ncomp, comp_size, xy), ...] (b global base ids) into
+    one result sorted by (b, o): (b, o, ncomp, comp_size, xy).  Vectorised: one sort of
+    the pairs, then the components and vertices of every pair gathered by index ranges."""
+    B = np.concatenate([np.asarray(p[0], np.int64) for p in parts]) if parts else np.zeros(0, np.int64)
+    O = np.concatenate([np.asarray(p[1], np.int64) for p in parts]) if parts else np.zeros(0, np.int64)
+    N = np.concatenate([np.asarray(p[2], np.int64) for p in parts]) if parts else np.zeros(0, np.int64)
+    S = np.concatenate([np.asarray(p[3], np.int64) for p in parts]) if parts else np.zeros(0, np.int64)
+    X = np.concatenate([np.asarray(p[4], np.float64) for p in parts]) if parts else np.zeros(0)
+    cstart = np.cumsum(N) - N                              # first component of each pair
+    vcomp = np.cumsum(S) - S                               # first vertex of each component
+    vpair = np.zeros(len(N), np.int64)                     # first vertex and vertex count per pair
+    nz = N > 0
+    vpair[nz] = vcomp[cstart[nz]]
+    vlen = np.add.reduceat(S, cstart[nz]) if nz.any() else np.zeros(0, np.int64)
+    vl = np.zeros(len(N), np.int64)
+    vl[nz] = vlen
+    order = np.lexsort((O, B))
+    comps = ranges_to_index(cstart[order], N[order])
+    verts = ranges_to_index(vpair[order], vl[order])
+    xy = X.reshape(-1, 2)[verts].reshape(-1) if len(verts) else np.zeros(0)
+    return (B[order].astype(np.int32), O[order].astype(np.int32), N[order].astype(np.int32),
+            S[comps].astype(np.int32), xy)
 
 
 def _all_gather_padded(dist, t, n_all, device):
@@ -74,18 +118,4 @@ def gather_results(dist, b, o, ncomp, comp_size, xy, device="cpu"):
     ts = _all_gather_padded(dist, torch.as_tensor(np.asarray(comp_size, np.int64), device=device), allc[:, 1],
                             device)
     tx = _all_gather_padded(dist, torch.as_tensor(np.asarray(xy, np.float64), device=device), allc[:, 2], device)
-    # per pair: its components and vertices, then reorder by (b, o)
-    rows = []
-    for r in range(len(tb)):
-        cbase = np.concatenate([[0], np.cumsum(tn[r])]).astype(np.int64)
-        vstart = np.concatenate([[0], np.cumsum(2 * ts[r])]).astype(np.int64)
-        for k in range(len(tb[r])):
-            c0, c1 = cbase[k], cbase[k + 1]
-            rows.append((int(tb[r][k]), int(to[r][k]), ts[r][c0:c1], tx[r][vstart[c0]:vstart[c1]]))
-    rows.sort(key=lambda t: (t[0], t[1]))
-    mb = np.array([t[0] for t in rows], np.int32)
-    mo = np.array([t[1] for t in rows], np.int32)
-    mn = np.array([len(t[2]) for t in rows], np.int32)
-    ms = np.concatenate([t[2] for t in rows]).astype(np.int32) if rows else np.zeros(0, np.int32)
-    mx = np.concatenate([t[3] for t in rows]) if rows else np.zeros(0)
-    return mb, mo, mn, ms, mx
+    return merge_results([(tb[r], to[r], tn[r], ts[r], tx[r]) for r in range(len(tb))])

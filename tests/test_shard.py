@@ -87,3 +87,23 @@ def test_slab_partition_is_a_partition():
         _, ids = shard.shard_base(base, 3, r)
         seen[ids] += 1
     assert (seen == 1).all()
+
+
+def test_merge_results_orders_pairs_and_their_vertices():
+    """Two parts with interleaved (b, o) keys: the merge sorts pairs and carries each pair's
+    components and vertices along, empty pairs included."""
+    p0 = (np.array([5, 1]), np.array([0, 2]), np.array([2, 0]), np.array([3, 1]),
+          np.arange(8, dtype=float))                            # pair (5,0): comps of 3 and 1 vertices
+    p1 = (np.array([3]), np.array([7]), np.array([1]), np.array([2]), np.array([100., 101., 102., 103.]))
+    b, o, nc, cs, xy = shard.merge_results([p0, p1])
+    assert list(zip(b, o)) == [(1, 2), (3, 7), (5, 0)]
+    assert list(nc) == [0, 1, 2] and list(cs) == [2, 3, 1]
+    assert list(xy) == [100., 101., 102., 103.] + list(np.arange(8, dtype=float))
+
+
+def test_subset_layer_matches_rings():
+    base, _ = synth.small_join(0, 200)
+    ids = np.array([7, 3, 150, 0])
+    sub = shard.subset_layer(base, ids)
+    for k, i in enumerate(ids):
+        assert np.array_equal(sub.ring(k), base.ring(int(i)))
