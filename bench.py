@@ -566,6 +566,10 @@ def run_ours(args, rank, world, local):
         ci = eng.clip_joined(db, do)
         return ji, ci
 
+    # the autotuner picks the size-bucket thresholds for this workload (outside the timing)
+    eng.join(db, do)
+    tuning = eng.autotune_joined(db, do)
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -689,6 +693,11 @@ def run_ours(args, rank, world, local):
                                        "ring vertex + 16 B per result vertex + 8 B per clipped pair"},
             "clocks": clocks,
             "gpu_launches": launches,
+            "autotune": {"chosen": {k: tuning[k] for k in ("bin_grid", "tile_label", "mid_label", "big_label",
+                                                            "wide_label")},
+                         "clip_ms_default": tuning["ms_default"], "clip_ms_tuned": tuning["ms_tuned"],
+                         "gain": tuning["ms_default"] / tuning["ms_tuned"] if tuning["ms_tuned"] else None,
+                         "configs_timed": tuning["configs_timed"]},
         }
         plain = plain_measure(eng, db, do, stream)
         plain["batched_over_plain"] = line["value"] / world / plain["value"]

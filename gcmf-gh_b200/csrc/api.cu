@@ -2,9 +2,12 @@
 // result export.  The reference's entry points exit the process on errors
 // (GPU_Manage.h:25-44, ghcuda.cpp:109-116); these return a status instead.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 #include "common.cuh"
 #include "engine.cuh"
@@ -91,8 +94,20 @@ __global__ void clip_stats_kernel(const int32_t* __restrict__ status, int64_t n,
 
 using namespace gcmfgh;
 
+// One record of the autotuner: the thresholds chosen for a workload signature.
+struct TuneRecord {
+  std::string gpu;
+  int pairs_log2 = 0, verts_log2 = 0, exact = 0;
+  int64_t bin_grid = 0, tile_label = 0, mid_label = 0, big_label = 0, wide_label = 0;
+  double ms_default = 0, ms_tuned = 0;
+};
+
 struct gcmfgh_ctx {
   int device = 0;
+  std::string gpu_name;
+  bool tuning_explicit = false;   // gcmfgh_set_tuning was called: recorded tunings are not applied
+  int join_f32 = 1;               // FP32 prefilters of the join (bit 0 MBR y test, bit 1 edge test)
+  std::vector<TuneRecord> tunings;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
   cudaStream_t aux = nullptr;     // high-priority stream for the long pairs' labelling
@@ -126,7 +141,7 @@ bool layer_ok(const gcmfgh_layer* L) {
   return true;
 }
 
-LayerDev to_dev(const gcmfgh_layer* L) { return LayerDev{L->coords, L->vnum, L->vps, L->n_polys}; }
+LayerDev to_dev(const gcmfgh_layer* L) { return LayerDev{L->coords, L->vnum, L->vps, L->n_polys, L->n_vertices}; }
 
 gcmfgh_status finish(gcmfgh_ctx* c, int st) {
   if (st != ST_OK) {
@@ -166,19 +181,121 @@ gcmfgh_status clip_info(gcmfgh_ctx* c, gcmfgh_clip_info* info) {
   return GCMFGH_OK;
 }
 
+int floor_log2(double v) { return v >= 1.0 ? (int)std::floor(std::log2(v)) : 0; }
+
+int mean_verts_log2(const gcmfgh_layer* b, const gcmfgh_layer* o) {
+  const int64_t np = b->n_polys + o->n_polys;
+  return np > 0 ? floor_log2((double)(b->n_vertices + o->n_vertices) / (double)np) : 0;
+}
+
+// the recorded thresholds for this workload's signature, if any
+const TuneRecord* find_tuning(const gcmfgh_ctx* c, int pl, int vl, int exact) {
+  for (const auto& t : c->tunings)
+    if (t.gpu == c->gpu_name && t.pairs_log2 == pl && t.verts_log2 == vl && t.exact == exact) return &t;
+  return nullptr;
+}
+
+void apply_tuning(ClipParams& p, const TuneRecord& t) {
+  p.bin_grid = t.bin_grid;
+  p.tile_label_max = t.tile_label;
+  p.mid_label_min = t.mid_label;
+  p.big_label_min = t.big_label;
+  p.wide_label_min = t.wide_label;
+}
+
+// the parameters a clip of n pairs on these layers runs with
+ClipParams clip_params(const gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, int64_t n) {
+  ClipParams p = c->prm;
+  if (!c->tuning_explicit) {
+    const TuneRecord* t = find_tuning(c, floor_log2((double)std::max<int64_t>(n, 1)), mean_verts_log2(b, o), p.exact);
+    if (t) apply_tuning(p, *t);
+  }
+  return p;
+}
+
 gcmfgh_status run_clip_ctx(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o,
                            const int32_t* pid, const int32_t* qid, int64_t n, gcmfgh_clip_info* info,
-                           const double* mbrB = nullptr, const double* mbrO = nullptr) {
+                           const double* mbrB = nullptr, const double* mbrO = nullptr,
+                           const ClipParams* force = nullptr) {
   c->clip_arena.reset();
   c->have_clip = false;
   c->marks[1].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
-  int st = run_clip(to_dev(b), to_dev(o), pid, qid, n, c->prm, c->clip_arena, c->clip, c->d_err,
+  const ClipParams prm = force ? *force : clip_params(c, b, o, n);
+  int st = run_clip(to_dev(b), to_dev(o), pid, qid, n, prm, c->clip_arena, c->clip, c->d_err,
                     c->h_scratch, c->stream, &c->marks[1], c->aux, nullptr, c->aux2, mbrB, mbrO);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_clip = true;
   return clip_info(c, info);
+}
+
+// ---- tuning records on disk: one JSON object per line
+bool json_str(const std::string& line, const char* key, std::string& out) {
+  std::string k = std::string("\"") + key + "\": \"";
+  size_t a = line.find(k);
+  if (a == std::string::npos) return false;
+  a += k.size();
+  size_t e = line.find('"', a);
+  if (e == std::string::npos) return false;
+  out = line.substr(a, e - a);
+  return true;
+}
+
+bool json_num(const std::string& line, const char* key, double& out) {
+  std::string k = std::string("\"") + key + "\": ";
+  size_t a = line.find(k);
+  if (a == std::string::npos) return false;
+  out = std::strtod(line.c_str() + a + k.size(), nullptr);
+  return true;
+}
+
+void load_tunings(const char* path, std::vector<TuneRecord>& out) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) return;
+  char buf[1024];
+  while (std::fgets(buf, sizeof(buf), f)) {
+    std::string line(buf);
+    TuneRecord t;
+    double v[10];
+    const char* keys[10] = {"pairs_log2", "verts_log2", "exact", "bin_grid", "tile_label", "mid_label",
+                            "big_label", "wide_label", "ms_default", "ms_tuned"};
+    bool ok = json_str(line, "gpu", t.gpu);
+    for (int i = 0; i < 10 && ok; ++i) ok = json_num(line, keys[i], v[i]);
+    if (!ok) continue;
+    t.pairs_log2 = (int)v[0]; t.verts_log2 = (int)v[1]; t.exact = (int)v[2];
+    t.bin_grid = (int64_t)v[3]; t.tile_label = (int64_t)v[4]; t.mid_label = (int64_t)v[5];
+    t.big_label = (int64_t)v[6]; t.wide_label = (int64_t)v[7]; t.ms_default = v[8]; t.ms_tuned = v[9];
+    out.push_back(t);
+  }
+  std::fclose(f);
+}
+
+void save_tunings(const char* path, const std::vector<TuneRecord>& recs) {
+  FILE* f = std::fopen(path, "w");
+  if (!f) return;
+  for (const auto& t : recs)
+    std::fprintf(f,
+                 "{\"gpu\": \"%s\", \"pairs_log2\": %d, \"verts_log2\": %d, \"exact\": %d, \"bin_grid\": %lld, "
+                 "\"tile_label\": %lld, \"mid_label\": %lld, \"big_label\": %lld, \"wide_label\": %lld, "
+                 "\"ms_default\": %.4f, \"ms_tuned\": %.4f}\n",
+                 t.gpu.c_str(), t.pairs_log2, t.verts_log2, t.exact, (long long)t.bin_grid, (long long)t.tile_label,
+                 (long long)t.mid_label, (long long)t.big_label, (long long)t.wide_label, t.ms_default, t.ms_tuned);
+  std::fclose(f);
+}
+
+TuneRecord record_of(const ClipParams& p) {
+  TuneRecord t;
+  t.bin_grid = p.bin_grid; t.tile_label = p.tile_label_max; t.mid_label = p.mid_label_min;
+  t.big_label = p.big_label_min; t.wide_label = p.wide_label_min;
+  return t;
+}
+
+void to_public(const TuneRecord& t, gcmfgh_tuning* out) {
+  out->bin_grid = t.bin_grid; out->tile_label = t.tile_label; out->mid_label = t.mid_label;
+  out->big_label = t.big_label; out->wide_label = t.wide_label;
+  out->pairs_log2 = t.pairs_log2; out->verts_log2 = t.verts_log2; out->exact = t.exact;
+  out->ms_default = t.ms_default; out->ms_tuned = t.ms_tuned;
 }
 
 struct FieldRef { const void* p; int64_t count; int esize; };
@@ -281,6 +398,10 @@ gcmfgh_status gcmfgh_create(int device, gcmfgh_ctx** out) {
   cudaMemset(c->d_err, 0, 64);
   for (auto& m : c->marks)
     for (int i = 0; i < Marks::kMax; ++i) cudaEventCreate(&m.ev[i]);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->gpu_name = prop.name;
+  else cudaGetLastError();
+  if (const char* f = std::getenv("GCMFGH_TUNING_FILE")) load_tunings(f, c->tunings);
   *out = c;
   return GCMFGH_OK;
 }
@@ -371,6 +492,11 @@ gcmfgh_status gcmfgh_set_precision(gcmfgh_ctx* c, int mode) {
 
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* c, int key, int64_t value) {
   if (!c || value < 0) return GCMFGH_INVALID_ARGUMENT;
+  if (key == GCMFGH_TUNE_F32_FILTER) {
+    c->join_f32 = (int)(value & 3);
+    return GCMFGH_OK;
+  }
+  c->tuning_explicit = true;
   if (key == GCMFGH_TUNE_BIN_GRID) c->prm.bin_grid = value;
   else if (key == GCMFGH_TUNE_BIG_LABEL) c->prm.big_label_min = value;
   else if (key == GCMFGH_TUNE_MID_LABEL) c->prm.mid_label_min = value;
@@ -392,7 +518,7 @@ gcmfgh_status gcmf_join(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer
   c->marks[0].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   int st = run_join(to_dev(b), to_dev(o), c->join_arena, c->join, c->d_err, c->h_scratch, c->stream,
-                    &c->marks[0], c->aux);
+                    &c->marks[0], c->aux, c->join_f32);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_join = true;
@@ -459,6 +585,104 @@ gcmfgh_status gh_clip_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_
   // the join's polygon MBRs of the same layers (mbr_kernel computes what the clip would)
   return run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, c->join.n_clip, info, c->join.mbr_b,
                       c->join.mbr_o);
+}
+
+gcmfgh_status gcmfgh_tuning_for(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, int64_t n,
+                                gcmfgh_tuning* out) {
+  if (!c || !layer_ok(b) || !layer_ok(o) || n < 0 || !out) return GCMFGH_INVALID_ARGUMENT;
+  TuneRecord t = record_of(clip_params(c, b, o, n));
+  t.pairs_log2 = floor_log2((double)std::max<int64_t>(n, 1));
+  t.verts_log2 = mean_verts_log2(b, o);
+  t.exact = c->prm.exact;
+  if (const TuneRecord* r = c->tuning_explicit ? nullptr : find_tuning(c, t.pairs_log2, t.verts_log2, t.exact)) {
+    t.ms_default = r->ms_default;
+    t.ms_tuned = r->ms_tuned;
+  }
+  std::memset(out, 0, sizeof(*out));
+  to_public(t, out);
+  return GCMFGH_OK;
+}
+
+gcmfgh_status gcmfgh_autotune_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o,
+                                     gcmfgh_tuning* out) {
+  if (!c || !layer_ok(b) || !layer_ok(o) || !out) return GCMFGH_INVALID_ARGUMENT;
+  if (!c->have_join) return GCMFGH_NOT_READY;
+  if (b->coords != c->join_b || o->coords != c->join_o) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->prm.no_swap = 0;
+  const int64_t n = c->join.n_clip;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return GCMFGH_CUDA_ERROR;
+  int timed = 0;
+  // median of three clips of the join's clip set under parameters p (ms), < 0 on failure
+  auto time_with = [&](const ClipParams& p) -> float {
+    float t[3];
+    gcmfgh_clip_info info;
+    for (int r = 0; r < 3; ++r) {
+      cudaEventRecord(e0, c->stream);
+      if (run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, n, &info, c->join.mbr_b, c->join.mbr_o, &p) !=
+          GCMFGH_OK)
+        return -1.0f;
+      cudaEventRecord(e1, c->stream);
+      cudaEventSynchronize(e1);
+      cudaEventElapsedTime(&t[r], e0, e1);
+    }
+    ++timed;
+    std::sort(t, t + 3);
+    return t[1];
+  };
+  ClipParams cur = clip_params(c, b, o, n);
+  gcmfgh_clip_info warm;
+  run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, n, &warm, c->join.mbr_b, c->join.mbr_o, &cur);
+  const float ms0 = time_with(cur);
+  if (ms0 < 0) { cudaEventDestroy(e0); cudaEventDestroy(e1); return GCMFGH_CUDA_ERROR; }
+  float best = ms0;
+  // one pass of coordinate descent; the candidates span the useful range of each limit
+  const int64_t kNever = INT64_MAX / 4;
+  using Field = int64_t ClipParams::*;
+  struct Knob { Field f; std::vector<int64_t> vals; };
+  const Knob knobs[] = {
+      {&ClipParams::bin_grid, {1ll << 10, 1ll << 12, 1ll << 14, 1ll << 16, 1ll << 20, 1ll << 24}},
+      {&ClipParams::tile_label_max, {0, 32, 64, 96, 128}},
+      {&ClipParams::mid_label_min, {256, 512, 1024, 2048, 4096}},
+      {&ClipParams::wide_label_min, {0, 1ll << 16, kNever}},
+  };
+  for (const Knob& k : knobs) {
+    const int64_t keep = cur.*(k.f);
+    int64_t chosen = keep;
+    for (int64_t v : k.vals) {
+      if (v == keep) continue;
+      ClipParams p = cur;
+      p.*(k.f) = v;
+      const float ms = time_with(p);
+      if (ms >= 0 && ms < best) { best = ms; chosen = v; }
+    }
+    cur.*(k.f) = chosen;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  TuneRecord t = record_of(cur);
+  t.gpu = c->gpu_name;
+  t.pairs_log2 = floor_log2((double)std::max<int64_t>(n, 1));
+  t.verts_log2 = mean_verts_log2(b, o);
+  t.exact = cur.exact;
+  t.ms_default = ms0;
+  t.ms_tuned = best;
+  bool replaced = false;
+  for (auto& r : c->tunings)
+    if (r.gpu == t.gpu && r.pairs_log2 == t.pairs_log2 && r.verts_log2 == t.verts_log2 && r.exact == t.exact) {
+      r = t;
+      replaced = true;
+    }
+  if (!replaced) c->tunings.push_back(t);
+  c->tuning_explicit = false;
+  if (const char* f = std::getenv("GCMFGH_TUNING_FILE")) save_tunings(f, c->tunings);
+  std::memset(out, 0, sizeof(*out));
+  to_public(t, out);
+  out->configs_timed = timed;
+  // leave the clip result of the chosen thresholds in place
+  gcmfgh_clip_info info;
+  return run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, n, &info, c->join.mbr_b, c->join.mbr_o, &cur);
 }
 
 gcmfgh_status gh_clip_get(gcmfgh_ctx* c, int f, void* dst, int64_t cap, int on_dev, int64_t* bytes) {

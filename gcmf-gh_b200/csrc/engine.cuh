@@ -44,6 +44,8 @@ struct LayerDev {
   const int32_t* vnum;
   const int64_t* vps;
   int64_t n;
+  int64_t nverts = 0;          // stored vertices (0: unknown)
+  const float2* xyf = nullptr; // FP32 copy of xy (round to nearest) for the join's prefilters
 };
 
 // Join outputs (device, owned by the join arena).  Pairs are sorted by (base, overlay).
@@ -118,7 +120,7 @@ int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s);
 // base layer's on s.
 int run_join(const LayerDev& base, const LayerDev& ovl, Arena& arena, JoinDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
-             cudaStream_t aux = nullptr);
+             cudaStream_t aux = nullptr, int f32 = 0);
 
 int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys, int64_t K, int obits,
                    Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,

@@ -61,7 +61,8 @@ struct JTile {
 // joins.  Valid polygons get the order-preserving key of their x1 for the sweep sort.
 __global__ void __launch_bounds__(kThreads)
 mbr_kernel(LayerDev L, double* __restrict__ mbr, uint8_t* __restrict__ valid,
-           uint64_t* __restrict__ key, uint32_t* __restrict__ id, unsigned long long* n_valid) {
+           uint64_t* __restrict__ key, uint32_t* __restrict__ id, unsigned long long* n_valid,
+           float2* __restrict__ xyf) {
   int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
   if (w >= L.n) return;
   const int nv = L.vnum[w];
@@ -70,6 +71,7 @@ mbr_kernel(LayerDev L, double* __restrict__ mbr, uint8_t* __restrict__ valid,
   double x1 = INFINITY, y1 = INFINITY, x2 = -INFINITY, y2 = -INFINITY;
   for (int k = lane_id(); k < nv; k += 32) {
     double2 p = __ldg(v + k);
+    if (xyf) xyf[s + k] = make_float2(__double2float_rn(p.x), __double2float_rn(p.y));
     x1 = fmin(x1, p.x); x2 = fmax(x2, p.x);
     y1 = fmin(y1, p.y); y2 = fmax(y2, p.y);
   }
@@ -84,7 +86,8 @@ mbr_kernel(LayerDev L, double* __restrict__ mbr, uint8_t* __restrict__ valid,
   }
 }
 
-struct SortedMbr { double *x1, *x2, *y1, *y2; uint32_t* id; int64_t n; };
+// yf: (y1 rounded down, y2 rounded up) in FP32 -- a box that contains the FP64 one
+struct SortedMbr { double *x1, *x2, *y1, *y2; uint32_t* id; int64_t n; float2* yf; };
 
 __global__ void gather_sorted_kernel(const double* __restrict__ mbr, const uint32_t* __restrict__ ids,
                                      int64_t n, SortedMbr S) {
@@ -93,6 +96,7 @@ __global__ void gather_sorted_kernel(const double* __restrict__ mbr, const uint3
   uint32_t id = ids[i];
   double4 m = reinterpret_cast<const double4*>(mbr)[id];
   S.x1[i] = m.x; S.y1[i] = m.y; S.x2[i] = m.z; S.y2[i] = m.w; S.id[i] = id;
+  if (S.yf) S.yf[i] = make_float2(__double2float_rd(m.y), __double2float_ru(m.w));
 }
 
 // Warp-cooperative search in an ascending array (all 32 lanes call it with the same
@@ -133,7 +137,10 @@ __device__ __forceinline__ int64_t upper_bound_d(const double* a, int64_t n, dou
 // takes the bases that start in (x1o, x2o]; both ranges are binary searches in the
 // other layer's x1-sorted array, and only the y test remains inside the range.
 // mode 0: count per element, mode 1: emit keys (b << obits | o) at offs[element].
-template <int kMode>
+// kF32: the y test first on outward-rounded FP32 boxes (8 bytes per candidate; a superset,
+// as rd(y1) <= y1 <= my2 <= ru(my2)), then in FP64 for the boxes that pass -- the same
+// candidates either way.
+template <int kMode, int kF32>
 __global__ void __launch_bounds__(kThreads, 8)
 sweep_kernel(SortedMbr B, SortedMbr O, int32_t* __restrict__ cnt, const int64_t* __restrict__ offs,
              uint64_t* __restrict__ keys, int obits) {
@@ -144,6 +151,7 @@ sweep_kernel(SortedMbr B, SortedMbr O, int32_t* __restrict__ cnt, const int64_t*
   const SortedMbr& ot = base_side ? O : B;
   const int64_t i = base_side ? w : w - B.n;
   const double mx1 = me.x1[i], mx2 = me.x2[i], my1 = me.y1[i], my2 = me.y2[i];
+  const float my1d = kF32 ? __double2float_rd(my1) : 0.f, my2u = kF32 ? __double2float_ru(my2) : 0.f;
   int64_t lo, hi;
   if (base_side) { lo = lower_bound_d(ot.x1, ot.n, mx1); hi = lower_bound_d(ot.x1, ot.n, mx2); }
   else { lo = upper_bound_d(ot.x1, ot.n, mx1); hi = upper_bound_d(ot.x1, ot.n, mx2); }
@@ -153,7 +161,15 @@ sweep_kernel(SortedMbr B, SortedMbr O, int32_t* __restrict__ cnt, const int64_t*
   for (int64_t k0 = lo; k0 < hi; k0 += 32) {
     int64_t k = k0 + lane_id();
     bool hit = false;
-    if (k < hi) hit = ot.y1[k] <= my2 && my1 <= ot.y2[k];
+    if (k < hi) {
+      if (kF32) {
+        const float2 q = ot.yf[k];
+        hit = q.x <= my2u && my1d <= q.y;
+        if (hit) hit = ot.y1[k] <= my2 && my1 <= ot.y2[k];
+      } else {
+        hit = ot.y1[k] <= my2 && my1 <= ot.y2[k];
+      }
+    }
     unsigned m = __ballot_sync(0xffffffffu, hit);
     if (kMode == 1 && hit) {
       uint64_t oid = ot.id[k];
@@ -238,7 +254,17 @@ pip_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32
 // from vertex k to k+1 and the last one from the closing vertex back to vertex 0.
 // mode 0 counts (and drops pairs with an empty side, :604-613), mode 1 writes the
 // surviving edge ids in ascending order (Apply_CMF :676-733, 32-bit ids here).
-template <int kMode, int W>
+// kF32: each edge is first tested on the FP32 copies of its vertices, rejected only when
+// the rejection holds with one FP32 ulp of room on each side (rn(v) is within half an ulp of
+// v, so nextafter(rn(v)) bounds v); the edges that pass are tested in FP64.  The edge sets
+// are those of the FP64 test alone.
+__device__ __forceinline__ bool f32_rejects(float2 a, float2 b, float cx1d, float cy1d, float cx2u, float cy2u) {
+  const float xmax = nextafterf(fmaxf(a.x, b.x), INFINITY), xmin = nextafterf(fminf(a.x, b.x), -INFINITY);
+  const float ymax = nextafterf(fmaxf(a.y, b.y), INFINITY), ymin = nextafterf(fminf(a.y, b.y), -INFINITY);
+  return cx1d > xmax || cx2u < xmin || cy1d > ymax || cy2u < ymin;
+}
+
+template <int kMode, int W, int kF32>
 __global__ void __launch_bounds__(kThreads, 8)
 cmf_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32_t* __restrict__ po,
            const double* __restrict__ cmbr, int64_t K, int8_t* __restrict__ join_flag,
@@ -258,12 +284,15 @@ cmf_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32
     if (size <= lo || size > hi) return;             // the other pass takes this pair
   }
   double4 c = reinterpret_cast<const double4*>(cmbr)[w];
+  const float cx1d = kF32 ? __double2float_rd(c.x) : 0.f, cy1d = kF32 ? __double2float_rd(c.y) : 0.f;
+  const float cx2u = kF32 ? __double2float_ru(c.z) : 0.f, cy2u = kF32 ? __double2float_ru(c.w) : 0.f;
   int counts[2];
   for (int side = 0; side < 2; ++side) {
     const LayerDev& L = side == 0 ? Lb : Lo;
     int id = side == 0 ? pb[w] : po[w];
     const int nv = L.vnum[id];
     const double2* v = reinterpret_cast<const double2*>(L.xy) + (L.vps[id] - nv);
+    const float2* vf = kF32 ? L.xyf + (L.vps[id] - nv) : nullptr;
     int64_t pos = 0;
     int32_t* list = nullptr;
     if (kMode == 1) { pos = side == 0 ? bOff[w] : oOff[w]; list = side == 0 ? bList : oList; }
@@ -272,8 +301,11 @@ cmf_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32
       int k = k0 + T.lane;
       bool hit = false;
       if (k < nv) {
-        double2 a = __ldg(v + k), b = __ldg(v + ((k < nv - 1) ? k + 1 : 0));
-        hit = edge_touches_box(a.x, a.y, b.x, b.y, c.x, c.y, c.z, c.w);
+        const int k2 = (k < nv - 1) ? k + 1 : 0;
+        if (!kF32 || !f32_rejects(__ldg(vf + k), __ldg(vf + k2), cx1d, cy1d, cx2u, cy2u)) {
+          double2 a = __ldg(v + k), b = __ldg(v + k2);
+          hit = edge_touches_box(a.x, a.y, b.x, b.y, c.x, c.y, c.z, c.w);
+        }
       }
       unsigned m = T.ballot(hit);
       if (kMode == 1 && hit) list[pos + cnt + __popc(m & T.lanes_below())] = k;
@@ -421,8 +453,13 @@ int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s) {
   return ST_OK;
 }
 
-int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* d_err,
-             int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux) {
+int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int* d_err,
+             int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux, int f32) {
+  // f32 bit 0: FP32 prefilter of the sweep's y test; bit 1: of the common-MBR edge test
+  // (needs the layers' vertex counts, for their FP32 copies)
+  const bool f32cmf = (f32 & 2) && Lb0.nverts > 0 && Lo0.nverts > 0;
+  f32 &= 1;
+  LayerDev Lb = Lb0, Lo = Lo0;
   Marks dummy;
   if (!mk) mk = &dummy;
   J = JoinDev();
@@ -441,6 +478,15 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   uint64_t* kAltO = A.take_n<uint64_t>(no);
   uint32_t* vAltO = A.take_n<uint32_t>(no);
   unsigned long long* d_cnt = A.take_n<unsigned long long>(8);
+  float2* xyfB = nullptr;
+  float2* xyfO = nullptr;
+  if (f32cmf) {
+    xyfB = A.take_n<float2>(Lb.nverts);
+    xyfO = A.take_n<float2>(Lo.nverts);
+    if (!xyfB || !xyfO) return ST_OUT_OF_MEMORY;
+    Lb.xyf = xyfB;
+    Lo.xyf = xyfO;
+  }
   void* tmp = A.take(std::max(radix_temp_bytes(nb), scan_temp_bytes(nb)));
   void* tmpO = A.take(std::max(radix_temp_bytes(no), scan_temp_bytes(no)));
   if (!J.mbr_b || !J.mbr_o || !J.valid_b || !J.valid_o || !keyB || !keyO || !idB || !idO || !kAlt ||
@@ -457,8 +503,8 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
     cudaStreamWaitEvent(aux, fork, 0);
     so = aux;
   }
-  { mbr_kernel<<<blocks_for_warps(nb), kThreads, 0, s>>>(Lb, J.mbr_b, J.valid_b, keyB, idB, d_cnt + 0); note_launch(); }
-  { mbr_kernel<<<blocks_for_warps(no), kThreads, 0, so>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1); note_launch(); }
+  { mbr_kernel<<<blocks_for_warps(nb), kThreads, 0, s>>>(Lb, J.mbr_b, J.valid_b, keyB, idB, d_cnt + 0, xyfB); note_launch(); }
+  { mbr_kernel<<<blocks_for_warps(no), kThreads, 0, so>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1, xyfO); note_launch(); }
   // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
   radix_sort_pairs(keyB, idB, kAlt, vAlt, nb, 64, tmp, d_err, s);
   radix_sort_pairs(keyO, idO, kAltO, vAltO, no, 64, tmpO, d_err, so);
@@ -473,9 +519,10 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
   const int64_t nvb = h_scratch[0], nvo = h_scratch[1];
   SortedMbr SB{A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb),
-               A.take_n<uint32_t>(nvb), nvb};
+               A.take_n<uint32_t>(nvb), nvb, f32 ? A.take_n<float2>(nvb) : nullptr};
   SortedMbr SO{A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo),
-               A.take_n<uint32_t>(nvo), nvo};
+               A.take_n<uint32_t>(nvo), nvo, f32 ? A.take_n<float2>(nvo) : nullptr};
+  if (f32 && (!SB.yf || !SO.yf)) return ST_OUT_OF_MEMORY;
   int32_t* cnt = A.take_n<int32_t>(nvb + nvo);
   int64_t* offs = A.take_n<int64_t>(nvb + nvo);
   int64_t* d_total = A.take_n<int64_t>(4);
@@ -490,7 +537,8 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   if (obits + bbits > 64) return ST_INVALID_ARGUMENT;
   const int64_t ne = nvb + nvo;
   if (ne > 0) {
-    { sweep_kernel<0><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr, nullptr, obits); note_launch(); }
+    { (f32 ? sweep_kernel<0, 1> : sweep_kernel<0, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr,
+                                                                                             nullptr, obits); note_launch(); }
     void* stmp = A.take(scan_temp_bytes(ne));
     if (!stmp) return ST_OUT_OF_MEMORY;
     exclusive_scan_i32(cnt, offs, ne, d_total, stmp, d_err, s);
@@ -509,7 +557,8 @@ int run_join(const LayerDev& Lb, const LayerDev& Lo, Arena& A, JoinDev& J, int* 
   uint32_t* pvAlt = A.take_n<uint32_t>(K);
   void* rtmp = A.take(radix_temp_bytes(K));
   if (!pkeys || !pvals || !pkAlt || !pvAlt || !rtmp) return ST_OUT_OF_MEMORY;
-  { sweep_kernel<1><<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs, pkeys, obits); note_launch(); }
+  { (f32 ? sweep_kernel<1, 1> : sweep_kernel<1, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs,
+                                                                                           pkeys, obits); note_launch(); }
   radix_sort_pairs(pkeys, pvals, pkAlt, pvAlt, K, ((obits + bbits + 7) / 8) * 8, rtmp, d_err, s);
   mk->mark("join:sweep-emit+sort", s);
   return join_from_keys(Lb, Lo, pkeys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, mk, aux);
@@ -567,10 +616,11 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
   mk->mark("join:cmbr+pip", s);
   // ---- J5 common-MBR edge filter: count, offsets, lists
   fork_aux();
-  { cmf_kernel<0, kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
+  const bool f32 = Lb.xyf && Lo.xyf;
+  { (f32 ? cmf_kernel<0, kJoinTile, 1> : cmf_kernel<0, kJoinTile, 0>)<<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
         Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, nullptr, nullptr, nullptr, nullptr, -1,
         kJoinTileMax); note_launch(); }
-  { cmf_kernel<0, 32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+  { (f32 ? cmf_kernel<0, 32, 1> : cmf_kernel<0, 32, 0>)<<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
                                                               J.oE, nullptr, nullptr, nullptr, nullptr, kJoinTileMax,
                                                               INT64_MAX); note_launch(); }
   join_aux();
@@ -583,9 +633,9 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
   int32_t* oList = A.take_n<int32_t>(nOl);
   if (!bList || !oList) return ST_OUT_OF_MEMORY;
   fork_aux();
-  { cmf_kernel<1, kJoinTile><<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
+  { (f32 ? cmf_kernel<1, kJoinTile, 1> : cmf_kernel<1, kJoinTile, 0>)<<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
         Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, bOff, oOff, bList, oList, -1, kJoinTileMax); note_launch(); }
-  { cmf_kernel<1, 32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+  { (f32 ? cmf_kernel<1, 32, 1> : cmf_kernel<1, 32, 0>)<<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
                                                               J.oE, bOff, oOff, bList, oList, kJoinTileMax,
                                                               INT64_MAX); note_launch(); }
   join_aux();

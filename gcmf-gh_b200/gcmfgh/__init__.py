@@ -46,6 +46,16 @@ class Layer(ctypes.Structure):
                 ("n_polys", ctypes.c_int64), ("n_vertices", ctypes.c_int64)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("bin_grid", ctypes.c_int64), ("tile_label", ctypes.c_int64), ("mid_label", ctypes.c_int64),
+                ("big_label", ctypes.c_int64), ("wide_label", ctypes.c_int64), ("pairs_log2", ctypes.c_int),
+                ("verts_log2", ctypes.c_int), ("exact", ctypes.c_int), ("ms_default", ctypes.c_double),
+                ("ms_tuned", ctypes.c_double), ("configs_timed", ctypes.c_int)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class JoinInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in
                 ("n_pairs", "n_pip_candidates", "n_within", "n_cmf", "n_seg", "n_clip")]
@@ -112,6 +122,8 @@ def lib():
         L.gcmf_join_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
         L.gh_clip_batch.argtypes = [vp, P(Layer), P(Layer), vp, vp, i64, P(ClipInfo)]
         L.gh_clip_joined.argtypes = [vp, P(Layer), P(Layer), P(ClipInfo)]
+        L.gcmfgh_autotune_joined.argtypes = [vp, P(Layer), P(Layer), P(Tuning)]
+        L.gcmfgh_tuning_for.argtypes = [vp, P(Layer), P(Layer), i64, P(Tuning)]
         L.gh_clip_batch_host_ids.argtypes = [vp, P(Layer), P(Layer), vp, vp, i64, P(ClipInfo)]
         L.gh_clip_get.argtypes = [vp, ctypes.c_int, vp, i64, ctypes.c_int, P(i64)]
         L.gh_clip_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
@@ -240,8 +252,12 @@ class Engine:
     def last_device_error(self):
         return lib().gcmfgh_last_device_error(self.h)
 
-    def set_tuning(self, bin_grid=None, big_label=None, mid_label=None, tile_label=None, wide_label=None):
-        """Work-distribution thresholds (results do not depend on them)."""
+    def set_tuning(self, bin_grid=None, big_label=None, mid_label=None, tile_label=None, wide_label=None,
+                   f32_filter=None):
+        """Work-distribution thresholds and the join's FP32 prefilters (results do not
+        depend on them)."""
+        if f32_filter is not None:      # bit 0: MBR y prefilter, bit 1: edge prefilter
+            _check(lib().gcmfgh_set_tuning(self.h, 5, int(f32_filter)))
         if bin_grid is not None:
             _check(lib().gcmfgh_set_tuning(self.h, 0, int(bin_grid)))
         if big_label is not None:
@@ -252,6 +268,19 @@ class Engine:
             _check(lib().gcmfgh_set_tuning(self.h, 3, int(tile_label)))
         if wide_label is not None:
             _check(lib().gcmfgh_set_tuning(self.h, 4, int(wide_label)))
+
+    def autotune_joined(self, dbase: DeviceLayer, dovl: DeviceLayer):
+        """Times the last join's clip set under candidate work-distribution thresholds and
+        records the fastest for this workload's signature (gcmfgh_autotune_joined)."""
+        t = Tuning()
+        _check(lib().gcmfgh_autotune_joined(self.h, ctypes.byref(dbase.c), ctypes.byref(dovl.c), ctypes.byref(t)))
+        return t.as_dict()
+
+    def tuning_for(self, dbase: DeviceLayer, dovl: DeviceLayer, n_pairs):
+        t = Tuning()
+        _check(lib().gcmfgh_tuning_for(self.h, ctypes.byref(dbase.c), ctypes.byref(dovl.c), int(n_pairs),
+                                       ctypes.byref(t)))
+        return t.as_dict()
 
     def set_timing(self, on=True):
         _check(lib().gcmfgh_set_timing(self.h, 1 if on else 0))

@@ -142,7 +142,41 @@ const char* gcmfgh_status_string(gcmfgh_status s);
  * kernels built for a full GPU (fewer registers, more resident warps); smaller batches
  * by the ones built for per-pair latency (default 65536) */
 #define GCMFGH_TUNE_WIDE_LABEL 4
+/* GCMFGH_TUNE_F32_FILTER: bit 0 runs the join's MBR y test (GPU_MBR.h:339-415) first on
+ * outward-rounded FP32 boxes, bit 1 the common-MBR edge test (GPU_Join.h:576-577) first
+ * on FP32 vertex copies with one ulp of room; both are guaranteed supersets, and the
+ * survivors are confirmed in FP64, so candidates and edge lists are those of the FP64
+ * tests.  Default 1: on the batched workload the MBR prefilter saves 0.03 ms and the
+ * edge prefilter costs 0.24 ms (most edges pass it and are tested twice).  Bit 1 needs
+ * the layers' n_vertices. */
+#define GCMFGH_TUNE_F32_FILTER 5
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* ctx, int key, int64_t value);
+
+/* ---- autotuner of the work-distribution thresholds.  No counterpart in the reference
+ * (its block sizes are picked per dataset by hand: switch (DATASET) at Join.h:112, 185,
+ * 262, 363, 442).
+ * A workload's signature is (GPU name, floor(log2 pairs), floor(log2 mean vertices per
+ * polygon of the two layers), precision mode).  gcmfgh_autotune_joined times
+ * gh_clip_joined on the last join's clip set under candidate thresholds (one pass of
+ * coordinate descent over bin grid, tile, block and wide-batch limits; median of three
+ * runs each), keeps the fastest, and records it for the signature.  Later clips of the
+ * context whose signature matches use the recorded thresholds, unless gcmfgh_set_tuning
+ * was called (explicit settings win).  When the environment variable
+ * GCMFGH_TUNING_FILE names a file, gcmfgh_create loads the records from it (JSON, one
+ * object per line) and gcmfgh_autotune_joined writes them back.  Results do not depend on
+ * the thresholds: only the time does. */
+typedef struct {
+  int64_t bin_grid, tile_label, mid_label, big_label, wide_label;
+  int pairs_log2, verts_log2, exact;
+  double ms_default;     /* clip time under the thresholds in force before tuning */
+  double ms_tuned;       /* clip time under the chosen thresholds */
+  int configs_timed;
+} gcmfgh_tuning;
+gcmfgh_status gcmfgh_autotune_joined(gcmfgh_ctx* ctx, const gcmfgh_layer* base, const gcmfgh_layer* overlay,
+                                     gcmfgh_tuning* out);
+/* the thresholds a clip of n_pairs on these layers would use now (recorded or default) */
+gcmfgh_status gcmfgh_tuning_for(gcmfgh_ctx* ctx, const gcmfgh_layer* base, const gcmfgh_layer* overlay,
+                                int64_t n_pairs, gcmfgh_tuning* out);
 /* device error word of the last call (0 none, 1 capacity, 2 trace budget, 4 wait limit) */
 int gcmfgh_last_device_error(gcmfgh_ctx* ctx);
 /* Stage timing, replacing the reference's StartTimer/StopTimer pairs around each stage

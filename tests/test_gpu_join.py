@@ -137,3 +137,44 @@ def test_join_matches_reference_gpu_join(engine, name, tmp_path):
     for f in ("b", "o", "pip_type", "pip_flag", "join_flag", "bE", "oE", "seg_flag"):
         assert np.array_equal(engine.join_field(f).astype(np.int64), r[f].astype(np.int64)), f
     assert np.array_equal(engine.join_field("cmbr").reshape(-1, 4), r["cmbr"])
+
+
+def _near_tie_layers(seed=3, n=400):
+    """Squares whose MBRs meet in y within a few FP64 ulps (far below one FP32 ulp): base
+    i spans y in [0, 1 + d_i], overlay i spans [1 + e_i, 2], with d_i, e_i of order 1e-9,
+    so the y overlap -- and the edges touching the common MBR -- are decided below FP32
+    resolution; plus shifted copies and a few random stars around them."""
+    rng = np.random.default_rng(seed)
+    rb, ro = [], []
+    for i in range(n):
+        x = 3.0 * i
+        d, e = rng.integers(-3, 4, size=2) * 1e-9
+        top = 1.0 + d
+        rb.append(np.array([[x, 0.0], [x + 1.0, 0.0], [x + 1.0, top], [x, top]]))
+        ro.append(np.array([[x + 0.5, 1.0 + e], [x + 1.5, 1.0 + e], [x + 1.5, 2.0], [x + 0.5, 2.0]]))
+        if i % 4 == 0:                                  # an edge ending a few ulps inside the CMBR
+            u = np.nextafter(1.0 + e, 2.0) if i % 8 == 0 else np.nextafter(1.0 + e, 0.0)
+            ro.append(np.array([[x + 0.2, u], [x + 0.8, 1.5], [x + 0.2, 1.9]]))
+    stars_b, stars_o = synth.small_join(seed, 200)
+    rb += [stars_b.ring(i) for i in range(stars_b.n_polys)]
+    ro += [stars_o.ring(i) for i in range(stars_o.n_polys)]
+    return synth.Layer.from_rings(rb), synth.Layer.from_rings(ro)
+
+
+def test_fp32_prefilters_keep_fp64_results(engine):
+    """The join's FP32 outward-rounded MBR and edge prefilters (GCMFGH_TUNE_F32_FILTER)
+    give the FP64 tests' candidates, flags and edge counts on near-tie boxes."""
+    base, ovl = _near_tie_layers()
+    o = pyoracle.join(base, ovl)
+    got = {}
+    for f32 in (0, 1, 2, 3):
+        engine.set_tuning(f32_filter=f32)
+        try:
+            _join_equal(engine, base, ovl)
+            got[f32] = [engine.join_field(f).copy() for f in FIELDS]
+        finally:
+            engine.set_tuning(f32_filter=1)
+    for f32 in (1, 2, 3):
+        for a, b in zip(got[0], got[f32]):
+            assert np.array_equal(a, b)
+    assert int(o.pip_type.size) > 250          # about half the near-tie squares join
