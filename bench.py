@@ -56,6 +56,7 @@ def parse():
                     help="compare every degenerate pair (not a sample) with the oracle")
     ap.add_argument("--no-precision", action="store_true", help="skip the degeneracy batch")
     ap.add_argument("--no-large-pair", action="store_true", help="skip the single large pair")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default size-bucket thresholds")
     return ap.parse_args()
 
 
@@ -568,7 +569,11 @@ def run_ours(args, rank, world, local):
 
     # the autotuner picks the size-bucket thresholds for this workload (outside the timing)
     eng.join(db, do)
-    tuning = eng.autotune_joined(db, do)
+    if args.no_autotune:
+        ci0 = eng.clip_joined(db, do)
+        tuning = eng.tuning_for(db, do, ci0["n_pairs"])
+    else:
+        tuning = eng.autotune_joined(db, do)
 
     for _ in range(args.warmup):
         step()

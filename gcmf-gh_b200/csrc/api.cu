@@ -250,6 +250,14 @@ bool json_num(const std::string& line, const char* key, double& out) {
   return true;
 }
 
+bool json_int(const std::string& line, const char* key, int64_t& out) {
+  std::string k = std::string("\"") + key + "\": ";
+  size_t a = line.find(k);
+  if (a == std::string::npos) return false;
+  out = (int64_t)std::strtoll(line.c_str() + a + k.size(), nullptr, 10);
+  return true;
+}
+
 void load_tunings(const char* path, std::vector<TuneRecord>& out) {
   FILE* f = std::fopen(path, "r");
   if (!f) return;
@@ -257,15 +265,15 @@ void load_tunings(const char* path, std::vector<TuneRecord>& out) {
   while (std::fgets(buf, sizeof(buf), f)) {
     std::string line(buf);
     TuneRecord t;
-    double v[10];
-    const char* keys[10] = {"pairs_log2", "verts_log2", "exact", "bin_grid", "tile_label", "mid_label",
-                            "big_label", "wide_label", "ms_default", "ms_tuned"};
+    int64_t v[8];
+    const char* keys[8] = {"pairs_log2", "verts_log2", "exact", "bin_grid", "tile_label", "mid_label",
+                           "big_label", "wide_label"};
     bool ok = json_str(line, "gpu", t.gpu);
-    for (int i = 0; i < 10 && ok; ++i) ok = json_num(line, keys[i], v[i]);
+    for (int i = 0; i < 8 && ok; ++i) ok = json_int(line, keys[i], v[i]);
+    ok = ok && json_num(line, "ms_default", t.ms_default) && json_num(line, "ms_tuned", t.ms_tuned);
     if (!ok) continue;
     t.pairs_log2 = (int)v[0]; t.verts_log2 = (int)v[1]; t.exact = (int)v[2];
-    t.bin_grid = (int64_t)v[3]; t.tile_label = (int64_t)v[4]; t.mid_label = (int64_t)v[5];
-    t.big_label = (int64_t)v[6]; t.wide_label = (int64_t)v[7]; t.ms_default = v[8]; t.ms_tuned = v[9];
+    t.bin_grid = v[3]; t.tile_label = v[4]; t.mid_label = v[5]; t.big_label = v[6]; t.wide_label = v[7];
     out.push_back(t);
   }
   std::fclose(f);
@@ -278,7 +286,7 @@ void save_tunings(const char* path, const std::vector<TuneRecord>& recs) {
     std::fprintf(f,
                  "{\"gpu\": \"%s\", \"pairs_log2\": %d, \"verts_log2\": %d, \"exact\": %d, \"bin_grid\": %lld, "
                  "\"tile_label\": %lld, \"mid_label\": %lld, \"big_label\": %lld, \"wide_label\": %lld, "
-                 "\"ms_default\": %.4f, \"ms_tuned\": %.4f}\n",
+                 "\"ms_default\": %.6f, \"ms_tuned\": %.6f}\n",
                  t.gpu.c_str(), t.pairs_log2, t.verts_log2, t.exact, (long long)t.bin_grid, (long long)t.tile_label,
                  (long long)t.mid_label, (long long)t.big_label, (long long)t.wide_label, t.ms_default, t.ms_tuned);
   std::fclose(f);
