@@ -275,7 +275,7 @@ def _latency_summary(infos, arrivals, rate):
             "errors": bad}
 
 
-def serve_measure(local, seconds=0.5):
+def serve_measure(local, seconds=2.0):
     """p50/p99 latency and pairs/s of the continuous-batching server at 2k/10k/50k req/s,
     and of the plain one-query-per-launch form (one worker, batches of one query)."""
     import gcmfgh
@@ -283,16 +283,23 @@ def serve_measure(local, seconds=0.5):
     resident, queries = synth.serving_workload(seed=4)
     rng = np.random.default_rng(44)
     out = {"workload": SERVE_WORKLOAD, "batched": [], "plain": []}
-    with gcmfgh.Server(resident, device=local, workers=2) as srv:
+    with gcmfgh.Server(resident, device=local, workers=4) as srv:
         _open_loop(srv, queries, 2000, 0.1, rng)                     # warm-up
         for rate in (2000, 10000, 50000):
+            ms0, w0 = srv.phases()
             infos, arr = _open_loop(srv, queries, rate, seconds, rng)
-            out["batched"].append(_latency_summary(infos, arr, rate))
+            ms1, w1 = srv.phases()
+            summ = _latency_summary(infos, arr, rate)
+            tot = sum(ms1[k] - ms0[k] for k in ms1) or 1.0
+            summ["phase_share"] = {k: round((ms1[k] - ms0[k]) / tot, 4) for k in ms1}
+            summ["phase_ms_summed"] = {k: round(ms1[k] - ms0[k], 2) for k in ms1}
+            summ["work"] = {k: w1[k] - w0[k] for k in w1}
+            out["batched"].append(summ)
         out["batched_stats"] = srv.stats()
     with gcmfgh.Server(resident, device=local, workers=1, max_batch_queries=1) as srv:
         _open_loop(srv, queries, 500, 0.1, rng)
         for rate in (2000, 10000, 50000):
-            infos, arr = _open_loop(srv, queries, rate, seconds, rng, max_requests=2000)
+            infos, arr = _open_loop(srv, queries, rate, seconds, rng, max_requests=1000)
             out["plain"].append(_latency_summary(infos, arr, rate))
     return out
 

@@ -146,6 +146,53 @@ __global__ void candidate_kernel(const double* __restrict__ qmbr, const uint8_t*
   if (kMode == 0 && lane_id() == 0) cnt[w] = c;
 }
 
+// Pinned host blocks for the batches' results, recycled: a batch's results are copied from
+// the device into one block, its requests read their ranges from it, and the block goes
+// back to the pool when the last of them has been taken.
+class PinnedPool {
+ public:
+  struct Block { char* p = nullptr; size_t cap = 0; };
+  ~PinnedPool() { for (auto& b : free_) cudaFreeHost(b.p); }
+  Block get(size_t n) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      size_t best = free_.size();
+      for (size_t i = 0; i < free_.size(); ++i)
+        if (free_[i].cap >= n && (best == free_.size() || free_[i].cap < free_[best].cap)) best = i;
+      if (best < free_.size()) {
+        Block b = free_[best];
+        free_.erase(free_.begin() + (std::ptrdiff_t)best);
+        return b;
+      }
+    }
+    Block b;
+    const size_t cap = std::max<size_t>(n + n / 4, size_t(16) << 20);
+    if (cudaMallocHost(&b.p, cap) != cudaSuccess) { cudaGetLastError(); return Block{}; }
+    b.cap = cap;
+    return b;
+  }
+  void put(Block b) {
+    if (!b.p) return;
+    std::lock_guard<std::mutex> lk(mu_);
+    free_.push_back(b);
+  }
+ private:
+  std::mutex mu_;
+  std::vector<Block> free_;
+};
+
+// A batch's results on the host, shared by its requests: pairs sorted by (query, resident
+// id), then their components and vertices in the same order, so each request's part is
+// one range of each array.
+struct BatchOut {
+  PinnedPool* pool = nullptr;
+  PinnedPool::Block blk;
+  size_t o_b = 0, o_o = 0, o_st = 0, o_nc = 0, o_cs = 0, o_xy = 0;
+  ~BatchOut() { if (pool) pool->put(blk); }
+  const int32_t* i32(size_t o) const { return reinterpret_cast<const int32_t*>(blk.p + o); }
+  const double* xy() const { return reinterpret_cast<const double*>(blk.p + o_xy); }
+};
+
 struct Request {
   std::vector<double> ring;      // open ring, interleaved x,y
   int32_t n = 0;
@@ -154,8 +201,8 @@ struct Request {
   int status = GCMFGH_OK;
   bool done = false;
   int64_t n_candidates = 0;
-  std::vector<int32_t> hit_ids, hit_status, hit_ncomp, comp_size;
-  std::vector<double> xy;
+  std::shared_ptr<const BatchOut> out;    // results: pairs [p0, p1), components [c0, c1), vertices [v0, v1)
+  int64_t p0 = 0, p1 = 0, c0 = 0, c1 = 0, v0 = 0, v1 = 0;
 };
 
 template <class T>
@@ -198,18 +245,25 @@ struct gcmfgh_server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<uint64_t> queue;
+  PinnedPool out_pool;           // declared before the requests, so it outlives their results
   std::unordered_map<uint64_t, std::shared_ptr<Request>> reqs;
   uint64_t next_ticket = 1;
   bool stopping = false;
   std::vector<std::thread> workers;
   std::atomic<int64_t> batches{0}, batched_queries{0}, peak_batch{0};
   int64_t next_batch = 0;
+  // per-phase time summed over batches (batches of different workers overlap on the GPU,
+  // so the sums show shares, not wall time): host staging, H2D, MBR candidates, join
+  // stages J3-J6, clip, D2H, host split; and totals of the work those phases did
+  std::mutex stats_mu;
+  double phase_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+  int64_t work[4] = {0, 0, 0, 0};     // query vertices, clipped pairs, merged-ring vertices, result vertices
 
   LayerDev resident() const { return LayerDev{r_xy, r_vnum, r_vps, r_n}; }
   void worker_main(int wid);
   int run_batch(std::vector<std::shared_ptr<Request>>& batch, int64_t batch_id, cudaStream_t s, cudaStream_t aux,
                 Arena& A,
-                Arena& C, int* d_err, int64_t* h_scratch, Pinned<char>& hin, Pinned<char>& hout);
+                Arena& C, int* d_err, int64_t* h_scratch, Pinned<char>& hin, cudaEvent_t* ev);
 };
 
 namespace {
@@ -223,9 +277,10 @@ size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64_t batch_id, cudaStream_t s,
                              cudaStream_t aux,
                              Arena& A, Arena& C, int* d_err, int64_t* h_scratch, Pinned<char>& hin,
-                             Pinned<char>& hout) {
+                             cudaEvent_t* ev) {
   A.reset();
   C.reset();
+  const int64_t t_stage0 = now_ns();
   const int64_t nq = (int64_t)batch.size();
   int64_t nv = 0;
   for (auto& r : batch) nv += r->n + 1;
@@ -255,9 +310,12 @@ int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64
   unsigned long long* d_cnt = A.take_n<unsigned long long>(8);
   void* stmp = A.take(scan_temp_bytes(nq));
   if (!dq || !qmbr || !qvalid || !qcnt || !qoff || !d_total || !d_cnt || !stmp) return ST_OUT_OF_MEMORY;
+  const int64_t t_stage1 = now_ns();
+  cudaEventRecord(ev[0], s);
   cudaMemsetAsync(d_err, 0, sizeof(int), s);
   cudaMemsetAsync(d_cnt, 0, 8 * sizeof(unsigned long long), s);
   cudaMemcpyAsync(dq, hin.p, bxy + bvn + bvp, cudaMemcpyHostToDevice, s);
+  cudaEventRecord(ev[1], s);
   LayerDev Lq{reinterpret_cast<double*>(dq), reinterpret_cast<int32_t*>(dq + bxy),
               reinterpret_cast<int64_t*>(dq + bxy + bvn), nq};
   { serve_mbr_kernel<<<blocks_for_warps(nq), kThreads, 0, s>>>(Lq, qmbr, qvalid); note_launch(); }
@@ -286,8 +344,10 @@ int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64
     { candidate_kernel<1><<<blocks_for_warps(nq), kThreads, 0, s>>>(qmbr, qvalid, nq, r_mbr, grid, nullptr, qoff,
                                                                      keys, obits); note_launch(); }
     radix_sort_pairs(keys, vals, kAlt, vAlt, K, ((obits + qbits + 7) / 8) * 8, rtmp, d_err, s);
+    cudaEventRecord(ev[2], s);
     st = join_from_keys(Lq, resident(), keys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, nullptr, aux);
     if (st != ST_OK) return st;
+    cudaEventRecord(ev[3], s);
     if (J.n_clip > 0) {
       ClipParams prm;
       prm.eps = opt.eps;
@@ -297,15 +357,22 @@ int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64
       st = run_clip(Lq, resident(), J.clip_b, J.clip_o, J.n_clip, prm, C, CD, d_err, h_scratch, s, nullptr, aux);
       if (st != ST_OK) return st;
     }
+  } else {
+    cudaEventRecord(ev[2], s);
+    cudaEventRecord(ev[3], s);
   }
+  cudaEventRecord(ev[4], s);
   // ---- results to the host
   const int64_t np = J.n_clip, nc = CD.n_components, nvo = CD.n_vertices;
   const size_t o_cnt = 0, o_b = align16(sizeof(int32_t) * nq), o_o = o_b + align16(sizeof(int32_t) * np),
                o_st = o_o + align16(sizeof(int32_t) * np), o_nc = o_st + align16(sizeof(int32_t) * np),
                o_cs = o_nc + align16(sizeof(int32_t) * np), o_xy = o_cs + align16(sizeof(int32_t) * nc),
                o_err = o_xy + align16(sizeof(double) * 2 * nvo), total = o_err + 16;
-  if (!hout.reserve(total)) return ST_OUT_OF_MEMORY;
-  char* H = hout.p;
+  auto out = std::make_shared<BatchOut>();
+  out->blk = out_pool.get(total);
+  if (!out->blk.p) return ST_OUT_OF_MEMORY;
+  out->pool = &out_pool;
+  char* H = out->blk.p;
   cudaMemcpyAsync(H + o_cnt, qcnt, sizeof(int32_t) * nq, cudaMemcpyDeviceToHost, s);
   if (np > 0) {
     cudaMemcpyAsync(H + o_b, J.clip_b, sizeof(int32_t) * np, cudaMemcpyDeviceToHost, s);
@@ -316,38 +383,42 @@ int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64
   if (nc > 0) cudaMemcpyAsync(H + o_cs, CD.comp_size, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, s);
   if (nvo > 0) cudaMemcpyAsync(H + o_xy, CD.xy, sizeof(double) * 2 * nvo, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(H + o_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaEventRecord(ev[5], s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
   if (*reinterpret_cast<int*>(H + o_err) != 0) return ST_DEVICE_ERROR;
   const int64_t t_done = now_ns();
+  float gpu_ms[5] = {0, 0, 0, 0, 0};
+  for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&gpu_ms[i], ev[i], ev[i + 1]);
+  // the batch's results stay in the block, shared by its requests (each takes its ranges)
+  out->o_b = o_b; out->o_o = o_o; out->o_st = o_st; out->o_nc = o_nc; out->o_cs = o_cs; out->o_xy = o_xy;
   const int32_t* hcnt = reinterpret_cast<const int32_t*>(H + o_cnt);
-  const int32_t* hb = reinterpret_cast<const int32_t*>(H + o_b);
-  const int32_t* ho = reinterpret_cast<const int32_t*>(H + o_o);
-  const int32_t* hst = reinterpret_cast<const int32_t*>(H + o_st);
-  const int32_t* hnc = reinterpret_cast<const int32_t*>(H + o_nc);
-  const int32_t* hcs = reinterpret_cast<const int32_t*>(H + o_cs);
-  const double* hxy2 = reinterpret_cast<const double*>(H + o_xy);
+  const int32_t* hb = out->i32(o_b);
+  const int32_t* hnc = out->i32(o_nc);
+  const int32_t* hcs = out->i32(o_cs);
   // pairs are sorted by (query, resident id); components and vertices follow pair order
   int64_t p = 0, c = 0, v = 0;
   for (int64_t i = 0; i < nq; ++i) {
     Request& r = *batch[i];
     r.n_candidates = hcnt[i];
-    r.hit_ids.clear(); r.hit_status.clear(); r.hit_ncomp.clear(); r.comp_size.clear(); r.xy.clear();
-    while (p < np && hb[p] == i) {
-      r.hit_ids.push_back(ho[p]);
-      r.hit_status.push_back(hst[p]);
-      r.hit_ncomp.push_back(hnc[p]);
-      for (int k = 0; k < hnc[p]; ++k) {
-        int32_t sz = hcs[c++];
-        r.comp_size.push_back(sz);
-        r.xy.insert(r.xy.end(), hxy2 + 2 * v, hxy2 + 2 * (v + sz));
-        v += sz;
-      }
-      ++p;
-    }
+    r.out = out;
+    r.p0 = p; r.c0 = c; r.v0 = v;
+    for (; p < np && hb[p] == i; ++p)
+      for (int k = 0; k < hnc[p]; ++k) v += hcs[c++];
+    r.p1 = p; r.c1 = c; r.v1 = v;
     r.done_ns = t_done;
     r.batch_id = batch_id;
     r.batch_queries = nq;
     r.status = GCMFGH_OK;
+  }
+  {
+    std::lock_guard<std::mutex> lk(stats_mu);
+    phase_ms[0] += (t_stage1 - t_stage0) * 1e-6;
+    for (int i = 0; i < 5; ++i) phase_ms[1 + i] += gpu_ms[i];
+    phase_ms[6] += (now_ns() - t_done) * 1e-6;
+    work[0] += nv;
+    work[1] += np;
+    work[2] += CD.n_ring_vertices;
+    work[3] += nvo;
   }
   return ST_OK;
 }
@@ -363,7 +434,9 @@ void gcmfgh_server::worker_main(int wid) {
   int64_t* h_scratch = nullptr;
   cudaMalloc(&d_err, sizeof(int));
   cudaMallocHost(&h_scratch, 64 * sizeof(int64_t));
-  Pinned<char> hin, hout;
+  Pinned<char> hin;
+  cudaEvent_t ev[6];
+  for (auto& e : ev) cudaEventCreate(&e);
   for (;;) {
     std::vector<std::shared_ptr<Request>> batch;
     int64_t bid;
@@ -395,14 +468,14 @@ void gcmfgh_server::worker_main(int wid) {
       if (!queue.empty()) cv_work.notify_one();
     }
     if (batch.empty()) continue;
-    int st = run_batch(batch, bid, s, aux, A, C, d_err, h_scratch, hin, hout);
+    int st = run_batch(batch, bid, s, aux, A, C, d_err, h_scratch, hin, ev);
     if (st == ST_OUT_OF_MEMORY && batch.size() > 1) {
       // split the batch until it fits; a single query that does not fit fails alone
       A.release(); C.release();
       std::vector<std::shared_ptr<Request>> half(batch.begin() + batch.size() / 2, batch.end());
       batch.resize(batch.size() / 2);
-      st = run_batch(batch, bid, s, aux, A, C, d_err, h_scratch, hin, hout);
-      int st2 = run_batch(half, bid, s, aux, A, C, d_err, h_scratch, hin, hout);
+      st = run_batch(batch, bid, s, aux, A, C, d_err, h_scratch, hin, ev);
+      int st2 = run_batch(half, bid, s, aux, A, C, d_err, h_scratch, hin, ev);
       if (st2 != ST_OK) for (auto& r : half) { r->status = st2; r->done_ns = now_ns(); }
       std::lock_guard<std::mutex> lk(mu);
       for (auto& r : half) r->done = true;
@@ -425,6 +498,7 @@ void gcmfgh_server::worker_main(int wid) {
   }
   A.release();
   C.release();
+  for (auto& e : ev) cudaEventDestroy(e);
   cudaFree(d_err);
   cudaFreeHost(h_scratch);
   cudaStreamDestroy(s);
@@ -564,9 +638,9 @@ gcmfgh_status gcmfgh_serve_submit(gcmfgh_server* S, const double* xy, int32_t n,
 static void fill_info(const Request& r, gcmfgh_serve_result* info) {
   if (!info) return;
   info->status = r.status;
-  info->n_hits = (int64_t)r.hit_ids.size();
-  info->n_components = (int64_t)r.comp_size.size();
-  info->n_vertices = (int64_t)r.xy.size() / 2;
+  info->n_hits = r.p1 - r.p0;
+  info->n_components = r.c1 - r.c0;
+  info->n_vertices = r.v1 - r.v0;
   info->n_candidates = r.n_candidates;
   info->arrival_ns = r.arrival_ns;
   info->admitted_ns = r.admitted_ns;
@@ -610,11 +684,14 @@ gcmfgh_status gcmfgh_serve_take(gcmfgh_server* S, uint64_t ticket, int32_t* hit_
     r = it->second;
     S->reqs.erase(it);
   }
-  if (hit_ids) std::copy(r->hit_ids.begin(), r->hit_ids.end(), hit_ids);
-  if (hit_status) std::copy(r->hit_status.begin(), r->hit_status.end(), hit_status);
-  if (hit_ncomp) std::copy(r->hit_ncomp.begin(), r->hit_ncomp.end(), hit_ncomp);
-  if (comp_size) std::copy(r->comp_size.begin(), r->comp_size.end(), comp_size);
-  if (xy) std::copy(r->xy.begin(), r->xy.end(), xy);
+  const BatchOut* o = r->out.get();
+  if (!o) return GCMFGH_OK;                       // a failed batch has no results
+  const int64_t np = r->p1 - r->p0, nc = r->c1 - r->c0, nv = r->v1 - r->v0;
+  if (hit_ids) std::memcpy(hit_ids, o->i32(o->o_o) + r->p0, sizeof(int32_t) * np);
+  if (hit_status) std::memcpy(hit_status, o->i32(o->o_st) + r->p0, sizeof(int32_t) * np);
+  if (hit_ncomp) std::memcpy(hit_ncomp, o->i32(o->o_nc) + r->p0, sizeof(int32_t) * np);
+  if (comp_size) std::memcpy(comp_size, o->i32(o->o_cs) + r->c0, sizeof(int32_t) * nc);
+  if (xy) std::memcpy(xy, o->xy() + 2 * r->v0, sizeof(double) * 2 * nv);
   return GCMFGH_OK;
 }
 
@@ -623,6 +700,14 @@ gcmfgh_status gcmfgh_serve_stats(gcmfgh_server* S, int64_t* batches, int64_t* qu
   if (batches) *batches = S->batches.load();
   if (queries) *queries = S->batched_queries.load();
   if (peak_batch) *peak_batch = S->peak_batch.load();
+  return GCMFGH_OK;
+}
+
+gcmfgh_status gcmfgh_serve_phases(gcmfgh_server* S, double* ms, int64_t* work) {
+  if (!S) return GCMFGH_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(S->stats_mu);
+  if (ms) for (int i = 0; i < 7; ++i) ms[i] = S->phase_ms[i];
+  if (work) for (int i = 0; i < 4; ++i) work[i] = S->work[i];
   return GCMFGH_OK;
 }
 

@@ -150,6 +150,7 @@ def lib():
         L.gcmfgh_serve_take.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp]
         L.gcmfgh_serve_stats.argtypes = [vp, P(i64), P(i64), P(i64)]
         L.gcmfgh_serve_close.argtypes = [vp]
+        L.gcmfgh_serve_phases.argtypes = [vp, vp, vp]
         _lib = L
     return _lib
 
@@ -517,6 +518,15 @@ class Server:
         b, q, p = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _check(lib().gcmfgh_serve_stats(self.h, ctypes.byref(b), ctypes.byref(q), ctypes.byref(p)))
         return {"batches": b.value, "queries": q.value, "peak_batch": p.value}
+
+    def phases(self):
+        """Per-phase serving time (ms, summed over batches) and work totals."""
+        ms = (ctypes.c_double * 7)()
+        work = (ctypes.c_int64 * 4)()
+        _check(lib().gcmfgh_serve_phases(self.h, ms, work))
+        names = ("host_stage", "h2d", "candidates", "join_J3_J6", "clip", "d2h", "host_split")
+        return ({n: ms[i] for i, n in enumerate(names)},
+                dict(zip(("query_vertices", "pairs", "ring_vertices", "result_vertices"), list(work))))
 
     def close(self):
         if self.h:

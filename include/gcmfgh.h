@@ -378,6 +378,13 @@ gcmfgh_status gcmfgh_serve_wait(gcmfgh_server* srv, uint64_t ticket, int64_t tim
 gcmfgh_status gcmfgh_serve_take(gcmfgh_server* srv, uint64_t ticket, int32_t* hit_ids, int32_t* hit_status,
                                 int32_t* hit_ncomp, int32_t* comp_size, double* xy);
 gcmfgh_status gcmfgh_serve_stats(gcmfgh_server* srv, int64_t* batches, int64_t* queries, int64_t* peak_batch);
+/* Where serving time goes, summed over all batches so far (batches of different workers
+ * overlap on the GPU, so these are shares, not wall time).  ms[7]: host staging, H2D,
+ * MBR candidates (grid index + sort), join stages J3-J6, clip, D2H (GPU times from CUDA
+ * events on the worker's stream), and the host split of the results.  work[4]: query
+ * vertices, clipped pairs, merged-ring vertices, result vertices.  No counterpart in the
+ * reference (it has no serving loop). */
+gcmfgh_status gcmfgh_serve_phases(gcmfgh_server* srv, double* ms, int64_t* work);
 /* finishes the queued queries, stops the workers and frees the device state */
 gcmfgh_status gcmfgh_serve_close(gcmfgh_server* srv);
 
