@@ -679,7 +679,8 @@ def run_ours(args, rank, world, local):
             b = stage_bytes(k, *counts)
             if b:
                 per_stage[k] = {"ms": round(v, 4), "algorithmic_bytes": b,
-                                "frac": round(b / (v * 1e-3) / 1e9 / peak, 5)}
+                                "frac": round(b / (v * 1e-3) / 1e9 / peak, 5),
+                                "traffic": traffic_from_profiles(k)}
         step_bytes = (32 * (base.n_polys + ovl.n_polys) + 8 * ji["n_pairs"] + 16 * cand_v
                       + 16 * ci["n_ring_vertices"] + 16 * ci["n_vertices"] + 8 * pairs)
         line = {
