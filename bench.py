@@ -715,6 +715,11 @@ def run_ours(args, rank, world, local):
         plain = plain_measure(eng, db, do, stream)
         plain["batched_over_plain"] = line["value"] / world / plain["value"]
         line["plain"] = plain
+    # the sections below run engines of their own: give back this one's device memory first
+    eng.close()
+    del db, do, flush, pinned
+    torch.cuda.empty_cache()
+    if rank == 0:
         if not args.no_serve:
             line["serving"] = serve_measure(local)
         if not args.no_large_pair:
@@ -731,7 +736,6 @@ def run_ours(args, rank, world, local):
                                               f"{p} clip pairs clipped by the reference's sequential GH "
                                               f"code built from its sources"}
         print(json.dumps(line), flush=True)
-    eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -518,7 +518,11 @@ int gcmfgh_last_device_error(gcmfgh_ctx* c) { return c ? c->last_err : -1; }
 
 unsigned long long gcmfgh_launch_count(void) { return launch_counter(); }
 
-gcmfgh_status gcmf_join(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, gcmfgh_join_info* info) {
+}  // extern "C"
+
+// gcmf_join; ovl_ready (may be null): an event recorded after the overlay's upload
+static gcmfgh_status join_impl(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, gcmfgh_join_info* info,
+                               cudaEvent_t ovl_ready) {
   if (!c || !layer_ok(b) || !layer_ok(o)) return GCMFGH_INVALID_ARGUMENT;
   cudaSetDevice(c->device);
   c->join_arena.reset();
@@ -526,7 +530,7 @@ gcmfgh_status gcmf_join(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer
   c->marks[0].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   int st = run_join(to_dev(b), to_dev(o), c->join_arena, c->join, c->d_err, c->h_scratch, c->stream,
-                    &c->marks[0], c->aux, c->join_f32);
+                    &c->marks[0], c->aux, c->join_f32, ovl_ready);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_join = true;
@@ -543,6 +547,12 @@ gcmfgh_status gcmf_join(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer
     info->n_clip = c->join.n_clip;
   }
   return GCMFGH_OK;
+}
+
+extern "C" {
+
+gcmfgh_status gcmf_join(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, gcmfgh_join_info* info) {
+  return join_impl(c, b, o, info, nullptr);
 }
 
 gcmfgh_status gcmf_join_get(gcmfgh_ctx* c, int f, void* dst, int64_t cap, int on_dev, int64_t* bytes) {
@@ -885,24 +895,31 @@ gcmfgh_status gcmfgh_join_clip_host(gcmfgh_ctx* c, const gcmfgh_layer* bh, const
   c->layer_arena.reset();
   gcmfgh_layer dl[2];
   const gcmfgh_layer* hl[2] = {bh, oh};
+  // The overlay goes up on the auxiliary stream, where the join processes it: the base
+  // layer's MBRs and sort on the main stream overlap the overlay's copy.
+  cudaEvent_t ovl_done = nullptr;
+  cudaStream_t ovl_stream = c->stream;
+  if (c->aux && cudaEventCreateWithFlags(&ovl_done, cudaEventDisableTiming) == cudaSuccess) ovl_stream = c->aux;
+  struct EvGuard { cudaEvent_t e; ~EvGuard() { if (e) { cudaEventSynchronize(e); cudaEventDestroy(e); } } } guard{ovl_done};
   for (int i = 0; i < 2; ++i) {
     const gcmfgh_layer* h = hl[i];
+    cudaStream_t cs = i == 0 ? c->stream : ovl_stream;
     double* xy = c->layer_arena.take_n<double>(2 * h->n_vertices);
     int32_t* vn = c->layer_arena.take_n<int32_t>(h->n_polys);
     int64_t* vp = c->layer_arena.take_n<int64_t>(h->n_polys);
     if (!xy || !vn || !vp) return GCMFGH_OUT_OF_MEMORY;
     if (h->n_polys > 0) {
       if (!h->coords || !h->vnum || !h->vps) return GCMFGH_INVALID_ARGUMENT;
-      if (cudaMemcpyAsync(xy, h->coords, sizeof(double) * 2 * h->n_vertices, cudaMemcpyHostToDevice, c->stream) !=
+      if (cudaMemcpyAsync(xy, h->coords, sizeof(double) * 2 * h->n_vertices, cudaMemcpyHostToDevice, cs) !=
               cudaSuccess ||
-          cudaMemcpyAsync(vn, h->vnum, sizeof(int32_t) * h->n_polys, cudaMemcpyHostToDevice, c->stream) !=
-              cudaSuccess ||
-          cudaMemcpyAsync(vp, h->vps, sizeof(int64_t) * h->n_polys, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+          cudaMemcpyAsync(vn, h->vnum, sizeof(int32_t) * h->n_polys, cudaMemcpyHostToDevice, cs) != cudaSuccess ||
+          cudaMemcpyAsync(vp, h->vps, sizeof(int64_t) * h->n_polys, cudaMemcpyHostToDevice, cs) != cudaSuccess)
         return GCMFGH_CUDA_ERROR;
     }
     dl[i] = gcmfgh_layer{xy, vn, vp, h->n_polys, h->n_vertices};
   }
-  gcmfgh_status r = gcmf_join(c, &dl[0], &dl[1], jinfo);
+  if (ovl_done) cudaEventRecord(ovl_done, ovl_stream);
+  gcmfgh_status r = join_impl(c, &dl[0], &dl[1], jinfo, ovl_done);
   if (r != GCMFGH_OK) return r;
   return gh_clip_joined(c, &dl[0], &dl[1], cinfo);
 }

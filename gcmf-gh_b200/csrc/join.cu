@@ -454,7 +454,7 @@ int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s) {
 }
 
 int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int* d_err,
-             int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux, int f32) {
+             int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux, int f32, cudaEvent_t ovl_ready) {
   // f32 bit 0: FP32 prefilter of the sweep's y test; bit 1: of the common-MBR edge test
   // (needs the layers' vertex counts, for their FP32 copies)
   const bool f32cmf = (f32 & 2) && Lb0.nverts > 0 && Lo0.nverts > 0;
@@ -504,6 +504,8 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
     so = aux;
   }
   { mbr_kernel<<<blocks_for_warps(nb), kThreads, 0, s>>>(Lb, J.mbr_b, J.valid_b, keyB, idB, d_cnt + 0, xyfB); note_launch(); }
+  // the overlay may still be on its way to the device (ovl_ready, recorded after its copy)
+  if (ovl_ready) cudaStreamWaitEvent(so, ovl_ready, 0);
   { mbr_kernel<<<blocks_for_warps(no), kThreads, 0, so>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1, xyfO); note_launch(); }
   // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
   radix_sort_pairs(keyB, idB, kAlt, vAlt, nb, 64, tmp, d_err, s);
