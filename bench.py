@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--no-precision", action="store_true", help="skip the degeneracy batch")
     ap.add_argument("--no-large-pair", action="store_true", help="skip the single large pair")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default size-bucket thresholds")
+    ap.add_argument("--fused-emit", type=int, default=None,
+                    help="0: count, then emit the intersection records; 1: one pass, block-wide "
+                         "appends; 2: one pass, warp appends (default: the library's)")
     return ap.parse_args()
 
 
@@ -136,6 +139,7 @@ def stage_bytes(stage, ji, ci, nb, no, vb, vo, cand_vertices=0):
         "clip:fill+link": 33 * recs + 20 * ring,
         "clip:count": 16 * ring + 8 * C,
         "clip:emit": 16 * ring + 33 * recs,
+        "clip:count+emit": 16 * ring + 8 * C + 33 * recs,
         "join:mbr+sort": 16 * (vb + vo) + 40 * (nb + no),
         "join:sweep-count": 36 * (nb + no),
         "join:sweep-emit+sort": 36 * (nb + no) + 16 * K,
@@ -574,6 +578,8 @@ def run_ours(args, rank, world, local):
         ci = eng.clip_joined(db, do)
         return ji, ci
 
+    if args.fused_emit is not None:
+        eng.set_tuning(fused_emit=args.fused_emit)
     # the autotuner picks the size-bucket thresholds for this workload (outside the timing)
     eng.join(db, do)
     if args.no_autotune:

@@ -107,6 +107,7 @@ struct gcmfgh_ctx {
   std::string gpu_name;
   bool tuning_explicit = false;   // gcmfgh_set_tuning was called: recorded tunings are not applied
   int join_f32 = 1;               // FP32 prefilters of the join (bit 0 MBR y test, bit 1 edge test)
+  bool hint_explicit = false;     // gcmfgh_set_tuning fixed the record capacity hint
   std::vector<TuneRecord> tunings;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
@@ -227,6 +228,7 @@ gcmfgh_status run_clip_ctx(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_la
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_clip = true;
+  if (!c->hint_explicit) c->prm.rec_hint = c->clip.n_records;   // the next clip's record capacity
   return clip_info(c, info);
 }
 
@@ -502,6 +504,16 @@ gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* c, int key, int64_t value) {
   if (!c || value < 0) return GCMFGH_INVALID_ARGUMENT;
   if (key == GCMFGH_TUNE_F32_FILTER) {
     c->join_f32 = (int)(value & 3);
+    return GCMFGH_OK;
+  }
+  if (key == GCMFGH_TUNE_FUSED_EMIT) {
+    if (value > 2) return GCMFGH_INVALID_ARGUMENT;
+    c->prm.fused_emit = (int)value;
+    return GCMFGH_OK;
+  }
+  if (key == GCMFGH_TUNE_RECORD_HINT) {
+    c->prm.rec_hint = value;
+    c->hint_explicit = value > 0;
     return GCMFGH_OK;
   }
   c->tuning_explicit = true;

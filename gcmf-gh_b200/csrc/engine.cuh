@@ -82,6 +82,8 @@ struct ClipParams {
                                        // high-occupancy labelling kernels
   int64_t mid_label_min = 1ll << 10;   // merged-ring slots above which a block labels a pair
   int64_t big_label_min = 1ll << 18;   // merged-ring slots above which a pair is labelled grid-wide
+  int fused_emit = 1;                  // count and emit the intersection records in one pass
+  int64_t rec_hint = 0;                // records expected (the last clip's count; 0 unknown)
 };
 
 // Clip outputs (device, owned by the clip arena).

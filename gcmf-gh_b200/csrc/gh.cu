@@ -48,6 +48,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarpsPerBlock = kThreads / 32;
 constexpr int kChunk = 64;             // edge pairs per warp work unit (2 x 32 lanes)
+constexpr int64_t kFirstRecordCap = 1 << 22;   // records held by a fused count + emit without a hint
 constexpr int kFilterTile = 4;         // lanes per small pair in the edge filter
 constexpr int64_t kFilterTileMax = 64; // ring size up to which the narrow tiles take a pair
 
@@ -268,18 +269,139 @@ intersect_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, const int64_t* 
   if (kMode == 0 && lane_id() == 0) { chunkRec[c] = recs; chunkQ[c] = qhits; }
 }
 
+// Count and emit in one pass over the chunks.  Each warp classifies its chunk's edge pairs
+// from both sides as the count pass does and stages its P-side records in shared memory;
+// the block then takes one range of a global counter and copies its records there.  The
+// records end up in block order, which nothing downstream depends on (the ring fill orders
+// a ring's insertions by parameter and other edge; a link keeps the largest other edge).
+// Per pair, the P-side records and the Q-side hits are added into pairRec / pairQ (skipped
+// when pairRec is null: a re-run after an overflow).  Records at or past cap are counted
+// and not written; the host then re-runs with arrays of the counted size.
+struct FusedRecords {
+  unsigned long long* total;   // records taken so far (all blocks)
+  int64_t cap;                 // records the arrays hold
+  int32_t* pairRec;            // per pair: P-side records
+  int32_t* pairQ;              // per pair: Q-side hits
+};
+
+template <int kExact, int kWarpAppend>
+__global__ void __launch_bounds__(kThreads, kExact ? 2 : 4)
+intersect_fused_kernel(LayerDev Lb, LayerDev Lo, PairDev D, const int64_t* __restrict__ chunkOff, int64_t nChunks,
+                       const int32_t* __restrict__ cP, const int32_t* __restrict__ cQ,
+                       const int64_t* __restrict__ offP, const int64_t* __restrict__ offQ,
+                       const int32_t* __restrict__ LP, const int32_t* __restrict__ LQ, double eps, Records R,
+                       const int32_t* __restrict__ chunkPair, FusedRecords F) {
+  constexpr int kWarps = kThreads / 32;
+  constexpr int kStage = kWarps * kChunk;           // at most one record per edge pair
+  __shared__ double sA[kStage], sB[kStage];
+  __shared__ int32_t sP[kStage], sQ[kStage];
+  __shared__ int8_t sT[kStage];
+  __shared__ int sOff[kWarps + 1];
+  __shared__ int32_t sK[kWarps];
+  __shared__ unsigned long long sBase;
+  const int wib = (int)(threadIdx.x >> 5);
+  const int64_t c = (int64_t)blockIdx.x * kWarps + wib;
+  int recs = 0, qhits = 0;
+  int64_t k = -1;
+  if (c < nChunks) {
+    k = chunkPair[c];
+    const int nq = cQ[k];
+    const int64_t W = (int64_t)cP[k] * nq;
+    const int64_t t0 = (c - chunkOff[k]) * kChunk;
+    const int pside = D.pSide[k];
+    const double2* pv = layer_xy(Lb, Lo, pside) + D.pS[k];
+    const double2* qv = layer_xy(Lb, Lo, 1 - pside) + D.qS[k];
+    const int np_ = D.nP[k], nq_ = D.nQ[k];
+    const int32_t* lp = LP + offP[k];
+    const int32_t* lq = LQ + offQ[k];
+    for (int it = 0; it < kChunk / 32; ++it) {
+      const int64_t t = t0 + it * 32 + lane_id();
+      int tp = 0, tq = 0, pe = 0, qe = 0;
+      double alpha = 0, beta = 0;
+      if (t < W) {
+        if (W <= INT32_MAX) {
+          const int tt = (int)t, r = tt / nq;
+          pe = lp[r];
+          qe = lq[tt - r * nq];
+        } else {
+          pe = lp[t / nq];
+          qe = lq[t % nq];
+        }
+        double2 P1 = __ldg(pv + pe), P2 = __ldg(pv + (pe + 1 < np_ ? pe + 1 : 0));
+        double2 Q1 = __ldg(qv + qe), Q2 = __ldg(qv + (qe + 1 < nq_ ? qe + 1 : 0));
+        if (edge_boxes_touch(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y)) {
+          if (!kExact) {
+            bool qhit;
+            tp = classify_edges_both(P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta, qhit);
+            tq = qhit ? 1 : 0;
+          } else {
+            double a2, b2;
+            tp = classify_mode(kExact, P1.x, P1.y, P2.x, P2.y, Q1.x, Q1.y, Q2.x, Q2.y, eps, alpha, beta);
+            tq = classify_mode(kExact, Q1.x, Q1.y, Q2.x, Q2.y, P1.x, P1.y, P2.x, P2.y, eps, a2, b2);
+          }
+        }
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, tp != 0);
+      if (tp != 0) {
+        const int i = wib * kChunk + recs + __popc(m & lanemask_lt());
+        sP[i] = pe; sQ[i] = qe; sA[i] = alpha; sB[i] = beta; sT[i] = (int8_t)tp;
+      }
+      recs += __popc(m);
+      qhits += __popc(__ballot_sync(0xffffffffu, tq != 0));
+    }
+  }
+  if (lane_id() == 0 && k >= 0 && F.pairRec) {
+    if (recs) atomicAdd(&F.pairRec[k], recs);
+    if (qhits) atomicAdd(&F.pairQ[k], qhits);
+  }
+  if (kWarpAppend) {                                // each warp takes its own range
+    unsigned long long b = 0;
+    if (lane_id() == 0 && recs) b = atomicAdd(F.total, (unsigned long long)recs);
+    const int64_t base = (int64_t)__shfl_sync(0xffffffffu, b, 0);
+    __syncwarp();
+    for (int j = lane_id(); j < recs; j += 32) {
+      const int i = wib * kChunk + j;
+      const int64_t r = base + j;
+      if (r < F.cap) { R.p[r] = sP[i]; R.q[r] = sQ[i]; R.a[r] = sA[i]; R.b[r] = sB[i]; R.t[r] = sT[i]; R.k[r] = (int32_t)k; }
+    }
+    return;
+  }
+  if (lane_id() == 0) { sOff[wib] = recs; sK[wib] = (int32_t)k; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int w = 0; w < kWarps; ++w) { const int n = sOff[w]; sOff[w] = run; run += n; }
+    sOff[kWarps] = run;
+    sBase = run ? atomicAdd(F.total, (unsigned long long)run) : 0ull;
+  }
+  __syncthreads();
+  const int n = sOff[kWarps];
+  const int64_t base = (int64_t)sBase;
+  for (int j = threadIdx.x; j < n; j += kThreads) {
+    int w = 0;
+    while (w + 1 < kWarps && sOff[w + 1] <= j) ++w;
+    const int i = w * kChunk + (j - sOff[w]);
+    const int64_t r = base + j;
+    if (r < F.cap) { R.p[r] = sP[i]; R.q[r] = sQ[i]; R.a[r] = sA[i]; R.b[r] = sB[i]; R.t[r] = sT[i]; R.k[r] = sK[w]; }
+  }
+}
+
 // per pair: record count (chunked + binned), validity
 __global__ void pair_records_kernel(const int64_t* __restrict__ chunkOff, const int64_t* __restrict__ nchunk,
                                     const int64_t* __restrict__ recScan, const int64_t* __restrict__ qScan,
                                     const int32_t* __restrict__ chunkRec, const int32_t* __restrict__ chunkQ,
                                     const int64_t* __restrict__ binRec, const int64_t* __restrict__ binQ,
                                     int64_t K, int64_t* __restrict__ nrec64, int32_t* __restrict__ nrec,
-                                    int64_t* __restrict__ count1, PairDev D) {
+                                    int64_t* __restrict__ count1, PairDev D,
+                                    const int32_t* __restrict__ pairRec, const int32_t* __restrict__ pairQ) {
   int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
   if (k >= K) return;
   int64_t c0 = chunkOff[k], n = nchunk[k];
   int64_t r = binRec[k], q = binQ[k];
-  if (n > 0) {
+  if (pairRec) {                                   // the fused pass counted per pair
+    r += pairRec[k];
+    q += pairQ[k];
+  } else if (n > 0) {
     r += recScan[c0 + n - 1] + chunkRec[c0 + n - 1] - recScan[c0];
     q += qScan[c0 + n - 1] + chunkQ[c0 + n - 1] - qScan[c0];
   }
@@ -424,14 +546,18 @@ __global__ void bin_cells_kernel(LayerDev Lb, LayerDev Lo, PairDev D, BinSet S, 
 
 // kMode 0: per binned P edge, its records (P side) into recCnt, and the pair's Q-side
 // count into binQ; kMode 1: write the records of each P edge at its offset (in cell
-// order: nothing downstream depends on record order).
+// order: nothing downstream depends on record order).  The offset is the pair's recOff
+// plus the edge's place in the pair, or, with recOff null (after the fused count + emit
+// of the chunked pairs), *recBase plus the edge's place among all binned edges; records
+// at or past cap are not written.
 template <int kMode, int kExact>
 __global__ void __launch_bounds__(kThreads, kExact ? 2 : 4)
 bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, BinSet S, int64_t np,
                  const int64_t* __restrict__ offP, const int32_t* __restrict__ LP,
                  const int64_t* __restrict__ cellOff, const int32_t* __restrict__ cellList, double eps,
                  int32_t* __restrict__ recCnt, int64_t* __restrict__ binQ,
-                 const int64_t* __restrict__ recPos, const int64_t* __restrict__ recOff, Records R) {
+                 const int64_t* __restrict__ recPos, const int64_t* __restrict__ recOff, Records R,
+                 const unsigned long long* __restrict__ recBase, int64_t cap) {
   const int64_t j = (int64_t)blockIdx.x * kThreads + threadIdx.x;
   if (j >= np) return;
   const int i = S.ownP[j];
@@ -449,7 +575,9 @@ bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, BinSet S, int64_t np,
   const int x0 = cell_1d(pminx, G.x0, G.cw, G.gx), x1 = cell_1d(pmaxx, G.x0, G.cw, G.gx);
   const int y0 = cell_1d(pminy, G.y0, G.ch, G.gy), y1 = cell_1d(pmaxy, G.y0, G.ch, G.gy);
   int recs = 0, qhits = 0;
-  const int64_t base = (kMode == 1) ? recOff[k] + recPos[j] - recPos[S.pBase[i]] : 0;
+  const int64_t base = (kMode == 0) ? 0
+                       : recOff ? recOff[k] + recPos[j] - recPos[S.pBase[i]]
+                                : (int64_t)*recBase + recPos[j];
   for (int y = y0; y <= y1; ++y)
     for (int x = x0; x <= x1; ++x) {
       const int64_t c = cb + (int64_t)y * G.gx + x;
@@ -467,7 +595,9 @@ bin_pairs_kernel(LayerDev Lb, LayerDev Lo, PairDev D, BinSet S, int64_t np,
           if (tp) ++recs;
         } else if (tp) {
           const int64_t r = base + recs++;
-          R.p[r] = p; R.q[r] = q; R.a[r] = alpha; R.b[r] = beta; R.t[r] = (int8_t)tp; R.k[r] = (int32_t)k;
+          if (r < cap) {
+            R.p[r] = p; R.q[r] = q; R.a[r] = alpha; R.b[r] = beta; R.t[r] = (int8_t)tp; R.k[r] = (int32_t)k;
+          }
         }
       }
     }
@@ -3406,16 +3536,32 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   const int nBigPairs = (int)hs[5];
   int32_t* LP = A.take_n<int32_t>(nLP);
   int32_t* LQ = A.take_n<int32_t>(nLQ);
-  int32_t* chunkRec = A.take_n<int32_t>(nCh);
+  // Count + emit in one pass (intersect_fused_kernel) unless the records are exported:
+  // the export keeps them in (pair, P edge, Q edge) order.
+  const bool fused = prm.fused_emit && !ex;
   int32_t* chunkPair = A.take_n<int32_t>(nCh);
-  int32_t* chunkQ = A.take_n<int32_t>(nCh);
-  int64_t* recScan = A.take_n<int64_t>(nCh);
-  int64_t* qScan = A.take_n<int64_t>(nCh);
-  void* stC = A.take(scan_temp_bytes(std::max<int64_t>(nCh, 1)));
+  int32_t* chunkRec = nullptr;
+  int32_t* chunkQ = nullptr;
+  int64_t* recScan = nullptr;
+  int64_t* qScan = nullptr;
+  void* stC = nullptr;
+  int32_t* pairRec = nullptr;
+  int32_t* pairQ = nullptr;
+  if (fused) {
+    pairRec = A.take_n<int32_t>(K);
+    pairQ = A.take_n<int32_t>(K);
+    if (!pairRec || !pairQ) return ST_OUT_OF_MEMORY;
+  } else {
+    chunkRec = A.take_n<int32_t>(nCh);
+    chunkQ = A.take_n<int32_t>(nCh);
+    recScan = A.take_n<int64_t>(nCh);
+    qScan = A.take_n<int64_t>(nCh);
+    stC = A.take(scan_temp_bytes(std::max<int64_t>(nCh, 1)));
+    if (!chunkRec || !chunkQ || !recScan || !qScan || !stC) return ST_OUT_OF_MEMORY;
+  }
   int64_t* binRec = A.take_n<int64_t>(K);
   int64_t* binQ = A.take_n<int64_t>(K);
-  if (!LP || !LQ || !chunkRec || !chunkPair || !chunkQ || !recScan || !qScan || !stC || !binRec || !binQ)
-    return ST_OUT_OF_MEMORY;
+  if (!LP || !LQ || !chunkPair || !binRec || !binQ) return ST_OUT_OF_MEMORY;
   if (nCh > 0) { chunk_pair_kernel<<<blocks_for_warps(K), kThreads, 0, s>>>(chunkOff, nchunk, K, chunkPair); note_launch(); }
   cudaMemsetAsync(binRec, 0, K * sizeof(int64_t), s);
   cudaMemsetAsync(binQ, 0, K * sizeof(int64_t), s);
@@ -3438,7 +3584,37 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   }
   // ---- G2 count: chunked pairs
   Records R{};
-  if (nCh > 0) {
+  unsigned long long* recTot = reinterpret_cast<unsigned long long*>(tot + 15);
+  int64_t recCap = 0;
+  auto take_records = [&](int64_t n) {
+    n = std::max<int64_t>(n, 1);
+    R.p = A.take_n<int32_t>(n); R.q = A.take_n<int32_t>(n);
+    R.a = A.take_n<double>(n); R.b = A.take_n<double>(n);
+    R.t = A.take_n<int8_t>(n); R.k = A.take_n<int32_t>(n);
+    return R.p && R.q && R.a && R.b && R.t && R.k;
+  };
+  auto launch_fused = [&](bool countPairs) {
+    if (nCh == 0) return;
+    const FusedRecords F{recTot, recCap, countPairs ? pairRec : nullptr, pairQ};
+    auto kern = prm.exact ? (prm.fused_emit == 2 ? intersect_fused_kernel<1, 1> : intersect_fused_kernel<1, 0>)
+                          : (prm.fused_emit == 2 ? intersect_fused_kernel<0, 1> : intersect_fused_kernel<0, 0>);
+    kern<<<blocks_for_warps(nCh), kThreads, 0, s>>>(Lb, Lo, D, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, R,
+                                                    chunkPair, F);
+    note_launch();
+  };
+  if (fused) {
+    // Capacity: the last clip's record count with room to spare, else a first guess,
+    // never more than one record per chunked edge pair when nothing is binned.  A clip
+    // that counts more records runs the pass again with arrays of the counted size.
+    recCap = prm.rec_hint > 0 ? prm.rec_hint + prm.rec_hint / 4 + 4096 : kFirstRecordCap;
+    if (nBigPairs == 0) recCap = std::min(recCap, std::max<int64_t>(nCh * kChunk, 1));
+    if (!take_records(recCap)) return ST_OUT_OF_MEMORY;
+    cudaMemsetAsync(recTot, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(pairRec, 0, K * sizeof(int32_t), s);
+    cudaMemsetAsync(pairQ, 0, K * sizeof(int32_t), s);
+    launch_fused(true);
+    if (sb != s) cudaEventRecord(bev[0], s);        // the binned records go after the chunked ones
+  } else if (nCh > 0) {
     { (prm.exact ? intersect_kernel<0, 1> : intersect_kernel<0, 0>)<<<blocks_for_warps(nCh), kThreads, 0, s>>>(
         Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, chunkRec, chunkQ, nullptr, nullptr, R, chunkPair); note_launch(); }
     exclusive_scan_i32(chunkRec, recScan, nCh, nullptr, stC, d_err, s);
@@ -3508,9 +3684,16 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     cudaMemsetAsync(binRecCnt + nBinP, 0, sizeof(int32_t), sb);     // so the scan's last entry is the total
     if (nBinP > 0)
       { (prm.exact ? bin_pairs_kernel<0, 1> : bin_pairs_kernel<0, 0>)<<<blocks_for(nBinP), kThreads, 0, sb>>>(
-            Lb, Lo, D, BS, nBinP, offP, LP, cellOff, cellList, prm.eps, binRecCnt, binQ, nullptr, nullptr, R); note_launch(); }
+            Lb, Lo, D, BS, nBinP, offP, LP, cellOff, cellList, prm.eps, binRecCnt, binQ, nullptr, nullptr, R, nullptr,
+            INT64_MAX); note_launch(); }
     exclusive_scan_i32(binRecCnt, binRecPos, nBinP + 1, nullptr, stP, d_err, sb);
     { bin_rec_total_kernel<<<blocks_for(B), kThreads, 0, sb>>>(BS, B, binRecPos, binRec); note_launch(); }
+    if (fused && nBinP > 0) {                       // emit now, after the chunked records
+      if (sb != s) cudaStreamWaitEvent(sb, bev[0], 0);
+      { (prm.exact ? bin_pairs_kernel<1, 1> : bin_pairs_kernel<1, 0>)<<<blocks_for(nBinP), kThreads, 0, sb>>>(
+            Lb, Lo, D, BS, nBinP, offP, LP, cellOff, cellList, prm.eps, nullptr, nullptr, binRecPos, nullptr, R,
+            recTot, recCap); note_launch(); }
+    }
   }
   if (sb != s) {
     cudaEventRecord(bev[1], sb);
@@ -3521,33 +3704,54 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   int32_t* nrec = A.take_n<int32_t>(K);
   if (!nrec64 || !recOff || !nrec) return ST_OUT_OF_MEMORY;
   { pair_records_kernel<<<blocks_for(K), kThreads, 0, s>>>(chunkOff, nchunk, recScan, qScan, chunkRec, chunkQ,
-                                                         binRec, binQ, K, nrec64, nrec, C.count1, D); note_launch(); }
-  exclusive_scan_i64(nrec64, recOff, K, tot + 5, stK, d_err, s);
-  mk->mark("clip:count", s);
-  cudaMemcpyAsync(hs, tot + 5, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-  if (!sync()) return ST_CUDA_ERROR;
-  const int64_t nR = hs[0];
-  if (nR >= (1ll << kLinkKeyShift)) return ST_OUT_OF_MEMORY;
-  // ---- G3 emit
-  R.p = A.take_n<int32_t>(nR); R.q = A.take_n<int32_t>(nR);
-  R.a = A.take_n<double>(nR); R.b = A.take_n<double>(nR);
-  R.t = A.take_n<int8_t>(nR); R.k = A.take_n<int32_t>(nR);
-  if (!R.p || !R.q || !R.a || !R.b || !R.t || !R.k) return ST_OUT_OF_MEMORY;
-  if (sb != s && nBigPairs > 0) {                   // the binned pairs' emit beside the chunked one
-    cudaEventRecord(bev[0], s);
-    cudaStreamWaitEvent(sb, bev[0], 0);
+                                                         binRec, binQ, K, nrec64, nrec, C.count1, D,
+                                                         pairRec, pairQ); note_launch(); }
+  int64_t nR = 0;
+  if (fused) {
+    mk->mark("clip:count+emit", s);
+    cudaMemcpyAsync(hs, recTot, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (nBinP > 0) cudaMemcpyAsync(hs + 1, binRecPos + nBinP, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return ST_CUDA_ERROR;
+    nR = hs[0] + (nBinP > 0 ? hs[1] : 0);
+    if (nR >= (1ll << kLinkKeyShift)) return ST_OUT_OF_MEMORY;
+    if (nR > recCap) {                              // the arrays were short: again, at the counted size
+      recCap = nR;
+      if (!take_records(recCap)) return ST_OUT_OF_MEMORY;
+      cudaMemsetAsync(recTot, 0, sizeof(unsigned long long), s);
+      launch_fused(false);
+      if (nBinP > 0)
+        { (prm.exact ? bin_pairs_kernel<1, 1> : bin_pairs_kernel<1, 0>)<<<blocks_for(nBinP), kThreads, 0, s>>>(
+              Lb, Lo, D, BS, nBinP, offP, LP, cellOff, cellList, prm.eps, nullptr, nullptr, binRecPos, nullptr, R,
+              recTot, recCap); note_launch(); }
+    }
+  } else {
+    exclusive_scan_i64(nrec64, recOff, K, tot + 5, stK, d_err, s);
+    mk->mark("clip:count", s);
+    cudaMemcpyAsync(hs, tot + 5, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return ST_CUDA_ERROR;
+    nR = hs[0];
+    if (nR >= (1ll << kLinkKeyShift)) return ST_OUT_OF_MEMORY;
+    // ---- G3 emit
+    if (!take_records(nR)) return ST_OUT_OF_MEMORY;
+    if (sb != s && nBigPairs > 0) {                 // the binned pairs' emit beside the chunked one
+      cudaEventRecord(bev[0], s);
+      cudaStreamWaitEvent(sb, bev[0], 0);
+    }
+    if (nCh > 0)
+      { (prm.exact ? intersect_kernel<1, 1> : intersect_kernel<1, 0>)<<<blocks_for_warps(nCh), kThreads, 0, s>>>(
+          Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, recOff, R,
+          chunkPair); note_launch(); }
+    if (nBinP > 0)
+      { (prm.exact ? bin_pairs_kernel<1, 1> : bin_pairs_kernel<1, 0>)<<<blocks_for(nBinP), kThreads, 0, sb>>>(
+          Lb, Lo, D, BS, nBinP, offP, LP, cellOff, cellList, prm.eps, nullptr, nullptr, binRecPos, recOff, R, nullptr,
+          INT64_MAX);
+        note_launch(); }
+    if (sb != s && nBigPairs > 0) {
+      cudaEventRecord(bev[1], sb);
+      cudaStreamWaitEvent(s, bev[1], 0);
+    }
+    mk->mark("clip:emit", s);
   }
-  if (nCh > 0)
-    { (prm.exact ? intersect_kernel<1, 1> : intersect_kernel<1, 0>)<<<blocks_for_warps(nCh), kThreads, 0, s>>>(
-        Lb, Lo, D, K, chunkOff, nCh, cP, cQ, offP, offQ, LP, LQ, prm.eps, nullptr, nullptr, recScan, recOff, R, chunkPair); note_launch(); }
-  if (nBinP > 0)
-    { (prm.exact ? bin_pairs_kernel<1, 1> : bin_pairs_kernel<1, 0>)<<<blocks_for(nBinP), kThreads, 0, sb>>>(
-        Lb, Lo, D, BS, nBinP, offP, LP, cellOff, cellList, prm.eps, nullptr, nullptr, binRecPos, recOff, R); note_launch(); }
-  if (sb != s && nBigPairs > 0) {
-    cudaEventRecord(bev[1], sb);
-    cudaStreamWaitEvent(s, bev[1], 0);
-  }
-  mk->mark("clip:emit", s);
   if (ex && ex->records_only) {
     ex->n_records = nR;
     ex->rec_p = R.p; ex->rec_q = R.q; ex->rec_a = R.a; ex->rec_b = R.b; ex->rec_t = R.t; ex->rec_k = R.k;

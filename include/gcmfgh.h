@@ -150,6 +150,15 @@ const char* gcmfgh_status_string(gcmfgh_status s);
  * edge prefilter costs 0.24 ms (most edges pass it and are tested twice).  Bit 1 needs
  * the layers' n_vertices. */
 #define GCMFGH_TUNE_F32_FILTER 5
+/* GCMFGH_TUNE_FUSED_EMIT: 1 (default) classifies the candidate edge pairs once and writes
+ * the intersection records in the same pass (the reference counts with
+ * gpuCountIntersections, gppolyclip_mDIV512.cu:1389-1420, and classifies again to write,
+ * :1567); 0 runs a count pass and an emit pass.  The results are the same. */
+#define GCMFGH_TUNE_FUSED_EMIT 6
+/* GCMFGH_TUNE_RECORD_HINT: intersection records the next clips should expect (the fused
+ * pass sizes its record arrays from it and runs again, at the counted size, when a clip
+ * finds more).  0 (default): the last clip's count. */
+#define GCMFGH_TUNE_RECORD_HINT 7
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* ctx, int key, int64_t value);
 
 /* ---- autotuner of the work-distribution thresholds.  No counterpart in the reference
