@@ -2511,6 +2511,10 @@ struct LabelArgs {
   const unsigned long long* midCount;
   unsigned long long* midNext; // work-stealing cursor of the block kernel
   int blockRunCap;            // runs the block kernel's shared run table holds (0: none)
+  // The one-thread and warp pairs in size order, largest first (label_order_kernel): the
+  // one-thread kernel takes order[0, nTile), the warp kernel order[nTile, nTile + nWarp).
+  const uint32_t* order;
+  int64_t nTile, nWarp;
 };
 
 // One pair labelled and traced by group g.  The group phases give the sequential result
@@ -2596,30 +2600,47 @@ __device__ void label_trace_pair(const G& g, const LabelArgs& a, int64_t k) {
 template <int EX, int kWide>
 __global__ void __launch_bounds__(128, (kWide && !EX) ? 6 : 4)
 label_trace_kernel(LabelArgs a) {
-  int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (k >= a.K) return;
-  if (a.D.status[k] != 0) return;
-  const int64_t slots = (int64_t)a.mP[k] + a.mQ[k];
-  if (slots > a.midLabelMin) return;                       // block or grid path
-  if (slots <= a.tileLabelMax) return;                     // tile path
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= a.nWarp) return;
   WarpGroup g;
-  label_trace_pair<EX>(g, a, k);
+  label_trace_pair<EX>(g, a, (int64_t)a.order[a.nTile + w]);
 }
 
-// Pairs whose merged rings have at most tileLabelMax slots: a tile of kTileLanes lanes per
-// pair, 32 / kTileLanes consecutive pairs per warp (one lane: SoloGroup, measured slightly
-// faster than 2-lane tiles on the batched workload).
-constexpr int kTileLanes = 1;
+// Pairs whose merged rings have at most tileLabelMax slots: one thread per pair
+// (SoloGroup, measured slightly faster than 2-lane tiles on the batched workload), the
+// pairs in size order so that the 32 pairs of a warp take about as long as each other.
 template <int EX, int kWide>
 __global__ void __launch_bounds__(128, (kWide && !EX) ? 12 : 4)
 label_trace_tile_kernel(LabelArgs a) {
-  const int64_t k = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / kTileLanes) +
-                    (lane_id() / kTileLanes);
-  if (k >= a.K || a.D.status[k] != 0) return;
-  const int64_t slots = (int64_t)a.mP[k] + a.mQ[k];
-  if (slots > a.tileLabelMax || slots > a.midLabelMin) return;
-  typename TileOf<kTileLanes>::type g;
-  label_trace_pair<EX>(g, a, k);
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nTile) return;
+  SoloGroup g;
+  label_trace_pair<EX>(g, a, (int64_t)a.order[i]);
+}
+
+// Sort keys of the one-thread and warp pairs: each class in 127 size buckets, largest
+// first (one-thread pairs 0..126, warp pairs 128..254, the rest 255), for one 8-bit
+// radix pass; the counts of the two classes go to cnt[0], cnt[1].
+__global__ void label_order_kernel(const int32_t* __restrict__ mP, const int32_t* __restrict__ mQ,
+                                   const int32_t* __restrict__ status, int64_t K, int64_t tileMax, int64_t midMin,
+                                   uint64_t* __restrict__ key, uint32_t* __restrict__ val,
+                                   unsigned long long* __restrict__ cnt) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  const int64_t slots = (int64_t)mP[k] + mQ[k];
+  const int64_t tl = tileMax < midMin ? tileMax : midMin;
+  uint64_t kk = 255;
+  if (status[k] == 0 && slots <= midMin) {
+    if (slots <= tl) {
+      kk = 126 - (uint64_t)((slots * 127) / (tl + 1));
+      atomicAdd(cnt, 1ull);
+    } else {
+      kk = 254 - (uint64_t)(((slots - tl) * 127) / (midMin - tl + 1));
+      atomicAdd(cnt + 1, 1ull);
+    }
+  }
+  key[k] = kk;
+  val[k] = (uint32_t)k;
 }
 
 // Pairs with midLabelMin < slots <= bigLabelMin: persistent blocks take pairs from the
@@ -3954,20 +3975,30 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   { out_sizes_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, nrec, D.status, K, vcap, ccap); note_launch(); }
   exclusive_scan_i64(vcap, vOff, K, tot + 13, stK, d_err, s);
   exclusive_scan_i32(ccap, cOff, K, tot + 14, stK, d_err, s);
-  // the pairs for the block kernel (their count is read with the output sizes)
+  // the pairs for the block kernel, and the one-thread and warp pairs in size order (their
+  // counts are read with the output sizes)
   int64_t* mlist = A.take_n<int64_t>(K);
-  unsigned long long* mcnt = A.take_n<unsigned long long>(2);
-  if (!mlist || !mcnt) return ST_OUT_OF_MEMORY;
-  cudaMemsetAsync(mcnt, 0, 2 * sizeof(unsigned long long), s);
+  unsigned long long* mcnt = A.take_n<unsigned long long>(4);
+  uint64_t* okey = A.take_n<uint64_t>(K);
+  uint32_t* oval = A.take_n<uint32_t>(K);
+  uint64_t* okeyAlt = A.take_n<uint64_t>(K);
+  uint32_t* ovalAlt = A.take_n<uint32_t>(K);
+  void* otmp = A.take(radix_temp_bytes(K));
+  if (!mlist || !mcnt || !okey || !oval || !okeyAlt || !ovalAlt || !otmp) return ST_OUT_OF_MEMORY;
+  cudaMemsetAsync(mcnt, 0, 4 * sizeof(unsigned long long), s);
   const int64_t midMin = std::min(prm.mid_label_min, prm.big_label_min);
   { mid_label_list_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, D.status, K, midMin, prm.big_label_min,
                                                             mlist, mcnt); note_launch(); }
+  { label_order_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, D.status, K, std::max<int64_t>(prm.tile_label_max, 0),
+                                                         midMin, okey, oval, mcnt + 2); note_launch(); }
+  radix_sort_pairs(okey, oval, okeyAlt, ovalAlt, K, 8, otmp, d_err, s);
   cudaMemcpyAsync(hs, tot + 13, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hs + 2, mcnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hs + 3, mcnt + 2, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
   double* oxy = A.take_n<double>(2 * hs[0]);
   int32_t* ocsz = A.take_n<int32_t>(hs[1]);
-  const int64_t nMid = hs[2];
+  const int64_t nMid = hs[2], nTile = hs[3], nWarp = hs[4];
   if (!oxy || !ocsz) return ST_OUT_OF_MEMORY;
   mk->mark("clip:fill+link", s);
   {
@@ -3977,7 +4008,8 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     LabelArgs la{D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ, SP, SQ, oxy, vOff, vcap, ocsz, cOff, ccap, nc, nv,
-                 prm, d_err, prm.tile_label_max, midMin, prm.big_label_min, mlist, mcnt, mcnt + 1};
+                 prm, d_err, prm.tile_label_max, midMin, prm.big_label_min, mlist, mcnt, mcnt + 1, 0, oval,
+                 nTile, nWarp};
     // long pairs: a block each, on the auxiliary stream when there is one, so they start
     // first and overlap the warp-per-pair kernel instead of trailing it
     cudaStream_t ls = s;
@@ -4009,13 +4041,12 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
       cudaStreamWaitEvent(aux2, wfork, 0);
       ws = aux2;
     }
-    { (prm.exact ? label_trace_kernel<1, 0>
-                 : (wide ? label_trace_kernel<0, 1> : label_trace_kernel<0, 0>))<<<(unsigned)((K + 3) / 4), 128, 0, ws>>>(la); note_launch(); }
-    if (prm.tile_label_max > 0) {
-      const int64_t pairsPerBlock = 4 * (32 / kTileLanes);
+    if (nWarp > 0)
+      { (prm.exact ? label_trace_kernel<1, 0>
+                   : (wide ? label_trace_kernel<0, 1> : label_trace_kernel<0, 0>))<<<(unsigned)((nWarp + 3) / 4), 128, 0, ws>>>(la); note_launch(); }
+    if (nTile > 0)
       { (prm.exact ? label_trace_tile_kernel<1, 0>
-                   : (wide ? label_trace_tile_kernel<0, 1> : label_trace_tile_kernel<0, 0>))<<<(unsigned)((K + pairsPerBlock - 1) / pairsPerBlock), 128, 0, s>>>(la); note_launch(); }
-    }
+                   : (wide ? label_trace_tile_kernel<0, 1> : label_trace_tile_kernel<0, 0>))<<<(unsigned)((nTile + 127) / 128), 128, 0, s>>>(la); note_launch(); }
     if (ws != s) {
       cudaEventRecord(wjoin, ws);
       cudaStreamWaitEvent(s, wjoin, 0);
