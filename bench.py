@@ -56,6 +56,7 @@ def parse():
                     help="compare every degenerate pair (not a sample) with the oracle")
     ap.add_argument("--no-precision", action="store_true", help="skip the degeneracy batch")
     ap.add_argument("--no-large-pair", action="store_true", help="skip the single large pair")
+    ap.add_argument("--no-multi", action="store_true", help="skip the multi-component pairs")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default size-bucket thresholds")
     ap.add_argument("--fused-emit", type=int, default=None,
                     help="0: count, then emit the intersection records; 1: one pass, block-wide "
@@ -364,6 +365,40 @@ def plain_measure(eng, db, do, stream, n=2000, seed=9):
 
 
 # ----------------------------------------------------------------------------- single large pair
+
+def multi_measure(local, n=5000, single=300, seed=41):
+    """Multi-component pairs (islands with 0-3 holes, 5-200 vertices per ring, seeded):
+    n pairs through one gh_clip_multi_batch call, against `single` of them through one
+    gh_clip_multi call each.  Host arrays in, results on the device; wall clock around
+    synchronised calls."""
+    import torch
+    import gcmfgh
+    from gcmfgh import synth
+    pairs = synth.holed_pairs(seed, n, 5, 200)
+    eng = gcmfgh.Engine(local)
+    try:
+        eng.clip_multi_batch(pairs[:100])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info = eng.clip_multi_batch(pairs)
+        torch.cuda.synchronize()
+        tb = time.perf_counter() - t0
+        for P, Q in pairs[:10]:
+            eng.clip_multi(P, Q)
+        t0 = time.perf_counter()
+        for P, Q in pairs[:single]:
+            eng.clip_multi(P, Q)
+        torch.cuda.synchronize()
+        ts = time.perf_counter() - t0
+    finally:
+        eng.close()
+    rings = sum(len(P) + len(Q) for P, Q in pairs)
+    return {"workload": f"{n} seeded pairs of islands with holes (holed_pairs seed {seed}, 5-200 vertices "
+                        f"per ring, {rings} rings), P and Q as given",
+            "batch_pairs_per_s": n / tb, "batch_ms": tb * 1e3, "records": info["n_records"],
+            "components_out": info["n_components"],
+            "single_call_pairs_per_s": single / ts, "batch_over_single": (n / tb) / (single / ts)}
+
 
 def large_pair_measure(local, nP=1_000_000, nQ=500_000, reps=2, cpu_div=64):
     """The single large pair (star of nP vertices, radius U(0.8,1.2), at the origin, clipped
@@ -730,6 +765,8 @@ def run_ours(args, rank, world, local):
             line["serving"] = serve_measure(local)
         if not args.no_large_pair:
             line["large_pair"] = large_pair_measure(local)
+        if not args.no_multi:
+            line["multi_component"] = multi_measure(local)
         if not args.no_precision:
             line["precision"] = precision_measure(local, total=args.precision_pairs, chunk=args.precision_chunk,
                                                   check_all_degenerate=args.precision_check_all)

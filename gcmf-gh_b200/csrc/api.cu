@@ -784,6 +784,23 @@ gcmfgh_status gh_clip_multi(gcmfgh_ctx* c, const double* P, const int32_t* p_siz
   return clip_info(c, info);
 }
 
+gcmfgh_status gh_clip_multi_batch(gcmfgh_ctx* c, int64_t n, const double* P, const int32_t* p_sizes,
+                                  const int32_t* p_rings, const double* Q, const int32_t* q_sizes,
+                                  const int32_t* q_rings, gcmfgh_clip_info* info) {
+  if (!c || n < 1 || !P || !Q || !p_sizes || !q_sizes || !p_rings || !q_rings) return GCMFGH_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->clip_arena.reset();
+  c->have_clip = false;
+  c->marks[1].n = 0;
+  cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  int st = run_clip_multi_batch(n, P, p_sizes, p_rings, Q, q_sizes, q_rings, c->prm, c->clip_arena, c->clip,
+                                c->d_err, c->h_scratch, c->stream);
+  gcmfgh_status r = finish(c, st);
+  if (r != GCMFGH_OK) return r;
+  c->have_clip = true;
+  return clip_info(c, info);
+}
+
 gcmfgh_status gh_calculate_intersections(gcmfgh_ctx* c, const gcmfgh_layer* pl, int32_t p_id,
                                          const gcmfgh_layer* ql, int32_t q_id, gcmfgh_intersections* out) {
   if (!out) return GCMFGH_INVALID_ARGUMENT;

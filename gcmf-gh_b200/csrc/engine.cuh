@@ -172,6 +172,12 @@ int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, co
 int run_clip_multi(const double* P, const int32_t* sizesP, int kP, const double* Q, const int32_t* sizesQ, int kQ,
                    const ClipParams& prm, Arena& arena, ClipDev& out, int* d_err, int64_t* h_scratch,
                    cudaStream_t s);
+// n pairs of multi-component polygons in one batch: pair i's P has ringsP[i] rings, taken
+// in order from sizesP / P (all pairs' rings one after the other), and the same for Q.
+// Results as n pairs of ClipDev (one thread per pair runs the phases after the records).
+int run_clip_multi_batch(int64_t n, const double* P, const int32_t* sizesP, const int32_t* ringsP,
+                         const double* Q, const int32_t* sizesQ, const int32_t* ringsQ, const ClipParams& prm,
+                         Arena& arena, ClipDev& out, int* d_err, int64_t* h_scratch, cudaStream_t s);
 
 // a non-blocking stream at the device's highest priority (nullptr on failure)
 cudaStream_t create_priority_stream();

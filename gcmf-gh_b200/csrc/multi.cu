@@ -43,8 +43,8 @@ struct MultiArgs {
   int kP, kQ;
   // intersection records of the ring pairs (pair k = i * kQ + j)
   const int32_t* rp; const int32_t* rq; const double* ra; const double* rb; const int8_t* rt;
-  const int32_t* rk;
-  int64_t nR;
+  const int32_t* rk;                         // ring pair of each record (absolute; k0 is this pair's first)
+  int64_t nR, k0;
   const int32_t* pairStatus; int64_t nPairs;
   // work arrays
   int32_t* cntP; int32_t* cntQ;              // per global edge (+1): insertion counts, then offsets
@@ -65,6 +65,9 @@ struct MultiArgs {
   double epsClean; int uni; int exact;
   int* err;
 };
+
+// the record's ring pair within this polygon pair, i * kQ + j
+__device__ __forceinline__ int m_k(const MultiArgs& a, int64_t r) { return (int)(a.rk[r] - a.k0); }
 
 __device__ int m_add(MRing& R, double X, double Y) {
   if (R.used >= R.cap) return -1;
@@ -231,13 +234,12 @@ __device__ void m_fail(const MultiArgs& a, int code) {
 
 // record order key for ties: (other component, other edge), larger = inserted later
 __device__ __forceinline__ long long m_other_key(const MultiArgs& a, int64_t r, int side) {
-  const int k = a.rk[r];
+  const int k = m_k(a, r);
   return side == 0 ? ((long long)(k % a.kQ) << 32) | (uint32_t)a.rq[r]
                    : ((long long)(k / a.kQ) << 32) | (uint32_t)a.rp[r];
 }
 
-__global__ void multi_clip_kernel(MultiArgs a) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+__device__ void multi_clip_pair(MultiArgs& a) {
   *a.outNC = 0;
   *a.outNV = 0;
   *a.status = 0;
@@ -251,7 +253,7 @@ __global__ void multi_clip_kernel(MultiArgs a) {
   for (int64_t e = 0; e <= EP; ++e) a.cntP[e] = 0;
   for (int64_t e = 0; e <= EQ; ++e) a.cntQ[e] = 0;
   for (int64_t r = 0; r < a.nR; ++r) {
-    const int t = a.rt[r], k = a.rk[r], i = k / a.kQ, j = k % a.kQ;
+    const int t = a.rt[r], k = m_k(a, r), i = k / a.kQ, j = k % a.kQ;
     a.insP[r] = a.insQ[r] = -1;
     if (t == 1 || t == 3 || t == 5 || t == 7) a.cntP[a.edgeP[i] + a.rp[r] + 1]++;
     if (t == 1 || t == 2 || t == 5 || t == 6) a.cntQ[a.edgeQ[j] + a.rq[r] + 1]++;
@@ -259,7 +261,7 @@ __global__ void multi_clip_kernel(MultiArgs a) {
   for (int64_t e = 0; e < EP; ++e) a.cntP[e + 1] += a.cntP[e];
   for (int64_t e = 0; e < EQ; ++e) a.cntQ[e + 1] += a.cntQ[e];
   for (int64_t r = 0; r < a.nR; ++r) {                          // counts become cursors
-    const int t = a.rt[r], k = a.rk[r], i = k / a.kQ, j = k % a.kQ;
+    const int t = a.rt[r], k = m_k(a, r), i = k / a.kQ, j = k % a.kQ;
     if (t == 1 || t == 3 || t == 5 || t == 7) a.lstP[a.cntP[a.edgeP[i] + a.rp[r]]++] = (int32_t)r;
     if (t == 1 || t == 2 || t == 5 || t == 6) a.lstQ[a.cntQ[a.edgeQ[j] + a.rq[r]]++] = (int32_t)r;
   }
@@ -313,7 +315,7 @@ __global__ void multi_clip_kernel(MultiArgs a) {
               X = (1.0 - a.ra[r]) * A.x + a.ra[r] * P2.x;
               Y = (1.0 - a.ra[r]) * A.y + a.ra[r] * P2.y;
             } else {                                             // a copy of Q1
-              const int j = a.rk[r] % a.kQ;
+              const int j = m_k(a, r) % a.kQ;
               const double2 Q1 = a.Q[a.startQ[j] + a.rq[r]];
               X = Q1.x; Y = Q1.y;
             }
@@ -321,7 +323,7 @@ __global__ void multi_clip_kernel(MultiArgs a) {
             if (a.rt[r] == 1) {                                  // the P-side point
               X = RP.x[a.insP[r]]; Y = RP.y[a.insP[r]];
             } else {                                             // a copy of P1
-              const int i = a.rk[r] / a.kQ;
+              const int i = m_k(a, r) / a.kQ;
               const double2 P1 = a.P[a.startP[i] + a.rp[r]];
               X = P1.x; Y = P1.y;
             }
@@ -340,7 +342,7 @@ __global__ void multi_clip_kernel(MultiArgs a) {
   for (int64_t e = 0; e < EP; ++e) a.winP[e] = -1;
   for (int64_t e = 0; e < EQ; ++e) a.winQ[e] = -1;
   for (int64_t r = 0; r < a.nR; ++r) {
-    const int t = a.rt[r], k = a.rk[r], i = k / a.kQ, j = k % a.kQ;
+    const int t = a.rt[r], k = m_k(a, r), i = k / a.kQ, j = k % a.kQ;
     const long long kp = m_other_key(a, r, 0), kq = m_other_key(a, r, 1);
     if (t == 2 || t == 4 || t == 5 || t == 6 || t == 8) {
       long long& w = a.winP[a.edgeP[i] + a.rp[r]];
@@ -352,7 +354,7 @@ __global__ void multi_clip_kernel(MultiArgs a) {
     }
   }
   for (int64_t r = 0; r < a.nR; ++r) {
-    const int t = a.rt[r], k = a.rk[r], i = k / a.kQ, j = k % a.kQ;
+    const int t = a.rt[r], k = m_k(a, r), i = k / a.kQ, j = k % a.kQ;
     const int64_t eP = a.edgeP[i] + a.rp[r], eQ = a.edgeQ[j] + a.rq[r];
     const int sp = a.srcP[eP], sq = a.srcQ[eQ];
     const bool wP = a.winP[eP] == m_other_key(a, r, 0), wQ = a.winQ[eQ] == m_other_key(a, r, 1);
@@ -593,75 +595,157 @@ __global__ void multi_clip_kernel(MultiArgs a) {
   *a.outNV = w;
 }
 
+// Where one polygon pair's data sits in the batch's arrays.
+struct MultiPairDesc {
+  int32_t kP, kQ;          // components
+  int64_t cP0, cQ0;        // first component (start, size, root and flag arrays)
+  int64_t k0;              // first ring pair (pair status; the records' ring pair index)
+  int64_t r0, nR;          // records
+  int64_t eP0, eQ0;        // first edge (source slots, links; the count arrays at eP0 + pair)
+  int64_t sP0, sQ0;        // first ring slot
+  int32_t capP, capQ;      // ring slots
+  int64_t v0, vcap;        // result vertices
+  int64_t c0;              // result components
+  int32_t ccap, pad;
+};
+
+// One thread per polygon pair: the sequential phases are a chain of dependent steps over
+// linked lists, so the batch's parallelism is across pairs (as the batched clip's
+// one-thread labelling kernel has it for small ring pairs).
+__global__ void __launch_bounds__(32) multi_clip_batch_kernel(MultiArgs b, const MultiPairDesc* __restrict__ desc,
+                                                               int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const MultiPairDesc d = desc[i];
+  MultiArgs a = b;
+  a.startP = b.startP + d.cP0; a.startQ = b.startQ + d.cQ0;
+  a.sizeP = b.sizeP + d.cP0; a.sizeQ = b.sizeQ + d.cQ0;
+  a.edgeP = b.edgeP + d.cP0 + i; a.edgeQ = b.edgeQ + d.cQ0 + i;
+  a.kP = d.kP; a.kQ = d.kQ;
+  a.rp = b.rp + d.r0; a.rq = b.rq + d.r0; a.ra = b.ra + d.r0; a.rb = b.rb + d.r0; a.rt = b.rt + d.r0;
+  a.rk = b.rk + d.r0;
+  a.nR = d.nR; a.k0 = d.k0;
+  a.pairStatus = b.pairStatus + d.k0; a.nPairs = (int64_t)d.kP * d.kQ;
+  a.cntP = b.cntP + d.eP0 + i; a.cntQ = b.cntQ + d.eQ0 + i;
+  a.lstP = b.lstP + d.r0; a.lstQ = b.lstQ + d.r0;
+  a.srcP = b.srcP + d.eP0; a.srcQ = b.srcQ + d.eQ0;
+  a.insP = b.insP + d.r0; a.insQ = b.insQ + d.r0;
+  a.winP = b.winP + d.eP0; a.winQ = b.winQ + d.eQ0;
+  for (int sd = 0; sd < 2; ++sd) {
+    MRing& R = a.R[sd];
+    const int64_t o = sd == 0 ? d.sP0 : d.sQ0;
+    R.x += o; R.y += o; R.nx += o; R.pv += o; R.nb += o; R.it += o; R.lb += o; R.ee += o;
+    R.used = 0;
+    R.cap = sd == 0 ? d.capP : d.capQ;
+    const int64_t c0 = sd == 0 ? d.cP0 : d.cQ0;
+    a.root[sd] = b.root[sd] + c0; a.noInter[sd] = b.noInter[sd] + c0; a.ident[sd] = b.ident[sd] + c0;
+    a.split[sd] = b.split[sd] + o; a.cand[sd] = b.cand[sd] + o;
+  }
+  a.mark = b.mark + d.sQ0;
+  a.oxy = b.oxy + 2 * d.v0; a.vcap = d.vcap; a.ocs = b.ocs + d.c0; a.ccap = d.ccap;
+  a.onx = b.onx + d.v0; a.opv = b.opv + d.v0; a.otmp = b.otmp + 2 * d.v0;
+  a.status = b.status + i; a.outNC = b.outNC + i; a.outNV = b.outNV + i;
+  multi_clip_pair(a);
+}
+
+// per-pair result regions -> one contiguous result (a warp per pair)
+__global__ void multi_compact_kernel(const MultiPairDesc* __restrict__ desc, int64_t n,
+                                     const int32_t* __restrict__ ocs, const double* __restrict__ oxy,
+                                     const int32_t* __restrict__ nc, const int64_t* __restrict__ nv,
+                                     const int64_t* __restrict__ compOff, const int64_t* __restrict__ vertOff,
+                                     int32_t* __restrict__ csz, double* __restrict__ xy) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= n) return;
+  const int64_t c0 = desc[i].c0, v0 = desc[i].v0;
+  for (int64_t j = lane_id(); j < nc[i]; j += 32) csz[compOff[i] + j] = ocs[c0 + j];
+  for (int64_t j = lane_id(); j < 2 * nv[i]; j += 32) xy[2 * vertOff[i] + j] = oxy[2 * v0 + j];
+}
+
 }  // namespace
 
-int run_clip_multi(const double* hP, const int32_t* sizesP, int kP, const double* hQ, const int32_t* sizesQ, int kQ,
-                   const ClipParams& prm, Arena& A, ClipDev& C, int* d_err, int64_t* hs, cudaStream_t s) {
+int run_clip_multi_batch(int64_t n, const double* hP, const int32_t* sizesP, const int32_t* ringsP,
+                         const double* hQ, const int32_t* sizesQ, const int32_t* ringsQ, const ClipParams& prm,
+                         Arena& A, ClipDev& C, int* d_err, int64_t* hs, cudaStream_t s) {
   C = ClipDev();
-  if (kP <= 0 || kQ <= 0) return ST_INVALID_ARGUMENT;
+  if (n <= 0 || !hP || !hQ || !sizesP || !sizesQ || !ringsP || !ringsQ) return ST_INVALID_ARGUMENT;
   auto sync = [&]() { return cudaStreamSynchronize(s) == cudaSuccess; };
-  // ---- the rings as two layers (closing vertex stored), ring-pair list i * kQ + j
-  int64_t ve[2] = {0, 0}, ee[2] = {0, 0};
-  const int k2[2] = {kP, kQ};
+  // ---- every ring of every pair as two layers (closing vertex stored); ring pairs of
+  // pair i are (P ring c, Q ring d) for its c, d, numbered i's k0 + c * kQ + d
+  const int32_t* rings[2] = {ringsP, ringsQ};
   const int32_t* sz[2] = {sizesP, sizesQ};
-  for (int sd = 0; sd < 2; ++sd)
-    for (int c = 0; c < k2[sd]; ++c) {
-      if (sz[sd][c] < 3) return ST_INVALID_ARGUMENT;
-      ve[sd] += sz[sd][c] + 1;
-      ee[sd] += sz[sd][c];
-    }
+  const double* src[2] = {hP, hQ};
+  std::vector<int64_t> c0[2], e0[2], ne[2];
   std::vector<double> hxy[2];
   std::vector<int32_t> hvn[2];
   std::vector<int64_t> hvp[2], hstart[2], hedge[2];
-  const double* src[2] = {hP, hQ};
+  int64_t nring[2] = {0, 0};
   for (int sd = 0; sd < 2; ++sd) {
-    hxy[sd].reserve(2 * ve[sd]);
-    int64_t o = 0, v = 0, e = 0;
-    for (int c = 0; c < k2[sd]; ++c) {
-      const int n = sz[sd][c];
-      hstart[sd].push_back(v);
-      hedge[sd].push_back(e);
-      hxy[sd].insert(hxy[sd].end(), src[sd] + 2 * o, src[sd] + 2 * (o + n));
-      hxy[sd].push_back(src[sd][2 * o]);
-      hxy[sd].push_back(src[sd][2 * o + 1]);
-      o += n;
-      v += n + 1;
-      e += n;
-      hvn[sd].push_back(n + 1);
-      hvp[sd].push_back(v);
+    c0[sd].resize(n); e0[sd].resize(n); ne[sd].resize(n);
+    int64_t ring = 0, o = 0, v = 0, e = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      if (rings[sd][i] < 1) return ST_INVALID_ARGUMENT;
+      c0[sd][i] = ring;
+      e0[sd][i] = e;
+      int64_t le = 0;
+      for (int c = 0; c < rings[sd][i]; ++c, ++ring) {
+        const int m = sz[sd][ring];
+        if (m < 3) return ST_INVALID_ARGUMENT;
+        hstart[sd].push_back(v);
+        hedge[sd].push_back(le);
+        hxy[sd].insert(hxy[sd].end(), src[sd] + 2 * o, src[sd] + 2 * (o + m));
+        hxy[sd].push_back(src[sd][2 * o]);
+        hxy[sd].push_back(src[sd][2 * o + 1]);
+        o += m;
+        v += m + 1;
+        le += m;
+        hvn[sd].push_back(m + 1);
+        hvp[sd].push_back(v);
+      }
+      hedge[sd].push_back(le);            // pair i's local edge offsets: rings + 1 entries
+      ne[sd][i] = le;
+      e += le;
     }
-    hedge[sd].push_back(e);
+    nring[sd] = ring;
+    if (ring > INT32_MAX) return ST_INVALID_ARGUMENT;
   }
-  const int64_t K = (int64_t)kP * kQ;
+  std::vector<int64_t> k0(n + 1);
+  k0[0] = 0;
+  for (int64_t i = 0; i < n; ++i) k0[i + 1] = k0[i] + (int64_t)ringsP[i] * ringsQ[i];
+  const int64_t K = k0[n];
   std::vector<int32_t> hpid(K), hqid(K);
-  for (int64_t k = 0; k < K; ++k) { hpid[k] = (int32_t)(k / kQ); hqid[k] = (int32_t)(k % kQ); }
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t k = 0; k < k0[i + 1] - k0[i]; ++k) {
+      hpid[k0[i] + k] = (int32_t)(c0[0][i] + k / ringsQ[i]);
+      hqid[k0[i] + k] = (int32_t)(c0[1][i] + k % ringsQ[i]);
+    }
   double* dxy[2];
   int32_t* dvn[2];
   int64_t *dvp[2], *dstart[2], *dedge[2];
+  int32_t* dsz[2];
   for (int sd = 0; sd < 2; ++sd) {
-    dxy[sd] = A.take_n<double>(2 * ve[sd]);
-    dvn[sd] = A.take_n<int32_t>(k2[sd]);
-    dvp[sd] = A.take_n<int64_t>(k2[sd]);
-    dstart[sd] = A.take_n<int64_t>(k2[sd]);
-    dedge[sd] = A.take_n<int64_t>(k2[sd] + 1);
-    if (!dxy[sd] || !dvn[sd] || !dvp[sd] || !dstart[sd] || !dedge[sd]) return ST_OUT_OF_MEMORY;
-    cudaMemcpyAsync(dxy[sd], hxy[sd].data(), 2 * ve[sd] * sizeof(double), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dvn[sd], hvn[sd].data(), k2[sd] * sizeof(int32_t), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dvp[sd], hvp[sd].data(), k2[sd] * sizeof(int64_t), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dstart[sd], hstart[sd].data(), k2[sd] * sizeof(int64_t), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dedge[sd], hedge[sd].data(), (k2[sd] + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+    const int64_t nr = nring[sd];
+    dxy[sd] = A.take_n<double>(hxy[sd].size());
+    dvn[sd] = A.take_n<int32_t>(nr);
+    dvp[sd] = A.take_n<int64_t>(nr);
+    dstart[sd] = A.take_n<int64_t>(nr);
+    dedge[sd] = A.take_n<int64_t>(nr + n);
+    dsz[sd] = A.take_n<int32_t>(nr);
+    if (!dxy[sd] || !dvn[sd] || !dvp[sd] || !dstart[sd] || !dedge[sd] || !dsz[sd]) return ST_OUT_OF_MEMORY;
+    cudaMemcpyAsync(dxy[sd], hxy[sd].data(), hxy[sd].size() * sizeof(double), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dvn[sd], hvn[sd].data(), nr * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dvp[sd], hvp[sd].data(), nr * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dstart[sd], hstart[sd].data(), nr * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dedge[sd], hedge[sd].data(), (nr + n) * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dsz[sd], sz[sd], nr * sizeof(int32_t), cudaMemcpyHostToDevice, s);
   }
-  int32_t* dsz[2] = {A.take_n<int32_t>(kP), A.take_n<int32_t>(kQ)};
   int32_t* dpid = A.take_n<int32_t>(K);
   int32_t* dqid = A.take_n<int32_t>(K);
-  if (!dsz[0] || !dsz[1] || !dpid || !dqid) return ST_OUT_OF_MEMORY;
-  cudaMemcpyAsync(dsz[0], sizesP, kP * sizeof(int32_t), cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(dsz[1], sizesQ, kQ * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+  if (!dpid || !dqid) return ST_OUT_OF_MEMORY;
   cudaMemcpyAsync(dpid, hpid.data(), K * sizeof(int32_t), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(dqid, hqid.data(), K * sizeof(int32_t), cudaMemcpyHostToDevice, s);
   if (!sync()) return ST_CUDA_ERROR;                         // host staging vectors end here
-  const LayerDev LP{dxy[0], dvn[0], dvp[0], kP}, LQ{dxy[1], dvn[1], dvp[1], kQ};
-  // ---- intersection records of every ring pair (stages G0-G3)
+  const LayerDev LP{dxy[0], dvn[0], dvp[0], nring[0]}, LQ{dxy[1], dvn[1], dvp[1], nring[1]};
+  // ---- intersection records of every ring pair (stages G0-G3), in ring-pair order
   ClipParams p2 = prm;
   p2.no_swap = 1;
   RingExport ex;
@@ -669,76 +753,105 @@ int run_clip_multi(const double* hP, const int32_t* sizesP, int kP, const double
   ClipDev CR;
   int st = run_clip(LP, LQ, dpid, dqid, K, p2, A, CR, d_err, hs, s, nullptr, nullptr, &ex);
   if (st != ST_OK) return st;
-  const int64_t nR = ex.n_records;
+  const int64_t nRall = ex.n_records;
   std::vector<int64_t> c1(K);
   cudaMemcpyAsync(c1.data(), CR.count1, K * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
-  int64_t count1 = 0;
-  for (int64_t v : c1) count1 += v;
-  // ---- work arrays and result
-  const int64_t EP = hedge[0][kP], EQ = hedge[1][kQ];
-  const int64_t capP = EP + 2 * nR + kP + 8, capQ = EQ + 2 * nR + kQ + 8;
-  if (capP > INT32_MAX || capQ > INT32_MAX) return ST_OUT_OF_MEMORY;
+  // ---- each pair's place in the work arrays and result regions
+  std::vector<MultiPairDesc> hd(n);
+  std::vector<int64_t> hcount1(n);
+  int64_t r = 0, sP = 0, sQ = 0, vo = 0, co = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    MultiPairDesc& d = hd[i];
+    int64_t nR = 0;
+    for (int64_t k = k0[i]; k < k0[i + 1]; ++k) nR += c1[k];
+    const int64_t capP = ne[0][i] + 2 * nR + ringsP[i] + 8, capQ = ne[1][i] + 2 * nR + ringsQ[i] + 8;
+    if (capP > INT32_MAX || capQ > INT32_MAX) return ST_OUT_OF_MEMORY;
+    d.kP = ringsP[i]; d.kQ = ringsQ[i];
+    d.cP0 = c0[0][i]; d.cQ0 = c0[1][i];
+    d.k0 = k0[i];
+    d.r0 = r; d.nR = nR;
+    d.eP0 = e0[0][i]; d.eQ0 = e0[1][i];
+    d.sP0 = sP; d.sQ0 = sQ; d.capP = (int32_t)capP; d.capQ = (int32_t)capQ;
+    d.v0 = vo; d.vcap = 2 * (capP + capQ) + 16;
+    d.c0 = co; d.ccap = (int32_t)std::min<int64_t>(2 * nR + ringsP[i] + ringsQ[i] + 16, INT32_MAX); d.pad = 0;
+    hcount1[i] = nR;
+    r += nR; sP += capP; sQ += capQ; vo += d.vcap; co += d.ccap;
+  }
+  if (r != nRall) return ST_CUDA_ERROR;                    // records are in ring-pair order
+  const int64_t EP = e0[0][n - 1] + ne[0][n - 1], EQ = e0[1][n - 1] + ne[1][n - 1];
   MultiArgs a{};
   a.P = reinterpret_cast<const double2*>(dxy[0]); a.Q = reinterpret_cast<const double2*>(dxy[1]);
   a.startP = dstart[0]; a.startQ = dstart[1]; a.sizeP = dsz[0]; a.sizeQ = dsz[1];
-  a.edgeP = dedge[0]; a.edgeQ = dedge[1]; a.kP = kP; a.kQ = kQ;
+  a.edgeP = dedge[0]; a.edgeQ = dedge[1];
   a.rp = ex.rec_p; a.rq = ex.rec_q; a.ra = ex.rec_a; a.rb = ex.rec_b; a.rt = ex.rec_t; a.rk = ex.rec_k;
-  a.nR = nR; a.pairStatus = CR.status; a.nPairs = K;
-  const int64_t nR1 = std::max<int64_t>(nR, 1);
-  a.cntP = A.take_n<int32_t>(EP + 1); a.cntQ = A.take_n<int32_t>(EQ + 1);
+  a.pairStatus = CR.status;
+  const int64_t nR1 = std::max<int64_t>(nRall, 1);
+  a.cntP = A.take_n<int32_t>(EP + n); a.cntQ = A.take_n<int32_t>(EQ + n);
   a.lstP = A.take_n<int32_t>(nR1); a.lstQ = A.take_n<int32_t>(nR1);
   a.srcP = A.take_n<int32_t>(EP); a.srcQ = A.take_n<int32_t>(EQ);
   a.insP = A.take_n<int32_t>(nR1); a.insQ = A.take_n<int32_t>(nR1);
   a.winP = A.take_n<long long>(EP); a.winQ = A.take_n<long long>(EQ);
   bool ok = a.cntP && a.cntQ && a.lstP && a.lstQ && a.srcP && a.srcQ && a.insP && a.insQ && a.winP && a.winQ;
-  const int64_t cap[2] = {capP, capQ};
+  const int64_t cap[2] = {sP, sQ};
   for (int sd = 0; sd < 2; ++sd) {
     MRing& R = a.R[sd];
     R.x = A.take_n<double>(cap[sd]); R.y = A.take_n<double>(cap[sd]);
     R.nx = A.take_n<int32_t>(cap[sd]); R.pv = A.take_n<int32_t>(cap[sd]); R.nb = A.take_n<int32_t>(cap[sd]);
     R.it = A.take_n<uint8_t>(cap[sd]); R.lb = A.take_n<int8_t>(cap[sd]); R.ee = A.take_n<int8_t>(cap[sd]);
-    R.used = 0; R.cap = (int)cap[sd];
-    a.root[sd] = A.take_n<int32_t>(k2[sd]);
-    a.noInter[sd] = A.take_n<uint8_t>(k2[sd]); a.ident[sd] = A.take_n<uint8_t>(k2[sd]);
+    a.root[sd] = A.take_n<int32_t>(nring[sd]);
+    a.noInter[sd] = A.take_n<uint8_t>(nring[sd]); a.ident[sd] = A.take_n<uint8_t>(nring[sd]);
     a.split[sd] = A.take_n<int32_t>(cap[sd]); a.cand[sd] = A.take_n<int32_t>(cap[sd]);
     ok = ok && R.x && R.y && R.nx && R.pv && R.nb && R.it && R.lb && R.ee && a.root[sd] && a.noInter[sd] &&
          a.ident[sd] && a.split[sd] && a.cand[sd];
   }
-  a.mark = A.take_n<uint8_t>(capQ);
-  a.vcap = 2 * (capP + capQ) + 16;
-  a.ccap = (int)std::min<int64_t>(2 * nR + kP + kQ + 16, INT32_MAX);
-  a.oxy = A.take_n<double>(2 * a.vcap); a.ocs = A.take_n<int32_t>(a.ccap);
-  a.onx = A.take_n<int32_t>(a.vcap); a.opv = A.take_n<int32_t>(a.vcap); a.otmp = A.take_n<double>(2 * a.vcap);
-  C.status = A.take_n<int32_t>(1);
-  C.ncomp = A.take_n<int32_t>(1);
-  C.comp_off = A.take_n<int64_t>(1);
-  C.count1 = A.take_n<int64_t>(1);
-  C.vert_off = A.take_n<int64_t>(1);
-  C.swapped = A.take_n<int32_t>(1);
-  int64_t* nvOut = A.take_n<int64_t>(1);
-  ok = ok && a.mark && a.oxy && a.ocs && a.onx && a.opv && a.otmp && C.status && C.ncomp && C.comp_off && C.count1 &&
-       C.vert_off && C.swapped && nvOut;
+  a.mark = A.take_n<uint8_t>(sQ);
+  a.oxy = A.take_n<double>(2 * vo); a.ocs = A.take_n<int32_t>(co);
+  a.onx = A.take_n<int32_t>(vo); a.opv = A.take_n<int32_t>(vo); a.otmp = A.take_n<double>(2 * vo);
+  MultiPairDesc* dd = A.take_n<MultiPairDesc>(n);
+  C.status = A.take_n<int32_t>(n);
+  C.ncomp = A.take_n<int32_t>(n);
+  C.comp_off = A.take_n<int64_t>(n);
+  C.count1 = A.take_n<int64_t>(n);
+  C.vert_off = A.take_n<int64_t>(n);
+  C.swapped = A.take_n<int32_t>(n);
+  int64_t* nvOut = A.take_n<int64_t>(n);
+  int64_t* tot = A.take_n<int64_t>(2);
+  void* stN = A.take(scan_temp_bytes(n));
+  ok = ok && a.mark && a.oxy && a.ocs && a.onx && a.opv && a.otmp && dd && C.status && C.ncomp && C.comp_off &&
+       C.count1 && C.vert_off && C.swapped && nvOut && tot && stN;
   if (!ok) return ST_OUT_OF_MEMORY;
   a.status = C.status; a.outNC = C.ncomp; a.outNV = nvOut;
   a.epsClean = prm.eps_clean; a.uni = prm.union_mode; a.exact = prm.exact; a.err = d_err;
-  cudaMemsetAsync(C.comp_off, 0, sizeof(int64_t), s);
-  cudaMemsetAsync(C.vert_off, 0, sizeof(int64_t), s);
-  cudaMemsetAsync(C.swapped, 0, sizeof(int32_t), s);
-  cudaMemcpyAsync(C.count1, &count1, sizeof(int64_t), cudaMemcpyHostToDevice, s);
-  { multi_clip_kernel<<<1, 1, 0, s>>>(a); note_launch(); }
-  int32_t hnc = 0;
-  int64_t hnv = 0;
-  cudaMemcpyAsync(&hnc, C.ncomp, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(&hnv, nvOut, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  cudaMemsetAsync(C.swapped, 0, n * sizeof(int32_t), s);
+  cudaMemcpyAsync(C.count1, hcount1.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dd, hd.data(), n * sizeof(MultiPairDesc), cudaMemcpyHostToDevice, s);
+  // a warp per block: a batch of a few thousand pairs then spreads over every SM
+  { multi_clip_batch_kernel<<<(unsigned)((n + 31) / 32), 32, 0, s>>>(a, dd, n); note_launch(); }
+  exclusive_scan_i32(C.ncomp, C.comp_off, n, tot, stN, d_err, s);
+  exclusive_scan_i64(nvOut, C.vert_off, n, tot + 1, stN, d_err, s);
+  cudaMemcpyAsync(hs, tot, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
-  C.n_pairs = 1;
-  C.n_components = hnc;
-  C.n_vertices = hnv;
-  C.n_records = nR;
-  C.comp_size = a.ocs;
-  C.xy = a.oxy;
+  const int64_t nComp = hs[0], nVert = hs[1];
+  C.comp_size = A.take_n<int32_t>(std::max<int64_t>(nComp, 1));
+  C.xy = A.take_n<double>(2 * std::max<int64_t>(nVert, 1));
+  if (!C.comp_size || !C.xy) return ST_OUT_OF_MEMORY;
+  { multi_compact_kernel<<<(unsigned)((32 * n + 127) / 128), 128, 0, s>>>(dd, n, a.ocs, a.oxy, C.ncomp, nvOut,
+                                                                          C.comp_off, C.vert_off, C.comp_size,
+                                                                          C.xy); note_launch(); }
+  if (!sync()) return ST_CUDA_ERROR;
+  C.n_pairs = n;
+  C.n_components = nComp;
+  C.n_vertices = nVert;
+  C.n_records = nRall;
   return ST_OK;
+}
+
+int run_clip_multi(const double* hP, const int32_t* sizesP, int kP, const double* hQ, const int32_t* sizesQ, int kQ,
+                   const ClipParams& prm, Arena& A, ClipDev& C, int* d_err, int64_t* hs, cudaStream_t s) {
+  if (kP <= 0 || kQ <= 0) return ST_INVALID_ARGUMENT;
+  const int32_t rp = kP, rq = kQ;
+  return run_clip_multi_batch(1, hP, sizesP, &rp, hQ, sizesQ, &rq, prm, A, C, d_err, hs, s);
 }
 
 }  // namespace gcmfgh

@@ -129,6 +129,7 @@ def lib():
         L.gh_clip_ptr.argtypes = [vp, ctypes.c_int, P(vp), P(i64)]
         L.gh_clip_pair.argtypes = [vp, vp, i32, vp, i32, P(ClipInfo)]
         L.gh_clip_multi.argtypes = [vp, vp, vp, i32, vp, vp, i32, P(ClipInfo)]
+        L.gh_clip_multi_batch.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp, P(ClipInfo)]
         L.gh_calculate_intersections.argtypes = [vp, P(Layer), i32, P(Layer), i32, P(Intersections)]
         L.gh_free_intersections.argtypes = [P(Intersections)]
         L.gh_free_intersections.restype = None
@@ -363,6 +364,22 @@ class Engine:
         info = ClipInfo()
         _check(lib().gh_clip_multi(self.h, _np_ptr(P), _np_ptr(sp), len(sp), _np_ptr(Q), _np_ptr(sq), len(sq),
                                    ctypes.byref(info)))
+        return info.as_dict()
+
+    def clip_multi_batch(self, pairs):
+        """Clip a batch of multi-component polygon pairs, [(P_rings, Q_rings), ...], in one
+        call (gh_clip_multi_batch); read the results with clip_result()."""
+        def side(idx):
+            rings = [np.asarray(r, np.float64).reshape(-1) for pq in pairs for r in pq[idx]]
+            xy = np.ascontiguousarray(np.concatenate(rings))
+            sizes = np.array([len(r) // 2 for r in rings], np.int32)
+            counts = np.array([len(pq[idx]) for pq in pairs], np.int32)
+            return xy, sizes, counts
+        P, sp, cp = side(0)
+        Q, sq, cq = side(1)
+        info = ClipInfo()
+        _check(lib().gh_clip_multi_batch(self.h, len(pairs), _np_ptr(P), _np_ptr(sp), _np_ptr(cp), _np_ptr(Q),
+                                         _np_ptr(sq), _np_ptr(cq), ctypes.byref(info)))
         return info.as_dict()
 
     def calculate_intersections(self, p_layer: DeviceLayer, p_id, q_layer: DeviceLayer, q_id):

@@ -238,6 +238,13 @@ gcmfgh_status gh_clip_pair(gcmfgh_ctx* ctx, const double* P, int32_t nP, const d
  * gh_clip_batch (gh_clip_get / gh_clip_ptr). */
 gcmfgh_status gh_clip_multi(gcmfgh_ctx* ctx, const double* P, const int32_t* p_sizes, int32_t p_rings,
                             const double* Q, const int32_t* q_sizes, int32_t q_rings, gcmfgh_clip_info* info);
+/* ---- n_pairs such pairs in one batch.  Pair i's P has p_rings[i] rings, taken in order
+ * from p_sizes / P (every pair's rings one after the other), and the same for Q.  The
+ * intersection records of all ring pairs come from one run of the batched stages; the
+ * labelling and tracing run one GPU thread per pair.  Read the result like gh_clip_batch's. */
+gcmfgh_status gh_clip_multi_batch(gcmfgh_ctx* ctx, int64_t n_pairs, const double* P, const int32_t* p_sizes,
+                                  const int32_t* p_rings, const double* Q, const int32_t* q_sizes,
+                                  const int32_t* q_rings, gcmfgh_clip_info* info);
 
 /* ---- the intersection phase of one pair: replaces calculateIntersections
  * (ghcuda.h:6-14, gppolyclip_mDIV512.cu:1298-1640), which hands the merged rings to the

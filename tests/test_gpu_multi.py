@@ -89,3 +89,54 @@ def test_large_island_with_many_holes(engine):
         assert r.status[0] == o.status[0] == 0
         assert len(o.components(0)) > 5
         assert same_components(r.components(0), o.components(0))
+
+
+def _gpu_batch(engine, pairs, union=False, exact=False):
+    engine.set_params(1e-7, 1e-7, union)
+    engine.set_precision(exact)
+    try:
+        info = engine.clip_multi_batch(pairs)
+        r = engine.clip_result()
+    finally:
+        engine.set_precision(False)
+        engine.set_params(1e-7, 1e-7, False)
+    assert info["n_pairs"] == len(pairs)
+    return r
+
+
+@pytest.mark.parametrize("union", [False, True])
+def test_batch_of_holed_pairs_matches_reference(engine, union):
+    """The reference clipper's results for every holed pair, from one batched call."""
+    pairs, inter, uni = unpack_multi(os.path.join(GOLDEN, "holed_pairs.npz"))
+    r = _gpu_batch(engine, pairs, union=union)
+    for i, exp in enumerate(uni if union else inter):
+        assert r.status[i] == 0
+        assert same_components(r.components(i), exp)
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_batch_equals_single_calls_and_oracle(engine, exact):
+    """A mixed batch (holed pairs, single rings, one invalid pair, the figures): each pair's
+    result equals its own gh_clip_multi call bit for bit, and the oracle's."""
+    pairs = [(P, Q) for P, Q in synth.holed_pairs(31, 40, 20, 300)]
+    pairs += [([P], [Q]) for P, Q in synth.random_star_pairs(32, 20, 5, 200)]
+    P, Q = synth.random_star_pairs(7, 1, 4, 12, spread=1.0)[0]
+    hole = synth._star(np.random.default_rng(1), 8, 0.0, 0.0, 0.1, 0.5, 1.0)
+    pairs.append(([P * 1e-3, hole * 50], [Q * 1e-3]))
+    for name in ("Fig18", "Fig19"):
+        pairs.append((load_poly(os.path.join(GOLDEN, "figs", f"{name}-P.poly")),
+                      load_poly(os.path.join(GOLDEN, "figs", f"{name}-Q.poly"))))
+    r = _gpu_batch(engine, pairs, exact=exact)
+    if not exact:                      # the tolerance classification disagrees on P and Q sides
+        assert r.status[len(pairs) - 3] == 1
+    for i, (P, Q) in enumerate(pairs):
+        s = _gpu(engine, P, Q, exact=exact)
+        assert r.status[i] == s.status[0]
+        assert r.count1[i] == s.count1[0]
+        assert r.ncomp[i] == s.ncomp[0]
+        a, b = r.components(i), s.components(0)
+        assert len(a) == len(b) and all(np.array_equal(x, y) for x, y in zip(a, b))
+        o = pyoracle.clip_multi(P, Q, exact=exact)
+        assert r.status[i] == o.status[0]
+        if o.status[0] == 0:
+            assert same_components(a, o.components(0))
