@@ -2,6 +2,7 @@
 // result export.  The reference's entry points exit the process on errors
 // (GPU_Manage.h:25-44, ghcuda.cpp:109-116); these return a status instead.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -27,8 +28,8 @@ cudaStream_t create_priority_stream() {
   return s;
 }
 
-unsigned long long& launch_counter() {
-  static unsigned long long n = 0;
+std::atomic<unsigned long long>& launch_counter() {
+  static std::atomic<unsigned long long> n{0};
   return n;
 }
 

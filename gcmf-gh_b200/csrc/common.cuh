@@ -4,6 +4,7 @@
 // with --fmad=false, so every a*b+c is two IEEE-rounded operations, exactly as the
 // reference's host code computes it; results are bit-identical to a CPU evaluation.
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -33,9 +34,10 @@ enum : int8_t { L_NONE = 0, L_CROSSING, L_BOUNCING, L_LEFT_ON, L_RIGHT_ON, L_ON_
 enum : int8_t { E_EXIT = 0, E_ENTRY = 1, E_NEITHER = 2 };
 enum : int { R_LEFT = 0, R_RIGHT = 1, R_IS_P_M = 2, R_IS_P_P = 3 };
 
-// host-side count of kernel launches issued by the library (gcmfgh_launch_count)
-unsigned long long& launch_counter();
-inline void note_launch() { ++launch_counter(); }
+// host-side count of kernel launches issued by the library (gcmfgh_launch_count); contexts
+// may launch from several host threads
+std::atomic<unsigned long long>& launch_counter();
+inline void note_launch() { launch_counter().fetch_add(1, std::memory_order_relaxed); }
 
 // ---- geometry (reference arithmetic, see file header)
 
