@@ -2618,6 +2618,26 @@ label_trace_tile_kernel(LabelArgs a) {
   label_trace_pair<EX>(g, a, (int64_t)a.order[i]);
 }
 
+// sizes in the labelling order, and the scanned offsets back to pair order
+__global__ void permute_sizes_kernel(const uint32_t* __restrict__ order, int64_t K, const int64_t* __restrict__ sP,
+                                     const int64_t* __restrict__ sQ, int64_t* __restrict__ oP, int64_t* __restrict__ oQ) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= K) return;
+  const uint32_t k = order[i];
+  oP[i] = sP[k];
+  oQ[i] = sQ[k];
+}
+
+__global__ void unpermute_offsets_kernel(const uint32_t* __restrict__ order, int64_t K,
+                                         const int64_t* __restrict__ offP, const int64_t* __restrict__ offQ,
+                                         int64_t* __restrict__ regP, int64_t* __restrict__ regQ) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= K) return;
+  const uint32_t k = order[i];
+  regP[k] = offP[i];
+  regQ[k] = offQ[i];
+}
+
 // Sort keys of the one-thread and warp pairs: each class in 127 size buckets, largest
 // first (one-thread pairs 0..126, warp pairs 128..254, the rest 255), for one 8-bit
 // radix pass; the counts of the two classes go to cnt[0], cnt[1].
@@ -3830,8 +3850,36 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
                                                       regSizeP, ringTot); note_launch(); }
   { pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffQ, vposQ, D.nQ, nrec, D.status, K, nEQ, vtotQ, mQ,
                                                       regSizeQ, ringTot); note_launch(); }
-  exclusive_scan_i64(regSizeP, regP, K, tot + 11, stK, d_err, s);
-  exclusive_scan_i64(regSizeQ, regQ, K, tot + 12, stK, d_err, s);
+  // The one-thread and warp labelling kernels take their pairs in size order (largest
+  // first, label_order_kernel), and the ring regions are laid out in that order, so that
+  // the pairs labelled side by side have neighbouring regions.  The record export keeps
+  // the regions in pair order.
+  const int64_t midMin = std::min(prm.mid_label_min, prm.big_label_min);
+  unsigned long long* mcnt = A.take_n<unsigned long long>(4);
+  uint32_t* oval = A.take_n<uint32_t>(K);
+  if (!mcnt || !oval) return ST_OUT_OF_MEMORY;
+  cudaMemsetAsync(mcnt, 0, 4 * sizeof(unsigned long long), s);
+  if (!ex) {
+    uint64_t* okey = A.take_n<uint64_t>(K);
+    uint64_t* okeyAlt = A.take_n<uint64_t>(K);
+    uint32_t* ovalAlt = A.take_n<uint32_t>(K);
+    void* otmp = A.take(radix_temp_bytes(K));
+    int64_t* sortedP = A.take_n<int64_t>(K);
+    int64_t* sortedQ = A.take_n<int64_t>(K);
+    int64_t* offSP = A.take_n<int64_t>(K);
+    int64_t* offSQ = A.take_n<int64_t>(K);
+    if (!okey || !okeyAlt || !ovalAlt || !otmp || !sortedP || !sortedQ || !offSP || !offSQ) return ST_OUT_OF_MEMORY;
+    { label_order_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, D.status, K, std::max<int64_t>(prm.tile_label_max, 0),
+                                                           midMin, okey, oval, mcnt + 2); note_launch(); }
+    radix_sort_pairs(okey, oval, okeyAlt, ovalAlt, K, 8, otmp, d_err, s);
+    { permute_sizes_kernel<<<blocks_for(K), kThreads, 0, s>>>(oval, K, regSizeP, regSizeQ, sortedP, sortedQ); note_launch(); }
+    exclusive_scan_i64(sortedP, offSP, K, tot + 11, stK, d_err, s);
+    exclusive_scan_i64(sortedQ, offSQ, K, tot + 12, stK, d_err, s);
+    { unpermute_offsets_kernel<<<blocks_for(K), kThreads, 0, s>>>(oval, K, offSP, offSQ, regP, regQ); note_launch(); }
+  } else {
+    exclusive_scan_i64(regSizeP, regP, K, tot + 11, stK, d_err, s);
+    exclusive_scan_i64(regSizeQ, regQ, K, tot + 12, stK, d_err, s);
+  }
   cudaMemcpyAsync(hs, tot + 11, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
   const int64_t regTotP = hs[0], regTotQ = hs[1];
@@ -3975,23 +4023,12 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   { out_sizes_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, nrec, D.status, K, vcap, ccap); note_launch(); }
   exclusive_scan_i64(vcap, vOff, K, tot + 13, stK, d_err, s);
   exclusive_scan_i32(ccap, cOff, K, tot + 14, stK, d_err, s);
-  // the pairs for the block kernel, and the one-thread and warp pairs in size order (their
-  // counts are read with the output sizes)
+  // the pairs for the block kernel (the one-thread and warp pairs' order and counts came
+  // with the ring layout; all counts are read with the output sizes)
   int64_t* mlist = A.take_n<int64_t>(K);
-  unsigned long long* mcnt = A.take_n<unsigned long long>(4);
-  uint64_t* okey = A.take_n<uint64_t>(K);
-  uint32_t* oval = A.take_n<uint32_t>(K);
-  uint64_t* okeyAlt = A.take_n<uint64_t>(K);
-  uint32_t* ovalAlt = A.take_n<uint32_t>(K);
-  void* otmp = A.take(radix_temp_bytes(K));
-  if (!mlist || !mcnt || !okey || !oval || !okeyAlt || !ovalAlt || !otmp) return ST_OUT_OF_MEMORY;
-  cudaMemsetAsync(mcnt, 0, 4 * sizeof(unsigned long long), s);
-  const int64_t midMin = std::min(prm.mid_label_min, prm.big_label_min);
+  if (!mlist) return ST_OUT_OF_MEMORY;
   { mid_label_list_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, D.status, K, midMin, prm.big_label_min,
                                                             mlist, mcnt); note_launch(); }
-  { label_order_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, D.status, K, std::max<int64_t>(prm.tile_label_max, 0),
-                                                         midMin, okey, oval, mcnt + 2); note_launch(); }
-  radix_sort_pairs(okey, oval, okeyAlt, ovalAlt, K, 8, otmp, d_err, s);
   cudaMemcpyAsync(hs, tot + 13, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hs + 2, mcnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hs + 3, mcnt + 2, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
