@@ -151,6 +151,11 @@ def stage_bytes(stage, ji, ci, nb, no, vb, vo, cand_vertices=0):
         "clip:emit": 16 * ring + 33 * recs,
         "clip:count+emit": 16 * ring + 8 * C + 33 * recs,
         "join:mbr+sort": 16 * (vb + vo) + 40 * (nb + no),
+        # MBRs of both layers, the overlay's extent and its grid listing
+        "join:mbr+grid": 16 * (vb + vo) + 36 * (nb + no) + 4 * no,
+        # each base MBR probes its cells; each listed overlay MBR it meets is read
+        "join:cand-count": 32 * (nb + no),
+        "join:cand-emit+sort": 32 * (nb + no) + 16 * K,
         "join:sweep-count": 36 * (nb + no),
         "join:sweep-emit+sort": 36 * (nb + no) + 16 * K,
         "join:cmf": 16 * cand_vertices + 40 * K,

@@ -107,7 +107,8 @@ struct gcmfgh_ctx {
   int device = 0;
   std::string gpu_name;
   bool tuning_explicit = false;   // gcmfgh_set_tuning was called: recorded tunings are not applied
-  int join_f32 = 1;               // FP32 prefilters of the join (bit 0 MBR y test, bit 1 edge test)
+  int join_f32 = 5;               // join options: FP32 prefilters (bit 0 MBR y test, bit 1 edge test),
+                                  // bit 2 the sort-sweep MBR filter instead of the grid probe
   bool hint_explicit = false;     // gcmfgh_set_tuning fixed the record capacity hint
   std::vector<TuneRecord> tunings;
   cudaStream_t own = nullptr;
@@ -504,7 +505,11 @@ gcmfgh_status gcmfgh_set_precision(gcmfgh_ctx* c, int mode) {
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* c, int key, int64_t value) {
   if (!c || value < 0) return GCMFGH_INVALID_ARGUMENT;
   if (key == GCMFGH_TUNE_F32_FILTER) {
-    c->join_f32 = (int)(value & 3);
+    c->join_f32 = (c->join_f32 & 4) | (int)(value & 3);
+    return GCMFGH_OK;
+  }
+  if (key == GCMFGH_TUNE_JOIN_SWEEP) {
+    c->join_f32 = (c->join_f32 & 3) | (value ? 4 : 0);
     return GCMFGH_OK;
   }
   if (key == GCMFGH_TUNE_FUSED_EMIT) {
@@ -674,7 +679,7 @@ gcmfgh_status gcmfgh_autotune_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const
   struct Knob { Field f; std::vector<int64_t> vals; };
   const Knob knobs[] = {
       {&ClipParams::bin_grid, {1ll << 10, 1ll << 12, 1ll << 14, 1ll << 16, 1ll << 20, 1ll << 24}},
-      {&ClipParams::tile_label_max, {0, 32, 64, 96, 128}},
+      {&ClipParams::tile_label_max, {0, 32, 64, 96, 128, 192, 256}},
       {&ClipParams::mid_label_min, {256, 512, 1024, 2048, 4096}},
       {&ClipParams::wide_label_min, {0, 1ll << 16, kNever}},
   };

@@ -11,8 +11,10 @@
 // [minx, miny, maxx, maxy] FP64 rows plus a sorted structure-of-arrays copy (x1, x2,
 // y1, y2, id) in ascending x1 order, which is what the sweep streams.
 #include <algorithm>
+#include <vector>
 #include "common.cuh"
 #include "engine.cuh"
+#include "grid.cuh"
 #include "prims.cuh"
 
 namespace gcmfgh {
@@ -458,6 +460,7 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
   // f32 bit 0: FP32 prefilter of the sweep's y test; bit 1: of the common-MBR edge test
   // (needs the layers' vertex counts, for their FP32 copies)
   const bool f32cmf = (f32 & 2) && Lb0.nverts > 0 && Lo0.nverts > 0;
+  const bool forceSweep = (f32 & 4) != 0;          // bit 2: the sort-sweep MBR filter, never the grid
   f32 &= 1;
   LayerDev Lb = Lb0, Lo = Lo0;
   Marks dummy;
@@ -497,6 +500,7 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
   // (about 100 blocks per pass), so the overlay's run on the auxiliary stream.
   cudaStream_t so = s;
   cudaEvent_t fork = nullptr, join = nullptr;
+  struct EvGuard { cudaEvent_t* a; cudaEvent_t* b; ~EvGuard() { if (*a) cudaEventDestroy(*a); if (*b) cudaEventDestroy(*b); } } evg{&fork, &join};
   if (aux && cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) == cudaSuccess &&
       cudaEventCreateWithFlags(&join, cudaEventDisableTiming) == cudaSuccess) {
     cudaEventRecord(fork, s);
@@ -507,62 +511,138 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
   // the overlay may still be on its way to the device (ovl_ready, recorded after its copy)
   if (ovl_ready) cudaStreamWaitEvent(so, ovl_ready, 0);
   { mbr_kernel<<<blocks_for_warps(no), kThreads, 0, so>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1, xyfO); note_launch(); }
-  // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
-  radix_sort_pairs(keyB, idB, kAlt, vAlt, nb, 64, tmp, d_err, s);
-  radix_sort_pairs(keyO, idO, kAltO, vAltO, no, 64, tmpO, d_err, so);
+  // the overlay's extent and mean box size, for the grid of the MBR filter
+  constexpr int kExtentBlocks = 148;
+  double* part = A.take_n<double>(7 * kExtentBlocks);
+  if (!part) return ST_OUT_OF_MEMORY;
+  { mbr_extent_kernel<<<kExtentBlocks, kExtentThreads, 0, so>>>(J.mbr_o, J.valid_o, no, part); note_launch(); }
   if (so != s) {
     cudaEventRecord(join, so);
     cudaStreamWaitEvent(s, join, 0);
   }
-  if (fork) cudaEventDestroy(fork);
-  if (join) cudaEventDestroy(join);
-  mk->mark("join:mbr+sort", s);
   cudaMemcpyAsync(h_scratch, d_cnt, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  std::vector<double> hpart(7 * kExtentBlocks);
+  cudaMemcpyAsync(hpart.data(), part, hpart.size() * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
   const int64_t nvb = h_scratch[0], nvo = h_scratch[1];
-  SortedMbr SB{A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb),
-               A.take_n<uint32_t>(nvb), nvb, f32 ? A.take_n<float2>(nvb) : nullptr};
-  SortedMbr SO{A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo),
-               A.take_n<uint32_t>(nvo), nvo, f32 ? A.take_n<float2>(nvo) : nullptr};
-  if (f32 && (!SB.yf || !SO.yf)) return ST_OUT_OF_MEMORY;
-  int32_t* cnt = A.take_n<int32_t>(nvb + nvo);
-  int64_t* offs = A.take_n<int64_t>(nvb + nvo);
-  int64_t* d_total = A.take_n<int64_t>(4);
-  if (!SB.x1 || !SB.x2 || !SB.y1 || !SB.y2 || !SB.id || !SO.x1 || !SO.x2 || !SO.y1 || !SO.y2 ||
-      !SO.id || !cnt || !offs || !d_total)
-    return ST_OUT_OF_MEMORY;
-  if (nvb) { gather_sorted_kernel<<<blocks_for(nvb), kThreads, 0, s>>>(J.mbr_b, idB, nvb, SB); note_launch(); }
-  if (nvo) { gather_sorted_kernel<<<blocks_for(nvo), kThreads, 0, s>>>(J.mbr_o, idO, nvo, SO); note_launch(); }
-  // ---- J2 sweep: count, scan, emit, canonical sort
   const int obits = bits_for(no);
   const int bbits = bits_for(nb);
   if (obits + bbits > 64) return ST_INVALID_ARGUMENT;
-  const int64_t ne = nvb + nvo;
-  if (ne > 0) {
-    { (f32 ? sweep_kernel<0, 1> : sweep_kernel<0, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr,
-                                                                                             nullptr, obits); note_launch(); }
-    void* stmp = A.take(scan_temp_bytes(ne));
-    if (!stmp) return ST_OUT_OF_MEMORY;
-    exclusive_scan_i32(cnt, offs, ne, d_total, stmp, d_err, s);
-  } else {
-    cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
+  int64_t* d_total = A.take_n<int64_t>(4);
+  if (!d_total) return ST_OUT_OF_MEMORY;
+  // ---- J2 MBR filter as a grid probe (grid.cuh): the overlay's valid MBRs listed in the
+  // cells of a uniform grid, every base polygon testing the entries of its cells.  The
+  // sort-sweep below, the reference's own form, takes over when the listing would be
+  // large (boxes spanning many cells).
+  uint64_t* pkeys = nullptr;
+  int64_t K = 0;
+  bool swept = true;
+  if (nvb > 0 && nvo > 0 && !forceSweep) {
+    double ext[7] = {INFINITY, INFINITY, -INFINITY, -INFINITY, 0.0, 0.0, 0.0};
+    for (int j = 0; j < kExtentBlocks; ++j) {
+      const double* r = &hpart[7 * j];
+      ext[0] = std::min(ext[0], r[0]); ext[1] = std::min(ext[1], r[1]);
+      ext[2] = std::max(ext[2], r[2]); ext[3] = std::max(ext[3], r[3]);
+      for (int k = 4; k < 7; ++k) ext[k] += r[k];
+    }
+    GridIndex G = grid_over(ext[0], ext[1], ext[2], ext[3], ext[4] / ext[6], ext[5] / ext[6]);
+    const int64_t ncell = (int64_t)G.gx * G.gy;
+    int32_t* cellCnt = A.take_n<int32_t>(ncell + 1);
+    int64_t* cellOff = A.take_n<int64_t>(ncell + 1);
+    void* ctmp = A.take(scan_temp_bytes(std::max<int64_t>(ncell + 1, nb)));
+    if (!cellCnt || !cellOff || !ctmp) return ST_OUT_OF_MEMORY;
+    cudaMemsetAsync(cellCnt, 0, (ncell + 1) * sizeof(int32_t), s);
+    { index_kernel<0><<<blocks_for(no), kThreads, 0, s>>>(J.mbr_o, J.valid_o, no, G, cellCnt, nullptr, nullptr); note_launch(); }
+    exclusive_scan_i32(cellCnt, cellOff, ncell + 1, d_total + 1, ctmp, d_err, s);
+    cudaMemcpyAsync(h_scratch, d_total + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+    const int64_t nent = h_scratch[0];
+    if (nent <= 8 * nvo + (1ll << 22)) {
+      swept = false;
+      int32_t* cellList = A.take_n<int32_t>(std::max<int64_t>(nent, 1));
+      int32_t* cnt = A.take_n<int32_t>(nb);
+      int64_t* offs = A.take_n<int64_t>(nb);
+      if (!cellList || !cnt || !offs) return ST_OUT_OF_MEMORY;
+      cudaMemsetAsync(cellCnt, 0, (ncell + 1) * sizeof(int32_t), s);
+      { index_kernel<1><<<blocks_for(no), kThreads, 0, s>>>(J.mbr_o, J.valid_o, no, G, cellCnt, cellOff, cellList); note_launch(); }
+      G.cellOff = cellOff;
+      G.cellList = cellList;
+      mk->mark("join:mbr+grid", s);
+      { candidate_kernel<0><<<blocks_for_warps(nb), kThreads, 0, s>>>(J.mbr_b, J.valid_b, nb, J.mbr_o, G, cnt,
+                                                                       nullptr, nullptr, obits); note_launch(); }
+      exclusive_scan_i32(cnt, offs, nb, d_total, ctmp, d_err, s);
+      mk->mark("join:cand-count", s);
+      cudaMemcpyAsync(h_scratch, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+      K = h_scratch[0];
+      J.n_pairs = K;
+      if (K == 0) return ST_OK;
+      pkeys = A.take_n<uint64_t>(K);
+      uint32_t* pvals = A.take_n<uint32_t>(K);
+      uint64_t* pkAlt = A.take_n<uint64_t>(K);
+      uint32_t* pvAlt = A.take_n<uint32_t>(K);
+      void* rtmp = A.take(radix_temp_bytes(K));
+      if (!pkeys || !pvals || !pkAlt || !pvAlt || !rtmp) return ST_OUT_OF_MEMORY;
+      { candidate_kernel<1><<<blocks_for_warps(nb), kThreads, 0, s>>>(J.mbr_b, J.valid_b, nb, J.mbr_o, G, nullptr,
+                                                                       offs, pkeys, obits); note_launch(); }
+      radix_sort_pairs(pkeys, pvals, pkAlt, pvAlt, K, ((obits + bbits + 7) / 8) * 8, rtmp, d_err, s);
+      mk->mark("join:cand-emit+sort", s);
+    }
   }
-  mk->mark("join:sweep-count", s);
-  cudaMemcpyAsync(h_scratch, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
-  const int64_t K = h_scratch[0];
-  J.n_pairs = K;
+  if (swept) {
+    // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
+    if (so != s) {                                  // the overlay's sort beside the base's
+      cudaEventRecord(fork, s);
+      cudaStreamWaitEvent(so, fork, 0);
+    }
+    radix_sort_pairs(keyB, idB, kAlt, vAlt, nb, 64, tmp, d_err, s);
+    radix_sort_pairs(keyO, idO, kAltO, vAltO, no, 64, tmpO, d_err, so);
+    if (so != s) {
+      cudaEventRecord(join, so);
+      cudaStreamWaitEvent(s, join, 0);
+    }
+    mk->mark("join:mbr+sort", s);
+    SortedMbr SB{A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb),
+                 A.take_n<uint32_t>(nvb), nvb, f32 ? A.take_n<float2>(nvb) : nullptr};
+    SortedMbr SO{A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo),
+                 A.take_n<uint32_t>(nvo), nvo, f32 ? A.take_n<float2>(nvo) : nullptr};
+    if (f32 && (!SB.yf || !SO.yf)) return ST_OUT_OF_MEMORY;
+    int32_t* cnt = A.take_n<int32_t>(nvb + nvo);
+    int64_t* offs = A.take_n<int64_t>(nvb + nvo);
+    if (!SB.x1 || !SB.x2 || !SB.y1 || !SB.y2 || !SB.id || !SO.x1 || !SO.x2 || !SO.y1 || !SO.y2 ||
+        !SO.id || !cnt || !offs)
+      return ST_OUT_OF_MEMORY;
+    if (nvb) { gather_sorted_kernel<<<blocks_for(nvb), kThreads, 0, s>>>(J.mbr_b, idB, nvb, SB); note_launch(); }
+    if (nvo) { gather_sorted_kernel<<<blocks_for(nvo), kThreads, 0, s>>>(J.mbr_o, idO, nvo, SO); note_launch(); }
+    // ---- J2 sweep: count, scan, emit, canonical sort
+    const int64_t ne = nvb + nvo;
+    if (ne > 0) {
+      { (f32 ? sweep_kernel<0, 1> : sweep_kernel<0, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr,
+                                                                                               nullptr, obits); note_launch(); }
+      void* stmp = A.take(scan_temp_bytes(ne));
+      if (!stmp) return ST_OUT_OF_MEMORY;
+      exclusive_scan_i32(cnt, offs, ne, d_total, stmp, d_err, s);
+    } else {
+      cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
+    }
+    mk->mark("join:sweep-count", s);
+    cudaMemcpyAsync(h_scratch, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+    K = h_scratch[0];
+    J.n_pairs = K;
+    if (K == 0) return ST_OK;
+    pkeys = A.take_n<uint64_t>(K);
+    uint32_t* pvals = A.take_n<uint32_t>(K);
+    uint64_t* pkAlt = A.take_n<uint64_t>(K);
+    uint32_t* pvAlt = A.take_n<uint32_t>(K);
+    void* rtmp = A.take(radix_temp_bytes(K));
+    if (!pkeys || !pvals || !pkAlt || !pvAlt || !rtmp) return ST_OUT_OF_MEMORY;
+    { (f32 ? sweep_kernel<1, 1> : sweep_kernel<1, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs,
+                                                                                             pkeys, obits); note_launch(); }
+    radix_sort_pairs(pkeys, pvals, pkAlt, pvAlt, K, ((obits + bbits + 7) / 8) * 8, rtmp, d_err, s);
+    mk->mark("join:sweep-emit+sort", s);
+  }
   if (K == 0) return ST_OK;
-  uint64_t* pkeys = A.take_n<uint64_t>(K);
-  uint32_t* pvals = A.take_n<uint32_t>(K);
-  uint64_t* pkAlt = A.take_n<uint64_t>(K);
-  uint32_t* pvAlt = A.take_n<uint32_t>(K);
-  void* rtmp = A.take(radix_temp_bytes(K));
-  if (!pkeys || !pvals || !pkAlt || !pvAlt || !rtmp) return ST_OUT_OF_MEMORY;
-  { (f32 ? sweep_kernel<1, 1> : sweep_kernel<1, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs,
-                                                                                           pkeys, obits); note_launch(); }
-  radix_sort_pairs(pkeys, pvals, pkAlt, pvAlt, K, ((obits + bbits + 7) / 8) * 8, rtmp, d_err, s);
-  mk->mark("join:sweep-emit+sort", s);
   return join_from_keys(Lb, Lo, pkeys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, mk, aux);
 }
 

@@ -26,6 +26,7 @@
 #include <vector>
 #include "common.cuh"
 #include "engine.cuh"
+#include "grid.cuh"
 #include "prims.cuh"
 #include "../../include/gcmfgh.h"
 
@@ -48,20 +49,6 @@ int64_t now_ns() {
              std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-struct GridIndex {
-  double x0, y0, cw, ch;
-  int gx, gy;
-  const int64_t* cellOff;
-  const int32_t* cellList;
-};
-
-__device__ __forceinline__ int cell_of(double v, double c0, double cs, int g) {
-  double t = (v - c0) / cs;
-  if (!(t > 0)) return 0;
-  if (t >= (double)g) return g - 1;
-  return (int)t;
-}
-
 // Polygon MBR over every stored vertex and the join's validity rule (mbr_kernel in
 // join.cu: at least two stored vertices, nonzero width and height).
 __global__ void serve_mbr_kernel(LayerDev L, double* __restrict__ mbr, uint8_t* __restrict__ valid) {
@@ -80,70 +67,6 @@ __global__ void serve_mbr_kernel(LayerDev L, double* __restrict__ mbr, uint8_t* 
     reinterpret_cast<double4*>(mbr)[w] = make_double4(x1, y1, x2, y2);
     valid[w] = (nv >= 2 && x1 != x2 && y1 != y2) ? 1 : 0;
   }
-}
-
-template <int kMode>
-__global__ void index_kernel(const double* __restrict__ mbr, const uint8_t* __restrict__ valid, int64_t n,
-                             GridIndex G, int32_t* __restrict__ cnt, const int64_t* __restrict__ off,
-                             int32_t* __restrict__ list) {
-  int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-  if (i >= n || !valid[i]) return;
-  double4 m = reinterpret_cast<const double4*>(mbr)[i];
-  int x0 = cell_of(m.x, G.x0, G.cw, G.gx), x1 = cell_of(m.z, G.x0, G.cw, G.gx);
-  int y0 = cell_of(m.y, G.y0, G.ch, G.gy), y1 = cell_of(m.w, G.y0, G.ch, G.gy);
-  for (int y = y0; y <= y1; ++y)
-    for (int x = x0; x <= x1; ++x) {
-      int64_t c = (int64_t)y * G.gx + x;
-      int slot = atomicAdd(&cnt[c], 1);
-      if (kMode == 1) list[off[c] + slot] = (int32_t)i;
-    }
-}
-
-// The join's MBR candidate predicate (sweep_kernel, join.cu; GPU_MBR.h:339-539):
-// x1b <= x1o < x2b or x1o < x1b <= x2o, and closed overlap in y.
-__device__ __forceinline__ bool sweep_pair(double4 B, double4 O) {
-  bool x = (B.x <= O.x && O.x < B.z) || (O.x < B.x && B.x <= O.z);
-  return x && O.y <= B.w && B.y <= O.w;
-}
-
-// Warp per query: the resident polygons listed in the cells of the query's MBR that pass
-// the predicate; a pair is taken only in the cell of its overlap's lower-left corner, so
-// each appears once.  mode 0 counts, mode 1 writes keys (q << obits | o).
-template <int kMode>
-__global__ void candidate_kernel(const double* __restrict__ qmbr, const uint8_t* __restrict__ qvalid, int64_t nq,
-                                 const double* __restrict__ rmbr, GridIndex G, int32_t* __restrict__ cnt,
-                                 const int64_t* __restrict__ off, uint64_t* __restrict__ keys, int obits) {
-  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
-  if (w >= nq) return;
-  int c = 0;
-  if (qvalid[w]) {
-    const double4 B = reinterpret_cast<const double4*>(qmbr)[w];
-    int x0 = cell_of(B.x, G.x0, G.cw, G.gx), x1 = cell_of(B.z, G.x0, G.cw, G.gx);
-    int y0 = cell_of(B.y, G.y0, G.ch, G.gy), y1 = cell_of(B.w, G.y0, G.ch, G.gy);
-    int64_t pos = (kMode == 1) ? off[w] : 0;
-    for (int y = y0; y <= y1; ++y)
-      for (int x = x0; x <= x1; ++x) {
-        const int64_t cell = (int64_t)y * G.gx + x;
-        const int64_t e0 = G.cellOff[cell], e1 = G.cellOff[cell + 1];
-        for (int64_t e = e0; e < e1; e += 32) {
-          bool hit = false;
-          int32_t o = 0;
-          if (e + lane_id() < e1) {
-            o = G.cellList[e + lane_id()];
-            const double4 O = reinterpret_cast<const double4*>(rmbr)[o];
-            if (sweep_pair(B, O)) {
-              double cx = fmax(B.x, O.x), cy = fmax(B.y, O.y);
-              hit = cell_of(cx, G.x0, G.cw, G.gx) == x && cell_of(cy, G.y0, G.ch, G.gy) == y;
-            }
-          }
-          unsigned m = __ballot_sync(0xffffffffu, hit);
-          if (kMode == 1 && hit) keys[pos + __popc(m & lanemask_lt())] = ((uint64_t)w << obits) | (uint64_t)o;
-          pos += __popc(m);
-          c += __popc(m);
-        }
-      }
-  }
-  if (kMode == 0 && lane_id() == 0) cnt[w] = c;
 }
 
 // Pinned host blocks for the batches' results, recycled: a batch's results are copied from
@@ -568,15 +491,7 @@ gcmfgh_status gcmfgh_serve_open(const gcmfgh_layer* L, const gcmfgh_serve_option
     ++nvalid;
   }
   GridIndex G{0, 0, 1, 1, 1, 1, nullptr, nullptr};
-  if (nvalid > 0) {
-    const double W = x1 - x0, H = y1 - y0;
-    const double mw = sw / nvalid, mh = sh / nvalid;
-    G.gx = (int)std::min(2048.0, std::max(1.0, std::ceil(W / std::max(mw, W / 2048.0))));
-    G.gy = (int)std::min(2048.0, std::max(1.0, std::ceil(H / std::max(mh, H / 2048.0))));
-    G.x0 = x0; G.y0 = y0;
-    G.cw = W > 0 ? W / G.gx : 1.0;
-    G.ch = H > 0 ? H / G.gy : 1.0;
-  }
+  if (nvalid > 0) G = grid_over(x0, y0, x1, y1, sw / nvalid, sh / nvalid);
   const int64_t ncell = (int64_t)G.gx * G.gy;
   int32_t* cnt = nullptr;
   int64_t* total = nullptr;

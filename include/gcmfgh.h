@@ -159,6 +159,11 @@ const char* gcmfgh_status_string(gcmfgh_status s);
  * pass sizes its record arrays from it and runs again, at the counted size, when a clip
  * finds more).  0 (default): the last clip's count. */
 #define GCMFGH_TUNE_RECORD_HINT 7
+/* GCMFGH_TUNE_JOIN_SWEEP: 1 finds the MBR candidates with the reference's sort-sweep on x
+ * (GPU_MBR.h:339-539) instead of the grid probe; 0 (default) uses the grid probe unless
+ * its listing would be large.  Both give the same candidates.  The FP32 prefilter bit 0
+ * of GCMFGH_TUNE_F32_FILTER applies to the sweep only. */
+#define GCMFGH_TUNE_JOIN_SWEEP 8
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* ctx, int key, int64_t value);
 
 /* ---- autotuner of the work-distribution thresholds.  No counterpart in the reference

@@ -178,3 +178,49 @@ def test_fp32_prefilters_keep_fp64_results(engine):
         for a, b in zip(got[0], got[f32]):
             assert np.array_equal(a, b)
     assert int(o.pip_type.size) > 250          # about half the near-tie squares join
+
+
+def _keys(engine, db, do):
+    engine.join(db, do)
+    return np.stack([engine.join_field("b").reshape(-1), engine.join_field("o").reshape(-1)])
+
+
+@pytest.mark.parametrize("case", ["small", "ties", "huge_boxes", "listing_limit", "degenerate_extent"])
+def test_grid_probe_equals_sort_sweep(engine, case):
+    """The MBR filter's grid probe (default) and the reference's sort-sweep form the same
+    candidate list: on a seeded layer pair; on boxes that touch at cell-size multiples; on
+    layers where most boxes span the whole extent (a coarse grid, every cell listing
+    them); on tiny boxes plus 500 boxes spanning everything (the listing passes its limit
+    and the sweep takes over); and on a thin extent (all boxes in one row of cells)."""
+    import gcmfgh
+    rng = np.random.default_rng(5)
+    if case == "small":
+        base, ovl = synth.small_join(11, 3000)
+    elif case == "ties":
+        rings = [_box(x, y, x + 1, y + 1) for x in range(0, 40, 1) for y in range(0, 40, 2)]
+        base = synth.Layer.from_rings(rings)
+        ovl = synth.Layer.from_rings([_box(x + 1, y, x + 2, y + 1) for x in range(0, 40, 2) for y in range(0, 40)])
+    elif case == "huge_boxes":
+        small = [_box(*c, *(c + 1.0)) for c in rng.uniform(0, 100, size=(3000, 2))]
+        huge = [_box(-1.0 - i, -1.0 - i, 101.0 + i, 101.0 + i) for i in range(2000)]
+        base = synth.Layer.from_rings(small + huge[:5])
+        ovl = synth.Layer.from_rings(huge + small[::3])
+    elif case == "listing_limit":
+        tiny = [_box(*c, *(c + 0.01)) for c in rng.uniform(0, 1000, size=(100000, 2))]
+        huge = [_box(-1.0 - i, -1.0 - i, 1001.0 + i, 1001.0 + i) for i in range(500)]
+        base = synth.Layer.from_rings(tiny[:3000] + huge[:3])
+        ovl = synth.Layer.from_rings(tiny + huge)
+    else:
+        base = synth.Layer.from_rings([_box(x, 0, x + 1.5, 1e-9) for x in rng.uniform(0, 1000, 2000)])
+        ovl = synth.Layer.from_rings([_box(x, 0, x + 0.5, 2e-9) for x in rng.uniform(0, 1000, 2000)])
+    db, do = gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl)
+    grid = _keys(engine, db, do)
+    engine.set_tuning(join_sweep=True)
+    try:
+        sweep = _keys(engine, db, do)
+    finally:
+        engine.set_tuning(join_sweep=False)
+    assert grid.shape[1] > 0
+    assert np.array_equal(grid, sweep)
+    o = pyoracle.join(base, ovl)
+    assert np.array_equal(grid[0], o.b) and np.array_equal(grid[1], o.o)
