@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--no-precision", action="store_true", help="skip the degeneracy batch")
     ap.add_argument("--no-large-pair", action="store_true", help="skip the single large pair")
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-component pairs")
+    ap.add_argument("--join-sweep", type=int, default=None,
+                    help="1: MBR candidates by the sort-sweep, 0: by the grid probe (default: the library's)")
     ap.add_argument("--lanes", type=int, default=3,
                     help="contexts (and host threads) of the pipelined measurement; 1 skips it")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default size-bucket thresholds")
@@ -380,7 +382,8 @@ def plain_measure(eng, db, do, stream, n=2000, seed=9):
 
 # ----------------------------------------------------------------------------- single large pair
 
-def pipelined_measure(local, db, do, pinned, out_sizes, tuning, steps, warmup, lanes, fused_emit):
+def pipelined_measure(local, db, do, pinned, out_sizes, tuning, steps, warmup, lanes, fused_emit,
+                      join_sweep=None):
     """Whole-job throughput of `lanes` contexts on one GPU, each on its own stream, driven by
     its own host thread and taking every lanes-th step, all with the same thresholds: while
     one context waits on a size read-back or on PCIe, the others' kernels run.  Each step
@@ -403,6 +406,8 @@ def pipelined_measure(local, db, do, pinned, out_sizes, tuning, steps, warmup, l
         e.set_tuning(**tuning)
         if fused_emit is not None:
             e.set_tuning(fused_emit=fused_emit)
+        if join_sweep is not None:
+            e.set_tuning(join_sweep=bool(join_sweep))
     outs = [(torch.empty(out_sizes[0], dtype=torch.float64).pin_memory(),
              torch.empty(out_sizes[1], dtype=torch.int32).pin_memory(),
              torch.empty(out_sizes[2], dtype=torch.int32).pin_memory()) for _ in range(lanes)]
@@ -719,6 +724,8 @@ def run_ours(args, rank, world, local):
 
     if args.fused_emit is not None:
         eng.set_tuning(fused_emit=args.fused_emit)
+    if args.join_sweep is not None:
+        eng.set_tuning(join_sweep=bool(args.join_sweep))
     # the autotuner picks the size-bucket thresholds for this workload (outside the timing)
     eng.join(db, do)
     if args.no_autotune:
@@ -805,7 +812,7 @@ def run_ours(args, rank, world, local):
         pipe = pipelined_measure(local, db, do, pinned, (out_xy.numel(), out_cs.numel(), out_nc.numel()),
                                  {k: tuning[k] for k in ("bin_grid", "tile_label", "mid_label", "big_label",
                                                          "wide_label")},
-                                 args.steps, args.warmup, args.lanes, args.fused_emit)
+                                 args.steps, args.warmup, args.lanes, args.fused_emit, args.join_sweep)
 
     # the clocks were sampled through the single-lane, end-to-end and pipelined regions
     clocks = sampler.stop() if sampler else None

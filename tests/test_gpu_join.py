@@ -214,9 +214,10 @@ def test_grid_probe_equals_sort_sweep(engine, case):
         base = synth.Layer.from_rings([_box(x, 0, x + 1.5, 1e-9) for x in rng.uniform(0, 1000, 2000)])
         ovl = synth.Layer.from_rings([_box(x, 0, x + 0.5, 2e-9) for x in rng.uniform(0, 1000, 2000)])
     db, do = gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl)
-    grid = _keys(engine, db, do)
-    engine.set_tuning(join_sweep=True)
     try:
+        engine.set_tuning(join_sweep=False)
+        grid = _keys(engine, db, do)
+        engine.set_tuning(join_sweep=True)
         sweep = _keys(engine, db, do)
     finally:
         engine.set_tuning(join_sweep=False)
