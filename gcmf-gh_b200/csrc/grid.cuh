@@ -77,43 +77,66 @@ __device__ __forceinline__ bool sweep_pair(double4 B, double4 O) {
 
 // Warp per probing polygon q (the "base" side of the predicate): the indexed polygons
 // listed in the cells of q's MBR that pass the predicate, each taken in the cell of the
-// overlap's lower-left corner.  kMode 0 counts (cnt[q]); kMode 1 writes keys
-// (q << obits | o) from off[q].
+// overlap's lower-left corner.  The lanes take the cells (32 at a time, row by row), each
+// lane every entry of its cell, so a box spanning thousands of cells is probed in
+// parallel.  kMode 0 counts (cnt[q]); kMode 1 writes keys (q << obits | o) from off[q]
+// (order within q is the cells' order; the caller sorts).
+__device__ __forceinline__ bool grid_hit(const double4& B, const double* __restrict__ rmbr, int32_t o,
+                                         const GridIndex& G, int x, int y) {
+  const double4 O = reinterpret_cast<const double4*>(rmbr)[o];
+  if (!sweep_pair(B, O)) return false;
+  const double cx = fmax(B.x, O.x), cy = fmax(B.y, O.y);
+  return cell_of(cx, G.x0, G.cw, G.gx) == x && cell_of(cy, G.y0, G.ch, G.gy) == y;
+}
+
 template <int kMode>
 __global__ void candidate_kernel(const double* __restrict__ qmbr, const uint8_t* __restrict__ qvalid, int64_t nq,
                                  const double* __restrict__ rmbr, GridIndex G, int32_t* __restrict__ cnt,
                                  const int64_t* __restrict__ off, uint64_t* __restrict__ keys, int obits) {
   int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= nq) return;
-  int c = 0;
+  int64_t c = 0;
   if (qvalid[w]) {
     const double4 B = reinterpret_cast<const double4*>(qmbr)[w];
-    int x0 = cell_of(B.x, G.x0, G.cw, G.gx), x1 = cell_of(B.z, G.x0, G.cw, G.gx);
-    int y0 = cell_of(B.y, G.y0, G.ch, G.gy), y1 = cell_of(B.w, G.y0, G.ch, G.gy);
+    const int x0 = cell_of(B.x, G.x0, G.cw, G.gx), x1 = cell_of(B.z, G.x0, G.cw, G.gx);
+    const int y0 = cell_of(B.y, G.y0, G.ch, G.gy), y1 = cell_of(B.w, G.y0, G.ch, G.gy);
+    const int nx = x1 - x0 + 1;
+    const int64_t ncells = (int64_t)nx * (y1 - y0 + 1);
     int64_t pos = (kMode == 1) ? off[w] : 0;
-    for (int y = y0; y <= y1; ++y)
-      for (int x = x0; x <= x1; ++x) {
+    for (int64_t j0 = 0; j0 < ncells; j0 += 32) {
+      const int64_t j = j0 + lane_id();
+      int x = 0, y = 0;
+      int64_t e0 = 0, e1 = 0;
+      if (j < ncells) {
+        y = y0 + (int)(j / nx);
+        x = x0 + (int)(j - (int64_t)(y - y0) * nx);
         const int64_t cell = (int64_t)y * G.gx + x;
-        const int64_t e0 = G.cellOff[cell], e1 = G.cellOff[cell + 1];
-        for (int64_t e = e0; e < e1; e += 32) {
-          bool hit = false;
-          int32_t o = 0;
-          if (e + lane_id() < e1) {
-            o = G.cellList[e + lane_id()];
-            const double4 O = reinterpret_cast<const double4*>(rmbr)[o];
-            if (sweep_pair(B, O)) {
-              double cx = fmax(B.x, O.x), cy = fmax(B.y, O.y);
-              hit = cell_of(cx, G.x0, G.cw, G.gx) == x && cell_of(cy, G.y0, G.ch, G.gy) == y;
-            }
-          }
-          unsigned m = __ballot_sync(0xffffffffu, hit);
-          if (kMode == 1 && hit) keys[pos + __popc(m & lanemask_lt())] = ((uint64_t)w << obits) | (uint64_t)o;
-          pos += __popc(m);
-          c += __popc(m);
-        }
+        e0 = G.cellOff[cell];
+        e1 = G.cellOff[cell + 1];
       }
+      int h = 0;
+      for (int64_t e = e0; e < e1; ++e) h += grid_hit(B, rmbr, G.cellList[e], G, x, y) ? 1 : 0;
+      if (kMode == 1) {
+        int incl = h;                                // this lane's first key: pos + exclusive scan
+        for (int d = 1; d < 32; d <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, incl, d);
+          if ((int)lane_id() >= d) incl += t;
+        }
+        int64_t p = pos + incl - h;
+        if (h)
+          for (int64_t e = e0; e < e1; ++e) {
+            const int32_t o = G.cellList[e];
+            if (grid_hit(B, rmbr, o, G, x, y)) keys[p++] = ((uint64_t)w << obits) | (uint64_t)o;
+          }
+        pos += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      c += h;
+    }
   }
-  if (kMode == 0 && lane_id() == 0) cnt[w] = c;
+  if (kMode == 0) {
+    for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(0xffffffffu, c, d);
+    if (lane_id() == 0) cnt[w] = (int32_t)c;
+  }
 }
 
 // Extent and mean box size of the valid MBRs: per block, (min x1, min y1, max x2, max
