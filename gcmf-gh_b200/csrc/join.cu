@@ -57,35 +57,83 @@ struct JTile {
 };
 
 // ---------------------------------------------------------------- J0: MBRs
-// One warp per polygon, 128-bit vertex loads.  The MBR covers every stored vertex,
-// the closing one included (SEQ_Overlay.h:316-344).  Zero-width or zero-height MBRs are
-// rejected like the reference reader does (SEQ_Overlay.h:336-344): such a polygon never
-// joins.  Valid polygons get the order-preserving key of their x1 for the sweep sort.
+// 128-bit vertex loads.  The MBR covers every stored vertex, the closing one included
+// (SEQ_Overlay.h:316-344).  Zero-width or zero-height MBRs are rejected like the
+// reference reader does (SEQ_Overlay.h:336-344): such a polygon never joins.  Valid
+// polygons get the order-preserving key of their x1 for the sweep sort.  A warp takes four
+// consecutive polygons: 8 lanes each when all four have at most 64 stored vertices (most
+// polygons), else all 32 lanes for one polygon after another.
+template <int W>
+__device__ __forceinline__ void mbr_reduce(double& x1, double& y1, double& x2, double& y2) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) {
+    double t = __shfl_xor_sync(0xffffffffu, x1, o); x1 = t < x1 ? t : x1;
+    t = __shfl_xor_sync(0xffffffffu, y1, o); y1 = t < y1 ? t : y1;
+    t = __shfl_xor_sync(0xffffffffu, x2, o); x2 = t > x2 ? t : x2;
+    t = __shfl_xor_sync(0xffffffffu, y2, o); y2 = t > y2 ? t : y2;
+  }
+}
+
+__device__ __forceinline__ bool mbr_write(int64_t w, int nv, double x1, double y1, double x2, double y2,
+                                          double* __restrict__ mbr, uint8_t* __restrict__ valid,
+                                          uint64_t* __restrict__ key, uint32_t* __restrict__ id) {
+  const bool ok = nv >= 2 && x1 != x2 && y1 != y2;
+  reinterpret_cast<double4*>(mbr)[w] = make_double4(x1, y1, x2, y2);
+  valid[w] = ok ? 1 : 0;
+  key[w] = ok ? ordered_key(x1) : ~0ull;
+  id[w] = (uint32_t)w;
+  return ok;
+}
+
+constexpr int kMbrPerWarp = 4;
+constexpr int kMbrSmallMax = 64;
+
 __global__ void __launch_bounds__(kThreads)
 mbr_kernel(LayerDev L, double* __restrict__ mbr, uint8_t* __restrict__ valid,
            uint64_t* __restrict__ key, uint32_t* __restrict__ id, unsigned long long* n_valid,
            float2* __restrict__ xyf) {
-  int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
-  if (w >= L.n) return;
-  const int nv = L.vnum[w];
-  const int64_t s = L.vps[w] - nv;
-  const double2* v = reinterpret_cast<const double2*>(L.xy) + s;
-  double x1 = INFINITY, y1 = INFINITY, x2 = -INFINITY, y2 = -INFINITY;
-  for (int k = lane_id(); k < nv; k += 32) {
-    double2 p = __ldg(v + k);
-    if (xyf) xyf[s + k] = make_float2(__double2float_rn(p.x), __double2float_rn(p.y));
-    x1 = fmin(x1, p.x); x2 = fmax(x2, p.x);
-    y1 = fmin(y1, p.y); y2 = fmax(y2, p.y);
+  const int64_t p0 = (((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5) * kMbrPerWarp;
+  if (p0 >= L.n) return;
+  const int lane = (int)lane_id();
+  const int mine = (lane < kMbrPerWarp && p0 + lane < L.n) ? L.vnum[p0 + lane] : 0;
+  int ok = 0;
+  if (__all_sync(0xffffffffu, mine <= kMbrSmallMax)) {
+    constexpr int W = 32 / kMbrPerWarp;
+    const int g = lane / W, t = lane % W;
+    const int64_t w = p0 + g;
+    const int nv = __shfl_sync(0xffffffffu, mine, g);
+    double x1 = INFINITY, y1 = INFINITY, x2 = -INFINITY, y2 = -INFINITY;
+    if (w < L.n) {
+      const int64_t s = L.vps[w] - nv;
+      const double2* v = reinterpret_cast<const double2*>(L.xy) + s;
+      for (int k = t; k < nv; k += W) {
+        double2 p = __ldg(v + k);
+        if (xyf) xyf[s + k] = make_float2(__double2float_rn(p.x), __double2float_rn(p.y));
+        x1 = fmin(x1, p.x); x2 = fmax(x2, p.x);
+        y1 = fmin(y1, p.y); y2 = fmax(y2, p.y);
+      }
+    }
+    mbr_reduce<W>(x1, y1, x2, y2);
+    if (t == 0 && w < L.n) ok = mbr_write(w, nv, x1, y1, x2, y2, mbr, valid, key, id) ? 1 : 0;
+  } else {
+    for (int g = 0; g < kMbrPerWarp && p0 + g < L.n; ++g) {
+      const int64_t w = p0 + g;
+      const int nv = __shfl_sync(0xffffffffu, mine, g);
+      const int64_t s = L.vps[w] - nv;
+      const double2* v = reinterpret_cast<const double2*>(L.xy) + s;
+      double x1 = INFINITY, y1 = INFINITY, x2 = -INFINITY, y2 = -INFINITY;
+      for (int k = lane; k < nv; k += 32) {
+        double2 p = __ldg(v + k);
+        if (xyf) xyf[s + k] = make_float2(__double2float_rn(p.x), __double2float_rn(p.y));
+        x1 = fmin(x1, p.x); x2 = fmax(x2, p.x);
+        y1 = fmin(y1, p.y); y2 = fmax(y2, p.y);
+      }
+      mbr_reduce<32>(x1, y1, x2, y2);
+      if (lane == 0) ok += mbr_write(w, nv, x1, y1, x2, y2, mbr, valid, key, id) ? 1 : 0;
+    }
   }
-  x1 = warp_min(x1); y1 = warp_min(y1); x2 = warp_max(x2); y2 = warp_max(y2);
-  if (lane_id() == 0) {
-    bool ok = nv >= 2 && x1 != x2 && y1 != y2;
-    reinterpret_cast<double4*>(mbr)[w] = make_double4(x1, y1, x2, y2);
-    valid[w] = ok ? 1 : 0;
-    key[w] = ok ? ordered_key(x1) : ~0ull;
-    id[w] = (uint32_t)w;
-    if (ok) atomicAdd(n_valid, 1ull);
-  }
+  ok = __reduce_add_sync(0xffffffffu, ok);
+  if (lane == 0 && ok) atomicAdd(n_valid, (unsigned long long)ok);
 }
 
 // yf: (y1 rounded down, y2 rounded up) in FP32 -- a box that contains the FP64 one
@@ -507,22 +555,24 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
     cudaStreamWaitEvent(aux, fork, 0);
     so = aux;
   }
-  { mbr_kernel<<<blocks_for_warps(nb), kThreads, 0, s>>>(Lb, J.mbr_b, J.valid_b, keyB, idB, d_cnt + 0, xyfB); note_launch(); }
+  { mbr_kernel<<<blocks_for_warps((nb + kMbrPerWarp - 1) / kMbrPerWarp), kThreads, 0, s>>>(Lb, J.mbr_b, J.valid_b, keyB, idB,
+                                                                                       d_cnt + 0, xyfB); note_launch(); }
   // the overlay may still be on its way to the device (ovl_ready, recorded after its copy)
   if (ovl_ready) cudaStreamWaitEvent(so, ovl_ready, 0);
-  { mbr_kernel<<<blocks_for_warps(no), kThreads, 0, so>>>(Lo, J.mbr_o, J.valid_o, keyO, idO, d_cnt + 1, xyfO); note_launch(); }
+  { mbr_kernel<<<blocks_for_warps((no + kMbrPerWarp - 1) / kMbrPerWarp), kThreads, 0, so>>>(Lo, J.mbr_o, J.valid_o, keyO, idO,
+                                                                                        d_cnt + 1, xyfO); note_launch(); }
   // the overlay's extent and mean box size, for the grid of the MBR filter
   constexpr int kExtentBlocks = 148;
   double* part = A.take_n<double>(7 * kExtentBlocks);
   if (!part) return ST_OUT_OF_MEMORY;
-  { mbr_extent_kernel<<<kExtentBlocks, kExtentThreads, 0, so>>>(J.mbr_o, J.valid_o, no, part); note_launch(); }
+  if (!forceSweep) { mbr_extent_kernel<<<kExtentBlocks, kExtentThreads, 0, so>>>(J.mbr_o, J.valid_o, no, part); note_launch(); }
   if (so != s) {
     cudaEventRecord(join, so);
     cudaStreamWaitEvent(s, join, 0);
   }
   cudaMemcpyAsync(h_scratch, d_cnt, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   std::vector<double> hpart(7 * kExtentBlocks);
-  cudaMemcpyAsync(hpart.data(), part, hpart.size() * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (!forceSweep) cudaMemcpyAsync(hpart.data(), part, hpart.size() * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
   const int64_t nvb = h_scratch[0], nvo = h_scratch[1];
   const int obits = bits_for(no);
