@@ -63,6 +63,16 @@ struct JTile {
 // polygons get the order-preserving key of their x1 for the sweep sort.  A warp takes four
 // consecutive polygons: 8 lanes each when all four have at most 64 stored vertices (most
 // polygons), else all 32 lanes for one polygon after another.
+// Sweep sort key of a valid polygon: the order-preserving bits of x1 rounded down to FP32,
+// at most 0xFFFFFFFE (0xFFFFFFFF marks the invalid ones, which sort last).  Monotone in x1,
+// so sorting these 32 bits (4 radix passes instead of 8) orders the polygons by x1 up to
+// runs of equal keys, which x1_fixup_kernel puts in exact (x1, id) order.
+__device__ __forceinline__ uint64_t x1_key32(double x1) {
+  const uint32_t b = __float_as_uint(__double2float_rd(x1));
+  const uint32_t k = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+  return k < 0xFFFFFFFFu ? k : 0xFFFFFFFEu;
+}
+
 template <int W>
 __device__ __forceinline__ void mbr_reduce(double& x1, double& y1, double& x2, double& y2) {
 #pragma unroll
@@ -80,7 +90,7 @@ __device__ __forceinline__ bool mbr_write(int64_t w, int nv, double x1, double y
   const bool ok = nv >= 2 && x1 != x2 && y1 != y2;
   reinterpret_cast<double4*>(mbr)[w] = make_double4(x1, y1, x2, y2);
   valid[w] = ok ? 1 : 0;
-  key[w] = ok ? ordered_key(x1) : ~0ull;
+  key[w] = ok ? x1_key32(x1) : ~0ull;
   id[w] = (uint32_t)w;
   return ok;
 }
@@ -134,6 +144,47 @@ mbr_kernel(LayerDev L, double* __restrict__ mbr, uint8_t* __restrict__ valid,
   }
   ok = __reduce_add_sync(0xffffffffu, ok);
   if (lane == 0 && ok) atomicAdd(n_valid, (unsigned long long)ok);
+}
+
+// Runs of equal 32-bit keys among the first nv sorted entries: each run's first thread
+// sorts the run's ids by (ordered_key(x1), id), which makes the order that of a stable sort
+// on the full 64-bit key.  Runs longer than kFixupMaxRun set *flag instead (the caller then
+// sorts on 64 bits).
+constexpr int kFixupMaxRun = 256;
+__global__ void x1_fixup_kernel(const uint64_t* __restrict__ key, uint32_t* __restrict__ id, int64_t nv,
+                                const double* __restrict__ mbr, unsigned long long* __restrict__ flag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  const uint64_t k = key[i];
+  if (i > 0 && key[i - 1] == k) return;                 // not the first of its run
+  if (i + 1 >= nv || key[i + 1] != k) return;           // a run of one
+  int64_t j = i + 1;
+  while (j < nv && key[j] == k) {
+    if (j - i >= kFixupMaxRun) { atomicAdd(flag, 1ull); return; }
+    ++j;
+  }
+  for (int64_t a = i + 1; a < j; ++a) {                 // insertion sort, stable in id
+    const uint32_t v = id[a];
+    const uint64_t kv = ordered_key(mbr[4 * (int64_t)v]);
+    int64_t b = a - 1;
+    while (b >= i) {
+      const uint32_t u = id[b];
+      const uint64_t ku = ordered_key(mbr[4 * (int64_t)u]);
+      if (ku < kv || (ku == kv && u < v)) break;
+      id[b + 1] = u;
+      --b;
+    }
+    id[b + 1] = v;
+  }
+}
+
+// the full 64-bit sweep keys (for layers whose 32-bit keys leave long runs)
+__global__ void x1_key64_kernel(const double* __restrict__ mbr, const uint8_t* __restrict__ valid, int64_t n,
+                                uint64_t* __restrict__ key, uint32_t* __restrict__ id) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  key[i] = valid[i] ? ordered_key(mbr[4 * i]) : ~0ull;
+  id[i] = (uint32_t)i;
 }
 
 // yf: (y1 rounded down, y2 rounded up) in FP32 -- a box that contains the FP64 one
@@ -640,18 +691,6 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
     }
   }
   if (swept) {
-    // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
-    if (so != s) {                                  // the overlay's sort beside the base's
-      cudaEventRecord(fork, s);
-      cudaStreamWaitEvent(so, fork, 0);
-    }
-    radix_sort_pairs(keyB, idB, kAlt, vAlt, nb, 64, tmp, d_err, s);
-    radix_sort_pairs(keyO, idO, kAltO, vAltO, no, 64, tmpO, d_err, so);
-    if (so != s) {
-      cudaEventRecord(join, so);
-      cudaStreamWaitEvent(s, join, 0);
-    }
-    mk->mark("join:mbr+sort", s);
     SortedMbr SB{A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb), A.take_n<double>(nvb),
                  A.take_n<uint32_t>(nvb), nvb, f32 ? A.take_n<float2>(nvb) : nullptr};
     SortedMbr SO{A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo), A.take_n<double>(nvo),
@@ -659,25 +698,57 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
     if (f32 && (!SB.yf || !SO.yf)) return ST_OUT_OF_MEMORY;
     int32_t* cnt = A.take_n<int32_t>(nvb + nvo);
     int64_t* offs = A.take_n<int64_t>(nvb + nvo);
-    if (!SB.x1 || !SB.x2 || !SB.y1 || !SB.y2 || !SB.id || !SO.x1 || !SO.x2 || !SO.y1 || !SO.y2 ||
-        !SO.id || !cnt || !offs)
-      return ST_OUT_OF_MEMORY;
-    if (nvb) { gather_sorted_kernel<<<blocks_for(nvb), kThreads, 0, s>>>(J.mbr_b, idB, nvb, SB); note_launch(); }
-    if (nvo) { gather_sorted_kernel<<<blocks_for(nvo), kThreads, 0, s>>>(J.mbr_o, idO, nvo, SO); note_launch(); }
-    // ---- J2 sweep: count, scan, emit, canonical sort
     const int64_t ne = nvb + nvo;
-    if (ne > 0) {
-      { (f32 ? sweep_kernel<0, 1> : sweep_kernel<0, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr,
-                                                                                               nullptr, obits); note_launch(); }
-      void* stmp = A.take(scan_temp_bytes(ne));
-      if (!stmp) return ST_OUT_OF_MEMORY;
-      exclusive_scan_i32(cnt, offs, ne, d_total, stmp, d_err, s);
-    } else {
-      cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
+    void* stmp = A.take(scan_temp_bytes(std::max<int64_t>(ne, 1)));
+    if (!SB.x1 || !SB.x2 || !SB.y1 || !SB.y2 || !SB.id || !SO.x1 || !SO.x2 || !SO.y1 || !SO.y2 ||
+        !SO.id || !cnt || !offs || !stmp)
+      return ST_OUT_OF_MEMORY;
+    // Attempt 0 sorts the 32-bit keys of mbr_kernel and mends the runs of equal keys;
+    // attempt 1, only for a layer with a run too long to mend, sorts the 64-bit keys.
+    bool redo[2] = {true, true};
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
+      if (so != s) {                                  // the overlay's sort beside the base's
+        cudaEventRecord(fork, s);
+        cudaStreamWaitEvent(so, fork, 0);
+      }
+      for (int side = 0; side < 2; ++side) {
+        if (!redo[side]) continue;
+        cudaStream_t ss = side == 0 ? s : so;
+        const int64_t n = side == 0 ? nb : no, nv = side == 0 ? nvb : nvo;
+        uint64_t* key = side == 0 ? keyB : keyO;
+        uint32_t* id = side == 0 ? idB : idO;
+        const double* mbr = side == 0 ? J.mbr_b : J.mbr_o;
+        if (attempt == 1)
+          { x1_key64_kernel<<<blocks_for(n), kThreads, 0, ss>>>(mbr, side == 0 ? J.valid_b : J.valid_o, n, key, id); note_launch(); }
+        radix_sort_pairs(key, id, side == 0 ? kAlt : kAltO, side == 0 ? vAlt : vAltO, n, attempt == 0 ? 32 : 64,
+                         side == 0 ? tmp : tmpO, d_err, ss);
+        if (attempt == 0 && nv > 1)
+          { x1_fixup_kernel<<<blocks_for(nv), kThreads, 0, ss>>>(key, id, nv, mbr, d_cnt + 2 + side); note_launch(); }
+      }
+      if (so != s) {
+        cudaEventRecord(join, so);
+        cudaStreamWaitEvent(s, join, 0);
+      }
+      if (attempt == 0) mk->mark("join:mbr+sort", s);
+      if (nvb) { gather_sorted_kernel<<<blocks_for(nvb), kThreads, 0, s>>>(J.mbr_b, idB, nvb, SB); note_launch(); }
+      if (nvo) { gather_sorted_kernel<<<blocks_for(nvo), kThreads, 0, s>>>(J.mbr_o, idO, nvo, SO); note_launch(); }
+      // ---- J2 sweep: count, scan, emit, canonical sort
+      if (ne > 0) {
+        { (f32 ? sweep_kernel<0, 1> : sweep_kernel<0, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr,
+                                                                                                 nullptr, obits); note_launch(); }
+        exclusive_scan_i32(cnt, offs, ne, d_total, stmp, d_err, s);
+      } else {
+        cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
+      }
+      if (attempt == 0) mk->mark("join:sweep-count", s);
+      cudaMemcpyAsync(h_scratch, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(h_scratch + 1, d_cnt + 2, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+      redo[0] = h_scratch[1] != 0;
+      redo[1] = h_scratch[2] != 0;
+      if (!redo[0] && !redo[1]) break;
     }
-    mk->mark("join:sweep-count", s);
-    cudaMemcpyAsync(h_scratch, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
     K = h_scratch[0];
     J.n_pairs = K;
     if (K == 0) return ST_OK;

@@ -220,8 +220,31 @@ def test_grid_probe_equals_sort_sweep(engine, case):
         engine.set_tuning(join_sweep=True)
         sweep = _keys(engine, db, do)
     finally:
-        engine.set_tuning(join_sweep=False)
+        engine.set_tuning(join_sweep=True)             # the default
     assert grid.shape[1] > 0
     assert np.array_equal(grid, sweep)
     o = pyoracle.join(base, ovl)
     assert np.array_equal(grid[0], o.b) and np.array_equal(grid[1], o.o)
+
+
+@pytest.mark.parametrize("run", [40, 200, 1000])
+def test_sweep_sort_keys_equal_in_fp32(engine, run):
+    """The sweep sorts 32-bit keys (x1 rounded down to FP32) and mends runs of equal keys to
+    the exact (x1, id) order; runs longer than 256 send the layer to a 64-bit sort. Boxes
+    whose x1 differ by 1e-9 near 1e5 share their FP32 key: runs of 40, 200 and 1,000, with
+    and without equal x1, against the oracle's candidate list."""
+    import gcmfgh
+    rng = np.random.default_rng(run)
+    x1 = 1e5 + rng.permutation(run) * 1e-9
+    x1[: run // 4] = x1[0]                                # some equal x1 too
+    base = synth.Layer.from_rings([_box(x, 0.0, x + 0.5, 1.0) for x in x1] +
+                                  [_box(x, 0.0, x + 1.0, 1.0) for x in rng.uniform(0, 2e5, 300)])
+    ovl = synth.Layer.from_rings([_box(x + 0.25, 0.5, x + 2.0, 2.0) for x in x1[::-1]] +
+                                 [_box(x, 0.5, x + 1.0, 1.5) for x in rng.uniform(0, 2e5, 300)])
+    engine.set_tuning(join_sweep=True)
+    db, do = gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl)
+    engine.join(db, do)
+    o = pyoracle.join(base, ovl)
+    assert len(o.b) > run
+    assert np.array_equal(engine.join_field("b").reshape(-1), o.b)
+    assert np.array_equal(engine.join_field("o").reshape(-1), o.o)
