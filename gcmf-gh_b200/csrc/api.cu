@@ -216,17 +216,27 @@ ClipParams clip_params(const gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_
   return p;
 }
 
+// the last join's edge lists, for a clip of its clip set
+JoinEdges join_edges(const gcmfgh_ctx* c) {
+  JoinEdges e;
+  const JoinDev& J = c->join;
+  if (!J.clip_cand || !J.bOff) return e;
+  e.cand = J.clip_cand; e.flag = J.join_flag; e.bE = J.bE; e.oE = J.oE;
+  e.bOff = J.bOff; e.oOff = J.oOff; e.bList = J.bList; e.oList = J.oList;
+  return e;
+}
+
 gcmfgh_status run_clip_ctx(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o,
                            const int32_t* pid, const int32_t* qid, int64_t n, gcmfgh_clip_info* info,
                            const double* mbrB = nullptr, const double* mbrO = nullptr,
-                           const ClipParams* force = nullptr) {
+                           const ClipParams* force = nullptr, const JoinEdges* je = nullptr) {
   c->clip_arena.reset();
   c->have_clip = false;
   c->marks[1].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   const ClipParams prm = force ? *force : clip_params(c, b, o, n);
   int st = run_clip(to_dev(b), to_dev(o), pid, qid, n, prm, c->clip_arena, c->clip, c->d_err,
-                    c->h_scratch, c->stream, &c->marks[1], c->aux, nullptr, c->aux2, mbrB, mbrO);
+                    c->h_scratch, c->stream, &c->marks[1], c->aux, nullptr, c->aux2, mbrB, mbrO, je);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_clip = true;
@@ -619,8 +629,9 @@ gcmfgh_status gh_clip_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_
   cudaSetDevice(c->device);
   c->prm.no_swap = 0;
   // the join's polygon MBRs of the same layers (mbr_kernel computes what the clip would)
+  const JoinEdges je = join_edges(c);
   return run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, c->join.n_clip, info, c->join.mbr_b,
-                      c->join.mbr_o);
+                      c->join.mbr_o, nullptr, &je);
 }
 
 gcmfgh_status gcmfgh_tuning_for(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfgh_layer* o, int64_t n,
@@ -647,6 +658,7 @@ gcmfgh_status gcmfgh_autotune_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const
   cudaSetDevice(c->device);
   c->prm.no_swap = 0;
   const int64_t n = c->join.n_clip;
+  const JoinEdges je = join_edges(c);
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return GCMFGH_CUDA_ERROR;
   int timed = 0;
@@ -656,7 +668,7 @@ gcmfgh_status gcmfgh_autotune_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const
     gcmfgh_clip_info info;
     for (int r = 0; r < 3; ++r) {
       cudaEventRecord(e0, c->stream);
-      if (run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, n, &info, c->join.mbr_b, c->join.mbr_o, &p) !=
+      if (run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, n, &info, c->join.mbr_b, c->join.mbr_o, &p, &je) !=
           GCMFGH_OK)
         return -1.0f;
       cudaEventRecord(e1, c->stream);
@@ -669,7 +681,7 @@ gcmfgh_status gcmfgh_autotune_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const
   };
   ClipParams cur = clip_params(c, b, o, n);
   gcmfgh_clip_info warm;
-  run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, n, &warm, c->join.mbr_b, c->join.mbr_o, &cur);
+  run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, n, &warm, c->join.mbr_b, c->join.mbr_o, &cur, &je);
   const float ms0 = time_with(cur);
   if (ms0 < 0) { cudaEventDestroy(e0); cudaEventDestroy(e1); return GCMFGH_CUDA_ERROR; }
   float best = ms0;
@@ -718,7 +730,7 @@ gcmfgh_status gcmfgh_autotune_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const
   out->configs_timed = timed;
   // leave the clip result of the chosen thresholds in place
   gcmfgh_clip_info info;
-  return run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, n, &info, c->join.mbr_b, c->join.mbr_o, &cur);
+  return run_clip_ctx(c, b, o, c->join.clip_b, c->join.clip_o, n, &info, c->join.mbr_b, c->join.mbr_o, &cur, &je);
 }
 
 gcmfgh_status gh_clip_get(gcmfgh_ctx* c, int f, void* dst, int64_t cap, int on_dev, int64_t* bytes) {

@@ -67,6 +67,24 @@ struct JoinDev {
   double* mbr_o = nullptr;
   uint8_t* valid_b = nullptr;
   uint8_t* valid_o = nullptr;
+  int64_t* clip_cand = nullptr;  // [n_clip] each clip pair's candidate index
+  int64_t* bOff = nullptr;       // [n_pairs] first entry of each candidate's edge lists
+  int64_t* oOff = nullptr;
+  int32_t* bList = nullptr;      // edges of the common-MBR filter (join_flag pairs), ascending
+  int32_t* oList = nullptr;
+};
+
+// The join's common-MBR edge lists seen from its clip set (gh_clip_joined): the clip's
+// edge filter (G1) takes a pair's lists from here instead of testing every edge again.
+struct JoinEdges {
+  const int64_t* cand = nullptr;   // per clip pair: candidate index (null: no lists)
+  const int8_t* flag = nullptr;    // per candidate: lists present (join_flag)
+  const int32_t* bE = nullptr;
+  const int32_t* oE = nullptr;
+  const int64_t* bOff = nullptr;
+  const int64_t* oOff = nullptr;
+  const int32_t* bList = nullptr;
+  const int32_t* oList = nullptr;
 };
 
 // Clip parameters (reference defaults: EPSILON 1e-7 in GH-CUDA/lib/constants.h:4).
@@ -165,7 +183,7 @@ int run_clip(const LayerDev& base, const LayerDev& ovl, const int32_t* d_pid, co
              int64_t n_pairs, const ClipParams& prm, Arena& arena, ClipDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
              cudaStream_t aux = nullptr, RingExport* ex = nullptr, cudaStream_t aux2 = nullptr,
-             const double* mbrB = nullptr, const double* mbrO = nullptr);
+             const double* mbrB = nullptr, const double* mbrO = nullptr, const JoinEdges* je = nullptr);
 
 // One pair of multi-component polygons (rings: host, interleaved, open; ring c has
 // sizes[c] >= 3 vertices), P clipped against Q as given.  Result as one pair of ClipDev.

@@ -102,12 +102,23 @@ __global__ void setup_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict
 // W lanes per pair (W = 32: a warp).  Two passes split the pairs by ring size: narrow
 // tiles for small pairs (they also zero the counts of pairs with nothing to test), whole
 // warps for the rest.
+// A pair of a join's clip set whose candidate has the join's common-MBR edge lists (the
+// same boxes, the same test) takes them from there: the join tests every stored edge
+// including the zero-length one from the stored closing vertex back to the first
+// (GPU_Join.h:576-577), which the clip's open ring does not have, so that entry (the last,
+// index n) is dropped; and both rings must be closed (stored closing vertex equal to the
+// first), so that the join's last real edge is the clip's.
+__device__ __forceinline__ bool ring_closed(const double2* v, int n) {
+  const double2 a = __ldg(v), b = __ldg(v + n);
+  return a.x == b.x && a.y == b.y;
+}
+
 template <int kMode, int W>
 __global__ void __launch_bounds__(kThreads, 6)
 edge_filter_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, int32_t* __restrict__ cP,
                    int32_t* __restrict__ cQ, const int64_t* __restrict__ offP,
                    const int64_t* __restrict__ offQ, int32_t* __restrict__ LP, int32_t* __restrict__ LQ,
-                   int64_t lo, int64_t hi) {
+                   int64_t lo, int64_t hi, JoinEdges je) {
   constexpr unsigned kBits = (W == 32) ? 0xffffffffu : ((1u << (W & 31)) - 1u);
   const int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) / W;
   const int tl = (int)(threadIdx.x & (W - 1));
@@ -119,8 +130,28 @@ edge_filter_kernel(LayerDev Lb, LayerDev Lo, PairDev D, int64_t K, int32_t* __re
     const int64_t size = (int64_t)D.nP[w] + D.nQ[w];
     if (size <= lo || size > hi) return;             // the other pass takes this pair
   }
-  double4 c = reinterpret_cast<const double4*>(D.cmbr)[w];
   const int pside = D.pSide[w];
+  if (je.cand) {
+    const int64_t cd = je.cand[w];
+    if (je.flag[cd] && ring_closed(layer_xy(Lb, Lo, pside) + D.pS[w], D.nP[w]) &&
+        ring_closed(layer_xy(Lb, Lo, 1 - pside) + D.qS[w], D.nQ[w])) {
+      for (int side = 0; side < 2; ++side) {
+        const bool base = (side == 0 ? pside : 1 - pside) == 0;
+        const int n = side == 0 ? D.nP[w] : D.nQ[w];
+        const int E = (base ? je.bE : je.oE)[cd];
+        const int32_t* src = base ? je.bList + je.bOff[cd] : je.oList + je.oOff[cd];
+        const int cnt = E - ((E > 0 && src[E - 1] == n) ? 1 : 0);
+        if (kMode == 0) {
+          if (tl == 0) (side == 0 ? cP : cQ)[w] = cnt;
+        } else {
+          int32_t* dst = side == 0 ? LP + offP[w] : LQ + offQ[w];
+          for (int j = tl; j < cnt; j += W) dst[j] = src[j];
+        }
+      }
+      return;
+    }
+  }
+  double4 c = reinterpret_cast<const double4*>(D.cmbr)[w];
   for (int side = 0; side < 2; ++side) {
     const double2* v = layer_xy(Lb, Lo, side == 0 ? pside : 1 - pside) + (side == 0 ? D.pS[w] : D.qS[w]);
     const int n = side == 0 ? D.nP[w] : D.nQ[w];
@@ -3497,10 +3528,11 @@ out_compact_kernel(int64_t K, const double* __restrict__ xy, const int64_t* __re
 int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const int32_t* d_qid,
              int64_t K, const ClipParams& prm, Arena& A, ClipDev& C, int* d_err, int64_t* hs,
              cudaStream_t s, Marks* mk, cudaStream_t aux, RingExport* ex, cudaStream_t aux2,
-             const double* mbrB, const double* mbrO) {
+             const double* mbrB, const double* mbrO, const JoinEdges* je) {
   Marks dummy;
   if (!mk) mk = &dummy;
   C = ClipDev();
+  const JoinEdges jed = je ? *je : JoinEdges{};
   mk->mark("clip:start", s);
   C.n_pairs = K;
   if (K <= 0) return ST_OK;
@@ -3554,10 +3586,10 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   // ---- G1 edge filter
   fork_aux();
   { edge_filter_kernel<0, kFilterTile><<<(unsigned)((K * kFilterTile + kThreads - 1) / kThreads), kThreads, 0, s>>>(
-        Lb, Lo, D, K, cP, cQ, nullptr, nullptr, nullptr, nullptr, -1, kFilterTileMax); note_launch(); }
+        Lb, Lo, D, K, cP, cQ, nullptr, nullptr, nullptr, nullptr, -1, kFilterTileMax, jed); note_launch(); }
   { edge_filter_kernel<0, 32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, D, K, cP, cQ, nullptr, nullptr,
                                                                        nullptr, nullptr, kFilterTileMax,
-                                                                       INT64_MAX); note_launch(); }
+                                                                       INT64_MAX, jed); note_launch(); }
   join_aux();
   exclusive_scan_i32(cP, offP, K, tot + 0, stK, d_err, s);
   exclusive_scan_i32(cQ, offQ, K, tot + 1, stK, d_err, s);
@@ -3608,9 +3640,9 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   cudaMemsetAsync(binQ, 0, K * sizeof(int64_t), s);
   fork_aux();
   { edge_filter_kernel<1, kFilterTile><<<(unsigned)((K * kFilterTile + kThreads - 1) / kThreads), kThreads, 0, s>>>(
-        Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ, -1, kFilterTileMax); note_launch(); }
+        Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ, -1, kFilterTileMax, jed); note_launch(); }
   { edge_filter_kernel<1, 32><<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, D, K, cP, cQ, offP, offQ, LP, LQ,
-                                                                       kFilterTileMax, INT64_MAX); note_launch(); }
+                                                                       kFilterTileMax, INT64_MAX, jed); note_launch(); }
   join_aux();
   // The binned pairs (below) go to the auxiliary stream when there is one: fork here, before
   // the chunked count is queued on s, so that the two run side by side.

@@ -517,11 +517,13 @@ __global__ void clip_flag_kernel(const int8_t* __restrict__ pip_type, const int8
 
 __global__ void clip_compact_kernel(const int8_t* __restrict__ clip, const int64_t* __restrict__ off,
                                     const int32_t* __restrict__ b, const int32_t* __restrict__ o,
-                                    int64_t K, int32_t* __restrict__ cb, int32_t* __restrict__ co) {
+                                    int64_t K, int32_t* __restrict__ cb, int32_t* __restrict__ co,
+                                    int64_t* __restrict__ cand) {
   int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
   if (k >= K || !clip[k]) return;
   cb[off[k]] = b[k];
   co[off[k]] = o[k];
+  cand[off[k]] = k;
 }
 
 // MBRs only (the clip pipeline's common MBRs), same definition as mbr_kernel
@@ -867,8 +869,11 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
   J.n_seg = h_scratch[4];
   J.clip_b = A.take_n<int32_t>(J.n_clip);
   J.clip_o = A.take_n<int32_t>(J.n_clip);
-  if (!J.clip_b || !J.clip_o) return ST_OUT_OF_MEMORY;
-  { clip_compact_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.clip, clipOff, J.b, J.o, K, J.clip_b, J.clip_o); note_launch(); }
+  J.clip_cand = A.take_n<int64_t>(J.n_clip);
+  if (!J.clip_b || !J.clip_o || !J.clip_cand) return ST_OUT_OF_MEMORY;
+  { clip_compact_kernel<<<blocks_for(K), kThreads, 0, s>>>(J.clip, clipOff, J.b, J.o, K, J.clip_b, J.clip_o,
+                                                         J.clip_cand); note_launch(); }
+  J.bOff = bOff; J.oOff = oOff; J.bList = bList; J.oList = oList;
   mk->mark("join:clipset", s);
   return ST_OK;
 }

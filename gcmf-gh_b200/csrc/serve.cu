@@ -277,7 +277,10 @@ int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64
       prm.eps_clean = opt.eps_clean;
       prm.union_mode = opt.union_mode ? 1 : 0;
       prm.exact = opt.exact ? 1 : 0;
-      st = run_clip(Lq, resident(), J.clip_b, J.clip_o, J.n_clip, prm, C, CD, d_err, h_scratch, s, nullptr, aux);
+      // the clip's edge filter takes the join's common-MBR edge lists of the clip set
+      const JoinEdges je{J.clip_cand, J.join_flag, J.bE, J.oE, J.bOff, J.oOff, J.bList, J.oList};
+      st = run_clip(Lq, resident(), J.clip_b, J.clip_o, J.n_clip, prm, C, CD, d_err, h_scratch, s, nullptr, aux,
+                    nullptr, nullptr, nullptr, nullptr, &je);
       if (st != ST_OK) return st;
     }
   } else {

@@ -248,3 +248,19 @@ def test_sweep_sort_keys_equal_in_fp32(engine, run):
     assert len(o.b) > run
     assert np.array_equal(engine.join_field("b").reshape(-1), o.b)
     assert np.array_equal(engine.join_field("o").reshape(-1), o.o)
+
+
+def test_clip_of_join_takes_join_edge_lists(engine):
+    """gh_clip_joined takes each clip pair's common-MBR edge lists from the join (dropping
+    the join's zero-length closing edge) when both rings are closed, and tests the edges
+    itself otherwise: a layer pair with every tenth stored closing vertex moved off the
+    first vertex gives the oracle's join and clip either way."""
+    import gcmfgh
+    base, ovl = synth.small_join(21, 3000)
+    xy = base.xy.reshape(-1, 2).copy()
+    for i in range(0, base.n_polys, 10):
+        xy[int(base.vps[i]) - 1] += 1e-3                  # the stored closing vertex
+    base = synth.Layer(xy, base.vnum)
+    db, do, info, _ = _join_equal(engine, base, ovl)
+    assert info["n_clip"] > 1000
+    _clip_equal(engine, db, do, base, ovl)
