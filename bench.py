@@ -11,7 +11,7 @@ The unit is one clipped polygon pair.  Under torchrun the ranks split that one w
 rank r joins and clips its x-slab of base polygons (equal counts by MBR x1) against the
 whole overlay layer, with no data-path collective (strong scaling).
 
-value: each rank runs the K timed steps on --lanes contexts (default 3), each on its own
+value: each rank runs the K timed steps on --lanes contexts (default 4), each on its own
 CUDA stream and host thread and taking every lanes-th step, so that one context's kernels
 run while another waits on a size read-back; every step starts with an L2 flush.  The
 time is the device time from a common start event to the last lane's end event, the
@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-component pairs")
     ap.add_argument("--join-sweep", type=int, default=None,
                     help="1: MBR candidates by the sort-sweep, 0: by the grid probe (default: the library's)")
-    ap.add_argument("--lanes", type=int, default=3,
+    ap.add_argument("--lanes", type=int, default=4,
                     help="contexts (and host threads) of the pipelined measurement; 1 skips it")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default size-bucket thresholds")
     ap.add_argument("--fused-emit", type=int, default=None,
