@@ -160,6 +160,9 @@ def stage_bytes(stage, ji, ci, nb, no, vb, vo, cand_vertices=0):
         "join:cand-emit+sort": 32 * (nb + no) + 16 * K,
         "join:sweep-count": 36 * (nb + no),
         "join:sweep-emit+sort": 36 * (nb + no) + 16 * K,
+        # one-pass sweep: the x1-sorted MBRs read once, the keys written; then their sort
+        "join:sweep": 36 * (nb + no) + 8 * K,
+        "join:sort": 16 * K,
         "join:cmf": 16 * cand_vertices + 40 * K,
     }
     return table.get(stage)

@@ -108,8 +108,10 @@ struct gcmfgh_ctx {
   std::string gpu_name;
   bool tuning_explicit = false;   // gcmfgh_set_tuning was called: recorded tunings are not applied
   int join_f32 = 5;               // join options: FP32 prefilters (bit 0 MBR y test, bit 1 edge test),
-                                  // bit 2 the sort-sweep MBR filter instead of the grid probe
+                                  // bit 2 the sort-sweep MBR filter instead of the grid probe,
+                                  // bit 3 the sweep as count and emit passes
   bool hint_explicit = false;     // gcmfgh_set_tuning fixed the record capacity hint
+  int64_t cand_hint = 0;          // MBR candidates of the last join (the one-pass sweep's capacity)
   std::vector<TuneRecord> tunings;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
@@ -515,11 +517,15 @@ gcmfgh_status gcmfgh_set_precision(gcmfgh_ctx* c, int mode) {
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* c, int key, int64_t value) {
   if (!c || value < 0) return GCMFGH_INVALID_ARGUMENT;
   if (key == GCMFGH_TUNE_F32_FILTER) {
-    c->join_f32 = (c->join_f32 & 4) | (int)(value & 3);
+    c->join_f32 = (c->join_f32 & 12) | (int)(value & 3);
+    return GCMFGH_OK;
+  }
+  if (key == GCMFGH_TUNE_SWEEP_TWO_PASS) {
+    c->join_f32 = (c->join_f32 & 7) | (value ? 8 : 0);
     return GCMFGH_OK;
   }
   if (key == GCMFGH_TUNE_JOIN_SWEEP) {
-    c->join_f32 = (c->join_f32 & 3) | (value ? 4 : 0);
+    c->join_f32 = (c->join_f32 & 11) | (value ? 4 : 0);
     return GCMFGH_OK;
   }
   if (key == GCMFGH_TUNE_FUSED_EMIT) {
@@ -558,10 +564,11 @@ static gcmfgh_status join_impl(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfg
   c->marks[0].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   int st = run_join(to_dev(b), to_dev(o), c->join_arena, c->join, c->d_err, c->h_scratch, c->stream,
-                    &c->marks[0], c->aux, c->join_f32, ovl_ready);
+                    &c->marks[0], c->aux, c->join_f32, ovl_ready, c->cand_hint);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_join = true;
+  c->cand_hint = c->join.n_pairs;                  // the next join's key capacity
   c->join_b = b->coords;
   c->join_o = o->coords;
   c->join_nb = b->n_polys;

@@ -140,7 +140,8 @@ int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s);
 // base layer's on s.
 int run_join(const LayerDev& base, const LayerDev& ovl, Arena& arena, JoinDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
-             cudaStream_t aux = nullptr, int f32 = 0, cudaEvent_t ovl_ready = nullptr);
+             cudaStream_t aux = nullptr, int f32 = 0, cudaEvent_t ovl_ready = nullptr,
+             int64_t cand_hint = 0);
 
 int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys, int64_t K, int obits,
                    Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,

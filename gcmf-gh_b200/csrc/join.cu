@@ -283,6 +283,80 @@ sweep_kernel(SortedMbr B, SortedMbr O, int32_t* __restrict__ cnt, const int64_t*
   if (kMode == 0 && lane_id() == 0) cnt[w] = c;
 }
 
+// The sweep's count and emit in one pass: the same range scan and tests as sweep_kernel,
+// with each warp staging its keys in shared memory (up to kSweepStage; a fuller stage is
+// appended by the warp itself) and the block appending all staged keys at one range of a
+// global counter.  Keys land in no particular order (the caller sorts them); those at or
+// past cap are counted and not written, and the caller runs the pass again with room for
+// the counted total.
+constexpr int kSweepStage = 64;
+template <int kF32>
+__global__ void __launch_bounds__(kThreads, 8)
+sweep_append_kernel(SortedMbr B, SortedMbr O, uint64_t* __restrict__ keys, int64_t cap,
+                    unsigned long long* __restrict__ total, int obits) {
+  __shared__ uint64_t stage[kWarpsPerBlock][kSweepStage];
+  __shared__ int sOff[kWarpsPerBlock + 1];
+  __shared__ unsigned long long sBase;
+  const int wib = (int)(threadIdx.x >> 5);
+  const int64_t w = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  int staged = 0;
+  if (w < B.n + O.n) {
+    const bool base_side = w < B.n;
+    const SortedMbr& me = base_side ? B : O;
+    const SortedMbr& ot = base_side ? O : B;
+    const int64_t i = base_side ? w : w - B.n;
+    const double mx1 = me.x1[i], mx2 = me.x2[i], my1 = me.y1[i], my2 = me.y2[i];
+    const float my1d = kF32 ? __double2float_rd(my1) : 0.f, my2u = kF32 ? __double2float_ru(my2) : 0.f;
+    int64_t lo, hi;
+    if (base_side) { lo = lower_bound_d(ot.x1, ot.n, mx1); hi = lower_bound_d(ot.x1, ot.n, mx2); }
+    else { lo = upper_bound_d(ot.x1, ot.n, mx1); hi = upper_bound_d(ot.x1, ot.n, mx2); }
+    const uint64_t myid = me.id[i];
+    for (int64_t k0 = lo; k0 < hi; k0 += 32) {
+      const int64_t k = k0 + lane_id();
+      bool hit = false;
+      if (k < hi) {
+        if (kF32) {
+          const float2 q = ot.yf[k];
+          hit = q.x <= my2u && my1d <= q.y;
+          if (hit) hit = ot.y1[k] <= my2 && my1 <= ot.y2[k];
+        } else {
+          hit = ot.y1[k] <= my2 && my1 <= ot.y2[k];
+        }
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      const int nh = __popc(m);
+      if (staged + nh > kSweepStage) {              // append the full stage now
+        unsigned long long b = 0;
+        if (lane_id() == 0) b = atomicAdd(total, (unsigned long long)staged);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        for (int j = lane_id(); j < staged; j += 32)
+          if ((int64_t)b + j < cap) keys[b + j] = stage[wib][j];
+        __syncwarp();
+        staged = 0;
+      }
+      if (hit) {
+        const uint64_t oid = ot.id[k];
+        const uint64_t bb = base_side ? myid : oid, oo = base_side ? oid : myid;
+        stage[wib][staged + __popc(m & lanemask_lt())] = (bb << obits) | oo;
+      }
+      __syncwarp();
+      staged += nh;
+    }
+  }
+  if (lane_id() == 0) sOff[wib] = staged;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int j = 0; j < kWarpsPerBlock; ++j) { const int n = sOff[j]; sOff[j] = run; run += n; }
+    sOff[kWarpsPerBlock] = run;
+    sBase = run ? atomicAdd(total, (unsigned long long)run) : 0ull;
+  }
+  __syncthreads();
+  const int64_t base = (int64_t)sBase + sOff[wib];
+  for (int j = lane_id(); j < staged; j += 32)
+    if (base + j < cap) keys[base + j] = stage[wib][j];
+}
+
 // ---------------------------------------------------------------- J3: common MBR
 // GPU_Join.h:468-506: CMBR = intersection of the FP64 MBRs; pip_type 1 when the base
 // MBR equals the CMBR (the overlay may contain the base), 2 when the overlay MBR does.
@@ -557,11 +631,13 @@ int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s) {
 }
 
 int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int* d_err,
-             int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux, int f32, cudaEvent_t ovl_ready) {
+             int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux, int f32, cudaEvent_t ovl_ready,
+             int64_t cand_hint) {
   // f32 bit 0: FP32 prefilter of the sweep's y test; bit 1: of the common-MBR edge test
   // (needs the layers' vertex counts, for their FP32 copies)
   const bool f32cmf = (f32 & 2) && Lb0.nverts > 0 && Lo0.nverts > 0;
   const bool forceSweep = (f32 & 4) != 0;          // bit 2: the sort-sweep MBR filter, never the grid
+  const int joinOpts = f32;                         // bit 3: the sweep's count and emit as two passes
   f32 &= 1;
   LayerDev Lb = Lb0, Lo = Lo0;
   Marks dummy;
@@ -707,6 +783,15 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
       return ST_OUT_OF_MEMORY;
     // Attempt 0 sorts the 32-bit keys of mbr_kernel and mends the runs of equal keys;
     // attempt 1, only for a layer with a run too long to mend, sorts the 64-bit keys.
+    // One-pass sweep: the keys go straight into an array sized from the last join's
+    // candidate count (with room to spare) or a first guess of 8 per polygon.
+    const bool fusedSweep = !(joinOpts & 8);
+    int64_t keyCap = 0;
+    if (fusedSweep) {
+      keyCap = cand_hint > 0 ? cand_hint + cand_hint / 4 + 65536 : 8 * ne + 65536;
+      pkeys = A.take_n<uint64_t>(keyCap);
+      if (!pkeys) return ST_OUT_OF_MEMORY;
+    }
     bool redo[2] = {true, true};
     for (int attempt = 0; attempt < 2; ++attempt) {
       // ---- J1 sort both layers by x1 (stable: equal x1 keep ascending id)
@@ -735,15 +820,20 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
       if (attempt == 0) mk->mark("join:mbr+sort", s);
       if (nvb) { gather_sorted_kernel<<<blocks_for(nvb), kThreads, 0, s>>>(J.mbr_b, idB, nvb, SB); note_launch(); }
       if (nvo) { gather_sorted_kernel<<<blocks_for(nvo), kThreads, 0, s>>>(J.mbr_o, idO, nvo, SO); note_launch(); }
-      // ---- J2 sweep: count, scan, emit, canonical sort
-      if (ne > 0) {
+      // ---- J2 sweep: count + emit in one pass (or count, scan, emit), then the canonical sort
+      if (fusedSweep) {
+        cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
+        if (ne > 0)
+          { (f32 ? sweep_append_kernel<1> : sweep_append_kernel<0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(
+                SB, SO, pkeys, keyCap, reinterpret_cast<unsigned long long*>(d_total), obits); note_launch(); }
+      } else if (ne > 0) {
         { (f32 ? sweep_kernel<0, 1> : sweep_kernel<0, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, cnt, nullptr,
                                                                                                  nullptr, obits); note_launch(); }
         exclusive_scan_i32(cnt, offs, ne, d_total, stmp, d_err, s);
       } else {
         cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
       }
-      if (attempt == 0) mk->mark("join:sweep-count", s);
+      if (attempt == 0) mk->mark(fusedSweep ? "join:sweep" : "join:sweep-count", s);
       cudaMemcpyAsync(h_scratch, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
       cudaMemcpyAsync(h_scratch + 1, d_cnt + 2, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
       if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
@@ -754,16 +844,25 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
     K = h_scratch[0];
     J.n_pairs = K;
     if (K == 0) return ST_OK;
-    pkeys = A.take_n<uint64_t>(K);
+    if (fusedSweep && K > keyCap) {               // the key array was short: again, at the counted size
+      keyCap = K;
+      pkeys = A.take_n<uint64_t>(K);
+      if (!pkeys) return ST_OUT_OF_MEMORY;
+      cudaMemsetAsync(d_total, 0, sizeof(int64_t), s);
+      { (f32 ? sweep_append_kernel<1> : sweep_append_kernel<0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(
+            SB, SO, pkeys, keyCap, reinterpret_cast<unsigned long long*>(d_total), obits); note_launch(); }
+    }
+    if (!fusedSweep) pkeys = A.take_n<uint64_t>(K);
     uint32_t* pvals = A.take_n<uint32_t>(K);
     uint64_t* pkAlt = A.take_n<uint64_t>(K);
     uint32_t* pvAlt = A.take_n<uint32_t>(K);
     void* rtmp = A.take(radix_temp_bytes(K));
     if (!pkeys || !pvals || !pkAlt || !pvAlt || !rtmp) return ST_OUT_OF_MEMORY;
-    { (f32 ? sweep_kernel<1, 1> : sweep_kernel<1, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs,
-                                                                                             pkeys, obits); note_launch(); }
+    if (!fusedSweep)
+      { (f32 ? sweep_kernel<1, 1> : sweep_kernel<1, 0>)<<<blocks_for_warps(ne), kThreads, 0, s>>>(SB, SO, nullptr, offs,
+                                                                                               pkeys, obits); note_launch(); }
     radix_sort_pairs(pkeys, pvals, pkAlt, pvAlt, K, ((obits + bbits + 7) / 8) * 8, rtmp, d_err, s);
-    mk->mark("join:sweep-emit+sort", s);
+    mk->mark(fusedSweep ? "join:sort" : "join:sweep-emit+sort", s);
   }
   if (K == 0) return ST_OK;
   return join_from_keys(Lb, Lo, pkeys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, mk, aux);

@@ -255,7 +255,8 @@ class Engine:
         return lib().gcmfgh_last_device_error(self.h)
 
     def set_tuning(self, bin_grid=None, big_label=None, mid_label=None, tile_label=None, wide_label=None,
-                   f32_filter=None, fused_emit=None, record_hint=None, join_sweep=None):
+                   f32_filter=None, fused_emit=None, record_hint=None, join_sweep=None,
+                   sweep_two_pass=None):
         """Work-distribution thresholds, the join's FP32 prefilters, the one-pass record
         count + emit and its capacity hint (results depend on none of them)."""
         if f32_filter is not None:      # bit 0: MBR y prefilter, bit 1: edge prefilter
@@ -266,6 +267,8 @@ class Engine:
             _check(lib().gcmfgh_set_tuning(self.h, 7, int(record_hint)))
         if join_sweep is not None:      # MBR candidates by the sort-sweep instead of the grid probe
             _check(lib().gcmfgh_set_tuning(self.h, 8, 1 if join_sweep else 0))
+        if sweep_two_pass is not None:  # the sweep's count and emit as two passes
+            _check(lib().gcmfgh_set_tuning(self.h, 9, 1 if sweep_two_pass else 0))
         if bin_grid is not None:
             _check(lib().gcmfgh_set_tuning(self.h, 0, int(bin_grid)))
         if big_label is not None:
