@@ -112,6 +112,7 @@ struct gcmfgh_ctx {
                                   // bit 3 the sweep as count and emit passes
   bool hint_explicit = false;     // gcmfgh_set_tuning fixed the record capacity hint
   int64_t cand_hint = 0;          // MBR candidates of the last join (the one-pass sweep's capacity)
+  int64_t list_hint[2] = {0, 0};  // common-MBR edge list entries of the last join (the one-pass filter's)
   std::vector<TuneRecord> tunings;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
@@ -564,11 +565,14 @@ static gcmfgh_status join_impl(gcmfgh_ctx* c, const gcmfgh_layer* b, const gcmfg
   c->marks[0].n = 0;
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   int st = run_join(to_dev(b), to_dev(o), c->join_arena, c->join, c->d_err, c->h_scratch, c->stream,
-                    &c->marks[0], c->aux, c->join_f32, ovl_ready, c->cand_hint);
+                    &c->marks[0], c->aux, c->join_f32, ovl_ready, c->cand_hint, c->list_hint[0],
+                    c->list_hint[1]);
   gcmfgh_status r = finish(c, st);
   if (r != GCMFGH_OK) return r;
   c->have_join = true;
-  c->cand_hint = c->join.n_pairs;                  // the next join's key capacity
+  c->cand_hint = c->join.n_pairs;                  // the next join's key and list capacities
+  c->list_hint[0] = c->join.n_blist;
+  c->list_hint[1] = c->join.n_olist;
   c->join_b = b->coords;
   c->join_o = o->coords;
   c->join_nb = b->n_polys;

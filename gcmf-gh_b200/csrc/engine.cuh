@@ -72,6 +72,7 @@ struct JoinDev {
   int64_t* oOff = nullptr;
   int32_t* bList = nullptr;      // edges of the common-MBR filter (join_flag pairs), ascending
   int32_t* oList = nullptr;
+  int64_t n_blist = 0, n_olist = 0;   // list entries (the next join's capacity hints)
 };
 
 // The join's common-MBR edge lists seen from its clip set (gh_clip_joined): the clip's
@@ -141,12 +142,12 @@ int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s);
 int run_join(const LayerDev& base, const LayerDev& ovl, Arena& arena, JoinDev& out,
              int* d_err, int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
              cudaStream_t aux = nullptr, int f32 = 0, cudaEvent_t ovl_ready = nullptr,
-             int64_t cand_hint = 0);
+             int64_t cand_hint = 0, int64_t list_hint_b = 0, int64_t list_hint_o = 0);
 
 int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys, int64_t K, int obits,
                    Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,
                    int64_t* h_scratch, cudaStream_t s, Marks* marks = nullptr,
-                   cudaStream_t aux = nullptr);
+                   cudaStream_t aux = nullptr, int64_t hintB = 0, int64_t hintO = 0, bool twoPass = false);
 
 // Merged rings of pair 0 after the neighbour links, as the reference's
 // calculateIntersections hands them back (gppolyclip_mDIV512.cu:1298-1640): vertices in

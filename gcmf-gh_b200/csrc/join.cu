@@ -494,6 +494,105 @@ cmf_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32
   }
 }
 
+// The common-MBR filter's count and lists in one pass.  Each tile (W lanes per pair) tests
+// its pair's edges once to count them, as cmf_kernel's count pass does; the block then takes
+// one range of each list array for all its pairs (two atomics per block), and each tile
+// tests its edges again, from L1, to write them in ascending order at its pair's offset.
+// A pair's lists stay contiguous and ascending; pairs sit in no particular order
+// (bOff/oOff say where).  Entries at or past cap are counted and not written: the caller
+// runs the pass again with room for the counted totals.
+struct CmfOut {
+  int64_t* bOff; int64_t* oOff;
+  int32_t* bList; int32_t* oList;
+  int64_t bCap, oCap;
+  unsigned long long* total;     // [2] entries taken so far (base, overlay)
+};
+
+template <int W, int kF32>
+__global__ void __launch_bounds__(kThreads, 8)
+cmf_append_kernel(LayerDev Lb, LayerDev Lo, const int32_t* __restrict__ pb, const int32_t* __restrict__ po,
+                  const double* __restrict__ cmbr, int64_t K, int8_t* __restrict__ join_flag,
+                  int32_t* __restrict__ bE, int32_t* __restrict__ oE, CmfOut out, int64_t lo, int64_t hi) {
+  constexpr int kTiles = kThreads / W;
+  __shared__ int sCnt[2][kTiles];
+  __shared__ unsigned long long sBase[2];
+  const JTile<W> T;
+  const int64_t w = JTile<W>::unit();
+  const int tib = (int)(threadIdx.x / W);
+  bool mine = w < K && join_flag[w];
+  if (w < K && !join_flag[w] && W != 32 && T.lane == 0) { bE[w] = 0; oE[w] = 0; }
+  if (mine) {
+    const int64_t size = (int64_t)Lb.vnum[pb[w]] + Lo.vnum[po[w]];
+    mine = size > lo && size <= hi;                 // else the other pass takes this pair
+  }
+  double4 c = make_double4(0, 0, 0, 0);
+  float cx1d = 0.f, cy1d = 0.f, cx2u = 0.f, cy2u = 0.f;
+  int counts[2] = {0, 0};
+  if (mine) {
+    c = reinterpret_cast<const double4*>(cmbr)[w];
+    if (kF32) {
+      cx1d = __double2float_rd(c.x); cy1d = __double2float_rd(c.y);
+      cx2u = __double2float_ru(c.z); cy2u = __double2float_ru(c.w);
+    }
+  }
+  // pass 0 counts, pass 1 writes
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {
+      if (T.lane == 0) {
+        const bool keep = mine && counts[0] > 0 && counts[1] > 0;
+        sCnt[0][tib] = keep ? counts[0] : 0;
+        sCnt[1][tib] = keep ? counts[1] : 0;
+        if (mine && !keep) { join_flag[w] = 0; bE[w] = 0; oE[w] = 0; }
+      }
+      __syncthreads();
+      if (threadIdx.x < 2) {
+        int run = 0;
+        for (int j = 0; j < kTiles; ++j) { const int n = sCnt[threadIdx.x][j]; sCnt[threadIdx.x][j] = run; run += n; }
+        sBase[threadIdx.x] = run ? atomicAdd(out.total + threadIdx.x, (unsigned long long)run) : 0ull;
+      }
+      __syncthreads();
+      if (!(mine && counts[0] > 0 && counts[1] > 0)) break;
+      if (T.lane == 0) {
+        out.bOff[w] = (int64_t)sBase[0] + sCnt[0][tib];
+        out.oOff[w] = (int64_t)sBase[1] + sCnt[1][tib];
+        bE[w] = counts[0];
+        oE[w] = counts[1];
+      }
+    } else if (!mine) {
+      continue;
+    }
+    for (int side = 0; side < 2; ++side) {
+      const LayerDev& L = side == 0 ? Lb : Lo;
+      const int id = side == 0 ? pb[w] : po[w];
+      const int nv = L.vnum[id];
+      const double2* v = reinterpret_cast<const double2*>(L.xy) + (L.vps[id] - nv);
+      const float2* vf = kF32 ? L.xyf + (L.vps[id] - nv) : nullptr;
+      const int64_t pos = pass == 1 ? (int64_t)sBase[side] + sCnt[side][tib] : 0;
+      int32_t* list = side == 0 ? out.bList : out.oList;
+      const int64_t cap = side == 0 ? out.bCap : out.oCap;
+      int cnt = 0;
+      for (int k0 = 0; k0 < nv; k0 += W) {
+        const int k = k0 + T.lane;
+        bool hit = false;
+        if (k < nv) {
+          const int k2 = (k < nv - 1) ? k + 1 : 0;
+          if (!kF32 || !f32_rejects(__ldg(vf + k), __ldg(vf + k2), cx1d, cy1d, cx2u, cy2u)) {
+            const double2 a = __ldg(v + k), b = __ldg(v + k2);
+            hit = edge_touches_box(a.x, a.y, b.x, b.y, c.x, c.y, c.z, c.w);
+          }
+        }
+        const unsigned m = T.ballot(hit);
+        if (pass == 1 && hit) {
+          const int64_t r = pos + cnt + __popc(m & T.lanes_below());
+          if (r < cap) list[r] = k;
+        }
+        cnt += __popc(m);
+      }
+      if (pass == 0) counts[side] = cnt;
+    }
+  }
+}
+
 // ---------------------------------------------------------------- J6: refine
 // Does any surviving (base edge, overlay edge) pair intersect?  The closed-form test of
 // GPU_Join.h:373-446 in its operation order: zero-length base edges are skipped, box
@@ -632,7 +731,7 @@ int layer_mbrs(const LayerDev& L, double* mbr, cudaStream_t s) {
 
 int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int* d_err,
              int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux, int f32, cudaEvent_t ovl_ready,
-             int64_t cand_hint) {
+             int64_t cand_hint, int64_t list_hint_b, int64_t list_hint_o) {
   // f32 bit 0: FP32 prefilter of the sweep's y test; bit 1: of the common-MBR edge test
   // (needs the layers' vertex counts, for their FP32 copies)
   const bool f32cmf = (f32 & 2) && Lb0.nverts > 0 && Lo0.nverts > 0;
@@ -811,7 +910,7 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
         radix_sort_pairs(key, id, side == 0 ? kAlt : kAltO, side == 0 ? vAlt : vAltO, n, attempt == 0 ? 32 : 64,
                          side == 0 ? tmp : tmpO, d_err, ss);
         if (attempt == 0 && nv > 1)
-          { x1_fixup_kernel<<<blocks_for(nv), kThreads, 0, ss>>>(key, id, nv, mbr, d_cnt + 2 + side); note_launch(); }
+          { x1_fixup_kernel<<<blocks_for(nv), kThreads, 0, ss>>>(key, id, nv, mbr, d_cnt + 6 + side); note_launch(); }
       }
       if (so != s) {
         cudaEventRecord(join, so);
@@ -835,7 +934,7 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
       }
       if (attempt == 0) mk->mark(fusedSweep ? "join:sweep" : "join:sweep-count", s);
       cudaMemcpyAsync(h_scratch, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-      cudaMemcpyAsync(h_scratch + 1, d_cnt + 2, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(h_scratch + 1, d_cnt + 6, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);   // fix-up flags
       if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
       redo[0] = h_scratch[1] != 0;
       redo[1] = h_scratch[2] != 0;
@@ -865,7 +964,8 @@ int run_join(const LayerDev& Lb0, const LayerDev& Lo0, Arena& A, JoinDev& J, int
     mk->mark(fusedSweep ? "join:sort" : "join:sweep-emit+sort", s);
   }
   if (K == 0) return ST_OK;
-  return join_from_keys(Lb, Lo, pkeys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, mk, aux);
+  return join_from_keys(Lb, Lo, pkeys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, mk, aux, list_hint_b,
+                        list_hint_o, (joinOpts & 8) != 0);
 }
 
 // Stages J3-J6 and the clip set over candidate pairs given as packed keys
@@ -877,7 +977,8 @@ constexpr int64_t kJoinTileMax = 64;
 
 int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys, int64_t K, int obits,
                    Arena& A, JoinDev& J, int64_t* d_total, unsigned long long* d_cnt, int* d_err,
-                   int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux) {
+                   int64_t* h_scratch, cudaStream_t s, Marks* mk, cudaStream_t aux, int64_t hintB,
+                   int64_t hintO, bool twoPass) {
   Marks dummy;
   if (!mk) mk = &dummy;
   J.n_pairs = K;
@@ -919,30 +1020,60 @@ int join_from_keys(const LayerDev& Lb, const LayerDev& Lo, const uint64_t* pkeys
   join_aux();
   mk->mark("join:cmbr+pip", s);
   // ---- J5 common-MBR edge filter: count, offsets, lists
-  fork_aux();
   const bool f32 = Lb.xyf && Lo.xyf;
-  { (f32 ? cmf_kernel<0, kJoinTile, 1> : cmf_kernel<0, kJoinTile, 0>)<<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
-        Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, nullptr, nullptr, nullptr, nullptr, -1,
-        kJoinTileMax); note_launch(); }
-  { (f32 ? cmf_kernel<0, 32, 1> : cmf_kernel<0, 32, 0>)<<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
-                                                              J.oE, nullptr, nullptr, nullptr, nullptr, kJoinTileMax,
-                                                              INT64_MAX); note_launch(); }
-  join_aux();
-  exclusive_scan_i32(J.bE, bOff, K, d_total + 1, stmpK, d_err, s);
-  exclusive_scan_i32(J.oE, oOff, K, d_total + 2, stmpK, d_err, s);
-  cudaMemcpyAsync(h_scratch, d_total + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
-  const int64_t nBl = h_scratch[0], nOl = h_scratch[1];
-  int32_t* bList = A.take_n<int32_t>(nBl);
-  int32_t* oList = A.take_n<int32_t>(nOl);
-  if (!bList || !oList) return ST_OUT_OF_MEMORY;
-  fork_aux();
-  { (f32 ? cmf_kernel<1, kJoinTile, 1> : cmf_kernel<1, kJoinTile, 0>)<<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
-        Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, bOff, oOff, bList, oList, -1, kJoinTileMax); note_launch(); }
-  { (f32 ? cmf_kernel<1, 32, 1> : cmf_kernel<1, 32, 0>)<<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
-                                                              J.oE, bOff, oOff, bList, oList, kJoinTileMax,
-                                                              INT64_MAX); note_launch(); }
-  join_aux();
+  int32_t* bList = nullptr;
+  int32_t* oList = nullptr;
+  if (twoPass) {
+    fork_aux();
+    { (f32 ? cmf_kernel<0, kJoinTile, 1> : cmf_kernel<0, kJoinTile, 0>)<<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
+          Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, nullptr, nullptr, nullptr, nullptr, -1,
+          kJoinTileMax); note_launch(); }
+    { (f32 ? cmf_kernel<0, 32, 1> : cmf_kernel<0, 32, 0>)<<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                                J.oE, nullptr, nullptr, nullptr, nullptr, kJoinTileMax,
+                                                                INT64_MAX); note_launch(); }
+    join_aux();
+    exclusive_scan_i32(J.bE, bOff, K, d_total + 1, stmpK, d_err, s);
+    exclusive_scan_i32(J.oE, oOff, K, d_total + 2, stmpK, d_err, s);
+    cudaMemcpyAsync(h_scratch, d_total + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+    const int64_t nBl = h_scratch[0], nOl = h_scratch[1];
+    bList = A.take_n<int32_t>(nBl);
+    oList = A.take_n<int32_t>(nOl);
+    if (!bList || !oList) return ST_OUT_OF_MEMORY;
+    J.n_blist = nBl; J.n_olist = nOl;
+    fork_aux();
+    { (f32 ? cmf_kernel<1, kJoinTile, 1> : cmf_kernel<1, kJoinTile, 0>)<<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
+          Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, bOff, oOff, bList, oList, -1, kJoinTileMax); note_launch(); }
+    { (f32 ? cmf_kernel<1, 32, 1> : cmf_kernel<1, 32, 0>)<<<blocks_for_warps(K), kThreads, 0, sw>>>(Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE,
+                                                                J.oE, bOff, oOff, bList, oList, kJoinTileMax,
+                                                                INT64_MAX); note_launch(); }
+    join_aux();
+  } else {
+    // one pass (cmf_append_kernel) into lists sized from the last join's totals, or a
+    // first guess of 8 edges per pair and side; again at the counted sizes on overflow
+    CmfOut out{bOff, oOff, nullptr, nullptr, hintB > 0 ? hintB + hintB / 4 + 65536 : 8 * K + 65536,
+               hintO > 0 ? hintO + hintO / 4 + 65536 : 8 * K + 65536,
+               reinterpret_cast<unsigned long long*>(d_total + 1)};
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      bList = A.take_n<int32_t>(out.bCap);
+      oList = A.take_n<int32_t>(out.oCap);
+      if (!bList || !oList) return ST_OUT_OF_MEMORY;
+      out.bList = bList; out.oList = oList;
+      cudaMemsetAsync(d_total + 1, 0, 2 * sizeof(int64_t), s);
+      fork_aux();
+      { (f32 ? cmf_append_kernel<kJoinTile, 1> : cmf_append_kernel<kJoinTile, 0>)<<<blocks_for_tiles(K, kJoinTile), kThreads, 0, s>>>(
+            Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, out, -1, kJoinTileMax); note_launch(); }
+      { (f32 ? cmf_append_kernel<32, 1> : cmf_append_kernel<32, 0>)<<<blocks_for_warps(K), kThreads, 0, sw>>>(
+            Lb, Lo, J.b, J.o, J.cmbr, K, J.join_flag, J.bE, J.oE, out, kJoinTileMax, INT64_MAX); note_launch(); }
+      join_aux();
+      cudaMemcpyAsync(h_scratch, d_total + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA_ERROR;
+      J.n_blist = h_scratch[0]; J.n_olist = h_scratch[1];
+      if (J.n_blist <= out.bCap && J.n_olist <= out.oCap) break;
+      out.bCap = std::max<int64_t>(J.n_blist, 1);
+      out.oCap = std::max<int64_t>(J.n_olist, 1);
+    }
+  }
   mk->mark("join:cmf", s);
   // ---- J6 refine
   fork_aux();

@@ -167,11 +167,11 @@ const char* gcmfgh_status_string(gcmfgh_status s);
  * to the sweep only.  On the batched star workload the sweep measured faster (1.54 ms
  * against 1.78 ms for the MBR stages). */
 #define GCMFGH_TUNE_JOIN_SWEEP 8
-/* GCMFGH_TUNE_SWEEP_TWO_PASS: 1 runs the sweep as the reference does, a counting pass
- * and a writing pass (GPU_MBR.h:420-539); 0 (default) tests each polygon's range once and
- * writes the candidates as it finds them, into an array sized from the last join's
- * candidate count (again, at the counted size, when a join finds more).  The candidates,
- * sorted by (base, overlay), are the same. */
+/* GCMFGH_TUNE_SWEEP_TWO_PASS: 1 runs the join's MBR sweep and common-MBR edge filter as
+ * the reference does, a counting pass and then a writing pass (GPU_MBR.h:420-539,
+ * Join.h:157-287); 0 (default) runs each as one pass that writes what it finds into arrays
+ * sized from the last join's totals (again, at the counted sizes, when a join finds
+ * more).  Candidates, flags, counts and edge lists are the same. */
 #define GCMFGH_TUNE_SWEEP_TWO_PASS 9
 gcmfgh_status gcmfgh_set_tuning(gcmfgh_ctx* ctx, int key, int64_t value);
 

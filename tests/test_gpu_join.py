@@ -266,24 +266,27 @@ def test_clip_of_join_takes_join_edge_lists(engine):
     _clip_equal(engine, db, do, base, ovl)
 
 
-def test_one_pass_sweep_equals_two_pass_and_overflows(engine):
-    """The sweep's one-pass form (default) against its count-then-emit form, on a small
-    join and then on a larger one whose candidates outnumber the key array sized from the
-    small join's count (the pass runs again at the counted size); both against the oracle."""
+def test_one_pass_sweep_and_filter_equal_two_pass_and_overflow(engine):
+    """The join's one-pass sweep and common-MBR edge filter (default) against their
+    count-then-write forms, on a small join and then on a larger one whose candidates and
+    edge lists outnumber the arrays sized from the small join's totals (each pass runs
+    again at the counted sizes); every join field and the clip against the oracle."""
     import gcmfgh
     for n in (2000, 40000):
         base, ovl = synth.small_join(31, n)
         db, do = gcmfgh.DeviceLayer(base), gcmfgh.DeviceLayer(ovl)
         info = engine.join(db, do)
-        one = (engine.join_field("b").reshape(-1).copy(), engine.join_field("o").reshape(-1).copy())
+        one = {f: engine.join_field(f).reshape(-1).copy() for f in FIELDS}
         engine.set_tuning(sweep_two_pass=True)
         try:
             info2 = engine.join(db, do)
-            two = (engine.join_field("b").reshape(-1), engine.join_field("o").reshape(-1))
+            two = {f: engine.join_field(f).reshape(-1).copy() for f in FIELDS}
         finally:
             engine.set_tuning(sweep_two_pass=False)
         assert info == info2
-        assert np.array_equal(one[0], two[0]) and np.array_equal(one[1], two[1])
-        o = pyoracle.join(base, ovl)
-        assert np.array_equal(one[0], o.b) and np.array_equal(one[1], o.o)
+        for f in FIELDS:
+            assert np.array_equal(one[f], two[f]), f
+        db, do, info, _ = _join_equal(engine, base, ovl)
+        if n == 2000:
+            _clip_equal(engine, db, do, base, ovl)
     assert info["n_pairs"] > 2000 * 1.25 + 65536
