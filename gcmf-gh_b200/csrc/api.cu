@@ -704,6 +704,7 @@ gcmfgh_status gcmfgh_autotune_joined(gcmfgh_ctx* c, const gcmfgh_layer* b, const
       {&ClipParams::bin_grid, {1ll << 10, 1ll << 12, 1ll << 14, 1ll << 16, 1ll << 20, 1ll << 24}},
       {&ClipParams::tile_label_max, {0, 32, 64, 96, 128, 192, 256}},
       {&ClipParams::mid_label_min, {256, 512, 1024, 2048, 4096}},
+      {&ClipParams::big_label_min, {1ll << 15, 1ll << 16, 1ll << 17, 1ll << 18, 1ll << 19}},
       {&ClipParams::wide_label_min, {0, 1ll << 16, kNever}},
   };
   for (const Knob& k : knobs) {
