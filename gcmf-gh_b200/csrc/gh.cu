@@ -2538,12 +2538,12 @@ struct LabelArgs {
   int64_t tileLabelMax;       // rings up to: a tile of lanes per pair
   int64_t midLabelMin;        // rings above: a block per pair
   int64_t bigLabelMin;        // rings above: the grid path
-  const int64_t* midList;     // pairs for the block kernel
   const unsigned long long* midCount;
   unsigned long long* midNext; // work-stealing cursor of the block kernel
   int blockRunCap;            // runs the block kernel's shared run table holds (0: none)
-  // The one-thread and warp pairs in size order, largest first (label_order_kernel): the
-  // one-thread kernel takes order[0, nTile), the warp kernel order[nTile, nTile + nWarp).
+  // The one-thread, warp and block pairs in size order, largest first (label_order_kernel):
+  // the one-thread kernel takes order[0, nTile), the warp kernel order[nTile, nTile + nWarp),
+  // the block kernel the *midCount entries after those.
   const uint32_t* order;
   int64_t nTile, nWarp;
 };
@@ -2669,12 +2669,13 @@ __global__ void unpermute_offsets_kernel(const uint32_t* __restrict__ order, int
   regQ[k] = offQ[i];
 }
 
-// Sort keys of the one-thread and warp pairs: each class in 127 size buckets, largest
-// first (one-thread pairs 0..126, warp pairs 128..254, the rest 255), for one 8-bit
-// radix pass; the counts of the two classes go to cnt[0], cnt[1].
+// Sort keys of the pairs by labelling class and size, for one 8-bit radix pass: one-thread
+// pairs 0..84, warp pairs 85..169, block pairs 170..254 (85 size buckets each, largest
+// first; the block class on a log scale, so that its largest pairs start first and do not
+// trail the stage), the rest 255.  Class counts: cnt[2] one-thread, cnt[3] warp, cnt[0] block.
 __global__ void label_order_kernel(const int32_t* __restrict__ mP, const int32_t* __restrict__ mQ,
                                    const int32_t* __restrict__ status, int64_t K, int64_t tileMax, int64_t midMin,
-                                   uint64_t* __restrict__ key, uint32_t* __restrict__ val,
+                                   int64_t bigMin, uint64_t* __restrict__ key, uint32_t* __restrict__ val,
                                    unsigned long long* __restrict__ cnt) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K) return;
@@ -2683,12 +2684,17 @@ __global__ void label_order_kernel(const int32_t* __restrict__ mP, const int32_t
   uint64_t kk = 255;
   if (status[k] == 0 && slots <= midMin) {
     if (slots <= tl) {
-      kk = 126 - (uint64_t)((slots * 127) / (tl + 1));
-      atomicAdd(cnt, 1ull);
+      kk = 84 - (uint64_t)((slots * 85) / (tl + 1));
+      atomicAdd(cnt + 2, 1ull);
     } else {
-      kk = 254 - (uint64_t)(((slots - tl) * 127) / (midMin - tl + 1));
-      atomicAdd(cnt + 1, 1ull);
+      kk = 169 - (uint64_t)(((slots - tl) * 85) / (midMin - tl + 1));
+      atomicAdd(cnt + 3, 1ull);
     }
+  } else if (status[k] == 0 && slots <= bigMin) {
+    const double r = log2((double)slots / (double)midMin) / log2((double)bigMin / (double)midMin);
+    const int b = (int)fmin(84.0, fmax(0.0, 85.0 * r));
+    kk = 254 - (uint64_t)b;
+    atomicAdd(cnt, 1ull);
   }
   key[k] = kk;
   val[k] = (uint32_t)k;
@@ -2710,20 +2716,11 @@ label_trace_block_kernel(LabelArgs a) {
     const long long i = next;
     __syncthreads();
     if (i >= (long long)n) return;
-    label_trace_pair<EX>(g, a, a.midList[i]);
+    label_trace_pair<EX>(g, a, (int64_t)a.order[a.nTile + a.nWarp + i]);
     __syncthreads();
   }
 }
 
-// pairs for the block kernel (order does not matter: each pair has its own output region)
-__global__ void mid_label_list_kernel(const int32_t* __restrict__ mP, const int32_t* __restrict__ mQ,
-                                      const int32_t* __restrict__ status, int64_t K, int64_t midMin, int64_t bigMin,
-                                      int64_t* __restrict__ list, unsigned long long* __restrict__ n) {
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= K || status[k] != 0) return;
-  const int64_t slots = (int64_t)mP[k] + mQ[k];
-  if (slots > midMin && slots <= bigMin) list[atomicAdd(n, 1ull)] = k;
-}
 
 // ================================================================ grid path for huge pairs
 // Pairs whose merged rings exceed ClipParams::big_label_min slots are labelled and traced
@@ -3902,7 +3899,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     int64_t* offSQ = A.take_n<int64_t>(K);
     if (!okey || !okeyAlt || !ovalAlt || !otmp || !sortedP || !sortedQ || !offSP || !offSQ) return ST_OUT_OF_MEMORY;
     { label_order_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, D.status, K, std::max<int64_t>(prm.tile_label_max, 0),
-                                                           midMin, okey, oval, mcnt + 2); note_launch(); }
+                                                           midMin, prm.big_label_min, okey, oval, mcnt); note_launch(); }
     radix_sort_pairs(okey, oval, okeyAlt, ovalAlt, K, 8, otmp, d_err, s);
     { permute_sizes_kernel<<<blocks_for(K), kThreads, 0, s>>>(oval, K, regSizeP, regSizeQ, sortedP, sortedQ); note_launch(); }
     exclusive_scan_i64(sortedP, offSP, K, tot + 11, stK, d_err, s);
@@ -4055,12 +4052,8 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   { out_sizes_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, nrec, D.status, K, vcap, ccap); note_launch(); }
   exclusive_scan_i64(vcap, vOff, K, tot + 13, stK, d_err, s);
   exclusive_scan_i32(ccap, cOff, K, tot + 14, stK, d_err, s);
-  // the pairs for the block kernel (the one-thread and warp pairs' order and counts came
-  // with the ring layout; all counts are read with the output sizes)
-  int64_t* mlist = A.take_n<int64_t>(K);
-  if (!mlist) return ST_OUT_OF_MEMORY;
-  { mid_label_list_kernel<<<blocks_for(K), kThreads, 0, s>>>(mP, mQ, D.status, K, midMin, prm.big_label_min,
-                                                            mlist, mcnt); note_launch(); }
+  // the pairs of the one-thread, warp and block kernels, in order, and their counts came
+  // with the ring layout; the counts are read with the output sizes
   cudaMemcpyAsync(hs, tot + 13, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hs + 2, mcnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hs + 3, mcnt + 2, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
@@ -4077,7 +4070,7 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     LabelArgs la{D, K, mP, mQ, regP, regQ, regSizeP, regSizeQ, SP, SQ, oxy, vOff, vcap, ocsz, cOff, ccap, nc, nv,
-                 prm, d_err, prm.tile_label_max, midMin, prm.big_label_min, mlist, mcnt, mcnt + 1, 0, oval,
+                 prm, d_err, prm.tile_label_max, midMin, prm.big_label_min, mcnt, mcnt + 1, 0, oval,
                  nTile, nWarp};
     // long pairs: a block each, on the auxiliary stream when there is one, so they start
     // first and overlap the warp-per-pair kernel instead of trailing it
