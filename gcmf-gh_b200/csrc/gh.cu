@@ -1660,7 +1660,7 @@ template <> struct TileOf<1> { using type = SoloGroup; };
 
 // Block-wide versions over shared scratch (kBlockLabelThreads / 32 warps); each call
 // begins with a barrier so the scratch of the previous call is free.
-constexpr int kBlockLabelThreads = 256;
+constexpr int kBlockLabelThreads = 512;
 // Dynamic shared memory of the block labelling kernel: the trace's run table of pairs with
 // up to 8,192 runs (two blocks per SM at its register budget).
 constexpr int kBlockRunTableBytes = 96 * 1024;
