@@ -47,7 +47,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarpsPerBlock = kThreads / 32;
-constexpr int kChunk = 64;             // edge pairs per warp work unit (2 x 32 lanes)
+constexpr int kChunk = 32;             // edge pairs per warp work unit (one per lane; 64 and 128 measured slower)
 constexpr int64_t kFirstRecordCap = 1 << 22;   // records held by a fused count + emit without a hint
 constexpr int kFilterTile = 4;         // lanes per small pair in the edge filter
 constexpr int64_t kFilterTileMax = 64; // ring size up to which the narrow tiles take a pair
