@@ -743,12 +743,14 @@ struct RingSet {
 // per pair: ring size, region offset (ring + room for added vertices)
 __global__ void pair_ring_kernel(const int64_t* __restrict__ eoff, const int64_t* __restrict__ vpos,
                                  const int32_t* __restrict__ n, const int32_t* __restrict__ nrec,
-                                 const int32_t* __restrict__ status, int64_t K, int64_t nE, int64_t vtot,
+                                 const int32_t* __restrict__ status, int64_t K, int64_t nE,
+                                 const int64_t* __restrict__ insTot,
                                  int32_t* __restrict__ m, int64_t* __restrict__ regSize,
                                  unsigned long long* __restrict__ ringTot) {
   int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
   unsigned long long mm = 0;
   if (k < K) {
+    const int64_t vtot = nE + *insTot;                      // slots of the side's merged rings
     int64_t e0 = eoff[k], e1 = e0 + (status[k] == 2 ? 0 : n[k]);
     int64_t v0 = e0 < nE ? vpos[e0] : vtot, v1 = e1 < nE ? vpos[e1] : vtot;
     mm = status[k] == 0 ? (unsigned long long)(v1 - v0) : 0ull;
@@ -3858,9 +3860,16 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   exclusive_scan_i32(insQ, insBaseQ, nEQ, tot + 10, stE, d_err, s);
   { edge_slots_kernel<<<blocks_for(nEP), kThreads, 0, s>>>(insBaseP, nEP, vposP); note_launch(); }
   { edge_slots_kernel<<<blocks_for(nEQ), kThreads, 0, s>>>(insBaseQ, nEQ, vposQ); note_launch(); }
-  cudaMemcpyAsync(hs + 2, tot + 9, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-  if (!sync()) return ST_CUDA_ERROR;
-  const int64_t nInsP = hs[2], nInsQ = hs[3], vtotP = nEP + nInsP, vtotQ = nEQ + nInsQ;
+  // Sizes: the record export reads the exact ones back; the clip takes bounds instead
+  // and saves the two host round trips (a record inserts at most one vertex per side).
+  const bool exactSizes = ex != nullptr;
+  int64_t nInsP = nR, nInsQ = nR;
+  if (exactSizes) {
+    cudaMemcpyAsync(hs + 2, tot + 9, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return ST_CUDA_ERROR;
+    nInsP = hs[2];
+    nInsQ = hs[3];
+  }
   int64_t* insListP = A.take_n<int64_t>(nInsP);
   int64_t* insListQ = A.take_n<int64_t>(nInsQ);
   int32_t* mP = A.take_n<int32_t>(K);
@@ -3873,11 +3882,11 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   if (nR > 0)
     { record_scatter_kernel<<<blocks_for(nR), kThreads, 0, s>>>(R, nR, eoffP, eoffQ, D.status, insBaseP, curP,
                                                               insListP, insBaseQ, curQ, insListQ); note_launch(); }
-  unsigned long long* ringTot = reinterpret_cast<unsigned long long*>(tot + 13);
+  unsigned long long* ringTot = reinterpret_cast<unsigned long long*>(tot + 6);
   cudaMemsetAsync(ringTot, 0, sizeof(unsigned long long), s);
-  { pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffP, vposP, D.nP, nrec, D.status, K, nEP, vtotP, mP,
+  { pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffP, vposP, D.nP, nrec, D.status, K, nEP, tot + 9, mP,
                                                       regSizeP, ringTot); note_launch(); }
-  { pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffQ, vposQ, D.nQ, nrec, D.status, K, nEQ, vtotQ, mQ,
+  { pair_ring_kernel<<<blocks_for(K), kThreads, 0, s>>>(eoffQ, vposQ, D.nQ, nrec, D.status, K, nEQ, tot + 10, mQ,
                                                       regSizeQ, ringTot); note_launch(); }
   // The one-thread and warp labelling kernels take their pairs in size order (largest
   // first, label_order_kernel), and the ring regions are laid out in that order, so that
@@ -3909,10 +3918,16 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
     exclusive_scan_i64(regSizeP, regP, K, tot + 11, stK, d_err, s);
     exclusive_scan_i64(regSizeQ, regQ, K, tot + 12, stK, d_err, s);
   }
-  cudaMemcpyAsync(hs, tot + 11, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-  if (!sync()) return ST_CUDA_ERROR;
-  const int64_t regTotP = hs[0], regTotQ = hs[1];
-  C.n_ring_vertices = hs[2];
+  // region slots: merged rings (edges + insertions) + 2 + 2 records per valid pair
+  int64_t regTotP = nEP + nInsP + 2 * K + 2 * nR, regTotQ = nEQ + nInsQ + 2 * K + 2 * nR;
+  if (exactSizes) {
+    cudaMemcpyAsync(hs, tot + 11, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hs + 2, tot + 6, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (!sync()) return ST_CUDA_ERROR;
+    regTotP = hs[0];
+    regTotQ = hs[1];
+    C.n_ring_vertices = hs[2];
+  }
   C.n_records = nR;
   auto take_ring = [&](int64_t n, RingSet& S) {
     const int64_t slots = (std::max<int64_t>(n, 1) + 15) & ~int64_t(15);
@@ -4057,7 +4072,9 @@ int run_clip(const LayerDev& Lb, const LayerDev& Lo, const int32_t* d_pid, const
   cudaMemcpyAsync(hs, tot + 13, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hs + 2, mcnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hs + 3, mcnt + 2, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hs + 5, tot + 6, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (!sync()) return ST_CUDA_ERROR;
+  C.n_ring_vertices = hs[5];
   double* oxy = A.take_n<double>(2 * hs[0]);
   int32_t* ocsz = A.take_n<int32_t>(hs[1]);
   const int64_t nMid = hs[2], nTile = hs[3], nWarp = hs[4];
