@@ -268,7 +268,11 @@ int gcmfgh_server::run_batch(std::vector<std::shared_ptr<Request>>& batch, int64
                                                                      keys, obits); note_launch(); }
     radix_sort_pairs(keys, vals, kAlt, vAlt, K, ((obits + qbits + 7) / 8) * 8, rtmp, d_err, s);
     cudaEventRecord(ev[2], s);
-    st = join_from_keys(Lq, resident(), keys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, nullptr, aux);
+    // The common-MBR filter counts, then writes (two passes): a batch's edge lists vary too
+    // much in size (queries of up to tens of thousands of vertices) for a one-pass capacity
+    // taken from the last batch, and every overflow would repeat the pass.
+    st = join_from_keys(Lq, resident(), keys, K, obits, A, J, d_total, d_cnt, d_err, h_scratch, s, nullptr, aux,
+                        0, 0, true);
     if (st != ST_OK) return st;
     cudaEventRecord(ev[3], s);
     if (J.n_clip > 0) {
