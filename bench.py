@@ -901,13 +901,15 @@ def run_ours(args, rank, world, local):
     del db, do, flush, pinned
     torch.cuda.empty_cache()
     if rank == 0:
-        if not args.no_serve:
+        # the one-GPU sections (serving, single large pair, multi-component pairs, degeneracy
+        # batch) run at N = 1 only: under torchrun the other ranks' GPUs would wait idle
+        if not args.no_serve and world == 1:
             line["serving"] = serve_measure(local)
-        if not args.no_large_pair:
+        if not args.no_large_pair and world == 1:
             line["large_pair"] = large_pair_measure(local)
-        if not args.no_multi:
+        if not args.no_multi and world == 1:
             line["multi_component"] = multi_measure(local)
-        if not args.no_precision:
+        if not args.no_precision and world == 1:
             line["precision"] = precision_measure(local, total=args.precision_pairs, chunk=args.precision_chunk,
                                                   check_all_degenerate=args.precision_check_all)
         if world == 1 and not args.no_cpu_baseline:
